@@ -1,0 +1,402 @@
+#!/usr/bin/env python
+"""Benchmark of the counting path: k-mers counted per second, bit-exact.
+
+Default workload (N=1): the single large job -- a seeded 100 Mbp genome with
+5% from 200 repeat families, 30x coverage of 150 bp reads (~20M reads, ~6.3 GB
+FASTQ), 1% substitutions, k = 31, the reference's Bloom singleton split with
+its filter sizing, min count 2, outputs sorted records + histogram.  Synthetic
+input of that shape stands in for sequencing data (the reference measures no
+public dataset).
+
+A step is one counting job over the whole FASTQ:
+  value -- input resident in HBM (kc_input_upload once), device time of the
+           job from CUDA events on its stream (sum over the timed steps);
+  e2e   -- the same job through the C ABI from pinned host buffers: upload,
+           counting, and the sorted records + histogram copied back, timed by
+           the host clock.
+--impl reference times the reference's own CPU programs (compiled from its
+sources into oracle/_ref) on a bounded sample of the same workload.
+
+Multi-GPU: the path is run as independent replicas (one job per GPU); value is
+all replicas' k-mers over the slowest replica's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+U32 = 0xFFFFFFFF
+METRIC = "k-mers counted/s (bit-exact)"
+MEMORY_GB = 64          # reference <memory_limit_gb>: sizes the Bloom filters
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+
+def make_input(scale: float, kc):
+    """The large-job FASTQ, written straight into pinned host memory."""
+    import ctypes as C
+    import numpy as np
+    import ktcountermemorygreedy_b200.synth as S
+    genome_len = max(1_000_000, int(100_000_000 * scale))
+    n_reads = S.large_job_reads(30.0, genome_len)
+    size = S.reads_size(2, n_reads, (150, 150))
+    p = C.c_void_p()
+    kc._check(kc.lib().kc_host_alloc(size, C.byref(p)))
+    buf = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint8)), shape=(size,))
+    g = S.large_job_genome(genome_len)
+    fq = S.reads(g, 2, n_reads, (150, 150), 0.01, 0.0, out=buf)
+    return fq, p, genome_len, n_reads
+
+
+JOB = dict(k=31, count_max=U32, bloom=True, memory_gb=MEMORY_GB, min_count=2, hist_min=2, hist_max=10000)
+
+
+def algorithmic_bytes(phase: str, r):
+    """Bytes a stage must move at minimum (per launch), from the unit costs:
+    S FASTQ bytes, O occurrences, h/l the non-FIRST/FIRST list lengths,
+    cap table slots, U distinct k-mers."""
+    S, O = r.input_bytes, r.occurrences
+    if phase == "count_pass":          # FASTQ + Bloom words read (16 B) + list write (8 B)
+        return S + 24 * O if r.low_len + r.high_len else S + 16 * O
+    if phase == "insert_high":         # list read (8 B) + slot key read and count update (16 B)
+        return 24 * r.high_len
+    if phase == "merge_low":
+        return 24 * r.low_len
+    if phase == "compact":
+        return 16 * r.table_capacity + 12 * r.n_records_total
+    if phase == "sort":
+        return math.ceil(2 * 31 / 8) * 24 * r.n_records_total
+    if phase in ("census", "scan"):
+        return S
+    return 0
+
+
+def traffic_for(phase: str, r):
+    """DRAM bytes per launch of the stage's kernel from a committed ncu summary
+    (profiles/dram_traffic.json), scaled by the occurrences it processed."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p)).get(phase)
+    if not d:
+        return None
+    per_occ = d["dram_bytes"] / max(1, d["occurrences"])
+    return int(per_occ * r.occurrences)
+
+
+# ---------------------------------------------------------------------------
+# the reference's CPU programs
+# ---------------------------------------------------------------------------
+
+def reference_run(fastq_path: str, threads: int, mem_gb: int, tmp: str):
+    """kmer_counter + histogram_tool precise + dump_tool precise --sort, as the
+    reference is used; returns (wall seconds, occurrences)."""
+    ref = os.path.join(ROOT, "oracle", "_ref")
+    d = os.path.join(tmp, "t")
+    shutil.rmtree(d, ignore_errors=True)
+    os.makedirs(d)
+    t0 = time.perf_counter()
+    p = subprocess.run([os.path.join(ref, "kmer_counter"), fastq_path, "31", str(threads), str(mem_gb), d, "1024",
+                        "2", str(U32), str(U32)], capture_output=True, text=True)
+    if p.returncode != 0:
+        raise RuntimeError(f"reference kmer_counter failed: {p.stderr[-500:]}")
+    subprocess.run([os.path.join(ref, "histogram_tool"), "precise", d, str(threads), str(mem_gb),
+                    os.path.join(tmp, "h.tsv"), "2", "10000"], check=True, capture_output=True)
+    subprocess.run([os.path.join(ref, "dump_tool"), "precise", d, str(threads), str(mem_gb),
+                    os.path.join(tmp, "d.txt"), "1", str(U32), "--sort"], check=True, capture_output=True)
+    wall = time.perf_counter() - t0
+    occ = 0
+    for line in p.stdout.splitlines():
+        if line.startswith("Total read k-mer count:"):
+            occ = int(line.split(":")[1])
+    return wall, occ
+
+
+def reference_sample(sample_reads: int, tmp: str):
+    """First `sample_reads` reads of the large job's stream (same genome and
+    read generator) written to a file."""
+    import ktcountermemorygreedy_b200.synth as S
+    g = S.large_job_genome(100_000_000)
+    fq = S.reads(g, 2, sample_reads, (150, 150), 0.01, 0.0)
+    path = os.path.join(tmp, "sample.fq")
+    fq.tofile(path)
+    return path, len(fq)
+
+
+def cpu_info():
+    model = ""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return os.cpu_count() or 1, model
+
+
+def run_reference_arm(args):
+    threads, model = cpu_info()
+    threads = max(6, threads)
+    mem = int(os.environ.get("KC_REF_MEM_GB", "32"))
+    with tempfile.TemporaryDirectory() as tmp:
+        path, nbytes = reference_sample(args.ref_reads, tmp)
+        for _ in range(args.warmup):
+            reference_run(path, threads, mem, tmp)
+        walls, occ = [], 0
+        for _ in range(args.steps):
+            w, occ = reference_run(path, threads, mem, tmp)
+            walls.append(w)
+    t = sum(walls)
+    value = occ * args.steps / t
+    sample = f"first {args.ref_reads} reads of the large job ({nbytes} B FASTQ, {occ} k-mers), counter + precise tools"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "k-mers/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": "single large job (100 Mbp genome, 5% repeats, 30x 150 bp, k=31, Bloom, min count 2)",
+                   "sample_reads": args.ref_reads},
+        "cpu_baseline": {"value": value, "unit": "k-mers/s", "cores": threads, "kind": "reference",
+                         "sample": sample, "cpu": model},
+        "e2e": {"value": value, "unit": "k-mers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, world: int) -> float:
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_ours(args):
+    world, rank, local = dist_setup(args)
+    import numpy as np
+    import ktcountermemorygreedy_b200 as kc
+
+    fq, pinned, genome_len, n_reads = make_input(args.scale, kc)
+    counter = kc.KmerCounter(device=local, max_inflight_jobs=1)
+    inp = counter.upload([fq])
+    for _ in range(args.warmup):
+        counter.count(input=inp, keep_records=False, **JOB)
+    barrier(world)
+    sampler = ClockSampler(local)
+    sampler.start()
+    l0 = kc.kernel_launches()
+    results = []
+    for _ in range(args.steps):
+        results.append(counter.count(input=inp, keep_records=False, **JOB))
+    launches = kc.kernel_launches() - l0
+    clocks = sampler.stop()
+    barrier(world)
+    dev_ms = sum(r.device_ms for r in results)
+    occ = sum(r.occurrences for r in results)
+    t_max = max_over_ranks(dev_ms, world)
+    occ_all = sum_over_ranks(occ, world)
+    value = occ_all / (t_max / 1000.0)
+
+    # end to end through the C ABI from pinned host buffers
+    e2e_val, h2d, d2h = None, 0, 0
+    if args.e2e_steps > 0:
+        walls, occ_e = [], 0
+        r = None
+        for _ in range(args.e2e_steps):
+            t0 = time.perf_counter()
+            r = counter.count([fq], keep_records=True, **JOB)
+            walls.append(time.perf_counter() - t0)
+            occ_e += r.occurrences
+        h2d = len(fq)
+        d2h = len(r.keys) * 12 + r.hist.nbytes
+        w = max_over_ranks(sum(walls), world)
+        e2e_val = sum_over_ranks(occ_e, world) / w
+
+    # roofline of the dominant single-kernel stage
+    phases = kc.PHASES
+    mean_ms = [statistics.mean(r.phase_ms[i] for r in results) for i in range(8)]
+    single = [i for i in range(8) if results[0].phase_launches[i] == 1 and mean_ms[i] > 0]
+    dom = max(single, key=lambda i: mean_ms[i]) if single else max(range(8), key=lambda i: mean_ms[i])
+    r0 = results[-1]
+    alg = algorithmic_bytes(phases[dom], r0)
+    achieved = alg / (mean_ms[dom] / max(1, r0.phase_launches[dom]) / 1000.0) / 1e9
+    peak, peak_kind = peaks()
+    roof = {"bound": "hbm", "kernel": phases[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic_for(phases[dom], r0),
+            "algorithmic_bytes": alg}
+    stages = {phases[i]: {"ms": mean_ms[i], "launches": int(r0.phase_launches[i]),
+                          "alg_GBps": (algorithmic_bytes(phases[i], r0) / (mean_ms[i] / 1000.0) / 1e9)
+                          if mean_ms[i] > 0 else None} for i in range(8) if mean_ms[i] > 0}
+
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_baseline:
+        try:
+            threads, model = cpu_info()
+            with tempfile.TemporaryDirectory() as tmp:
+                path, nbytes = reference_sample(args.ref_reads, tmp)
+                w, o = reference_run(path, max(6, threads), int(os.environ.get("KC_REF_MEM_GB", "32")), tmp)
+            cpu = {"value": o / w, "unit": "k-mers/s", "cores": max(6, threads), "kind": "reference",
+                   "sample": f"first {args.ref_reads} reads of the workload ({nbytes} B, {o} k-mers), "
+                             f"counter + precise tools, {model}"}
+        except Exception as e:   # the baseline is reported, never required
+            cpu = {"value": None, "unit": "k-mers/s", "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
+
+    counter.free_input(inp)
+    counter.close()
+    kc.lib().kc_host_free(pinned)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "k-mers/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": "single large job (100 Mbp genome, 5% repeats from 200 families, 30x 150 bp, "
+                                   "1% errors, k=31, Bloom singleton filter, min count 2)",
+                       "genome_bp": genome_len, "reads": n_reads, "fastq_bytes": len(fq),
+                       "occurrences_per_step": results[0].occurrences, "records": results[0].n_records_total,
+                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (FASTQ > 126 MB)",
+                       "memory_gb": MEMORY_GB, "scale": args.scale},
+            "e2e": {"value": e2e_val, "unit": "k-mers/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": int(launches),
+            "stages": stages,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="genome size factor (1.0 = the 100 Mbp workload)")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--ref-reads", type=int, default=1_000_000)
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return
+        run_reference_arm(args)
+        return
+    run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,205 @@
+/*
+ * kc.h -- C ABI of the B200 k-mer counter (libkc.so).
+ *
+ * The reference (ScorchShana/KTCounterMemoryGreedy) has no library API: its
+ * boundary is three programs and the files they exchange.  These entry points
+ * are what a binding to its counting path needs, one per step of that path:
+ *
+ *   kc_open / kc_close     replace process start-up and the global state of
+ *                          src/main.cpp:481-633 (argv parsing, thread split,
+ *                          memory pool of memory_limit GB)
+ *   kc_submit / kc_wait    replace process_main<N> (src/main.cpp:246-478):
+ *                          FASTQ in -> exact canonical counts
+ *   kc_result              the precise outputs of tool/histogram_tool.cpp
+ *                          (run_precise_histogram_tool_impl :735) and
+ *                          tool/dump_tool.cpp (run_precise_impl :1202,
+ *                          --sort), as memory instead of text files
+ *   kc_write_tmpdir        the tmp_dir files infos.bin / high.bin / low.bin
+ *                          (src/main.cpp:590-597, src/FinalDrainWriter.h:71-146,
+ *                          src/ExportWriter.h:296-313) that the unmodified
+ *                          reference tools read
+ *
+ * Conventions: every call returns a status code (KC_OK = 0) and never exits
+ * the process; kc_last_error() describes the last failure of the calling
+ * thread.  Inputs are caller-owned and only read.  Result memory is owned by
+ * the job and stays valid until kc_release() or kc_close().  A handle may be
+ * used from several host threads; jobs submitted to one handle run
+ * concurrently on the device (one CUDA stream each), admitted in submission
+ * order as device memory frees up.
+ *
+ * k-mer words: a k-mer (k <= 32) is the reference's kmer<1> word
+ * (src/kmer.h:15): base i of the printed canonical string sits at bit
+ * 64 - 2k + 2i, padding bits are zero.  Record arrays are sorted in
+ * printed-string order (the order of dump_tool --sort).
+ */
+#ifndef KC_H
+#define KC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KC_OK 0
+#define KC_ERR_INVALID 1     /* bad argument */
+#define KC_ERR_CUDA 2        /* CUDA runtime failure */
+#define KC_ERR_NOMEM 3       /* device or pinned host allocation failed */
+#define KC_ERR_TIMEOUT 4     /* kc_wait ran out of time; the job keeps running */
+#define KC_ERR_NOT_FOUND 5   /* unknown job id */
+#define KC_ERR_DEVICE 6      /* a kernel reported an error flag */
+#define KC_ERR_IO 7          /* file write failed */
+#define KC_ERR_NO_DEVICE 8   /* no usable CUDA device */
+#define KC_ERR_FAILED 9      /* the job failed; kc_last_error after kc_wait says why */
+
+typedef struct kc_handle kc_handle;
+typedef struct kc_input kc_input;
+typedef uint64_t kc_job_id;
+
+typedef struct {
+    int32_t device;               /* CUDA device ordinal */
+    uint32_t max_inflight_jobs;   /* jobs on the device at once (streams); 0 -> 4 */
+    uint64_t hbm_budget_bytes;    /* device memory jobs may reserve; 0 -> 90% of free memory */
+    uint64_t reserved[6];
+} kc_config;
+
+typedef struct {
+    const char *data;             /* one FASTQ file, uncompressed, in host memory */
+    uint64_t size;
+} kc_buffer;
+
+typedef struct {
+    /* input: either host files or a device-resident input from kc_input_upload */
+    const kc_buffer *files;
+    uint32_t n_files;
+    uint32_t k;                   /* 1..32 (reference: <k_len>) */
+    const kc_input *input;        /* non-NULL: use this resident input, ignore files */
+    uint32_t count_max;           /* saturation of counts (reference [count_max], default 255) */
+    uint32_t bloom;               /* 1: reference Bloom singleton split (src/BloomFilter.h) */
+    uint64_t memory_gb;           /* reference <memory_limit_gb>, sizes the Bloom filters */
+    uint32_t filter_min;          /* reference [filter_min]/[filter_max], applied by */
+    uint32_t filter_max;          /*   kc_write_tmpdir to the high.bin records */
+    uint32_t min_count;           /* records kept: min_count <= count <= max_count */
+    uint32_t max_count;
+    uint32_t hist_min;            /* histogram bins hist_min..hist_max */
+    uint32_t hist_max;
+    uint32_t top_n;               /* 0: no top-N query */
+    uint32_t want_le2;            /* 1: the records with count <= 2 */
+    uint32_t keep_records;        /* 1: copy the sorted records to host memory */
+    uint32_t reserved0;
+    uint64_t reserved[6];
+} kc_job;
+
+typedef struct {
+    uint64_t n_records;           /* sorted records (if keep_records) */
+    const uint64_t *keys;
+    const uint32_t *counts;
+    uint64_t hist_len;            /* hist[i] = k-mers with count hist_min + i */
+    const int64_t *hist;
+    uint64_t n_top;               /* top_n by count desc, then printed string asc */
+    const uint64_t *top_keys;
+    const uint32_t *top_counts;
+    uint64_t n_le2;               /* records with count <= 2, printed-string order */
+    const uint64_t *le2_keys;
+    const uint32_t *le2_counts;
+    uint64_t occurrences;         /* k-mer occurrences counted */
+    uint64_t distinct;            /* distinct canonical k-mers */
+    uint64_t low_only;            /* Bloom mode: k-mers seen once and only as FIRST */
+    uint64_t table_capacity;      /* slots of the counting table */
+    double device_ms;             /* device time of the counting pipeline */
+    double queue_ms;              /* submission -> start */
+    double run_ms;                /* start -> end (host clock) */
+    /* device time per stage (CUDA events on the job's stream):
+     * [0] newline census + tile line numbers, [1] SCAN pass, [2] INSERT or
+     * BLOOM pass, [3] insert of the non-FIRST list, [4] merge of the FIRST
+     * list, [5] compaction + histogram, [6] radix sort, [7] queries */
+    double phase_ms[8];
+    uint64_t phase_launches[8];   /* kernel launches per stage */
+    uint64_t low_len;             /* Bloom mode: FIRST occurrences */
+    uint64_t high_len;            /* Bloom mode: other occurrences */
+    uint64_t input_bytes;         /* FASTQ bytes of the job */
+    uint64_t n_records_total;     /* records on the device (also when keep_records = 0) */
+} kc_result_t;
+
+/* Kernel launches issued by this process so far (all handles). */
+uint64_t kc_kernel_launches(void);
+
+/* ---- handle ------------------------------------------------------------ */
+int kc_open(const kc_config *cfg, kc_handle **out);
+void kc_close(kc_handle *h);
+const char *kc_last_error(void);
+void kc_job_defaults(kc_job *job);   /* reference defaults: count_max 255, filter 2..u32max, ... */
+
+/* ---- device-resident input --------------------------------------------- */
+int kc_input_upload(kc_handle *h, const kc_buffer *files, uint32_t n_files, kc_input **out);
+void kc_input_free(kc_handle *h, kc_input *in);
+
+/* ---- jobs ---------------------------------------------------------------- */
+int kc_submit(kc_handle *h, const kc_job *job, kc_job_id *id);
+int kc_wait(kc_handle *h, kc_job_id id, int32_t timeout_ms);   /* <0: no limit */
+int kc_result(kc_handle *h, kc_job_id id, kc_result_t *out);
+int kc_write_tmpdir(kc_handle *h, kc_job_id id, const char *dir);
+int kc_release(kc_handle *h, kc_job_id id);
+
+/* Batched jobs: every job of the array is counted in one set of device passes
+ * (one persistent extraction kernel over all samples' tiles, per-sample
+ * tables in one arena).  Bloom mode is not available here.  ids[i] is the
+ * id of jobs[i]; results are read per id as for kc_submit. */
+int kc_submit_batch(kc_handle *h, const kc_job *jobs, uint32_t n_jobs, kc_job_id *ids);
+
+/* ---- pinned host memory (for zero-copy-speed uploads) -------------------- */
+int kc_host_alloc(uint64_t bytes, void **p);
+int kc_host_free(void *p);
+
+/* ---- single steps of the path, for tests and tools ----------------------- */
+
+/* Canonical k-mer occurrences of one FASTQ file (src/FastqReader.h:559-698
+ * record splitting + src/GetKmer.h:58-130 extraction), in no particular
+ * order.  *n_out receives the number of occurrences even if it exceeds cap. */
+int kc_extract_kmers(const char *fastq, uint64_t len, uint32_t k, uint64_t *out, uint64_t cap,
+                     uint64_t *n_out);
+
+/* out[5i..5i+4] = XXH3_128bits.low64, .high64, XXH3_64bits, rapidhash,
+ * komihash(seed 0) of the 8-byte word keys[i] (include/xxhash.h 0.8.3,
+ * include/rapidhash.h V3, include/komihash.h 5.29 as called at
+ * src/BloomFilter.h:217, tool/FlatConcurrentHashMap.h:95,
+ * src/ConcurrentMap.h:143-144). */
+int kc_hash_kmers(const uint64_t *keys, uint64_t n, uint64_t *out);
+
+/* Stable LSD radix sort of (key, count) pairs on the low `bits` bits of the
+ * keys (sort/ExportRecordRadixSort.h:225-269, tool/dump_tool.cpp:373-454). */
+int kc_sort_records(uint64_t *keys, uint32_t *counts, uint64_t n, uint32_t bits);
+
+/* Pre-pass statistics and Bloom sizing of a job (src/main.cpp:262-335 with
+ * get_MAX_BLOOM_FILTER_CAPACITY :41 and calculate_bloom_filter_capacity :111):
+ * raw root-prefix counts over the sample, average quality, capacities. */
+int kc_bloom_plan(const kc_buffer *files, uint32_t n_files, uint32_t k, uint64_t memory_gb,
+                  uint32_t *prefix_counts /*256*/, uint32_t *avg_quality,
+                  uint64_t *capacities /*256*/, uint64_t *max_capacity);
+
+/* The reference's Bloom filter sizing alone (host arithmetic, no device):
+ * src/main.cpp:41-57 and :111-153 applied to raw pre-pass root-prefix counts
+ * (counts below 1000 are raised to 1000 as src/main.cpp:306-315 does). */
+int kc_plan_bloom(const uint32_t *raw_prefix_counts /*256*/, uint32_t avg_quality, uint64_t est_file_size,
+                  uint64_t memory_gb, uint32_t k, uint64_t *capacities /*256*/, uint64_t *max_capacity);
+
+/* The precise merge of the reference tools (tool/histogram_tool.cpp:735-791
+ * with tool/LowFrequencyQueryThreadPool.h:186-240; tool/dump_tool.cpp:1202-1272)
+ * on the device: high.bin records (keys, counts) and low.bin k-mers become
+ * exact counts -- min(high + 1, count_max) for a k-mer in both files, the
+ * high count for one only in high.bin, 1 for one only in low.bin.  Records
+ * with min_count <= count <= max_count are written sorted in printed-string
+ * order (*n_out receives their number even if it exceeds out_cap); hist
+ * (hist_max - hist_min + 1 entries, may be NULL) receives the histogram of
+ * all merged counts. */
+int kc_merge_records(const uint64_t *high_keys, const uint32_t *high_counts, uint64_t n_high,
+                     const uint64_t *low_keys, uint64_t n_low, uint32_t k, uint32_t count_max,
+                     uint32_t min_count, uint32_t max_count, uint32_t hist_min, uint32_t hist_max,
+                     uint64_t *out_keys, uint32_t *out_counts, uint64_t out_cap, uint64_t *n_out,
+                     int64_t *hist);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,412 @@
+"""B200 k-mer counter: Python binding of libkc.so (include/kc.h).
+
+The reference (ScorchShana/KTCounterMemoryGreedy) is driven through three
+programs: ``kmer_counter`` (src/main.cpp:481) writes ``tmp_dir/{infos,high,
+low}.bin``; ``histogram_tool precise`` (tool/histogram_tool.cpp:905) and
+``dump_tool precise --sort`` (tool/dump_tool.cpp:1447) turn those files into
+the exact count histogram and the sorted ``KMER\\tcount`` dump.  This module
+mirrors that surface on top of the C ABI:
+
+* :class:`KmerCounter` -- a handle (``kc_open``); ``count()`` runs one job
+  (FASTQ bytes in, exact sorted records + histogram + queries out),
+  ``submit()``/``wait()`` run jobs concurrently, ``count_batch()`` counts many
+  samples in one set of device passes.
+* :func:`histogram_text` / :func:`dump_text` -- the text outputs of the two
+  reference tools for a result.
+* :func:`kmer_string` -- ``kmer_to_buf`` (tool/dump_tool.cpp:103).
+
+k-mer words follow the reference's ``kmer<1>`` layout (src/kmer.h:15): base i
+of the printed canonical string at bit ``64 - 2k + 2i``.
+
+There is no CPU path: every call runs on the GPU through libkc.so and raises
+:class:`KcError` when the library or a device is unavailable.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Iterable, List, Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libkc.so")
+
+KC_OK = 0
+ERRORS = {
+    1: "KC_ERR_INVALID", 2: "KC_ERR_CUDA", 3: "KC_ERR_NOMEM", 4: "KC_ERR_TIMEOUT",
+    5: "KC_ERR_NOT_FOUND", 6: "KC_ERR_DEVICE", 7: "KC_ERR_IO", 8: "KC_ERR_NO_DEVICE",
+    9: "KC_ERR_FAILED",
+}
+U32_MAX = 0xFFFFFFFF
+
+
+class KcError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class kc_config(C.Structure):
+    _fields_ = [("device", C.c_int32), ("max_inflight_jobs", C.c_uint32),
+                ("hbm_budget_bytes", C.c_uint64), ("reserved", C.c_uint64 * 6)]
+
+
+class kc_buffer(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("size", C.c_uint64)]
+
+
+class kc_job(C.Structure):
+    _fields_ = [("files", C.POINTER(kc_buffer)), ("n_files", C.c_uint32), ("k", C.c_uint32),
+                ("input", C.c_void_p), ("count_max", C.c_uint32), ("bloom", C.c_uint32),
+                ("memory_gb", C.c_uint64), ("filter_min", C.c_uint32), ("filter_max", C.c_uint32),
+                ("min_count", C.c_uint32), ("max_count", C.c_uint32), ("hist_min", C.c_uint32),
+                ("hist_max", C.c_uint32), ("top_n", C.c_uint32), ("want_le2", C.c_uint32),
+                ("keep_records", C.c_uint32), ("reserved0", C.c_uint32), ("reserved", C.c_uint64 * 6)]
+
+
+class kc_result_t(C.Structure):
+    _fields_ = [("n_records", C.c_uint64), ("keys", C.POINTER(C.c_uint64)), ("counts", C.POINTER(C.c_uint32)),
+                ("hist_len", C.c_uint64), ("hist", C.POINTER(C.c_int64)),
+                ("n_top", C.c_uint64), ("top_keys", C.POINTER(C.c_uint64)), ("top_counts", C.POINTER(C.c_uint32)),
+                ("n_le2", C.c_uint64), ("le2_keys", C.POINTER(C.c_uint64)), ("le2_counts", C.POINTER(C.c_uint32)),
+                ("occurrences", C.c_uint64), ("distinct", C.c_uint64), ("low_only", C.c_uint64),
+                ("table_capacity", C.c_uint64), ("device_ms", C.c_double), ("queue_ms", C.c_double),
+                ("run_ms", C.c_double), ("phase_ms", C.c_double * 8), ("phase_launches", C.c_uint64 * 8),
+                ("low_len", C.c_uint64), ("high_len", C.c_uint64), ("input_bytes", C.c_uint64),
+                ("n_records_total", C.c_uint64)]
+
+PHASES = ["census", "scan", "count_pass", "insert_high", "merge_low", "compact", "sort", "queries"]
+
+
+# (name, restype, argtypes) of every symbol include/kc.h declares
+SIGNATURES = [
+    ("kc_open", C.c_int, [C.POINTER(kc_config), C.POINTER(C.c_void_p)]),
+    ("kc_close", None, [C.c_void_p]),
+    ("kc_last_error", C.c_char_p, []),
+    ("kc_job_defaults", None, [C.POINTER(kc_job)]),
+    ("kc_input_upload", C.c_int, [C.c_void_p, C.POINTER(kc_buffer), C.c_uint32, C.POINTER(C.c_void_p)]),
+    ("kc_input_free", None, [C.c_void_p, C.c_void_p]),
+    ("kc_submit", C.c_int, [C.c_void_p, C.POINTER(kc_job), C.POINTER(C.c_uint64)]),
+    ("kc_wait", C.c_int, [C.c_void_p, C.c_uint64, C.c_int32]),
+    ("kc_result", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(kc_result_t)]),
+    ("kc_write_tmpdir", C.c_int, [C.c_void_p, C.c_uint64, C.c_char_p]),
+    ("kc_release", C.c_int, [C.c_void_p, C.c_uint64]),
+    ("kc_submit_batch", C.c_int, [C.c_void_p, C.POINTER(kc_job), C.c_uint32, C.POINTER(C.c_uint64)]),
+    ("kc_host_alloc", C.c_int, [C.c_uint64, C.POINTER(C.c_void_p)]),
+    ("kc_host_free", C.c_int, [C.c_void_p]),
+    ("kc_extract_kmers", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p, C.c_uint64,
+                                   C.POINTER(C.c_uint64)]),
+    ("kc_hash_kmers", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p]),
+    ("kc_sort_records", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32]),
+    ("kc_bloom_plan", C.c_int, [C.POINTER(kc_buffer), C.c_uint32, C.c_uint32, C.c_uint64, C.c_void_p,
+                                C.POINTER(C.c_uint32), C.c_void_p, C.POINTER(C.c_uint64)]),
+    ("kc_kernel_launches", C.c_uint64, []),
+    ("kc_plan_bloom", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p,
+                                C.POINTER(C.c_uint64)]),
+    ("kc_merge_records", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_uint32,
+                                   C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
+                                   C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64), C.c_void_p]),
+]
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libkc.so (built in-tree by ``make -C ktcountermemorygreedy_b200``)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise KcError(8, f"{LIB_PATH} is missing; build it with __graft_entry__.build()")
+        L = C.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != KC_OK:
+        msg = lib().kc_last_error()
+        raise KcError(rc, msg.decode() if msg else "")
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _buffers(files: Sequence[bytes]):
+    arr = (kc_buffer * max(len(files), 1))()
+    keep = []
+    for i, f in enumerate(files):
+        if isinstance(f, np.ndarray):
+            mv = f
+            arr[i].data = f.ctypes.data
+            arr[i].size = f.nbytes
+        else:
+            mv = np.frombuffer(f, dtype=np.uint8) if len(f) else np.zeros(1, np.uint8)
+            arr[i].data = mv.ctypes.data
+            arr[i].size = len(f)
+        keep.append(mv)
+    return arr, keep
+
+
+def kmer_string(key: int, k: int) -> str:
+    """Printed form of a kmer<1> word (tool/dump_tool.cpp:103-124)."""
+    return "".join("ACGT"[(key >> (64 - 2 * k + 2 * i)) & 3] for i in range(k))
+
+
+def string_key(key: int, k: int) -> int:
+    """Printed-string order key: the k bases packed first-base-high
+    (tool/dump_tool.cpp:346-354)."""
+    s = 0
+    for i in range(k):
+        s = (s << 2) | ((key >> (64 - 2 * k + 2 * i)) & 3)
+    return s
+
+
+@dataclass
+class Result:
+    """Outputs of one job: the precise histogram/dump of the reference tools."""
+    k: int
+    keys: np.ndarray               # uint64 kmer<1> words, printed-string order
+    counts: np.ndarray             # uint32 exact counts (saturated at count_max)
+    hist: np.ndarray               # int64, bins hist_min..hist_max
+    hist_min: int
+    top_keys: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint64))
+    top_counts: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint32))
+    le2_keys: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint64))
+    le2_counts: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint32))
+    occurrences: int = 0
+    distinct: int = 0
+    low_only: int = 0
+    table_capacity: int = 0
+    device_ms: float = 0.0
+    queue_ms: float = 0.0
+    run_ms: float = 0.0
+    phase_ms: tuple = ()
+    phase_launches: tuple = ()
+    low_len: int = 0
+    high_len: int = 0
+    input_bytes: int = 0
+    n_records_total: int = 0
+
+
+def _copy(ptr, n, dtype):
+    if n == 0 or not ptr:
+        return np.zeros(0, dtype)
+    return np.ctypeslib.as_array(ptr, shape=(n,)).copy()
+
+
+class KmerCounter:
+    """Handle on one GPU (``kc_open``).  ``max_inflight_jobs`` jobs run on the
+    device at once; further jobs are admitted in submission order as device
+    memory frees up."""
+
+    def __init__(self, device: int = 0, max_inflight_jobs: int = 4, hbm_budget_bytes: int = 0):
+        cfg = kc_config()
+        cfg.device = device
+        cfg.max_inflight_jobs = max_inflight_jobs
+        cfg.hbm_budget_bytes = hbm_budget_bytes
+        h = C.c_void_p()
+        _check(lib().kc_open(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._inputs = {}
+
+    def close(self):
+        if self._h:
+            lib().kc_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- jobs -------------------------------------------------------------
+    @staticmethod
+    def make_job(k: int = 31, count_max: int = 255, bloom: bool = False, memory_gb: int = 4,
+                 filter_min: int = 2, filter_max: int = U32_MAX, min_count: int = 1,
+                 max_count: int = U32_MAX, hist_min: int = 1, hist_max: int = 10000, top_n: int = 0,
+                 want_le2: bool = False, keep_records: bool = True) -> kc_job:
+        j = kc_job()
+        lib().kc_job_defaults(C.byref(j))
+        j.k, j.count_max, j.bloom, j.memory_gb = k, count_max, int(bloom), memory_gb
+        j.filter_min, j.filter_max, j.min_count, j.max_count = filter_min, filter_max, min_count, max_count
+        j.hist_min, j.hist_max, j.top_n, j.want_le2 = hist_min, hist_max, top_n, int(want_le2)
+        j.keep_records = int(keep_records)
+        return j
+
+    def upload(self, files: Sequence[bytes]):
+        """Device-resident copy of the inputs (``kc_input_upload``)."""
+        arr, keep = _buffers(files)
+        p = C.c_void_p()
+        _check(lib().kc_input_upload(self._h, arr, len(files), C.byref(p)))
+        return p
+
+    def free_input(self, p):
+        lib().kc_input_free(self._h, p)
+
+    def submit(self, files: Sequence[bytes] = (), input=None, **kw) -> int:
+        j = self.make_job(**kw)
+        arr, keep = _buffers(files)
+        j.files = C.cast(arr, C.POINTER(kc_buffer))
+        j.n_files = len(files)
+        if input is not None:
+            j.input = input
+        jid = C.c_uint64()
+        _check(lib().kc_submit(self._h, C.byref(j), C.byref(jid)))
+        self._inputs[jid.value] = (arr, keep)   # host buffers stay alive until wait()
+        return jid.value
+
+    def submit_batch(self, samples: Sequence[Sequence[bytes]], ks: Sequence[int], **kw) -> List[int]:
+        n = len(samples)
+        jobs = (kc_job * n)()
+        keep = []
+        for i, (files, k) in enumerate(zip(samples, ks)):
+            j = self.make_job(k=k, **kw)
+            arr, kk = _buffers(files)
+            keep.append((arr, kk))
+            j.files = C.cast(arr, C.POINTER(kc_buffer))
+            j.n_files = len(files)
+            jobs[i] = j
+        ids = (C.c_uint64 * n)()
+        _check(lib().kc_submit_batch(self._h, jobs, n, ids))
+        for i in range(n):
+            self._inputs[ids[i]] = keep[i]
+        return list(ids)
+
+    def wait(self, jid: int, timeout_ms: int = -1):
+        try:
+            _check(lib().kc_wait(self._h, jid, timeout_ms))
+        finally:
+            pass
+
+    def result(self, jid: int, k: int, release: bool = True) -> Result:
+        r = kc_result_t()
+        _check(lib().kc_result(self._h, jid, C.byref(r)))
+        out = Result(
+            k=k,
+            keys=_copy(r.keys, r.n_records, np.uint64), counts=_copy(r.counts, r.n_records, np.uint32),
+            hist=_copy(r.hist, r.hist_len, np.int64), hist_min=0,
+            top_keys=_copy(r.top_keys, r.n_top, np.uint64), top_counts=_copy(r.top_counts, r.n_top, np.uint32),
+            le2_keys=_copy(r.le2_keys, r.n_le2, np.uint64), le2_counts=_copy(r.le2_counts, r.n_le2, np.uint32),
+            occurrences=r.occurrences, distinct=r.distinct, low_only=r.low_only,
+            table_capacity=r.table_capacity, device_ms=r.device_ms, queue_ms=r.queue_ms, run_ms=r.run_ms,
+            phase_ms=tuple(r.phase_ms), phase_launches=tuple(r.phase_launches), low_len=r.low_len,
+            high_len=r.high_len, input_bytes=r.input_bytes, n_records_total=r.n_records_total)
+        if release:
+            self.release(jid)
+        return out
+
+    def release(self, jid: int):
+        self._inputs.pop(jid, None)
+        _check(lib().kc_release(self._h, jid))
+
+    def write_tmpdir(self, jid: int, path: str):
+        _check(lib().kc_write_tmpdir(self._h, jid, path.encode()))
+
+    def count(self, files: Sequence[bytes] = (), input=None, **kw) -> Result:
+        """One job: FASTQ files -> exact canonical counts (blocking)."""
+        jid = self.submit(files, input=input, **kw)
+        self.wait(jid)
+        res = self.result(jid, kw.get("k", 31))
+        res.hist_min = kw.get("hist_min", 1)
+        return res
+
+    def count_batch(self, samples: Sequence[Sequence[bytes]], ks: Sequence[int], **kw) -> List[Result]:
+        ids = self.submit_batch(samples, ks, **kw)
+        out = []
+        for jid, k in zip(ids, ks):
+            self.wait(jid)
+            r = self.result(jid, k)
+            r.hist_min = kw.get("hist_min", 1)
+            out.append(r)
+        return out
+
+
+# ---- single steps ----------------------------------------------------------
+
+def kernel_launches() -> int:
+    """Kernel launches issued by libkc.so in this process."""
+    return int(lib().kc_kernel_launches())
+
+
+def extract_kmers(fastq: bytes, k: int) -> np.ndarray:
+    """Canonical k-mer occurrences of one FASTQ file (unordered)."""
+    data = np.frombuffer(fastq, dtype=np.uint8) if len(fastq) else np.zeros(1, np.uint8)
+    cap = max(len(fastq), 1)
+    out = np.zeros(cap, np.uint64)
+    n = C.c_uint64()
+    _check(lib().kc_extract_kmers(_ptr(data), len(fastq), k, _ptr(out), cap, C.byref(n)))
+    return out[: n.value].copy()
+
+
+def hash_kmers(keys: np.ndarray) -> np.ndarray:
+    keys = np.ascontiguousarray(keys, dtype=np.uint64)
+    out = np.zeros(5 * max(len(keys), 1), np.uint64)
+    _check(lib().kc_hash_kmers(_ptr(keys), len(keys), _ptr(out)))
+    return out[: 5 * len(keys)].reshape(-1, 5)
+
+
+def sort_records(keys: np.ndarray, counts: np.ndarray, bits: int):
+    keys = np.ascontiguousarray(keys, dtype=np.uint64).copy()
+    counts = np.ascontiguousarray(counts, dtype=np.uint32).copy()
+    _check(lib().kc_sort_records(_ptr(keys), _ptr(counts), len(keys), bits))
+    return keys, counts
+
+
+def bloom_plan(files: Sequence[bytes], k: int, memory_gb: int):
+    arr, keep = _buffers(files)
+    pc = np.zeros(256, np.uint32)
+    caps = np.zeros(256, np.uint64)
+    avg = C.c_uint32()
+    mx = C.c_uint64()
+    _check(lib().kc_bloom_plan(arr, len(files), k, memory_gb, _ptr(pc), C.byref(avg), _ptr(caps), C.byref(mx)))
+    return pc, avg.value, caps, mx.value
+
+
+def plan_bloom(raw_prefix_counts, avg_quality: int, est_file_size: int, memory_gb: int, k: int):
+    """The reference's Bloom filter sizing (host arithmetic only)."""
+    pc = np.ascontiguousarray(raw_prefix_counts, dtype=np.uint32)
+    caps = np.zeros(256, np.uint64)
+    mx = C.c_uint64()
+    _check(lib().kc_plan_bloom(_ptr(pc), avg_quality, est_file_size, memory_gb, k, _ptr(caps), C.byref(mx)))
+    return caps, mx.value
+
+
+def merge_records(high_keys, high_counts, low_keys, k: int, count_max: int, min_count: int = 1,
+                  max_count: int = U32_MAX, hist_min: int = 1, hist_max: int = 10000):
+    hk = np.ascontiguousarray(high_keys, dtype=np.uint64)
+    hc = np.ascontiguousarray(high_counts, dtype=np.uint32)
+    lk = np.ascontiguousarray(low_keys, dtype=np.uint64)
+    cap = max(len(hk) + len(lk), 1)
+    ok = np.zeros(cap, np.uint64)
+    oc = np.zeros(cap, np.uint32)
+    hist = np.zeros(hist_max - hist_min + 1, np.int64)
+    n = C.c_uint64()
+    _check(lib().kc_merge_records(_ptr(hk), _ptr(hc), len(hk), _ptr(lk), len(lk), k, count_max, min_count,
+                                  max_count, hist_min, hist_max, _ptr(ok), _ptr(oc), cap, C.byref(n), _ptr(hist)))
+    return ok[: n.value], oc[: n.value], hist
+
+
+# ---- text outputs of the reference tools -------------------------------------
+
+def histogram_text(hist: np.ndarray, hist_min: int) -> str:
+    """histogram_tool output: ``f\\tcount\\n`` for every f (tool/histogram_tool.cpp:462-478)."""
+    return "".join(f"{hist_min + i}\t{int(v)}\n" for i, v in enumerate(hist))
+
+
+def dump_text(keys: np.ndarray, counts: np.ndarray, k: int) -> str:
+    """dump_tool output: ``KMER\\tcount\\n`` lines (tool/dump_tool.cpp:1172-1193)."""
+    return "".join(f"{kmer_string(int(w), k)}\t{int(c)}\n" for w, c in zip(keys, counts))

@@ -1,0 +1,1153 @@
+// kc_api.cpp -- C++ host runtime behind include/kc.h.
+//
+// A handle owns a pool of worker threads, one CUDA stream each.  Submitted
+// jobs wait in a FIFO queue and are admitted, in order, when their device
+// memory reservation fits the handle's HBM budget (or when nothing else runs),
+// so jobs that arrive while others are on the device start as soon as a
+// worker slot and memory free up, and their kernels overlap on the GPU.
+//
+// One job is the reference's counter run followed by its precise tools:
+//   upload (tile-aligned, zero padded)  -> newline census -> tile line numbers
+//   -> SCAN pass (occurrences, HyperLogLog; Bloom pre-pass statistics)
+//   -> plain:  INSERT pass into a table sized from the HyperLogLog estimate
+//      Bloom:  BLOOM pass (reference filter sizing and probes), then insert
+//              the non-FIRST occurrences and merge the FIRST ones back
+//   -> compaction + histogram -> radix sort in printed-string order
+//   -> queries -> host.
+// All device memory is stream-ordered (cudaMallocAsync on the worker stream)
+// from a pool that keeps freed memory for the next job.
+#include "kc.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "kc_host.h"
+#include "kc_kernels.cuh"
+#include "kc_plan.h"
+
+using namespace kc;
+
+namespace {
+
+double now_ms()
+{
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+double hll_estimate(const uint32_t *regs, uint32_t m)
+{
+    double sum = 0.0;
+    uint32_t zeros = 0;
+    for (uint32_t i = 0; i < m; ++i) {
+        sum += std::ldexp(1.0, -(int)regs[i]);
+        zeros += regs[i] == 0;
+    }
+    double alpha = 0.7213 / (1.0 + 1.079 / m);
+    double e = alpha * m * (double)m / sum;
+    if (e <= 2.5 * m && zeros) e = m * std::log((double)m / zeros);
+    return e;
+}
+
+uint64_t table_capacity_for(double est)
+{
+    uint64_t want = (uint64_t)std::ceil(std::max(est, 16.0) * 1.8);
+    return std::max<uint64_t>(1024, bit_ceil64(want));
+}
+
+int fail(int code, const std::string &msg) { return set_error(code, msg); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// jobs and the handle
+// ---------------------------------------------------------------------------
+
+namespace {
+
+enum class JobState { QUEUED, RUNNING, DONE, FAILED };
+
+struct Job {
+    kc_job_id id = 0;
+    kc_job p{};
+    std::vector<kc_buffer> files;
+    const kc_input *input = nullptr;
+    uint64_t reserve = 0;
+    JobState state = JobState::QUEUED;
+    int err = KC_OK;
+    std::string err_msg;
+    double t_submit = 0, t_start = 0, t_end = 0;
+    // results
+    std::vector<uint64_t> keys;
+    std::vector<uint32_t> counts;
+    std::vector<int64_t> hist;
+    std::vector<uint64_t> top_keys, le2_keys;
+    std::vector<uint32_t> top_counts, le2_counts;
+    uint64_t occurrences = 0, distinct = 0, low_only = 0, table_cap = 0;
+    uint64_t low_len = 0, high_len = 0, input_bytes = 0, n_records_total = 0;
+    double device_ms = 0;
+    double phase_ms[8] = {0};
+    uint64_t phase_launches[8] = {0};
+};
+
+// Device time and kernel launches per pipeline stage, from CUDA events on
+// the job's stream.  Launches are counted on the worker thread that issues
+// them, so overlapping jobs on other workers do not mix in.
+struct PhaseClock {
+    cudaStream_t st;
+    struct Span {
+        int phase;
+        cudaEvent_t a, b;
+    };
+    std::vector<Span> spans;
+    int cur = -1;
+    cudaEvent_t cur_a = nullptr;
+    unsigned long long l0 = 0;
+    uint64_t launches[8] = {0};
+    explicit PhaseClock(cudaStream_t s) : st(s) {}
+    void begin(int phase)
+    {
+        CK(cudaEventCreate(&cur_a));
+        CK(cudaEventRecord(cur_a, st));
+        cur = phase;
+        l0 = thread_kernel_launches();
+    }
+    void end()
+    {
+        cudaEvent_t b;
+        CK(cudaEventCreate(&b));
+        CK(cudaEventRecord(b, st));
+        spans.push_back({cur, cur_a, b});
+        launches[cur] += thread_kernel_launches() - l0;
+        cur_a = nullptr;
+    }
+    void collect(double *ms, uint64_t *ln)
+    {
+        for (auto &s : spans) {
+            float t = 0;
+            if (cudaEventElapsedTime(&t, s.a, s.b) == cudaSuccess) ms[s.phase] += t;
+        }
+        for (int i = 0; i < 8; ++i) ln[i] += launches[i];
+    }
+    ~PhaseClock()
+    {
+        for (auto &s : spans) {
+            cudaEventDestroy(s.a);
+            cudaEventDestroy(s.b);
+        }
+        if (cur_a) cudaEventDestroy(cur_a);
+    }
+};
+
+struct Task {
+    std::vector<std::shared_ptr<Job>> jobs;   // one job, or a batch
+    bool batch = false;
+    uint64_t reserve = 0;
+};
+
+}  // namespace
+
+struct kc_handle {
+    int device = 0;
+    uint64_t budget = 0;
+    uint64_t reserved = 0;
+    uint32_t running = 0;
+    bool closing = false;
+    kc_job_id next_id = 1;
+    std::mutex mu;
+    std::condition_variable cv_work;
+    std::condition_variable cv_done;
+    std::deque<std::shared_ptr<Task>> queue;
+    std::map<kc_job_id, std::shared_ptr<Job>> jobs;
+    std::vector<std::thread> workers;
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// the counting pipeline of one job
+// ---------------------------------------------------------------------------
+
+struct Plan {
+    uint32_t k;
+    bool bloom;
+};
+
+void check_flags(unsigned long long flags, const char *where)
+{
+    if (flags & ERR_WAIT_TIMEOUT) throw KcError{KC_ERR_DEVICE, std::string(where) + ": bounded wait expired"};
+    if (flags & ERR_LIST_FULL) throw KcError{KC_ERR_DEVICE, std::string(where) + ": occurrence list overflow"};
+    if (flags & ERR_RECORDS_FULL) throw KcError{KC_ERR_DEVICE, std::string(where) + ": record buffer overflow"};
+    if (flags & ERR_HIST_OVERFLOW_FULL) throw KcError{KC_ERR_DEVICE, std::string(where) + ": histogram overflow list full"};
+}
+
+struct Counters {
+    unsigned long long v[C_COUNT];
+};
+
+Counters read_counters(const unsigned long long *d, cudaStream_t st)
+{
+    Counters c{};
+    CK(cudaMemcpyAsync(c.v, d, sizeof(c.v), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return c;
+}
+
+void run_job(Job &job, cudaStream_t st)
+{
+    const kc_job &P = job.p;
+    const uint32_t k = P.k;
+    DevScope ds(st);
+    std::vector<uint32_t> tile_seg_host;
+
+    // ---- input -----------------------------------------------------------
+    kc_input local;
+    const kc_input *in = job.input;
+    if (!in) {
+        build_input(local, job.files.data(), (uint32_t)job.files.size(), st, &ds, tile_seg_host);
+        in = &local;
+    }
+    cudaEvent_t ev0, ev1;
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); }
+    } evg{ev0, ev1};
+    CK(cudaEventRecord(ev0, st));
+    PhaseClock clk(st);
+
+    const uint64_t T = in->n_tiles;
+    const uint32_t n_seg = (uint32_t)in->segs.size();
+    std::vector<Seg> segs = in->segs;
+    // the pre-pass samples the first 256 MiB of a single file, 128 MiB of each
+    // of several files (src/FastqPreReader.h:98-102)
+    const uint64_t sample_limit = (in->sizes.size() == 1) ? (256ULL << 20) : (128ULL << 20);
+    std::vector<uint64_t> seg_chunk0(std::max<uint32_t>(n_seg, 1), 0);
+    uint64_t n_chunks = 0;
+    for (uint32_t i = 0; i < n_seg; ++i) {
+        segs[i].k = k;
+        segs[i].sample = 0;
+        segs[i].sample_end = std::min(segs[i].len, sample_limit);
+        seg_chunk0[i] = n_chunks;
+        n_chunks += (segs[i].len + PREPASS_CHUNK - 1) / PREPASS_CHUNK;
+    }
+    Seg *d_segs = ds.n<Seg>(std::max<uint32_t>(n_seg, 1));
+    if (n_seg) CK(cudaMemcpyAsync(d_segs, segs.data(), n_seg * sizeof(Seg), cudaMemcpyHostToDevice, st));
+
+    unsigned long long *counters = ds.n<unsigned long long>(C_COUNT);
+    CK(cudaMemsetAsync(counters, 0, C_COUNT * 8, st));
+
+    // ---- line numbers of tile starts --------------------------------------
+    uint32_t *tile_nl = ds.n<uint32_t>(std::max<uint64_t>(T, 1));
+    int32_t *tile_lastnl = ds.n<int32_t>(std::max<uint64_t>(T, 1));
+    unsigned long long *tile_prefix = ds.n<unsigned long long>(std::max<uint64_t>(T, 1));
+    unsigned long long *scan_tmp = ds.n<unsigned long long>(scan_tmp_words(std::max<uint64_t>(T, 1)));
+    clk.begin(0);
+    CK(launch_newlines(in->buf, T, tile_nl, tile_lastnl, st));
+    CK(launch_scan_u32(tile_nl, tile_prefix, T, scan_tmp, st));
+    clk.end();
+
+    // ---- SCAN pass ---------------------------------------------------------
+    unsigned long long *occ = ds.n<unsigned long long>(1);
+    uint32_t *hll = ds.n<uint32_t>(HLL_M);
+    CK(cudaMemsetAsync(occ, 0, 8, st));
+    CK(cudaMemsetAsync(hll, 0, HLL_M * 4, st));
+    ExtractArgs a{};
+    a.buf = in->buf;
+    a.n_tiles = T;
+    a.tile_prefix = reinterpret_cast<const uint64_t *>(tile_prefix);
+    a.tile_seg = in->d_tile_seg;
+    a.segs = d_segs;
+    a.counters = counters;
+    a.occ = occ;
+    a.hll = hll;
+    uint32_t *prefix_hist = nullptr;
+    unsigned long long *qual = nullptr;
+    clk.begin(1);
+    if (P.bloom) {
+        int32_t *chunk_lastnl = ds.n<int32_t>(std::max<uint64_t>(n_chunks, 1));
+        uint64_t *d_chunk0 = ds.n<uint64_t>(seg_chunk0.size());
+        prefix_hist = ds.n<uint32_t>(256);
+        qual = ds.n<unsigned long long>(2);
+        CK(cudaMemsetAsync(chunk_lastnl, 0xff, std::max<uint64_t>(n_chunks, 1) * 4, st));
+        CK(cudaMemcpyAsync(d_chunk0, seg_chunk0.data(), seg_chunk0.size() * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(prefix_hist, 0, 256 * 4, st));
+        CK(cudaMemsetAsync(qual, 0, 16, st));
+        CK(launch_chunk_lastnl(tile_lastnl, in->d_tile_seg, d_segs, d_chunk0, T, chunk_lastnl, st));
+        a.prepass = 1;
+        a.chunk_lastnl = chunk_lastnl;
+        a.seg_chunk0 = d_chunk0;
+        a.prefix_hist = prefix_hist;
+        a.qual = qual;
+    }
+    CK(launch_extract(MODE_SCAN, a, 0, st));
+    clk.end();
+    std::vector<uint32_t> hll_h(HLL_M);
+    unsigned long long O = 0;
+    CK(cudaMemcpyAsync(&O, occ, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hll_h.data(), hll, HLL_M * 4, cudaMemcpyDeviceToHost, st));
+    std::vector<uint32_t> ph(256, 0);
+    unsigned long long qh[2] = {0, 0};
+    if (P.bloom) {
+        CK(cudaMemcpyAsync(ph.data(), prefix_hist, 256 * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(qh, qual, 16, cudaMemcpyDeviceToHost, st));
+    }
+    Counters c0 = read_counters(counters, st);
+    check_flags(c0.v[C_FLAGS], "scan");
+    job.occurrences = O;
+
+    // ---- counting ---------------------------------------------------------
+    TableRef tr{};
+    TableRef *d_tr = ds.n<TableRef>(1);
+    uint64_t cap = 0;
+    unsigned long long *list = nullptr;
+    unsigned long long low_len = 0, high_len = 0;
+    double est = hll_estimate(hll_h.data(), HLL_M);
+    auto alloc_table = [&](uint64_t c) {
+        if (tr.slots) ds.release(tr.slots);
+        cap = c;
+        tr.slots = static_cast<Slot *>(ds.get(cap * sizeof(Slot)));
+        tr.mask = cap - 1;
+        CK(launch_init_slots(tr.slots, cap, st));
+        CK(cudaMemcpyAsync(d_tr, &tr, sizeof(tr), cudaMemcpyHostToDevice, st));
+    };
+    const uint32_t max_probe_cap = 1u << 16;
+    if (!P.bloom) {
+        cap = table_capacity_for(est);
+        for (int attempt = 0;; ++attempt) {
+            alloc_table(cap);
+            CK(cudaMemsetAsync(counters, 0, 8, st));
+            a.tables = d_tr;
+            a.max_probe = (uint32_t)std::min<uint64_t>(cap, max_probe_cap);
+            clk.begin(2);
+            CK(launch_extract(MODE_INSERT, a, 0, st));
+            clk.end();
+            Counters c = read_counters(counters, st);
+            check_flags(c.v[C_FLAGS], "insert");
+            if (!(c.v[C_FLAGS] & ERR_TABLE_FULL)) break;
+            if (attempt >= 3) throw KcError{KC_ERR_DEVICE, "counting table overflow"};
+            cap *= 2;
+        }
+    } else {
+        // reference sizing (src/main.cpp:41-153) from the pre-pass statistics
+        uint8_t avg_q = qh[1] ? (uint8_t)(qh[0] / qh[1]) : 0;
+        BloomPlan bp = bloom_plan(ph.data(), avg_q, in->total_bytes, P.memory_gb, k);
+        std::vector<unsigned long long> boff(256), bcap(256);
+        unsigned long long words = 0;
+        for (int i = 0; i < 256; ++i) {
+            boff[i] = words;
+            bcap[i] = bp.caps[i];
+            words += 2 * bp.caps[i];
+        }
+        unsigned long long *bits = ds.n<unsigned long long>(words);
+        unsigned long long *d_boff = ds.n<unsigned long long>(256);
+        unsigned long long *d_bcap = ds.n<unsigned long long>(256);
+        CK(cudaMemsetAsync(bits, 0, words * 8, st));
+        CK(cudaMemcpyAsync(d_boff, boff.data(), 256 * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_bcap, bcap.data(), 256 * 8, cudaMemcpyHostToDevice, st));
+        uint32_t *hll_high = ds.n<uint32_t>(HLL_M);
+        CK(cudaMemsetAsync(hll_high, 0, HLL_M * 4, st));
+        list = ds.n<unsigned long long>(std::max<unsigned long long>(O, 1));
+        a.bloom_off = d_boff;
+        a.bloom_cap = d_bcap;
+        a.bloom_bits = bits;
+        a.hll_high = hll_high;
+        a.list = list;
+        a.list_cap = std::max<unsigned long long>(O, 1);
+        a.prepass = 0;
+        clk.begin(2);
+        CK(launch_extract(MODE_BLOOM, a, 0, st));
+        clk.end();
+        CK(cudaMemcpyAsync(hll_h.data(), hll_high, HLL_M * 4, cudaMemcpyDeviceToHost, st));
+        Counters c = read_counters(counters, st);
+        check_flags(c.v[C_FLAGS], "bloom");
+        low_len = c.v[C_LOW_LEN];
+        high_len = c.v[C_HIGH_LEN];
+        ds.release(bits);
+        double est_high = high_len ? hll_estimate(hll_h.data(), HLL_M) : 0.0;
+        cap = table_capacity_for(est_high);
+        for (int attempt = 0;; ++attempt) {
+            alloc_table(cap);
+            CK(cudaMemsetAsync(counters, 0, 8, st));
+            uint32_t mp = (uint32_t)std::min<uint64_t>(cap, max_probe_cap);
+            clk.begin(3);
+            CK(launch_insert_list(list + a.list_cap - high_len, high_len, tr, mp, counters, st));
+            clk.end();
+            Counters cc = read_counters(counters, st);
+            check_flags(cc.v[C_FLAGS], "insert");
+            if (!(cc.v[C_FLAGS] & ERR_TABLE_FULL)) break;
+            if (attempt >= 3) throw KcError{KC_ERR_DEVICE, "counting table overflow"};
+            cap *= 2;
+        }
+    }
+    job.table_cap = cap;
+
+    // ---- records ------------------------------------------------------------
+    const uint32_t count_max = P.count_max ? P.count_max : 255u;
+    unsigned long long *n_keys = ds.n<unsigned long long>(1);
+    CK(cudaMemsetAsync(n_keys, 0, 8, st));
+    clk.begin(5);
+    CK(launch_count_keys(tr.slots, cap, n_keys, st));
+    clk.end();
+    unsigned long long in_table = 0;
+    CK(cudaMemcpyAsync(&in_table, n_keys, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const uint64_t rec_cap = std::max<uint64_t>(in_table + low_len, 1);
+    unsigned long long *rec_keys = ds.n<unsigned long long>(rec_cap);
+    uint32_t *rec_counts = ds.n<uint32_t>(rec_cap);
+    unsigned long long *hist = ds.n<unsigned long long>(HIST_BINS);
+    const uint64_t ovf_cap = 1 << 20;
+    uint32_t *ovf = ds.n<uint32_t>(ovf_cap);
+    CK(cudaMemsetAsync(hist, 0, HIST_BINS * 8, st));
+    if (P.bloom && low_len) {
+        clk.begin(4);
+        CK(launch_merge_low(list, low_len, tr, (uint32_t)std::min<uint64_t>(cap, max_probe_cap), P.min_count,
+                            P.max_count, rec_keys, rec_counts, rec_cap, counters, st));
+        clk.end();
+    }
+    clk.begin(5);
+    CK(launch_compact(tr, cap, count_max, P.min_count, P.max_count, rec_keys, rec_counts, rec_cap, hist, ovf, ovf_cap,
+                      counters, st));
+    clk.end();
+    Counters c2 = read_counters(counters, st);
+    check_flags(c2.v[C_FLAGS], "compact");
+    if (c2.v[C_FLAGS] & ERR_TABLE_FULL) throw KcError{KC_ERR_DEVICE, "counting table lookup overflow"};
+    const uint64_t n_rec = c2.v[C_REC_LEN];
+    job.distinct = c2.v[C_DISTINCT] + c2.v[C_LOW_ONLY];
+    job.low_only = c2.v[C_LOW_ONLY];
+    if (list) ds.release(list);
+    ds.release(tr.slots);
+    tr.slots = nullptr;
+
+    // ---- sort in printed-string order ---------------------------------------
+    clk.begin(6);
+    if (n_rec > 1) {
+        void *stmp = ds.get(sort_tmp_bytes(n_rec));
+        CK(launch_radix_sort(rec_keys, rec_counts, n_rec, 2 * k, stmp, st));
+        ds.release(stmp);
+    }
+    CK(launch_pair_reverse(rec_keys, n_rec, st));
+    clk.end();
+
+    // ---- histogram ----------------------------------------------------------
+    std::vector<unsigned long long> hd(HIST_BINS);
+    CK(cudaMemcpyAsync(hd.data(), hist, HIST_BINS * 8, cudaMemcpyDeviceToHost, st));
+    const uint64_t n_ovf = std::min<uint64_t>(c2.v[C_OVF_LEN], ovf_cap);
+    std::vector<uint32_t> ovf_h(n_ovf);
+    if (n_ovf) CK(cudaMemcpyAsync(ovf_h.data(), ovf, n_ovf * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    hd[1] += job.low_only;   // FIRST-only k-mers have count 1 (count_max >= 1)
+    {
+        uint32_t lo = P.hist_min, hi = P.hist_max;
+        if (hi < lo) hi = lo;
+        uint64_t len = (uint64_t)hi - lo + 1;
+        job.hist.assign(len, 0);
+        for (uint64_t c = std::max<uint64_t>(lo, 1); c < HIST_BINS && c <= hi; ++c) job.hist[c - lo] = (int64_t)hd[c];
+        for (uint32_t c : ovf_h)
+            if (c >= lo && c <= hi) job.hist[c - lo]++;
+    }
+
+    // ---- queries --------------------------------------------------------------
+    if (P.top_n || P.want_le2) {
+        clk.begin(7);
+        uint32_t *flags = ds.n<uint32_t>(std::max<uint64_t>(n_rec, 1));
+        unsigned long long *pos = ds.n<unsigned long long>(std::max<uint64_t>(n_rec, 1));
+        unsigned long long *qtmp = ds.n<unsigned long long>(scan_tmp_words(std::max<uint64_t>(n_rec, 1)));
+        if (P.top_n && n_rec) {
+            // threshold from the histogram restricted to the record range
+            auto count_at = [&](uint64_t c) -> uint64_t { return c < HIST_BINS ? hd[c] : 0; };
+            std::vector<uint32_t> big;
+            for (uint32_t c : ovf_h)
+                if (c >= P.min_count && c <= P.max_count) big.push_back(c);
+            std::sort(big.begin(), big.end(), std::greater<uint32_t>());
+            uint64_t above = 0;
+            uint32_t thr = std::max<uint32_t>(P.min_count, 1);
+            bool found = false;
+            for (size_t i = 0; i < big.size(); ++i) {
+                if (above + 1 >= P.top_n) { thr = big[i]; found = true; break; }
+                ++above;
+            }
+            if (!found) {
+                uint64_t hi = std::min<uint64_t>((uint64_t)P.max_count, HIST_BINS - 1);
+                for (uint64_t c = hi; c >= std::max<uint32_t>(P.min_count, 1); --c) {
+                    uint64_t h = count_at(c);
+                    if (above + h >= P.top_n) { thr = (uint32_t)c; found = true; break; }
+                    above += h;
+                    if (c == 0) break;
+                }
+            }
+            // strictly above the threshold
+            unsigned long long *ak = ds.n<unsigned long long>(P.top_n);
+            uint32_t *ac = ds.n<uint32_t>(P.top_n);
+            unsigned long long *bk = ds.n<unsigned long long>(P.top_n);
+            uint32_t *bc = ds.n<uint32_t>(P.top_n);
+            uint64_t n_above = 0, n_at = 0;
+            if (thr < 0xffffffffu) {
+                CK(launch_select_range(rec_keys, rec_counts, n_rec, thr + 1, 0xffffffffu, P.top_n, ak, ac, flags, pos,
+                                       qtmp, counters, C_SEL_A, st));
+            } else {
+                CK(cudaMemsetAsync(&counters[C_SEL_A], 0, 8, st));
+            }
+            Counters ca = read_counters(counters, st);
+            n_above = std::min<uint64_t>(ca.v[C_SEL_A], P.top_n);
+            uint64_t need = P.top_n - n_above;
+            if (need) {
+                CK(launch_select_range(rec_keys, rec_counts, n_rec, thr, thr, need, bk, bc, flags, pos, qtmp, counters,
+                                       C_SEL_B, st));
+                Counters cb = read_counters(counters, st);
+                n_at = std::min<uint64_t>(cb.v[C_SEL_B], need);
+            }
+            std::vector<uint64_t> tk(n_above), tk2(n_at);
+            std::vector<uint32_t> tc(n_above), tc2(n_at);
+            if (n_above) {
+                CK(cudaMemcpyAsync(tk.data(), ak, n_above * 8, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(tc.data(), ac, n_above * 4, cudaMemcpyDeviceToHost, st));
+            }
+            if (n_at) {
+                CK(cudaMemcpyAsync(tk2.data(), bk, n_at * 8, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(tc2.data(), bc, n_at * 4, cudaMemcpyDeviceToHost, st));
+            }
+            CK(cudaStreamSynchronize(st));
+            // records above the threshold: count desc, then printed string asc
+            // (they arrive in printed-string order; a stable sort keeps it)
+            std::vector<size_t> idx(n_above);
+            for (size_t i = 0; i < n_above; ++i) idx[i] = i;
+            std::stable_sort(idx.begin(), idx.end(), [&](size_t x, size_t y) { return tc[x] > tc[y]; });
+            for (size_t i : idx) { job.top_keys.push_back(tk[i]); job.top_counts.push_back(tc[i]); }
+            for (size_t i = 0; i < n_at; ++i) { job.top_keys.push_back(tk2[i]); job.top_counts.push_back(tc2[i]); }
+        }
+        if (P.want_le2 && n_rec) {
+            unsigned long long *lk = ds.n<unsigned long long>(n_rec);
+            uint32_t *lc = ds.n<uint32_t>(n_rec);
+            CK(launch_select_range(rec_keys, rec_counts, n_rec, 0, 2, n_rec, lk, lc, flags, pos, qtmp, counters, C_SEL_A,
+                                   st));
+            Counters cl = read_counters(counters, st);
+            uint64_t nl = std::min<uint64_t>(cl.v[C_SEL_A], n_rec);
+            job.le2_keys.resize(nl);
+            job.le2_counts.resize(nl);
+            if (nl) {
+                CK(cudaMemcpyAsync(job.le2_keys.data(), lk, nl * 8, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(job.le2_counts.data(), lc, nl * 4, cudaMemcpyDeviceToHost, st));
+            }
+        }
+        clk.end();
+    }
+    CK(cudaEventRecord(ev1, st));
+
+    // ---- records to host ------------------------------------------------------
+    if (P.keep_records) {
+        job.keys.resize(n_rec);
+        job.counts.resize(n_rec);
+        if (n_rec) {
+            CK(cudaMemcpyAsync(job.keys.data(), rec_keys, n_rec * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(job.counts.data(), rec_counts, n_rec * 4, cudaMemcpyDeviceToHost, st));
+        }
+    }
+    CK(cudaStreamSynchronize(st));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ev0, ev1));
+    job.device_ms = ms;
+    clk.collect(job.phase_ms, job.phase_launches);
+    job.low_len = low_len;
+    job.high_len = high_len;
+    job.input_bytes = in->total_bytes;
+    job.n_records_total = n_rec;
+}
+
+void validate_job(const kc_job &p)
+{
+    if (p.k < 1 || p.k > 32) throw KcError{KC_ERR_INVALID, "k must be in 1..32"};
+    if (!p.input && p.n_files && !p.files) throw KcError{KC_ERR_INVALID, "files is NULL"};
+    if (p.count_max == 0) throw KcError{KC_ERR_INVALID, "count_max must be >= 1"};
+    if (p.filter_max < p.filter_min) throw KcError{KC_ERR_INVALID, "filter_max < filter_min"};
+    if (p.max_count < p.min_count) throw KcError{KC_ERR_INVALID, "max_count < min_count"};
+    if (p.hist_max < p.hist_min) throw KcError{KC_ERR_INVALID, "hist_max < hist_min"};
+    if ((uint64_t)p.hist_max - p.hist_min + 1 > (1ULL << 28)) throw KcError{KC_ERR_INVALID, "histogram range too large"};
+    if (p.bloom && p.memory_gb == 0) throw KcError{KC_ERR_INVALID, "Bloom mode needs memory_gb >= 1"};
+}
+
+uint64_t input_bytes(const kc_job &p)
+{
+    if (p.input) return 0;
+    uint64_t s = 0;
+    for (uint32_t i = 0; i < p.n_files; ++i) s += p.files[i].size;
+    return s;
+}
+
+uint64_t reserve_for(const kc_job &p, uint64_t resident_bytes)
+{
+    uint64_t s = p.input ? resident_bytes : input_bytes(p);
+    // input + per-tile tables + table/records/sort sized for distinct <= s/2
+    return (p.input ? 0 : s) + s / 256 + 24 * s + (64ULL << 20);
+}
+
+// Batched jobs: every sample's files in one device buffer, one SCAN and one
+// INSERT launch over all tiles (each tile counts into its sample's table in a
+// shared slot arena), one batched compaction, one segmented radix sort.
+void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st)
+{
+    const uint32_t n = (uint32_t)jobs.size();
+    if (n > MAX_BATCH) throw KcError{KC_ERR_INVALID, "more than 4096 jobs in one batch"};
+    DevScope ds(st);
+    std::vector<kc_buffer> files;
+    std::vector<uint32_t> fsample;
+    for (uint32_t i = 0; i < n; ++i)
+        for (const auto &f : jobs[i]->files) {
+            files.push_back(f);
+            fsample.push_back(i);
+        }
+    kc_input in;
+    std::vector<uint32_t> tile_seg_host;
+    build_input(in, files.data(), (uint32_t)files.size(), st, &ds, tile_seg_host, fsample.data());
+    cudaEvent_t ev0, ev1;
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); }
+    } evg{ev0, ev1};
+    CK(cudaEventRecord(ev0, st));
+
+    const uint64_t T = in.n_tiles;
+    std::vector<Seg> segs = in.segs;
+    uint32_t max_k = 1;
+    for (auto &sg : segs) {
+        sg.k = jobs[sg.sample]->p.k;
+        max_k = std::max(max_k, sg.k);
+    }
+    Seg *d_segs = ds.n<Seg>(std::max<size_t>(segs.size(), 1));
+    if (!segs.empty()) CK(cudaMemcpyAsync(d_segs, segs.data(), segs.size() * sizeof(Seg), cudaMemcpyHostToDevice, st));
+    unsigned long long *counters = ds.n<unsigned long long>(C_COUNT);
+    CK(cudaMemsetAsync(counters, 0, C_COUNT * 8, st));
+    uint32_t *tile_nl = ds.n<uint32_t>(std::max<uint64_t>(T, 1));
+    int32_t *tile_lastnl = ds.n<int32_t>(std::max<uint64_t>(T, 1));
+    unsigned long long *tile_prefix = ds.n<unsigned long long>(std::max<uint64_t>(T, 1));
+    unsigned long long *scan_tmp = ds.n<unsigned long long>(scan_tmp_words(std::max<uint64_t>(T, 1)));
+    CK(launch_newlines(in.buf, T, tile_nl, tile_lastnl, st));
+    CK(launch_scan_u32(tile_nl, tile_prefix, T, scan_tmp, st));
+
+    unsigned long long *occ = ds.n<unsigned long long>(n);
+    uint32_t *hll = ds.n<uint32_t>((size_t)n * HLL_M);
+    CK(cudaMemsetAsync(occ, 0, (size_t)n * 8, st));
+    CK(cudaMemsetAsync(hll, 0, (size_t)n * HLL_M * 4, st));
+    ExtractArgs a{};
+    a.buf = in.buf;
+    a.n_tiles = T;
+    a.tile_prefix = reinterpret_cast<const uint64_t *>(tile_prefix);
+    a.tile_seg = in.d_tile_seg;
+    a.segs = d_segs;
+    a.counters = counters;
+    a.occ = occ;
+    a.hll = hll;
+    CK(launch_extract(MODE_SCAN, a, 0, st));
+    std::vector<unsigned long long> occ_h(n);
+    std::vector<uint32_t> hll_h((size_t)n * HLL_M);
+    CK(cudaMemcpyAsync(occ_h.data(), occ, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hll_h.data(), hll, (size_t)n * HLL_M * 4, cudaMemcpyDeviceToHost, st));
+    Counters c0 = read_counters(counters, st);
+    check_flags(c0.v[C_FLAGS], "scan");
+
+    std::vector<uint64_t> caps(n);
+    for (uint32_t i = 0; i < n; ++i) caps[i] = table_capacity_for(hll_estimate(&hll_h[(size_t)i * HLL_M], HLL_M));
+    std::vector<SampleCfg> cfg(n);
+    Slot *arena = nullptr;
+    uint64_t total_slots = 0;
+    SampleCfg *d_cfg = ds.n<SampleCfg>(n);
+    TableRef *d_tables = ds.n<TableRef>(n);
+    for (int attempt = 0;; ++attempt) {
+        total_slots = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            cfg[i] = SampleCfg{};
+            cfg[i].slot_base = total_slots;
+            cfg[i].slot_cap = caps[i];
+            cfg[i].count_max = jobs[i]->p.count_max;
+            cfg[i].min_count = jobs[i]->p.min_count;
+            cfg[i].max_count = jobs[i]->p.max_count;
+            cfg[i].k = jobs[i]->p.k;
+            total_slots += caps[i];
+        }
+        if (arena) ds.release(arena);
+        arena = static_cast<Slot *>(ds.get(total_slots * sizeof(Slot)));
+        CK(launch_init_slots(arena, total_slots, st));
+        std::vector<TableRef> trs(n);
+        for (uint32_t i = 0; i < n; ++i) trs[i] = TableRef{arena + cfg[i].slot_base, caps[i] - 1};
+        CK(cudaMemcpyAsync(d_tables, trs.data(), n * sizeof(TableRef), cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(counters, 0, 8, st));
+        a.tables = d_tables;
+        a.max_probe = 1u << 16;
+        CK(launch_extract(MODE_INSERT, a, 0, st));
+        Counters c = read_counters(counters, st);
+        check_flags(c.v[C_FLAGS], "insert");
+        if (!(c.v[C_FLAGS] & ERR_TABLE_FULL)) break;
+        if (attempt >= 3) throw KcError{KC_ERR_DEVICE, "counting table overflow"};
+        for (auto &cp : caps) cp *= 2;
+    }
+    CK(cudaMemcpyAsync(d_cfg, cfg.data(), n * sizeof(SampleCfg), cudaMemcpyHostToDevice, st));
+    unsigned long long *distinct = ds.n<unsigned long long>(n);
+    CK(cudaMemsetAsync(distinct, 0, (size_t)n * 8, st));
+    CK(launch_compact_batch(arena, total_slots, d_cfg, n, nullptr, nullptr, nullptr, nullptr, nullptr, 0, distinct,
+                            counters, 1, st));
+    std::vector<unsigned long long> dist_h(n);
+    CK(cudaMemcpyAsync(dist_h.data(), distinct, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    uint64_t total_rec = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        cfg[i].rec_base = total_rec;
+        cfg[i].rec_cap = dist_h[i];
+        total_rec += dist_h[i];
+    }
+    CK(cudaMemcpyAsync(d_cfg, cfg.data(), n * sizeof(SampleCfg), cudaMemcpyHostToDevice, st));
+    unsigned long long *rec_keys = ds.n<unsigned long long>(std::max<uint64_t>(total_rec, 1));
+    uint32_t *rec_counts = ds.n<uint32_t>(std::max<uint64_t>(total_rec, 1));
+    unsigned long long *rec_len = ds.n<unsigned long long>(n);
+    unsigned long long *hist = ds.n<unsigned long long>((size_t)n * HIST_BINS_BATCH);
+    const uint64_t ovf_cap = 1 << 20;
+    unsigned long long *ovf = ds.n<unsigned long long>(ovf_cap);
+    CK(cudaMemsetAsync(rec_len, 0, (size_t)n * 8, st));
+    CK(cudaMemsetAsync(hist, 0, (size_t)n * HIST_BINS_BATCH * 8, st));
+    CK(cudaMemsetAsync(distinct, 0, (size_t)n * 8, st));
+    CK(launch_compact_batch(arena, total_slots, d_cfg, n, rec_len, rec_keys, rec_counts, hist, ovf, ovf_cap, distinct,
+                            counters, 0, st));
+    ds.release(arena);
+    std::vector<unsigned long long> len_h(n);
+    CK(cudaMemcpyAsync(len_h.data(), rec_len, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+    Counters c2 = read_counters(counters, st);
+    check_flags(c2.v[C_FLAGS], "compact");
+
+    std::vector<uint64_t> seg_start(n), seg_len(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        seg_start[i] = cfg[i].rec_base;
+        seg_len[i] = len_h[i];
+    }
+    if (total_rec > 1) {
+        void *stmp = ds.get(sort_tmp_bytes_segmented(total_rec, seg_len.data(), n));
+        CK(launch_radix_sort_segmented(rec_keys, rec_counts, total_rec, seg_start.data(), seg_len.data(), n, 2 * max_k,
+                                       stmp, st));
+        ds.release(stmp);
+    }
+    CK(launch_pair_reverse(rec_keys, total_rec, st));
+    CK(cudaEventRecord(ev1, st));
+
+    std::vector<unsigned long long> hist_h((size_t)n * HIST_BINS_BATCH);
+    CK(cudaMemcpyAsync(hist_h.data(), hist, hist_h.size() * 8, cudaMemcpyDeviceToHost, st));
+    const uint64_t n_ovf = std::min<uint64_t>(c2.v[C_OVF_LEN], ovf_cap);
+    std::vector<unsigned long long> ovf_h(n_ovf);
+    if (n_ovf) CK(cudaMemcpyAsync(ovf_h.data(), ovf, n_ovf * 8, cudaMemcpyDeviceToHost, st));
+    for (uint32_t i = 0; i < n; ++i) {
+        Job &j = *jobs[i];
+        if (!j.p.keep_records) continue;
+        j.keys.resize(len_h[i]);
+        j.counts.resize(len_h[i]);
+        if (len_h[i]) {
+            CK(cudaMemcpyAsync(j.keys.data(), rec_keys + cfg[i].rec_base, len_h[i] * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(j.counts.data(), rec_counts + cfg[i].rec_base, len_h[i] * 4, cudaMemcpyDeviceToHost, st));
+        }
+    }
+    CK(cudaStreamSynchronize(st));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ev0, ev1));
+    for (uint32_t i = 0; i < n; ++i) {
+        Job &j = *jobs[i];
+        j.device_ms = ms;
+        j.occurrences = occ_h[i];
+        j.distinct = dist_h[i];
+        j.table_cap = caps[i];
+        uint32_t lo = j.p.hist_min, hi = std::max(j.p.hist_max, j.p.hist_min);
+        j.hist.assign((uint64_t)hi - lo + 1, 0);
+        for (uint64_t c = std::max<uint64_t>(lo, 1); c < HIST_BINS_BATCH && c <= hi; ++c)
+            j.hist[c - lo] = (int64_t)hist_h[(size_t)i * HIST_BINS_BATCH + c];
+    }
+    for (unsigned long long e : ovf_h) {
+        uint32_t smp = (uint32_t)(e >> 32), c = (uint32_t)e;
+        Job &j = *jobs[smp];
+        if (c >= j.p.hist_min && c <= j.p.hist_max) j.hist[c - j.p.hist_min]++;
+    }
+}
+
+void worker_main(kc_handle *h)
+{
+    cudaSetDevice(h->device);
+    cudaStream_t st;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    for (;;) {
+        std::shared_ptr<Task> task;
+        {
+            std::unique_lock<std::mutex> lk(h->mu);
+            h->cv_work.wait(lk, [&] {
+                if (h->closing) return true;
+                if (h->queue.empty()) return false;
+                const auto &f = h->queue.front();
+                return h->running == 0 || h->reserved + f->reserve <= h->budget;
+            });
+            if (h->closing) break;
+            task = h->queue.front();
+            h->queue.pop_front();
+            h->reserved += task->reserve;
+            h->running++;
+            for (auto &j : task->jobs) {
+                j->state = JobState::RUNNING;
+                j->t_start = now_ms();
+            }
+        }
+        int code = KC_OK;
+        std::string msg;
+        try {
+            if (task->batch) run_batch(task->jobs, st);
+            else run_job(*task->jobs[0], st);
+        } catch (const KcError &e) {
+            code = e.code;
+            msg = e.msg;
+        } catch (const std::exception &e) {
+            code = KC_ERR_FAILED;
+            msg = e.what();
+        }
+        if (code != KC_OK) cudaStreamSynchronize(st);
+        {
+            std::lock_guard<std::mutex> lk(h->mu);
+            for (auto &j : task->jobs) {
+                j->t_end = now_ms();
+                j->state = code == KC_OK ? JobState::DONE : JobState::FAILED;
+                j->err = code;
+                j->err_msg = msg;
+            }
+            h->reserved -= task->reserve;
+            h->running--;
+        }
+        h->cv_work.notify_all();
+        h->cv_done.notify_all();
+    }
+    cudaStreamDestroy(st);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+uint64_t kc_kernel_launches(void) { return kernel_launches(); }
+
+void kc_job_defaults(kc_job *job)
+{
+    if (!job) return;
+    std::memset(job, 0, sizeof(*job));
+    job->k = 31;
+    job->count_max = 255;
+    job->memory_gb = 4;
+    job->filter_min = 2;
+    job->filter_max = 0xffffffffu;
+    job->min_count = 1;
+    job->max_count = 0xffffffffu;
+    job->hist_min = 1;
+    job->hist_max = 10000;
+    job->keep_records = 1;
+}
+
+int kc_open(const kc_config *cfg, kc_handle **out)
+{
+    if (!out) return fail(KC_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(KC_ERR_NO_DEVICE, "no CUDA device");
+    }
+    int dev = cfg ? cfg->device : 0;
+    if (dev < 0 || dev >= ndev) return fail(KC_ERR_INVALID, "device ordinal out of range");
+    if (cudaSetDevice(dev) != cudaSuccess) return fail(KC_ERR_CUDA, "cudaSetDevice failed");
+    // keep freed stream-ordered memory in the pool for the next job
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    auto *h = new kc_handle();
+    h->device = dev;
+    h->budget = (cfg && cfg->hbm_budget_bytes) ? cfg->hbm_budget_bytes : (uint64_t)(free_b * 0.9);
+    uint32_t nw = (cfg && cfg->max_inflight_jobs) ? cfg->max_inflight_jobs : 4;
+    for (uint32_t i = 0; i < nw; ++i) h->workers.emplace_back(worker_main, h);
+    *out = h;
+    return KC_OK;
+}
+
+void kc_close(kc_handle *h)
+{
+    if (!h) return;
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        h->closing = true;
+        for (auto &t : h->queue)
+            for (auto &j : t->jobs) {
+                j->state = JobState::FAILED;
+                j->err = KC_ERR_FAILED;
+                j->err_msg = "handle closed before the job started";
+            }
+        h->queue.clear();
+    }
+    h->cv_work.notify_all();
+    h->cv_done.notify_all();
+    for (auto &w : h->workers) w.join();
+    delete h;
+}
+
+int kc_input_upload(kc_handle *h, const kc_buffer *files, uint32_t n_files, kc_input **out)
+{
+    if (!h || !out || (n_files && !files)) return fail(KC_ERR_INVALID, "bad argument");
+    try {
+        cudaSetDevice(h->device);
+        auto *in = new kc_input();
+        std::vector<uint32_t> ts;
+        cudaStream_t st;
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        try {
+            build_input(*in, files, n_files, st, nullptr, ts);
+            CK(cudaStreamSynchronize(st));
+        } catch (...) {
+            cudaStreamDestroy(st);
+            if (in->base) cudaFree(in->base);
+            if (in->d_tile_seg) cudaFree(in->d_tile_seg);
+            delete in;
+            throw;
+        }
+        cudaStreamDestroy(st);
+        *out = in;
+        return KC_OK;
+    } catch (const KcError &e) {
+        return fail(e.code, e.msg);
+    }
+}
+
+void kc_input_free(kc_handle *h, kc_input *in)
+{
+    if (!in) return;
+    if (h) cudaSetDevice(h->device);
+    if (!in->stream_owned) {
+        cudaFree(in->base);
+        cudaFree(in->d_tile_seg);
+    }
+    delete in;
+}
+
+static int submit_task(kc_handle *h, const kc_job *jobs, uint32_t n, kc_job_id *ids, bool batch)
+{
+    if (!h || !jobs || !ids || n == 0) return fail(KC_ERR_INVALID, "bad argument");
+    auto task = std::make_shared<Task>();
+    task->batch = batch;
+    try {
+        for (uint32_t i = 0; i < n; ++i) {
+            validate_job(jobs[i]);
+            if (batch && jobs[i].bloom) throw KcError{KC_ERR_INVALID, "Bloom mode is not available for batched jobs"};
+            if (batch && (jobs[i].top_n || jobs[i].want_le2))
+                throw KcError{KC_ERR_INVALID, "count queries are not available for batched jobs"};
+            if (batch && jobs[i].input) throw KcError{KC_ERR_INVALID, "batched jobs take host files"};
+            auto j = std::make_shared<Job>();
+            j->p = jobs[i];
+            if (!jobs[i].input) j->files.assign(jobs[i].files, jobs[i].files + jobs[i].n_files);
+            j->p.files = nullptr;
+            j->input = jobs[i].input;
+            j->reserve = reserve_for(jobs[i], jobs[i].input ? jobs[i].input->total_bytes : 0);
+            task->reserve += j->reserve;
+            task->jobs.push_back(j);
+        }
+    } catch (const KcError &e) {
+        return fail(e.code, e.msg);
+    }
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        if (h->closing) return fail(KC_ERR_INVALID, "handle is closing");
+        double t = now_ms();
+        for (uint32_t i = 0; i < n; ++i) {
+            auto &j = task->jobs[i];
+            j->id = h->next_id++;
+            j->t_submit = t;
+            h->jobs[j->id] = j;
+            ids[i] = j->id;
+        }
+        h->queue.push_back(task);
+    }
+    h->cv_work.notify_all();
+    return KC_OK;
+}
+
+int kc_submit(kc_handle *h, const kc_job *job, kc_job_id *id) { return submit_task(h, job, 1, id, false); }
+
+int kc_submit_batch(kc_handle *h, const kc_job *jobs, uint32_t n_jobs, kc_job_id *ids)
+{
+    return submit_task(h, jobs, n_jobs, ids, true);
+}
+
+int kc_wait(kc_handle *h, kc_job_id id, int32_t timeout_ms)
+{
+    if (!h) return fail(KC_ERR_INVALID, "handle is NULL");
+    std::unique_lock<std::mutex> lk(h->mu);
+    auto it = h->jobs.find(id);
+    if (it == h->jobs.end()) return fail(KC_ERR_NOT_FOUND, "unknown job id");
+    auto j = it->second;
+    auto done = [&] { return j->state == JobState::DONE || j->state == JobState::FAILED; };
+    if (timeout_ms < 0) h->cv_done.wait(lk, done);
+    else if (!h->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), done))
+        return fail(KC_ERR_TIMEOUT, "job still running");
+    if (j->state == JobState::FAILED) return fail(j->err ? j->err : KC_ERR_FAILED, j->err_msg);
+    return KC_OK;
+}
+
+int kc_result(kc_handle *h, kc_job_id id, kc_result_t *out)
+{
+    if (!h || !out) return fail(KC_ERR_INVALID, "bad argument");
+    std::lock_guard<std::mutex> lk(h->mu);
+    auto it = h->jobs.find(id);
+    if (it == h->jobs.end()) return fail(KC_ERR_NOT_FOUND, "unknown job id");
+    Job &j = *it->second;
+    if (j.state != JobState::DONE) return fail(j.state == JobState::FAILED ? j.err : KC_ERR_INVALID, "job not finished");
+    std::memset(out, 0, sizeof(*out));
+    out->n_records = j.keys.size();
+    out->keys = j.keys.data();
+    out->counts = j.counts.data();
+    out->hist_len = j.hist.size();
+    out->hist = j.hist.data();
+    out->n_top = j.top_keys.size();
+    out->top_keys = j.top_keys.data();
+    out->top_counts = j.top_counts.data();
+    out->n_le2 = j.le2_keys.size();
+    out->le2_keys = j.le2_keys.data();
+    out->le2_counts = j.le2_counts.data();
+    out->occurrences = j.occurrences;
+    out->distinct = j.distinct;
+    out->low_only = j.low_only;
+    out->table_capacity = j.table_cap;
+    out->device_ms = j.device_ms;
+    out->queue_ms = j.t_start - j.t_submit;
+    out->run_ms = j.t_end - j.t_start;
+    for (int i = 0; i < 8; ++i) {
+        out->phase_ms[i] = j.phase_ms[i];
+        out->phase_launches[i] = j.phase_launches[i];
+    }
+    out->low_len = j.low_len;
+    out->high_len = j.high_len;
+    out->input_bytes = j.input_bytes;
+    out->n_records_total = j.n_records_total;
+    return KC_OK;
+}
+
+int kc_release(kc_handle *h, kc_job_id id)
+{
+    if (!h) return fail(KC_ERR_INVALID, "handle is NULL");
+    std::lock_guard<std::mutex> lk(h->mu);
+    auto it = h->jobs.find(id);
+    if (it == h->jobs.end()) return fail(KC_ERR_NOT_FOUND, "unknown job id");
+    if (it->second->state == JobState::QUEUED || it->second->state == JobState::RUNNING)
+        return fail(KC_ERR_INVALID, "job still running");
+    h->jobs.erase(it);
+    return KC_OK;
+}
+
+int kc_host_alloc(uint64_t bytes, void **p)
+{
+    if (!p) return fail(KC_ERR_INVALID, "p is NULL");
+    cudaError_t e = cudaHostAlloc(p, bytes ? bytes : 1, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return fail(KC_ERR_NOMEM, cudaGetErrorString(e));
+    }
+    return KC_OK;
+}
+
+int kc_host_free(void *p)
+{
+    if (p) cudaFreeHost(p);
+    return KC_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// reference tmp_dir files
+// ---------------------------------------------------------------------------
+
+namespace {
+
+bool write_all(FILE *f, const void *p, size_t n) { return n == 0 || fwrite(p, 1, n, f) == n; }
+
+}  // namespace
+
+extern "C" int kc_write_tmpdir(kc_handle *h, kc_job_id id, const char *dir)
+{
+    if (!h || !dir) return fail(KC_ERR_INVALID, "bad argument");
+    std::shared_ptr<Job> jp;
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        auto it = h->jobs.find(id);
+        if (it == h->jobs.end()) return fail(KC_ERR_NOT_FOUND, "unknown job id");
+        jp = it->second;
+        if (jp->state != JobState::DONE) return fail(KC_ERR_INVALID, "job not finished");
+    }
+    const Job &j = *jp;
+    if (!j.p.keep_records) return fail(KC_ERR_INVALID, "job was run without keep_records");
+    std::string d(dir);
+    if (!d.empty() && d.back() != '/') d += '/';
+    // infos.bin: u32 k, u32 count_max (src/main.cpp:590-597)
+    FILE *f = fopen((d + "infos.bin").c_str(), "wb");
+    if (!f) return fail(KC_ERR_IO, "cannot open " + d + "infos.bin");
+    uint32_t info[2] = {j.p.k, j.p.count_max};
+    bool ok = write_all(f, info, sizeof(info));
+    ok = (fclose(f) == 0) && ok;
+    if (!ok) return fail(KC_ERR_IO, "write failed: infos.bin");
+    // high.bin: exact counts, record = tail bytes of the masked word + count
+    // bytes (src/FinalDrainWriter.h:71-88); the counter-side filter
+    // (src/FinalDrainWriter.h:101) is applied to the exact count
+    const uint32_t k = j.p.k;
+    const uint32_t tail_bits = 2 * (k % 32), tail_bytes = (tail_bits + 7) / 8, full = k / 32;
+    const uint64_t tmask = tail_bits ? (~0ULL << (64 - tail_bits)) : 0;
+    const uint32_t cb = j.p.count_max <= 0xFF ? 1 : j.p.count_max <= 0xFFFF ? 2 : j.p.count_max <= 0xFFFFFF ? 3 : 4;
+    const uint32_t rec = full * 8 + tail_bytes + cb;
+    f = fopen((d + "high.bin").c_str(), "wb");
+    if (!f) return fail(KC_ERR_IO, "cannot open " + d + "high.bin");
+    std::vector<uint8_t> buf;
+    buf.reserve(std::min<size_t>(j.keys.size(), 1 << 20) * rec);
+    for (size_t i = 0; i < j.keys.size(); ++i) {
+        uint32_t c = j.counts[i];
+        if ((uint64_t)c + 1 < j.p.filter_min || c > j.p.filter_max) continue;
+        uint8_t r[16];
+        uint64_t w = j.keys[i];
+        if (full) std::memcpy(r, &w, 8);
+        else {
+            uint64_t t = w & tmask;
+            std::memcpy(r, reinterpret_cast<const uint8_t *>(&t) + (8 - tail_bytes), tail_bytes);
+        }
+        std::memcpy(r + full * 8 + tail_bytes, &c, cb);
+        buf.insert(buf.end(), r, r + rec);
+        if (buf.size() >= (64u << 20)) {
+            if (!write_all(f, buf.data(), buf.size())) { fclose(f); return fail(KC_ERR_IO, "write failed: high.bin"); }
+            buf.clear();
+        }
+    }
+    ok = write_all(f, buf.data(), buf.size());
+    ok = (fclose(f) == 0) && ok;
+    if (!ok) return fail(KC_ERR_IO, "write failed: high.bin");
+    // low.bin: every k-mer's occurrences are already merged into high.bin
+    f = fopen((d + "low.bin").c_str(), "wb");
+    if (!f) return fail(KC_ERR_IO, "cannot open " + d + "low.bin");
+    if (fclose(f) != 0) return fail(KC_ERR_IO, "write failed: low.bin");
+    return KC_OK;
+}
+

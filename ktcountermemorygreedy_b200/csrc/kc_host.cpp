@@ -1,0 +1,327 @@
+// kc_host.cpp -- shared host helpers and the single-step entry points of
+// include/kc.h (kc_extract_kmers, kc_hash_kmers, kc_sort_records,
+// kc_bloom_plan).  The single-step calls run synchronously on the current
+// device with a private stream.
+#include "kc_host.h"
+
+#include <algorithm>
+#include <cstring>
+
+#include "kc_plan.h"
+
+namespace kc {
+
+namespace {
+thread_local std::string g_err;
+}
+
+int set_error(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+void *DevScope::get(size_t bytes)
+{
+    void *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    bytes = (bytes + 255) & ~size_t(255);
+    cudaError_t e = cudaMallocAsync(&p, bytes, st);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw KcError{KC_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed"};
+    }
+    ptrs.push_back(p);
+    return p;
+}
+
+void DevScope::release(void *p)
+{
+    auto it = std::find(ptrs.begin(), ptrs.end(), p);
+    if (it != ptrs.end()) {
+        cudaFreeAsync(p, st);
+        ptrs.erase(it);
+    }
+}
+
+DevScope::~DevScope()
+{
+    for (void *p : ptrs) cudaFreeAsync(p, st);
+}
+
+uint64_t bit_ceil64(uint64_t x)
+{
+    if (x <= 1) return 1;
+    return 1ULL << (64 - __builtin_clzll(x - 1));
+}
+
+void build_input(kc_input &in, const kc_buffer *files, uint32_t n_files, cudaStream_t st, DevScope *scope,
+                 std::vector<uint32_t> &tile_seg_host, const uint32_t *file_sample)
+{
+    in.segs.clear();
+    in.sizes.clear();
+    in.total_bytes = 0;
+    uint64_t tiles = 0;
+    for (uint32_t f = 0; f < n_files; ++f) {
+        uint64_t sz = files[f].size;
+        in.sizes.push_back(sz);
+        in.total_bytes += sz;
+        if (sz == 0) continue;
+        Seg s{};
+        s.first_tile = tiles;
+        s.n_tiles = (sz + TILE - 1) / TILE;
+        s.len = sz;
+        s.sample = file_sample ? file_sample[f] : 0;
+        in.segs.push_back(s);
+        tiles += s.n_tiles;
+    }
+    in.n_tiles = tiles;
+    const size_t bytes = FRONT_PAD + tiles * (size_t)TILE + 256;
+    if (scope) {
+        in.base = static_cast<uint8_t *>(scope->get(bytes));
+        in.d_tile_seg = scope->n<uint32_t>(std::max<uint64_t>(tiles, 1));
+        in.stream_owned = true;
+    } else {
+        CK(cudaMalloc(&in.base, bytes));
+        CK(cudaMalloc(&in.d_tile_seg, std::max<uint64_t>(tiles, 1) * 4));
+    }
+    in.buf = in.base + FRONT_PAD;
+    CK(cudaMemsetAsync(in.base, 0, FRONT_PAD, st));
+    CK(cudaMemsetAsync(in.buf + tiles * (size_t)TILE, 0, 256, st));
+    tile_seg_host.assign(std::max<uint64_t>(tiles, 1), 0);
+    uint32_t si = 0;
+    for (uint32_t f = 0; f < n_files; ++f) {
+        if (files[f].size == 0) continue;
+        const Seg &s = in.segs[si];
+        uint8_t *dst = in.buf + s.first_tile * TILE;
+        CK(cudaMemcpyAsync(dst, files[f].data, files[f].size, cudaMemcpyHostToDevice, st));
+        const uint64_t pad = s.n_tiles * TILE - s.len;
+        if (pad) CK(cudaMemsetAsync(dst + s.len, 0, pad, st));
+        for (uint64_t t = 0; t < s.n_tiles; ++t) tile_seg_host[s.first_tile + t] = si;
+        ++si;
+    }
+    CK(cudaMemcpyAsync(in.d_tile_seg, tile_seg_host.data(), tile_seg_host.size() * 4, cudaMemcpyHostToDevice, st));
+}
+
+namespace {
+
+struct StreamGuard {
+    cudaStream_t st = nullptr;
+    StreamGuard()
+    {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+            cudaGetLastError();
+            throw KcError{KC_ERR_NO_DEVICE, "no CUDA device"};
+        }
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    }
+    ~StreamGuard()
+    {
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+    }
+};
+
+// Newline census + tile line numbers + per-file descriptors for one input.
+struct Prepared {
+    unsigned long long *tile_prefix = nullptr;
+    int32_t *tile_lastnl = nullptr;
+    Seg *d_segs = nullptr;
+    std::vector<Seg> segs;
+};
+
+Prepared prepare(const kc_input &in, uint32_t k, DevScope &ds, cudaStream_t st)
+{
+    Prepared p;
+    const uint64_t T = std::max<uint64_t>(in.n_tiles, 1);
+    uint32_t *tile_nl = ds.n<uint32_t>(T);
+    p.tile_lastnl = ds.n<int32_t>(T);
+    p.tile_prefix = ds.n<unsigned long long>(T);
+    unsigned long long *tmp = ds.n<unsigned long long>(scan_tmp_words(T));
+    CK(launch_newlines(in.buf, in.n_tiles, tile_nl, p.tile_lastnl, st));
+    CK(launch_scan_u32(tile_nl, p.tile_prefix, in.n_tiles, tmp, st));
+    p.segs = in.segs;
+    for (auto &s : p.segs) s.k = k;
+    p.d_segs = ds.n<Seg>(std::max<size_t>(p.segs.size(), 1));
+    if (!p.segs.empty())
+        CK(cudaMemcpyAsync(p.d_segs, p.segs.data(), p.segs.size() * sizeof(Seg), cudaMemcpyHostToDevice, st));
+    return p;
+}
+
+}  // namespace
+
+}  // namespace kc
+
+using namespace kc;
+
+extern "C" {
+
+const char *kc_last_error(void) { return kc::g_err.c_str(); }
+
+int kc_extract_kmers(const char *fastq, uint64_t len, uint32_t k, uint64_t *out, uint64_t cap, uint64_t *n_out)
+{
+    if ((!fastq && len) || (!out && cap) || !n_out) return set_error(KC_ERR_INVALID, "bad argument");
+    if (k < 1 || k > 32) return set_error(KC_ERR_INVALID, "k must be in 1..32");
+    try {
+        StreamGuard sg;
+        cudaStream_t st = sg.st;
+        DevScope ds(st);
+        kc_input in;
+        std::vector<uint32_t> ts;
+        kc_buffer f{fastq, len};
+        build_input(in, &f, 1, st, &ds, ts);
+        Prepared pr = prepare(in, k, ds, st);
+        unsigned long long *counters = ds.n<unsigned long long>(C_COUNT);
+        CK(cudaMemsetAsync(counters, 0, C_COUNT * 8, st));
+        const uint64_t lcap = std::max<uint64_t>(cap, 1);
+        unsigned long long *list = ds.n<unsigned long long>(lcap);
+        ExtractArgs a{};
+        a.buf = in.buf;
+        a.n_tiles = in.n_tiles;
+        a.tile_prefix = reinterpret_cast<const uint64_t *>(pr.tile_prefix);
+        a.tile_seg = in.d_tile_seg;
+        a.segs = pr.d_segs;
+        a.counters = counters;
+        a.list = list;
+        a.list_cap = cap;
+        CK(launch_extract(MODE_EMIT, a, 0, st));
+        unsigned long long c[C_COUNT];
+        CK(cudaMemcpyAsync(c, counters, sizeof(c), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (c[C_FLAGS] & ERR_WAIT_TIMEOUT) return set_error(KC_ERR_DEVICE, "bounded wait expired");
+        *n_out = c[C_EMIT_LEN];
+        uint64_t n = std::min<uint64_t>(c[C_EMIT_LEN], cap);
+        if (n) CK(cudaMemcpyAsync(out, list, n * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return KC_OK;
+    } catch (const KcError &e) {
+        return set_error(e.code, e.msg);
+    }
+}
+
+int kc_hash_kmers(const uint64_t *keys, uint64_t n, uint64_t *out)
+{
+    if ((!keys || !out) && n) return set_error(KC_ERR_INVALID, "bad argument");
+    if (!n) return KC_OK;
+    try {
+        StreamGuard sg;
+        DevScope ds(sg.st);
+        unsigned long long *dk = ds.n<unsigned long long>(n);
+        unsigned long long *dout = ds.n<unsigned long long>(5 * n);
+        CK(cudaMemcpyAsync(dk, keys, n * 8, cudaMemcpyHostToDevice, sg.st));
+        CK(launch_hash_batch(dk, n, dout, sg.st));
+        CK(cudaMemcpyAsync(out, dout, 5 * n * 8, cudaMemcpyDeviceToHost, sg.st));
+        CK(cudaStreamSynchronize(sg.st));
+        return KC_OK;
+    } catch (const KcError &e) {
+        return set_error(e.code, e.msg);
+    }
+}
+
+int kc_sort_records(uint64_t *keys, uint32_t *counts, uint64_t n, uint32_t bits)
+{
+    if ((!keys || !counts) && n) return set_error(KC_ERR_INVALID, "bad argument");
+    if (bits > 64) return set_error(KC_ERR_INVALID, "bits must be <= 64");
+    if (n <= 1) return KC_OK;
+    try {
+        StreamGuard sg;
+        DevScope ds(sg.st);
+        unsigned long long *dk = ds.n<unsigned long long>(n);
+        uint32_t *dv = ds.n<uint32_t>(n);
+        void *tmp = ds.get(sort_tmp_bytes(n));
+        CK(cudaMemcpyAsync(dk, keys, n * 8, cudaMemcpyHostToDevice, sg.st));
+        CK(cudaMemcpyAsync(dv, counts, n * 4, cudaMemcpyHostToDevice, sg.st));
+        CK(launch_radix_sort(dk, dv, n, bits, tmp, sg.st));
+        CK(cudaMemcpyAsync(keys, dk, n * 8, cudaMemcpyDeviceToHost, sg.st));
+        CK(cudaMemcpyAsync(counts, dv, n * 4, cudaMemcpyDeviceToHost, sg.st));
+        CK(cudaStreamSynchronize(sg.st));
+        return KC_OK;
+    } catch (const KcError &e) {
+        return set_error(e.code, e.msg);
+    }
+}
+
+int kc_plan_bloom(const uint32_t *raw_prefix_counts, uint32_t avg_quality, uint64_t est_file_size,
+                  uint64_t memory_gb, uint32_t k, uint64_t *capacities, uint64_t *max_capacity)
+{
+    if (!raw_prefix_counts || !capacities || !max_capacity) return set_error(KC_ERR_INVALID, "bad argument");
+    if (avg_quality > 255) return set_error(KC_ERR_INVALID, "avg_quality must fit in 8 bits");
+    BloomPlan bp = bloom_plan(raw_prefix_counts, (uint8_t)avg_quality, est_file_size, memory_gb, k);
+    std::memcpy(capacities, bp.caps, sizeof(bp.caps));
+    *max_capacity = bp.max_cap;
+    return KC_OK;
+}
+
+int kc_bloom_plan(const kc_buffer *files, uint32_t n_files, uint32_t k, uint64_t memory_gb, uint32_t *prefix_counts,
+                  uint32_t *avg_quality, uint64_t *capacities, uint64_t *max_capacity)
+{
+    if (!files || !n_files || !prefix_counts || !avg_quality || !capacities || !max_capacity)
+        return set_error(KC_ERR_INVALID, "bad argument");
+    if (k < 1 || k > 32) return set_error(KC_ERR_INVALID, "k must be in 1..32");
+    try {
+        StreamGuard sg;
+        cudaStream_t st = sg.st;
+        DevScope ds(st);
+        kc_input in;
+        std::vector<uint32_t> ts;
+        build_input(in, files, n_files, st, &ds, ts);
+        Prepared pr = prepare(in, k, ds, st);
+        const uint64_t limit = n_files == 1 ? (256ULL << 20) : (128ULL << 20);
+        std::vector<uint64_t> chunk0(std::max<size_t>(pr.segs.size(), 1), 0);
+        uint64_t n_chunks = 0;
+        for (size_t i = 0; i < pr.segs.size(); ++i) {
+            pr.segs[i].sample_end = std::min(pr.segs[i].len, limit);
+            chunk0[i] = n_chunks;
+            n_chunks += (pr.segs[i].len + PREPASS_CHUNK - 1) / PREPASS_CHUNK;
+        }
+        if (!pr.segs.empty())
+            CK(cudaMemcpyAsync(pr.d_segs, pr.segs.data(), pr.segs.size() * sizeof(Seg), cudaMemcpyHostToDevice, st));
+        int32_t *chunk_lastnl = ds.n<int32_t>(std::max<uint64_t>(n_chunks, 1));
+        uint64_t *d_chunk0 = ds.n<uint64_t>(chunk0.size());
+        uint32_t *ph = ds.n<uint32_t>(256);
+        unsigned long long *qual = ds.n<unsigned long long>(2);
+        unsigned long long *occ = ds.n<unsigned long long>(1);
+        uint32_t *hll = ds.n<uint32_t>(HLL_M);
+        unsigned long long *counters = ds.n<unsigned long long>(C_COUNT);
+        CK(cudaMemsetAsync(chunk_lastnl, 0xff, std::max<uint64_t>(n_chunks, 1) * 4, st));
+        CK(cudaMemcpyAsync(d_chunk0, chunk0.data(), chunk0.size() * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(ph, 0, 1024, st));
+        CK(cudaMemsetAsync(qual, 0, 16, st));
+        CK(cudaMemsetAsync(occ, 0, 8, st));
+        CK(cudaMemsetAsync(hll, 0, HLL_M * 4, st));
+        CK(cudaMemsetAsync(counters, 0, C_COUNT * 8, st));
+        CK(launch_chunk_lastnl(pr.tile_lastnl, in.d_tile_seg, pr.d_segs, d_chunk0, in.n_tiles, chunk_lastnl, st));
+        ExtractArgs a{};
+        a.buf = in.buf;
+        a.n_tiles = in.n_tiles;
+        a.tile_prefix = reinterpret_cast<const uint64_t *>(pr.tile_prefix);
+        a.tile_seg = in.d_tile_seg;
+        a.segs = pr.d_segs;
+        a.counters = counters;
+        a.occ = occ;
+        a.hll = hll;
+        a.prepass = 1;
+        a.chunk_lastnl = chunk_lastnl;
+        a.seg_chunk0 = d_chunk0;
+        a.prefix_hist = ph;
+        a.qual = qual;
+        CK(launch_extract(MODE_SCAN, a, 0, st));
+        unsigned long long q[2];
+        CK(cudaMemcpyAsync(prefix_counts, ph, 1024, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(q, qual, 16, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        uint8_t avg = q[1] ? (uint8_t)(q[0] / q[1]) : 0;
+        *avg_quality = avg;
+        BloomPlan bp = bloom_plan(prefix_counts, avg, in.total_bytes, memory_gb, k);
+        std::memcpy(capacities, bp.caps, sizeof(bp.caps));
+        *max_capacity = bp.max_cap;
+        return KC_OK;
+    } catch (const KcError &e) {
+        return set_error(e.code, e.msg);
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,1280 @@
+// kc_kernels.cu -- the sm_100a device pipeline of the k-mer counter.
+//
+// Stages (one job; batched jobs run the same kernels over many files):
+//   k_newlines      per-tile '\n' count and last '\n' offset (16-byte loads)
+//   scan            exclusive prefix of the tile counts -> line number of
+//                   every tile start (FASTQ line state machine without a
+//                   sequential pass)
+//   k_extract<M>    TMA-bulk-loaded 8 KiB tiles; per 32-byte segment the
+//                   2-bit codes, valid-base mask and sequence-line mask; the
+//                   ends of all windows of k valid bases found with a
+//                   bit-parallel run test; canonical words formed directly
+//                   from the packed codes.  The mode decides what happens to
+//                   each canonical k-mer: count + HyperLogLog (SCAN), insert
+//                   into the open-addressing table (INSERT), classify with the
+//                   reference's two-level Bloom filter (BLOOM) or append to a
+//                   list (EMIT).
+//   k_insert_list   insert a k-mer list (Bloom non-FIRST occurrences)
+//   k_merge_low     add the FIRST occurrences back (exact merged counts)
+//   k_compact       table -> (string-order key, count) records + histogram
+//   radix sort      LSD, 8-bit digits, warp match ranking, stable
+//   selection       stable range selection for the count queries
+#include <algorithm>
+#include <atomic>
+#include <utility>
+#include <vector>
+
+#include "kc_device.cuh"
+#include "kc_kernels.cuh"
+
+namespace kc {
+
+namespace {
+
+constexpr uint32_t FULL = 0xffffffffu;
+constexpr uint32_t BUF_BYTES = TILE + HALO;   // 8224, a multiple of 16
+
+__device__ __forceinline__ uint32_t lanemask_lt()
+{
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Exclusive scan of one value per thread over a 256-thread block.
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *s_warp, uint32_t &total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < 8 ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            uint32_t y = __shfl_up_sync(FULL, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < 8) s_warp[lane] = w;
+    }
+    __syncthreads();
+    uint32_t base = warp ? s_warp[warp - 1] : 0;
+    total = s_warp[7];
+    __syncthreads();
+    return base + x - v;
+}
+
+// 2-bit codes (A0 C1 G2 T/U3, case-insensitive, as the reference's
+// char_to_2bit table and its AVX2 classifier), valid-base mask and newline
+// mask of 32 bytes at p (16-byte aligned shared memory).
+__device__ __forceinline__ void classify32(const uint8_t *p, uint64_t &codes, uint32_t &valid, uint32_t &nl)
+{
+    const uint4 a = *reinterpret_cast<const uint4 *>(p);
+    const uint4 b = *reinterpret_cast<const uint4 *>(p + 16);
+    const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    uint64_t c = 0;
+    uint32_t v = 0, n = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        // newline bytes: __vcmpeq4 sets a byte to 0xff where equal
+        uint32_t eq = __vcmpeq4(w[i], 0x0a0a0a0au);
+        n |= (((eq >> 7) & 1u) | ((eq >> 14) & 2u) | ((eq >> 21) & 4u) | ((eq >> 28) & 8u)) << (4 * i);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            uint32_t u = (w[i] >> (8 * j)) & 0xDFu;
+            uint32_t d = u - 0x40u;
+            uint32_t ok = (d < 32u) ? ((0x30008Au >> d) & 1u) : 0u;   // A C G T U
+            uint32_t code = ((u >> 1) & 3u) ^ ((u >> 2) & 1u);
+            c |= (uint64_t)code << (2 * (4 * i + j));
+            v |= ok << (4 * i + j);
+        }
+    }
+    codes = c;
+    valid = v;
+    nl = n;
+}
+
+__device__ __forceinline__ uint32_t range_mask(uint32_t a, uint32_t b)
+{
+    uint32_t hi = b >= 32 ? FULL : ((1u << b) - 1u);
+    uint32_t lo = a >= 32 ? FULL : ((1u << a) - 1u);
+    return hi & ~lo;
+}
+
+// Bytes of the 32-byte segment that lie in lines whose number is
+// `want` mod 4, given the line number at the segment start.
+__device__ __forceinline__ uint32_t line_mask(uint64_t line0, uint32_t nl, uint32_t want)
+{
+    uint32_t m = 0, pos = 0, bits = nl;
+    uint64_t cur = line0;
+    while (bits) {
+        uint32_t j = __ffs(bits) - 1;
+        if ((cur & 3) == want) m |= range_mask(pos, j);
+        ++cur;
+        pos = j + 1;
+        bits &= bits - 1;
+    }
+    if ((cur & 3) == want) m |= range_mask(pos, 32);
+    return m;
+}
+
+// Bit b (b >= 32) of the result is set when bits b-k+1 .. b of g are all set.
+__device__ __forceinline__ uint32_t run_ends(uint64_t g, uint32_t k)
+{
+    uint64_t r1 = g, r2 = r1 & (r1 << 1), r4 = r2 & (r2 << 2), r8 = r4 & (r4 << 4), r16 = r8 & (r8 << 8);
+    uint64_t acc = ~0ULL;
+    uint32_t sh = 0;
+    if (k & 32) { acc &= r16 & (r16 << 16); sh = 32; }
+    if (k & 16) { acc &= r16 << sh; sh += 16; }
+    if (k & 8) { acc &= r8 << sh; sh += 8; }
+    if (k & 4) { acc &= r4 << sh; sh += 4; }
+    if (k & 2) { acc &= r2 << sh; sh += 2; }
+    if (k & 1) { acc &= r1 << sh; sh += 1; }
+    return (uint32_t)(acc >> 32);
+}
+
+struct KParams {
+    uint32_t k;
+    uint64_t kmask;     // low 2k bits
+    uint64_t topmask;   // high 2k bits
+    uint32_t fwd_shift; // 64 - 2k
+};
+
+__device__ __forceinline__ KParams kparams(uint32_t k)
+{
+    KParams p;
+    p.k = k;
+    p.kmask = k >= 32 ? ~0ULL : ((1ULL << (2 * k)) - 1ULL);
+    p.fwd_shift = 64 - 2 * k;
+    p.topmask = k >= 32 ? ~0ULL : (~0ULL << p.fwd_shift);
+    return p;
+}
+
+// Canonical internal word of the window ending at position j (0..31) of the
+// current segment.  prev/cur hold the 2-bit codes of the previous and current
+// segments, base q at bits 2q.  The forward word puts base i of the window at
+// bit 64-2k+2i (the reference's kmer<1> layout); the reverse complement is the
+// 2-bit-group reversal with every code complemented.  The canonical word is
+// the smaller of the two, as GetKmer::canonicalize.
+__device__ __forceinline__ unsigned long long window_key(uint64_t prev, uint64_t cur, uint32_t j, const KParams &kp)
+{
+    int s = 33 + (int)j - (int)kp.k;   // window start in the 64-position span, 1..63
+    uint64_t x;
+    if (s >= 32) x = cur >> (2 * (s - 32));
+    else x = (prev >> (2 * s)) | (cur << (64 - 2 * s));
+    x &= kp.kmask;
+    uint64_t fwd = kp.fwd_shift >= 64 ? 0 : (x << kp.fwd_shift);
+    uint64_t rc = pair_reverse(x) ^ kp.topmask;
+    return fwd < rc ? fwd : rc;
+}
+
+__device__ __forceinline__ void hll_add(uint32_t *regs, unsigned long long key)
+{
+    uint64_t h = slot_hash(key ^ 0x5bd1e9955bd1e995ULL);
+    uint32_t r = (uint32_t)(h >> (64 - HLL_BITS));
+    uint32_t rank = __clzll((h << HLL_BITS) | (1ULL << (HLL_BITS - 1))) + 1;
+    if (rank > *(volatile uint32_t *)&regs[r]) atomicMax(&regs[r], rank);
+}
+
+__device__ __forceinline__ bool table_add(Slot *slots, unsigned long long mask, unsigned long long key,
+                                          unsigned int c, uint32_t max_probe)
+{
+    unsigned long long i = slot_hash(key) & mask;
+    for (uint32_t n = 0; n < max_probe; ++n) {
+        unsigned long long cur = __ldcg(&slots[i].key);
+        if (cur == key) {
+            atomicAdd(&slots[i].count, c);
+            return true;
+        }
+        if (cur == EMPTY_KEY) {
+            unsigned long long prev = atomicCAS(&slots[i].key, EMPTY_KEY, key);
+            if (prev == EMPTY_KEY || prev == key) {
+                atomicAdd(&slots[i].count, c);
+                return true;
+            }
+        }
+        i = (i + 1) & mask;
+    }
+    return false;
+}
+
+__device__ __forceinline__ Slot *table_find(Slot *slots, unsigned long long mask, unsigned long long key,
+                                            uint32_t max_probe, bool &overflow)
+{
+    unsigned long long i = slot_hash(key) & mask;
+    for (uint32_t n = 0; n < max_probe; ++n) {
+        unsigned long long cur = __ldcg(&slots[i].key);
+        if (cur == key) return &slots[i];
+        if (cur == EMPTY_KEY) return nullptr;
+        i = (i + 1) & mask;
+    }
+    overflow = true;
+    return nullptr;
+}
+
+// Warp-aggregated insert: lanes holding the same k-mer elect one leader that
+// adds the group's size.
+__device__ __forceinline__ void warp_insert(bool act, unsigned long long key, const TableRef &tr,
+                                            uint32_t max_probe, unsigned long long *flags)
+{
+    unsigned long long k = act ? key : EMPTY_KEY;
+    uint32_t peers = __match_any_sync(FULL, k);
+    if (act && (int)(threadIdx.x & 31) == __ffs(peers) - 1) {
+        if (!table_add(tr.slots, tr.mask, k, __popc(peers), max_probe)) atomicOr(flags, ERR_TABLE_FULL);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// newline census
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256) k_newlines(const uint8_t *buf, uint64_t n_tiles, uint32_t *tile_nl,
+                                                  int32_t *tile_lastnl)
+{
+    __shared__ uint32_t s_cnt[8];
+    __shared__ int32_t s_last[8];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (uint64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        const uint4 *p = reinterpret_cast<const uint4 *>(buf + t * TILE + 32 * tid);
+        uint4 a = __ldcs(p), b = __ldcs(p + 1);
+        const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        uint32_t cnt = 0;
+        int32_t last = -1;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            uint32_t eq = __vcmpeq4(w[i], 0x0a0a0a0au);
+            cnt += __popc(eq) >> 3;
+            if (eq) last = 32 * tid + 4 * i + (31 - __clz(eq)) / 8;
+        }
+        cnt = __reduce_add_sync(FULL, cnt);
+        last = __reduce_max_sync(FULL, last);
+        if (lane == 0) { s_cnt[warp] = cnt; s_last[warp] = last; }
+        __syncthreads();
+        if (tid == 0) {
+            uint32_t c = 0;
+            int32_t l = -1;
+            for (int i = 0; i < 8; ++i) { c += s_cnt[i]; l = max(l, s_last[i]); }
+            tile_nl[t] = c;
+            tile_lastnl[t] = l;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_chunk_lastnl(const int32_t *tile_lastnl, const uint32_t *tile_seg, const Seg *segs,
+                               const uint64_t *seg_chunk0, uint64_t n_tiles, int32_t *chunk_lastnl)
+{
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n_tiles; t += (uint64_t)gridDim.x * blockDim.x) {
+        int32_t l = tile_lastnl[t];
+        if (l < 0) continue;
+        uint32_t s = tile_seg[t];
+        uint64_t fo = (t - segs[s].first_tile) * TILE;
+        uint64_t c = seg_chunk0[s] + fo / PREPASS_CHUNK;
+        atomicMax(&chunk_lastnl[c], (int32_t)(fo % PREPASS_CHUNK) + l);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// extraction
+// ---------------------------------------------------------------------------
+
+template <int MODE>
+__global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t stage_cap)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint8_t *sbuf[2] = {smem, smem + BUF_BYTES};
+    uint64_t *s_codes = reinterpret_cast<uint64_t *>(smem + 2 * BUF_BYTES);   // 257 used
+    uint32_t *s_good = reinterpret_cast<uint32_t *>(s_codes + 264);           // 257 used
+    unsigned long long *s_stage = reinterpret_cast<unsigned long long *>(s_good + 264);
+
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t s_warp[8];
+    __shared__ uint32_t s_hist[256];
+    __shared__ unsigned long long s_bcast[2];
+    __shared__ unsigned long long s_boff[MODE == MODE_BLOOM ? 256 : 1];
+    __shared__ unsigned long long s_bcap[MODE == MODE_BLOOM ? 256 : 1];
+
+    const int tid = threadIdx.x, lane = tid & 31;
+    uint64_t t = blockIdx.x;
+    if (t >= a.n_tiles) return;
+
+    if (tid == 0) {
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        fence_mbar_init();
+    }
+    if (MODE == MODE_SCAN) s_hist[tid] = 0;
+    if (MODE == MODE_BLOOM) {
+        s_boff[tid] = a.bloom_off[tid];
+        s_bcap[tid] = a.bloom_cap[tid];
+    }
+    __syncthreads();
+    if (tid == 0) {
+        mbar_expect_tx(&mbar[0], BUF_BYTES);
+        bulk_load(sbuf[0], a.buf + t * TILE - HALO, BUF_BYTES, &mbar[0]);
+    }
+
+    unsigned long long *flags = &a.counters[C_FLAGS];
+    uint32_t iter = 0;
+    bool pending_next = false;
+    for (; t < a.n_tiles; t += gridDim.x, ++iter) {
+        const int s = iter & 1;
+        const uint64_t tn = t + gridDim.x;
+        pending_next = tn < a.n_tiles;
+        if (tid == 0 && pending_next) {
+            fence_proxy_async_smem();
+            mbar_expect_tx(&mbar[s ^ 1], BUF_BYTES);
+            bulk_load(sbuf[s ^ 1], a.buf + tn * TILE - HALO, BUF_BYTES, &mbar[s ^ 1]);
+        }
+        bool ok = mbar_wait(&mbar[s], (iter >> 1) & 1);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicOr(flags, ERR_WAIT_TIMEOUT);
+            if (pending_next) mbar_wait(&mbar[s ^ 1], ((iter + 1) >> 1) & 1);
+            return;
+        }
+        const uint8_t *tb = sbuf[s];
+
+        const uint32_t seg_id = a.tile_seg[t];
+        const Seg sg = a.segs[seg_id];
+        const bool first = (t == sg.first_tile);
+        const uint64_t line0 = a.tile_prefix[t] - a.tile_prefix[sg.first_tile];
+        const uint64_t fo = (t - sg.first_tile) * TILE;
+        const KParams kp = kparams(sg.k);
+
+        // per-segment classification
+        uint64_t codes;
+        uint32_t valid, nl;
+        classify32(tb + HALO + 32 * tid, codes, valid, nl);
+        uint32_t tot_nl;
+        const uint32_t excl_nl = block_excl_scan(__popc(nl), s_warp, tot_nl);
+        const uint64_t lstart = line0 + excl_nl;
+        s_codes[tid + 1] = codes;
+        s_good[tid + 1] = valid & line_mask(lstart, nl, 1);
+        if (tid == 0) {
+            if (first) {
+                s_codes[0] = 0;
+                s_good[0] = 0;
+            } else {
+                uint64_t c0;
+                uint32_t v0, n0;
+                classify32(tb, c0, v0, n0);
+                s_codes[0] = c0;
+                s_good[0] = v0 & line_mask(line0 - __popc(n0), n0, 1);
+            }
+        }
+        const uint64_t seg_pos = fo + 32 * (uint64_t)tid;   // file offset of this thread's segment
+        if (MODE == MODE_SCAN && a.prepass) {
+            // quality bytes of complete quality lines, counted from the start
+            // of the 2 MiB chunk holding the line's '\n' (the reference's
+            // reader sums per chunk)
+            uint32_t qm = 0;
+            if (seg_pos < sg.sample_end) {
+                qm = line_mask(lstart, nl, 3) & ~nl;
+                uint64_t lim = sg.sample_end - seg_pos;
+                if (lim < 32) qm &= (1u << lim) - 1u;
+                int32_t cl = a.chunk_lastnl[a.seg_chunk0[seg_id] + seg_pos / PREPASS_CHUNK];
+                int64_t room = (int64_t)cl - (int64_t)(seg_pos % PREPASS_CHUNK);
+                if (room <= 0) qm = 0;
+                else if (room < 32) qm &= (1u << room) - 1u;
+            }
+            long long qs = 0;
+            const uint8_t *pb = tb + HALO + 32 * tid;
+            for (uint32_t m = qm; m; m &= m - 1) qs += (long long)(signed char)pb[__ffs(m) - 1];
+            unsigned qn = __reduce_add_sync(FULL, (unsigned)__popc(qm));
+            for (int o = 16; o > 0; o >>= 1) qs += __shfl_down_sync(FULL, qs, o);
+            if (lane == 0 && qn) {
+                atomicAdd(&a.qual[2 * sg.sample], (unsigned long long)qs);
+                atomicAdd(&a.qual[2 * sg.sample + 1], (unsigned long long)qn);
+            }
+        }
+        __syncthreads();
+
+        // windows of k valid bases ending in this thread's segment
+        const uint64_t prev = s_codes[tid], cur = s_codes[tid + 1];
+        const uint64_t g = (uint64_t)s_good[tid] | ((uint64_t)s_good[tid + 1] << 32);
+        uint32_t ends = run_ends(g, kp.k);
+
+        if (MODE == MODE_SCAN) {
+            uint32_t sample_ok = 0;
+            if (a.prepass && seg_pos < sg.sample_end) {
+                uint64_t lim = sg.sample_end - seg_pos;
+                sample_ok = lim >= 32 ? FULL : ((1u << lim) - 1u);
+            }
+            uint32_t e = ends;
+            uint32_t hll_base = sg.sample * HLL_M;
+            while (e) {
+                uint32_t j = __ffs(e) - 1;
+                e &= e - 1;
+                unsigned long long key = window_key(prev, cur, j, kp);
+                hll_add(a.hll + hll_base, key);
+                if ((sample_ok >> j) & 1u) atomicAdd(&s_hist[key >> 56], 1u);
+            }
+            unsigned n = __reduce_add_sync(FULL, (unsigned)__popc(ends));
+            if (lane == 0 && n) atomicAdd(&a.occ[sg.sample], (unsigned long long)n);
+        } else {
+            uint32_t tot;
+            const uint32_t off = block_excl_scan(__popc(ends), s_warp, tot);
+            for (uint32_t base = 0; base < tot; base += stage_cap) {
+                uint32_t e = ends, idx = off;
+                while (e) {
+                    uint32_t j = __ffs(e) - 1;
+                    e &= e - 1;
+                    if (idx >= base && idx < base + stage_cap) s_stage[idx - base] = window_key(prev, cur, j, kp);
+                    ++idx;
+                }
+                __syncthreads();
+                const uint32_t nr = min(stage_cap, tot - base);
+                if (MODE == MODE_INSERT) {
+                    const TableRef tr = a.tables[sg.sample];
+                    for (uint32_t r0 = 0; r0 < nr; r0 += EXT_THREADS) {
+                        uint32_t i = r0 + tid;
+                        bool act = i < nr;
+                        warp_insert(act, act ? s_stage[i] : EMPTY_KEY, tr, a.max_probe, flags);
+                    }
+                } else if (MODE == MODE_EMIT) {
+                    if (tid == 0) s_bcast[0] = atomicAdd(&a.counters[C_EMIT_LEN], (unsigned long long)nr);
+                    __syncthreads();
+                    const unsigned long long b0 = s_bcast[0];
+                    for (uint32_t i = tid; i < nr; i += EXT_THREADS) {
+                        if (b0 + i < a.list_cap) a.list[b0 + i] = s_stage[i];
+                        else atomicOr(flags, ERR_LIST_FULL);
+                    }
+                } else if (MODE == MODE_BLOOM) {
+                    uint32_t firsts = 0, highs = 0;
+                    for (uint32_t r = 0, i = tid; i < nr; ++r, i += EXT_THREADS) {
+                        unsigned long long key = s_stage[i];
+                        uint32_t p = (uint32_t)(key >> 56);
+                        uint64_t block, m;
+                        bloom_probe(key, s_bcap[p], block, m);
+                        unsigned long long *cell = a.bloom_bits + s_boff[p] + 2 * block;
+                        // ConcurrentBloomFilter::insert_prepared (src/BloomFilter.h:233-273)
+                        bool first_occ = false;
+                        unsigned long long bf1 = __ldcg(&cell[0]);
+                        if ((bf1 & m) != m) {
+                            unsigned long long bf2 = __ldcg(&cell[1]);
+                            if ((bf2 & m) == m) {
+                                atomicOr(&cell[0], (unsigned long long)m);
+                            } else {
+                                unsigned long long old2 = atomicOr(&cell[1], (unsigned long long)m);
+                                if ((old2 & m) == m) atomicOr(&cell[0], (unsigned long long)m);
+                                else first_occ = true;
+                            }
+                        }
+                        if (first_occ) firsts |= 1u << r;
+                        else {
+                            highs |= 1u << r;
+                            hll_add(a.hll_high, key);
+                        }
+                    }
+                    uint32_t tf, th;
+                    const uint32_t of = block_excl_scan(__popc(firsts), s_warp, tf);
+                    const uint32_t oh = block_excl_scan(__popc(highs), s_warp, th);
+                    if (tid == 0) {
+                        s_bcast[0] = atomicAdd(&a.counters[C_LOW_LEN], (unsigned long long)tf);
+                        s_bcast[1] = atomicAdd(&a.counters[C_HIGH_LEN], (unsigned long long)th);
+                    }
+                    __syncthreads();
+                    const unsigned long long lb = s_bcast[0] + of, hb = s_bcast[1] + oh;
+                    uint32_t nf = 0, nh = 0;
+                    for (uint32_t r = 0, i = tid; i < nr; ++r, i += EXT_THREADS) {
+                        unsigned long long key = s_stage[i];
+                        if ((firsts >> r) & 1u) {
+                            unsigned long long pos = lb + nf++;
+                            if (pos < a.list_cap) a.list[pos] = key;
+                            else atomicOr(flags, ERR_LIST_FULL);
+                        } else {
+                            unsigned long long pos = hb + nh++;
+                            if (pos < a.list_cap) a.list[a.list_cap - 1 - pos] = key;
+                            else atomicOr(flags, ERR_LIST_FULL);
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        __syncthreads();
+    }
+
+    if (MODE == MODE_SCAN && a.prepass) {
+        // one file-sample per job in Bloom mode; the histogram belongs to sample 0
+        uint32_t v = s_hist[tid];
+        if (v) atomicAdd(&a.prefix_hist[tid], v);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// table phases
+// ---------------------------------------------------------------------------
+
+__global__ void k_init_slots(Slot *slots, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        slots[i].key = EMPTY_KEY;
+        slots[i].count = 0;
+        slots[i].pad = 0;
+    }
+}
+
+__global__ void k_count_keys(const Slot *slots, uint64_t n, unsigned long long *out)
+{
+    unsigned c = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        c += slots[i].key != EMPTY_KEY;
+    c = __reduce_add_sync(FULL, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, (unsigned long long)c);
+}
+
+__global__ void k_fill_u64(unsigned long long *p, uint64_t n, unsigned long long v)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+__global__ void __launch_bounds__(256) k_insert_list(const unsigned long long *keys, uint64_t n, TableRef t,
+                                                     uint32_t max_probe, unsigned long long *counters)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    // whole warps iterate together so __match_any_sync sees all lanes
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        uint64_t i = base + (threadIdx.x & 31);
+        bool act = i < n;
+        warp_insert(act, act ? keys[i] : EMPTY_KEY, t, max_probe, &counters[C_FLAGS]);
+    }
+}
+
+__global__ void k_insert_pairs(const unsigned long long *keys, const uint32_t *counts, uint64_t n, TableRef t,
+                               uint32_t max_probe, unsigned long long *counters)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if (!table_add(t.slots, t.mask, keys[i], counts[i], max_probe)) atomicOr(&counters[C_FLAGS], ERR_TABLE_FULL);
+}
+
+// Block-aggregated append of (string key, count) records.
+__device__ __forceinline__ void append_records(bool keep, unsigned long long skey, uint32_t c,
+                                               unsigned long long *rec_keys, uint32_t *rec_counts,
+                                               uint64_t rec_cap, unsigned long long *counters,
+                                               uint32_t *s_warp, unsigned long long *s_base)
+{
+    uint32_t tot;
+    uint32_t off = block_excl_scan(keep ? 1u : 0u, s_warp, tot);
+    if (threadIdx.x == 0) *s_base = tot ? atomicAdd(&counters[C_REC_LEN], (unsigned long long)tot) : 0ull;
+    __syncthreads();
+    unsigned long long pos = *s_base + off;
+    if (keep) {
+        if (pos < rec_cap) {
+            rec_keys[pos] = skey;
+            rec_counts[pos] = c;
+        } else {
+            atomicOr(&counters[C_FLAGS], ERR_RECORDS_FULL);
+        }
+    }
+    __syncthreads();
+}
+
+// FIRST occurrences: a hit adds the low-list occurrence to the table count
+// (the tools' merge, LowFrequencyQueryThreadPool::process_block); a miss is a
+// k-mer whose only occurrence is this one.
+__global__ void __launch_bounds__(256) k_merge_low(const unsigned long long *keys, uint64_t n, TableRef t,
+                                                   uint32_t max_probe, uint32_t min_count, uint32_t max_count,
+                                                   unsigned long long *rec_keys, uint32_t *rec_counts,
+                                                   uint64_t rec_cap, unsigned long long *counters)
+{
+    __shared__ uint32_t s_warp[8];
+    __shared__ unsigned long long s_base;
+    const bool want1 = (min_count <= 1 && 1 <= max_count);
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t rounds = (n + stride - 1) / stride;
+    for (uint64_t r = 0; r < rounds; ++r) {
+        uint64_t i = r * stride + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        bool miss = false;
+        unsigned long long key = 0;
+        if (i < n) {
+            key = keys[i];
+            bool ovf = false;
+            Slot *sl = table_find(t.slots, t.mask, key, max_probe, ovf);
+            if (ovf) atomicOr(&counters[C_FLAGS], ERR_TABLE_FULL);
+            if (sl) atomicAdd(&sl->count, 1u);
+            else miss = true;
+        }
+        unsigned m = __reduce_add_sync(FULL, miss ? 1u : 0u);
+        if ((threadIdx.x & 31) == 0 && m) atomicAdd(&counters[C_LOW_ONLY], (unsigned long long)m);
+        append_records(miss && want1, pair_reverse(key), 1u, rec_keys, rec_counts, rec_cap, counters, s_warp, &s_base);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_compact(TableRef t, uint64_t cap, uint32_t count_max, uint32_t min_count,
+                                                 uint32_t max_count, unsigned long long *rec_keys,
+                                                 uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist,
+                                                 uint32_t *ovf, uint64_t ovf_cap, unsigned long long *counters)
+{
+    __shared__ uint32_t s_warp[8];
+    __shared__ unsigned long long s_base;
+    __shared__ uint32_t s_hist[2048];
+    for (int i = threadIdx.x; i < 2048; i += blockDim.x) s_hist[i] = 0;
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t rounds = (cap + stride - 1) / stride;
+    uint32_t distinct = 0;
+    for (uint64_t r = 0; r < rounds; ++r) {
+        uint64_t i = r * stride + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        bool keep = false;
+        unsigned long long skey = 0;
+        uint32_t c = 0;
+        if (i < cap) {
+            Slot sl = t.slots[i];
+            if (sl.key != EMPTY_KEY) {
+                ++distinct;
+                c = sl.count < count_max ? sl.count : count_max;
+                if (c < 2048) atomicAdd(&s_hist[c], 1u);
+                else if (c < HIST_BINS) atomicAdd(&hist[c], 1ull);
+                else {
+                    unsigned long long p = atomicAdd(&counters[C_OVF_LEN], 1ull);
+                    if (p < ovf_cap) ovf[p] = c;
+                    else atomicOr(&counters[C_FLAGS], ERR_HIST_OVERFLOW_FULL);
+                }
+                keep = (c >= min_count && c <= max_count);
+                skey = pair_reverse(sl.key);
+            }
+        }
+        append_records(keep, skey, c, rec_keys, rec_counts, rec_cap, counters, s_warp, &s_base);
+    }
+    unsigned d = __reduce_add_sync(FULL, distinct);
+    if ((threadIdx.x & 31) == 0 && d) atomicAdd(&counters[C_DISTINCT], (unsigned long long)d);
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2048; i += blockDim.x)
+        if (s_hist[i]) atomicAdd(&hist[i], (unsigned long long)s_hist[i]);
+}
+
+// Batched jobs keep all samples' tables in one slot arena.  Sample s owns
+// slots [slot_base, slot_base + slot_cap).
+__device__ __forceinline__ uint32_t sample_of_slot(const unsigned long long *s_base, uint32_t n, uint64_t i)
+{
+    uint32_t lo = 0, hi = n;   // last sample with base <= i
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (s_base[mid] <= i) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(256) k_compact_batch(const Slot *slots, uint64_t total, const SampleCfg *cfg,
+                                                       uint32_t n_samples, unsigned long long *rec_len,
+                                                       unsigned long long *rec_keys, uint32_t *rec_counts,
+                                                       unsigned long long *hist, unsigned long long *ovf,
+                                                       uint64_t ovf_cap, unsigned long long *distinct,
+                                                       unsigned long long *counters, int count_only)
+{
+    extern __shared__ unsigned long long s_base[];
+    for (uint32_t i = threadIdx.x; i < n_samples; i += blockDim.x) s_base[i] = cfg[i].slot_base;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t rounds = (total + stride - 1) / stride;
+    for (uint64_t r = 0; r < rounds; ++r) {
+        const uint64_t i = r * stride + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        bool present = false, keep = false;
+        uint32_t smp = 0, c = 0;
+        unsigned long long key = EMPTY_KEY;
+        if (i < total) {
+            key = __ldcg(&slots[i].key);
+            if (key != EMPTY_KEY) {
+                present = true;
+                smp = sample_of_slot(s_base, n_samples, i);
+                const SampleCfg sc = cfg[smp];
+                c = slots[i].count < sc.count_max ? slots[i].count : sc.count_max;
+                keep = c >= sc.min_count && c <= sc.max_count;
+            }
+        }
+        // per-sample warp aggregation of the distinct count
+        uint32_t tag = present ? smp : 0xffffffffu;
+        uint32_t peers = __match_any_sync(FULL, tag);
+        int leader = __ffs(peers) - 1;
+        if (present && lane == leader) atomicAdd(&distinct[smp], (unsigned long long)__popc(peers));
+        if (count_only) continue;
+        if (present) {
+            if (c < HIST_BINS_BATCH) atomicAdd(&hist[(uint64_t)smp * HIST_BINS_BATCH + c], 1ull);
+            else {
+                unsigned long long p = atomicAdd(&counters[C_OVF_LEN], 1ull);
+                if (p < ovf_cap) ovf[p] = ((unsigned long long)smp << 32) | c;
+                else atomicOr(&counters[C_FLAGS], ERR_HIST_OVERFLOW_FULL);
+            }
+        }
+        tag = keep ? smp : 0xffffffffu;
+        peers = __match_any_sync(FULL, tag);
+        leader = __ffs(peers) - 1;
+        unsigned long long b = 0;
+        if (keep && lane == leader) b = atomicAdd(&rec_len[smp], (unsigned long long)__popc(peers));
+        b = __shfl_sync(FULL, b, leader);
+        if (keep) {
+            const SampleCfg sc = cfg[smp];
+            unsigned long long pos = b + __popc(peers & lanemask_lt());
+            if (pos < sc.rec_cap) {
+                rec_keys[sc.rec_base + pos] = pair_reverse(key);
+                rec_counts[sc.rec_base + pos] = c;
+            } else {
+                atomicOr(&counters[C_FLAGS], ERR_RECORDS_FULL);
+            }
+        }
+    }
+}
+
+__global__ void k_pair_reverse(unsigned long long *keys, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        keys[i] = pair_reverse(keys[i]);
+}
+
+// ---------------------------------------------------------------------------
+// scan
+// ---------------------------------------------------------------------------
+
+constexpr uint32_t SCAN_ITEMS = 8;
+constexpr uint32_t SCAN_BLOCK = 256 * SCAN_ITEMS;
+
+__global__ void __launch_bounds__(256) k_scan_reduce(const uint32_t *in, uint64_t n, unsigned long long *sums)
+{
+    __shared__ unsigned long long s[8];
+    const uint64_t base = (uint64_t)blockIdx.x * SCAN_BLOCK;
+    unsigned long long acc = 0;
+    for (uint32_t j = 0; j < SCAN_ITEMS; ++j) {
+        uint64_t i = base + j * 256 + threadIdx.x;
+        if (i < n) acc += in[i];
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL, acc, o);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int i = 0; i < 8; ++i) t += s[i];
+        sums[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_scan_top(unsigned long long *sums, uint64_t nb)
+{
+    __shared__ unsigned long long s[32];
+    __shared__ unsigned long long carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint64_t b0 = 0; b0 < nb; b0 += 1024) {
+        uint64_t i = b0 + threadIdx.x;
+        unsigned long long v = i < nb ? sums[i] : 0, x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned long long y = __shfl_up_sync(FULL, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            unsigned long long w = s[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                unsigned long long y = __shfl_up_sync(FULL, w, o);
+                if (lane >= o) w += y;
+            }
+            s[lane] = w;
+        }
+        __syncthreads();
+        unsigned long long excl = carry + (warp ? s[warp - 1] : 0) + x - v;
+        if (i < nb) sums[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += s[31];
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_scan_down(const uint32_t *in, uint64_t n, const unsigned long long *sums,
+                                                   unsigned long long *out)
+{
+    __shared__ unsigned long long s[8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t base = (uint64_t)blockIdx.x * SCAN_BLOCK;
+    // each thread owns SCAN_ITEMS consecutive items
+    uint32_t v[SCAN_ITEMS];
+    unsigned long long local = 0;
+    for (uint32_t j = 0; j < SCAN_ITEMS; ++j) {
+        uint64_t i = base + threadIdx.x * SCAN_ITEMS + j;
+        v[j] = i < n ? in[i] : 0;
+        local += v[j];
+    }
+    unsigned long long x = local;
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned long long y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s[warp] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long c = 0;
+        for (int i = 0; i < 8; ++i) { unsigned long long t = s[i]; s[i] = c; c += t; }
+    }
+    __syncthreads();
+    unsigned long long run = sums[blockIdx.x] + s[warp] + x - local;
+    for (uint32_t j = 0; j < SCAN_ITEMS; ++j) {
+        uint64_t i = base + threadIdx.x * SCAN_ITEMS + j;
+        if (i < n) out[i] = run;
+        run += v[j];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// radix sort (LSD, 8-bit digits)
+// ---------------------------------------------------------------------------
+
+constexpr uint32_t RS_THREADS = 256;
+constexpr uint32_t RS_ITEMS = 16;
+constexpr uint32_t RS_TILE = RS_THREADS * RS_ITEMS;   // 4096
+constexpr uint32_t RS_WARP_ITEMS = 32 * RS_ITEMS;     // 512 contiguous items per warp
+
+__global__ void __launch_bounds__(RS_THREADS) k_radix_count(const unsigned long long *keys, const SortTile *tiles,
+                                                            uint32_t shift, uint32_t *counts)
+{
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const SortTile tl = tiles[blockIdx.x];
+    for (uint32_t j = 0; j < RS_ITEMS; ++j) {
+        uint64_t i = tl.begin + j * RS_THREADS + threadIdx.x;
+        if (i < tl.end) atomicAdd(&h[(keys[i] >> shift) & 255], 1u);
+    }
+    __syncthreads();
+    counts[tl.cbase + (uint64_t)threadIdx.x * tl.stride] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const unsigned long long *kin, const uint32_t *vin,
+                                                              unsigned long long *kout, uint32_t *vout,
+                                                              const SortTile *tiles, uint32_t shift,
+                                                              const unsigned long long *offsets)
+{
+    extern __shared__ __align__(16) uint8_t rs_smem[];
+    unsigned long long *s_keys = reinterpret_cast<unsigned long long *>(rs_smem);       // RS_TILE
+    uint32_t *s_vals = reinterpret_cast<uint32_t *>(s_keys + RS_TILE);                   // RS_TILE
+    uint32_t *s_wcnt = s_vals + RS_TILE;                                                 // 8 x 256
+    uint32_t *s_start = s_wcnt + 8 * 256;                                                // 256
+    __shared__ uint32_t s_warp[8];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < 8 * 256; i += RS_THREADS) s_wcnt[i] = 0;
+    __syncthreads();
+
+    const SortTile tl = tiles[blockIdx.x];
+    const uint64_t tile_base = tl.begin;
+    const uint64_t tile_n = tl.end - tl.begin;
+    unsigned long long k[RS_ITEMS];
+    uint32_t v[RS_ITEMS];
+    uint16_t rank[RS_ITEMS];
+    uint16_t dig[RS_ITEMS];
+    uint32_t *wc = s_wcnt + warp * 256;
+#pragma unroll
+    for (uint32_t r = 0; r < RS_ITEMS; ++r) {
+        uint64_t li = warp * RS_WARP_ITEMS + r * 32 + lane;
+        bool act = li < tile_n;
+        k[r] = act ? kin[tile_base + li] : 0;
+        v[r] = act ? vin[tile_base + li] : 0;
+        uint32_t d = act ? (uint32_t)((k[r] >> shift) & 255) : 256u;
+        uint32_t peers = __match_any_sync(FULL, d);
+        uint32_t before = __popc(peers & lanemask_lt());
+        uint32_t cnt = act ? wc[d] : 0;
+        __syncwarp();
+        if (act && before == 0) wc[d] = cnt + __popc(peers);
+        __syncwarp();
+        rank[r] = (uint16_t)(cnt + before);
+        dig[r] = (uint16_t)d;
+    }
+    __syncthreads();
+    // per digit: exclusive prefix over warps, total for the tile
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+        uint32_t c = s_wcnt[w * 256 + tid];
+        s_wcnt[w * 256 + tid] = run;
+        run += c;
+    }
+    uint32_t tot;
+    uint32_t start = block_excl_scan(run, s_warp, tot);
+    s_start[tid] = start;
+    __syncthreads();
+#pragma unroll
+    for (uint32_t r = 0; r < RS_ITEMS; ++r) {
+        if (dig[r] < 256) {
+            uint32_t pos = s_start[dig[r]] + s_wcnt[warp * 256 + dig[r]] + rank[r];
+            s_keys[pos] = k[r];
+            s_vals[pos] = v[r];
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = tid; i < tile_n; i += RS_THREADS) {
+        unsigned long long key = s_keys[i];
+        uint32_t d = (uint32_t)((key >> shift) & 255);
+        unsigned long long dst = offsets[tl.cbase + (uint64_t)d * tl.stride] + tl.adjust + (i - s_start[d]);
+        kout[dst] = key;
+        vout[dst] = s_vals[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// selection
+// ---------------------------------------------------------------------------
+
+__global__ void k_range_flags(const uint32_t *counts, uint64_t n, uint32_t lo, uint32_t hi, uint32_t *flags)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        flags[i] = (counts[i] >= lo && counts[i] <= hi) ? 1u : 0u;
+}
+
+__global__ void k_scatter_selected(const unsigned long long *keys, const uint32_t *counts, const uint32_t *flags,
+                                   const unsigned long long *pos, uint64_t n, uint64_t limit,
+                                   unsigned long long *out_keys, uint32_t *out_counts, unsigned long long *counters,
+                                   int counter_idx)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (flags[i] && pos[i] < limit) {
+            out_keys[pos[i]] = keys[i];
+            out_counts[pos[i]] = counts[i];
+        }
+        if (i == n - 1) counters[counter_idx] = pos[i] + flags[i];
+    }
+}
+
+__global__ void k_hash_batch(const unsigned long long *keys, uint64_t n, unsigned long long *out)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t w = keys[i], lo, hi;
+        xxh3_128_8(w, lo, hi);
+        out[5 * i + 0] = lo;
+        out[5 * i + 1] = hi;
+        out[5 * i + 2] = xxh3_64_8(w);
+        out[5 * i + 3] = rapidhash_8(w);
+        out[5 * i + 4] = komihash_8(w);
+    }
+}
+
+std::atomic<unsigned long long> g_launches{0};
+thread_local unsigned long long t_launches = 0;
+
+inline void note_launch()
+{
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    ++t_launches;
+}
+
+int sm_count()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+int grid_for(uint64_t n, int threads, int per_sm = 8)
+{
+    uint64_t g = (n + threads - 1) / threads;
+    uint64_t cap = (uint64_t)sm_count() * per_sm;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+
+unsigned long long kernel_launches() { return g_launches.load(std::memory_order_relaxed); }
+unsigned long long thread_kernel_launches() { return t_launches; }
+
+size_t extract_smem_bytes_for(int mode, uint32_t stage_cap)
+{
+    size_t b = 2 * BUF_BYTES + 264 * 8 + 264 * 4;
+    if (mode != MODE_SCAN) b += (size_t)stage_cap * 8;
+    return b;
+}
+
+size_t extract_smem_bytes() { return extract_smem_bytes_for(MODE_INSERT, STAGE_CAP); }
+
+cudaError_t launch_newlines(const uint8_t *buf, uint64_t n_tiles, uint32_t *tile_nl, int32_t *tile_lastnl,
+                            cudaStream_t st)
+{
+    if (!n_tiles) return cudaSuccess;
+    note_launch();
+    k_newlines<<<grid_for(n_tiles, 1, 16), 256, 0, st>>>(buf, n_tiles, tile_nl, tile_lastnl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_chunk_lastnl(const int32_t *tile_lastnl, const uint32_t *tile_seg, const Seg *segs,
+                                const uint64_t *seg_chunk0, uint64_t n_tiles, int32_t *chunk_lastnl, cudaStream_t st)
+{
+    if (!n_tiles) return cudaSuccess;
+    note_launch();
+    k_chunk_lastnl<<<grid_for(n_tiles, 256), 256, 0, st>>>(tile_lastnl, tile_seg, segs, seg_chunk0, n_tiles,
+                                                           chunk_lastnl);
+    return cudaGetLastError();
+}
+
+template <int M>
+static cudaError_t launch_extract_t(const ExtractArgs &a, int grid, uint32_t stage_cap, cudaStream_t st)
+{
+    size_t smem = extract_smem_bytes_for(M, stage_cap);
+    cudaError_t e = cudaFuncSetAttribute(k_extract<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (grid <= 0) {
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_extract<M>, EXT_THREADS, smem);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) per_sm = 1;
+        grid = sm_count() * per_sm;
+    }
+    if ((uint64_t)grid > a.n_tiles) grid = (int)a.n_tiles;
+    note_launch();
+    k_extract<M><<<grid, EXT_THREADS, smem, st>>>(a, stage_cap);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_extract(int mode, const ExtractArgs &a, int grid, cudaStream_t st)
+{
+    if (!a.n_tiles) return cudaSuccess;
+    switch (mode) {
+    case MODE_SCAN: return launch_extract_t<MODE_SCAN>(a, grid, STAGE_CAP, st);
+    case MODE_INSERT: return launch_extract_t<MODE_INSERT>(a, grid, STAGE_CAP, st);
+    case MODE_BLOOM: return launch_extract_t<MODE_BLOOM>(a, grid, STAGE_CAP, st);
+    case MODE_EMIT: return launch_extract_t<MODE_EMIT>(a, grid, STAGE_CAP, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+size_t scan_tmp_words(uint64_t n) { return (n + SCAN_BLOCK - 1) / SCAN_BLOCK + 1; }
+
+cudaError_t launch_scan_u32(const uint32_t *in, unsigned long long *out, uint64_t n, unsigned long long *tmp,
+                            cudaStream_t st)
+{
+    if (!n) return cudaSuccess;
+    uint64_t nb = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
+    note_launch();
+    k_scan_reduce<<<(unsigned)nb, 256, 0, st>>>(in, n, tmp);
+    note_launch();
+    k_scan_top<<<1, 1024, 0, st>>>(tmp, nb);
+    note_launch();
+    k_scan_down<<<(unsigned)nb, 256, 0, st>>>(in, n, tmp, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_u64(unsigned long long *p, uint64_t n, unsigned long long v, cudaStream_t st)
+{
+    if (!n) return cudaSuccess;
+    note_launch();
+    k_fill_u64<<<grid_for(n, 256), 256, 0, st>>>(p, n, v);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_init_slots(Slot *slots, uint64_t n, cudaStream_t st)
+{
+    if (!n) return cudaSuccess;
+    note_launch();
+    k_init_slots<<<grid_for(n, 256), 256, 0, st>>>(slots, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_count_keys(const Slot *slots, uint64_t n, unsigned long long *out, cudaStream_t st)
+{
+    if (!n) return cudaSuccess;
+    note_launch();
+    k_count_keys<<<grid_for(n, 256), 256, 0, st>>>(slots, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_insert_list(const unsigned long long *keys, uint64_t n, TableRef t, uint32_t max_probe,
+                               unsigned long long *counters, cudaStream_t st)
+{
+    if (!n) return cudaSuccess;
+    note_launch();
+    k_insert_list<<<grid_for(n, 256), 256, 0, st>>>(keys, n, t, max_probe, counters);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_insert_pairs(const unsigned long long *keys, const uint32_t *counts, uint64_t n, TableRef t,
+                                uint32_t max_probe, unsigned long long *counters, cudaStream_t st)
+{
+    if (!n) return cudaSuccess;
+    note_launch();
+    k_insert_pairs<<<grid_for(n, 256), 256, 0, st>>>(keys, counts, n, t, max_probe, counters);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_merge_low(const unsigned long long *keys, uint64_t n, TableRef t, uint32_t max_probe,
+                             uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys, uint32_t *rec_counts,
+                             uint64_t rec_cap, unsigned long long *counters, cudaStream_t st)
+{
+    if (!n) return cudaSuccess;
+    note_launch();
+    k_merge_low<<<grid_for(n, 256), 256, 0, st>>>(keys, n, t, max_probe, min_count, max_count, rec_keys, rec_counts,
+                                                  rec_cap, counters);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compact(TableRef t, uint64_t cap, uint32_t count_max, uint32_t min_count, uint32_t max_count,
+                           unsigned long long *rec_keys, uint32_t *rec_counts, uint64_t rec_cap,
+                           unsigned long long *hist, uint32_t *ovf, uint64_t ovf_cap, unsigned long long *counters,
+                           cudaStream_t st)
+{
+    if (!cap) return cudaSuccess;
+    note_launch();
+    k_compact<<<grid_for(cap, 256, 4), 256, 0, st>>>(t, cap, count_max, min_count, max_count, rec_keys, rec_counts,
+                                                     rec_cap, hist, ovf, ovf_cap, counters);
+    return cudaGetLastError();
+}
+
+static uint64_t sort_tiles_for(const uint64_t *seg_len, uint32_t n_segs)
+{
+    uint64_t t = 0;
+    for (uint32_t i = 0; i < n_segs; ++i) t += (seg_len[i] + RS_TILE - 1) / RS_TILE;
+    return t;
+}
+
+static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+size_t sort_tmp_bytes_segmented(uint64_t n_total, const uint64_t *seg_len, uint32_t n_segs)
+{
+    const uint64_t n_tiles = sort_tiles_for(seg_len, n_segs);
+    const uint64_t nc = 256 * std::max<uint64_t>(n_tiles, 1);
+    return align256(n_total * 8) + align256(n_total * 4) + align256(nc * 4) + align256(nc * 8) +
+           align256(scan_tmp_words(nc) * 8) + align256(std::max<uint64_t>(n_tiles, 1) * sizeof(SortTile));
+}
+
+size_t sort_tmp_bytes(uint64_t n) { return sort_tmp_bytes_segmented(n, &n, 1); }
+
+// Segments [seg_start[i], seg_start[i] + seg_len[i]) of the arrays are sorted
+// independently; they must be disjoint and in increasing address order.
+cudaError_t launch_radix_sort_segmented(unsigned long long *keys, uint32_t *vals, uint64_t n_total,
+                                        const uint64_t *seg_start, const uint64_t *seg_len, uint32_t n_segs,
+                                        uint32_t bits, void *tmp, cudaStream_t st)
+{
+    const uint64_t n_tiles = sort_tiles_for(seg_len, n_segs);
+    if (n_tiles == 0 || bits == 0) return cudaSuccess;
+    const uint64_t nc = 256 * n_tiles;
+    std::vector<SortTile> tiles;
+    tiles.reserve(n_tiles);
+    uint64_t tb = 0, actual = 0;
+    for (uint32_t sgi = 0; sgi < n_segs; ++sgi) {
+        const uint64_t nt = (seg_len[sgi] + RS_TILE - 1) / RS_TILE;
+        for (uint64_t j = 0; j < nt; ++j) {
+            SortTile t;
+            t.begin = seg_start[sgi] + j * RS_TILE;
+            t.end = std::min(seg_start[sgi] + seg_len[sgi], t.begin + RS_TILE);
+            t.cbase = 256 * tb + j;
+            t.stride = nt;
+            t.adjust = seg_start[sgi] - actual;
+            tiles.push_back(t);
+        }
+        tb += nt;
+        actual += seg_len[sgi];
+    }
+    uint8_t *p = static_cast<uint8_t *>(tmp);
+    unsigned long long *k2 = reinterpret_cast<unsigned long long *>(p);
+    p += align256(n_total * 8);
+    uint32_t *v2 = reinterpret_cast<uint32_t *>(p);
+    p += align256(n_total * 4);
+    uint32_t *counts = reinterpret_cast<uint32_t *>(p);
+    p += align256(nc * 4);
+    unsigned long long *offs = reinterpret_cast<unsigned long long *>(p);
+    p += align256(nc * 8);
+    unsigned long long *stmp = reinterpret_cast<unsigned long long *>(p);
+    p += align256(scan_tmp_words(nc) * 8);
+    SortTile *d_tiles = reinterpret_cast<SortTile *>(p);
+    cudaError_t e = cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(SortTile), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+
+    const size_t smem = RS_TILE * 8 + RS_TILE * 4 + 8 * 256 * 4 + 256 * 4;
+    e = cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    unsigned long long *ks = keys, *kd = k2;
+    uint32_t *vs = vals, *vd = v2;
+    const uint32_t passes = (bits + 7) / 8;
+    for (uint32_t pass = 0; pass < passes; ++pass) {
+        const uint32_t shift = pass * 8;
+        note_launch();
+        k_radix_count<<<(unsigned)n_tiles, RS_THREADS, 0, st>>>(ks, d_tiles, shift, counts);
+        e = launch_scan_u32(counts, offs, nc, stmp, st);
+        if (e != cudaSuccess) return e;
+        note_launch();
+        k_radix_scatter<<<(unsigned)n_tiles, RS_THREADS, smem, st>>>(ks, vs, kd, vd, d_tiles, shift, offs);
+        std::swap(ks, kd);
+        std::swap(vs, vd);
+    }
+    if (ks != keys) {
+        for (uint32_t sgi = 0; sgi < n_segs; ++sgi) {
+            if (!seg_len[sgi]) continue;
+            cudaMemcpyAsync(keys + seg_start[sgi], ks + seg_start[sgi], seg_len[sgi] * 8, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(vals + seg_start[sgi], vs + seg_start[sgi], seg_len[sgi] * 4, cudaMemcpyDeviceToDevice, st);
+        }
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_radix_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
+                              cudaStream_t st)
+{
+    if (n <= 1 || bits == 0) return cudaSuccess;
+    const uint64_t start = 0;
+    return launch_radix_sort_segmented(keys, vals, n, &start, &n, 1, bits, tmp, st);
+}
+
+cudaError_t launch_compact_batch(const Slot *slots, uint64_t total, const SampleCfg *cfg, uint32_t n_samples,
+                                 unsigned long long *rec_len, unsigned long long *rec_keys, uint32_t *rec_counts,
+                                 unsigned long long *hist, unsigned long long *ovf, uint64_t ovf_cap,
+                                 unsigned long long *distinct, unsigned long long *counters, int count_only,
+                                 cudaStream_t st)
+{
+    if (!total || !n_samples) return cudaSuccess;
+    size_t smem = (size_t)n_samples * 8;
+    cudaError_t e = cudaFuncSetAttribute(k_compact_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    note_launch();
+    k_compact_batch<<<grid_for(total, 256, 4), 256, smem, st>>>(slots, total, cfg, n_samples, rec_len, rec_keys,
+                                                                rec_counts, hist, ovf, ovf_cap, distinct, counters,
+                                                                count_only);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pair_reverse(unsigned long long *keys, uint64_t n, cudaStream_t st)
+{
+    if (!n) return cudaSuccess;
+    note_launch();
+    k_pair_reverse<<<grid_for(n, 256), 256, 0, st>>>(keys, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_select_range(const unsigned long long *keys, const uint32_t *counts, uint64_t n, uint32_t lo,
+                                uint32_t hi, uint64_t limit, unsigned long long *out_keys, uint32_t *out_counts,
+                                uint32_t *flags, unsigned long long *pos, unsigned long long *tmp,
+                                unsigned long long *counters, int counter_idx, cudaStream_t st)
+{
+    if (!n) return cudaMemsetAsync(&counters[counter_idx], 0, 8, st);
+    note_launch();
+    k_range_flags<<<grid_for(n, 256), 256, 0, st>>>(counts, n, lo, hi, flags);
+    cudaError_t e = launch_scan_u32(flags, pos, n, tmp, st);
+    if (e != cudaSuccess) return e;
+    note_launch();
+    k_scatter_selected<<<grid_for(n, 256), 256, 0, st>>>(keys, counts, flags, pos, n, limit, out_keys, out_counts,
+                                                         counters, counter_idx);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hash_batch(const unsigned long long *keys, uint64_t n, unsigned long long *out, cudaStream_t st)
+{
+    if (!n) return cudaSuccess;
+    note_launch();
+    k_hash_batch<<<grid_for(n, 256), 256, 0, st>>>(keys, n, out);
+    return cudaGetLastError();
+}
+
+}  // namespace kc

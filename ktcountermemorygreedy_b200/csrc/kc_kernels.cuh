@@ -1,0 +1,170 @@
+// kc_kernels.cuh -- host-visible declarations of the device pipeline stages.
+// All launches are stream-ordered; none allocates memory.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace kc {
+
+constexpr uint32_t TILE = 8192;         // FASTQ bytes per extraction tile
+constexpr uint32_t HALO = 32;           // bytes before a tile read with it (k <= 32)
+constexpr uint32_t FRONT_PAD = 256;     // zero bytes before tile 0 in the device buffer
+constexpr uint32_t EXT_THREADS = 256;   // one 32-byte segment per thread
+constexpr uint32_t STAGE_CAP = 4096;    // staged k-mers per extraction round
+constexpr uint32_t HLL_BITS = 12;       // HyperLogLog registers per sample = 2^12
+constexpr uint32_t HLL_M = 1u << HLL_BITS;
+constexpr uint32_t HIST_BINS = 1u << 16;  // dense count histogram; larger counts go to a list
+constexpr uint32_t HIST_BINS_BATCH = 4096;  // per-sample dense histogram of batched jobs
+constexpr uint32_t MAX_BATCH = 4096;        // samples in one batched job
+constexpr uint64_t PREPASS_CHUNK = 2ULL * 1024 * 1024;  // reference reader chunk
+
+// error flags (bit mask in counters[C_FLAGS])
+constexpr unsigned long long ERR_TABLE_FULL = 1ull << 0;
+constexpr unsigned long long ERR_LIST_FULL = 1ull << 1;
+constexpr unsigned long long ERR_WAIT_TIMEOUT = 1ull << 2;
+constexpr unsigned long long ERR_RECORDS_FULL = 1ull << 3;
+constexpr unsigned long long ERR_HIST_OVERFLOW_FULL = 1ull << 4;
+
+// indexes into the per-job device counter block (unsigned long long each)
+enum Counter : int {
+    C_FLAGS = 0,
+    C_LOW_LEN = 1,       // Bloom FIRST occurrences (low list, front of the list buffer)
+    C_HIGH_LEN = 2,      // other occurrences (back of the list buffer)
+    C_EMIT_LEN = 3,      // plain occurrence list (testing entry point)
+    C_REC_LEN = 4,       // output records
+    C_LOW_ONLY = 5,      // low k-mers absent from the table (final count 1)
+    C_DISTINCT = 6,      // distinct k-mers seen by compaction
+    C_OVF_LEN = 7,       // histogram counts >= HIST_BINS
+    C_SEL_A = 8,         // query selections
+    C_SEL_B = 9,
+    C_COUNT = 16
+};
+
+// One FASTQ file inside a job's device buffer.  Files start on tile
+// boundaries; bytes between a file's end and the next tile boundary are zero.
+struct Seg {
+    uint64_t first_tile;
+    uint64_t n_tiles;
+    uint64_t len;          // file bytes
+    uint64_t sample_end;   // the pre-pass reads bytes [0, sample_end)
+    uint32_t k;
+    uint32_t sample;       // owning sample (batched jobs); 0 for a single job
+};
+
+struct Slot {              // open-addressing table slot (16 bytes)
+    unsigned long long key;
+    unsigned int count;
+    unsigned int pad;
+};
+
+struct TableRef {
+    Slot *slots;
+    unsigned long long mask;   // capacity - 1 (capacity is a power of two)
+};
+
+struct SampleCfg {          // one sample of a batched job
+    unsigned long long slot_base, slot_cap;   // its table inside the slot arena
+    unsigned long long rec_base, rec_cap;     // its record region
+    uint32_t count_max, min_count, max_count, k;
+};
+
+struct SortTile {           // one radix-sort tile of a (possibly segmented) sort
+    uint64_t begin, end;    // record range
+    uint64_t cbase;         // digit-count index of digit 0; digit d at cbase + d * stride
+    uint64_t stride;
+    uint64_t adjust;        // segment start minus records of earlier segments
+};
+
+struct ExtractArgs {
+    const uint8_t *buf;             // first byte of tile 0 (FRONT_PAD zero bytes before it)
+    uint64_t n_tiles;
+    const uint64_t *tile_prefix;    // exclusive newline count before each tile
+    const uint32_t *tile_seg;       // file of each tile
+    const Seg *segs;
+    unsigned long long *counters;   // C_COUNT words
+    // scan mode
+    unsigned long long *occ;        // occurrences per sample
+    uint32_t *hll;                  // HLL_M registers per sample
+    int prepass;                    // also accumulate the pre-pass statistics
+    const int32_t *chunk_lastnl;    // per 2 MiB chunk (global chunk index), last '\n' offset in chunk
+    const uint64_t *seg_chunk0;     // first global chunk index of each file
+    uint32_t *prefix_hist;          // 256 per sample
+    unsigned long long *qual;       // 2 per sample: byte sum, byte count
+    // insert mode
+    const TableRef *tables;         // per sample
+    uint32_t max_probe;
+    // bloom mode (single sample)
+    const unsigned long long *bloom_off;   // 256 word offsets
+    const unsigned long long *bloom_cap;   // 256 capacities (blocks of two words)
+    unsigned long long *bloom_bits;
+    uint32_t *hll_high;             // HLL registers of the non-FIRST occurrences
+    // emit / bloom output list
+    unsigned long long *list;
+    unsigned long long list_cap;
+};
+
+enum ExtractMode : int { MODE_SCAN = 0, MODE_INSERT = 1, MODE_BLOOM = 2, MODE_EMIT = 3 };
+
+size_t extract_smem_bytes();
+unsigned long long kernel_launches();          // launches issued by this process
+unsigned long long thread_kernel_launches();   // launches issued by the calling thread
+cudaError_t launch_newlines(const uint8_t *buf, uint64_t n_tiles, uint32_t *tile_nl, int32_t *tile_lastnl,
+                            cudaStream_t st);
+cudaError_t launch_chunk_lastnl(const int32_t *tile_lastnl, const uint32_t *tile_seg, const Seg *segs,
+                                const uint64_t *seg_chunk0, uint64_t n_tiles, int32_t *chunk_lastnl,
+                                cudaStream_t st);
+cudaError_t launch_extract(int mode, const ExtractArgs &a, int grid, cudaStream_t st);
+
+// Exclusive prefix sum of n 32-bit values into 64-bit outputs.  tmp must
+// hold scan_tmp_words(n) 64-bit words.
+size_t scan_tmp_words(uint64_t n);
+cudaError_t launch_scan_u32(const uint32_t *in, unsigned long long *out, uint64_t n, unsigned long long *tmp,
+                            cudaStream_t st);
+
+cudaError_t launch_init_slots(Slot *slots, uint64_t n, cudaStream_t st);
+cudaError_t launch_count_keys(const Slot *slots, uint64_t n, unsigned long long *out, cudaStream_t st);
+cudaError_t launch_fill_u64(unsigned long long *p, uint64_t n, unsigned long long v, cudaStream_t st);
+cudaError_t launch_insert_list(const unsigned long long *keys, uint64_t n, TableRef t, uint32_t max_probe,
+                               unsigned long long *counters, cudaStream_t st);
+cudaError_t launch_insert_pairs(const unsigned long long *keys, const uint32_t *counts, uint64_t n, TableRef t,
+                                uint32_t max_probe, unsigned long long *counters, cudaStream_t st);
+cudaError_t launch_merge_low(const unsigned long long *keys, uint64_t n, TableRef t, uint32_t max_probe,
+                             uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
+                             uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *counters,
+                             cudaStream_t st);
+cudaError_t launch_compact(TableRef t, uint64_t cap, uint32_t count_max, uint32_t min_count, uint32_t max_count,
+                           unsigned long long *rec_keys, uint32_t *rec_counts, uint64_t rec_cap,
+                           unsigned long long *hist, uint32_t *ovf, uint64_t ovf_cap,
+                           unsigned long long *counters, cudaStream_t st);
+
+// LSD radix sort of (key, value) pairs on the low `bits` bits of the keys,
+// 8 bits per pass.  Result ends in keys/vals.
+size_t sort_tmp_bytes(uint64_t n);
+size_t sort_tmp_bytes_segmented(uint64_t n_total, const uint64_t *seg_len, uint32_t n_segs);
+cudaError_t launch_radix_sort_segmented(unsigned long long *keys, uint32_t *vals, uint64_t n_total,
+                                        const uint64_t *seg_start, const uint64_t *seg_len, uint32_t n_segs,
+                                        uint32_t bits, void *tmp, cudaStream_t st);
+cudaError_t launch_radix_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
+                              cudaStream_t st);
+
+cudaError_t launch_compact_batch(const Slot *slots, uint64_t total, const SampleCfg *cfg, uint32_t n_samples,
+                                 unsigned long long *rec_len, unsigned long long *rec_keys, uint32_t *rec_counts,
+                                 unsigned long long *hist, unsigned long long *ovf, uint64_t ovf_cap,
+                                 unsigned long long *distinct, unsigned long long *counters, int count_only,
+                                 cudaStream_t st);
+cudaError_t launch_pair_reverse(unsigned long long *keys, uint64_t n, cudaStream_t st);
+
+// Stable selection of records whose count satisfies lo <= c <= hi: writes the
+// selected keys/counts in input order.  Uses the scan temp space.
+cudaError_t launch_select_range(const unsigned long long *keys, const uint32_t *counts, uint64_t n, uint32_t lo,
+                                uint32_t hi, uint64_t limit, unsigned long long *out_keys, uint32_t *out_counts,
+                                uint32_t *flags, unsigned long long *pos, unsigned long long *tmp,
+                                unsigned long long *counters, int counter_idx, cudaStream_t st);
+
+// Batch of hash evaluations for the parity tests: out[5*i..5*i+4] =
+// xxh3_128.lo, xxh3_128.hi, xxh3_64, rapidhash, komihash (all of keys[i]).
+cudaError_t launch_hash_batch(const unsigned long long *keys, uint64_t n, unsigned long long *out,
+                              cudaStream_t st);
+
+}  // namespace kc

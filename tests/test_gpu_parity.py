@@ -1,0 +1,263 @@
+"""Parity of the CUDA path (libkc.so, called through the C ABI) with the oracle
+and with the golden outputs of the reference's own programs.  Integer work:
+every comparison is exact."""
+import hashlib
+import json
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+import fixtures
+import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = json.load(open(os.path.join(ROOT, "tests", "golden", "golden.json")))
+U32 = 0xFFFFFFFF
+
+
+@pytest.fixture(scope="module")
+def kc():
+    import ktcountermemorygreedy_b200 as kc
+    return kc
+
+
+@pytest.fixture(scope="module")
+def counter(kc):
+    c = kc.KmerCounter(max_inflight_jobs=4)
+    yield c
+    c.close()
+
+
+def _case_files(name):
+    for n, files, _ in fixtures.E2E_CASES:
+        if n == name:
+            return files
+    raise KeyError(name)
+
+
+def test_hashes_bit_exact(kc):
+    keys = np.array([int(r[0], 16) for r in GOLDEN["hashes"]], np.uint64)
+    h = kc.hash_kmers(keys)
+    for row, got in zip(GOLDEN["hashes"], h):
+        assert [int(x) for x in got] == [int(row[1], 16), int(row[2], 16), int(row[3], 16), int(row[4], 16),
+                                         int(row[5], 16)]
+
+
+def test_extract_matches_getkmer_golden(kc):
+    for case in GOLDEN["getkmer"]:
+        bases = case["bases"]
+        fq = f"@x\n{bases}\n+\n{'I' * len(bases)}\n".encode()
+        got = np.sort(kc.extract_kmers(fq, case["k"]))
+        want = np.sort(np.array([int(x, 16) for x in case["canonical"]], np.uint64))
+        assert got.tolist() == want.tolist(), case["k"]
+
+
+@pytest.mark.parametrize("name", [c[0] for c in fixtures.E2E_CASES])
+@pytest.mark.parametrize("k", [1, 5, 11, 16, 21, 25, 31, 32])
+def test_extract_matches_oracle(kc, name, k):
+    for f in _case_files(name):
+        got = np.sort(kc.extract_kmers(f, k))
+        want = np.sort(O.extract(f, k))
+        assert len(got) == len(want)
+        assert np.array_equal(got, want)
+
+
+def test_extract_empty_and_tiny(kc):
+    assert len(kc.extract_kmers(b"", 21)) == 0
+    assert len(kc.extract_kmers(b"@a\n", 21)) == 0
+    assert kc.extract_kmers(b"@a\nACGTA", 5).tolist() == O.extract(b"@a\nACGTA", 5).tolist()
+    # exactly one tile, and one byte more
+    for n in (8192 - 7, 8192, 8193, 3 * 8192 + 5):
+        seq = ("ACGT" * (n // 4 + 1))[: max(0, n - 12)]
+        fq = f"@a\n{seq}\n+\n".encode()[:n]
+        assert np.array_equal(np.sort(kc.extract_kmers(fq, 31)), np.sort(O.extract(fq, 31)))
+
+
+@pytest.mark.parametrize("bits", [1, 8, 13, 42, 62, 64])
+def test_radix_sort_is_stable_and_ordered(kc, bits):
+    rng = np.random.default_rng(bits)
+    n = 300_001
+    keys = rng.integers(0, 2**63, size=n, dtype=np.uint64) * np.uint64(2) + rng.integers(0, 2, size=n, dtype=np.uint64)
+    if bits < 64:
+        keys &= np.uint64((1 << bits) - 1)
+    vals = np.arange(n, dtype=np.uint32)
+    sk, sv = kc.sort_records(keys, vals, bits)
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(sk, keys[order])
+    assert np.array_equal(sv, vals[order])
+
+
+@pytest.mark.parametrize("case", GOLDEN["e2e"], ids=lambda c: f"{c['name']}-k{c['k']}-cm{c['count_max']}")
+def test_job_matches_reference_tools(counter, kc, case):
+    files = _case_files(case["name"])
+    r = counter.count(files, k=case["k"], count_max=case["count_max"], hist_min=1, hist_max=10000)
+    sparse = {str(i + 1): int(v) for i, v in enumerate(r.hist) if v}
+    assert sparse == case["hist"]
+    text = kc.dump_text(r.keys, r.counts, case["k"]).encode()
+    assert text.count(b"\n") == case["dump_lines"]
+    assert hashlib.sha256(text).hexdigest() == case["dump_sha256"]
+    assert r.occurrences == sum(len(O.extract(f, case["k"])) for f in files)
+
+
+@pytest.mark.parametrize("name,k", [("plain_small", 31), ("repeat", 21), ("mixed", 21), ("edge", 25)])
+@pytest.mark.parametrize("min_count", [1, 2])
+def test_bloom_job_exact(counter, name, k, min_count):
+    files = _case_files(name)
+    want_k, want_c = O.exact_records(files, k, U32, min_count=min_count)
+    r = counter.count(files, k=k, count_max=U32, bloom=True, memory_gb=1, min_count=min_count, hist_min=1,
+                      hist_max=5000)
+    assert np.array_equal(r.keys, want_k)
+    assert np.array_equal(r.counts, want_c)
+    all_k, all_c = O.exact_records(files, k, U32)
+    assert r.hist.tolist() == O.histogram(all_c, 1, 5000).tolist()
+    assert r.distinct == len(all_k)
+
+
+@pytest.mark.parametrize("rec", GOLDEN["prepass"], ids=lambda r: r["name"])
+def test_bloom_plan_matches_reference(kc, rec):
+    import test_oracle_golden as T
+    files = T._prepass_files(rec["name"])
+    pc, avg, caps, mx = kc.bloom_plan(files, rec["k"], rec["memory_gb"])
+    assert pc.tolist() == rec["raw_prefix_counts"]
+    assert avg == rec["avg_quality"]
+    assert mx == rec["max_bloom_capacity"]
+    assert caps.tolist() == rec["bloom_capacities"]
+
+
+def test_plain_job_full_size(counter):
+    """The plain job at its full size (1 Mbp genome, 200k x 150 bp)."""
+    import ktcountermemorygreedy_b200.synth as S
+    fq, k = S.plain_job()
+    fq = fq.tobytes()
+    want_k, want_c = O.exact_records([fq], k, U32)
+    r = counter.count([fq], k=k, count_max=U32, hist_max=10000)
+    assert r.occurrences == int(want_c.sum(dtype=np.uint64))
+    assert np.array_equal(r.keys, want_k)
+    assert np.array_equal(r.counts, want_c)
+    assert r.hist.tolist() == O.histogram(want_c, 1, 10000).tolist()
+
+
+def test_queries(counter, kc):
+    files = _case_files("repeat")
+    k = 21
+    want_k, want_c = O.exact_records(files, k, U32)
+    r = counter.count(files, k=k, count_max=U32, top_n=1000, want_le2=True)
+    strs = [kc.string_key(int(w), k) for w in want_k]
+    order = sorted(range(len(want_k)), key=lambda i: (-int(want_c[i]), strs[i]))[:1000]
+    assert r.top_keys.tolist() == [int(want_k[i]) for i in order]
+    assert r.top_counts.tolist() == [int(want_c[i]) for i in order]
+    m = want_c <= 2
+    assert r.le2_keys.tolist() == want_k[m].tolist()
+    assert r.le2_counts.tolist() == want_c[m].tolist()
+
+
+def test_count_filters_and_saturation(counter):
+    files = _case_files("repeat")
+    for cm, lo, hi in [(255, 1, U32), (100, 50, 100), (U32, 3, 7)]:
+        want_k, want_c = O.exact_records(files, 31, cm, min_count=lo, max_count=hi)
+        r = counter.count(files, k=31, count_max=cm, min_count=lo, max_count=hi)
+        assert np.array_equal(r.keys, want_k) and np.array_equal(r.counts, want_c)
+
+
+def test_batch_matches_oracle(counter):
+    samples, ks = [], []
+    for i, (name, files, kl) in enumerate(fixtures.E2E_CASES):
+        samples.append(files)
+        ks.append(kl[-1])
+    samples.append([fixtures.random_fastq(40, 50, (120, 120), genome_len=1000)])
+    ks.append(21)
+    res = counter.count_batch(samples, ks, count_max=U32)
+    for files, k, r in zip(samples, ks, res):
+        want_k, want_c = O.exact_records(files, k, U32)
+        assert np.array_equal(r.keys, want_k), k
+        assert np.array_equal(r.counts, want_c)
+        assert r.hist.tolist() == O.histogram(want_c, 1, 10000).tolist()
+
+
+def test_jobs_same_alone_and_in_the_mix(kc):
+    jobs = []
+    for i in range(12):
+        f = fixtures.random_fastq(100 + i, 300 + 97 * i, (100, 150), genome_len=2000 + 500 * i)
+        jobs.append(([f], [21, 25, 31][i % 3]))
+    alone = []
+    with kc.KmerCounter(max_inflight_jobs=1) as c1:
+        for files, k in jobs:
+            alone.append(c1.count(files, k=k, count_max=U32, top_n=50, want_le2=True))
+    with kc.KmerCounter(max_inflight_jobs=6) as c6:
+        ids = [c6.submit(files, k=k, count_max=U32, top_n=50, want_le2=True) for files, k in jobs]
+        mixed = []
+        for jid, (files, k) in zip(ids, jobs):
+            c6.wait(jid)
+            mixed.append(c6.result(jid, k))
+    for (files, k), a, m in zip(jobs, alone, mixed):
+        want_k, want_c = O.exact_records(files, k, U32)
+        for r in (a, m):
+            assert np.array_equal(r.keys, want_k) and np.array_equal(r.counts, want_c)
+        assert np.array_equal(a.top_keys, m.top_keys) and np.array_equal(a.le2_keys, m.le2_keys)
+        assert np.array_equal(a.hist, m.hist)
+
+
+def test_resident_input(counter):
+    files = _case_files("mixed")
+    inp = counter.upload(files)
+    try:
+        r = counter.count(input=inp, k=21, count_max=U32)
+        want_k, want_c = O.exact_records(files, 21, U32)
+        assert np.array_equal(r.keys, want_k) and np.array_equal(r.counts, want_c)
+    finally:
+        counter.free_input(inp)
+
+
+def test_merge_records_matches_tool_merge(kc):
+    """A high/low split like the reference counter writes (each k-mer in
+    high.bin, low.bin or both, at most one low occurrence) merges to the
+    exact counts, as histogram_tool/dump_tool precise compute them."""
+    rng = np.random.default_rng(7)
+    files = _case_files("plain_small")
+    k = 31
+    uk, uc = O.count(O.extract_files(files, k))
+    in_low = rng.random(len(uk)) < 0.6
+    high_part = uc.astype(np.int64) - in_low
+    hm = high_part > 0
+    for cm in (U32, 255, 3):
+        ok, oc, hist = kc.merge_records(uk[hm], high_part[hm].clip(0, cm).astype(np.uint32), uk[in_low], k, cm,
+                                        hist_min=1, hist_max=300)
+        want_k, want_c = O.sort_string_order(uk, np.minimum(uc, cm).astype(np.uint32), k)
+        assert np.array_equal(ok, want_k) and np.array_equal(oc, want_c)
+        assert hist.tolist() == O.histogram(want_c, 1, 300).tolist()
+
+
+def test_cli_round_trip():
+    """kmer_counter -> tmp_dir -> histogram_tool / dump_tool, byte-identical to
+    the reference tools' outputs recorded in the golden vectors."""
+    bin_dir = os.path.join(ROOT, "ktcountermemorygreedy_b200", "bin")
+    case = [c for c in GOLDEN["e2e"] if c["name"] == "multi" and c["k"] == 31][0]
+    with tempfile.TemporaryDirectory() as tmp:
+        paths = []
+        for i, data in enumerate(_case_files("multi")):
+            p = os.path.join(tmp, f"m{i}.fq")
+            open(p, "wb").write(data)
+            paths.append(p)
+        d = os.path.join(tmp, "t")
+        os.makedirs(d)
+        subprocess.run([os.path.join(bin_dir, "kmer_counter"), ",".join(paths), "31", "8", "1", d, "1024", "2",
+                        str(U32), str(U32)], check=True, capture_output=True)
+        assert os.path.getsize(os.path.join(d, "low.bin")) == 0
+        h = os.path.join(tmp, "h.tsv")
+        subprocess.run([os.path.join(bin_dir, "histogram_tool"), "precise", d, "8", "1", h, "1", "10000"], check=True,
+                       capture_output=True)
+        sparse = {}
+        for line in open(h):
+            a, b = line.split("\t")
+            if int(b):
+                sparse[a] = int(b)
+        assert sparse == case["hist"]
+        o = os.path.join(tmp, "d.txt")
+        subprocess.run([os.path.join(bin_dir, "dump_tool"), "precise", d, "8", "1", o, "1", str(U32), "--sort"],
+                       check=True, capture_output=True)
+        assert hashlib.sha256(open(o, "rb").read()).hexdigest() == case["dump_sha256"]
