@@ -316,7 +316,7 @@ def run_ours(args):
         r = None
         for _ in range(args.e2e_steps):
             t0 = time.perf_counter()
-            r = counter.count([fq], keep_records=True, **JOB)
+            r = counter.count([fq], keep_records=True, copy=False, **JOB)
             walls.append(time.perf_counter() - t0)
             occ_e += r.occurrences
         h2d = len(fq)

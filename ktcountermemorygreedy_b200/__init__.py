@@ -201,6 +201,30 @@ def _copy(ptr, n, dtype):
     return np.ctypeslib.as_array(ptr, shape=(n,)).copy()
 
 
+class _JobLease:
+    """Keeps a finished job (and the pinned result memory it owns) alive
+    while numpy views of its results exist; releases it afterwards."""
+
+    def __init__(self, counter, jid):
+        self.counter, self.jid = counter, jid
+
+    def __del__(self):
+        try:
+            if self.counter._h:
+                self.counter.release(self.jid)
+        except Exception:
+            pass
+
+
+def _view(ptr, n, dtype, lease):
+    if n == 0 or not ptr:
+        return np.zeros(0, dtype)
+    ctype = C.c_uint64 if dtype == np.uint64 else C.c_uint32
+    raw = (ctype * n).from_address(C.addressof(ptr.contents))
+    raw._lease = lease   # the array's base keeps the job alive
+    return np.frombuffer(raw, dtype=dtype)
+
+
 class KmerCounter:
     """Handle on one GPU (``kc_open``).  ``max_inflight_jobs`` jobs run on the
     device at once; further jobs are admitted in submission order as device
@@ -292,12 +316,21 @@ class KmerCounter:
         finally:
             pass
 
-    def result(self, jid: int, k: int, release: bool = True) -> Result:
+    def result(self, jid: int, k: int, release: bool = True, copy: bool = True) -> Result:
+        """Results of a finished job.  copy=False returns the sorted records
+        as views of the job's pinned host memory; the job is released when
+        the last view is gone."""
         r = kc_result_t()
         _check(lib().kc_result(self._h, jid, C.byref(r)))
+        if copy:
+            keys, counts = _copy(r.keys, r.n_records, np.uint64), _copy(r.counts, r.n_records, np.uint32)
+        else:
+            lease = _JobLease(self, jid)
+            keys, counts = _view(r.keys, r.n_records, np.uint64, lease), _view(r.counts, r.n_records, np.uint32, lease)
+            release = False
         out = Result(
             k=k,
-            keys=_copy(r.keys, r.n_records, np.uint64), counts=_copy(r.counts, r.n_records, np.uint32),
+            keys=keys, counts=counts,
             hist=_copy(r.hist, r.hist_len, np.int64), hist_min=0,
             top_keys=_copy(r.top_keys, r.n_top, np.uint64), top_counts=_copy(r.top_counts, r.n_top, np.uint32),
             le2_keys=_copy(r.le2_keys, r.n_le2, np.uint64), le2_counts=_copy(r.le2_counts, r.n_le2, np.uint32),
@@ -316,11 +349,11 @@ class KmerCounter:
     def write_tmpdir(self, jid: int, path: str):
         _check(lib().kc_write_tmpdir(self._h, jid, path.encode()))
 
-    def count(self, files: Sequence[bytes] = (), input=None, **kw) -> Result:
+    def count(self, files: Sequence[bytes] = (), input=None, copy: bool = True, **kw) -> Result:
         """One job: FASTQ files -> exact canonical counts (blocking)."""
         jid = self.submit(files, input=input, **kw)
         self.wait(jid)
-        res = self.result(jid, kw.get("k", 31))
+        res = self.result(jid, kw.get("k", 31), copy=copy)
         res.hist_min = kw.get("hist_min", 1)
         return res
 

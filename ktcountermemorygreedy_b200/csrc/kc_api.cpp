@@ -92,8 +92,7 @@ struct Job {
     std::string err_msg;
     double t_submit = 0, t_start = 0, t_end = 0;
     // results
-    std::vector<uint64_t> keys;
-    std::vector<uint32_t> counts;
+    HostRecords recs;
     std::vector<int64_t> hist;
     std::vector<uint64_t> top_keys, le2_keys;
     std::vector<uint32_t> top_counts, le2_counts;
@@ -135,11 +134,17 @@ struct PhaseClock {
         launches[cur] += thread_kernel_launches() - l0;
         cur_a = nullptr;
     }
-    void collect(double *ms, uint64_t *ln)
+    void collect(double *ms, uint64_t *ln, cudaEvent_t origin)
     {
+        static const bool trace = getenv("KC_TRACE") && getenv("KC_TRACE")[0] == '1';
         for (auto &s : spans) {
             float t = 0;
             if (cudaEventElapsedTime(&t, s.a, s.b) == cudaSuccess) ms[s.phase] += t;
+            if (trace) {
+                float t0 = 0;
+                cudaEventElapsedTime(&t0, origin, s.a);
+                fprintf(stderr, "[kc trace] stage %d: %.3f .. %.3f ms\n", s.phase, t0, t0 + t);
+            }
         }
         for (int i = 0; i < 8; ++i) ln[i] += launches[i];
     }
@@ -201,17 +206,20 @@ struct Counters {
 
 Counters read_counters(const unsigned long long *d, cudaStream_t st)
 {
+    static const bool trace = getenv("KC_TRACE") && getenv("KC_TRACE")[0] == '1';
     Counters c{};
+    double t0 = trace ? now_ms() : 0;
     CK(cudaMemcpyAsync(c.v, d, sizeof(c.v), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    if (trace) fprintf(stderr, "[kc trace] counter read-back waited %.3f ms (host clock %.3f)\n", now_ms() - t0, now_ms());
     return c;
 }
 
-void run_job(Job &job, cudaStream_t st)
+void run_job(Job &job, cudaStream_t st, Workspace &ws)
 {
     const kc_job &P = job.p;
     const uint32_t k = P.k;
-    DevScope ds(st);
+    DevScope ds(st, &ws);
     std::vector<uint32_t> tile_seg_host;
 
     // ---- input -----------------------------------------------------------
@@ -276,10 +284,16 @@ void run_job(Job &job, cudaStream_t st)
     a.counters = counters;
     a.occ = occ;
     a.hll = hll;
+    a.hll_local = 1;
     uint32_t *prefix_hist = nullptr;
     unsigned long long *qual = nullptr;
+    unsigned long long *bucket_hist = nullptr;
     clk.begin(1);
     if (P.bloom) {
+        a.hll = nullptr;   // the tables are sized from the non-FIRST occurrences instead
+        bucket_hist = ds.n<unsigned long long>(N_BUCKETS);
+        CK(cudaMemsetAsync(bucket_hist, 0, N_BUCKETS * 8, st));
+        a.bucket_hist = bucket_hist;
         int32_t *chunk_lastnl = ds.n<int32_t>(std::max<uint64_t>(n_chunks, 1));
         uint64_t *d_chunk0 = ds.n<uint64_t>(seg_chunk0.size());
         prefix_hist = ds.n<uint32_t>(256);
@@ -327,6 +341,11 @@ void run_job(Job &job, cudaStream_t st)
         CK(cudaMemcpyAsync(d_tr, &tr, sizeof(tr), cudaMemcpyHostToDevice, st));
     };
     const uint32_t max_probe_cap = 1u << 16;
+    BucketCfg *d_cfg = nullptr;           // partitioned pipeline state kept for the merge
+    unsigned long long *bucket_ovf = nullptr;
+    WorkItem *low_items = nullptr;
+    size_t n_low_items = 0;
+    unsigned int *merge_next = nullptr;
     if (!P.bloom) {
         cap = table_capacity_for(est);
         for (int attempt = 0;; ++attempt) {
@@ -344,55 +363,139 @@ void run_job(Job &job, cudaStream_t st)
             cap *= 2;
         }
     } else {
+        // ---- root-prefix buckets (the reference's 256 root prefixes,
+        // src/NewKmerTree.h:1488-1495): exact sizes from the SCAN pass, one
+        // scatter pass, then every bucket's Bloom filter and table slice is
+        // processed while it sits in L2
+        std::vector<unsigned long long> bh(N_BUCKETS);
+        CK(cudaMemcpyAsync(bh.data(), bucket_hist, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        std::vector<BucketCfg> cfg(N_BUCKETS);
+        unsigned long long off = 0;
+        for (uint32_t b = 0; b < N_BUCKETS; ++b) {
+            cfg[b].key_base = off;
+            cfg[b].key_len = bh[b];
+            off += bh[b];
+        }
+        if (off != O) throw KcError{KC_ERR_DEVICE, "bucket census does not add up to the occurrences"};
+        const unsigned long long ocap = std::max<unsigned long long>(O, 1);
         // reference sizing (src/main.cpp:41-153) from the pre-pass statistics
         uint8_t avg_q = qh[1] ? (uint8_t)(qh[0] / qh[1]) : 0;
         BloomPlan bp = bloom_plan(ph.data(), avg_q, in->total_bytes, P.memory_gb, k);
-        std::vector<unsigned long long> boff(256), bcap(256);
         unsigned long long words = 0;
-        for (int i = 0; i < 256; ++i) {
-            boff[i] = words;
-            bcap[i] = bp.caps[i];
-            words += 2 * bp.caps[i];
+        for (uint32_t b = 0; b < N_BUCKETS; ++b) {
+            cfg[b].bloom_off = words;
+            cfg[b].bloom_cap = bp.caps[b];
+            words += 2 * bp.caps[b];
         }
+        // allocation order lets the scattered k-mers and then the filter be
+        // given back before the tables are laid out
+        list = ds.n<unsigned long long>(ocap);
         unsigned long long *bits = ds.n<unsigned long long>(words);
-        unsigned long long *d_boff = ds.n<unsigned long long>(256);
-        unsigned long long *d_bcap = ds.n<unsigned long long>(256);
+        unsigned long long *keys = ds.n<unsigned long long>(ocap);
+        BucketCfg *d_cfg_b = ds.n<BucketCfg>(N_BUCKETS);
+        unsigned long long *cursor = ds.n<unsigned long long>(N_BUCKETS);
+        unsigned long long *bbase = ds.n<unsigned long long>(N_BUCKETS);
+        unsigned long long *lh_cnt = ds.n<unsigned long long>(2 * N_BUCKETS);
+        uint32_t *hll_high = ds.n<uint32_t>((size_t)N_BUCKETS * BUCKET_HLL_M);
+        unsigned int *next_item = ds.n<unsigned int>(1);
+        std::vector<unsigned long long> bb(N_BUCKETS);
+        for (uint32_t b = 0; b < N_BUCKETS; ++b) bb[b] = cfg[b].key_base;
+        CK(cudaMemsetAsync(cursor, 0, N_BUCKETS * 8, st));
+        CK(cudaMemcpyAsync(bbase, bb.data(), N_BUCKETS * 8, cudaMemcpyHostToDevice, st));
         CK(cudaMemsetAsync(bits, 0, words * 8, st));
-        CK(cudaMemcpyAsync(d_boff, boff.data(), 256 * 8, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_bcap, bcap.data(), 256 * 8, cudaMemcpyHostToDevice, st));
-        uint32_t *hll_high = ds.n<uint32_t>(HLL_M);
-        CK(cudaMemsetAsync(hll_high, 0, HLL_M * 4, st));
-        list = ds.n<unsigned long long>(std::max<unsigned long long>(O, 1));
-        a.bloom_off = d_boff;
-        a.bloom_cap = d_bcap;
-        a.bloom_bits = bits;
-        a.hll_high = hll_high;
-        a.list = list;
-        a.list_cap = std::max<unsigned long long>(O, 1);
+        CK(cudaMemsetAsync(lh_cnt, 0, 2 * N_BUCKETS * 8, st));
+        CK(cudaMemsetAsync(hll_high, 0, (size_t)N_BUCKETS * BUCKET_HLL_M * 4, st));
+        CK(cudaMemcpyAsync(d_cfg_b, cfg.data(), N_BUCKETS * sizeof(BucketCfg), cudaMemcpyHostToDevice, st));
+        a.hll = nullptr;
         a.prepass = 0;
+        a.bucket_hist = nullptr;
+        a.list = keys;
+        a.list_cap = ocap;
+        a.bucket_cursor = cursor;
+        a.bucket_base = bbase;
         clk.begin(2);
-        CK(launch_extract(MODE_BLOOM, a, 0, st));
+        CK(launch_extract(MODE_PART, a, 0, st));
+        std::vector<WorkItem> items;
+        auto add_items = [&](uint32_t b, unsigned long long begin, unsigned long long end) {
+            for (unsigned long long s = begin; s < end; s += WORK_ITEM_KEYS)
+                items.push_back(WorkItem{s, std::min<unsigned long long>(end, s + WORK_ITEM_KEYS), b, 0});
+        };
+        for (uint32_t b = 0; b < N_BUCKETS; ++b) add_items(b, cfg[b].key_base, cfg[b].key_base + cfg[b].key_len);
+        WorkItem *d_items = ds.n<WorkItem>(std::max<size_t>(items.size(), 1));
+        if (!items.empty())
+            CK(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, st));
+        CK(launch_bloom_buckets(keys, d_items, (uint32_t)items.size(), next_item, d_cfg_b, bits, list, lh_cnt,
+                                lh_cnt + N_BUCKETS, hll_high, st));
         clk.end();
-        CK(cudaMemcpyAsync(hll_h.data(), hll_high, HLL_M * 4, cudaMemcpyDeviceToHost, st));
+        std::vector<unsigned long long> lh(2 * N_BUCKETS);
+        std::vector<uint32_t> hh((size_t)N_BUCKETS * BUCKET_HLL_M);
+        CK(cudaMemcpyAsync(lh.data(), lh_cnt, 2 * N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hh.data(), hll_high, hh.size() * 4, cudaMemcpyDeviceToHost, st));
         Counters c = read_counters(counters, st);
-        check_flags(c.v[C_FLAGS], "bloom");
-        low_len = c.v[C_LOW_LEN];
-        high_len = c.v[C_HIGH_LEN];
+        check_flags(c.v[C_FLAGS], "partition");
+        ds.release(d_items);
+        ds.release(next_item);
+        ds.release(hll_high);
+        ds.release(lh_cnt);
+        ds.release(bbase);
+        ds.release(cursor);
+        ds.release(d_cfg_b);
+        ds.release(keys);
         ds.release(bits);
-        double est_high = high_len ? hll_estimate(hll_h.data(), HLL_M) : 0.0;
-        cap = table_capacity_for(est_high);
+        low_len = high_len = 0;
+        std::vector<uint64_t> bcaps(N_BUCKETS);
+        for (uint32_t b = 0; b < N_BUCKETS; ++b) {
+            low_len += lh[b];
+            high_len += lh[N_BUCKETS + b];
+            double e = lh[N_BUCKETS + b] ? hll_estimate(&hh[(size_t)b * BUCKET_HLL_M], BUCKET_HLL_M) : 0.0;
+            bcaps[b] = table_capacity_for(e);
+        }
+        // per-bucket sub-tables in one arena; a bucket whose table overflows
+        // gets twice the slots and the insert is repeated
+        d_cfg = ds.n<BucketCfg>(N_BUCKETS);
+        bucket_ovf = ds.n<unsigned long long>(N_BUCKETS);
+        next_item = ds.n<unsigned int>(1);
+        merge_next = ds.n<unsigned int>(1);
+        items.clear();
+        for (uint32_t b = 0; b < N_BUCKETS; ++b)
+            add_items(b, cfg[b].key_base + cfg[b].key_len - lh[N_BUCKETS + b], cfg[b].key_base + cfg[b].key_len);
+        const size_t n_high_items = items.size();
+        for (uint32_t b = 0; b < N_BUCKETS; ++b) add_items(b, cfg[b].key_base, cfg[b].key_base + lh[b]);
+        n_low_items = items.size() - n_high_items;
+        d_items = ds.n<WorkItem>(std::max<size_t>(items.size(), 1));
+        if (!items.empty())
+            CK(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, st));
+        low_items = d_items + n_high_items;
         for (int attempt = 0;; ++attempt) {
-            alloc_table(cap);
-            CK(cudaMemsetAsync(counters, 0, 8, st));
-            uint32_t mp = (uint32_t)std::min<uint64_t>(cap, max_probe_cap);
+            cap = 0;
+            for (uint32_t b = 0; b < N_BUCKETS; ++b) {
+                cfg[b].slot_base = cap;
+                cfg[b].slot_cap = bcaps[b];
+                cap += bcaps[b];
+            }
+            if (tr.slots) ds.release(tr.slots);
+            tr.slots = static_cast<Slot *>(ds.get(cap * sizeof(Slot)));
+            tr.mask = 0;   // the arena is addressed per bucket
+            CK(launch_init_slots(tr.slots, cap, st));
+            CK(cudaMemcpyAsync(d_cfg, cfg.data(), N_BUCKETS * sizeof(BucketCfg), cudaMemcpyHostToDevice, st));
+            CK(cudaMemsetAsync(bucket_ovf, 0, N_BUCKETS * 8, st));
             clk.begin(3);
-            CK(launch_insert_list(list + a.list_cap - high_len, high_len, tr, mp, counters, st));
+            CK(launch_insert_buckets(list, d_items, (uint32_t)n_high_items, next_item, d_cfg, tr.slots,
+                                     max_probe_cap, bucket_ovf, st));
             clk.end();
+            std::vector<unsigned long long> ov(N_BUCKETS);
+            CK(cudaMemcpyAsync(ov.data(), bucket_ovf, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
             Counters cc = read_counters(counters, st);
             check_flags(cc.v[C_FLAGS], "insert");
-            if (!(cc.v[C_FLAGS] & ERR_TABLE_FULL)) break;
+            bool any = false;
+            for (uint32_t b = 0; b < N_BUCKETS; ++b)
+                if (ov[b]) {
+                    bcaps[b] *= 2;
+                    any = true;
+                }
+            if (!any) break;
             if (attempt >= 3) throw KcError{KC_ERR_DEVICE, "counting table overflow"};
-            cap *= 2;
         }
     }
     job.table_cap = cap;
@@ -416,8 +519,8 @@ void run_job(Job &job, cudaStream_t st)
     CK(cudaMemsetAsync(hist, 0, HIST_BINS * 8, st));
     if (P.bloom && low_len) {
         clk.begin(4);
-        CK(launch_merge_low(list, low_len, tr, (uint32_t)std::min<uint64_t>(cap, max_probe_cap), P.min_count,
-                            P.max_count, rec_keys, rec_counts, rec_cap, counters, st));
+        CK(launch_merge_buckets(list, low_items, (uint32_t)n_low_items, merge_next, d_cfg, tr.slots, max_probe_cap,
+                                P.min_count, P.max_count, rec_keys, rec_counts, rec_cap, counters, st));
         clk.end();
     }
     clk.begin(5);
@@ -551,18 +654,17 @@ void run_job(Job &job, cudaStream_t st)
 
     // ---- records to host ------------------------------------------------------
     if (P.keep_records) {
-        job.keys.resize(n_rec);
-        job.counts.resize(n_rec);
+        job.recs.allocate(n_rec);
         if (n_rec) {
-            CK(cudaMemcpyAsync(job.keys.data(), rec_keys, n_rec * 8, cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(job.counts.data(), rec_counts, n_rec * 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(job.recs.keys(), rec_keys, n_rec * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(job.recs.counts(), rec_counts, n_rec * 4, cudaMemcpyDeviceToHost, st));
         }
     }
     CK(cudaStreamSynchronize(st));
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, ev0, ev1));
     job.device_ms = ms;
-    clk.collect(job.phase_ms, job.phase_launches);
+    clk.collect(job.phase_ms, job.phase_launches, ev0);
     job.low_len = low_len;
     job.high_len = high_len;
     job.input_bytes = in->total_bytes;
@@ -599,11 +701,11 @@ uint64_t reserve_for(const kc_job &p, uint64_t resident_bytes)
 // Batched jobs: every sample's files in one device buffer, one SCAN and one
 // INSERT launch over all tiles (each tile counts into its sample's table in a
 // shared slot arena), one batched compaction, one segmented radix sort.
-void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st)
+void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st, Workspace &ws)
 {
     const uint32_t n = (uint32_t)jobs.size();
     if (n > MAX_BATCH) throw KcError{KC_ERR_INVALID, "more than 4096 jobs in one batch"};
-    DevScope ds(st);
+    DevScope ds(st, &ws);
     std::vector<kc_buffer> files;
     std::vector<uint32_t> fsample;
     for (uint32_t i = 0; i < n; ++i)
@@ -654,6 +756,7 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st)
     a.counters = counters;
     a.occ = occ;
     a.hll = hll;
+    a.hll_local = n == 1;
     CK(launch_extract(MODE_SCAN, a, 0, st));
     std::vector<unsigned long long> occ_h(n);
     std::vector<uint32_t> hll_h((size_t)n * HLL_M);
@@ -750,12 +853,15 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st)
     if (n_ovf) CK(cudaMemcpyAsync(ovf_h.data(), ovf, n_ovf * 8, cudaMemcpyDeviceToHost, st));
     for (uint32_t i = 0; i < n; ++i) {
         Job &j = *jobs[i];
+        j.n_records_total = len_h[i];
+        j.input_bytes = 0;
+        for (const auto &f : j.files) j.input_bytes += f.size;
         if (!j.p.keep_records) continue;
-        j.keys.resize(len_h[i]);
-        j.counts.resize(len_h[i]);
+        j.recs.allocate(len_h[i]);
         if (len_h[i]) {
-            CK(cudaMemcpyAsync(j.keys.data(), rec_keys + cfg[i].rec_base, len_h[i] * 8, cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(j.counts.data(), rec_counts + cfg[i].rec_base, len_h[i] * 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(j.recs.keys(), rec_keys + cfg[i].rec_base, len_h[i] * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(j.recs.counts(), rec_counts + cfg[i].rec_base, len_h[i] * 4, cudaMemcpyDeviceToHost,
+                               st));
         }
     }
     CK(cudaStreamSynchronize(st));
@@ -784,6 +890,7 @@ void worker_main(kc_handle *h)
     cudaSetDevice(h->device);
     cudaStream_t st;
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    auto ws = std::make_unique<Workspace>(st);
     for (;;) {
         std::shared_ptr<Task> task;
         {
@@ -807,8 +914,9 @@ void worker_main(kc_handle *h)
         int code = KC_OK;
         std::string msg;
         try {
-            if (task->batch) run_batch(task->jobs, st);
-            else run_job(*task->jobs[0], st);
+            ws->begin_job();
+            if (task->batch) run_batch(task->jobs, st, *ws);
+            else run_job(*task->jobs[0], st, *ws);
         } catch (const KcError &e) {
             code = e.code;
             msg = e.msg;
@@ -817,6 +925,7 @@ void worker_main(kc_handle *h)
             msg = e.what();
         }
         if (code != KC_OK) cudaStreamSynchronize(st);
+        ws->end_job();
         {
             std::lock_guard<std::mutex> lk(h->mu);
             for (auto &j : task->jobs) {
@@ -831,6 +940,7 @@ void worker_main(kc_handle *h)
         h->cv_work.notify_all();
         h->cv_done.notify_all();
     }
+    ws.reset();
     cudaStreamDestroy(st);
 }
 
@@ -1019,9 +1129,9 @@ int kc_result(kc_handle *h, kc_job_id id, kc_result_t *out)
     Job &j = *it->second;
     if (j.state != JobState::DONE) return fail(j.state == JobState::FAILED ? j.err : KC_ERR_INVALID, "job not finished");
     std::memset(out, 0, sizeof(*out));
-    out->n_records = j.keys.size();
-    out->keys = j.keys.data();
-    out->counts = j.counts.data();
+    out->n_records = j.recs.n;
+    out->keys = j.recs.n ? j.recs.keys() : nullptr;
+    out->counts = j.recs.n ? j.recs.counts() : nullptr;
     out->hist_len = j.hist.size();
     out->hist = j.hist.data();
     out->n_top = j.top_keys.size();
@@ -1123,12 +1233,12 @@ extern "C" int kc_write_tmpdir(kc_handle *h, kc_job_id id, const char *dir)
     f = fopen((d + "high.bin").c_str(), "wb");
     if (!f) return fail(KC_ERR_IO, "cannot open " + d + "high.bin");
     std::vector<uint8_t> buf;
-    buf.reserve(std::min<size_t>(j.keys.size(), 1 << 20) * rec);
-    for (size_t i = 0; i < j.keys.size(); ++i) {
-        uint32_t c = j.counts[i];
+    buf.reserve(std::min<size_t>(j.recs.n, 1 << 20) * rec);
+    for (size_t i = 0; i < j.recs.n; ++i) {
+        uint32_t c = j.recs.counts()[i];
         if ((uint64_t)c + 1 < j.p.filter_min || c > j.p.filter_max) continue;
         uint8_t r[16];
-        uint64_t w = j.keys[i];
+        uint64_t w = j.recs.keys()[i];
         if (full) std::memcpy(r, &w, 8);
         else {
             uint64_t t = w & tmask;

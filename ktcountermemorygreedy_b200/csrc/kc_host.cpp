@@ -5,7 +5,12 @@
 #include "kc_host.h"
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include "kc_plan.h"
 
@@ -21,38 +26,198 @@ int set_error(int code, const std::string &msg)
     return code;
 }
 
-void *DevScope::get(size_t bytes)
+namespace {
+
+bool trace_on()
+{
+    static const bool t = getenv("KC_TRACE") && getenv("KC_TRACE")[0] == '1';
+    return t;
+}
+
+void *pool_alloc(size_t bytes, cudaStream_t st)
 {
     void *p = nullptr;
-    if (bytes == 0) bytes = 16;
-    bytes = (bytes + 255) & ~size_t(255);
+    auto t0 = std::chrono::steady_clock::now();
     cudaError_t e = cudaMallocAsync(&p, bytes, st);
+    if (trace_on()) {
+        double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (ms > 0.5) fprintf(stderr, "[kc trace] cudaMallocAsync %zu bytes took %.2f ms\n", bytes, ms);
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         throw KcError{KC_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed"};
     }
-    ptrs.push_back(p);
+    return p;
+}
+
+}  // namespace
+
+void Workspace::begin_job()
+{
+    top_ = 0;
+    if (high_ > cap_) {
+        // grow once to the high-water mark (plus headroom for jobs that vary)
+        CK(cudaStreamSynchronize(st_));
+        if (base_) cudaFree(base_);
+        base_ = nullptr;
+        cap_ = 0;
+        // the spilled blocks of earlier jobs are back in the pool: return them
+        int dev = 0;
+        cudaMemPool_t pool;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess)
+            cudaMemPoolTrimTo(pool, 0);
+        size_t want = (high_ + high_ / 8 + (64u << 20)) & ~size_t((2u << 20) - 1);
+        if (cudaMalloc(&base_, want) != cudaSuccess) {
+            cudaGetLastError();
+            base_ = nullptr;   // keep going from the pool
+            return;
+        }
+        cap_ = want;
+        if (trace_on()) fprintf(stderr, "[kc trace] workspace grown to %zu bytes\n", want);
+    }
+}
+
+void *Workspace::get(size_t bytes)
+{
+    if (base_ && top_ + bytes <= cap_) {
+        void *p = base_ + top_;
+        top_ += bytes;
+        high_ = std::max(high_, top_);
+        return p;
+    }
+    high_ = std::max(high_, top_ + bytes);
+    void *p = pool_alloc(bytes, st_);
+    spill_.push_back(p);
+    return p;
+}
+
+bool Workspace::release_top(void *p, size_t bytes)
+{
+    if (base_ && p == base_ + top_ - bytes) {
+        top_ -= bytes;
+        return true;
+    }
+    return false;
+}
+
+void Workspace::end_job()
+{
+    for (void *p : spill_) cudaFreeAsync(p, st_);
+    spill_.clear();
+    top_ = 0;
+}
+
+Workspace::~Workspace()
+{
+    end_job();
+    cudaStreamSynchronize(st_);
+    if (base_) cudaFree(base_);
+}
+
+void *DevScope::get(size_t bytes)
+{
+    if (bytes == 0) bytes = 16;
+    bytes = (bytes + 255) & ~size_t(255);
+    void *p = ws ? ws->get(bytes) : pool_alloc(bytes, st);
+    ptrs.emplace_back(p, bytes);
     return p;
 }
 
 void DevScope::release(void *p)
 {
-    auto it = std::find(ptrs.begin(), ptrs.end(), p);
-    if (it != ptrs.end()) {
-        cudaFreeAsync(p, st);
-        ptrs.erase(it);
-    }
+    auto it = std::find_if(ptrs.begin(), ptrs.end(), [&](const std::pair<void *, size_t> &x) { return x.first == p; });
+    if (it == ptrs.end()) return;
+    if (!ws) cudaFreeAsync(p, st);
+    else ws->release_top(p, it->second);   // memory further down stays until the job ends
+    ptrs.erase(it);
 }
 
 DevScope::~DevScope()
 {
-    for (void *p : ptrs) cudaFreeAsync(p, st);
+    if (!ws)
+        for (auto &x : ptrs) cudaFreeAsync(x.first, st);
 }
 
 uint64_t bit_ceil64(uint64_t x)
 {
     if (x <= 1) return 1;
     return 1ULL << (64 - __builtin_clzll(x - 1));
+}
+
+struct PinnedPool::Impl {
+    std::mutex mu;
+    std::multimap<size_t, void *> free_blocks;
+    size_t cached = 0;
+};
+
+PinnedPool::PinnedPool() : impl_(new Impl) {}
+
+PinnedPool &PinnedPool::instance()
+{
+    static PinnedPool pool;
+    return pool;
+}
+
+void *PinnedPool::get(size_t bytes, size_t &got)
+{
+    bytes = std::max<size_t>(bytes, 4096);
+    {
+        std::lock_guard<std::mutex> lk(impl_->mu);
+        auto it = impl_->free_blocks.lower_bound(bytes);
+        if (it != impl_->free_blocks.end() && it->first <= 2 * bytes + (64u << 20)) {
+            void *p = it->second;
+            got = it->first;
+            impl_->cached -= got;
+            impl_->free_blocks.erase(it);
+            return p;
+        }
+    }
+    void *p = nullptr;
+    const size_t want = (bytes + (2u << 20) - 1) & ~size_t((2u << 20) - 1);
+    if (cudaHostAlloc(&p, want, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        throw KcError{KC_ERR_NOMEM, "pinned host allocation of " + std::to_string(want) + " bytes failed"};
+    }
+    got = want;
+    return p;
+}
+
+void PinnedPool::put(void *p, size_t bytes)
+{
+    if (!p) return;
+    const size_t keep_limit = 32ULL << 30;
+    {
+        std::lock_guard<std::mutex> lk(impl_->mu);
+        if (impl_->cached + bytes <= keep_limit) {
+            impl_->free_blocks.emplace(bytes, p);
+            impl_->cached += bytes;
+            return;
+        }
+    }
+    cudaFreeHost(p);
+}
+
+PinnedPool::~PinnedPool()
+{
+    // process exit: the driver reclaims pinned memory; freeing here could run
+    // after the CUDA runtime has shut down
+    delete impl_;
+}
+
+void HostRecords::allocate(uint64_t count)
+{
+    reset();
+    n = count;
+    const size_t need = ((count * 8 + 255) & ~size_t(255)) + count * 4 + 256;
+    block = PinnedPool::instance().get(need, bytes);
+}
+
+void HostRecords::reset()
+{
+    if (block) PinnedPool::instance().put(block, bytes);
+    block = nullptr;
+    bytes = 0;
+    n = 0;
 }
 
 void build_input(kc_input &in, const kc_buffer *files, uint32_t n_files, cudaStream_t st, DevScope *scope,
@@ -302,7 +467,7 @@ int kc_bloom_plan(const kc_buffer *files, uint32_t n_files, uint32_t k, uint64_t
         a.segs = pr.d_segs;
         a.counters = counters;
         a.occ = occ;
-        a.hll = hll;
+        a.hll = nullptr;   // only the pre-pass sample needs k-mers
         a.prepass = 1;
         a.chunk_lastnl = chunk_lastnl;
         a.seg_chunk0 = d_chunk0;

@@ -31,11 +31,38 @@ int set_error(int code, const std::string &msg);
         }                                                                                                \
     } while (0)
 
-// Stream-ordered device allocations released together.
+// Device memory of one worker stream, reused job after job: one block sized
+// to the high-water mark of the jobs seen so far, handed out by a bump
+// pointer (the most recent allocation can be given back).  Allocation-heavy
+// jobs would otherwise spend tens to hundreds of milliseconds per multi-GB
+// stream-ordered allocation.  Requests that do not fit go to the stream's
+// memory pool for this job; the next job then gets a block that fits all.
+class Workspace {
+public:
+    explicit Workspace(cudaStream_t st) : st_(st) {}
+    Workspace(const Workspace &) = delete;
+    Workspace &operator=(const Workspace &) = delete;
+    void begin_job();
+    void *get(size_t bytes);
+    bool release_top(void *p, size_t bytes);
+    void end_job();
+    ~Workspace();
+    size_t capacity() const { return cap_; }
+
+private:
+    cudaStream_t st_;
+    uint8_t *base_ = nullptr;
+    size_t cap_ = 0, top_ = 0, high_ = 0;
+    std::vector<void *> spill_;
+};
+
+// Device allocations of one job step, from a Workspace or (without one)
+// from the stream's memory pool.  Everything is released with the scope.
 struct DevScope {
     cudaStream_t st = nullptr;
-    std::vector<void *> ptrs;
-    explicit DevScope(cudaStream_t s) : st(s) {}
+    Workspace *ws = nullptr;
+    std::vector<std::pair<void *, size_t>> ptrs;
+    explicit DevScope(cudaStream_t s, Workspace *w = nullptr) : st(s), ws(w) {}
     DevScope(const DevScope &) = delete;
     DevScope &operator=(const DevScope &) = delete;
     void *get(size_t bytes);
@@ -49,6 +76,39 @@ struct DevScope {
 };
 
 uint64_t bit_ceil64(uint64_t x);
+
+// Pinned host blocks reused across jobs: result copies from the device run at
+// link speed and no block is pinned (or zero-filled) twice.
+class PinnedPool {
+public:
+    static PinnedPool &instance();
+    void *get(size_t bytes, size_t &got);   // throws KcError on failure
+    void put(void *p, size_t bytes);
+    ~PinnedPool();
+
+private:
+    struct Impl;
+    Impl *impl_ = nullptr;
+    PinnedPool();
+};
+
+// (key, count) records of one job in a pinned block.
+struct HostRecords {
+    void *block = nullptr;
+    size_t bytes = 0;
+    uint64_t n = 0;
+    HostRecords() = default;
+    HostRecords(const HostRecords &) = delete;
+    HostRecords &operator=(const HostRecords &) = delete;
+    void allocate(uint64_t count);
+    uint64_t *keys() const { return static_cast<uint64_t *>(block); }
+    uint32_t *counts() const
+    {
+        return reinterpret_cast<uint32_t *>(static_cast<uint8_t *>(block) + ((n * 8 + 255) & ~uint64_t(255)));
+    }
+    void reset();
+    ~HostRecords() { reset(); }
+};
 
 }  // namespace kc
 

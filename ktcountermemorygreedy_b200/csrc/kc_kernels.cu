@@ -181,6 +181,14 @@ __device__ __forceinline__ void hll_add(uint32_t *regs, unsigned long long key)
     if (rank > *(volatile uint32_t *)&regs[r]) atomicMax(&regs[r], rank);
 }
 
+__device__ __forceinline__ void hll_add_shared(uint32_t *regs, unsigned long long key)
+{
+    uint64_t h = slot_hash(key ^ 0x5bd1e9955bd1e995ULL);
+    uint32_t r = (uint32_t)(h >> (64 - HLL_BITS));
+    uint32_t rank = __clzll((h << HLL_BITS) | (1ULL << (HLL_BITS - 1))) + 1;
+    if (rank > regs[r]) atomicMax(&regs[r], rank);
+}
+
 __device__ __forceinline__ bool table_add(Slot *slots, unsigned long long mask, unsigned long long key,
                                           unsigned int c, uint32_t max_probe)
 {
@@ -291,10 +299,17 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
     uint64_t *s_codes = reinterpret_cast<uint64_t *>(smem + 2 * BUF_BYTES);   // 257 used
     uint32_t *s_good = reinterpret_cast<uint32_t *>(s_codes + 264);           // 257 used
     unsigned long long *s_stage = reinterpret_cast<unsigned long long *>(s_good + 264);
+    uint32_t *s_hll = reinterpret_cast<uint32_t *>(s_good + 264);   // SCAN mode: registers of sample 0
+    const bool hll_local = MODE == MODE_SCAN && a.hll && a.hll_local;
+
+    // PART mode: rank of each staged k-mer inside its bucket's share of the tile
+    uint16_t *s_rank = reinterpret_cast<uint16_t *>(s_stage + stage_cap);
 
     __shared__ __align__(8) uint64_t mbar[2];
     __shared__ uint32_t s_warp[8];
     __shared__ uint32_t s_hist[256];
+    __shared__ uint32_t s_bhist[MODE == MODE_SCAN || MODE == MODE_PART ? 256 : 1];
+    __shared__ unsigned long long s_bpos[MODE == MODE_PART ? 256 : 1];
     __shared__ unsigned long long s_bcast[2];
     __shared__ unsigned long long s_boff[MODE == MODE_BLOOM ? 256 : 1];
     __shared__ unsigned long long s_bcap[MODE == MODE_BLOOM ? 256 : 1];
@@ -308,7 +323,12 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
         mbar_init(&mbar[1], 1);
         fence_mbar_init();
     }
-    if (MODE == MODE_SCAN) s_hist[tid] = 0;
+    if (MODE == MODE_SCAN) {
+        s_hist[tid] = 0;
+        s_bhist[tid] = 0;
+    }
+    if (hll_local)
+        for (uint32_t i = tid; i < HLL_M; i += EXT_THREADS) s_hll[i] = 0;
     if (MODE == MODE_BLOOM) {
         s_boff[tid] = a.bloom_off[tid];
         s_bcap[tid] = a.bloom_cap[tid];
@@ -405,13 +425,17 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
                 uint64_t lim = sg.sample_end - seg_pos;
                 sample_ok = lim >= 32 ? FULL : ((1u << lim) - 1u);
             }
-            uint32_t e = ends;
+            // keys are needed for the HyperLogLog, the bucket histogram and
+            // the pre-pass sample; otherwise only the windows are counted
+            uint32_t e = (a.hll || a.bucket_hist) ? ends : (ends & sample_ok);
             uint32_t hll_base = sg.sample * HLL_M;
             while (e) {
                 uint32_t j = __ffs(e) - 1;
                 e &= e - 1;
                 unsigned long long key = window_key(prev, cur, j, kp);
-                hll_add(a.hll + hll_base, key);
+                if (hll_local) hll_add_shared(s_hll, key);
+                else if (a.hll) hll_add(a.hll + hll_base, key);
+                if (a.bucket_hist) atomicAdd(&s_bhist[key >> 56], 1u);
                 if ((sample_ok >> j) & 1u) atomicAdd(&s_hist[key >> 56], 1u);
             }
             unsigned n = __reduce_add_sync(FULL, (unsigned)__popc(ends));
@@ -435,6 +459,26 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
                         uint32_t i = r0 + tid;
                         bool act = i < nr;
                         warp_insert(act, act ? s_stage[i] : EMPTY_KEY, tr, a.max_probe, flags);
+                    }
+                } else if (MODE == MODE_PART) {
+                    // scatter into the root-prefix buckets: rank inside the
+                    // tile's share of each bucket, one cursor update per bucket
+                    s_bhist[tid] = 0;
+                    __syncthreads();
+                    for (uint32_t i = tid; i < nr; i += EXT_THREADS)
+                        s_rank[i] = (uint16_t)atomicAdd(&s_bhist[(uint32_t)(s_stage[i] >> 56)], 1u);
+                    __syncthreads();
+                    {
+                        const uint32_t c = s_bhist[tid];
+                        s_bpos[tid] = c ? a.bucket_base[tid] + atomicAdd(&a.bucket_cursor[tid], (unsigned long long)c)
+                                        : 0ull;
+                    }
+                    __syncthreads();
+                    for (uint32_t i = tid; i < nr; i += EXT_THREADS) {
+                        const unsigned long long key = s_stage[i];
+                        const unsigned long long pos = s_bpos[(uint32_t)(key >> 56)] + s_rank[i];
+                        if (pos < a.list_cap) a.list[pos] = key;
+                        else atomicOr(flags, ERR_LIST_FULL);
                     }
                 } else if (MODE == MODE_EMIT) {
                     if (tid == 0) s_bcast[0] = atomicAdd(&a.counters[C_EMIT_LEN], (unsigned long long)nr);
@@ -504,6 +548,16 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
         // one file-sample per job in Bloom mode; the histogram belongs to sample 0
         uint32_t v = s_hist[tid];
         if (v) atomicAdd(&a.prefix_hist[tid], v);
+    }
+    if (MODE == MODE_SCAN && a.bucket_hist) {
+        uint32_t v = s_bhist[tid];
+        if (v) atomicAdd(&a.bucket_hist[tid], (unsigned long long)v);
+    }
+    if (hll_local) {
+        for (uint32_t i = tid; i < HLL_M; i += EXT_THREADS) {
+            uint32_t v = s_hll[i];
+            if (v > *(volatile uint32_t *)&a.hll[i]) atomicMax(&a.hll[i], v);
+        }
     }
 }
 
@@ -941,6 +995,177 @@ __global__ void k_scatter_selected(const unsigned long long *keys, const uint32_
     }
 }
 
+// ---------------------------------------------------------------------------
+// bucket-major kernels of the partitioned pipeline
+// ---------------------------------------------------------------------------
+
+constexpr uint32_t ITEM_PER_THREAD = WORK_ITEM_KEYS / 256;
+
+// Claims the next work item for the whole block; false when none is left.
+__device__ __forceinline__ bool next_work(unsigned int *next_item, uint32_t n_items, uint32_t *s_item, uint32_t &it)
+{
+    if (threadIdx.x == 0) *s_item = atomicAdd(next_item, 1u);
+    __syncthreads();
+    it = *s_item;
+    __syncthreads();
+    return it < n_items;
+}
+
+__device__ __forceinline__ void hll_add_bits(uint32_t *regs, unsigned long long key, uint32_t bits)
+{
+    uint64_t h = slot_hash(key ^ 0x5bd1e9955bd1e995ULL);
+    uint32_t r = (uint32_t)(h >> (64 - bits));
+    uint32_t rank = __clzll((h << bits) | (1ULL << (bits - 1))) + 1;
+    if (rank > *(volatile uint32_t *)&regs[r]) atomicMax(&regs[r], rank);
+}
+
+// The reference's two-level Bloom classification (src/BloomFilter.h:233-273)
+// over the partitioned k-mers.  FIRST occurrences go to the front of the
+// bucket's range in `out`, the others to its back.  Only FIRST versus not
+// FIRST matters downstream, so both filter words are read with one 16-byte
+// load and the first word is set without reading its old value.
+__global__ void __launch_bounds__(256) k_bloom_buckets(const unsigned long long *keys, const WorkItem *items,
+                                                       uint32_t n_items, unsigned int *next_item,
+                                                       const BucketCfg *cfg, unsigned long long *bits,
+                                                       unsigned long long *out, unsigned long long *low_cnt,
+                                                       unsigned long long *high_cnt, uint32_t *hll_high)
+{
+    __shared__ uint32_t s_item, s_warp[8];
+    __shared__ unsigned long long s_lb, s_hb;
+    const int tid = threadIdx.x;
+    uint32_t it;
+    while (next_work(next_item, n_items, &s_item, it)) {
+        const WorkItem w = items[it];
+        const BucketCfg bc = cfg[w.bucket];
+        const uint64_t n = w.end - w.begin;
+        unsigned long long k[ITEM_PER_THREAD];
+        uint32_t firsts = 0, highs = 0;
+#pragma unroll
+        for (uint32_t g = 0; g < ITEM_PER_THREAD; g += 4) {
+            unsigned long long m[4];
+            ulonglong2 *cell[4];
+            ulonglong2 v[4];
+#pragma unroll
+            for (uint32_t u = 0; u < 4; ++u) {
+                const uint64_t i = (uint64_t)(g + u) * 256 + tid;
+                k[g + u] = i < n ? keys[w.begin + i] : EMPTY_KEY;
+                uint64_t block = 0, mask = 0;
+                if (i < n) bloom_probe(k[g + u], bc.bloom_cap, block, mask);
+                m[u] = mask;
+                cell[u] = reinterpret_cast<ulonglong2 *>(bits + bc.bloom_off + 2 * block);
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < 4; ++u)
+                if ((uint64_t)(g + u) * 256 + tid < n) v[u] = __ldcg(cell[u]);
+#pragma unroll
+            for (uint32_t u = 0; u < 4; ++u) {
+                if ((uint64_t)(g + u) * 256 + tid >= n) continue;
+                unsigned long long *c = reinterpret_cast<unsigned long long *>(cell[u]);
+                bool first = false;
+                if ((v[u].x & m[u]) != m[u]) {
+                    if ((v[u].y & m[u]) == m[u]) {
+                        atomicOr(&c[0], m[u]);
+                    } else {
+                        unsigned long long old2 = atomicOr(&c[1], m[u]);
+                        if ((old2 & m[u]) == m[u]) atomicOr(&c[0], m[u]);
+                        else first = true;
+                    }
+                }
+                if (first) firsts |= 1u << (g + u);
+                else {
+                    highs |= 1u << (g + u);
+                    hll_add_bits(hll_high + (size_t)w.bucket * BUCKET_HLL_M, k[g + u], BUCKET_HLL_BITS);
+                }
+            }
+        }
+        uint32_t tf, th;
+        const uint32_t of = block_excl_scan(__popc(firsts), s_warp, tf);
+        const uint32_t oh = block_excl_scan(__popc(highs), s_warp, th);
+        if (tid == 0) {
+            s_lb = atomicAdd(&low_cnt[w.bucket], (unsigned long long)tf);
+            s_hb = atomicAdd(&high_cnt[w.bucket], (unsigned long long)th);
+        }
+        __syncthreads();
+        unsigned long long lp = bc.key_base + s_lb + of;
+        unsigned long long hp = bc.key_base + bc.key_len - 1 - (s_hb + oh);
+#pragma unroll
+        for (uint32_t r = 0; r < ITEM_PER_THREAD; ++r) {
+            if ((firsts >> r) & 1u) out[lp++] = k[r];
+            else if ((highs >> r) & 1u) out[hp--] = k[r];
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_insert_buckets(const unsigned long long *keys, const WorkItem *items,
+                                                        uint32_t n_items, unsigned int *next_item,
+                                                        const BucketCfg *cfg, Slot *arena, uint32_t max_probe,
+                                                        unsigned long long *bucket_ovf)
+{
+    __shared__ uint32_t s_item;
+    const int tid = threadIdx.x;
+    uint32_t it;
+    while (next_work(next_item, n_items, &s_item, it)) {
+        const WorkItem w = items[it];
+        const BucketCfg bc = cfg[w.bucket];
+        const TableRef tr{arena + bc.slot_base, bc.slot_cap - 1};
+        const uint64_t n = w.end - w.begin;
+        unsigned long long k[ITEM_PER_THREAD];
+#pragma unroll
+        for (uint32_t r = 0; r < ITEM_PER_THREAD; ++r) {
+            const uint64_t i = (uint64_t)r * 256 + tid;
+            k[r] = i < n ? keys[w.begin + i] : EMPTY_KEY;
+        }
+#pragma unroll
+        for (uint32_t r = 0; r < ITEM_PER_THREAD; ++r)
+            warp_insert((uint64_t)r * 256 + tid < n, k[r], tr, max_probe, &bucket_ovf[w.bucket]);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_merge_buckets(const unsigned long long *keys, const WorkItem *items,
+                                                       uint32_t n_items, unsigned int *next_item,
+                                                       const BucketCfg *cfg, Slot *arena, uint32_t max_probe,
+                                                       uint32_t min_count, uint32_t max_count,
+                                                       unsigned long long *rec_keys, uint32_t *rec_counts,
+                                                       uint64_t rec_cap, unsigned long long *counters)
+{
+    __shared__ uint32_t s_item, s_warp[8];
+    __shared__ unsigned long long s_base;
+    const int tid = threadIdx.x;
+    const bool want1 = (min_count <= 1 && 1 <= max_count);
+    uint32_t it;
+    while (next_work(next_item, n_items, &s_item, it)) {
+        const WorkItem w = items[it];
+        const BucketCfg bc = cfg[w.bucket];
+        const TableRef tr{arena + bc.slot_base, bc.slot_cap - 1};
+        const uint64_t n = w.end - w.begin;
+        unsigned long long k[ITEM_PER_THREAD];
+#pragma unroll
+        for (uint32_t r = 0; r < ITEM_PER_THREAD; ++r) {
+            const uint64_t i = (uint64_t)r * 256 + tid;
+            k[r] = i < n ? keys[w.begin + i] : EMPTY_KEY;
+        }
+        uint32_t misses = 0;
+#pragma unroll
+        for (uint32_t r = 0; r < ITEM_PER_THREAD; ++r) {
+            if ((uint64_t)r * 256 + tid >= n) continue;
+            bool ovf = false;
+            Slot *sl = table_find(tr.slots, tr.mask, k[r], max_probe, ovf);
+            if (ovf) atomicOr(&counters[C_FLAGS], ERR_TABLE_FULL);
+            if (sl) atomicAdd(&sl->count, 1u);
+            else misses |= 1u << r;
+        }
+        unsigned nm = __reduce_add_sync(FULL, (unsigned)__popc(misses));
+        if ((tid & 31) == 0 && nm) atomicAdd(&counters[C_LOW_ONLY], (unsigned long long)nm);
+        if (want1) {
+#pragma unroll
+            for (uint32_t r = 0; r < ITEM_PER_THREAD; ++r)
+                append_records((misses >> r) & 1u, pair_reverse(k[r]), 1u, rec_keys, rec_counts, rec_cap, counters,
+                               s_warp, &s_base);
+        }
+    }
+}
+
 __global__ void k_hash_batch(const unsigned long long *keys, uint64_t n, unsigned long long *out)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -997,6 +1222,8 @@ size_t extract_smem_bytes_for(int mode, uint32_t stage_cap)
 {
     size_t b = 2 * BUF_BYTES + 264 * 8 + 264 * 4;
     if (mode != MODE_SCAN) b += (size_t)stage_cap * 8;
+    else b += HLL_M * 4;
+    if (mode == MODE_PART) b += (size_t)stage_cap * 2;
     return b;
 }
 
@@ -1048,6 +1275,7 @@ cudaError_t launch_extract(int mode, const ExtractArgs &a, int grid, cudaStream_
     case MODE_INSERT: return launch_extract_t<MODE_INSERT>(a, grid, STAGE_CAP, st);
     case MODE_BLOOM: return launch_extract_t<MODE_BLOOM>(a, grid, STAGE_CAP, st);
     case MODE_EMIT: return launch_extract_t<MODE_EMIT>(a, grid, STAGE_CAP, st);
+    case MODE_PART: return launch_extract_t<MODE_PART>(a, grid, STAGE_CAP, st);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -1266,6 +1494,56 @@ cudaError_t launch_select_range(const unsigned long long *keys, const uint32_t *
     note_launch();
     k_scatter_selected<<<grid_for(n, 256), 256, 0, st>>>(keys, counts, flags, pos, n, limit, out_keys, out_counts,
                                                          counters, counter_idx);
+    return cudaGetLastError();
+}
+
+template <typename K>
+static int persistent_grid(K kernel)
+{
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+    return sm_count() * per_sm;
+}
+
+cudaError_t launch_bloom_buckets(const unsigned long long *keys, const WorkItem *items, uint32_t n_items,
+                                 unsigned int *next_item, const BucketCfg *cfg, unsigned long long *bits,
+                                 unsigned long long *out, unsigned long long *low_cnt, unsigned long long *high_cnt,
+                                 uint32_t *hll_high, cudaStream_t st)
+{
+    if (!n_items) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(next_item, 0, 4, st);
+    if (e != cudaSuccess) return e;
+    note_launch();
+    k_bloom_buckets<<<std::min<int>(persistent_grid(k_bloom_buckets), n_items), 256, 0, st>>>(
+        keys, items, n_items, next_item, cfg, bits, out, low_cnt, high_cnt, hll_high);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_insert_buckets(const unsigned long long *keys, const WorkItem *items, uint32_t n_items,
+                                  unsigned int *next_item, const BucketCfg *cfg, Slot *arena, uint32_t max_probe,
+                                  unsigned long long *bucket_ovf, cudaStream_t st)
+{
+    if (!n_items) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(next_item, 0, 4, st);
+    if (e != cudaSuccess) return e;
+    note_launch();
+    k_insert_buckets<<<std::min<int>(persistent_grid(k_insert_buckets), n_items), 256, 0, st>>>(
+        keys, items, n_items, next_item, cfg, arena, max_probe, bucket_ovf);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_merge_buckets(const unsigned long long *keys, const WorkItem *items, uint32_t n_items,
+                                 unsigned int *next_item, const BucketCfg *cfg, Slot *arena, uint32_t max_probe,
+                                 uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
+                                 uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *counters, cudaStream_t st)
+{
+    if (!n_items) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(next_item, 0, 4, st);
+    if (e != cudaSuccess) return e;
+    note_launch();
+    k_merge_buckets<<<std::min<int>(persistent_grid(k_merge_buckets), n_items), 256, 0, st>>>(
+        keys, items, n_items, next_item, cfg, arena, max_probe, min_count, max_count, rec_keys, rec_counts, rec_cap,
+        counters);
     return cudaGetLastError();
 }
 

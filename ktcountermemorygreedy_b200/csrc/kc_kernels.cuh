@@ -85,7 +85,8 @@ struct ExtractArgs {
     unsigned long long *counters;   // C_COUNT words
     // scan mode
     unsigned long long *occ;        // occurrences per sample
-    uint32_t *hll;                  // HLL_M registers per sample
+    uint32_t *hll;                  // HLL_M registers per sample; NULL: no distinct estimate
+    int hll_local;                  // single sample: registers kept in shared memory per block
     int prepass;                    // also accumulate the pre-pass statistics
     const int32_t *chunk_lastnl;    // per 2 MiB chunk (global chunk index), last '\n' offset in chunk
     const uint64_t *seg_chunk0;     // first global chunk index of each file
@@ -99,12 +100,37 @@ struct ExtractArgs {
     const unsigned long long *bloom_cap;   // 256 capacities (blocks of two words)
     unsigned long long *bloom_bits;
     uint32_t *hll_high;             // HLL registers of the non-FIRST occurrences
-    // emit / bloom output list
+    // emit / bloom / part output list
     unsigned long long *list;
     unsigned long long list_cap;
+    // root-prefix buckets (single sample): SCAN counts, PART scatters
+    unsigned long long *bucket_hist;          // 256 counts (SCAN)
+    unsigned long long *bucket_cursor;        // 256 fill levels (PART)
+    const unsigned long long *bucket_base;    // 256 start offsets in `list` (PART)
 };
 
-enum ExtractMode : int { MODE_SCAN = 0, MODE_INSERT = 1, MODE_BLOOM = 2, MODE_EMIT = 3 };
+enum ExtractMode : int { MODE_SCAN = 0, MODE_INSERT = 1, MODE_BLOOM = 2, MODE_EMIT = 3, MODE_PART = 4 };
+
+constexpr uint32_t WORK_ITEM_KEYS = 2048;   // k-mers per work item (8 per thread)
+constexpr uint32_t BUCKET_HLL_BITS = 10;    // HyperLogLog registers per bucket = 2^10
+constexpr uint32_t BUCKET_HLL_M = 1u << BUCKET_HLL_BITS;
+constexpr uint32_t N_BUCKETS = 256;         // root prefix = top 8 bits of the k-mer word
+
+// A run of k-mers of one root-prefix bucket processed by one block of the
+// bucket-major kernels (work items are issued in bucket order, so the blocks
+// in flight touch one or two buckets' filters and tables, which stay in L2).
+struct WorkItem {
+    unsigned long long begin, end;   // range in the key array
+    uint32_t bucket;
+    uint32_t pad;
+};
+
+// Per-bucket state of the partitioned pipeline.
+struct BucketCfg {
+    unsigned long long key_base, key_len;    // bucket's range in the partitioned key array
+    unsigned long long bloom_off, bloom_cap; // its Bloom filter (words offset, blocks)
+    unsigned long long slot_base, slot_cap;  // its sub-table in the slot arena
+};
 
 size_t extract_smem_bytes();
 unsigned long long kernel_launches();          // launches issued by this process
@@ -161,6 +187,19 @@ cudaError_t launch_select_range(const unsigned long long *keys, const uint32_t *
                                 uint32_t hi, uint64_t limit, unsigned long long *out_keys, uint32_t *out_counts,
                                 uint32_t *flags, unsigned long long *pos, unsigned long long *tmp,
                                 unsigned long long *counters, int counter_idx, cudaStream_t st);
+
+// Bucket-major kernels of the partitioned pipeline; each resets *next_item.
+cudaError_t launch_bloom_buckets(const unsigned long long *keys, const WorkItem *items, uint32_t n_items,
+                                 unsigned int *next_item, const BucketCfg *cfg, unsigned long long *bits,
+                                 unsigned long long *out, unsigned long long *low_cnt, unsigned long long *high_cnt,
+                                 uint32_t *hll_high, cudaStream_t st);
+cudaError_t launch_insert_buckets(const unsigned long long *keys, const WorkItem *items, uint32_t n_items,
+                                  unsigned int *next_item, const BucketCfg *cfg, Slot *arena, uint32_t max_probe,
+                                  unsigned long long *bucket_ovf, cudaStream_t st);
+cudaError_t launch_merge_buckets(const unsigned long long *keys, const WorkItem *items, uint32_t n_items,
+                                 unsigned int *next_item, const BucketCfg *cfg, Slot *arena, uint32_t max_probe,
+                                 uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
+                                 uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *counters, cudaStream_t st);
 
 // Batch of hash evaluations for the parity tests: out[5*i..5*i+4] =
 // xxh3_128.lo, xxh3_128.hi, xxh3_64, rapidhash, komihash (all of keys[i]).
