@@ -128,8 +128,10 @@ def algorithmic_bytes(phase: str, r):
     S FASTQ bytes, O occurrences, h/l the non-FIRST/FIRST list lengths,
     cap table slots, U distinct k-mers."""
     S, O = r.input_bytes, r.occurrences
-    if phase == "count_pass":          # FASTQ + Bloom words read (16 B) + list write (8 B)
-        return S + 24 * O if r.low_len + r.high_len else S + 16 * O
+    if phase == "count_pass":          # Bloom mode: FASTQ + bucketed k-mer write; plain: FASTQ + table update
+        return S + 8 * O if r.low_len + r.high_len else S + 16 * O
+    if phase == "bloom":               # bucketed k-mers read + list write (16 B) + two filter words (16 B)
+        return 32 * O
     if phase == "insert_high":         # list read (8 B) + slot key read and count update (16 B)
         return 24 * r.high_len
     if phase == "merge_low":
@@ -314,6 +316,9 @@ def run_ours(args):
     if args.e2e_steps > 0:
         walls, occ_e = [], 0
         r = None
+        # one untimed host-buffer job: the worker's device workspace and the
+        # pinned result pool grow to this job shape once
+        counter.count([fq], keep_records=True, copy=False, **JOB)
         for _ in range(args.e2e_steps):
             t0 = time.perf_counter()
             r = counter.count([fq], keep_records=True, copy=False, **JOB)
@@ -326,9 +331,10 @@ def run_ours(args):
 
     # roofline of the dominant single-kernel stage
     phases = kc.PHASES
-    mean_ms = [statistics.mean(r.phase_ms[i] for r in results) for i in range(8)]
-    single = [i for i in range(8) if results[0].phase_launches[i] == 1 and mean_ms[i] > 0]
-    dom = max(single, key=lambda i: mean_ms[i]) if single else max(range(8), key=lambda i: mean_ms[i])
+    ns = len(phases)
+    mean_ms = [statistics.mean(r.phase_ms[i] for r in results) for i in range(ns)]
+    single = [i for i in range(ns) if results[0].phase_launches[i] == 1 and mean_ms[i] > 0]
+    dom = max(single, key=lambda i: mean_ms[i]) if single else max(range(ns), key=lambda i: mean_ms[i])
     r0 = results[-1]
     alg = algorithmic_bytes(phases[dom], r0)
     achieved = alg / (mean_ms[dom] / max(1, r0.phase_launches[dom]) / 1000.0) / 1e9
@@ -338,7 +344,7 @@ def run_ours(args):
             "algorithmic_bytes": alg}
     stages = {phases[i]: {"ms": mean_ms[i], "launches": int(r0.phase_launches[i]),
                           "alg_GBps": (algorithmic_bytes(phases[i], r0) / (mean_ms[i] / 1000.0) / 1e9)
-                          if mean_ms[i] > 0 else None} for i in range(8) if mean_ms[i] > 0}
+                          if mean_ms[i] > 0 else None} for i in range(ns) if mean_ms[i] > 0}
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_baseline:

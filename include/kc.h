@@ -52,6 +52,8 @@ extern "C" {
 #define KC_ERR_NO_DEVICE 8   /* no usable CUDA device */
 #define KC_ERR_FAILED 9      /* the job failed; kc_last_error after kc_wait says why */
 
+#define KC_STAGES 12         /* entries of kc_result_t.phase_ms */
+
 typedef struct kc_handle kc_handle;
 typedef struct kc_input kc_input;
 typedef uint64_t kc_job_id;
@@ -110,11 +112,13 @@ typedef struct {
     double queue_ms;              /* submission -> start */
     double run_ms;                /* start -> end (host clock) */
     /* device time per stage (CUDA events on the job's stream):
-     * [0] newline census + tile line numbers, [1] SCAN pass, [2] INSERT or
-     * BLOOM pass, [3] insert of the non-FIRST list, [4] merge of the FIRST
-     * list, [5] compaction + histogram, [6] radix sort, [7] queries */
-    double phase_ms[8];
-    uint64_t phase_launches[8];   /* kernel launches per stage */
+     * [0] newline census + tile line numbers, [1] SCAN pass, [2] INSERT pass
+     * (plain) or scatter into the root-prefix buckets (Bloom), [3] insert of
+     * the non-FIRST k-mers, [4] merge of the FIRST k-mers, [5] compaction +
+     * histogram, [6] radix sort, [7] queries, [8] Bloom classification,
+     * [9..11] unused */
+    double phase_ms[KC_STAGES];
+    uint64_t phase_launches[KC_STAGES];   /* kernel launches per stage */
     uint64_t low_len;             /* Bloom mode: FIRST occurrences */
     uint64_t high_len;            /* Bloom mode: other occurrences */
     uint64_t input_bytes;         /* FASTQ bytes of the job */

@@ -73,11 +73,13 @@ class kc_result_t(C.Structure):
                 ("n_le2", C.c_uint64), ("le2_keys", C.POINTER(C.c_uint64)), ("le2_counts", C.POINTER(C.c_uint32)),
                 ("occurrences", C.c_uint64), ("distinct", C.c_uint64), ("low_only", C.c_uint64),
                 ("table_capacity", C.c_uint64), ("device_ms", C.c_double), ("queue_ms", C.c_double),
-                ("run_ms", C.c_double), ("phase_ms", C.c_double * 8), ("phase_launches", C.c_uint64 * 8),
+                ("run_ms", C.c_double), ("phase_ms", C.c_double * 12), ("phase_launches", C.c_uint64 * 12),
                 ("low_len", C.c_uint64), ("high_len", C.c_uint64), ("input_bytes", C.c_uint64),
                 ("n_records_total", C.c_uint64)]
 
-PHASES = ["census", "scan", "count_pass", "insert_high", "merge_low", "compact", "sort", "queries"]
+# stage names of kc_result_t.phase_ms
+PHASES = ["census", "scan", "count_pass", "insert_high", "merge_low", "compact", "sort", "queries", "bloom",
+          "stage9", "stage10", "stage11"]
 
 
 # (name, restype, argtypes) of every symbol include/kc.h declares

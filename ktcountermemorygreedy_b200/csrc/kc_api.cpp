@@ -99,8 +99,8 @@ struct Job {
     uint64_t occurrences = 0, distinct = 0, low_only = 0, table_cap = 0;
     uint64_t low_len = 0, high_len = 0, input_bytes = 0, n_records_total = 0;
     double device_ms = 0;
-    double phase_ms[8] = {0};
-    uint64_t phase_launches[8] = {0};
+    double phase_ms[KC_STAGES] = {0};
+    uint64_t phase_launches[KC_STAGES] = {0};
 };
 
 // Device time and kernel launches per pipeline stage, from CUDA events on
@@ -116,7 +116,7 @@ struct PhaseClock {
     int cur = -1;
     cudaEvent_t cur_a = nullptr;
     unsigned long long l0 = 0;
-    uint64_t launches[8] = {0};
+    uint64_t launches[KC_STAGES] = {0};
     explicit PhaseClock(cudaStream_t s) : st(s) {}
     void begin(int phase)
     {
@@ -146,7 +146,7 @@ struct PhaseClock {
                 fprintf(stderr, "[kc trace] stage %d: %.3f .. %.3f ms\n", s.phase, t0, t0 + t);
             }
         }
-        for (int i = 0; i < 8; ++i) ln[i] += launches[i];
+        for (int i = 0; i < KC_STAGES; ++i) ln[i] += launches[i];
     }
     ~PhaseClock()
     {
@@ -215,7 +215,10 @@ Counters read_counters(const unsigned long long *d, cudaStream_t st)
     return c;
 }
 
-void run_job(Job &job, cudaStream_t st, Workspace &ws)
+// A root-prefix bucket outgrew the region estimated from the sampled census.
+struct CensusOverflow {};
+
+void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
 {
     const kc_job &P = job.p;
     const uint32_t k = P.k;
@@ -294,6 +297,9 @@ void run_job(Job &job, cudaStream_t st, Workspace &ws)
         bucket_hist = ds.n<unsigned long long>(N_BUCKETS);
         CK(cudaMemsetAsync(bucket_hist, 0, N_BUCKETS * 8, st));
         a.bucket_hist = bucket_hist;
+        // the bucket census reads every 8th tile of large inputs; buckets get
+        // regions with headroom and an outgrown region triggers an exact redo
+        a.bucket_sample_mask = (exact_census || T < 512) ? 0 : 7;
         int32_t *chunk_lastnl = ds.n<int32_t>(std::max<uint64_t>(n_chunks, 1));
         uint64_t *d_chunk0 = ds.n<uint64_t>(seg_chunk0.size());
         prefix_hist = ds.n<uint32_t>(256);
@@ -371,14 +377,20 @@ void run_job(Job &job, cudaStream_t st, Workspace &ws)
         CK(cudaMemcpyAsync(bh.data(), bucket_hist, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         std::vector<BucketCfg> cfg(N_BUCKETS);
+        std::vector<unsigned long long> region(N_BUCKETS);
+        unsigned long long sampled = 0;
+        for (uint32_t b = 0; b < N_BUCKETS; ++b) sampled += bh[b];
+        const bool exact = a.bucket_sample_mask == 0;
+        if (exact && sampled != O) throw KcError{KC_ERR_DEVICE, "bucket census does not add up to the occurrences"};
+        if (!exact && sampled < 65536 && O > sampled) throw CensusOverflow{};   // too thin a sample
         unsigned long long off = 0;
         for (uint32_t b = 0; b < N_BUCKETS; ++b) {
+            region[b] = exact ? bh[b]
+                              : (unsigned long long)std::ceil((double)O * (double)bh[b] / (double)sampled * 1.15) + 8192;
             cfg[b].key_base = off;
-            cfg[b].key_len = bh[b];
-            off += bh[b];
+            off += region[b];
         }
-        if (off != O) throw KcError{KC_ERR_DEVICE, "bucket census does not add up to the occurrences"};
-        const unsigned long long ocap = std::max<unsigned long long>(O, 1);
+        const unsigned long long ocap = std::max<unsigned long long>(off, 1);
         // reference sizing (src/main.cpp:41-153) from the pre-pass statistics
         uint8_t avg_q = qh[1] ? (uint8_t)(qh[0] / qh[1]) : 0;
         BloomPlan bp = bloom_plan(ph.data(), avg_q, in->total_bytes, P.memory_gb, k);
@@ -395,18 +407,20 @@ void run_job(Job &job, cudaStream_t st, Workspace &ws)
         unsigned long long *keys = ds.n<unsigned long long>(ocap);
         BucketCfg *d_cfg_b = ds.n<BucketCfg>(N_BUCKETS);
         unsigned long long *cursor = ds.n<unsigned long long>(N_BUCKETS);
-        unsigned long long *bbase = ds.n<unsigned long long>(N_BUCKETS);
+        unsigned long long *bbase = ds.n<unsigned long long>(2 * N_BUCKETS);
         unsigned long long *lh_cnt = ds.n<unsigned long long>(2 * N_BUCKETS);
         uint32_t *hll_high = ds.n<uint32_t>((size_t)N_BUCKETS * BUCKET_HLL_M);
         unsigned int *next_item = ds.n<unsigned int>(1);
-        std::vector<unsigned long long> bb(N_BUCKETS);
-        for (uint32_t b = 0; b < N_BUCKETS; ++b) bb[b] = cfg[b].key_base;
+        std::vector<unsigned long long> bb(2 * N_BUCKETS);
+        for (uint32_t b = 0; b < N_BUCKETS; ++b) {
+            bb[b] = cfg[b].key_base;
+            bb[N_BUCKETS + b] = cfg[b].key_base + region[b];
+        }
         CK(cudaMemsetAsync(cursor, 0, N_BUCKETS * 8, st));
-        CK(cudaMemcpyAsync(bbase, bb.data(), N_BUCKETS * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(bbase, bb.data(), 2 * N_BUCKETS * 8, cudaMemcpyHostToDevice, st));
         CK(cudaMemsetAsync(bits, 0, words * 8, st));
         CK(cudaMemsetAsync(lh_cnt, 0, 2 * N_BUCKETS * 8, st));
         CK(cudaMemsetAsync(hll_high, 0, (size_t)N_BUCKETS * BUCKET_HLL_M * 4, st));
-        CK(cudaMemcpyAsync(d_cfg_b, cfg.data(), N_BUCKETS * sizeof(BucketCfg), cudaMemcpyHostToDevice, st));
         a.hll = nullptr;
         a.prepass = 0;
         a.bucket_hist = nullptr;
@@ -414,8 +428,22 @@ void run_job(Job &job, cudaStream_t st, Workspace &ws)
         a.list_cap = ocap;
         a.bucket_cursor = cursor;
         a.bucket_base = bbase;
+        a.bucket_end = bbase + N_BUCKETS;
         clk.begin(2);
         CK(launch_extract(MODE_PART, a, 0, st));
+        clk.end();
+        std::vector<unsigned long long> fill(N_BUCKETS);
+        CK(cudaMemcpyAsync(fill.data(), cursor, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        unsigned long long filled = 0;
+        for (uint32_t b = 0; b < N_BUCKETS; ++b) {
+            if (fill[b] > region[b]) throw CensusOverflow{};
+            cfg[b].key_len = fill[b];
+            filled += fill[b];
+        }
+        if (filled != O) throw KcError{KC_ERR_DEVICE, "partition does not add up to the occurrences"};
+        CK(cudaMemcpyAsync(d_cfg_b, cfg.data(), N_BUCKETS * sizeof(BucketCfg), cudaMemcpyHostToDevice, st));
+        clk.begin(8);
         std::vector<WorkItem> items;
         auto add_items = [&](uint32_t b, unsigned long long begin, unsigned long long end) {
             for (unsigned long long s = begin; s < end; s += WORK_ITEM_KEYS)
@@ -696,6 +724,19 @@ uint64_t reserve_for(const kc_job &p, uint64_t resident_bytes)
     uint64_t s = p.input ? resident_bytes : input_bytes(p);
     // input + per-tile tables + table/records/sort sized for distinct <= s/2
     return (p.input ? 0 : s) + s / 256 + 24 * s + (64ULL << 20);
+}
+
+void run_job(Job &job, cudaStream_t st, Workspace &ws)
+{
+    try {
+        run_job_once(job, st, ws, false);
+    } catch (const CensusOverflow &) {
+        // the sampled census missed a skewed bucket: count every tile instead
+        CK(cudaStreamSynchronize(st));
+        ws.end_job();
+        ws.begin_job();
+        run_job_once(job, st, ws, true);
+    }
 }
 
 // Batched jobs: every sample's files in one device buffer, one SCAN and one
@@ -1147,7 +1188,7 @@ int kc_result(kc_handle *h, kc_job_id id, kc_result_t *out)
     out->device_ms = j.device_ms;
     out->queue_ms = j.t_start - j.t_submit;
     out->run_ms = j.t_end - j.t_start;
-    for (int i = 0; i < 8; ++i) {
+    for (int i = 0; i < KC_STAGES; ++i) {
         out->phase_ms[i] = j.phase_ms[i];
         out->phase_launches[i] = j.phase_launches[i];
     }

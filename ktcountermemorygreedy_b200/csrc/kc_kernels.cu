@@ -161,15 +161,23 @@ __device__ __forceinline__ KParams kparams(uint32_t k)
 // bit 64-2k+2i (the reference's kmer<1> layout); the reverse complement is the
 // 2-bit-group reversal with every code complemented.  The canonical word is
 // the smaller of the two, as GetKmer::canonicalize.
-__device__ __forceinline__ unsigned long long window_key(uint64_t prev, uint64_t cur, uint32_t j, const KParams &kp)
+// The reverse complement comes from the per-segment words rprev/rcur =
+// pair_reverse(~codes), computed once per segment: in the 128-bit value
+// (rprev:rcur) span position q sits at 2-bit group 63 - q, so the
+// reverse-complement word of the window starting at s is that value shifted
+// right by 64 - 2s (equal to pair_reverse(x) ^ topmask for the window x).
+__device__ __forceinline__ unsigned long long window_key_rc(uint64_t prev, uint64_t cur, uint64_t rprev,
+                                                            uint64_t rcur, uint32_t j, const KParams &kp)
 {
-    int s = 33 + (int)j - (int)kp.k;   // window start in the 64-position span, 1..63
-    uint64_t x;
+    const int s = 33 + (int)j - (int)kp.k;
+    uint64_t x, rc;
     if (s >= 32) x = cur >> (2 * (s - 32));
     else x = (prev >> (2 * s)) | (cur << (64 - 2 * s));
-    x &= kp.kmask;
-    uint64_t fwd = kp.fwd_shift >= 64 ? 0 : (x << kp.fwd_shift);
-    uint64_t rc = pair_reverse(x) ^ kp.topmask;
+    if (s == 32) rc = rcur;
+    else if (s < 32) rc = (rcur >> (64 - 2 * s)) | (rprev << (2 * s));
+    else rc = rcur << (2 * s - 64);
+    const uint64_t fwd = (x & kp.kmask) << (kp.fwd_shift & 63);
+    rc &= kp.topmask;
     return fwd < rc ? fwd : rc;
 }
 
@@ -297,7 +305,8 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t *sbuf[2] = {smem, smem + BUF_BYTES};
     uint64_t *s_codes = reinterpret_cast<uint64_t *>(smem + 2 * BUF_BYTES);   // 257 used
-    uint32_t *s_good = reinterpret_cast<uint32_t *>(s_codes + 264);           // 257 used
+    uint64_t *s_rcodes = s_codes + 264;                                       // 257 used
+    uint32_t *s_good = reinterpret_cast<uint32_t *>(s_rcodes + 264);          // 257 used
     unsigned long long *s_stage = reinterpret_cast<unsigned long long *>(s_good + 264);
     uint32_t *s_hll = reinterpret_cast<uint32_t *>(s_good + 264);   // SCAN mode: registers of sample 0
     const bool hll_local = MODE == MODE_SCAN && a.hll && a.hll_local;
@@ -374,16 +383,19 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
         const uint32_t excl_nl = block_excl_scan(__popc(nl), s_warp, tot_nl);
         const uint64_t lstart = line0 + excl_nl;
         s_codes[tid + 1] = codes;
+        s_rcodes[tid + 1] = pair_reverse(~codes);
         s_good[tid + 1] = valid & line_mask(lstart, nl, 1);
         if (tid == 0) {
             if (first) {
                 s_codes[0] = 0;
+                s_rcodes[0] = ~0ULL;
                 s_good[0] = 0;
             } else {
                 uint64_t c0;
                 uint32_t v0, n0;
                 classify32(tb, c0, v0, n0);
                 s_codes[0] = c0;
+                s_rcodes[0] = pair_reverse(~c0);
                 s_good[0] = v0 & line_mask(line0 - __popc(n0), n0, 1);
             }
         }
@@ -416,6 +428,7 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
 
         // windows of k valid bases ending in this thread's segment
         const uint64_t prev = s_codes[tid], cur = s_codes[tid + 1];
+        const uint64_t rprev = s_rcodes[tid], rcur = s_rcodes[tid + 1];
         const uint64_t g = (uint64_t)s_good[tid] | ((uint64_t)s_good[tid + 1] << 32);
         uint32_t ends = run_ends(g, kp.k);
 
@@ -425,17 +438,19 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
                 uint64_t lim = sg.sample_end - seg_pos;
                 sample_ok = lim >= 32 ? FULL : ((1u << lim) - 1u);
             }
-            // keys are needed for the HyperLogLog, the bucket histogram and
-            // the pre-pass sample; otherwise only the windows are counted
-            uint32_t e = (a.hll || a.bucket_hist) ? ends : (ends & sample_ok);
+            // keys are needed for the HyperLogLog, the bucket census (every
+            // tile, or a 1-in-2^n sample of the tiles) and the pre-pass
+            // sample; otherwise only the windows are counted
+            const bool census = a.bucket_hist && (t & a.bucket_sample_mask) == 0;
+            uint32_t e = (a.hll || census) ? ends : (ends & sample_ok);
             uint32_t hll_base = sg.sample * HLL_M;
             while (e) {
                 uint32_t j = __ffs(e) - 1;
                 e &= e - 1;
-                unsigned long long key = window_key(prev, cur, j, kp);
+                unsigned long long key = window_key_rc(prev, cur, rprev, rcur, j, kp);
                 if (hll_local) hll_add_shared(s_hll, key);
                 else if (a.hll) hll_add(a.hll + hll_base, key);
-                if (a.bucket_hist) atomicAdd(&s_bhist[key >> 56], 1u);
+                if (census) atomicAdd(&s_bhist[key >> 56], 1u);
                 if ((sample_ok >> j) & 1u) atomicAdd(&s_hist[key >> 56], 1u);
             }
             unsigned n = __reduce_add_sync(FULL, (unsigned)__popc(ends));
@@ -448,7 +463,8 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
                 while (e) {
                     uint32_t j = __ffs(e) - 1;
                     e &= e - 1;
-                    if (idx >= base && idx < base + stage_cap) s_stage[idx - base] = window_key(prev, cur, j, kp);
+                    if (idx >= base && idx < base + stage_cap)
+                        s_stage[idx - base] = window_key_rc(prev, cur, rprev, rcur, j, kp);
                     ++idx;
                 }
                 __syncthreads();
@@ -476,9 +492,11 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
                     __syncthreads();
                     for (uint32_t i = tid; i < nr; i += EXT_THREADS) {
                         const unsigned long long key = s_stage[i];
-                        const unsigned long long pos = s_bpos[(uint32_t)(key >> 56)] + s_rank[i];
-                        if (pos < a.list_cap) a.list[pos] = key;
-                        else atomicOr(flags, ERR_LIST_FULL);
+                        const uint32_t b = (uint32_t)(key >> 56);
+                        const unsigned long long pos = s_bpos[b] + s_rank[i];
+                        // a bucket that outgrows its estimated region is
+                        // reported (its cursor passes the end) and redone
+                        if (pos < a.bucket_end[b] && pos < a.list_cap) a.list[pos] = key;
                     }
                 } else if (MODE == MODE_EMIT) {
                     if (tid == 0) s_bcast[0] = atomicAdd(&a.counters[C_EMIT_LEN], (unsigned long long)nr);
@@ -1220,7 +1238,7 @@ unsigned long long thread_kernel_launches() { return t_launches; }
 
 size_t extract_smem_bytes_for(int mode, uint32_t stage_cap)
 {
-    size_t b = 2 * BUF_BYTES + 264 * 8 + 264 * 4;
+    size_t b = 2 * BUF_BYTES + 264 * 8 * 2 + 264 * 4;
     if (mode != MODE_SCAN) b += (size_t)stage_cap * 8;
     else b += HLL_M * 4;
     if (mode == MODE_PART) b += (size_t)stage_cap * 2;

@@ -105,8 +105,10 @@ struct ExtractArgs {
     unsigned long long list_cap;
     // root-prefix buckets (single sample): SCAN counts, PART scatters
     unsigned long long *bucket_hist;          // 256 counts (SCAN)
+    uint64_t bucket_sample_mask;              // SCAN counts tiles t with (t & mask) == 0
     unsigned long long *bucket_cursor;        // 256 fill levels (PART)
     const unsigned long long *bucket_base;    // 256 start offsets in `list` (PART)
+    const unsigned long long *bucket_end;     // 256 end offsets in `list` (PART)
 };
 
 enum ExtractMode : int { MODE_SCAN = 0, MODE_INSERT = 1, MODE_BLOOM = 2, MODE_EMIT = 3, MODE_PART = 4 };
