@@ -311,7 +311,8 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
     uint32_t *s_hll = reinterpret_cast<uint32_t *>(s_good + 264);   // SCAN mode: registers of sample 0
     const bool hll_local = MODE == MODE_SCAN && a.hll && a.hll_local;
 
-    // PART mode: rank of each staged k-mer inside its bucket's share of the tile
+    // staged modes: (segment, position) of each window, then (PART mode) the
+    // rank of each staged k-mer inside its bucket's share of the tile
     uint16_t *s_rank = reinterpret_cast<uint16_t *>(s_stage + stage_cap);
 
     __shared__ __align__(8) uint64_t mbar[2];
@@ -459,16 +460,25 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
             uint32_t tot;
             const uint32_t off = block_excl_scan(__popc(ends), s_warp, tot);
             for (uint32_t base = 0; base < tot; base += stage_cap) {
+                // list the windows of this round as (segment, end position),
+                // then form the k-mers with every thread busy: segments of
+                // header and quality lines have no windows, so forming keys
+                // per owning thread would leave most lanes idle
                 uint32_t e = ends, idx = off;
                 while (e) {
                     uint32_t j = __ffs(e) - 1;
                     e &= e - 1;
-                    if (idx >= base && idx < base + stage_cap)
-                        s_stage[idx - base] = window_key_rc(prev, cur, rprev, rcur, j, kp);
+                    if (idx >= base && idx < base + stage_cap) s_rank[idx - base] = (uint16_t)((tid << 5) | j);
                     ++idx;
                 }
                 __syncthreads();
                 const uint32_t nr = min(stage_cap, tot - base);
+                for (uint32_t i = tid; i < nr; i += EXT_THREADS) {
+                    const uint32_t item = s_rank[i], sgm = item >> 5;
+                    s_stage[i] = window_key_rc(s_codes[sgm], s_codes[sgm + 1], s_rcodes[sgm], s_rcodes[sgm + 1],
+                                               item & 31u, kp);
+                }
+                __syncthreads();
                 if (MODE == MODE_INSERT) {
                     const TableRef tr = a.tables[sg.sample];
                     for (uint32_t r0 = 0; r0 < nr; r0 += EXT_THREADS) {
@@ -1029,11 +1039,16 @@ __device__ __forceinline__ bool next_work(unsigned int *next_item, uint32_t n_it
     return it < n_items;
 }
 
-__device__ __forceinline__ void hll_add_bits(uint32_t *regs, unsigned long long key, uint32_t bits)
+// HyperLogLog of a 1-in-8 hash sample of the keys (the estimate is scaled by
+// 8 on the host): an eighth of the register traffic for the same accuracy on
+// the large sets the tables are sized for.
+__device__ __forceinline__ void hll_add_sampled(uint32_t *regs, unsigned long long key, uint32_t bits)
 {
     uint64_t h = slot_hash(key ^ 0x5bd1e9955bd1e995ULL);
-    uint32_t r = (uint32_t)(h >> (64 - bits));
-    uint32_t rank = __clzll((h << bits) | (1ULL << (bits - 1))) + 1;
+    if (h & 7) return;
+    h >>= 3;
+    uint32_t r = (uint32_t)(h >> (61 - bits));
+    uint32_t rank = __clzll((h << (bits + 3)) | (1ULL << (bits + 2))) + 1;
     if (rank > *(volatile uint32_t *)&regs[r]) atomicMax(&regs[r], rank);
 }
 
@@ -1042,7 +1057,7 @@ __device__ __forceinline__ void hll_add_bits(uint32_t *regs, unsigned long long 
 // bucket's range in `out`, the others to its back.  Only FIRST versus not
 // FIRST matters downstream, so both filter words are read with one 16-byte
 // load and the first word is set without reading its old value.
-__global__ void __launch_bounds__(256) k_bloom_buckets(const unsigned long long *keys, const WorkItem *items,
+__global__ void __launch_bounds__(256, 4) k_bloom_buckets(const unsigned long long *keys, const WorkItem *items,
                                                        uint32_t n_items, unsigned int *next_item,
                                                        const BucketCfg *cfg, unsigned long long *bits,
                                                        unsigned long long *out, unsigned long long *low_cnt,
@@ -1058,6 +1073,12 @@ __global__ void __launch_bounds__(256) k_bloom_buckets(const unsigned long long 
         const uint64_t n = w.end - w.begin;
         unsigned long long k[ITEM_PER_THREAD];
         uint32_t firsts = 0, highs = 0;
+        // the k-mer stream is read once: keep it from evicting filter lines
+#pragma unroll
+        for (uint32_t r = 0; r < ITEM_PER_THREAD; ++r) {
+            const uint64_t i = (uint64_t)r * 256 + tid;
+            k[r] = i < n ? __ldcs(&keys[w.begin + i]) : EMPTY_KEY;
+        }
 #pragma unroll
         for (uint32_t g = 0; g < ITEM_PER_THREAD; g += 4) {
             unsigned long long m[4];
@@ -1066,7 +1087,6 @@ __global__ void __launch_bounds__(256) k_bloom_buckets(const unsigned long long 
 #pragma unroll
             for (uint32_t u = 0; u < 4; ++u) {
                 const uint64_t i = (uint64_t)(g + u) * 256 + tid;
-                k[g + u] = i < n ? keys[w.begin + i] : EMPTY_KEY;
                 uint64_t block = 0, mask = 0;
                 if (i < n) bloom_probe(k[g + u], bc.bloom_cap, block, mask);
                 m[u] = mask;
@@ -1092,7 +1112,7 @@ __global__ void __launch_bounds__(256) k_bloom_buckets(const unsigned long long 
                 if (first) firsts |= 1u << (g + u);
                 else {
                     highs |= 1u << (g + u);
-                    hll_add_bits(hll_high + (size_t)w.bucket * BUCKET_HLL_M, k[g + u], BUCKET_HLL_BITS);
+                    hll_add_sampled(hll_high + (size_t)w.bucket * BUCKET_HLL_M, k[g + u], BUCKET_HLL_BITS);
                 }
             }
         }
@@ -1108,8 +1128,8 @@ __global__ void __launch_bounds__(256) k_bloom_buckets(const unsigned long long 
         unsigned long long hp = bc.key_base + bc.key_len - 1 - (s_hb + oh);
 #pragma unroll
         for (uint32_t r = 0; r < ITEM_PER_THREAD; ++r) {
-            if ((firsts >> r) & 1u) out[lp++] = k[r];
-            else if ((highs >> r) & 1u) out[hp--] = k[r];
+            if ((firsts >> r) & 1u) __stcs(&out[lp++], k[r]);
+            else if ((highs >> r) & 1u) __stcs(&out[hp--], k[r]);
         }
         __syncthreads();
     }
@@ -1132,7 +1152,7 @@ __global__ void __launch_bounds__(256) k_insert_buckets(const unsigned long long
 #pragma unroll
         for (uint32_t r = 0; r < ITEM_PER_THREAD; ++r) {
             const uint64_t i = (uint64_t)r * 256 + tid;
-            k[r] = i < n ? keys[w.begin + i] : EMPTY_KEY;
+            k[r] = i < n ? __ldcs(&keys[w.begin + i]) : EMPTY_KEY;
         }
 #pragma unroll
         for (uint32_t r = 0; r < ITEM_PER_THREAD; ++r)
@@ -1161,7 +1181,7 @@ __global__ void __launch_bounds__(256) k_merge_buckets(const unsigned long long 
 #pragma unroll
         for (uint32_t r = 0; r < ITEM_PER_THREAD; ++r) {
             const uint64_t i = (uint64_t)r * 256 + tid;
-            k[r] = i < n ? keys[w.begin + i] : EMPTY_KEY;
+            k[r] = i < n ? __ldcs(&keys[w.begin + i]) : EMPTY_KEY;
         }
         uint32_t misses = 0;
 #pragma unroll
@@ -1241,7 +1261,7 @@ size_t extract_smem_bytes_for(int mode, uint32_t stage_cap)
     size_t b = 2 * BUF_BYTES + 264 * 8 * 2 + 264 * 4;
     if (mode != MODE_SCAN) b += (size_t)stage_cap * 8;
     else b += HLL_M * 4;
-    if (mode == MODE_PART) b += (size_t)stage_cap * 2;
+    if (mode != MODE_SCAN) b += (size_t)stage_cap * 2;
     return b;
 }
 

@@ -142,6 +142,37 @@ def test_plain_job_full_size(counter):
     assert r.hist.tolist() == O.histogram(want_c, 1, 10000).tolist()
 
 
+def test_bloom_job_sampled_census(counter):
+    """Inputs of 512+ tiles size the root-prefix buckets from a 1-in-8 tile
+    sample of the census; the result stays exact."""
+    import ktcountermemorygreedy_b200.synth as S
+    g = S.genome(21, 2_000_000)
+    fq = S.reads(g, 21, 30_000, (150, 150), 0.01, 0.0).tobytes()
+    assert len(fq) > 512 * 8192
+    for mc in (1, 2):
+        want_k, want_c = O.exact_records([fq], 31, U32, min_count=mc)
+        r = counter.count([fq], k=31, count_max=U32, bloom=True, memory_gb=2, min_count=mc)
+        assert np.array_equal(r.keys, want_k) and np.array_equal(r.counts, want_c)
+
+
+def test_bloom_job_census_overflow_falls_back_to_exact(counter):
+    """Every 8th tile random, the others one homopolymer: the sampled census
+    underestimates the homopolymer's bucket, its region overflows and the job
+    is redone with an exact census -- same exact result."""
+    import random
+    rnd = random.Random(5)
+    recs = []
+    for i in range(600):
+        seq = "".join(rnd.choice("ACGT") for _ in range(4000)) if i % 8 == 0 else "A" * 4000
+        header = "@" + "h" * 186 + "\n"
+        recs.append(header + seq + "\n+\n" + "I" * 4000 + "\n")
+    fq = "".join(recs).encode()
+    assert all(len(r) == 8192 for r in recs)
+    want_k, want_c = O.exact_records([fq], 21, U32)
+    r = counter.count([fq], k=21, count_max=U32, bloom=True, memory_gb=1)
+    assert np.array_equal(r.keys, want_k) and np.array_equal(r.counts, want_c)
+
+
 def test_queries(counter, kc):
     files = _case_files("repeat")
     k = 21
