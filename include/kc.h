@@ -174,6 +174,24 @@ int kc_hash_kmers(const uint64_t *keys, uint64_t n, uint64_t *out);
  * keys (sort/ExportRecordRadixSort.h:225-269, tool/dump_tool.cpp:373-454). */
 int kc_sort_records(uint64_t *keys, uint32_t *counts, uint64_t n, uint32_t bits);
 
+/* kc_sort_records for callers that cannot allocate device memory.  No
+ * counterpart in the reference.  Some callers may not call cudaMalloc where
+ * they need sorted records (a fixed, pre-accounted device-memory budget owned
+ * by another allocator, or a latency-critical path where an allocation can
+ * stall or synchronize the device).  This call sorts the caller's DEVICE
+ * arrays d_keys/d_counts (n records, low `bits` bits of the keys, stable) in
+ * place on `stream` (a cudaStream_t, NULL for the default stream) and returns
+ * when the sort is done.  It allocates nothing: its working memory is a fixed
+ * 13 MiB device array inside libkc.so that every GPU loading the library holds
+ * until the process exits, so n is limited to KC_SORT_NOALLOC_MAX records
+ * (larger n is rejected with KC_ERR_INVALID).  The first call on a device
+ * looks up that array's device address (cudaGetSymbolAddress) with the device
+ * current; make that first call before capturing a stream into a graph.  All
+ * calls share the one array: calls that overlap on the GPU (another host
+ * thread, another stream) race and must be serialized by the caller. */
+#define KC_SORT_NOALLOC_MAX (1u << 20)
+int kc_sort_records_noalloc(uint64_t *d_keys, uint32_t *d_counts, uint64_t n, uint32_t bits, void *stream);
+
 /* Pre-pass statistics and Bloom sizing of a job (src/main.cpp:262-335 with
  * get_MAX_BLOOM_FILTER_CAPACITY :41 and calculate_bloom_filter_capacity :111):
  * raw root-prefix counts over the sample, average quality, capacities. */

@@ -105,6 +105,7 @@ SIGNATURES = [
     ("kc_bloom_plan", C.c_int, [C.POINTER(kc_buffer), C.c_uint32, C.c_uint32, C.c_uint64, C.c_void_p,
                                 C.POINTER(C.c_uint32), C.c_void_p, C.POINTER(C.c_uint64)]),
     ("kc_kernel_launches", C.c_uint64, []),
+    ("kc_sort_records_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]),
     ("kc_plan_bloom", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p,
                                 C.POINTER(C.c_uint64)]),
     ("kc_merge_records", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_uint32,

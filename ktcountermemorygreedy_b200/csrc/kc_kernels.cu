@@ -1486,6 +1486,65 @@ cudaError_t launch_radix_sort_segmented(unsigned long long *keys, uint32_t *vals
     return cudaGetLastError();
 }
 
+// Tile descriptors of a one-segment sort, written by the device.
+__global__ void k_single_segment_tiles(SortTile *tiles, uint64_t n, uint64_t n_tiles)
+{
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n_tiles; t += (uint64_t)gridDim.x * blockDim.x) {
+        SortTile d;
+        d.begin = t * RS_TILE;
+        d.end = n < d.begin + RS_TILE ? n : d.begin + RS_TILE;
+        d.cbase = t;
+        d.stride = n_tiles;
+        d.adjust = 0;
+        tiles[t] = d;
+    }
+}
+
+cudaError_t launch_radix_sort_in_scratch(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits,
+                                         void *tmp, cudaStream_t st)
+{
+    if (n <= 1 || bits == 0) return cudaSuccess;
+    const uint64_t n_tiles = (n + RS_TILE - 1) / RS_TILE;
+    const uint64_t nc = 256 * n_tiles;
+    uint8_t *p = static_cast<uint8_t *>(tmp);
+    unsigned long long *k2 = reinterpret_cast<unsigned long long *>(p);
+    p += align256(n * 8);
+    uint32_t *v2 = reinterpret_cast<uint32_t *>(p);
+    p += align256(n * 4);
+    uint32_t *counts = reinterpret_cast<uint32_t *>(p);
+    p += align256(nc * 4);
+    unsigned long long *offs = reinterpret_cast<unsigned long long *>(p);
+    p += align256(nc * 8);
+    unsigned long long *stmp = reinterpret_cast<unsigned long long *>(p);
+    p += align256(scan_tmp_words(nc) * 8);
+    SortTile *d_tiles = reinterpret_cast<SortTile *>(p);
+    note_launch();
+    k_single_segment_tiles<<<grid_for(n_tiles, 256), 256, 0, st>>>(d_tiles, n, n_tiles);
+    const size_t smem = RS_TILE * 8 + RS_TILE * 4 + 8 * 256 * 4 + 256 * 4;
+    cudaError_t e = cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    unsigned long long *ks = keys, *kd = k2;
+    uint32_t *vs = vals, *vd = v2;
+    const uint32_t passes = (bits + 7) / 8;
+    for (uint32_t pass = 0; pass < passes; ++pass) {
+        const uint32_t shift = pass * 8;
+        note_launch();
+        k_radix_count<<<(unsigned)n_tiles, RS_THREADS, 0, st>>>(ks, d_tiles, shift, counts);
+        e = launch_scan_u32(counts, offs, nc, stmp, st);
+        if (e != cudaSuccess) return e;
+        note_launch();
+        k_radix_scatter<<<(unsigned)n_tiles, RS_THREADS, smem, st>>>(ks, vs, kd, vd, d_tiles, shift, offs);
+        std::swap(ks, kd);
+        std::swap(vs, vd);
+    }
+    if (ks != keys) {
+        e = cudaMemcpyAsync(keys, ks, n * 8, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(vals, vs, n * 4, cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_radix_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
                               cudaStream_t st)
 {

@@ -181,6 +181,11 @@ cudaError_t launch_compact_batch(const Slot *slots, uint64_t total, const Sample
                                  unsigned long long *hist, unsigned long long *ovf, uint64_t ovf_cap,
                                  unsigned long long *distinct, unsigned long long *counters, int count_only,
                                  cudaStream_t st);
+// The same sort with every buffer, tile descriptors included, taken from tmp
+// (sort_tmp_bytes(n) bytes) and nothing copied from the host.
+cudaError_t launch_radix_sort_in_scratch(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits,
+                                         void *tmp, cudaStream_t st);
+
 cudaError_t launch_pair_reverse(unsigned long long *keys, uint64_t n, cudaStream_t st);
 
 // Stable selection of records whose count satisfies lo <= c <= hi: writes the
