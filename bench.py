@@ -346,6 +346,20 @@ def run_ours(args):
                           "alg_GBps": (algorithmic_bytes(phases[i], r0) / (mean_ms[i] / 1000.0) / 1e9)
                           if mean_ms[i] > 0 else None} for i in range(ns) if mean_ms[i] > 0}
 
+    # atomic throughput of the table insert against random-atomicAdd peaks
+    # measured here: a 4 GiB buffer (DRAM sector RMW) and a 32 MiB buffer
+    # (L2-resident, like one bucket's sub-table)
+    atomics = None
+    ih = phases.index("insert_high")
+    if mean_ms[ih] > 0:
+        pk_dram, _ = kc.atomic_peak(4 << 30)
+        pk_l2, _ = kc.atomic_peak(32 << 20)
+        rate = r0.high_len / (mean_ms[ih] / 1000.0)
+        atomics = {"kernel": "insert_high", "inserts_per_s": rate, "unit": "atomics/s",
+                   "peak_dram_random": pk_dram, "peak_l2_random": pk_l2,
+                   "frac_of_dram_peak": rate / pk_dram, "frac_of_l2_peak": rate / pk_l2,
+                   "note": "one count atomicAdd per non-FIRST occurrence before warp aggregation"}
+
     cpu = None
     if rank == 0 and world == 1 and args.cpu_baseline:
         try:
@@ -375,7 +389,7 @@ def run_ours(args):
                        "memory_gb": MEMORY_GB, "scale": args.scale},
             "e2e": {"value": e2e_val, "unit": "k-mers/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": int(launches),
-            "stages": stages,
+            "stages": stages, "atomics": atomics,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

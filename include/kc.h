@@ -192,6 +192,14 @@ int kc_sort_records(uint64_t *keys, uint32_t *counts, uint64_t n, uint32_t bits)
 #define KC_SORT_NOALLOC_MAX (1u << 20)
 int kc_sort_records_noalloc(uint64_t *d_keys, uint32_t *d_counts, uint64_t n, uint32_t bits, void *stream);
 
+/* Measurement aid, no counterpart in the reference: throughput of random
+ * 32-bit atomicAdd (no return value) over a device buffer of buffer_bytes (a
+ * power of two), averaged over `repeats` launches.  A buffer far larger than
+ * L2 gives the DRAM atomic peak the table insert is compared with; a buffer
+ * that fits in L2 gives the L2 atomic peak (the per-bucket tables are sized
+ * to stay L2-resident). */
+int kc_atomic_peak(uint64_t buffer_bytes, uint32_t repeats, double *atomics_per_s, double *ms_per_launch);
+
 /* Pre-pass statistics and Bloom sizing of a job (src/main.cpp:262-335 with
  * get_MAX_BLOOM_FILTER_CAPACITY :41 and calculate_bloom_filter_capacity :111):
  * raw root-prefix counts over the sample, average quality, capacities. */

@@ -106,6 +106,7 @@ SIGNATURES = [
                                 C.POINTER(C.c_uint32), C.c_void_p, C.POINTER(C.c_uint64)]),
     ("kc_kernel_launches", C.c_uint64, []),
     ("kc_sort_records_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]),
+    ("kc_atomic_peak", C.c_int, [C.c_uint64, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("kc_plan_bloom", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p,
                                 C.POINTER(C.c_uint64)]),
     ("kc_merge_records", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_uint32,
@@ -376,6 +377,14 @@ class KmerCounter:
 def kernel_launches() -> int:
     """Kernel launches issued by libkc.so in this process."""
     return int(lib().kc_kernel_launches())
+
+
+def atomic_peak(buffer_bytes: int, repeats: int = 5):
+    """(atomics/s, ms per launch) of random 32-bit atomicAdd over a device
+    buffer of buffer_bytes (power of two)."""
+    rate, ms = C.c_double(), C.c_double()
+    _check(lib().kc_atomic_peak(buffer_bytes, repeats, C.byref(rate), C.byref(ms)))
+    return rate.value, ms.value
 
 
 def extract_kmers(fastq: bytes, k: int) -> np.ndarray:

@@ -300,6 +300,22 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
         // the bucket census reads every 8th tile of large inputs; buckets get
         // regions with headroom and an outgrown region triggers an exact redo
         a.bucket_sample_mask = (exact_census || T < 512) ? 0 : 7;
+        if (a.bucket_sample_mask) {
+            // only the census tiles and the pre-pass sample of each file are
+            // read; the exact occurrence count comes from the partition pass
+            std::vector<uint32_t> visit;
+            visit.reserve(T / (a.bucket_sample_mask + 1) + 1);
+            for (uint32_t i = 0; i < n_seg; ++i) {
+                const uint64_t pre = (segs[i].sample_end + TILE - 1) / TILE;
+                for (uint64_t t = segs[i].first_tile; t < segs[i].first_tile + segs[i].n_tiles; ++t)
+                    if ((t & a.bucket_sample_mask) == 0 || t - segs[i].first_tile < pre) visit.push_back((uint32_t)t);
+            }
+            uint32_t *d_visit = ds.n<uint32_t>(std::max<size_t>(visit.size(), 1));
+            if (!visit.empty())
+                CK(cudaMemcpyAsync(d_visit, visit.data(), visit.size() * 4, cudaMemcpyHostToDevice, st));
+            a.visit = d_visit;
+            a.n_visit = visit.size();
+        }
         int32_t *chunk_lastnl = ds.n<int32_t>(std::max<uint64_t>(n_chunks, 1));
         uint64_t *d_chunk0 = ds.n<uint64_t>(seg_chunk0.size());
         prefix_hist = ds.n<uint32_t>(256);
@@ -381,12 +397,15 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
         unsigned long long sampled = 0;
         for (uint32_t b = 0; b < N_BUCKETS; ++b) sampled += bh[b];
         const bool exact = a.bucket_sample_mask == 0;
-        if (exact && sampled != O) throw KcError{KC_ERR_DEVICE, "bucket census does not add up to the occurrences"};
-        if (!exact && sampled < 65536 && O > sampled) throw CensusOverflow{};   // too thin a sample
+        // SCAN counted the occurrences of the census tiles (all tiles when exact)
+        if (sampled != O) throw KcError{KC_ERR_DEVICE, "bucket census does not add up to the occurrences"};
+        if (!exact && sampled < 65536) throw CensusOverflow{};   // too thin a sample
+        // census tiles: t with (t & mask) == 0
+        const double scale =
+            exact ? 1.0 : (double)T / (double)((T + a.bucket_sample_mask) / (a.bucket_sample_mask + 1));
         unsigned long long off = 0;
         for (uint32_t b = 0; b < N_BUCKETS; ++b) {
-            region[b] = exact ? bh[b]
-                              : (unsigned long long)std::ceil((double)O * (double)bh[b] / (double)sampled * 1.15) + 8192;
+            region[b] = exact ? bh[b] : (unsigned long long)std::ceil((double)bh[b] * scale * 1.15) + 8192;
             cfg[b].key_base = off;
             off += region[b];
         }
@@ -441,7 +460,9 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
             cfg[b].key_len = fill[b];
             filled += fill[b];
         }
-        if (filled != O) throw KcError{KC_ERR_DEVICE, "partition does not add up to the occurrences"};
+        if (exact && filled != O) throw KcError{KC_ERR_DEVICE, "partition does not add up to the occurrences"};
+        O = filled;
+        job.occurrences = O;
         CK(cudaMemcpyAsync(d_cfg_b, cfg.data(), N_BUCKETS * sizeof(BucketCfg), cudaMemcpyHostToDevice, st));
         clk.begin(8);
         std::vector<WorkItem> items;
@@ -571,11 +592,12 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
     clk.begin(6);
     if (n_rec > 1) {
         void *stmp = ds.get(sort_tmp_bytes(n_rec));
-        CK(launch_radix_sort(rec_keys, rec_counts, n_rec, 2 * k, stmp, st));
+        CK(launch_radix_sort(rec_keys, rec_counts, n_rec, 2 * k, stmp, st, counters + C_FLAGS));
         ds.release(stmp);
     }
     CK(launch_pair_reverse(rec_keys, n_rec, st));
     clk.end();
+    check_flags(read_counters(counters, st).v[C_FLAGS], "sort");
 
     // ---- histogram ----------------------------------------------------------
     std::vector<unsigned long long> hd(HIST_BINS);

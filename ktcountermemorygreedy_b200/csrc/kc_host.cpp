@@ -397,12 +397,50 @@ int kc_sort_records(uint64_t *keys, uint32_t *counts, uint64_t n, uint32_t bits)
         unsigned long long *dk = ds.n<unsigned long long>(n);
         uint32_t *dv = ds.n<uint32_t>(n);
         void *tmp = ds.get(sort_tmp_bytes(n));
+        unsigned long long *dflags = ds.n<unsigned long long>(1);
+        CK(cudaMemsetAsync(dflags, 0, 8, sg.st));
         CK(cudaMemcpyAsync(dk, keys, n * 8, cudaMemcpyHostToDevice, sg.st));
         CK(cudaMemcpyAsync(dv, counts, n * 4, cudaMemcpyHostToDevice, sg.st));
-        CK(launch_radix_sort(dk, dv, n, bits, tmp, sg.st));
+        CK(launch_radix_sort(dk, dv, n, bits, tmp, sg.st, dflags));
         CK(cudaMemcpyAsync(keys, dk, n * 8, cudaMemcpyDeviceToHost, sg.st));
         CK(cudaMemcpyAsync(counts, dv, n * 4, cudaMemcpyDeviceToHost, sg.st));
+        unsigned long long flags = 0;
+        CK(cudaMemcpyAsync(&flags, dflags, 8, cudaMemcpyDeviceToHost, sg.st));
         CK(cudaStreamSynchronize(sg.st));
+        if (flags) return set_error(KC_ERR_DEVICE, "record sort reported error flags");
+        return KC_OK;
+    } catch (const KcError &e) {
+        return set_error(e.code, e.msg);
+    }
+}
+
+int kc_atomic_peak(uint64_t buffer_bytes, uint32_t repeats, double *atomics_per_s, double *ms_per_launch)
+{
+    if (!atomics_per_s || !ms_per_launch || !repeats) return set_error(KC_ERR_INVALID, "bad argument");
+    if (buffer_bytes < 4096 || (buffer_bytes & (buffer_bytes - 1)))
+        return set_error(KC_ERR_INVALID, "buffer_bytes must be a power of two >= 4096");
+    try {
+        StreamGuard sg;
+        DevScope ds(sg.st);
+        const uint64_t words = buffer_bytes / 4;
+        uint32_t *buf = ds.n<uint32_t>(words);
+        CK(cudaMemsetAsync(buf, 0, buffer_bytes, sg.st));
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        uint64_t ops = 0;
+        const uint32_t iters = 512;
+        CK(launch_atomic_peak(buf, words, iters, 1, &ops, sg.st));   // warm-up
+        CK(cudaEventRecord(e0, sg.st));
+        for (uint32_t r = 0; r < repeats; ++r) CK(launch_atomic_peak(buf, words, iters, 2 + r, &ops, sg.st));
+        CK(cudaEventRecord(e1, sg.st));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *ms_per_launch = ms / repeats;
+        *atomics_per_s = (double)ops * repeats / (ms * 1e-3);
         return KC_OK;
     } catch (const KcError &e) {
         return set_error(e.code, e.msg);

@@ -325,8 +325,11 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
     __shared__ unsigned long long s_bcap[MODE == MODE_BLOOM ? 256 : 1];
 
     const int tid = threadIdx.x, lane = tid & 31;
-    uint64_t t = blockIdx.x;
-    if (t >= a.n_tiles) return;
+    // u walks the visited tiles (all tiles, or the SCAN subset a.visit)
+    const uint64_t n_iter = (MODE == MODE_SCAN && a.visit) ? a.n_visit : a.n_tiles;
+    uint64_t u = blockIdx.x;
+    if (u >= n_iter) return;
+    uint64_t t = (MODE == MODE_SCAN && a.visit) ? (uint64_t)a.visit[u] : u;
 
     if (tid == 0) {
         mbar_init(&mbar[0], 1);
@@ -352,11 +355,13 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
     unsigned long long *flags = &a.counters[C_FLAGS];
     uint32_t iter = 0;
     bool pending_next = false;
-    for (; t < a.n_tiles; t += gridDim.x, ++iter) {
+    for (; u < n_iter; u += gridDim.x, ++iter) {
+        t = (MODE == MODE_SCAN && a.visit) ? (uint64_t)a.visit[u] : u;
         const int s = iter & 1;
-        const uint64_t tn = t + gridDim.x;
-        pending_next = tn < a.n_tiles;
+        const uint64_t un = u + gridDim.x;
+        pending_next = un < n_iter;
         if (tid == 0 && pending_next) {
+            const uint64_t tn = (MODE == MODE_SCAN && a.visit) ? (uint64_t)a.visit[un] : un;
             fence_proxy_async_smem();
             mbar_expect_tx(&mbar[s ^ 1], BUF_BYTES);
             bulk_load(sbuf[s ^ 1], a.buf + tn * TILE - HALO, BUF_BYTES, &mbar[s ^ 1]);
@@ -454,8 +459,10 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
                 if (census) atomicAdd(&s_bhist[key >> 56], 1u);
                 if ((sample_ok >> j) & 1u) atomicAdd(&s_hist[key >> 56], 1u);
             }
-            unsigned n = __reduce_add_sync(FULL, (unsigned)__popc(ends));
-            if (lane == 0 && n) atomicAdd(&a.occ[sg.sample], (unsigned long long)n);
+            if (!a.visit || census) {
+                unsigned n = __reduce_add_sync(FULL, (unsigned)__popc(ends));
+                if (lane == 0 && n) atomicAdd(&a.occ[sg.sample], (unsigned long long)n);
+            }
         } else {
             uint32_t tot;
             const uint32_t off = block_excl_scan(__popc(ends), s_warp, tot);
@@ -1000,6 +1007,159 @@ __global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const unsigned lon
 }
 
 // ---------------------------------------------------------------------------
+// radix sort of one segment, one kernel per pass (single-pass prefix with
+// decoupled look-back: every tile publishes its per-digit counts, then adds up
+// its predecessors' counts until it meets a published inclusive prefix)
+// ---------------------------------------------------------------------------
+
+constexpr uint32_t OS_MAX_PASSES = 8;
+constexpr int LB_VALUE_BITS = 40;                                // count field of a look-back word
+constexpr unsigned long long LB_VALUE_MASK = (1ull << LB_VALUE_BITS) - 1;
+
+// Digit histograms of every pass in one read of the keys.
+__global__ void __launch_bounds__(256) k_radix_hist_all(const unsigned long long *keys, uint64_t n, uint32_t passes,
+                                                        unsigned long long *hist)
+{
+    __shared__ uint32_t h[OS_MAX_PASSES * 256];
+    for (uint32_t i = threadIdx.x; i < OS_MAX_PASSES * 256; i += 256) h[i] = 0;
+    __syncthreads();
+    for (uint64_t i = blockIdx.x * 256ull + threadIdx.x; i < n; i += (uint64_t)gridDim.x * 256) {
+        const unsigned long long k = __ldcs(&keys[i]);
+        for (uint32_t p = 0; p < passes; ++p) atomicAdd(&h[p * 256 + (uint32_t)((k >> (8 * p)) & 255)], 1u);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < passes * 256; i += 256)
+        if (h[i]) atomicAdd(&hist[i], (unsigned long long)h[i]);
+}
+
+// Exclusive prefix sum over the block's 256 threads of 64-bit values.
+__device__ __forceinline__ unsigned long long block_excl_scan64(unsigned long long v, unsigned long long *s_w)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned long long y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_w[warp] = x;
+    __syncthreads();
+    unsigned long long base = 0;
+    for (int w = 0; w < warp; ++w) base += s_w[w];
+    __syncthreads();
+    return base + x - v;
+}
+
+// One LSD pass over 8 bits at `shift`.  Tiles are taken in launch order from
+// tile_ctr, so every tile a block waits on belongs to a block that is already
+// running and publishes its counts before it waits itself.  Look-back words:
+// bits 40.. hold the tag (2*pass+1: tile count, 2*pass+2: inclusive prefix),
+// bits 0..39 the value; the array starts zeroed, and older passes' tags are
+// smaller, so it is reused across passes.  A wait that exceeds the spin limit
+// sets ERR_WAIT_TIMEOUT in *flags and carries on.
+__global__ void __launch_bounds__(RS_THREADS, 3) k_radix_onesweep(const unsigned long long *kin, const uint32_t *vin,
+                                                                  unsigned long long *kout, uint32_t *vout,
+                                                                  uint64_t n, uint32_t pass,
+                                                                  const unsigned long long *hist,
+                                                                  unsigned long long *look, unsigned int *tile_ctr,
+                                                                  unsigned long long *flags)
+{
+    extern __shared__ __align__(16) uint8_t rs_smem[];
+    unsigned long long *s_keys = reinterpret_cast<unsigned long long *>(rs_smem);       // RS_TILE
+    uint32_t *s_vals = reinterpret_cast<uint32_t *>(s_keys + RS_TILE);                   // RS_TILE
+    uint32_t *s_wcnt = s_vals + RS_TILE;                                                 // 8 x 256
+    __shared__ uint32_t s_start[256], s_warp[8], s_tile;
+    __shared__ unsigned long long s_dst[256], s_w64[8];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t shift = 8 * pass;
+    if (tid == 0) s_tile = atomicAdd(&tile_ctr[pass], 1u);
+    for (int i = tid; i < 8 * 256; i += RS_THREADS) s_wcnt[i] = 0;
+    __syncthreads();
+    const uint64_t j = s_tile;
+    const uint64_t base = j * RS_TILE;
+    const uint32_t tile_n = (uint32_t)(n - base < RS_TILE ? n - base : RS_TILE);
+
+    // stable rank of every key among the tile's keys with the same digit
+    unsigned long long k[RS_ITEMS];
+    uint32_t rd[RS_ITEMS];   // rank << 16 | digit (digit 256: no key)
+    uint32_t *wc = s_wcnt + warp * 256;
+#pragma unroll
+    for (uint32_t r = 0; r < RS_ITEMS; ++r) {
+        const uint32_t li = warp * RS_WARP_ITEMS + r * 32 + lane;
+        const bool act = li < tile_n;
+        k[r] = act ? __ldcs(&kin[base + li]) : 0;
+        const uint32_t d = act ? (uint32_t)((k[r] >> shift) & 255) : 256u;
+        const uint32_t peers = __match_any_sync(FULL, d);
+        const uint32_t before = __popc(peers & lanemask_lt());
+        const uint32_t cnt = act ? wc[d] : 0;
+        __syncwarp();
+        if (act && before == 0) wc[d] = cnt + __popc(peers);
+        __syncwarp();
+        rd[r] = ((cnt + before) << 16) | d;
+    }
+    __syncthreads();
+    uint32_t own = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+        const uint32_t c = s_wcnt[w * 256 + tid];
+        s_wcnt[w * 256 + tid] = own;
+        own += c;
+    }
+    // publish this tile's count of digit tid, then find the keys of digit tid
+    // in the tiles before it
+    const unsigned long long tag_a = 2ull * pass + 1, tag_i = 2ull * pass + 2;
+    volatile unsigned long long *mine = look + j * 256 + tid;
+    *mine = ((j == 0 ? tag_i : tag_a) << LB_VALUE_BITS) | own;
+    uint32_t tot;
+    const uint32_t start = block_excl_scan(own, s_warp, tot);
+    s_start[tid] = start;
+    unsigned long long excl = 0;
+    if (j > 0) {
+        bool gave_up = false;
+        for (int64_t p = (int64_t)j - 1; p >= 0; --p) {
+            const volatile unsigned long long *w = look + (uint64_t)p * 256 + tid;
+            unsigned long long v = *w;
+            uint32_t spins = 0;
+            while ((v >> LB_VALUE_BITS) < tag_a) {
+                if (++spins > SPIN_LIMIT) { gave_up = true; break; }
+                __nanosleep(32);
+                v = *w;
+            }
+            if (gave_up) break;
+            excl += v & LB_VALUE_MASK;
+            if ((v >> LB_VALUE_BITS) >= tag_i) break;
+        }
+        if (gave_up) atomicOr(flags, ERR_WAIT_TIMEOUT);
+        *mine = (tag_i << LB_VALUE_BITS) | (excl + own);
+    }
+    const unsigned long long gofs = block_excl_scan64(hist[pass * 256 + tid], s_w64);
+    s_dst[tid] = gofs + excl - start;
+    __syncthreads();
+    // reorder the tile by digit in shared memory, then write runs of equal
+    // digits to consecutive addresses
+#pragma unroll
+    for (uint32_t r = 0; r < RS_ITEMS; ++r) {
+        const uint32_t d = rd[r] & 0xFFFFu;
+        if (d < 256) {
+            const uint32_t li = warp * RS_WARP_ITEMS + r * 32 + lane;
+            const uint32_t pos = s_start[d] + s_wcnt[warp * 256 + d] + (rd[r] >> 16);
+            s_keys[pos] = k[r];
+            s_vals[pos] = __ldcs(&vin[base + li]);
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = tid; i < tile_n; i += RS_THREADS) {
+        const unsigned long long key = s_keys[i];
+        const unsigned long long dst = s_dst[(uint32_t)((key >> shift) & 255)] + i;
+        if (dst < n) {   // only a look-back that gave up can point elsewhere
+            kout[dst] = key;
+            vout[dst] = s_vals[i];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // selection
 // ---------------------------------------------------------------------------
 
@@ -1299,7 +1459,9 @@ static cudaError_t launch_extract_t(const ExtractArgs &a, int grid, uint32_t sta
         if (per_sm < 1) per_sm = 1;
         grid = sm_count() * per_sm;
     }
-    if ((uint64_t)grid > a.n_tiles) grid = (int)a.n_tiles;
+    const uint64_t n_iter = (M == MODE_SCAN && a.visit) ? a.n_visit : a.n_tiles;
+    if (!n_iter) return cudaSuccess;
+    if ((uint64_t)grid > n_iter) grid = (int)n_iter;
     note_launch();
     k_extract<M><<<grid, EXT_THREADS, smem, st>>>(a, stage_cap);
     return cudaGetLastError();
@@ -1416,7 +1578,19 @@ size_t sort_tmp_bytes_segmented(uint64_t n_total, const uint64_t *seg_len, uint3
            align256(scan_tmp_words(nc) * 8) + align256(std::max<uint64_t>(n_tiles, 1) * sizeof(SortTile));
 }
 
-size_t sort_tmp_bytes(uint64_t n) { return sort_tmp_bytes_segmented(n, &n, 1); }
+// working memory of launch_radix_sort: second key/value arrays, the digit
+// histograms of all passes, one look-back word per (tile, digit), the tile
+// counters of the passes and an error word
+static size_t onesweep_tmp_bytes(uint64_t n)
+{
+    const uint64_t n_tiles = std::max<uint64_t>((n + RS_TILE - 1) / RS_TILE, 1);
+    return align256(n * 8) + align256(n * 4) + align256(OS_MAX_PASSES * 256 * 8) + align256(n_tiles * 256 * 8) +
+           align256(OS_MAX_PASSES * 4 + 8);
+}
+
+size_t sort_tmp_bytes(uint64_t n) { return onesweep_tmp_bytes(n); }
+
+size_t sort_tmp_bytes_in_scratch(uint64_t n) { return sort_tmp_bytes_segmented(n, &n, 1); }
 
 // Segments [seg_start[i], seg_start[i] + seg_len[i]) of the arrays are sorted
 // independently; they must be disjoint and in increasing address order.
@@ -1546,11 +1720,48 @@ cudaError_t launch_radix_sort_in_scratch(unsigned long long *keys, uint32_t *val
 }
 
 cudaError_t launch_radix_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
-                              cudaStream_t st)
+                              cudaStream_t st, unsigned long long *flags)
 {
     if (n <= 1 || bits == 0) return cudaSuccess;
-    const uint64_t start = 0;
-    return launch_radix_sort_segmented(keys, vals, n, &start, &n, 1, bits, tmp, st);
+    if (bits > 64) return cudaErrorInvalidValue;
+    const uint32_t passes = (bits + 7) / 8;
+    const uint64_t n_tiles = (n + RS_TILE - 1) / RS_TILE;
+    uint8_t *p = static_cast<uint8_t *>(tmp);
+    unsigned long long *k2 = reinterpret_cast<unsigned long long *>(p);
+    p += align256(n * 8);
+    uint32_t *v2 = reinterpret_cast<uint32_t *>(p);
+    p += align256(n * 4);
+    unsigned long long *hist = reinterpret_cast<unsigned long long *>(p);
+    p += align256(OS_MAX_PASSES * 256 * 8);
+    unsigned long long *look = reinterpret_cast<unsigned long long *>(p);
+    p += align256(n_tiles * 256 * 8);
+    unsigned int *tile_ctr = reinterpret_cast<unsigned int *>(p);
+    unsigned long long *own_flags = reinterpret_cast<unsigned long long *>(p + OS_MAX_PASSES * 4);
+    if (!flags) flags = own_flags;
+    cudaError_t e = cudaMemsetAsync(hist, 0, OS_MAX_PASSES * 256 * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(look, 0, n_tiles * 256 * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(tile_ctr, 0, OS_MAX_PASSES * 4 + 8, st);
+    if (e != cudaSuccess) return e;
+    note_launch();
+    k_radix_hist_all<<<grid_for(n, 256, 4), 256, 0, st>>>(keys, n, passes, hist);
+    const size_t smem = RS_TILE * 8 + RS_TILE * 4 + 8 * 256 * 4;
+    e = cudaFuncSetAttribute(k_radix_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    unsigned long long *ks = keys, *kd = k2;
+    uint32_t *vs = vals, *vd = v2;
+    for (uint32_t pass = 0; pass < passes; ++pass) {
+        note_launch();
+        k_radix_onesweep<<<(unsigned)n_tiles, RS_THREADS, smem, st>>>(ks, vs, kd, vd, n, pass, hist, look, tile_ctr,
+                                                                      flags);
+        std::swap(ks, kd);
+        std::swap(vs, vd);
+    }
+    if (ks != keys) {
+        e = cudaMemcpyAsync(keys, ks, n * 8, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(vals, vs, n * 4, cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_compact_batch(const Slot *slots, uint64_t total, const SampleCfg *cfg, uint32_t n_samples,
@@ -1649,6 +1860,36 @@ cudaError_t launch_hash_batch(const unsigned long long *keys, uint64_t n, unsign
     if (!n) return cudaSuccess;
     note_launch();
     k_hash_batch<<<grid_for(n, 256), 256, 0, st>>>(keys, n, out);
+    return cudaGetLastError();
+}
+
+// Random 32-bit atomicAdd throughput: every thread adds 1 at `iters`
+// pseudo-random word indexes (xorshift64*, independent per thread) of a buffer
+// of mask+1 words.  With a buffer far larger than L2 each add is a DRAM
+// read-modify-write of one 32-byte sector; with a buffer that fits in L2 it
+// measures the L2 atomic units.  The adds do not use their return value (the
+// counting tables' count increments do not either).
+__global__ void __launch_bounds__(256) k_atomic_peak(uint32_t *buf, uint64_t mask, uint32_t iters, uint64_t seed)
+{
+    uint64_t x = seed ^ ((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x + 1) * 0x9E3779B97F4A7C15ull);
+    x ^= x >> 31;
+    if (!x) x = 1;
+#pragma unroll 4
+    for (uint32_t i = 0; i < iters; ++i) {
+        x ^= x >> 12;
+        x ^= x << 25;
+        x ^= x >> 27;
+        atomicAdd(buf + ((x * 0x2545F4914F6CDD1Dull) >> 20 & mask), 1u);
+    }
+}
+
+cudaError_t launch_atomic_peak(uint32_t *buf, uint64_t words, uint32_t iters, uint64_t seed, uint64_t *ops,
+                               cudaStream_t st)
+{
+    const unsigned grid = (unsigned)sm_count() * 8;
+    *ops = (uint64_t)grid * 256 * iters;
+    note_launch();
+    k_atomic_peak<<<grid, 256, 0, st>>>(buf, words - 1, iters, seed);
     return cudaGetLastError();
 }
 

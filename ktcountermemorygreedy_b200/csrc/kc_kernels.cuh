@@ -106,6 +106,11 @@ struct ExtractArgs {
     // root-prefix buckets (single sample): SCAN counts, PART scatters
     unsigned long long *bucket_hist;          // 256 counts (SCAN)
     uint64_t bucket_sample_mask;              // SCAN counts tiles t with (t & mask) == 0
+    // SCAN over a subset of the tiles: visit[0..n_visit) ascending tile
+    // indexes (NULL: every tile); occurrences are then counted on the census
+    // tiles only
+    const uint32_t *visit;
+    uint64_t n_visit;
     unsigned long long *bucket_cursor;        // 256 fill levels (PART)
     const unsigned long long *bucket_base;    // 256 start offsets in `list` (PART)
     const unsigned long long *bucket_end;     // 256 end offsets in `list` (PART)
@@ -173,16 +178,20 @@ size_t sort_tmp_bytes_segmented(uint64_t n_total, const uint64_t *seg_len, uint3
 cudaError_t launch_radix_sort_segmented(unsigned long long *keys, uint32_t *vals, uint64_t n_total,
                                         const uint64_t *seg_start, const uint64_t *seg_len, uint32_t n_segs,
                                         uint32_t bits, void *tmp, cudaStream_t st);
+// One segment, one kernel per 8-bit pass; a look-back wait that gave up sets
+// ERR_WAIT_TIMEOUT in *flags (NULL: a word inside tmp).
 cudaError_t launch_radix_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
-                              cudaStream_t st);
+                              cudaStream_t st, unsigned long long *flags = nullptr);
 
 cudaError_t launch_compact_batch(const Slot *slots, uint64_t total, const SampleCfg *cfg, uint32_t n_samples,
                                  unsigned long long *rec_len, unsigned long long *rec_keys, uint32_t *rec_counts,
                                  unsigned long long *hist, unsigned long long *ovf, uint64_t ovf_cap,
                                  unsigned long long *distinct, unsigned long long *counters, int count_only,
                                  cudaStream_t st);
-// The same sort with every buffer, tile descriptors included, taken from tmp
-// (sort_tmp_bytes(n) bytes) and nothing copied from the host.
+// A sort of one segment with every buffer, tile descriptors included, taken
+// from tmp (sort_tmp_bytes_in_scratch(n) bytes) and nothing copied from the
+// host (digit counts, a scan and a scatter per pass).
+size_t sort_tmp_bytes_in_scratch(uint64_t n);
 cudaError_t launch_radix_sort_in_scratch(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits,
                                          void *tmp, cudaStream_t st);
 
@@ -212,5 +221,10 @@ cudaError_t launch_merge_buckets(const unsigned long long *keys, const WorkItem 
 // xxh3_128.lo, xxh3_128.hi, xxh3_64, rapidhash, komihash (all of keys[i]).
 cudaError_t launch_hash_batch(const unsigned long long *keys, uint64_t n, unsigned long long *out,
                               cudaStream_t st);
+
+// Random 32-bit atomicAdd microbenchmark over `words` (a power of two) words;
+// *ops receives the number of adds the launch performs.
+cudaError_t launch_atomic_peak(uint32_t *buf, uint64_t words, uint32_t iters, uint64_t seed, uint64_t *ops,
+                               cudaStream_t st);
 
 }  // namespace kc

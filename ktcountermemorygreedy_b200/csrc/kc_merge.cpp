@@ -66,7 +66,7 @@ extern "C" int kc_merge_records(const uint64_t *high_keys, const uint32_t *high_
         const uint64_t n_rec = c[C_REC_LEN];
         if (n_rec > 1) {
             void *tmp = ds.get(sort_tmp_bytes(n_rec));
-            CK(launch_radix_sort(rk, rc, n_rec, 2 * k, tmp, st));
+            CK(launch_radix_sort(rk, rc, n_rec, 2 * k, tmp, st, counters + C_FLAGS));
         }
         CK(launch_pair_reverse(rk, n_rec, st));
         std::vector<unsigned long long> hh(HIST_BINS);
@@ -79,7 +79,10 @@ extern "C" int kc_merge_records(const uint64_t *high_keys, const uint32_t *high_
             CK(cudaMemcpyAsync(out_keys, rk, n_copy * 8, cudaMemcpyDeviceToHost, st));
             CK(cudaMemcpyAsync(out_counts, rc, n_copy * 4, cudaMemcpyDeviceToHost, st));
         }
+        unsigned long long sort_flags = 0;
+        CK(cudaMemcpyAsync(&sort_flags, counters + C_FLAGS, 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        if (sort_flags) return set_error(KC_ERR_DEVICE, "record sort reported error flags");
         hh[1] += c[C_LOW_ONLY];
         *n_out = n_rec;
         if (hist) {

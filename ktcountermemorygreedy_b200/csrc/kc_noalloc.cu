@@ -75,7 +75,7 @@ extern "C" int kc_sort_records_noalloc(uint64_t *d_keys, uint32_t *d_counts, uin
         return kc::set_error(KC_ERR_INVALID, "kc_sort_records_noalloc sorts at most " +
                                                  std::to_string((unsigned long long)KC_SORT_NOALLOC_MAX) +
                                                  " records; got " + std::to_string((unsigned long long)n));
-    const size_t need = kc::sort_tmp_bytes(n);
+    const size_t need = kc::sort_tmp_bytes_in_scratch(n);
     if (need > SCRATCH_BYTES) return kc::set_error(KC_ERR_INVALID, "scratch array too small for this sort");
     void *scratch = nullptr;
     int rc = scratch_for_current_device(&scratch);
