@@ -300,7 +300,7 @@ __global__ void k_chunk_lastnl(const int32_t *tile_lastnl, const uint32_t *tile_
 // ---------------------------------------------------------------------------
 
 template <int MODE>
-__global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t stage_cap)
+__global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extract(ExtractArgs a, uint32_t stage_cap)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t *sbuf[2] = {smem, smem + BUF_BYTES};
@@ -501,16 +501,39 @@ __global__ void __launch_bounds__(EXT_THREADS) k_extract(ExtractArgs a, uint32_t
                     for (uint32_t i = tid; i < nr; i += EXT_THREADS)
                         s_rank[i] = (uint16_t)atomicAdd(&s_bhist[(uint32_t)(s_stage[i] >> 56)], 1u);
                     __syncthreads();
-                    {
-                        const uint32_t c = s_bhist[tid];
-                        s_bpos[tid] = c ? a.bucket_base[tid] + atomicAdd(&a.bucket_cursor[tid], (unsigned long long)c)
-                                        : 0ull;
+                    // the round's k-mers are reordered by bucket in shared
+                    // memory, so that consecutive threads store consecutive
+                    // addresses of one bucket's region (a warp's store then
+                    // touches a few sectors instead of one per k-mer)
+                    uint32_t tot_b;
+                    const uint32_t c = s_bhist[tid];
+                    const uint32_t bstart = block_excl_scan(c, s_warp, tot_b);
+                    s_hist[tid] = bstart;
+                    // destination of sorted index i of bucket b: s_bpos[b] + i
+                    s_bpos[tid] = c ? a.bucket_base[tid] + atomicAdd(&a.bucket_cursor[tid], (unsigned long long)c) -
+                                          bstart
+                                    : 0ull;
+                    __syncthreads();
+                    unsigned long long kr[STAGE_CAP / EXT_THREADS];
+#pragma unroll
+                    for (uint32_t r = 0; r < STAGE_CAP / EXT_THREADS; ++r) {
+                        const uint32_t i = tid + r * EXT_THREADS;
+                        if (i < nr) {
+                            kr[r] = s_stage[i];
+                            s_rank[i] = (uint16_t)(s_hist[(uint32_t)(kr[r] >> 56)] + s_rank[i]);
+                        }
+                    }
+                    __syncthreads();
+#pragma unroll
+                    for (uint32_t r = 0; r < STAGE_CAP / EXT_THREADS; ++r) {
+                        const uint32_t i = tid + r * EXT_THREADS;
+                        if (i < nr) s_stage[s_rank[i]] = kr[r];
                     }
                     __syncthreads();
                     for (uint32_t i = tid; i < nr; i += EXT_THREADS) {
                         const unsigned long long key = s_stage[i];
                         const uint32_t b = (uint32_t)(key >> 56);
-                        const unsigned long long pos = s_bpos[b] + s_rank[i];
+                        const unsigned long long pos = s_bpos[b] + i;
                         // a bucket that outgrows its estimated region is
                         // reported (its cursor passes the end) and redone
                         if (pos < a.bucket_end[b] && pos < a.list_cap) a.list[pos] = key;
