@@ -358,7 +358,7 @@ def run_ours(args):
         atomics = {"kernel": "insert_high", "inserts_per_s": rate, "unit": "atomics/s",
                    "peak_dram_random": pk_dram, "peak_l2_random": pk_l2,
                    "frac_of_dram_peak": rate / pk_dram, "frac_of_l2_peak": rate / pk_l2,
-                   "note": "one count atomicAdd per non-FIRST occurrence before warp aggregation"}
+                   "note": "one slot-key read and one count atomicAdd per non-FIRST occurrence"}
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_baseline:

@@ -497,8 +497,10 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
         for (uint32_t b = 0; b < N_BUCKETS; ++b) {
             low_len += lh[b];
             high_len += lh[N_BUCKETS + b];
-            // the registers hold a 1-in-8 hash sample of the non-FIRST k-mers
-            double e = lh[N_BUCKETS + b] ? 8.0 * hll_estimate(&hh[(size_t)b * BUCKET_HLL_M], BUCKET_HLL_M) : 0.0;
+            // the registers hold a hash sample of the non-FIRST k-mers
+            double e = lh[N_BUCKETS + b] ? (double)(1u << BUCKET_HLL_SAMPLE_BITS) *
+                                               hll_estimate(&hh[(size_t)b * BUCKET_HLL_M], BUCKET_HLL_M)
+                                         : 0.0;
             e = std::max(e, (double)std::min<unsigned long long>(lh[N_BUCKETS + b], 4096));
             bcaps[b] = table_capacity_for(e);
         }

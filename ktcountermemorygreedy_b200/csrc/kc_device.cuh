@@ -137,6 +137,19 @@ __device__ __forceinline__ void bloom_probe(uint64_t w, uint64_t cap, uint64_t &
     block = lo & (cap - 1);
 }
 
+// The same probe, also returning the high 64 bits of the hash (used as the
+// hash of the k-mer for sampled distinct counting).
+__device__ __forceinline__ void bloom_probe_hi(uint64_t w, uint64_t cap, uint64_t &block, uint64_t &mask,
+                                               uint64_t &hi_out)
+{
+    uint64_t lo, hi;
+    xxh3_128_8(w, lo, hi);
+    uint64_t h2 = hi | 1ULL;
+    mask = (1ULL << (lo & 63)) | (1ULL << ((lo + h2) & 63)) | (1ULL << ((lo + 2 * h2) & 63));
+    block = lo & (cap - 1);
+    hi_out = hi;
+}
+
 // ---------------------------------------------------------------------------
 // bounded waits
 // ---------------------------------------------------------------------------

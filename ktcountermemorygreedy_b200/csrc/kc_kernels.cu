@@ -1222,17 +1222,25 @@ __device__ __forceinline__ bool next_work(unsigned int *next_item, uint32_t n_it
     return it < n_items;
 }
 
-// HyperLogLog of a 1-in-8 hash sample of the keys (the estimate is scaled by
-// 8 on the host): an eighth of the register traffic for the same accuracy on
-// the large sets the tables are sized for.
-__device__ __forceinline__ void hll_add_sampled(uint32_t *regs, unsigned long long key, uint32_t bits)
+// HyperLogLog of a 1-in-64 hash sample of the non-FIRST k-mers, from the
+// high 64 bits h of their XXH3-128 hash (the estimate is scaled by 64 on the
+// host).  hll_token packs (register << 8 | rank), 0 for a hash outside the
+// sample.  The sample is thin because all blocks working on a bucket update
+// the same 1024 registers; an update is skipped when the register already
+// holds the rank.
+__device__ __forceinline__ uint32_t hll_token(uint64_t h, uint32_t bits)
 {
-    uint64_t h = slot_hash(key ^ 0x5bd1e9955bd1e995ULL);
-    if (h & 7) return;
-    h >>= 3;
-    uint32_t r = (uint32_t)(h >> (61 - bits));
-    uint32_t rank = __clzll((h << (bits + 3)) | (1ULL << (bits + 2))) + 1;
-    if (rank > *(volatile uint32_t *)&regs[r]) atomicMax(&regs[r], rank);
+    if (h & ((1u << BUCKET_HLL_SAMPLE_BITS) - 1)) return 0;
+    const uint32_t r = (uint32_t)(h >> (64 - bits));
+    const uint32_t rank = __clzll((h << bits) | (1ULL << (bits + BUCKET_HLL_SAMPLE_BITS - 1))) + 1;
+    return (r << 8) | rank;
+}
+
+__device__ __forceinline__ void hll_add_token(uint32_t *regs, uint32_t tok)
+{
+    if (!tok) return;
+    uint32_t *p = &regs[tok >> 8];
+    if ((tok & 0xFFu) > *(volatile uint32_t *)p) atomicMax(p, tok & 0xFFu);
 }
 
 // The reference's two-level Bloom classification (src/BloomFilter.h:233-273)
@@ -1248,54 +1256,70 @@ __global__ void __launch_bounds__(256, 4) k_bloom_buckets(const unsigned long lo
 {
     __shared__ uint32_t s_item, s_warp[8];
     __shared__ unsigned long long s_lb, s_hb;
+    // each thread's k-mers wait here (not in registers) while their filter
+    // words are read; a thread only reads back what it wrote itself
+    __shared__ unsigned long long s_k[WORK_ITEM_KEYS];
     const int tid = threadIdx.x;
     uint32_t it;
     while (next_work(next_item, n_items, &s_item, it)) {
         const WorkItem w = items[it];
         const BucketCfg bc = cfg[w.bucket];
         const uint64_t n = w.end - w.begin;
-        unsigned long long k[ITEM_PER_THREAD];
         uint32_t firsts = 0, highs = 0;
         // the k-mer stream is read once: keep it from evicting filter lines
 #pragma unroll
         for (uint32_t r = 0; r < ITEM_PER_THREAD; ++r) {
             const uint64_t i = (uint64_t)r * 256 + tid;
-            k[r] = i < n ? __ldcs(&keys[w.begin + i]) : EMPTY_KEY;
+            s_k[r * 256 + tid] = i < n ? __ldcs(&keys[w.begin + i]) : EMPTY_KEY;
         }
+        uint32_t *regs = hll_high + (size_t)w.bucket * BUCKET_HLL_M;
 #pragma unroll
         for (uint32_t g = 0; g < ITEM_PER_THREAD; g += 4) {
             unsigned long long m[4];
+            uint32_t tok[4];
             ulonglong2 *cell[4];
             ulonglong2 v[4];
 #pragma unroll
             for (uint32_t u = 0; u < 4; ++u) {
                 const uint64_t i = (uint64_t)(g + u) * 256 + tid;
-                uint64_t block = 0, mask = 0;
-                if (i < n) bloom_probe(k[g + u], bc.bloom_cap, block, mask);
+                uint64_t block = 0, mask = 0, hi = 0;
+                if (i < n) bloom_probe_hi(s_k[(g + u) * 256 + tid], bc.bloom_cap, block, mask, hi);
                 m[u] = mask;
+                tok[u] = hll_token(hi, BUCKET_HLL_BITS);
                 cell[u] = reinterpret_cast<ulonglong2 *>(bits + bc.bloom_off + 2 * block);
             }
 #pragma unroll
             for (uint32_t u = 0; u < 4; ++u)
                 if ((uint64_t)(g + u) * 256 + tid < n) v[u] = __ldcg(cell[u]);
+            // occurrences not yet known to be repeats set their bits in the
+            // seen-once word; the four returning atomics are issued back to
+            // back and their old values examined afterwards
+            unsigned long long old2[4];
+            uint32_t pending = 0;
 #pragma unroll
             for (uint32_t u = 0; u < 4; ++u) {
                 if ((uint64_t)(g + u) * 256 + tid >= n) continue;
                 unsigned long long *c = reinterpret_cast<unsigned long long *>(cell[u]);
+                if ((v[u].x & m[u]) == m[u]) continue;              // seen twice already
+                if ((v[u].y & m[u]) == m[u]) atomicOr(&c[0], m[u]);   // seen once: now twice
+                else {
+                    old2[u] = atomicOr(&c[1], m[u]);
+                    pending |= 1u << u;
+                }
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < 4; ++u) {
+                if ((uint64_t)(g + u) * 256 + tid >= n) continue;
                 bool first = false;
-                if ((v[u].x & m[u]) != m[u]) {
-                    if ((v[u].y & m[u]) == m[u]) {
-                        atomicOr(&c[0], m[u]);
-                    } else {
-                        unsigned long long old2 = atomicOr(&c[1], m[u]);
-                        if ((old2 & m[u]) == m[u]) atomicOr(&c[0], m[u]);
-                        else first = true;
-                    }
+                if ((pending >> u) & 1u) {
+                    unsigned long long *c = reinterpret_cast<unsigned long long *>(cell[u]);
+                    if ((old2[u] & m[u]) == m[u]) atomicOr(&c[0], m[u]);
+                    else first = true;
                 }
                 if (first) firsts |= 1u << (g + u);
                 else {
                     highs |= 1u << (g + u);
-                    hll_add_sampled(hll_high + (size_t)w.bucket * BUCKET_HLL_M, k[g + u], BUCKET_HLL_BITS);
+                    hll_add_token(regs, tok[u]);
                 }
             }
         }
@@ -1311,8 +1335,8 @@ __global__ void __launch_bounds__(256, 4) k_bloom_buckets(const unsigned long lo
         unsigned long long hp = bc.key_base + bc.key_len - 1 - (s_hb + oh);
 #pragma unroll
         for (uint32_t r = 0; r < ITEM_PER_THREAD; ++r) {
-            if ((firsts >> r) & 1u) __stcs(&out[lp++], k[r]);
-            else if ((highs >> r) & 1u) __stcs(&out[hp--], k[r]);
+            if ((firsts >> r) & 1u) __stcs(&out[lp++], s_k[r * 256 + tid]);
+            else if ((highs >> r) & 1u) __stcs(&out[hp--], s_k[r * 256 + tid]);
         }
         __syncthreads();
     }
@@ -1337,9 +1361,13 @@ __global__ void __launch_bounds__(256) k_insert_buckets(const unsigned long long
             const uint64_t i = (uint64_t)r * 256 + tid;
             k[r] = i < n ? __ldcs(&keys[w.begin + i]) : EMPTY_KEY;
         }
+        // a bucket list is in extraction order, so a warp almost never holds
+        // two copies of one k-mer: every thread inserts its own k-mers (no
+        // warp aggregation)
 #pragma unroll
         for (uint32_t r = 0; r < ITEM_PER_THREAD; ++r)
-            warp_insert((uint64_t)r * 256 + tid < n, k[r], tr, max_probe, &bucket_ovf[w.bucket]);
+            if ((uint64_t)r * 256 + tid < n && !table_add(tr.slots, tr.mask, k[r], 1u, max_probe))
+                atomicOr(&bucket_ovf[w.bucket], ERR_TABLE_FULL);
     }
 }
 

@@ -121,6 +121,7 @@ enum ExtractMode : int { MODE_SCAN = 0, MODE_INSERT = 1, MODE_BLOOM = 2, MODE_EM
 constexpr uint32_t WORK_ITEM_KEYS = 2048;   // k-mers per work item (8 per thread)
 constexpr uint32_t BUCKET_HLL_BITS = 10;    // HyperLogLog registers per bucket = 2^10
 constexpr uint32_t BUCKET_HLL_M = 1u << BUCKET_HLL_BITS;
+constexpr uint32_t BUCKET_HLL_SAMPLE_BITS = 6;  // the bucket registers see a 1-in-64 hash sample
 constexpr uint32_t N_BUCKETS = 256;         // root prefix = top 8 bits of the k-mer word
 
 // A run of k-mers of one root-prefix bucket processed by one block of the
