@@ -62,7 +62,10 @@ typedef struct {
     int32_t device;               /* CUDA device ordinal */
     uint32_t max_inflight_jobs;   /* jobs on the device at once (streams); 0 -> 4 */
     uint64_t hbm_budget_bytes;    /* device memory jobs may reserve; 0 -> 90% of free memory */
-    uint64_t reserved[6];
+    uint64_t workspace_bytes;     /* device workspace each worker allocates at kc_open (a server sized
+                                     for its largest job never allocates, or synchronizes the device
+                                     to grow, while jobs run); 0 -> grown to the largest job seen */
+    uint64_t reserved[5];
 } kc_config;
 
 typedef struct {

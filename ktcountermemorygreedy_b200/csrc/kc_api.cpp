@@ -94,8 +94,9 @@ struct Job {
     // results
     HostRecords recs;
     std::vector<int64_t> hist;
-    std::vector<uint64_t> top_keys, le2_keys;
-    std::vector<uint32_t> top_counts, le2_counts;
+    std::vector<uint64_t> top_keys;
+    std::vector<uint32_t> top_counts;
+    HostRecords le2;   // records with count <= 2 (pinned: often most of the records)
     uint64_t occurrences = 0, distinct = 0, low_only = 0, table_cap = 0;
     uint64_t low_len = 0, high_len = 0, input_bytes = 0, n_records_total = 0;
     double device_ms = 0;
@@ -169,6 +170,7 @@ struct Task {
 struct kc_handle {
     int device = 0;
     uint64_t budget = 0;
+    uint64_t workspace_bytes = 0;   // per worker, allocated when the worker starts
     uint64_t reserved = 0;
     uint32_t running = 0;
     bool closing = false;
@@ -695,11 +697,10 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
                                    st));
             Counters cl = read_counters(counters, st);
             uint64_t nl = std::min<uint64_t>(cl.v[C_SEL_A], n_rec);
-            job.le2_keys.resize(nl);
-            job.le2_counts.resize(nl);
+            job.le2.allocate(nl);
             if (nl) {
-                CK(cudaMemcpyAsync(job.le2_keys.data(), lk, nl * 8, cudaMemcpyDeviceToHost, st));
-                CK(cudaMemcpyAsync(job.le2_counts.data(), lc, nl * 4, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(job.le2.keys(), lk, nl * 8, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(job.le2.counts(), lc, nl * 4, cudaMemcpyDeviceToHost, st));
             }
         }
         clk.end();
@@ -782,7 +783,11 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st, Workspa
         }
     kc_input in;
     std::vector<uint32_t> tile_seg_host;
+    static const bool trace = getenv("KC_TRACE") && getenv("KC_TRACE")[0] == '1';
+    const double th0 = now_ms();
     build_input(in, files.data(), (uint32_t)files.size(), st, &ds, tile_seg_host, fsample.data());
+    if (trace) fprintf(stderr, "[kc trace] batch upload of %u files enqueued in %.3f ms\n", (uint32_t)files.size(),
+                       now_ms() - th0);
     cudaEvent_t ev0, ev1;
     CK(cudaEventCreate(&ev0));
     CK(cudaEventCreate(&ev1));
@@ -791,6 +796,7 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st, Workspa
         ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); }
     } evg{ev0, ev1};
     CK(cudaEventRecord(ev0, st));
+    PhaseClock clk(st);
 
     const uint64_t T = in.n_tiles;
     std::vector<Seg> segs = in.segs;
@@ -807,8 +813,10 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st, Workspa
     int32_t *tile_lastnl = ds.n<int32_t>(std::max<uint64_t>(T, 1));
     unsigned long long *tile_prefix = ds.n<unsigned long long>(std::max<uint64_t>(T, 1));
     unsigned long long *scan_tmp = ds.n<unsigned long long>(scan_tmp_words(std::max<uint64_t>(T, 1)));
+    clk.begin(0);
     CK(launch_newlines(in.buf, T, tile_nl, tile_lastnl, st));
     CK(launch_scan_u32(tile_nl, tile_prefix, T, scan_tmp, st));
+    clk.end();
 
     unsigned long long *occ = ds.n<unsigned long long>(n);
     uint32_t *hll = ds.n<uint32_t>((size_t)n * HLL_M);
@@ -824,7 +832,9 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st, Workspa
     a.occ = occ;
     a.hll = hll;
     a.hll_local = n == 1;
+    clk.begin(1);
     CK(launch_extract(MODE_SCAN, a, 0, st));
+    clk.end();
     std::vector<unsigned long long> occ_h(n);
     std::vector<uint32_t> hll_h((size_t)n * HLL_M);
     CK(cudaMemcpyAsync(occ_h.data(), occ, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
@@ -833,7 +843,14 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st, Workspa
     check_flags(c0.v[C_FLAGS], "scan");
 
     std::vector<uint64_t> caps(n);
-    for (uint32_t i = 0; i < n; ++i) caps[i] = table_capacity_for(hll_estimate(&hll_h[(size_t)i * HLL_M], HLL_M));
+    for (uint32_t i = 0; i < n; ++i) {
+        // one sample: exact registers; several: a 1-in-64 hash sample
+        double e = hll_estimate(&hll_h[(size_t)i * HLL_M], HLL_M);
+        if (n > 1)
+            e = std::max((double)(1u << BATCH_HLL_SAMPLE_BITS) * e, (double)std::min<unsigned long long>(occ_h[i], 4096));
+        e = std::min(e, (double)occ_h[i]);
+        caps[i] = table_capacity_for(e);
+    }
     std::vector<SampleCfg> cfg(n);
     Slot *arena = nullptr;
     uint64_t total_slots = 0;
@@ -860,7 +877,9 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st, Workspa
         CK(cudaMemsetAsync(counters, 0, 8, st));
         a.tables = d_tables;
         a.max_probe = 1u << 16;
+        clk.begin(2);
         CK(launch_extract(MODE_INSERT, a, 0, st));
+        clk.end();
         Counters c = read_counters(counters, st);
         check_flags(c.v[C_FLAGS], "insert");
         if (!(c.v[C_FLAGS] & ERR_TABLE_FULL)) break;
@@ -870,8 +889,10 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st, Workspa
     CK(cudaMemcpyAsync(d_cfg, cfg.data(), n * sizeof(SampleCfg), cudaMemcpyHostToDevice, st));
     unsigned long long *distinct = ds.n<unsigned long long>(n);
     CK(cudaMemsetAsync(distinct, 0, (size_t)n * 8, st));
+    clk.begin(5);
     CK(launch_compact_batch(arena, total_slots, d_cfg, n, nullptr, nullptr, nullptr, nullptr, nullptr, 0, distinct,
                             counters, 1, st));
+    clk.end();
     std::vector<unsigned long long> dist_h(n);
     CK(cudaMemcpyAsync(dist_h.data(), distinct, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -891,8 +912,10 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st, Workspa
     CK(cudaMemsetAsync(rec_len, 0, (size_t)n * 8, st));
     CK(cudaMemsetAsync(hist, 0, (size_t)n * HIST_BINS_BATCH * 8, st));
     CK(cudaMemsetAsync(distinct, 0, (size_t)n * 8, st));
+    clk.begin(5);
     CK(launch_compact_batch(arena, total_slots, d_cfg, n, rec_len, rec_keys, rec_counts, hist, ovf, ovf_cap, distinct,
                             counters, 0, st));
+    clk.end();
     ds.release(arena);
     std::vector<unsigned long long> len_h(n);
     CK(cudaMemcpyAsync(len_h.data(), rec_len, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
@@ -904,14 +927,17 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st, Workspa
         seg_start[i] = cfg[i].rec_base;
         seg_len[i] = len_h[i];
     }
+    clk.begin(6);
     if (total_rec > 1) {
         void *stmp = ds.get(sort_tmp_bytes_segmented(total_rec, seg_len.data(), n));
         CK(launch_radix_sort_segmented(rec_keys, rec_counts, total_rec, seg_start.data(), seg_len.data(), n, 2 * max_k,
-                                       stmp, st));
+                                       stmp, st, counters + C_FLAGS));
         ds.release(stmp);
     }
     CK(launch_pair_reverse(rec_keys, total_rec, st));
+    clk.end();
     CK(cudaEventRecord(ev1, st));
+    check_flags(read_counters(counters, st).v[C_FLAGS], "sort");
 
     std::vector<unsigned long long> hist_h((size_t)n * HIST_BINS_BATCH);
     CK(cudaMemcpyAsync(hist_h.data(), hist, hist_h.size() * 8, cudaMemcpyDeviceToHost, st));
@@ -931,12 +957,21 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st, Workspa
                                st));
         }
     }
+    const double th1 = now_ms();
     CK(cudaStreamSynchronize(st));
+    if (trace) fprintf(stderr, "[kc trace] batch results to host: %.3f ms after the last enqueue\n", now_ms() - th1);
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, ev0, ev1));
+    double phase_ms[KC_STAGES] = {0};
+    uint64_t phase_launches[KC_STAGES] = {0};
+    clk.collect(phase_ms, phase_launches, ev0);
     for (uint32_t i = 0; i < n; ++i) {
         Job &j = *jobs[i];
         j.device_ms = ms;
+        for (int q = 0; q < KC_STAGES; ++q) {
+            j.phase_ms[q] = phase_ms[q];
+            j.phase_launches[q] = phase_launches[q];
+        }
         j.occurrences = occ_h[i];
         j.distinct = dist_h[i];
         j.table_cap = caps[i];
@@ -958,6 +993,7 @@ void worker_main(kc_handle *h)
     cudaStream_t st;
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     auto ws = std::make_unique<Workspace>(st);
+    if (h->workspace_bytes) ws->reserve(h->workspace_bytes);
     for (;;) {
         std::shared_ptr<Task> task;
         {
@@ -1060,6 +1096,7 @@ int kc_open(const kc_config *cfg, kc_handle **out)
     auto *h = new kc_handle();
     h->device = dev;
     h->budget = (cfg && cfg->hbm_budget_bytes) ? cfg->hbm_budget_bytes : (uint64_t)(free_b * 0.9);
+    h->workspace_bytes = cfg ? cfg->workspace_bytes : 0;
     uint32_t nw = (cfg && cfg->max_inflight_jobs) ? cfg->max_inflight_jobs : 4;
     for (uint32_t i = 0; i < nw; ++i) h->workers.emplace_back(worker_main, h);
     *out = h;
@@ -1204,9 +1241,9 @@ int kc_result(kc_handle *h, kc_job_id id, kc_result_t *out)
     out->n_top = j.top_keys.size();
     out->top_keys = j.top_keys.data();
     out->top_counts = j.top_counts.data();
-    out->n_le2 = j.le2_keys.size();
-    out->le2_keys = j.le2_keys.data();
-    out->le2_counts = j.le2_counts.data();
+    out->n_le2 = j.le2.n;
+    out->le2_keys = j.le2.n ? j.le2.keys() : nullptr;
+    out->le2_counts = j.le2.n ? j.le2.counts() : nullptr;
     out->occurrences = j.occurrences;
     out->distinct = j.distinct;
     out->low_only = j.low_only;

@@ -77,6 +77,12 @@ void Workspace::begin_job()
     }
 }
 
+void Workspace::reserve(size_t bytes)
+{
+    high_ = std::max(high_, bytes);
+    begin_job();
+}
+
 void *Workspace::get(size_t bytes)
 {
     if (base_ && top_ + bytes <= cap_) {
@@ -160,7 +166,12 @@ PinnedPool &PinnedPool::instance()
 
 void *PinnedPool::get(size_t bytes, size_t &got)
 {
+    // sizes are rounded up to classes (powers of two from 16 MiB, 2 MiB steps
+    // below) so that blocks come back for jobs of similar size: pinning new
+    // host memory costs far more than the copy it serves
     bytes = std::max<size_t>(bytes, 4096);
+    if (bytes >= (16u << 20)) bytes = (size_t)bit_ceil64(bytes);
+    else bytes = (bytes + (2u << 20) - 1) & ~size_t((2u << 20) - 1);
     {
         std::lock_guard<std::mutex> lk(impl_->mu);
         auto it = impl_->free_blocks.lower_bound(bytes);

@@ -43,6 +43,7 @@ public:
     Workspace(const Workspace &) = delete;
     Workspace &operator=(const Workspace &) = delete;
     void begin_job();
+    void reserve(size_t bytes);   // grow the block to at least `bytes` now
     void *get(size_t bytes);
     bool release_top(void *p, size_t bytes);
     void end_job();

@@ -189,6 +189,19 @@ __device__ __forceinline__ void hll_add(uint32_t *regs, unsigned long long key)
     if (rank > *(volatile uint32_t *)&regs[r]) atomicMax(&regs[r], rank);
 }
 
+// Batched jobs keep one register set per sample in global memory, shared by
+// all blocks: only a 1-in-64 hash sample of the k-mers updates them (the host
+// scales the estimate by 64), and an update is skipped when the register
+// already holds the rank.
+__device__ __forceinline__ void hll_add_sampled(uint32_t *regs, unsigned long long key)
+{
+    uint64_t h = slot_hash(key ^ 0x5bd1e9955bd1e995ULL);
+    if (h & ((1u << BATCH_HLL_SAMPLE_BITS) - 1)) return;
+    uint32_t r = (uint32_t)(h >> (64 - HLL_BITS));
+    uint32_t rank = __clzll((h << HLL_BITS) | (1ULL << (HLL_BITS + BATCH_HLL_SAMPLE_BITS - 1))) + 1;
+    if (rank > *(volatile uint32_t *)&regs[r]) atomicMax(&regs[r], rank);
+}
+
 __device__ __forceinline__ void hll_add_shared(uint32_t *regs, unsigned long long key)
 {
     uint64_t h = slot_hash(key ^ 0x5bd1e9955bd1e995ULL);
@@ -455,7 +468,7 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
                 e &= e - 1;
                 unsigned long long key = window_key_rc(prev, cur, rprev, rcur, j, kp);
                 if (hll_local) hll_add_shared(s_hll, key);
-                else if (a.hll) hll_add(a.hll + hll_base, key);
+                else if (a.hll) hll_add_sampled(a.hll + hll_base, key);
                 if (census) atomicAdd(&s_bhist[key >> 56], 1u);
                 if ((sample_ok >> j) & 1u) atomicAdd(&s_hist[key >> 56], 1u);
             }
@@ -1039,6 +1052,16 @@ constexpr uint32_t OS_MAX_PASSES = 8;
 constexpr int LB_VALUE_BITS = 40;                                // count field of a look-back word
 constexpr unsigned long long LB_VALUE_MASK = (1ull << LB_VALUE_BITS) - 1;
 
+// With segment tiles (segmented sort), each tile belongs to one segment: the
+// look-back stops at the segment's first tile, and the digit offsets come from
+// that segment's histograms and start.
+struct OsTile {
+    uint64_t begin, end;    // key range of the tile
+    uint64_t seg_start;     // first key of the tile's segment
+    uint32_t first_tile;    // index of the segment's first tile
+    uint32_t seg;           // segment index (its histograms)
+};
+
 // Digit histograms of every pass in one read of the keys.
 __global__ void __launch_bounds__(256) k_radix_hist_all(const unsigned long long *keys, uint64_t n, uint32_t passes,
                                                         unsigned long long *hist)
@@ -1053,6 +1076,41 @@ __global__ void __launch_bounds__(256) k_radix_hist_all(const unsigned long long
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < passes * 256; i += 256)
         if (h[i]) atomicAdd(&hist[i], (unsigned long long)h[i]);
+}
+
+// Digit histograms of every pass per segment: each block takes a run of
+// consecutive tiles and adds its counts to the segment's histograms when the
+// segment changes and at the end.
+__global__ void __launch_bounds__(256) k_radix_hist_seg(const unsigned long long *keys, const OsTile *tiles,
+                                                        uint64_t n_tiles, uint64_t tiles_per_block, uint32_t passes,
+                                                        unsigned long long *hist)
+{
+    __shared__ uint32_t h[OS_MAX_PASSES * 256];
+    const uint64_t t0 = blockIdx.x * tiles_per_block;
+    const uint64_t t1 = t0 + tiles_per_block < n_tiles ? t0 + tiles_per_block : n_tiles;
+    if (t0 >= t1) return;
+    for (uint32_t i = threadIdx.x; i < OS_MAX_PASSES * 256; i += 256) h[i] = 0;
+    uint32_t seg = tiles[t0].seg;
+    __syncthreads();
+    for (uint64_t t = t0; t < t1; ++t) {
+        const OsTile tl = tiles[t];
+        if (tl.seg != seg) {
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < passes * 256; i += 256) {
+                if (h[i]) atomicAdd(&hist[(uint64_t)seg * OS_MAX_PASSES * 256 + i], (unsigned long long)h[i]);
+                h[i] = 0;
+            }
+            seg = tl.seg;
+            __syncthreads();
+        }
+        for (uint64_t i = tl.begin + threadIdx.x; i < tl.end; i += 256) {
+            const unsigned long long k = __ldcs(&keys[i]);
+            for (uint32_t p = 0; p < passes; ++p) atomicAdd(&h[p * 256 + (uint32_t)((k >> (8 * p)) & 255)], 1u);
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < passes * 256; i += 256)
+        if (h[i]) atomicAdd(&hist[(uint64_t)seg * OS_MAX_PASSES * 256 + i], (unsigned long long)h[i]);
 }
 
 // Exclusive prefix sum over the block's 256 threads of 64-bit values.
@@ -1085,7 +1143,7 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_radix_onesweep(const unsigned
                                                                   uint64_t n, uint32_t pass,
                                                                   const unsigned long long *hist,
                                                                   unsigned long long *look, unsigned int *tile_ctr,
-                                                                  unsigned long long *flags)
+                                                                  unsigned long long *flags, const OsTile *tiles)
 {
     extern __shared__ __align__(16) uint8_t rs_smem[];
     unsigned long long *s_keys = reinterpret_cast<unsigned long long *>(rs_smem);       // RS_TILE
@@ -1100,8 +1158,20 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_radix_onesweep(const unsigned
     for (int i = tid; i < 8 * 256; i += RS_THREADS) s_wcnt[i] = 0;
     __syncthreads();
     const uint64_t j = s_tile;
-    const uint64_t base = j * RS_TILE;
-    const uint32_t tile_n = (uint32_t)(n - base < RS_TILE ? n - base : RS_TILE);
+    uint64_t base, first = 0, seg_start = 0;
+    uint32_t tile_n;
+    const unsigned long long *hp = hist;
+    if (tiles) {
+        const OsTile tl = tiles[j];
+        base = tl.begin;
+        tile_n = (uint32_t)(tl.end - tl.begin);
+        first = tl.first_tile;
+        seg_start = tl.seg_start;
+        hp = hist + (uint64_t)tl.seg * OS_MAX_PASSES * 256;
+    } else {
+        base = j * RS_TILE;
+        tile_n = (uint32_t)(n - base < RS_TILE ? n - base : RS_TILE);
+    }
 
     // stable rank of every key among the tile's keys with the same digit
     unsigned long long k[RS_ITEMS];
@@ -1133,14 +1203,14 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_radix_onesweep(const unsigned
     // in the tiles before it
     const unsigned long long tag_a = 2ull * pass + 1, tag_i = 2ull * pass + 2;
     volatile unsigned long long *mine = look + j * 256 + tid;
-    *mine = ((j == 0 ? tag_i : tag_a) << LB_VALUE_BITS) | own;
+    *mine = ((j == first ? tag_i : tag_a) << LB_VALUE_BITS) | own;
     uint32_t tot;
     const uint32_t start = block_excl_scan(own, s_warp, tot);
     s_start[tid] = start;
     unsigned long long excl = 0;
-    if (j > 0) {
+    if (j > first) {
         bool gave_up = false;
-        for (int64_t p = (int64_t)j - 1; p >= 0; --p) {
+        for (int64_t p = (int64_t)j - 1; p >= (int64_t)first; --p) {
             const volatile unsigned long long *w = look + (uint64_t)p * 256 + tid;
             unsigned long long v = *w;
             uint32_t spins = 0;
@@ -1156,7 +1226,7 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_radix_onesweep(const unsigned
         if (gave_up) atomicOr(flags, ERR_WAIT_TIMEOUT);
         *mine = (tag_i << LB_VALUE_BITS) | (excl + own);
     }
-    const unsigned long long gofs = block_excl_scan64(hist[pass * 256 + tid], s_w64);
+    const unsigned long long gofs = seg_start + block_excl_scan64(hp[pass * 256 + tid], s_w64);
     s_dst[tid] = gofs + excl - start;
     __syncthreads();
     // reorder the tile by digit in shared memory, then write runs of equal
@@ -1621,12 +1691,26 @@ static uint64_t sort_tiles_for(const uint64_t *seg_len, uint32_t n_segs)
 
 static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
+// working memory of the digit-count/scan/scatter sort kept for
+// launch_radix_sort_in_scratch: second key/value arrays, per-tile digit counts
+// and offsets, the scan's temporary words and the tile descriptors
+static size_t scratch_sort_bytes(uint64_t n)
+{
+    const uint64_t n_tiles = (n + RS_TILE - 1) / RS_TILE;
+    const uint64_t nc = 256 * std::max<uint64_t>(n_tiles, 1);
+    return align256(n * 8) + align256(n * 4) + align256(nc * 4) + align256(nc * 8) + align256(scan_tmp_words(nc) * 8) +
+           align256(std::max<uint64_t>(n_tiles, 1) * sizeof(SortTile));
+}
+
+// working memory of launch_radix_sort_segmented: second key/value arrays,
+// per-segment digit histograms of all passes, the look-back words, the pass
+// tile counters and an error word, and the tile descriptors
 size_t sort_tmp_bytes_segmented(uint64_t n_total, const uint64_t *seg_len, uint32_t n_segs)
 {
-    const uint64_t n_tiles = sort_tiles_for(seg_len, n_segs);
-    const uint64_t nc = 256 * std::max<uint64_t>(n_tiles, 1);
-    return align256(n_total * 8) + align256(n_total * 4) + align256(nc * 4) + align256(nc * 8) +
-           align256(scan_tmp_words(nc) * 8) + align256(std::max<uint64_t>(n_tiles, 1) * sizeof(SortTile));
+    const uint64_t n_tiles = std::max<uint64_t>(sort_tiles_for(seg_len, n_segs), 1);
+    return align256(n_total * 8) + align256(n_total * 4) +
+           align256((uint64_t)std::max<uint32_t>(n_segs, 1) * OS_MAX_PASSES * 256 * 8) + align256(n_tiles * 256 * 8) +
+           align256(OS_MAX_PASSES * 4 + 8) + align256(n_tiles * sizeof(OsTile));
 }
 
 // working memory of launch_radix_sort: second key/value arrays, the digit
@@ -1641,71 +1725,79 @@ static size_t onesweep_tmp_bytes(uint64_t n)
 
 size_t sort_tmp_bytes(uint64_t n) { return onesweep_tmp_bytes(n); }
 
-size_t sort_tmp_bytes_in_scratch(uint64_t n) { return sort_tmp_bytes_segmented(n, &n, 1); }
+size_t sort_tmp_bytes_in_scratch(uint64_t n) { return scratch_sort_bytes(n); }
 
 // Segments [seg_start[i], seg_start[i] + seg_len[i]) of the arrays are sorted
 // independently; they must be disjoint and in increasing address order.
 cudaError_t launch_radix_sort_segmented(unsigned long long *keys, uint32_t *vals, uint64_t n_total,
                                         const uint64_t *seg_start, const uint64_t *seg_len, uint32_t n_segs,
-                                        uint32_t bits, void *tmp, cudaStream_t st)
+                                        uint32_t bits, void *tmp, cudaStream_t st, unsigned long long *flags)
 {
     const uint64_t n_tiles = sort_tiles_for(seg_len, n_segs);
     if (n_tiles == 0 || bits == 0) return cudaSuccess;
-    const uint64_t nc = 256 * n_tiles;
-    std::vector<SortTile> tiles;
+    if (bits > 64) return cudaErrorInvalidValue;
+    std::vector<OsTile> tiles;
     tiles.reserve(n_tiles);
-    uint64_t tb = 0, actual = 0;
     for (uint32_t sgi = 0; sgi < n_segs; ++sgi) {
         const uint64_t nt = (seg_len[sgi] + RS_TILE - 1) / RS_TILE;
+        const uint32_t first = (uint32_t)tiles.size();
         for (uint64_t j = 0; j < nt; ++j) {
-            SortTile t;
+            OsTile t;
             t.begin = seg_start[sgi] + j * RS_TILE;
             t.end = std::min(seg_start[sgi] + seg_len[sgi], t.begin + RS_TILE);
-            t.cbase = 256 * tb + j;
-            t.stride = nt;
-            t.adjust = seg_start[sgi] - actual;
+            t.seg_start = seg_start[sgi];
+            t.first_tile = first;
+            t.seg = sgi;
             tiles.push_back(t);
         }
-        tb += nt;
-        actual += seg_len[sgi];
     }
+    const uint32_t passes = (bits + 7) / 8;
     uint8_t *p = static_cast<uint8_t *>(tmp);
     unsigned long long *k2 = reinterpret_cast<unsigned long long *>(p);
     p += align256(n_total * 8);
     uint32_t *v2 = reinterpret_cast<uint32_t *>(p);
     p += align256(n_total * 4);
-    uint32_t *counts = reinterpret_cast<uint32_t *>(p);
-    p += align256(nc * 4);
-    unsigned long long *offs = reinterpret_cast<unsigned long long *>(p);
-    p += align256(nc * 8);
-    unsigned long long *stmp = reinterpret_cast<unsigned long long *>(p);
-    p += align256(scan_tmp_words(nc) * 8);
-    SortTile *d_tiles = reinterpret_cast<SortTile *>(p);
-    cudaError_t e = cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(SortTile), cudaMemcpyHostToDevice, st);
+    unsigned long long *hist = reinterpret_cast<unsigned long long *>(p);
+    const size_t hist_bytes = (size_t)std::max<uint32_t>(n_segs, 1) * OS_MAX_PASSES * 256 * 8;
+    p += align256(hist_bytes);
+    unsigned long long *look = reinterpret_cast<unsigned long long *>(p);
+    p += align256(n_tiles * 256 * 8);
+    unsigned int *tile_ctr = reinterpret_cast<unsigned int *>(p);
+    unsigned long long *own_flags = reinterpret_cast<unsigned long long *>(p + OS_MAX_PASSES * 4);
+    p += align256(OS_MAX_PASSES * 4 + 8);
+    OsTile *d_tiles = reinterpret_cast<OsTile *>(p);
+    if (!flags) flags = own_flags;
+    cudaError_t e = cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(OsTile), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(hist, 0, hist_bytes, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(look, 0, n_tiles * 256 * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(tile_ctr, 0, OS_MAX_PASSES * 4 + 8, st);
     if (e != cudaSuccess) return e;
-
-    const size_t smem = RS_TILE * 8 + RS_TILE * 4 + 8 * 256 * 4 + 256 * 4;
-    e = cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const uint64_t hblocks = std::min<uint64_t>(n_tiles, (uint64_t)sm_count() * 8);
+    const uint64_t per_block = (n_tiles + hblocks - 1) / hblocks;
+    note_launch();
+    k_radix_hist_seg<<<(unsigned)((n_tiles + per_block - 1) / per_block), 256, 0, st>>>(keys, d_tiles, n_tiles,
+                                                                                        per_block, passes, hist);
+    const size_t smem = RS_TILE * 8 + RS_TILE * 4 + 8 * 256 * 4;
+    e = cudaFuncSetAttribute(k_radix_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     unsigned long long *ks = keys, *kd = k2;
     uint32_t *vs = vals, *vd = v2;
-    const uint32_t passes = (bits + 7) / 8;
     for (uint32_t pass = 0; pass < passes; ++pass) {
-        const uint32_t shift = pass * 8;
         note_launch();
-        k_radix_count<<<(unsigned)n_tiles, RS_THREADS, 0, st>>>(ks, d_tiles, shift, counts);
-        e = launch_scan_u32(counts, offs, nc, stmp, st);
-        if (e != cudaSuccess) return e;
-        note_launch();
-        k_radix_scatter<<<(unsigned)n_tiles, RS_THREADS, smem, st>>>(ks, vs, kd, vd, d_tiles, shift, offs);
+        k_radix_onesweep<<<(unsigned)n_tiles, RS_THREADS, smem, st>>>(ks, vs, kd, vd, n_total, pass, hist, look,
+                                                                      tile_ctr, flags, d_tiles);
         std::swap(ks, kd);
         std::swap(vs, vd);
     }
     if (ks != keys) {
         for (uint32_t sgi = 0; sgi < n_segs; ++sgi) {
             if (!seg_len[sgi]) continue;
-            cudaMemcpyAsync(keys + seg_start[sgi], ks + seg_start[sgi], seg_len[sgi] * 8, cudaMemcpyDeviceToDevice, st);
-            cudaMemcpyAsync(vals + seg_start[sgi], vs + seg_start[sgi], seg_len[sgi] * 4, cudaMemcpyDeviceToDevice, st);
+            e = cudaMemcpyAsync(keys + seg_start[sgi], ks + seg_start[sgi], seg_len[sgi] * 8, cudaMemcpyDeviceToDevice,
+                                st);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(vals + seg_start[sgi], vs + seg_start[sgi], seg_len[sgi] * 4,
+                                    cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) return e;
         }
     }
     return cudaGetLastError();
@@ -1803,7 +1895,7 @@ cudaError_t launch_radix_sort(unsigned long long *keys, uint32_t *vals, uint64_t
     for (uint32_t pass = 0; pass < passes; ++pass) {
         note_launch();
         k_radix_onesweep<<<(unsigned)n_tiles, RS_THREADS, smem, st>>>(ks, vs, kd, vd, n, pass, hist, look, tile_ctr,
-                                                                      flags);
+                                                                      flags, nullptr);
         std::swap(ks, kd);
         std::swap(vs, vd);
     }

@@ -14,6 +14,7 @@ constexpr uint32_t EXT_THREADS = 256;   // one 32-byte segment per thread
 constexpr uint32_t STAGE_CAP = 4096;    // staged k-mers per extraction round
 constexpr uint32_t HLL_BITS = 12;       // HyperLogLog registers per sample = 2^12
 constexpr uint32_t HLL_M = 1u << HLL_BITS;
+constexpr uint32_t BATCH_HLL_SAMPLE_BITS = 6;  // batched samples' registers see a 1-in-64 hash sample
 constexpr uint32_t HIST_BINS = 1u << 16;  // dense count histogram; larger counts go to a list
 constexpr uint32_t HIST_BINS_BATCH = 4096;  // per-sample dense histogram of batched jobs
 constexpr uint32_t MAX_BATCH = 4096;        // samples in one batched job
@@ -178,7 +179,7 @@ size_t sort_tmp_bytes(uint64_t n);
 size_t sort_tmp_bytes_segmented(uint64_t n_total, const uint64_t *seg_len, uint32_t n_segs);
 cudaError_t launch_radix_sort_segmented(unsigned long long *keys, uint32_t *vals, uint64_t n_total,
                                         const uint64_t *seg_start, const uint64_t *seg_len, uint32_t n_segs,
-                                        uint32_t bits, void *tmp, cudaStream_t st);
+                                        uint32_t bits, void *tmp, cudaStream_t st, unsigned long long *flags = nullptr);
 // One segment, one kernel per 8-bit pass; a look-back wait that gave up sets
 // ERR_WAIT_TIMEOUT in *flags (NULL: a word inside tmp).
 cudaError_t launch_radix_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
