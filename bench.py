@@ -285,6 +285,109 @@ def barrier(world: int):
         dist.barrier()
 
 
+SERVED_JOB = dict(count_max=U32, min_count=1, hist_min=1, hist_max=10000, top_n=1000, want_le2=True,
+                  keep_records=False)
+
+
+def served_bench(kc, args, local):
+    """Served request stream: Poisson arrivals, log-normal job sizes (median
+    200k reads, sigma 1.5), 150 bp reads at 1% from one shared 50 Mbp genome,
+    k from {21, 25, 31}; every job returns its histogram, top-1000 and
+    count <= 2 queries.  Jobs are contiguous runs of a pool of reads drawn from
+    the genome (the pool bounds the largest job).  Each rate is measured on
+    its own stream of jobs; 'plain' is the same jobs one at a time through a
+    handle with one worker."""
+    import ctypes as C
+    import numpy as np
+    import ktcountermemorygreedy_b200.synth as S
+    from ktcountermemorygreedy_b200 import serving
+    pool_reads = args.served_pool_reads
+    g = S.genome(4, 50_000_000)
+    size = S.reads_size(4, pool_reads, (150, 150))
+    p = C.c_void_p()
+    kc._check(kc.lib().kc_host_alloc(size, C.byref(p)))
+    buf = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint8)), shape=(size,))
+    fq = S.reads(g, 4, pool_reads, (150, 150), 0.01, 0.0, out=buf)
+    nl = np.flatnonzero(fq == 10)
+    starts = np.concatenate([[0], nl[3::4] + 1]).astype(np.int64)   # byte offset of read i (and the end)
+
+    def make_requests(rate, n_jobs, seed):
+        rng = np.random.default_rng(seed)
+        t, reqs = 0.0, []
+        for _ in range(n_jobs):
+            t += float(rng.exponential(1.0 / rate))
+            n = int(min(pool_reads, max(1.0, math.exp(rng.normal(math.log(200_000), 1.5)))))
+            k = int(rng.choice([21, 25, 31]))
+            i0 = int(rng.integers(0, pool_reads - n + 1))
+            reqs.append(serving.Request(t, [fq[starts[i0]:starts[i0 + n]]], k, dict(SERVED_JOB)))
+        return reqs
+
+    # every worker's device workspace is grown to the largest job shape (the
+    # whole pool, k=21: the most k-mers) before the timed streams, as a server
+    # sized for its largest request would be
+    def warm(h, workers):
+        big = [serving.Request(0.0, [fq], 21, dict(SERVED_JOB)) for _ in range(workers)]
+        serving.serve(h, big)
+
+    out = {"workload": f"served stream: Poisson arrivals, log-normal sizes (median 200k reads, sigma 1.5, "
+                       f"capped at the {pool_reads}-read pool), 150 bp at 1% from a 50 Mbp genome, "
+                       f"k in {{21,25,31}}, histogram + top-1000 + count<=2 per job",
+           "max_inflight_jobs": args.served_inflight, "rates": {}}
+    with kc.KmerCounter(device=local, max_inflight_jobs=1) as plain:
+        warm(plain, 1)
+        reqs = make_requests(1e9, args.served_jobs, 4000)   # all at once, one worker: back to back
+        stats, wall = serving.serve(plain, reqs)
+        out["plain"] = serving.summarize(stats, wall)
+    with kc.KmerCounter(device=local, max_inflight_jobs=args.served_inflight) as srv:
+        warm(srv, args.served_inflight)
+        for rate in args.served_rates:
+            reqs = make_requests(rate, args.served_jobs, 4000 + int(rate))
+            stats, wall = serving.serve(srv, reqs)
+            out["rates"][str(rate)] = serving.summarize(stats, wall)
+    kc.lib().kc_host_free(p)
+    return out
+
+
+def batched_bench(kc, args, local):
+    """Batched samples: each sample has its own seeded 5-50 Mbp genome,
+    log-uniform read count in [1e4, 2e6] (times --batch-scale), read lengths
+    U[100, 250], substitutions U[0.5%, 2%], k = 21 / 31 alternating.  All
+    samples go to the device as one batched job (per-sample tables in one
+    arena, one extraction launch over all samples, segmented sort) and, for
+    comparison, as one job per sample through a one-worker handle.  Both
+    include the host->device upload and the records + histograms coming back
+    to pinned host memory."""
+    import ktcountermemorygreedy_b200.synth as S
+    samples = S.batch_samples(args.batch_samples, scale=args.batch_scale)
+    files = [[fq] for fq, _ in samples]
+    ks = [k for _, k in samples]
+    job = dict(count_max=U32, min_count=1, hist_min=1, hist_max=4095)
+    with kc.KmerCounter(device=local, max_inflight_jobs=1) as h:
+        h.count_batch(files, ks, copy=False, **job)          # warm-up
+        t0 = time.perf_counter()
+        res_b = h.count_batch(files, ks, copy=False, **job)
+        t_b = time.perf_counter() - t0
+        for f, k in zip(files, ks):                          # warm-up
+            h.count(f, k=k, copy=False, **job)
+        t0 = time.perf_counter()
+        res_p = [h.count(f, k=k, copy=False, **job) for f, k in zip(files, ks)]
+        t_p = time.perf_counter() - t0
+        occ = sum(r.occurrences for r in res_b)
+        dev_b = res_b[0].device_ms if res_b else 0.0
+        dev_p = sum(r.device_ms for r in res_p)
+        same = all(len(a.keys) == len(b.keys) and (a.hist == b.hist).all() and (a.counts == b.counts).all()
+                   and (a.keys == b.keys).all() for a, b in zip(res_b, res_p))
+        stages_b = {kc.PHASES[i]: res_b[0].phase_ms[i] for i in range(len(kc.PHASES)) if res_b[0].phase_ms[i] > 0}
+        del res_b, res_p
+    return {"workload": f"{len(samples)} samples, own 5-50 Mbp genomes, log-uniform 1e4-2e6 reads x "
+                        f"{args.batch_scale}, 100-250 bp, 0.5-2% errors, k=21/31",
+            "samples": len(samples), "fastq_bytes": int(sum(len(f[0]) for f in files)), "occurrences": int(occ),
+            "batched_kmers_per_s": occ / t_b, "batched_s": t_b, "batched_device_ms": dev_b,
+            "batched_stages_ms": stages_b,
+            "plain_kmers_per_s": occ / t_p, "plain_s": t_p, "plain_device_ms": dev_p,
+            "speedup_vs_plain": t_p / t_b, "identical_to_plain": bool(same)}
+
+
 def run_ours(args):
     world, rank, local = dist_setup(args)
     import numpy as np
@@ -376,6 +479,11 @@ def run_ours(args):
     counter.free_input(inp)
     counter.close()
     kc.lib().kc_host_free(pinned)
+    served = batched = None
+    if rank == 0 and world == 1 and args.served:
+        served = served_bench(kc, args, local)
+    if rank == 0 and world == 1 and args.batched:
+        batched = batched_bench(kc, args, local)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "k-mers/s", "n_gpus": world, "steps": args.steps,
@@ -389,7 +497,7 @@ def run_ours(args):
                        "memory_gb": MEMORY_GB, "scale": args.scale},
             "e2e": {"value": e2e_val, "unit": "k-mers/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": int(launches),
-            "stages": stages, "atomics": atomics,
+            "stages": stages, "atomics": atomics, "served": served, "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -407,6 +515,14 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ref-reads", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-served", dest="served", action="store_false")
+    ap.add_argument("--served-jobs", type=int, default=200)
+    ap.add_argument("--served-rates", type=float, nargs="+", default=[10.0, 50.0, 200.0])
+    ap.add_argument("--served-inflight", type=int, default=4)
+    ap.add_argument("--served-pool-reads", type=int, default=4_000_000)
+    ap.add_argument("--no-batched", dest="batched", action="store_false")
+    ap.add_argument("--batch-samples", type=int, default=256)
+    ap.add_argument("--batch-scale", type=float, default=0.125)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -363,12 +363,15 @@ class KmerCounter:
         res.hist_min = kw.get("hist_min", 1)
         return res
 
-    def count_batch(self, samples: Sequence[Sequence[bytes]], ks: Sequence[int], **kw) -> List[Result]:
+    def count_batch(self, samples: Sequence[Sequence[bytes]], ks: Sequence[int], copy: bool = True,
+                    **kw) -> List[Result]:
+        """Many samples as one batched job (``kc_submit_batch``); copy=False
+        returns each sample's records as views of pinned host memory."""
         ids = self.submit_batch(samples, ks, **kw)
         out = []
         for jid, k in zip(ids, ks):
             self.wait(jid)
-            r = self.result(jid, k)
+            r = self.result(jid, k, copy=copy)
             r.hist_min = kw.get("hist_min", 1)
             out.append(r)
         return out
