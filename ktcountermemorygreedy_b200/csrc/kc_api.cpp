@@ -887,38 +887,54 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st, Workspa
         for (auto &cp : caps) cp *= 2;
     }
     CK(cudaMemcpyAsync(d_cfg, cfg.data(), n * sizeof(SampleCfg), cudaMemcpyHostToDevice, st));
+    // compaction in chunks of slots of one sample: count the records of every
+    // chunk, scan the counts (the samples' records end up packed in sample
+    // order), then write each chunk's records at its offset
+    std::vector<uint32_t> chunk0(n + 1, 0);
+    uint64_t n_chunks = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        chunk0[i] = (uint32_t)n_chunks;
+        n_chunks += compact_chunks_of(cfg[i].slot_cap);
+    }
+    chunk0[n] = (uint32_t)n_chunks;
+    uint32_t *d_chunk0 = ds.n<uint32_t>(n + 1);
+    uint32_t *chunk_keep = ds.n<uint32_t>(std::max<uint64_t>(n_chunks, 1));
+    unsigned long long *chunk_pos = ds.n<unsigned long long>(std::max<uint64_t>(n_chunks, 1));
+    unsigned long long *ctmp = ds.n<unsigned long long>(scan_tmp_words(std::max<uint64_t>(n_chunks, 1)));
     unsigned long long *distinct = ds.n<unsigned long long>(n);
+    CK(cudaMemcpyAsync(d_chunk0, chunk0.data(), (n + 1) * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(distinct, 0, (size_t)n * 8, st));
     clk.begin(5);
-    CK(launch_compact_batch(arena, total_slots, d_cfg, n, nullptr, nullptr, nullptr, nullptr, nullptr, 0, distinct,
-                            counters, 1, st));
+    CK(launch_compact_chunks(arena, d_cfg, d_chunk0, n, n_chunks, chunk_keep, nullptr, nullptr, nullptr, nullptr,
+                             nullptr, 0, distinct, counters, 1, st));
+    CK(launch_scan_u32(chunk_keep, chunk_pos, n_chunks, ctmp, st));
     clk.end();
-    std::vector<unsigned long long> dist_h(n);
+    std::vector<unsigned long long> dist_h(n), pos_h(n_chunks);
+    uint32_t last_keep = 0;
     CK(cudaMemcpyAsync(dist_h.data(), distinct, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    uint64_t total_rec = 0;
-    for (uint32_t i = 0; i < n; ++i) {
-        cfg[i].rec_base = total_rec;
-        cfg[i].rec_cap = dist_h[i];
-        total_rec += dist_h[i];
+    if (n_chunks) {
+        CK(cudaMemcpyAsync(pos_h.data(), chunk_pos, n_chunks * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&last_keep, chunk_keep + n_chunks - 1, 4, cudaMemcpyDeviceToHost, st));
     }
-    CK(cudaMemcpyAsync(d_cfg, cfg.data(), n * sizeof(SampleCfg), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    const uint64_t total_rec = n_chunks ? pos_h[n_chunks - 1] + last_keep : 0;
+    std::vector<unsigned long long> len_h(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        cfg[i].rec_base = chunk0[i] < n_chunks ? pos_h[chunk0[i]] : total_rec;
+        const uint64_t next = chunk0[i + 1] < n_chunks ? pos_h[chunk0[i + 1]] : total_rec;
+        len_h[i] = next - cfg[i].rec_base;
+        cfg[i].rec_cap = len_h[i];
+    }
     unsigned long long *rec_keys = ds.n<unsigned long long>(std::max<uint64_t>(total_rec, 1));
     uint32_t *rec_counts = ds.n<uint32_t>(std::max<uint64_t>(total_rec, 1));
-    unsigned long long *rec_len = ds.n<unsigned long long>(n);
     unsigned long long *hist = ds.n<unsigned long long>((size_t)n * HIST_BINS_BATCH);
     const uint64_t ovf_cap = 1 << 20;
     unsigned long long *ovf = ds.n<unsigned long long>(ovf_cap);
-    CK(cudaMemsetAsync(rec_len, 0, (size_t)n * 8, st));
     CK(cudaMemsetAsync(hist, 0, (size_t)n * HIST_BINS_BATCH * 8, st));
-    CK(cudaMemsetAsync(distinct, 0, (size_t)n * 8, st));
     clk.begin(5);
-    CK(launch_compact_batch(arena, total_slots, d_cfg, n, rec_len, rec_keys, rec_counts, hist, ovf, ovf_cap, distinct,
-                            counters, 0, st));
+    CK(launch_compact_chunks(arena, d_cfg, d_chunk0, n, n_chunks, chunk_keep, chunk_pos, rec_keys, rec_counts, hist,
+                             ovf, ovf_cap, nullptr, counters, 0, st));
     clk.end();
-    ds.release(arena);
-    std::vector<unsigned long long> len_h(n);
-    CK(cudaMemcpyAsync(len_h.data(), rec_len, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
     Counters c2 = read_counters(counters, st);
     check_flags(c2.v[C_FLAGS], "compact");
 
@@ -930,8 +946,10 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st, Workspa
     clk.begin(6);
     if (total_rec > 1) {
         void *stmp = ds.get(sort_tmp_bytes_segmented(total_rec, seg_len.data(), n));
+        std::vector<uint32_t> seg_bits(n);
+        for (uint32_t i = 0; i < n; ++i) seg_bits[i] = 2 * cfg[i].k;
         CK(launch_radix_sort_segmented(rec_keys, rec_counts, total_rec, seg_start.data(), seg_len.data(), n, 2 * max_k,
-                                       stmp, st, counters + C_FLAGS));
+                                       stmp, st, counters + C_FLAGS, seg_bits.data()));
         ds.release(stmp);
     }
     CK(launch_pair_reverse(rec_keys, total_rec, st));

@@ -12,6 +12,8 @@
 #include <map>
 #include <mutex>
 
+#include <unistd.h>
+
 #include "kc_plan.h"
 
 namespace kc {
@@ -91,7 +93,9 @@ void *Workspace::get(size_t bytes)
         high_ = std::max(high_, top_);
         return p;
     }
-    high_ = std::max(high_, top_ + bytes);
+    // the job needs all of the workspace in use plus everything it spilled
+    spilled_ += bytes;
+    high_ = std::max(high_, top_ + spilled_);
     void *p = pool_alloc(bytes, st_);
     spill_.push_back(p);
     return p;
@@ -110,6 +114,7 @@ void Workspace::end_job()
 {
     for (void *p : spill_) cudaFreeAsync(p, st_);
     spill_.clear();
+    spilled_ = 0;
     top_ = 0;
 }
 
@@ -166,16 +171,20 @@ PinnedPool &PinnedPool::instance()
 
 void *PinnedPool::get(size_t bytes, size_t &got)
 {
-    // sizes are rounded up to classes (powers of two from 16 MiB, 2 MiB steps
-    // below) so that blocks come back for jobs of similar size: pinning new
-    // host memory costs far more than the copy it serves
+    // sizes are rounded up to classes (eight per power of two from 16 MiB,
+    // 2 MiB steps below) so that blocks come back for jobs of similar size:
+    // pinning new host memory costs far more than the copy it serves
     bytes = std::max<size_t>(bytes, 4096);
-    if (bytes >= (16u << 20)) bytes = (size_t)bit_ceil64(bytes);
-    else bytes = (bytes + (2u << 20) - 1) & ~size_t((2u << 20) - 1);
+    if (bytes >= (16u << 20)) {
+        const size_t step = (size_t)bit_ceil64(bytes) / 16;
+        bytes = (bytes + step - 1) / step * step;
+    } else {
+        bytes = (bytes + (2u << 20) - 1) & ~size_t((2u << 20) - 1);
+    }
     {
         std::lock_guard<std::mutex> lk(impl_->mu);
         auto it = impl_->free_blocks.lower_bound(bytes);
-        if (it != impl_->free_blocks.end() && it->first <= 2 * bytes + (64u << 20)) {
+        if (it != impl_->free_blocks.end() && it->first <= bytes + bytes / 4 + (64u << 20)) {
             void *p = it->second;
             got = it->first;
             impl_->cached -= got;
@@ -196,7 +205,12 @@ void *PinnedPool::get(size_t bytes, size_t &got)
 void PinnedPool::put(void *p, size_t bytes)
 {
     if (!p) return;
-    const size_t keep_limit = 32ULL << 30;
+    // keep up to a third of the host's memory pinned for reuse
+    static const size_t keep_limit = [] {
+        const long pages = sysconf(_SC_PHYS_PAGES), page = sysconf(_SC_PAGE_SIZE);
+        const size_t phys = (pages > 0 && page > 0) ? (size_t)pages * (size_t)page : (size_t(96) << 30);
+        return std::max<size_t>(phys / 3, size_t(8) << 30);
+    }();
     {
         std::lock_guard<std::mutex> lk(impl_->mu);
         if (impl_->cached + bytes <= keep_limit) {

@@ -54,6 +54,7 @@ private:
     cudaStream_t st_;
     uint8_t *base_ = nullptr;
     size_t cap_ = 0, top_ = 0, high_ = 0;
+    size_t spilled_ = 0;   // bytes of this job's blocks taken from the pool
     std::vector<void *> spill_;
 };
 

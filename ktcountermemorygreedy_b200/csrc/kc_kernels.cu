@@ -776,75 +776,109 @@ __global__ void __launch_bounds__(256) k_compact(TableRef t, uint64_t cap, uint3
 }
 
 // Batched jobs keep all samples' tables in one slot arena.  Sample s owns
-// slots [slot_base, slot_base + slot_cap).
-__device__ __forceinline__ uint32_t sample_of_slot(const unsigned long long *s_base, uint32_t n, uint64_t i)
+// slots [slot_base, slot_base + slot_cap), cut into chunks of COMPACT_CHUNK
+// slots; chunk0[s] is the index of its first chunk (chunk0[n] = all chunks),
+// so every chunk belongs to one sample.
+constexpr uint32_t COMPACT_CHUNK = 4096;
+
+__device__ __forceinline__ uint32_t sample_of_chunk(const uint32_t *s_chunk0, uint32_t n, uint64_t c)
 {
-    uint32_t lo = 0, hi = n;   // last sample with base <= i
+    uint32_t lo = 0, hi = n;   // last sample whose first chunk is <= c
     while (hi - lo > 1) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (s_base[mid] <= i) lo = mid; else hi = mid;
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_chunk0[mid] <= c) lo = mid; else hi = mid;
     }
     return lo;
 }
 
-__global__ void __launch_bounds__(256) k_compact_batch(const Slot *slots, uint64_t total, const SampleCfg *cfg,
-                                                       uint32_t n_samples, unsigned long long *rec_len,
-                                                       unsigned long long *rec_keys, uint32_t *rec_counts,
-                                                       unsigned long long *hist, unsigned long long *ovf,
-                                                       uint64_t ovf_cap, unsigned long long *distinct,
-                                                       unsigned long long *counters, int count_only)
+// count_only: chunk_keep[c] = records chunk c keeps, distinct[s] += its
+// occupied slots.  Otherwise chunk c writes its records from
+// rec_keys[chunk_pos[c]] on (chunk_pos = exclusive scan of chunk_keep, so the
+// samples' records are packed one after the other in sample order) and adds
+// its counts to the sample's histogram through a shared-memory histogram.
+__global__ void __launch_bounds__(256) k_compact_chunks(const Slot *slots, const SampleCfg *cfg,
+                                                        const uint32_t *chunk0, uint32_t n_samples,
+                                                        uint64_t n_chunks, uint32_t *chunk_keep,
+                                                        const unsigned long long *chunk_pos,
+                                                        unsigned long long *rec_keys, uint32_t *rec_counts,
+                                                        unsigned long long *hist, unsigned long long *ovf,
+                                                        uint64_t ovf_cap, unsigned long long *distinct,
+                                                        unsigned long long *counters, int count_only)
 {
-    extern __shared__ unsigned long long s_base[];
-    for (uint32_t i = threadIdx.x; i < n_samples; i += blockDim.x) s_base[i] = cfg[i].slot_base;
+    extern __shared__ uint32_t s_chunk0[];   // n_samples + 1
+    __shared__ uint32_t s_hist[2048];
+    __shared__ uint32_t s_warp[8];
+    __shared__ uint32_t s_red[2][8];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (uint32_t i = tid; i <= n_samples; i += 256) s_chunk0[i] = chunk0[i];
+    for (uint32_t i = tid; i < 2048; i += 256) s_hist[i] = 0;
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    const uint64_t rounds = (total + stride - 1) / stride;
-    for (uint64_t r = 0; r < rounds; ++r) {
-        const uint64_t i = r * stride + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-        bool present = false, keep = false;
-        uint32_t smp = 0, c = 0;
-        unsigned long long key = EMPTY_KEY;
-        if (i < total) {
-            key = __ldcg(&slots[i].key);
-            if (key != EMPTY_KEY) {
-                present = true;
-                smp = sample_of_slot(s_base, n_samples, i);
-                const SampleCfg sc = cfg[smp];
-                c = slots[i].count < sc.count_max ? slots[i].count : sc.count_max;
-                keep = c >= sc.min_count && c <= sc.max_count;
+    for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
+        const uint32_t smp = sample_of_chunk(s_chunk0, n_samples, c);
+        const SampleCfg sc = cfg[smp];
+        const uint64_t lo = sc.slot_base + (c - s_chunk0[smp]) * COMPACT_CHUNK;
+        const uint64_t end = sc.slot_base + sc.slot_cap;
+        const uint64_t hi = lo + COMPACT_CHUNK < end ? lo + COMPACT_CHUNK : end;
+        if (count_only) {
+            uint32_t present = 0, keep = 0;
+            for (uint64_t i = lo + tid; i < hi; i += 256) {
+                const Slot sl = slots[i];
+                if (sl.key == EMPTY_KEY) continue;
+                ++present;
+                const uint32_t cnt = sl.count < sc.count_max ? sl.count : sc.count_max;
+                keep += (cnt >= sc.min_count && cnt <= sc.max_count);
+            }
+            present = __reduce_add_sync(FULL, present);
+            keep = __reduce_add_sync(FULL, keep);
+            if (lane == 0) { s_red[0][warp] = present; s_red[1][warp] = keep; }
+            __syncthreads();
+            if (tid == 0) {
+                uint32_t p = 0, k = 0;
+                for (int w = 0; w < 8; ++w) { p += s_red[0][w]; k += s_red[1][w]; }
+                chunk_keep[c] = k;
+                if (p) atomicAdd(&distinct[smp], (unsigned long long)p);
+            }
+            __syncthreads();
+            continue;
+        }
+        unsigned long long run = chunk_pos[c];
+        for (uint64_t base = lo; base < hi; base += 256) {
+            const uint64_t i = base + tid;
+            bool keep = false;
+            uint32_t cnt = 0;
+            unsigned long long key = EMPTY_KEY;
+            if (i < hi) {
+                const Slot sl = slots[i];
+                key = sl.key;
+                if (key != EMPTY_KEY) {
+                    cnt = sl.count < sc.count_max ? sl.count : sc.count_max;
+                    if (cnt < 2048) atomicAdd(&s_hist[cnt], 1u);
+                    else if (cnt < HIST_BINS_BATCH) atomicAdd(&hist[(uint64_t)smp * HIST_BINS_BATCH + cnt], 1ull);
+                    else {
+                        const unsigned long long p = atomicAdd(&counters[C_OVF_LEN], 1ull);
+                        if (p < ovf_cap) ovf[p] = ((unsigned long long)smp << 32) | cnt;
+                        else atomicOr(&counters[C_FLAGS], ERR_HIST_OVERFLOW_FULL);
+                    }
+                    keep = cnt >= sc.min_count && cnt <= sc.max_count;
+                }
+            }
+            uint32_t tot;
+            const uint32_t off = block_excl_scan(keep ? 1u : 0u, s_warp, tot);
+            if (keep) {
+                rec_keys[run + off] = pair_reverse(key);
+                rec_counts[run + off] = cnt;
+            }
+            run += tot;
+        }
+        __syncthreads();
+        for (uint32_t b = tid; b < 2048; b += 256) {
+            const uint32_t v = s_hist[b];
+            if (v) {
+                atomicAdd(&hist[(uint64_t)smp * HIST_BINS_BATCH + b], (unsigned long long)v);
+                s_hist[b] = 0;
             }
         }
-        // per-sample warp aggregation of the distinct count
-        uint32_t tag = present ? smp : 0xffffffffu;
-        uint32_t peers = __match_any_sync(FULL, tag);
-        int leader = __ffs(peers) - 1;
-        if (present && lane == leader) atomicAdd(&distinct[smp], (unsigned long long)__popc(peers));
-        if (count_only) continue;
-        if (present) {
-            if (c < HIST_BINS_BATCH) atomicAdd(&hist[(uint64_t)smp * HIST_BINS_BATCH + c], 1ull);
-            else {
-                unsigned long long p = atomicAdd(&counters[C_OVF_LEN], 1ull);
-                if (p < ovf_cap) ovf[p] = ((unsigned long long)smp << 32) | c;
-                else atomicOr(&counters[C_FLAGS], ERR_HIST_OVERFLOW_FULL);
-            }
-        }
-        tag = keep ? smp : 0xffffffffu;
-        peers = __match_any_sync(FULL, tag);
-        leader = __ffs(peers) - 1;
-        unsigned long long b = 0;
-        if (keep && lane == leader) b = atomicAdd(&rec_len[smp], (unsigned long long)__popc(peers));
-        b = __shfl_sync(FULL, b, leader);
-        if (keep) {
-            const SampleCfg sc = cfg[smp];
-            unsigned long long pos = b + __popc(peers & lanemask_lt());
-            if (pos < sc.rec_cap) {
-                rec_keys[sc.rec_base + pos] = pair_reverse(key);
-                rec_counts[sc.rec_base + pos] = c;
-            } else {
-                atomicOr(&counters[C_FLAGS], ERR_RECORDS_FULL);
-            }
-        }
+        __syncthreads();
     }
 }
 
@@ -1060,6 +1094,8 @@ struct OsTile {
     uint64_t seg_start;     // first key of the tile's segment
     uint32_t first_tile;    // index of the segment's first tile
     uint32_t seg;           // segment index (its histograms)
+    uint32_t passes;        // 8-bit passes the segment needs (it sits out later ones)
+    uint32_t pad;
 };
 
 // Digit histograms of every pass in one read of the keys.
@@ -1103,9 +1139,18 @@ __global__ void __launch_bounds__(256) k_radix_hist_seg(const unsigned long long
             seg = tl.seg;
             __syncthreads();
         }
-        for (uint64_t i = tl.begin + threadIdx.x; i < tl.end; i += 256) {
-            const unsigned long long k = __ldcs(&keys[i]);
-            for (uint32_t p = 0; p < passes; ++p) atomicAdd(&h[p * 256 + (uint32_t)((k >> (8 * p)) & 255)], 1u);
+        // lanes with the same digit add once (the high digits of short keys
+        // are all zero, and 32 lanes adding to one bin would serialize)
+        const uint32_t np = tl.passes < passes ? tl.passes : passes;
+        for (uint64_t b = tl.begin; b < tl.end; b += 256) {
+            const uint64_t i = b + threadIdx.x;
+            const bool act = i < tl.end;
+            const unsigned long long k = act ? __ldcs(&keys[i]) : 0;
+            for (uint32_t p = 0; p < np; ++p) {
+                const uint32_t d = act ? (uint32_t)((k >> (8 * p)) & 255) : 256u;
+                const uint32_t peers = __match_any_sync(FULL, d);
+                if (act && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&h[p * 256 + d], __popc(peers));
+            }
         }
     }
     __syncthreads();
@@ -1168,6 +1213,7 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_radix_onesweep(const unsigned
         first = tl.first_tile;
         seg_start = tl.seg_start;
         hp = hist + (uint64_t)tl.seg * OS_MAX_PASSES * 256;
+        if (pass >= tl.passes) return;   // the segment is sorted already (no tile of it waits or is waited on)
     } else {
         base = j * RS_TILE;
         tile_n = (uint32_t)(n - base < RS_TILE ? n - base : RS_TILE);
@@ -1729,18 +1775,39 @@ size_t sort_tmp_bytes_in_scratch(uint64_t n) { return scratch_sort_bytes(n); }
 
 // Segments [seg_start[i], seg_start[i] + seg_len[i]) of the arrays are sorted
 // independently; they must be disjoint and in increasing address order.
+// Consecutive segments are sorted in groups of about SORT_GROUP_RECORDS
+// records, every pass of a group before the next group, so that a group's
+// keys and values stay in L2 across its passes.
+constexpr uint64_t SORT_GROUP_RECORDS = 4ull << 20;   // 48 MiB of keys + values
+
 cudaError_t launch_radix_sort_segmented(unsigned long long *keys, uint32_t *vals, uint64_t n_total,
                                         const uint64_t *seg_start, const uint64_t *seg_len, uint32_t n_segs,
-                                        uint32_t bits, void *tmp, cudaStream_t st, unsigned long long *flags)
+                                        uint32_t bits, void *tmp, cudaStream_t st, unsigned long long *flags,
+                                        const uint32_t *seg_bits)
 {
     const uint64_t n_tiles = sort_tiles_for(seg_len, n_segs);
     if (n_tiles == 0 || bits == 0) return cudaSuccess;
     if (bits > 64) return cudaErrorInvalidValue;
+    // groups of whole segments; a tile's first_tile is relative to its group
+    struct Group {
+        uint64_t t0, t1;
+        uint32_t passes;
+    };
+    std::vector<Group> groups;
     std::vector<OsTile> tiles;
     tiles.reserve(n_tiles);
+    uint64_t group_records = 0;
     for (uint32_t sgi = 0; sgi < n_segs; ++sgi) {
         const uint64_t nt = (seg_len[sgi] + RS_TILE - 1) / RS_TILE;
-        const uint32_t first = (uint32_t)tiles.size();
+        if (!nt) continue;
+        const uint32_t b = seg_bits ? std::min(seg_bits[sgi], bits) : bits;
+        const uint32_t sp = (b + 7) / 8;
+        if (groups.empty() || group_records + seg_len[sgi] > SORT_GROUP_RECORDS) {
+            groups.push_back(Group{tiles.size(), tiles.size(), 0});
+            group_records = 0;
+        }
+        Group &g = groups.back();
+        const uint32_t first = (uint32_t)(tiles.size() - g.t0);
         for (uint64_t j = 0; j < nt; ++j) {
             OsTile t;
             t.begin = seg_start[sgi] + j * RS_TILE;
@@ -1748,10 +1815,14 @@ cudaError_t launch_radix_sort_segmented(unsigned long long *keys, uint32_t *vals
             t.seg_start = seg_start[sgi];
             t.first_tile = first;
             t.seg = sgi;
+            t.passes = sp;
+            t.pad = 0;
             tiles.push_back(t);
         }
+        g.t1 = tiles.size();
+        g.passes = std::max(g.passes, sp);
+        group_records += seg_len[sgi];
     }
-    const uint32_t passes = (bits + 7) / 8;
     uint8_t *p = static_cast<uint8_t *>(tmp);
     unsigned long long *k2 = reinterpret_cast<unsigned long long *>(p);
     p += align256(n_total * 8);
@@ -1770,35 +1841,40 @@ cudaError_t launch_radix_sort_segmented(unsigned long long *keys, uint32_t *vals
     cudaError_t e = cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(OsTile), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(hist, 0, hist_bytes, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(look, 0, n_tiles * 256 * 8, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(tile_ctr, 0, OS_MAX_PASSES * 4 + 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(own_flags, 0, 8, st);
     if (e != cudaSuccess) return e;
-    const uint64_t hblocks = std::min<uint64_t>(n_tiles, (uint64_t)sm_count() * 8);
-    const uint64_t per_block = (n_tiles + hblocks - 1) / hblocks;
-    note_launch();
-    k_radix_hist_seg<<<(unsigned)((n_tiles + per_block - 1) / per_block), 256, 0, st>>>(keys, d_tiles, n_tiles,
-                                                                                        per_block, passes, hist);
     const size_t smem = RS_TILE * 8 + RS_TILE * 4 + 8 * 256 * 4;
     e = cudaFuncSetAttribute(k_radix_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    unsigned long long *ks = keys, *kd = k2;
-    uint32_t *vs = vals, *vd = v2;
-    for (uint32_t pass = 0; pass < passes; ++pass) {
+    for (const Group &g : groups) {
+        const uint64_t gt = g.t1 - g.t0;
+        e = cudaMemsetAsync(tile_ctr, 0, OS_MAX_PASSES * 4, st);
+        if (e != cudaSuccess) return e;
+        const uint64_t hblocks = std::min<uint64_t>(gt, (uint64_t)sm_count() * 8);
+        const uint64_t per_block = (gt + hblocks - 1) / hblocks;
         note_launch();
-        k_radix_onesweep<<<(unsigned)n_tiles, RS_THREADS, smem, st>>>(ks, vs, kd, vd, n_total, pass, hist, look,
-                                                                      tile_ctr, flags, d_tiles);
-        std::swap(ks, kd);
-        std::swap(vs, vd);
-    }
-    if (ks != keys) {
-        for (uint32_t sgi = 0; sgi < n_segs; ++sgi) {
-            if (!seg_len[sgi]) continue;
-            e = cudaMemcpyAsync(keys + seg_start[sgi], ks + seg_start[sgi], seg_len[sgi] * 8, cudaMemcpyDeviceToDevice,
-                                st);
-            if (e == cudaSuccess)
-                e = cudaMemcpyAsync(vals + seg_start[sgi], vs + seg_start[sgi], seg_len[sgi] * 4,
-                                    cudaMemcpyDeviceToDevice, st);
-            if (e != cudaSuccess) return e;
+        k_radix_hist_seg<<<(unsigned)((gt + per_block - 1) / per_block), 256, 0, st>>>(keys, d_tiles + g.t0, gt,
+                                                                                         per_block, g.passes, hist);
+        unsigned long long *ks = keys, *kd = k2;
+        uint32_t *vs = vals, *vd = v2;
+        for (uint32_t pass = 0; pass < g.passes; ++pass) {
+            note_launch();
+            k_radix_onesweep<<<(unsigned)gt, RS_THREADS, smem, st>>>(ks, vs, kd, vd, n_total, pass, hist,
+                                                                     look + g.t0 * 256, tile_ctr, flags,
+                                                                     d_tiles + g.t0);
+            std::swap(ks, kd);
+            std::swap(vs, vd);
         }
+    }
+    // a segment that took an odd number of passes ends in the second arrays
+    for (uint32_t sgi = 0; sgi < n_segs; ++sgi) {
+        const uint32_t b = seg_bits ? std::min(seg_bits[sgi], bits) : bits;
+        if (!seg_len[sgi] || ((b + 7) / 8) % 2 == 0) continue;
+        e = cudaMemcpyAsync(keys + seg_start[sgi], k2 + seg_start[sgi], seg_len[sgi] * 8, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(vals + seg_start[sgi], v2 + seg_start[sgi], seg_len[sgi] * 4, cudaMemcpyDeviceToDevice,
+                                st);
+        if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();
 }
@@ -1907,20 +1983,23 @@ cudaError_t launch_radix_sort(unsigned long long *keys, uint32_t *vals, uint64_t
     return cudaGetLastError();
 }
 
-cudaError_t launch_compact_batch(const Slot *slots, uint64_t total, const SampleCfg *cfg, uint32_t n_samples,
-                                 unsigned long long *rec_len, unsigned long long *rec_keys, uint32_t *rec_counts,
-                                 unsigned long long *hist, unsigned long long *ovf, uint64_t ovf_cap,
-                                 unsigned long long *distinct, unsigned long long *counters, int count_only,
-                                 cudaStream_t st)
+uint64_t compact_chunks_of(uint64_t slot_cap) { return (slot_cap + COMPACT_CHUNK - 1) / COMPACT_CHUNK; }
+
+cudaError_t launch_compact_chunks(const Slot *slots, const SampleCfg *cfg, const uint32_t *chunk0, uint32_t n_samples,
+                                  uint64_t n_chunks, uint32_t *chunk_keep, const unsigned long long *chunk_pos,
+                                  unsigned long long *rec_keys, uint32_t *rec_counts, unsigned long long *hist,
+                                  unsigned long long *ovf, uint64_t ovf_cap, unsigned long long *distinct,
+                                  unsigned long long *counters, int count_only, cudaStream_t st)
 {
-    if (!total || !n_samples) return cudaSuccess;
-    size_t smem = (size_t)n_samples * 8;
-    cudaError_t e = cudaFuncSetAttribute(k_compact_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (!n_chunks || !n_samples) return cudaSuccess;
+    const size_t smem = ((size_t)n_samples + 1) * 4;
+    cudaError_t e = cudaFuncSetAttribute(k_compact_chunks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    const uint64_t grid = std::min<uint64_t>(n_chunks, (uint64_t)sm_count() * 8);
     note_launch();
-    k_compact_batch<<<grid_for(total, 256, 4), 256, smem, st>>>(slots, total, cfg, n_samples, rec_len, rec_keys,
-                                                                rec_counts, hist, ovf, ovf_cap, distinct, counters,
-                                                                count_only);
+    k_compact_chunks<<<(unsigned)grid, 256, smem, st>>>(slots, cfg, chunk0, n_samples, n_chunks, chunk_keep, chunk_pos,
+                                                         rec_keys, rec_counts, hist, ovf, ovf_cap, distinct, counters,
+                                                         count_only);
     return cudaGetLastError();
 }
 

@@ -179,17 +179,24 @@ size_t sort_tmp_bytes(uint64_t n);
 size_t sort_tmp_bytes_segmented(uint64_t n_total, const uint64_t *seg_len, uint32_t n_segs);
 cudaError_t launch_radix_sort_segmented(unsigned long long *keys, uint32_t *vals, uint64_t n_total,
                                         const uint64_t *seg_start, const uint64_t *seg_len, uint32_t n_segs,
-                                        uint32_t bits, void *tmp, cudaStream_t st, unsigned long long *flags = nullptr);
+                                        uint32_t bits, void *tmp, cudaStream_t st, unsigned long long *flags = nullptr,
+                                        const uint32_t *seg_bits = nullptr);   // per segment, <= bits
 // One segment, one kernel per 8-bit pass; a look-back wait that gave up sets
 // ERR_WAIT_TIMEOUT in *flags (NULL: a word inside tmp).
 cudaError_t launch_radix_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
                               cudaStream_t st, unsigned long long *flags = nullptr);
 
-cudaError_t launch_compact_batch(const Slot *slots, uint64_t total, const SampleCfg *cfg, uint32_t n_samples,
-                                 unsigned long long *rec_len, unsigned long long *rec_keys, uint32_t *rec_counts,
-                                 unsigned long long *hist, unsigned long long *ovf, uint64_t ovf_cap,
-                                 unsigned long long *distinct, unsigned long long *counters, int count_only,
-                                 cudaStream_t st);
+// Compaction of a batched job's slot arena in chunks of slots that each
+// belong to one sample: count_only fills chunk_keep (records per chunk) and
+// distinct (per sample); the write pass puts chunk c's records at
+// chunk_pos[c] (the exclusive scan of chunk_keep) and fills the per-sample
+// histograms.  chunk0 has n_samples + 1 entries: first chunk of each sample.
+uint64_t compact_chunks_of(uint64_t slot_cap);
+cudaError_t launch_compact_chunks(const Slot *slots, const SampleCfg *cfg, const uint32_t *chunk0, uint32_t n_samples,
+                                  uint64_t n_chunks, uint32_t *chunk_keep, const unsigned long long *chunk_pos,
+                                  unsigned long long *rec_keys, uint32_t *rec_counts, unsigned long long *hist,
+                                  unsigned long long *ovf, uint64_t ovf_cap, unsigned long long *distinct,
+                                  unsigned long long *counters, int count_only, cudaStream_t st);
 // A sort of one segment with every buffer, tile descriptors included, taken
 // from tmp (sort_tmp_bytes_in_scratch(n) bytes) and nothing copied from the
 // host (digit counts, a scan and a scatter per pass).

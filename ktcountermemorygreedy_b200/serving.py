@@ -37,6 +37,7 @@ class RequestStats:
     queue_ms: float                  # submission -> start on a worker
     run_ms: float                    # start -> end
     submit_late_ms: float            # actual submission - scheduled arrival
+    device_ms: float                 # device time of the job's pipeline
     occurrences: int
     distinct: int
     n_le2: int
@@ -76,17 +77,18 @@ def serve(counter, requests: Sequence[Request]):
         submitted[i].wait()
         r = requests[i]
         if errors[i]:
-            stats[i] = RequestStats(math.nan, 0, 0, late[i], 0, 0, 0, 0, errors[i])
+            stats[i] = RequestStats(math.nan, 0, 0, late[i], 0, 0, 0, 0, 0, errors[i])
             continue
         try:
             counter.wait(ids[i])
             res = counter.result(ids[i], r.k, copy=False)
         except Exception as e:
-            stats[i] = RequestStats(math.nan, 0, 0, late[i], 0, 0, 0, 0, str(e))
+            stats[i] = RequestStats(math.nan, 0, 0, late[i], 0, 0, 0, 0, 0, str(e))
             continue
         lat = late[i] + res.queue_ms + res.run_ms
         end_max = max(end_max, r.arrival_s * 1000.0 + lat)
-        stats[i] = RequestStats(lat, res.queue_ms, res.run_ms, late[i], int(res.occurrences), int(res.distinct),
+        stats[i] = RequestStats(lat, res.queue_ms, res.run_ms, late[i], res.device_ms, int(res.occurrences),
+                                int(res.distinct),
                                 int(len(res.le2_keys)), int(np.asarray(res.hist).sum()))
         del res
     th.join()
@@ -102,4 +104,5 @@ def summarize(stats: Sequence[RequestStats], wall_s: float) -> dict:
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_ms": float(lat.mean()), "kmers_per_s": occ / wall_s, "wall_s": wall_s, "occurrences": occ,
             "mean_queue_ms": float(np.mean([s.queue_ms for s in ok])) if ok else 0.0,
-            "mean_run_ms": float(np.mean([s.run_ms for s in ok])) if ok else 0.0}
+            "mean_run_ms": float(np.mean([s.run_ms for s in ok])) if ok else 0.0,
+            "mean_device_ms": float(np.mean([s.device_ms for s in ok])) if ok else 0.0}

@@ -210,6 +210,27 @@ def test_batch_matches_oracle(counter):
         assert r.hist.tolist() == O.histogram(want_c, 1, 10000).tolist()
 
 
+def test_batch_spanning_several_sort_groups_matches_single_jobs(counter):
+    """A batch of more than 4M records is sorted in several groups of
+    samples; each sample (k = 21, 25 and 31 mixed, so the samples take 6, 7
+    and 8 radix passes) must equal the same sample counted alone, and the
+    per-sample totals must add up."""
+    import ktcountermemorygreedy_b200.synth as S
+    samples, ks = [], []
+    for i in range(7):
+        g = S.genome(7000 + i, 3_000_000)
+        samples.append([S.reads(g, 7000 + i, 12_000 + 1000 * i, (150, 150), 0.02, 0.0)])
+        ks.append([21, 25, 31][i % 3])
+    res = counter.count_batch(samples, ks, count_max=U32, hist_max=4095)
+    assert sum(len(r.keys) for r in res) > (4 << 20)
+    for files, k, r in zip(samples, ks, res):
+        one = counter.count(files, k=k, count_max=U32, hist_max=4095)
+        assert np.array_equal(r.keys, one.keys), k
+        assert np.array_equal(r.counts, one.counts), k
+        assert np.array_equal(r.hist, one.hist), k
+        assert r.occurrences == one.occurrences
+
+
 def test_jobs_same_alone_and_in_the_mix(kc):
     jobs = []
     for i in range(12):

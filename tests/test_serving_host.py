@@ -52,6 +52,7 @@ class FakeCounter:
     def result(self, jid, k, copy=True):
         r = self.jobs[jid]
         return SimpleNamespace(queue_ms=1000 * (r["t_start"] - r["t_sub"]), run_ms=1000 * (r["t_end"] - r["t_start"]),
+                               device_ms=self.service_ms,
                                occurrences=r["n"], distinct=r["n"] // 2, le2_keys=np.zeros(3, np.uint64),
                                hist=np.array([1, 2, 3]))
 
