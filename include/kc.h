@@ -122,8 +122,9 @@ typedef struct {
      * [9..11] unused */
     double phase_ms[KC_STAGES];
     uint64_t phase_launches[KC_STAGES];   /* kernel launches per stage */
-    uint64_t low_len;             /* Bloom mode: FIRST occurrences */
-    uint64_t high_len;            /* Bloom mode: other occurrences */
+    uint64_t low_len;             /* Bloom mode: FIRST occurrences (merged after the inserts) */
+    uint64_t high_len;            /* occurrences inserted into root-prefix bucket tables (Bloom mode:
+                                     the non-FIRST ones; large plain jobs: all); 0 for one table */
     uint64_t input_bytes;         /* FASTQ bytes of the job */
     uint64_t n_records_total;     /* records on the device (also when keep_records = 0) */
 } kc_result_t;

@@ -63,6 +63,10 @@ double hll_estimate(const uint32_t *regs, uint32_t m)
     return e;
 }
 
+// A plain job whose table would hold more slots than this (64 MiB of slots,
+// half of L2) is counted through the root-prefix buckets.
+constexpr uint64_t PLAIN_PART_MIN_SLOTS = 1ull << 22;
+
 uint64_t table_capacity_for(double est)
 {
     uint64_t want = (uint64_t)std::ceil(std::max(est, 16.0) * 1.8);
@@ -332,6 +336,13 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
         a.seg_chunk0 = d_chunk0;
         a.prefix_hist = prefix_hist;
         a.qual = qual;
+    } else {
+        // plain jobs: an exact root-prefix census beside the distinct
+        // estimate, for the partitioned path of large tables
+        bucket_hist = ds.n<unsigned long long>(N_BUCKETS);
+        CK(cudaMemsetAsync(bucket_hist, 0, N_BUCKETS * 8, st));
+        a.bucket_hist = bucket_hist;
+        a.bucket_sample_mask = 0;
     }
     CK(launch_extract(MODE_SCAN, a, 0, st));
     clk.end();
@@ -370,7 +381,11 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
     WorkItem *low_items = nullptr;
     size_t n_low_items = 0;
     unsigned int *merge_next = nullptr;
-    if (!P.bloom) {
+    // a plain job whose table would not fit in L2 takes the partitioned path
+    // too (without the Bloom split): scattered by root prefix, every bucket's
+    // sub-table is filled while it sits in L2
+    const bool plain_part = !P.bloom && table_capacity_for(est) > PLAIN_PART_MIN_SLOTS;
+    if (!P.bloom && !plain_part) {
         cap = table_capacity_for(est);
         for (int attempt = 0;; ++attempt) {
             alloc_table(cap);
@@ -412,20 +427,29 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
             off += region[b];
         }
         const unsigned long long ocap = std::max<unsigned long long>(off, 1);
-        // reference sizing (src/main.cpp:41-153) from the pre-pass statistics
-        uint8_t avg_q = qh[1] ? (uint8_t)(qh[0] / qh[1]) : 0;
-        BloomPlan bp = bloom_plan(ph.data(), avg_q, in->total_bytes, P.memory_gb, k);
         unsigned long long words = 0;
-        for (uint32_t b = 0; b < N_BUCKETS; ++b) {
-            cfg[b].bloom_off = words;
-            cfg[b].bloom_cap = bp.caps[b];
-            words += 2 * bp.caps[b];
+        if (P.bloom) {
+            // reference sizing (src/main.cpp:41-153) from the pre-pass statistics
+            uint8_t avg_q = qh[1] ? (uint8_t)(qh[0] / qh[1]) : 0;
+            BloomPlan bp = bloom_plan(ph.data(), avg_q, in->total_bytes, P.memory_gb, k);
+            for (uint32_t b = 0; b < N_BUCKETS; ++b) {
+                cfg[b].bloom_off = words;
+                cfg[b].bloom_cap = bp.caps[b];
+                words += 2 * bp.caps[b];
+            }
         }
         // allocation order lets the scattered k-mers and then the filter be
-        // given back before the tables are laid out
-        list = ds.n<unsigned long long>(ocap);
-        unsigned long long *bits = ds.n<unsigned long long>(words);
-        unsigned long long *keys = ds.n<unsigned long long>(ocap);
+        // given back before the tables are laid out (Bloom mode); without the
+        // Bloom split the scattered k-mers are the insert's input
+        unsigned long long *bits = nullptr, *keys = nullptr;
+        if (P.bloom) {
+            list = ds.n<unsigned long long>(ocap);
+            bits = ds.n<unsigned long long>(words);
+            keys = ds.n<unsigned long long>(ocap);
+        } else {
+            keys = ds.n<unsigned long long>(ocap);
+            list = keys;
+        }
         BucketCfg *d_cfg_b = ds.n<BucketCfg>(N_BUCKETS);
         unsigned long long *cursor = ds.n<unsigned long long>(N_BUCKETS);
         unsigned long long *bbase = ds.n<unsigned long long>(2 * N_BUCKETS);
@@ -439,7 +463,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
         }
         CK(cudaMemsetAsync(cursor, 0, N_BUCKETS * 8, st));
         CK(cudaMemcpyAsync(bbase, bb.data(), 2 * N_BUCKETS * 8, cudaMemcpyHostToDevice, st));
-        CK(cudaMemsetAsync(bits, 0, words * 8, st));
+        if (P.bloom) CK(cudaMemsetAsync(bits, 0, words * 8, st));
         CK(cudaMemsetAsync(lh_cnt, 0, 2 * N_BUCKETS * 8, st));
         CK(cudaMemsetAsync(hll_high, 0, (size_t)N_BUCKETS * BUCKET_HLL_M * 4, st));
         a.hll = nullptr;
@@ -466,44 +490,60 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
         O = filled;
         job.occurrences = O;
         CK(cudaMemcpyAsync(d_cfg_b, cfg.data(), N_BUCKETS * sizeof(BucketCfg), cudaMemcpyHostToDevice, st));
-        clk.begin(8);
         std::vector<WorkItem> items;
         auto add_items = [&](uint32_t b, unsigned long long begin, unsigned long long end) {
             for (unsigned long long s = begin; s < end; s += WORK_ITEM_KEYS)
                 items.push_back(WorkItem{s, std::min<unsigned long long>(end, s + WORK_ITEM_KEYS), b, 0});
         };
-        for (uint32_t b = 0; b < N_BUCKETS; ++b) add_items(b, cfg[b].key_base, cfg[b].key_base + cfg[b].key_len);
-        WorkItem *d_items = ds.n<WorkItem>(std::max<size_t>(items.size(), 1));
-        if (!items.empty())
-            CK(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, st));
-        CK(launch_bloom_buckets(keys, d_items, (uint32_t)items.size(), next_item, d_cfg_b, bits, list, lh_cnt,
-                                lh_cnt + N_BUCKETS, hll_high, st));
-        clk.end();
-        std::vector<unsigned long long> lh(2 * N_BUCKETS);
-        std::vector<uint32_t> hh((size_t)N_BUCKETS * BUCKET_HLL_M);
-        CK(cudaMemcpyAsync(lh.data(), lh_cnt, 2 * N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(hh.data(), hll_high, hh.size() * 4, cudaMemcpyDeviceToHost, st));
+        std::vector<unsigned long long> lh(2 * N_BUCKETS, 0);
+        std::vector<uint32_t> hh;
+        if (P.bloom) {
+            clk.begin(8);
+            for (uint32_t b = 0; b < N_BUCKETS; ++b) add_items(b, cfg[b].key_base, cfg[b].key_base + cfg[b].key_len);
+            WorkItem *d_items = ds.n<WorkItem>(std::max<size_t>(items.size(), 1));
+            if (!items.empty())
+                CK(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, st));
+            CK(launch_bloom_buckets(keys, d_items, (uint32_t)items.size(), next_item, d_cfg_b, bits, list, lh_cnt,
+                                    lh_cnt + N_BUCKETS, hll_high, st));
+            clk.end();
+            hh.resize((size_t)N_BUCKETS * BUCKET_HLL_M);
+            CK(cudaMemcpyAsync(lh.data(), lh_cnt, 2 * N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(hh.data(), hll_high, hh.size() * 4, cudaMemcpyDeviceToHost, st));
+            ds.release(d_items);
+        } else {
+            // every occurrence goes to the table: the whole bucket is "high"
+            for (uint32_t b = 0; b < N_BUCKETS; ++b) lh[N_BUCKETS + b] = cfg[b].key_len;
+        }
         Counters c = read_counters(counters, st);
         check_flags(c.v[C_FLAGS], "partition");
-        ds.release(d_items);
         ds.release(next_item);
         ds.release(hll_high);
         ds.release(lh_cnt);
         ds.release(bbase);
         ds.release(cursor);
         ds.release(d_cfg_b);
-        ds.release(keys);
-        ds.release(bits);
+        if (P.bloom) {
+            ds.release(keys);
+            ds.release(bits);
+        }
         low_len = high_len = 0;
         std::vector<uint64_t> bcaps(N_BUCKETS);
         for (uint32_t b = 0; b < N_BUCKETS; ++b) {
+            const unsigned long long hb = lh[N_BUCKETS + b];
             low_len += lh[b];
-            high_len += lh[N_BUCKETS + b];
-            // the registers hold a hash sample of the non-FIRST k-mers
-            double e = lh[N_BUCKETS + b] ? (double)(1u << BUCKET_HLL_SAMPLE_BITS) *
-                                               hll_estimate(&hh[(size_t)b * BUCKET_HLL_M], BUCKET_HLL_M)
-                                         : 0.0;
-            e = std::max(e, (double)std::min<unsigned long long>(lh[N_BUCKETS + b], 4096));
+            high_len += hb;
+            double e;
+            if (P.bloom) {
+                // the registers hold a hash sample of the non-FIRST k-mers
+                e = hb ? (double)(1u << BUCKET_HLL_SAMPLE_BITS) *
+                             hll_estimate(&hh[(size_t)b * BUCKET_HLL_M], BUCKET_HLL_M)
+                       : 0.0;
+            } else {
+                // the job's distinct estimate, shared out by occurrences
+                e = O ? est * (double)hb / (double)O : 0.0;
+                e = std::min(e, (double)hb);
+            }
+            e = std::max(e, (double)std::min<unsigned long long>(hb, 4096));
             bcaps[b] = table_capacity_for(e);
         }
         // per-bucket sub-tables in one arena; a bucket whose table overflows
@@ -518,7 +558,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
         const size_t n_high_items = items.size();
         for (uint32_t b = 0; b < N_BUCKETS; ++b) add_items(b, cfg[b].key_base, cfg[b].key_base + lh[b]);
         n_low_items = items.size() - n_high_items;
-        d_items = ds.n<WorkItem>(std::max<size_t>(items.size(), 1));
+        WorkItem *d_items = ds.n<WorkItem>(std::max<size_t>(items.size(), 1));
         if (!items.empty())
             CK(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, st));
         low_items = d_items + n_high_items;

@@ -136,10 +136,36 @@ def test_plain_job_full_size(counter):
     fq = fq.tobytes()
     want_k, want_c = O.exact_records([fq], k, U32)
     r = counter.count([fq], k=k, count_max=U32, hist_max=10000)
+    # about 4.3M distinct k-mers: too many for one L2-resident table, so the
+    # job is counted through the root-prefix buckets
+    assert r.high_len == r.occurrences
     assert r.occurrences == int(want_c.sum(dtype=np.uint64))
     assert np.array_equal(r.keys, want_k)
     assert np.array_equal(r.counts, want_c)
     assert r.hist.tolist() == O.histogram(want_c, 1, 10000).tolist()
+
+
+def test_plain_partitioned_job_queries_and_filters(counter, kc):
+    """A plain job on the partitioned path, k = 25, with count filters,
+    saturation and both queries, against the oracle."""
+    import ktcountermemorygreedy_b200.synth as S
+    g = S.genome(31, 3_000_000)
+    fq = S.reads(g, 31, 60_000, (150, 150), 0.01, 0.0).tobytes()
+    k = 25
+    small = counter.count([fq[: 4000 * 316]], k=k, count_max=U32)
+    assert small.high_len == 0                      # a small job keeps one table
+    all_k, all_c = O.exact_records([fq], k, 7)
+    r = counter.count([fq], k=k, count_max=7, min_count=2, max_count=6, top_n=500, want_le2=True, hist_max=20)
+    assert r.high_len == r.occurrences
+    m = (all_c >= 2) & (all_c <= 6)
+    assert np.array_equal(r.keys, all_k[m]) and np.array_equal(r.counts, all_c[m])
+    assert r.hist.tolist() == O.histogram(all_c, 1, 20).tolist()
+    keep_k, keep_c = all_k[m], all_c[m]
+    strs = [kc.string_key(int(w), k) for w in keep_k]
+    order = sorted(range(len(keep_k)), key=lambda i: (-int(keep_c[i]), strs[i]))[:500]
+    assert r.top_keys.tolist() == [int(keep_k[i]) for i in order]
+    le = keep_c <= 2
+    assert r.le2_keys.tolist() == keep_k[le].tolist()
 
 
 def test_bloom_job_sampled_census(counter):
