@@ -332,13 +332,14 @@ def served_bench(kc, args, local):
     out = {"workload": f"served stream: Poisson arrivals, log-normal sizes (median 200k reads, sigma 1.5, "
                        f"capped at the {pool_reads}-read pool), 150 bp at 1% from a 50 Mbp genome, "
                        f"k in {{21,25,31}}, histogram + top-1000 + count<=2 per job",
-           "max_inflight_jobs": args.served_inflight, "rates": {}}
-    with kc.KmerCounter(device=local, max_inflight_jobs=1) as plain:
+           "max_inflight_jobs": args.served_inflight, "pinned_arena_gb": args.served_pinned_gb, "rates": {}}
+    pinned = args.served_pinned_gb << 30
+    with kc.KmerCounter(device=local, max_inflight_jobs=1, pinned_bytes=pinned) as plain:
         warm(plain, 1)
         reqs = make_requests(1e9, args.served_jobs, 4000)   # all at once, one worker: back to back
         stats, wall = serving.serve(plain, reqs)
         out["plain"] = serving.summarize(stats, wall)
-    with kc.KmerCounter(device=local, max_inflight_jobs=args.served_inflight) as srv:
+    with kc.KmerCounter(device=local, max_inflight_jobs=args.served_inflight) as srv:   # shares the arena
         warm(srv, args.served_inflight)
         for rate in args.served_rates:
             reqs = make_requests(rate, args.served_jobs, 4000 + int(rate))
@@ -357,10 +358,22 @@ def batched_bench(kc, args, local):
     comparison, as one job per sample through a one-worker handle.  Both
     include the host->device upload and the records + histograms coming back
     to pinned host memory."""
+    import ctypes as C
+    import numpy as np
     import ktcountermemorygreedy_b200.synth as S
     samples = S.batch_samples(args.batch_samples, scale=args.batch_scale)
-    files = [[fq] for fq, _ in samples]
+    # the samples sit in pinned host memory, as a server's receive buffers would
+    total = sum(len(fq) for fq, _ in samples)
+    p = C.c_void_p()
+    kc._check(kc.lib().kc_host_alloc(max(total, 1), C.byref(p)))
+    buf = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint8)), shape=(max(total, 1),))
+    files, off = [], 0
+    for fq, _ in samples:
+        buf[off:off + len(fq)] = fq
+        files.append([buf[off:off + len(fq)]])
+        off += len(fq)
     ks = [k for _, k in samples]
+    del samples
     job = dict(count_max=U32, min_count=1, hist_min=1, hist_max=4095)
     with kc.KmerCounter(device=local, max_inflight_jobs=1) as h:
         h.count_batch(files, ks, copy=False, **job)          # warm-up
@@ -379,9 +392,12 @@ def batched_bench(kc, args, local):
                    and (a.keys == b.keys).all() for a, b in zip(res_b, res_p))
         stages_b = {kc.PHASES[i]: res_b[0].phase_ms[i] for i in range(len(kc.PHASES)) if res_b[0].phase_ms[i] > 0}
         del res_b, res_p
+    fastq_bytes = int(sum(len(f[0]) for f in files))
+    del files
+    kc.lib().kc_host_free(p)
     return {"workload": f"{len(samples)} samples, own 5-50 Mbp genomes, log-uniform 1e4-2e6 reads x "
                         f"{args.batch_scale}, 100-250 bp, 0.5-2% errors, k=21/31",
-            "samples": len(samples), "fastq_bytes": int(sum(len(f[0]) for f in files)), "occurrences": int(occ),
+            "samples": len(ks), "fastq_bytes": fastq_bytes, "occurrences": int(occ), "inputs": "pinned host memory",
             "batched_kmers_per_s": occ / t_b, "batched_s": t_b, "batched_device_ms": dev_b,
             "batched_stages_ms": stages_b,
             "plain_kmers_per_s": occ / t_p, "plain_s": t_p, "plain_device_ms": dev_p,
@@ -520,6 +536,7 @@ def main():
     ap.add_argument("--served-rates", type=float, nargs="+", default=[10.0, 50.0, 200.0])
     ap.add_argument("--served-inflight", type=int, default=4)
     ap.add_argument("--served-pool-reads", type=int, default=4_000_000)
+    ap.add_argument("--served-pinned-gb", type=int, default=24)
     ap.add_argument("--no-batched", dest="batched", action="store_false")
     ap.add_argument("--batch-samples", type=int, default=256)
     ap.add_argument("--batch-scale", type=float, default=0.125)

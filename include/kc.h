@@ -65,7 +65,11 @@ typedef struct {
     uint64_t workspace_bytes;     /* device workspace each worker allocates at kc_open (a server sized
                                      for its largest job never allocates, or synchronizes the device
                                      to grow, while jobs run); 0 -> grown to the largest job seen */
-    uint64_t reserved[5];
+    uint64_t pinned_bytes;        /* pinned host memory kc_open sets aside for job results (records,
+                                     count <= 2 sets), shared by all handles of the process and kept
+                                     until it exits; results that do not fit use pinned blocks
+                                     allocated on demand; 0 -> none */
+    uint64_t reserved[4];
 } kc_config;
 
 typedef struct {

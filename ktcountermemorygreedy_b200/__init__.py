@@ -50,7 +50,8 @@ class KcError(RuntimeError):
 
 class kc_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("max_inflight_jobs", C.c_uint32),
-                ("hbm_budget_bytes", C.c_uint64), ("workspace_bytes", C.c_uint64), ("reserved", C.c_uint64 * 5)]
+                ("hbm_budget_bytes", C.c_uint64), ("workspace_bytes", C.c_uint64), ("pinned_bytes", C.c_uint64),
+                ("reserved", C.c_uint64 * 4)]
 
 
 class kc_buffer(C.Structure):
@@ -235,12 +236,13 @@ class KmerCounter:
     memory frees up."""
 
     def __init__(self, device: int = 0, max_inflight_jobs: int = 4, hbm_budget_bytes: int = 0,
-                 workspace_bytes: int = 0):
+                 workspace_bytes: int = 0, pinned_bytes: int = 0):
         cfg = kc_config()
         cfg.device = device
         cfg.max_inflight_jobs = max_inflight_jobs
         cfg.hbm_budget_bytes = hbm_budget_bytes
         cfg.workspace_bytes = workspace_bytes
+        cfg.pinned_bytes = pinned_bytes
         h = C.c_void_p()
         _check(lib().kc_open(C.byref(cfg), C.byref(h)))
         self._h = h

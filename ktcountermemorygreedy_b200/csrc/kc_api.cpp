@@ -1155,6 +1155,14 @@ int kc_open(const kc_config *cfg, kc_handle **out)
     h->device = dev;
     h->budget = (cfg && cfg->hbm_budget_bytes) ? cfg->hbm_budget_bytes : (uint64_t)(free_b * 0.9);
     h->workspace_bytes = cfg ? cfg->workspace_bytes : 0;
+    if (cfg && cfg->pinned_bytes) {
+        try {
+            PinnedPool::instance().add_arena(cfg->pinned_bytes);
+        } catch (const KcError &e) {
+            delete h;
+            return fail(e.code, e.msg);
+        }
+    }
     uint32_t nw = (cfg && cfg->max_inflight_jobs) ? cfg->max_inflight_jobs : 4;
     for (uint32_t i = 0; i < nw; ++i) h->workers.emplace_back(worker_main, h);
     *out = h;

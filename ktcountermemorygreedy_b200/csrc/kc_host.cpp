@@ -159,6 +159,55 @@ struct PinnedPool::Impl {
     std::mutex mu;
     std::multimap<size_t, void *> free_blocks;
     size_t cached = 0;
+    struct Arena {
+        uint8_t *base;
+        size_t size;
+        std::map<size_t, size_t> free;   // offset -> length of each free range
+    };
+    std::vector<Arena> arenas;
+
+    // best-fit range of an arena (caller holds mu); nullptr if none fits
+    void *arena_get(size_t bytes)
+    {
+        Arena *ba = nullptr;
+        std::map<size_t, size_t>::iterator bi;
+        for (auto &a : arenas)
+            for (auto it = a.free.begin(); it != a.free.end(); ++it)
+                if (it->second >= bytes && (!ba || it->second < bi->second)) {
+                    ba = &a;
+                    bi = it;
+                }
+        if (!ba) return nullptr;
+        const size_t off = bi->first, len = bi->second;
+        ba->free.erase(bi);
+        if (len > bytes) ba->free.emplace(off + bytes, len - bytes);
+        return ba->base + off;
+    }
+
+    bool arena_put(void *p, size_t bytes)
+    {
+        uint8_t *q = static_cast<uint8_t *>(p);
+        for (auto &a : arenas) {
+            if (q < a.base || q >= a.base + a.size) continue;
+            size_t off = (size_t)(q - a.base), len = bytes;
+            auto next = a.free.lower_bound(off);
+            if (next != a.free.end() && off + len == next->first) {   // merge with the range after
+                len += next->second;
+                next = a.free.erase(next);
+            }
+            if (next != a.free.begin()) {                              // and with the one before
+                auto prev = std::prev(next);
+                if (prev->first + prev->second == off) {
+                    off = prev->first;
+                    len += prev->second;
+                    a.free.erase(prev);
+                }
+            }
+            a.free.emplace(off, len);
+            return true;
+        }
+        return false;
+    }
 };
 
 PinnedPool::PinnedPool() : impl_(new Impl) {}
@@ -183,6 +232,10 @@ void *PinnedPool::get(size_t bytes, size_t &got)
     }
     {
         std::lock_guard<std::mutex> lk(impl_->mu);
+        if (void *p = impl_->arena_get(bytes)) {
+            got = bytes;
+            return p;
+        }
         auto it = impl_->free_blocks.lower_bound(bytes);
         if (it != impl_->free_blocks.end() && it->first <= bytes + bytes / 4 + (64u << 20)) {
             void *p = it->second;
@@ -205,6 +258,10 @@ void *PinnedPool::get(size_t bytes, size_t &got)
 void PinnedPool::put(void *p, size_t bytes)
 {
     if (!p) return;
+    {
+        std::lock_guard<std::mutex> lk(impl_->mu);
+        if (impl_->arena_put(p, bytes)) return;
+    }
     // keep up to a third of the host's memory pinned for reuse
     static const size_t keep_limit = [] {
         const long pages = sysconf(_SC_PHYS_PAGES), page = sysconf(_SC_PAGE_SIZE);
@@ -220,6 +277,21 @@ void PinnedPool::put(void *p, size_t bytes)
         }
     }
     cudaFreeHost(p);
+}
+
+void PinnedPool::add_arena(size_t bytes)
+{
+    bytes = (bytes + (2u << 20) - 1) & ~size_t((2u << 20) - 1);
+    if (!bytes) return;
+    void *p = nullptr;
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        throw KcError{KC_ERR_NOMEM, "pinned host arena of " + std::to_string(bytes) + " bytes failed"};
+    }
+    std::lock_guard<std::mutex> lk(impl_->mu);
+    Impl::Arena a{static_cast<uint8_t *>(p), bytes, {}};
+    a.free.emplace(0, bytes);
+    impl_->arenas.push_back(std::move(a));
 }
 
 PinnedPool::~PinnedPool()

@@ -86,6 +86,9 @@ public:
     static PinnedPool &instance();
     void *get(size_t bytes, size_t &got);   // throws KcError on failure
     void put(void *p, size_t bytes);
+    // pins `bytes` of host memory once; later blocks are carved from it
+    // first (best fit) and returned to it.  Kept until the process exits.
+    void add_arena(size_t bytes);           // throws KcError on failure
     ~PinnedPool();
 
 private:

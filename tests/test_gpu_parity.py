@@ -257,6 +257,27 @@ def test_batch_spanning_several_sort_groups_matches_single_jobs(counter):
         assert r.occurrences == one.occurrences
 
 
+def test_pinned_arena_results_match(kc):
+    """Results carved from a pinned arena set aside at kc_open (records and
+    count <= 2 sets of several sizes, released and reused across rounds) are
+    the same as results in blocks pinned on demand."""
+    jobs = []
+    for i in range(6):
+        f = fixtures.random_fastq(300 + i, 200 + 150 * i, (100, 150), genome_len=3000 + 700 * i)
+        jobs.append(([f], [21, 25, 31][i % 3]))
+    with kc.KmerCounter(max_inflight_jobs=2) as c0:
+        want = [c0.count(f, k=k, count_max=U32, want_le2=True) for f, k in jobs]
+    with kc.KmerCounter(max_inflight_jobs=3, pinned_bytes=64 << 20) as c1:
+        for rnd in range(3):
+            ids = [c1.submit(f, k=k, count_max=U32, want_le2=True) for f, k in jobs]
+            for jid, (f, k), w in zip(ids, jobs, want):
+                c1.wait(jid)
+                r = c1.result(jid, k, copy=(rnd != 1))
+                assert np.array_equal(r.keys, w.keys) and np.array_equal(r.counts, w.counts)
+                assert np.array_equal(r.le2_keys, w.le2_keys) and np.array_equal(r.le2_counts, w.le2_counts)
+                del r
+
+
 def test_jobs_same_alone_and_in_the_mix(kc):
     jobs = []
     for i in range(12):
