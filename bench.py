@@ -395,7 +395,7 @@ def batched_bench(kc, args, local):
     fastq_bytes = int(sum(len(f[0]) for f in files))
     del files
     kc.lib().kc_host_free(p)
-    return {"workload": f"{len(samples)} samples, own 5-50 Mbp genomes, log-uniform 1e4-2e6 reads x "
+    return {"workload": f"{len(ks)} samples, own 5-50 Mbp genomes, log-uniform 1e4-2e6 reads x "
                         f"{args.batch_scale}, 100-250 bp, 0.5-2% errors, k=21/31",
             "samples": len(ks), "fastq_bytes": fastq_bytes, "occurrences": int(occ), "inputs": "pinned host memory",
             "batched_kmers_per_s": occ / t_b, "batched_s": t_b, "batched_device_ms": dev_b,

@@ -96,7 +96,11 @@ typedef struct {
     uint32_t want_le2;            /* 1: the records with count <= 2 */
     uint32_t keep_records;        /* 1: copy the sorted records to host memory */
     uint32_t reserved0;
-    uint64_t reserved[6];
+    uint64_t pass_bytes;          /* device memory one counting pass may use; a job that needs more
+                                     runs in passes over ranges of root prefixes, each pass's records
+                                     held in pinned host memory until the final sort; 0 -> 70% of the
+                                     device memory free for the job when its counting starts */
+    uint64_t reserved[5];
 } kc_job;
 
 typedef struct {
@@ -131,6 +135,8 @@ typedef struct {
                                      the non-FIRST ones; large plain jobs: all); 0 for one table */
     uint64_t input_bytes;         /* FASTQ bytes of the job */
     uint64_t n_records_total;     /* records on the device (also when keep_records = 0) */
+    uint32_t passes;              /* counting passes over ranges of root prefixes (1: the whole job at once) */
+    uint32_t reserved0;
 } kc_result_t;
 
 /* Kernel launches issued by this process so far (all handles). */

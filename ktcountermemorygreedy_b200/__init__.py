@@ -64,7 +64,8 @@ class kc_job(C.Structure):
                 ("memory_gb", C.c_uint64), ("filter_min", C.c_uint32), ("filter_max", C.c_uint32),
                 ("min_count", C.c_uint32), ("max_count", C.c_uint32), ("hist_min", C.c_uint32),
                 ("hist_max", C.c_uint32), ("top_n", C.c_uint32), ("want_le2", C.c_uint32),
-                ("keep_records", C.c_uint32), ("reserved0", C.c_uint32), ("reserved", C.c_uint64 * 6)]
+                ("keep_records", C.c_uint32), ("reserved0", C.c_uint32), ("pass_bytes", C.c_uint64),
+                ("reserved", C.c_uint64 * 5)]
 
 
 class kc_result_t(C.Structure):
@@ -76,7 +77,7 @@ class kc_result_t(C.Structure):
                 ("table_capacity", C.c_uint64), ("device_ms", C.c_double), ("queue_ms", C.c_double),
                 ("run_ms", C.c_double), ("phase_ms", C.c_double * 12), ("phase_launches", C.c_uint64 * 12),
                 ("low_len", C.c_uint64), ("high_len", C.c_uint64), ("input_bytes", C.c_uint64),
-                ("n_records_total", C.c_uint64)]
+                ("n_records_total", C.c_uint64), ("passes", C.c_uint32), ("reserved0", C.c_uint32)]
 
 # stage names of kc_result_t.phase_ms
 PHASES = ["census", "scan", "count_pass", "insert_high", "merge_low", "compact", "sort", "queries", "bloom",
@@ -198,6 +199,7 @@ class Result:
     high_len: int = 0
     input_bytes: int = 0
     n_records_total: int = 0
+    passes: int = 1
 
 
 def _copy(ptr, n, dtype):
@@ -270,13 +272,14 @@ class KmerCounter:
     def make_job(k: int = 31, count_max: int = 255, bloom: bool = False, memory_gb: int = 4,
                  filter_min: int = 2, filter_max: int = U32_MAX, min_count: int = 1,
                  max_count: int = U32_MAX, hist_min: int = 1, hist_max: int = 10000, top_n: int = 0,
-                 want_le2: bool = False, keep_records: bool = True) -> kc_job:
+                 want_le2: bool = False, keep_records: bool = True, pass_bytes: int = 0) -> kc_job:
         j = kc_job()
         lib().kc_job_defaults(C.byref(j))
         j.k, j.count_max, j.bloom, j.memory_gb = k, count_max, int(bloom), memory_gb
         j.filter_min, j.filter_max, j.min_count, j.max_count = filter_min, filter_max, min_count, max_count
         j.hist_min, j.hist_max, j.top_n, j.want_le2 = hist_min, hist_max, top_n, int(want_le2)
         j.keep_records = int(keep_records)
+        j.pass_bytes = pass_bytes
         return j
 
     def upload(self, files: Sequence[bytes]):
@@ -345,7 +348,7 @@ class KmerCounter:
             occurrences=r.occurrences, distinct=r.distinct, low_only=r.low_only,
             table_capacity=r.table_capacity, device_ms=r.device_ms, queue_ms=r.queue_ms, run_ms=r.run_ms,
             phase_ms=tuple(r.phase_ms), phase_launches=tuple(r.phase_launches), low_len=r.low_len,
-            high_len=r.high_len, input_bytes=r.input_bytes, n_records_total=r.n_records_total)
+            high_len=r.high_len, input_bytes=r.input_bytes, n_records_total=r.n_records_total, passes=r.passes)
         if release:
             self.release(jid)
         return out

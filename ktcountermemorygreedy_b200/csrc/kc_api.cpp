@@ -103,6 +103,7 @@ struct Job {
     HostRecords le2;   // records with count <= 2 (pinned: often most of the records)
     uint64_t occurrences = 0, distinct = 0, low_only = 0, table_cap = 0;
     uint64_t low_len = 0, high_len = 0, input_bytes = 0, n_records_total = 0;
+    uint32_t passes = 1;
     double device_ms = 0;
     double phase_ms[KC_STAGES] = {0};
     uint64_t phase_launches[KC_STAGES] = {0};
@@ -361,34 +362,70 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
     job.occurrences = O;
 
     // ---- counting ---------------------------------------------------------
-    TableRef tr{};
-    TableRef *d_tr = ds.n<TableRef>(1);
-    uint64_t cap = 0;
-    unsigned long long *list = nullptr;
-    unsigned long long low_len = 0, high_len = 0;
-    double est = hll_estimate(hll_h.data(), HLL_M);
-    auto alloc_table = [&](uint64_t c) {
-        if (tr.slots) ds.release(tr.slots);
-        cap = c;
-        tr.slots = static_cast<Slot *>(ds.get(cap * sizeof(Slot)));
-        tr.mask = cap - 1;
-        CK(launch_init_slots(tr.slots, cap, st));
-        CK(cudaMemcpyAsync(d_tr, &tr, sizeof(tr), cudaMemcpyHostToDevice, st));
-    };
+    const uint32_t count_max = P.count_max ? P.count_max : 255u;
     const uint32_t max_probe_cap = 1u << 16;
-    BucketCfg *d_cfg = nullptr;           // partitioned pipeline state kept for the merge
-    unsigned long long *bucket_ovf = nullptr;
-    WorkItem *low_items = nullptr;
-    size_t n_low_items = 0;
-    unsigned int *merge_next = nullptr;
+    const double est = hll_estimate(hll_h.data(), HLL_M);
+    unsigned long long *hist = ds.n<unsigned long long>(HIST_BINS);
+    const uint64_t ovf_cap = 1 << 20;
+    uint32_t *ovf = ds.n<uint32_t>(ovf_cap);
+    unsigned long long *n_keys = ds.n<unsigned long long>(1);
+    CK(cudaMemsetAsync(hist, 0, HIST_BINS * 8, st));
+    unsigned long long low_len = 0, high_len = 0;
+    uint64_t table_cap = 0;
+    job.distinct = job.low_only = 0;
+
+    // Records of one counted table: the FIRST occurrences are merged in (Bloom
+    // mode), every occupied slot is compacted into new record arrays, and the
+    // histogram (shared by all tables of the job) is added to.
+    unsigned long long *rec_keys = nullptr;
+    uint32_t *rec_counts = nullptr;
+    uint64_t n_rec = 0;
+    auto compact_table = [&](const TableRef &t, uint64_t cap, uint64_t n_low, const unsigned long long *lst,
+                             const WorkItem *low_items, size_t n_low_items, unsigned int *merge_next,
+                             const BucketCfg *d_cfg) {
+        CK(cudaMemsetAsync(n_keys, 0, 8, st));
+        CK(cudaMemsetAsync(counters + C_REC_LEN, 0, 3 * 8, st));   // C_REC_LEN, C_LOW_ONLY, C_DISTINCT
+        clk.begin(5);
+        CK(launch_count_keys(t.slots, cap, n_keys, st));
+        clk.end();
+        unsigned long long in_table = 0;
+        CK(cudaMemcpyAsync(&in_table, n_keys, 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        const uint64_t rec_cap = std::max<uint64_t>(in_table + n_low, 1);
+        rec_keys = ds.n<unsigned long long>(rec_cap);
+        rec_counts = ds.n<uint32_t>(rec_cap);
+        if (n_low) {
+            clk.begin(4);
+            CK(launch_merge_buckets(lst, low_items, (uint32_t)n_low_items, merge_next, d_cfg, t.slots, max_probe_cap,
+                                    P.min_count, P.max_count, rec_keys, rec_counts, rec_cap, counters, st));
+            clk.end();
+        }
+        clk.begin(5);
+        CK(launch_compact(t, cap, count_max, P.min_count, P.max_count, rec_keys, rec_counts, rec_cap, hist, ovf,
+                          ovf_cap, counters, st));
+        clk.end();
+        Counters c2 = read_counters(counters, st);
+        check_flags(c2.v[C_FLAGS], "compact");
+        if (c2.v[C_FLAGS] & ERR_TABLE_FULL) throw KcError{KC_ERR_DEVICE, "counting table lookup overflow"};
+        n_rec = c2.v[C_REC_LEN];
+        job.distinct += c2.v[C_DISTINCT] + c2.v[C_LOW_ONLY];
+        job.low_only += c2.v[C_LOW_ONLY];
+    };
+
     // a plain job whose table would not fit in L2 takes the partitioned path
     // too (without the Bloom split): scattered by root prefix, every bucket's
     // sub-table is filled while it sits in L2
     const bool plain_part = !P.bloom && table_capacity_for(est) > PLAIN_PART_MIN_SLOTS;
     if (!P.bloom && !plain_part) {
-        cap = table_capacity_for(est);
+        TableRef tr{};
+        TableRef *d_tr = ds.n<TableRef>(1);
+        uint64_t cap = table_capacity_for(est);
         for (int attempt = 0;; ++attempt) {
-            alloc_table(cap);
+            if (tr.slots) ds.release(tr.slots);
+            tr.slots = static_cast<Slot *>(ds.get(cap * sizeof(Slot)));
+            tr.mask = cap - 1;
+            CK(launch_init_slots(tr.slots, cap, st));
+            CK(cudaMemcpyAsync(d_tr, &tr, sizeof(tr), cudaMemcpyHostToDevice, st));
             CK(cudaMemsetAsync(counters, 0, 8, st));
             a.tables = d_tr;
             a.max_probe = (uint32_t)std::min<uint64_t>(cap, max_probe_cap);
@@ -401,15 +438,16 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
             if (attempt >= 3) throw KcError{KC_ERR_DEVICE, "counting table overflow"};
             cap *= 2;
         }
+        table_cap = cap;
+        compact_table(tr, cap, 0, nullptr, nullptr, 0, nullptr, nullptr);
     } else {
         // ---- root-prefix buckets (the reference's 256 root prefixes,
-        // src/NewKmerTree.h:1488-1495): exact sizes from the SCAN pass, one
+        // src/NewKmerTree.h:1488-1495): sizes from the SCAN census, one
         // scatter pass, then every bucket's Bloom filter and table slice is
         // processed while it sits in L2
         std::vector<unsigned long long> bh(N_BUCKETS);
         CK(cudaMemcpyAsync(bh.data(), bucket_hist, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        std::vector<BucketCfg> cfg(N_BUCKETS);
         std::vector<unsigned long long> region(N_BUCKETS);
         unsigned long long sampled = 0;
         for (uint32_t b = 0; b < N_BUCKETS; ++b) sampled += bh[b];
@@ -420,217 +458,252 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
         // census tiles: t with (t & mask) == 0
         const double scale =
             exact ? 1.0 : (double)T / (double)((T + a.bucket_sample_mask) / (a.bucket_sample_mask + 1));
-        unsigned long long off = 0;
-        for (uint32_t b = 0; b < N_BUCKETS; ++b) {
+        for (uint32_t b = 0; b < N_BUCKETS; ++b)
             region[b] = exact ? bh[b] : (unsigned long long)std::ceil((double)bh[b] * scale * 1.15) + 8192;
-            cfg[b].key_base = off;
-            off += region[b];
-        }
-        const unsigned long long ocap = std::max<unsigned long long>(off, 1);
-        unsigned long long words = 0;
+        std::vector<uint64_t> fcap(N_BUCKETS, 0);
         if (P.bloom) {
             // reference sizing (src/main.cpp:41-153) from the pre-pass statistics
             uint8_t avg_q = qh[1] ? (uint8_t)(qh[0] / qh[1]) : 0;
             BloomPlan bp = bloom_plan(ph.data(), avg_q, in->total_bytes, P.memory_gb, k);
+            for (uint32_t b = 0; b < N_BUCKETS; ++b) fcap[b] = bp.caps[b];
+        }
+        // passes over ranges of buckets, each within the device-memory budget
+        // of a pass (k-mer arrays, filters, tables, records of its buckets)
+        uint64_t budget = P.pass_bytes;
+        if (!budget) {
+            // free device memory plus the part of this worker's workspace the
+            // job has not used yet
+            size_t free_b = 0, total_b = 0;
+            CK(cudaMemGetInfo(&free_b, &total_b));
+            const size_t ws_free = ws.capacity() > ws.mark().top ? ws.capacity() - ws.mark().top : 0;
+            budget = (uint64_t)(0.7 * (double)(free_b + ws_free));
+        }
+        const uint64_t per_occ = P.bloom ? 40 : 48;
+        std::vector<std::pair<uint32_t, uint32_t>> ranges;
+        {
+            uint32_t lo = 0;
+            uint64_t need = 0;
             for (uint32_t b = 0; b < N_BUCKETS; ++b) {
-                cfg[b].bloom_off = words;
-                cfg[b].bloom_cap = bp.caps[b];
-                words += 2 * bp.caps[b];
+                const uint64_t nb = region[b] * per_occ + fcap[b] * 16;
+                if (b > lo && need + nb > budget) {
+                    ranges.push_back({lo, b});
+                    lo = b;
+                    need = 0;
+                }
+                need += nb;
             }
+            ranges.push_back({lo, N_BUCKETS});
         }
-        // allocation order lets the scattered k-mers and then the filter be
-        // given back before the tables are laid out (Bloom mode); without the
-        // Bloom split the scattered k-mers are the insert's input
-        unsigned long long *bits = nullptr, *keys = nullptr;
-        if (P.bloom) {
-            list = ds.n<unsigned long long>(ocap);
-            bits = ds.n<unsigned long long>(words);
-            keys = ds.n<unsigned long long>(ocap);
-        } else {
-            keys = ds.n<unsigned long long>(ocap);
-            list = keys;
-        }
-        BucketCfg *d_cfg_b = ds.n<BucketCfg>(N_BUCKETS);
-        unsigned long long *cursor = ds.n<unsigned long long>(N_BUCKETS);
-        unsigned long long *bbase = ds.n<unsigned long long>(2 * N_BUCKETS);
-        unsigned long long *lh_cnt = ds.n<unsigned long long>(2 * N_BUCKETS);
-        uint32_t *hll_high = ds.n<uint32_t>((size_t)N_BUCKETS * BUCKET_HLL_M);
-        unsigned int *next_item = ds.n<unsigned int>(1);
-        std::vector<unsigned long long> bb(2 * N_BUCKETS);
-        for (uint32_t b = 0; b < N_BUCKETS; ++b) {
-            bb[b] = cfg[b].key_base;
-            bb[N_BUCKETS + b] = cfg[b].key_base + region[b];
-        }
-        CK(cudaMemsetAsync(cursor, 0, N_BUCKETS * 8, st));
-        CK(cudaMemcpyAsync(bbase, bb.data(), 2 * N_BUCKETS * 8, cudaMemcpyHostToDevice, st));
-        if (P.bloom) CK(cudaMemsetAsync(bits, 0, words * 8, st));
-        CK(cudaMemsetAsync(lh_cnt, 0, 2 * N_BUCKETS * 8, st));
-        CK(cudaMemsetAsync(hll_high, 0, (size_t)N_BUCKETS * BUCKET_HLL_M * 4, st));
-        a.hll = nullptr;
-        a.prepass = 0;
-        a.bucket_hist = nullptr;
-        a.list = keys;
-        a.list_cap = ocap;
-        a.bucket_cursor = cursor;
-        a.bucket_base = bbase;
-        a.bucket_end = bbase + N_BUCKETS;
-        clk.begin(2);
-        CK(launch_extract(MODE_PART, a, 0, st));
-        clk.end();
-        std::vector<unsigned long long> fill(N_BUCKETS);
-        CK(cudaMemcpyAsync(fill.data(), cursor, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        unsigned long long filled = 0;
-        for (uint32_t b = 0; b < N_BUCKETS; ++b) {
-            if (fill[b] > region[b]) throw CensusOverflow{};
-            cfg[b].key_len = fill[b];
-            filled += fill[b];
-        }
-        if (exact && filled != O) throw KcError{KC_ERR_DEVICE, "partition does not add up to the occurrences"};
-        O = filled;
-        job.occurrences = O;
-        CK(cudaMemcpyAsync(d_cfg_b, cfg.data(), N_BUCKETS * sizeof(BucketCfg), cudaMemcpyHostToDevice, st));
-        std::vector<WorkItem> items;
-        auto add_items = [&](uint32_t b, unsigned long long begin, unsigned long long end) {
-            for (unsigned long long s = begin; s < end; s += WORK_ITEM_KEYS)
-                items.push_back(WorkItem{s, std::min<unsigned long long>(end, s + WORK_ITEM_KEYS), b, 0});
-        };
-        std::vector<unsigned long long> lh(2 * N_BUCKETS, 0);
-        std::vector<uint32_t> hh;
-        if (P.bloom) {
-            clk.begin(8);
-            for (uint32_t b = 0; b < N_BUCKETS; ++b) add_items(b, cfg[b].key_base, cfg[b].key_base + cfg[b].key_len);
+        const bool multi = ranges.size() > 1;
+        std::vector<std::unique_ptr<HostRecords>> spilled;
+        uint64_t spilled_total = 0, filled_total = 0;
+        for (const auto &rg : ranges) {
+            const uint32_t lo = rg.first, hi = rg.second;
+            const DevScope::Mark mk = ds.mark();
+            std::vector<BucketCfg> cfg(N_BUCKETS);
+            unsigned long long off = 0, words = 0;
+            for (uint32_t b = lo; b < hi; ++b) {
+                cfg[b].key_base = off;
+                off += region[b];
+                cfg[b].bloom_off = words;
+                cfg[b].bloom_cap = fcap[b];
+                words += 2 * fcap[b];
+            }
+            const unsigned long long ocap = std::max<unsigned long long>(off, 1);
+            // allocation order lets the scattered k-mers and then the filter be
+            // given back before the tables are laid out (Bloom mode); without
+            // the Bloom split the scattered k-mers are the insert's input
+            unsigned long long *list = nullptr, *bits = nullptr, *keys = nullptr;
+            if (P.bloom) {
+                list = ds.n<unsigned long long>(ocap);
+                bits = ds.n<unsigned long long>(std::max<unsigned long long>(words, 1));
+                keys = ds.n<unsigned long long>(ocap);
+            } else {
+                keys = ds.n<unsigned long long>(ocap);
+                list = keys;
+            }
+            BucketCfg *d_cfg_b = ds.n<BucketCfg>(N_BUCKETS);
+            unsigned long long *cursor = ds.n<unsigned long long>(N_BUCKETS);
+            unsigned long long *bbase = ds.n<unsigned long long>(2 * N_BUCKETS);
+            unsigned long long *lh_cnt = ds.n<unsigned long long>(2 * N_BUCKETS);
+            uint32_t *hll_high = ds.n<uint32_t>((size_t)N_BUCKETS * BUCKET_HLL_M);
+            unsigned int *next_item = ds.n<unsigned int>(1);
+            std::vector<unsigned long long> bb(2 * N_BUCKETS, 0);
+            for (uint32_t b = lo; b < hi; ++b) {
+                bb[b] = cfg[b].key_base;
+                bb[N_BUCKETS + b] = cfg[b].key_base + region[b];
+            }
+            CK(cudaMemsetAsync(cursor, 0, N_BUCKETS * 8, st));
+            CK(cudaMemcpyAsync(bbase, bb.data(), 2 * N_BUCKETS * 8, cudaMemcpyHostToDevice, st));
+            if (P.bloom) CK(cudaMemsetAsync(bits, 0, words * 8, st));
+            CK(cudaMemsetAsync(lh_cnt, 0, 2 * N_BUCKETS * 8, st));
+            CK(cudaMemsetAsync(hll_high, 0, (size_t)N_BUCKETS * BUCKET_HLL_M * 4, st));
+            a.hll = nullptr;
+            a.prepass = 0;
+            a.bucket_hist = nullptr;
+            a.list = keys;
+            a.list_cap = ocap;
+            a.bucket_cursor = cursor;
+            a.bucket_base = bbase;
+            a.bucket_end = bbase + N_BUCKETS;
+            a.bucket_lo = lo;
+            a.bucket_hi = hi;
+            clk.begin(2);
+            CK(launch_extract(MODE_PART, a, 0, st));
+            clk.end();
+            std::vector<unsigned long long> fill(N_BUCKETS);
+            CK(cudaMemcpyAsync(fill.data(), cursor, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            for (uint32_t b = lo; b < hi; ++b) {
+                if (fill[b] > region[b]) throw CensusOverflow{};
+                cfg[b].key_len = fill[b];
+                filled_total += fill[b];
+            }
+            CK(cudaMemcpyAsync(d_cfg_b, cfg.data(), N_BUCKETS * sizeof(BucketCfg), cudaMemcpyHostToDevice, st));
+            std::vector<WorkItem> items;
+            auto add_items = [&](uint32_t b, unsigned long long begin, unsigned long long end) {
+                for (unsigned long long s0 = begin; s0 < end; s0 += WORK_ITEM_KEYS)
+                    items.push_back(WorkItem{s0, std::min<unsigned long long>(end, s0 + WORK_ITEM_KEYS), b, 0});
+            };
+            std::vector<unsigned long long> lh(2 * N_BUCKETS, 0);
+            std::vector<uint32_t> hh;
+            if (P.bloom) {
+                clk.begin(8);
+                for (uint32_t b = lo; b < hi; ++b) add_items(b, cfg[b].key_base, cfg[b].key_base + cfg[b].key_len);
+                WorkItem *d_items = ds.n<WorkItem>(std::max<size_t>(items.size(), 1));
+                if (!items.empty())
+                    CK(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice,
+                                       st));
+                CK(launch_bloom_buckets(keys, d_items, (uint32_t)items.size(), next_item, d_cfg_b, bits, list, lh_cnt,
+                                        lh_cnt + N_BUCKETS, hll_high, st));
+                clk.end();
+                hh.resize((size_t)N_BUCKETS * BUCKET_HLL_M);
+                CK(cudaMemcpyAsync(lh.data(), lh_cnt, 2 * N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(hh.data(), hll_high, hh.size() * 4, cudaMemcpyDeviceToHost, st));
+                ds.release(d_items);
+            } else {
+                // every occurrence goes to the table: the whole bucket is "high"
+                for (uint32_t b = lo; b < hi; ++b) lh[N_BUCKETS + b] = cfg[b].key_len;
+            }
+            Counters c = read_counters(counters, st);
+            check_flags(c.v[C_FLAGS], "partition");
+            ds.release(next_item);
+            ds.release(hll_high);
+            ds.release(lh_cnt);
+            ds.release(bbase);
+            ds.release(cursor);
+            ds.release(d_cfg_b);
+            if (P.bloom) {
+                ds.release(keys);
+                ds.release(bits);
+            }
+            uint64_t pass_low = 0;
+            std::vector<uint64_t> bcaps(N_BUCKETS, 0);
+            for (uint32_t b = lo; b < hi; ++b) {
+                const unsigned long long hb = lh[N_BUCKETS + b];
+                pass_low += lh[b];
+                high_len += hb;
+                double e;
+                if (P.bloom) {
+                    // the registers hold a hash sample of the non-FIRST k-mers
+                    e = hb ? (double)(1u << BUCKET_HLL_SAMPLE_BITS) *
+                                 hll_estimate(&hh[(size_t)b * BUCKET_HLL_M], BUCKET_HLL_M)
+                           : 0.0;
+                } else {
+                    // the job's distinct estimate, shared out by occurrences
+                    e = O ? est * (double)hb / (double)O : 0.0;
+                    e = std::min(e, (double)hb);
+                }
+                e = std::max(e, (double)std::min<unsigned long long>(hb, 4096));
+                bcaps[b] = table_capacity_for(e);
+            }
+            low_len += pass_low;
+            // per-bucket sub-tables in one arena; a bucket whose table
+            // overflows gets twice the slots and the insert is repeated
+            BucketCfg *d_cfg = ds.n<BucketCfg>(N_BUCKETS);
+            unsigned long long *bucket_ovf = ds.n<unsigned long long>(N_BUCKETS);
+            next_item = ds.n<unsigned int>(1);
+            unsigned int *merge_next = ds.n<unsigned int>(1);
+            items.clear();
+            for (uint32_t b = lo; b < hi; ++b)
+                add_items(b, cfg[b].key_base + cfg[b].key_len - lh[N_BUCKETS + b], cfg[b].key_base + cfg[b].key_len);
+            const size_t n_high_items = items.size();
+            for (uint32_t b = lo; b < hi; ++b) add_items(b, cfg[b].key_base, cfg[b].key_base + lh[b]);
+            const size_t n_low_items = items.size() - n_high_items;
             WorkItem *d_items = ds.n<WorkItem>(std::max<size_t>(items.size(), 1));
             if (!items.empty())
                 CK(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, st));
-            CK(launch_bloom_buckets(keys, d_items, (uint32_t)items.size(), next_item, d_cfg_b, bits, list, lh_cnt,
-                                    lh_cnt + N_BUCKETS, hll_high, st));
-            clk.end();
-            hh.resize((size_t)N_BUCKETS * BUCKET_HLL_M);
-            CK(cudaMemcpyAsync(lh.data(), lh_cnt, 2 * N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(hh.data(), hll_high, hh.size() * 4, cudaMemcpyDeviceToHost, st));
-            ds.release(d_items);
-        } else {
-            // every occurrence goes to the table: the whole bucket is "high"
-            for (uint32_t b = 0; b < N_BUCKETS; ++b) lh[N_BUCKETS + b] = cfg[b].key_len;
-        }
-        Counters c = read_counters(counters, st);
-        check_flags(c.v[C_FLAGS], "partition");
-        ds.release(next_item);
-        ds.release(hll_high);
-        ds.release(lh_cnt);
-        ds.release(bbase);
-        ds.release(cursor);
-        ds.release(d_cfg_b);
-        if (P.bloom) {
-            ds.release(keys);
-            ds.release(bits);
-        }
-        low_len = high_len = 0;
-        std::vector<uint64_t> bcaps(N_BUCKETS);
-        for (uint32_t b = 0; b < N_BUCKETS; ++b) {
-            const unsigned long long hb = lh[N_BUCKETS + b];
-            low_len += lh[b];
-            high_len += hb;
-            double e;
-            if (P.bloom) {
-                // the registers hold a hash sample of the non-FIRST k-mers
-                e = hb ? (double)(1u << BUCKET_HLL_SAMPLE_BITS) *
-                             hll_estimate(&hh[(size_t)b * BUCKET_HLL_M], BUCKET_HLL_M)
-                       : 0.0;
-            } else {
-                // the job's distinct estimate, shared out by occurrences
-                e = O ? est * (double)hb / (double)O : 0.0;
-                e = std::min(e, (double)hb);
-            }
-            e = std::max(e, (double)std::min<unsigned long long>(hb, 4096));
-            bcaps[b] = table_capacity_for(e);
-        }
-        // per-bucket sub-tables in one arena; a bucket whose table overflows
-        // gets twice the slots and the insert is repeated
-        d_cfg = ds.n<BucketCfg>(N_BUCKETS);
-        bucket_ovf = ds.n<unsigned long long>(N_BUCKETS);
-        next_item = ds.n<unsigned int>(1);
-        merge_next = ds.n<unsigned int>(1);
-        items.clear();
-        for (uint32_t b = 0; b < N_BUCKETS; ++b)
-            add_items(b, cfg[b].key_base + cfg[b].key_len - lh[N_BUCKETS + b], cfg[b].key_base + cfg[b].key_len);
-        const size_t n_high_items = items.size();
-        for (uint32_t b = 0; b < N_BUCKETS; ++b) add_items(b, cfg[b].key_base, cfg[b].key_base + lh[b]);
-        n_low_items = items.size() - n_high_items;
-        WorkItem *d_items = ds.n<WorkItem>(std::max<size_t>(items.size(), 1));
-        if (!items.empty())
-            CK(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, st));
-        low_items = d_items + n_high_items;
-        for (int attempt = 0;; ++attempt) {
-            cap = 0;
-            for (uint32_t b = 0; b < N_BUCKETS; ++b) {
-                cfg[b].slot_base = cap;
-                cfg[b].slot_cap = bcaps[b];
-                cap += bcaps[b];
-            }
-            if (tr.slots) ds.release(tr.slots);
-            tr.slots = static_cast<Slot *>(ds.get(cap * sizeof(Slot)));
-            tr.mask = 0;   // the arena is addressed per bucket
-            CK(launch_init_slots(tr.slots, cap, st));
-            CK(cudaMemcpyAsync(d_cfg, cfg.data(), N_BUCKETS * sizeof(BucketCfg), cudaMemcpyHostToDevice, st));
-            CK(cudaMemsetAsync(bucket_ovf, 0, N_BUCKETS * 8, st));
-            clk.begin(3);
-            CK(launch_insert_buckets(list, d_items, (uint32_t)n_high_items, next_item, d_cfg, tr.slots,
-                                     max_probe_cap, bucket_ovf, st));
-            clk.end();
-            std::vector<unsigned long long> ov(N_BUCKETS);
-            CK(cudaMemcpyAsync(ov.data(), bucket_ovf, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
-            Counters cc = read_counters(counters, st);
-            check_flags(cc.v[C_FLAGS], "insert");
-            bool any = false;
-            for (uint32_t b = 0; b < N_BUCKETS; ++b)
-                if (ov[b]) {
-                    bcaps[b] *= 2;
-                    any = true;
+            TableRef tr{};
+            uint64_t cap = 0;
+            for (int attempt = 0;; ++attempt) {
+                cap = 0;
+                for (uint32_t b = 0; b < N_BUCKETS; ++b) {
+                    cfg[b].slot_base = cap;
+                    cfg[b].slot_cap = bcaps[b];
+                    cap += bcaps[b];
                 }
-            if (!any) break;
-            if (attempt >= 3) throw KcError{KC_ERR_DEVICE, "counting table overflow"};
+                if (tr.slots) ds.release(tr.slots);
+                tr.slots = static_cast<Slot *>(ds.get(std::max<uint64_t>(cap, 1) * sizeof(Slot)));
+                tr.mask = 0;   // the arena is addressed per bucket
+                CK(launch_init_slots(tr.slots, cap, st));
+                CK(cudaMemcpyAsync(d_cfg, cfg.data(), N_BUCKETS * sizeof(BucketCfg), cudaMemcpyHostToDevice, st));
+                CK(cudaMemsetAsync(bucket_ovf, 0, N_BUCKETS * 8, st));
+                clk.begin(3);
+                CK(launch_insert_buckets(list, d_items, (uint32_t)n_high_items, next_item, d_cfg, tr.slots,
+                                         max_probe_cap, bucket_ovf, st));
+                clk.end();
+                std::vector<unsigned long long> ov(N_BUCKETS);
+                CK(cudaMemcpyAsync(ov.data(), bucket_ovf, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
+                Counters cc = read_counters(counters, st);
+                check_flags(cc.v[C_FLAGS], "insert");
+                bool any = false;
+                for (uint32_t b = 0; b < N_BUCKETS; ++b)
+                    if (ov[b]) {
+                        bcaps[b] *= 2;
+                        any = true;
+                    }
+                if (!any) break;
+                if (attempt >= 3) throw KcError{KC_ERR_DEVICE, "counting table overflow"};
+            }
+            table_cap = std::max(table_cap, cap);
+            compact_table(tr, cap, pass_low, list, d_items + n_high_items, n_low_items, merge_next, d_cfg);
+            if (multi) {
+                // this pass's records wait in pinned host memory; its device
+                // memory goes to the next pass
+                auto hr = std::make_unique<HostRecords>();
+                hr->allocate(n_rec);
+                if (n_rec) {
+                    CK(cudaMemcpyAsync(hr->keys(), rec_keys, n_rec * 8, cudaMemcpyDeviceToHost, st));
+                    CK(cudaMemcpyAsync(hr->counts(), rec_counts, n_rec * 4, cudaMemcpyDeviceToHost, st));
+                }
+                CK(cudaStreamSynchronize(st));
+                spilled_total += n_rec;
+                spilled.push_back(std::move(hr));
+                ds.rewind(mk);
+            }
+        }
+        if (exact && filled_total != O)
+            throw KcError{KC_ERR_DEVICE, "partition does not add up to the occurrences"};
+        O = filled_total;
+        job.occurrences = O;
+        job.passes = (uint32_t)ranges.size();
+        if (multi) {
+            n_rec = spilled_total;
+            rec_keys = ds.n<unsigned long long>(std::max<uint64_t>(n_rec, 1));
+            rec_counts = ds.n<uint32_t>(std::max<uint64_t>(n_rec, 1));
+            uint64_t at = 0;
+            for (auto &hr : spilled) {
+                if (hr->n) {
+                    CK(cudaMemcpyAsync(rec_keys + at, hr->keys(), hr->n * 8, cudaMemcpyHostToDevice, st));
+                    CK(cudaMemcpyAsync(rec_counts + at, hr->counts(), hr->n * 4, cudaMemcpyHostToDevice, st));
+                }
+                at += hr->n;
+            }
+            CK(cudaStreamSynchronize(st));
         }
     }
-    job.table_cap = cap;
-
-    // ---- records ------------------------------------------------------------
-    const uint32_t count_max = P.count_max ? P.count_max : 255u;
-    unsigned long long *n_keys = ds.n<unsigned long long>(1);
-    CK(cudaMemsetAsync(n_keys, 0, 8, st));
-    clk.begin(5);
-    CK(launch_count_keys(tr.slots, cap, n_keys, st));
-    clk.end();
-    unsigned long long in_table = 0;
-    CK(cudaMemcpyAsync(&in_table, n_keys, 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    const uint64_t rec_cap = std::max<uint64_t>(in_table + low_len, 1);
-    unsigned long long *rec_keys = ds.n<unsigned long long>(rec_cap);
-    uint32_t *rec_counts = ds.n<uint32_t>(rec_cap);
-    unsigned long long *hist = ds.n<unsigned long long>(HIST_BINS);
-    const uint64_t ovf_cap = 1 << 20;
-    uint32_t *ovf = ds.n<uint32_t>(ovf_cap);
-    CK(cudaMemsetAsync(hist, 0, HIST_BINS * 8, st));
-    if (P.bloom && low_len) {
-        clk.begin(4);
-        CK(launch_merge_buckets(list, low_items, (uint32_t)n_low_items, merge_next, d_cfg, tr.slots, max_probe_cap,
-                                P.min_count, P.max_count, rec_keys, rec_counts, rec_cap, counters, st));
-        clk.end();
-    }
-    clk.begin(5);
-    CK(launch_compact(tr, cap, count_max, P.min_count, P.max_count, rec_keys, rec_counts, rec_cap, hist, ovf, ovf_cap,
-                      counters, st));
-    clk.end();
-    Counters c2 = read_counters(counters, st);
-    check_flags(c2.v[C_FLAGS], "compact");
-    if (c2.v[C_FLAGS] & ERR_TABLE_FULL) throw KcError{KC_ERR_DEVICE, "counting table lookup overflow"};
-    const uint64_t n_rec = c2.v[C_REC_LEN];
-    job.distinct = c2.v[C_DISTINCT] + c2.v[C_LOW_ONLY];
-    job.low_only = c2.v[C_LOW_ONLY];
-    if (list) ds.release(list);
-    ds.release(tr.slots);
-    tr.slots = nullptr;
+    job.table_cap = table_cap;
+    const Counters c2 = read_counters(counters, st);
 
     // ---- sort in printed-string order ---------------------------------------
     clk.begin(6);
@@ -1325,6 +1398,7 @@ int kc_result(kc_handle *h, kc_job_id id, kc_result_t *out)
     out->high_len = j.high_len;
     out->input_bytes = j.input_bytes;
     out->n_records_total = j.n_records_total;
+    out->passes = j.passes;
     return KC_OK;
 }
 

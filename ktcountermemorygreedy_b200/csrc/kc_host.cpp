@@ -101,6 +101,15 @@ void *Workspace::get(size_t bytes)
     return p;
 }
 
+void Workspace::rewind(const Mark &m)
+{
+    if (m.top <= top_) top_ = m.top;
+    while (spill_.size() > m.n_spill) {
+        cudaFreeAsync(spill_.back(), st_);
+        spill_.pop_back();
+    }
+}
+
 bool Workspace::release_top(void *p, size_t bytes)
 {
     if (base_ && p == base_ + top_ - bytes) {
@@ -141,6 +150,14 @@ void DevScope::release(void *p)
     if (!ws) cudaFreeAsync(p, st);
     else ws->release_top(p, it->second);   // memory further down stays until the job ends
     ptrs.erase(it);
+}
+
+void DevScope::rewind(const Mark &m)
+{
+    if (ws) ws->rewind(m.ws);
+    else
+        for (size_t i = m.n_ptrs; i < ptrs.size(); ++i) cudaFreeAsync(ptrs[i].first, st);
+    if (ptrs.size() > m.n_ptrs) ptrs.resize(m.n_ptrs);
 }
 
 DevScope::~DevScope()

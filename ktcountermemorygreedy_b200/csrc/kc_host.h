@@ -44,6 +44,12 @@ public:
     Workspace &operator=(const Workspace &) = delete;
     void begin_job();
     void reserve(size_t bytes);   // grow the block to at least `bytes` now
+    // everything handed out after a mark can be taken back at once
+    struct Mark {
+        size_t top, n_spill;
+    };
+    Mark mark() const { return Mark{top_, spill_.size()}; }
+    void rewind(const Mark &m);
     void *get(size_t bytes);
     bool release_top(void *p, size_t bytes);
     void end_job();
@@ -74,6 +80,13 @@ struct DevScope {
         return static_cast<T *>(get(count * sizeof(T)));
     }
     void release(void *p);
+    // takes back every allocation of this scope made after the mark
+    struct Mark {
+        size_t n_ptrs;
+        Workspace::Mark ws;
+    };
+    Mark mark() const { return Mark{ptrs.size(), ws ? ws->mark() : Workspace::Mark{0, 0}}; }
+    void rewind(const Mark &m);
     ~DevScope();
 };
 

@@ -509,10 +509,14 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
                 } else if (MODE == MODE_PART) {
                     // scatter into the root-prefix buckets: rank inside the
                     // tile's share of each bucket, one cursor update per bucket
+                    // (a pass of a multi-pass job keeps only its range of buckets)
+                    const uint32_t blo = a.bucket_lo, bhi = a.bucket_hi ? a.bucket_hi : N_BUCKETS;
                     s_bhist[tid] = 0;
                     __syncthreads();
-                    for (uint32_t i = tid; i < nr; i += EXT_THREADS)
-                        s_rank[i] = (uint16_t)atomicAdd(&s_bhist[(uint32_t)(s_stage[i] >> 56)], 1u);
+                    for (uint32_t i = tid; i < nr; i += EXT_THREADS) {
+                        const uint32_t b = (uint32_t)(s_stage[i] >> 56);
+                        s_rank[i] = (b >= blo && b < bhi) ? (uint16_t)atomicAdd(&s_bhist[b], 1u) : (uint16_t)0xFFFFu;
+                    }
                     __syncthreads();
                     // the round's k-mers are reordered by bucket in shared
                     // memory, so that consecutive threads store consecutive
@@ -531,7 +535,7 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
 #pragma unroll
                     for (uint32_t r = 0; r < STAGE_CAP / EXT_THREADS; ++r) {
                         const uint32_t i = tid + r * EXT_THREADS;
-                        if (i < nr) {
+                        if (i < nr && s_rank[i] != 0xFFFFu) {
                             kr[r] = s_stage[i];
                             s_rank[i] = (uint16_t)(s_hist[(uint32_t)(kr[r] >> 56)] + s_rank[i]);
                         }
@@ -540,10 +544,10 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
 #pragma unroll
                     for (uint32_t r = 0; r < STAGE_CAP / EXT_THREADS; ++r) {
                         const uint32_t i = tid + r * EXT_THREADS;
-                        if (i < nr) s_stage[s_rank[i]] = kr[r];
+                        if (i < nr && s_rank[i] != 0xFFFFu) s_stage[s_rank[i]] = kr[r];
                     }
                     __syncthreads();
-                    for (uint32_t i = tid; i < nr; i += EXT_THREADS) {
+                    for (uint32_t i = tid; i < tot_b; i += EXT_THREADS) {
                         const unsigned long long key = s_stage[i];
                         const uint32_t b = (uint32_t)(key >> 56);
                         const unsigned long long pos = s_bpos[b] + i;

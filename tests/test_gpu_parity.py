@@ -181,6 +181,27 @@ def test_bloom_job_sampled_census(counter):
         assert np.array_equal(r.keys, want_k) and np.array_equal(r.counts, want_c)
 
 
+def test_multi_pass_jobs_match_single_pass(counter):
+    """A job whose pass budget is smaller than its k-mer arrays, filters and
+    tables runs in several passes over ranges of root prefixes, each pass's
+    records kept in pinned host memory until the final sort.  Bloom and plain
+    jobs, with count filters and queries, against the oracle and against the
+    same job in one pass."""
+    import ktcountermemorygreedy_b200.synth as S
+    g = S.genome(41, 2_000_000)
+    fq = S.reads(g, 41, 30_000, (150, 150), 0.01, 0.0).tobytes()
+    kw = dict(count_max=U32, top_n=300, want_le2=True, hist_max=100)
+    for bloom, mc in ((True, 2), (False, 1)):
+        want_k, want_c = O.exact_records([fq], 31, U32, min_count=mc)
+        one = counter.count([fq], k=31, bloom=bloom, memory_gb=2, min_count=mc, **kw)
+        many = counter.count([fq], k=31, bloom=bloom, memory_gb=2, min_count=mc, pass_bytes=24 << 20, **kw)
+        assert one.passes == 1 and many.passes >= 4, (one.passes, many.passes)
+        assert np.array_equal(many.keys, want_k) and np.array_equal(many.counts, want_c)
+        for f in ("keys", "counts", "hist", "top_keys", "top_counts", "le2_keys", "le2_counts"):
+            assert np.array_equal(getattr(many, f), getattr(one, f)), (bloom, f)
+        assert many.occurrences == one.occurrences and many.distinct == one.distinct
+
+
 def test_bloom_job_census_overflow_falls_back_to_exact(counter):
     """Every 8th tile random, the others one homopolymer: the sampled census
     underestimates the homopolymer's bucket, its region overflows and the job
