@@ -381,7 +381,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
     uint32_t *rec_counts = nullptr;
     uint64_t n_rec = 0;
     auto compact_table = [&](const TableRef &t, uint64_t cap, uint64_t n_low, const unsigned long long *lst,
-                             const WorkItem *low_items, size_t n_low_items, unsigned int *merge_next,
+                             const BucketRanges *low_rg, uint32_t n_low_items, unsigned int *merge_next,
                              const BucketCfg *d_cfg) {
         CK(cudaMemsetAsync(n_keys, 0, 8, st));
         CK(cudaMemsetAsync(counters + C_REC_LEN, 0, 3 * 8, st));   // C_REC_LEN, C_LOW_ONLY, C_DISTINCT
@@ -396,7 +396,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
         rec_counts = ds.n<uint32_t>(rec_cap);
         if (n_low) {
             clk.begin(4);
-            CK(launch_merge_buckets(lst, low_items, (uint32_t)n_low_items, merge_next, d_cfg, t.slots, max_probe_cap,
+            CK(launch_merge_buckets(lst, low_rg, n_low_items, merge_next, d_cfg, t.slots, max_probe_cap,
                                     P.min_count, P.max_count, rec_keys, rec_counts, rec_cap, counters, st));
             clk.end();
         }
@@ -471,12 +471,22 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
         // of a pass (k-mer arrays, filters, tables, records of its buckets)
         uint64_t budget = P.pass_bytes;
         if (!budget) {
-            // free device memory plus the part of this worker's workspace the
-            // job has not used yet
+            // free device memory, the part of this worker's workspace the job
+            // has not used yet, and what the stream-ordered pool holds unused
             size_t free_b = 0, total_b = 0;
             CK(cudaMemGetInfo(&free_b, &total_b));
             const size_t ws_free = ws.capacity() > ws.mark().top ? ws.capacity() - ws.mark().top : 0;
-            budget = (uint64_t)(0.7 * (double)(free_b + ws_free));
+            uint64_t pool_slack = 0;
+            int dev = 0;
+            cudaMemPool_t pool;
+            if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+                uint64_t reserved = 0, used = 0;
+                if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+                    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+                    pool_slack = reserved - used;
+            }
+            cudaGetLastError();
+            budget = (uint64_t)(0.7 * (double)(free_b + ws_free + pool_slack));
         }
         const uint64_t per_occ = P.bloom ? 40 : 48;
         std::vector<std::pair<uint32_t, uint32_t>> ranges;
@@ -560,27 +570,31 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
                 filled_total += fill[b];
             }
             CK(cudaMemcpyAsync(d_cfg_b, cfg.data(), N_BUCKETS * sizeof(BucketCfg), cudaMemcpyHostToDevice, st));
-            std::vector<WorkItem> items;
-            auto add_items = [&](uint32_t b, unsigned long long begin, unsigned long long end) {
-                for (unsigned long long s0 = begin; s0 < end; s0 += WORK_ITEM_KEYS)
-                    items.push_back(WorkItem{s0, std::min<unsigned long long>(end, s0 + WORK_ITEM_KEYS), b, 0});
+            // each bucket-major launch gets its 256 ranges, not a list of items
+            auto upload_ranges = [&](BucketRanges &r, uint32_t &n_items) {
+                n_items = fill_item_starts(r);
+                BucketRanges *d = ds.n<BucketRanges>(1);
+                CK(cudaMemcpyAsync(d, &r, sizeof(BucketRanges), cudaMemcpyHostToDevice, st));
+                return d;
             };
             std::vector<unsigned long long> lh(2 * N_BUCKETS, 0);
             std::vector<uint32_t> hh;
             if (P.bloom) {
                 clk.begin(8);
-                for (uint32_t b = lo; b < hi; ++b) add_items(b, cfg[b].key_base, cfg[b].key_base + cfg[b].key_len);
-                WorkItem *d_items = ds.n<WorkItem>(std::max<size_t>(items.size(), 1));
-                if (!items.empty())
-                    CK(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice,
-                                       st));
-                CK(launch_bloom_buckets(keys, d_items, (uint32_t)items.size(), next_item, d_cfg_b, bits, list, lh_cnt,
-                                        lh_cnt + N_BUCKETS, hll_high, st));
+                BucketRanges br{};
+                for (uint32_t b = lo; b < hi; ++b) {
+                    br.begin[b] = cfg[b].key_base;
+                    br.len[b] = cfg[b].key_len;
+                }
+                uint32_t n_items = 0;
+                BucketRanges *d_br = upload_ranges(br, n_items);
+                CK(launch_bloom_buckets(keys, d_br, n_items, next_item, d_cfg_b, bits, list, lh_cnt, lh_cnt + N_BUCKETS,
+                                        hll_high, st));
                 clk.end();
                 hh.resize((size_t)N_BUCKETS * BUCKET_HLL_M);
                 CK(cudaMemcpyAsync(lh.data(), lh_cnt, 2 * N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
                 CK(cudaMemcpyAsync(hh.data(), hll_high, hh.size() * 4, cudaMemcpyDeviceToHost, st));
-                ds.release(d_items);
+                ds.release(d_br);
             } else {
                 // every occurrence goes to the table: the whole bucket is "high"
                 for (uint32_t b = lo; b < hi; ++b) lh[N_BUCKETS + b] = cfg[b].key_len;
@@ -624,15 +638,16 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
             unsigned long long *bucket_ovf = ds.n<unsigned long long>(N_BUCKETS);
             next_item = ds.n<unsigned int>(1);
             unsigned int *merge_next = ds.n<unsigned int>(1);
-            items.clear();
-            for (uint32_t b = lo; b < hi; ++b)
-                add_items(b, cfg[b].key_base + cfg[b].key_len - lh[N_BUCKETS + b], cfg[b].key_base + cfg[b].key_len);
-            const size_t n_high_items = items.size();
-            for (uint32_t b = lo; b < hi; ++b) add_items(b, cfg[b].key_base, cfg[b].key_base + lh[b]);
-            const size_t n_low_items = items.size() - n_high_items;
-            WorkItem *d_items = ds.n<WorkItem>(std::max<size_t>(items.size(), 1));
-            if (!items.empty())
-                CK(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, st));
+            BucketRanges hr{}, lr{};
+            for (uint32_t b = lo; b < hi; ++b) {
+                hr.begin[b] = cfg[b].key_base + cfg[b].key_len - lh[N_BUCKETS + b];
+                hr.len[b] = lh[N_BUCKETS + b];
+                lr.begin[b] = cfg[b].key_base;
+                lr.len[b] = lh[b];
+            }
+            uint32_t n_high_items = 0, n_low_items = 0;
+            BucketRanges *d_hr = upload_ranges(hr, n_high_items);
+            BucketRanges *d_lr = upload_ranges(lr, n_low_items);
             TableRef tr{};
             uint64_t cap = 0;
             for (int attempt = 0;; ++attempt) {
@@ -649,8 +664,8 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
                 CK(cudaMemcpyAsync(d_cfg, cfg.data(), N_BUCKETS * sizeof(BucketCfg), cudaMemcpyHostToDevice, st));
                 CK(cudaMemsetAsync(bucket_ovf, 0, N_BUCKETS * 8, st));
                 clk.begin(3);
-                CK(launch_insert_buckets(list, d_items, (uint32_t)n_high_items, next_item, d_cfg, tr.slots,
-                                         max_probe_cap, bucket_ovf, st));
+                CK(launch_insert_buckets(list, d_hr, n_high_items, next_item, d_cfg, tr.slots, max_probe_cap, bucket_ovf,
+                                         st));
                 clk.end();
                 std::vector<unsigned long long> ov(N_BUCKETS);
                 CK(cudaMemcpyAsync(ov.data(), bucket_ovf, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
@@ -666,7 +681,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
                 if (attempt >= 3) throw KcError{KC_ERR_DEVICE, "counting table overflow"};
             }
             table_cap = std::max(table_cap, cap);
-            compact_table(tr, cap, pass_low, list, d_items + n_high_items, n_low_items, merge_next, d_cfg);
+            compact_table(tr, cap, pass_low, list, d_lr, n_low_items, merge_next, d_cfg);
             if (multi) {
                 // this pass's records wait in pinned host memory; its device
                 // memory goes to the next pass

@@ -513,9 +513,14 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
                     const uint32_t blo = a.bucket_lo, bhi = a.bucket_hi ? a.bucket_hi : N_BUCKETS;
                     s_bhist[tid] = 0;
                     __syncthreads();
-                    for (uint32_t i = tid; i < nr; i += EXT_THREADS) {
-                        const uint32_t b = (uint32_t)(s_stage[i] >> 56);
-                        s_rank[i] = (b >= blo && b < bhi) ? (uint16_t)atomicAdd(&s_bhist[b], 1u) : (uint16_t)0xFFFFu;
+                    if (blo == 0 && bhi == N_BUCKETS) {
+                        for (uint32_t i = tid; i < nr; i += EXT_THREADS)
+                            s_rank[i] = (uint16_t)atomicAdd(&s_bhist[(uint32_t)(s_stage[i] >> 56)], 1u);
+                    } else {
+                        for (uint32_t i = tid; i < nr; i += EXT_THREADS) {
+                            const uint32_t b = (uint32_t)(s_stage[i] >> 56);
+                            s_rank[i] = (b >= blo && b < bhi) ? (uint16_t)atomicAdd(&s_bhist[b], 1u) : (uint16_t)0xFFFFu;
+                        }
                     }
                     __syncthreads();
                     // the round's k-mers are reordered by bucket in shared
@@ -1333,6 +1338,30 @@ __global__ void k_scatter_selected(const unsigned long long *keys, const uint32_
 constexpr uint32_t ITEM_PER_THREAD = WORK_ITEM_KEYS / 256;
 
 // Claims the next work item for the whole block; false when none is left.
+// Work item `it` of a launch: its bucket is the last one whose first item is
+// at or before it (empty buckets share their first item with the next one).
+__device__ __forceinline__ WorkItem work_item(const BucketRanges *rg, const uint32_t *s_item0, uint32_t it)
+{
+    uint32_t lo = 0, hi = N_BUCKETS;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_item0[mid] <= it) lo = mid; else hi = mid;
+    }
+    WorkItem w;
+    w.bucket = lo;
+    const unsigned long long b0 = rg->begin[lo], e0 = b0 + rg->len[lo];
+    w.begin = b0 + (unsigned long long)(it - s_item0[lo]) * WORK_ITEM_KEYS;
+    w.end = w.begin + WORK_ITEM_KEYS < e0 ? w.begin + WORK_ITEM_KEYS : e0;
+    w.pad = 0;
+    return w;
+}
+
+__device__ __forceinline__ void load_item_starts(const BucketRanges *rg, uint32_t *s_item0)
+{
+    for (uint32_t i = threadIdx.x; i <= N_BUCKETS; i += blockDim.x) s_item0[i] = rg->item0[i];
+    __syncthreads();
+}
+
 __device__ __forceinline__ bool next_work(unsigned int *next_item, uint32_t n_items, uint32_t *s_item, uint32_t &it)
 {
     if (threadIdx.x == 0) *s_item = atomicAdd(next_item, 1u);
@@ -1368,12 +1397,18 @@ __device__ __forceinline__ void hll_add_token(uint32_t *regs, uint32_t tok)
 // bucket's range in `out`, the others to its back.  Only FIRST versus not
 // FIRST matters downstream, so both filter words are read with one 16-byte
 // load and the first word is set without reading its old value.
-__global__ void __launch_bounds__(256, 4) k_bloom_buckets(const unsigned long long *keys, const WorkItem *items,
+// k-mers per thread whose filter words are in flight together: two keep the
+// kernel at 40 registers (six blocks per SM); four needed 64 (four blocks).
+constexpr uint32_t BLOOM_GROUP = 2;
+
+__global__ void __launch_bounds__(256, 6) k_bloom_buckets(const unsigned long long *keys, const BucketRanges *rg,
                                                        uint32_t n_items, unsigned int *next_item,
                                                        const BucketCfg *cfg, unsigned long long *bits,
                                                        unsigned long long *out, unsigned long long *low_cnt,
                                                        unsigned long long *high_cnt, uint32_t *hll_high)
 {
+    __shared__ uint32_t s_item0[N_BUCKETS + 1];
+    load_item_starts(rg, s_item0);
     __shared__ uint32_t s_item, s_warp[8];
     __shared__ unsigned long long s_lb, s_hb;
     // each thread's k-mers wait here (not in registers) while their filter
@@ -1382,7 +1417,7 @@ __global__ void __launch_bounds__(256, 4) k_bloom_buckets(const unsigned long lo
     const int tid = threadIdx.x;
     uint32_t it;
     while (next_work(next_item, n_items, &s_item, it)) {
-        const WorkItem w = items[it];
+        const WorkItem w = work_item(rg, s_item0, it);
         const BucketCfg bc = cfg[w.bucket];
         const uint64_t n = w.end - w.begin;
         uint32_t firsts = 0, highs = 0;
@@ -1394,13 +1429,13 @@ __global__ void __launch_bounds__(256, 4) k_bloom_buckets(const unsigned long lo
         }
         uint32_t *regs = hll_high + (size_t)w.bucket * BUCKET_HLL_M;
 #pragma unroll
-        for (uint32_t g = 0; g < ITEM_PER_THREAD; g += 4) {
-            unsigned long long m[4];
-            uint32_t tok[4];
-            ulonglong2 *cell[4];
-            ulonglong2 v[4];
+        for (uint32_t g = 0; g < ITEM_PER_THREAD; g += BLOOM_GROUP) {
+            unsigned long long m[BLOOM_GROUP];
+            uint32_t tok[BLOOM_GROUP];
+            ulonglong2 *cell[BLOOM_GROUP];
+            ulonglong2 v[BLOOM_GROUP];
 #pragma unroll
-            for (uint32_t u = 0; u < 4; ++u) {
+            for (uint32_t u = 0; u < BLOOM_GROUP; ++u) {
                 const uint64_t i = (uint64_t)(g + u) * 256 + tid;
                 uint64_t block = 0, mask = 0, hi = 0;
                 if (i < n) bloom_probe_hi(s_k[(g + u) * 256 + tid], bc.bloom_cap, block, mask, hi);
@@ -1409,15 +1444,15 @@ __global__ void __launch_bounds__(256, 4) k_bloom_buckets(const unsigned long lo
                 cell[u] = reinterpret_cast<ulonglong2 *>(bits + bc.bloom_off + 2 * block);
             }
 #pragma unroll
-            for (uint32_t u = 0; u < 4; ++u)
+            for (uint32_t u = 0; u < BLOOM_GROUP; ++u)
                 if ((uint64_t)(g + u) * 256 + tid < n) v[u] = __ldcg(cell[u]);
             // occurrences not yet known to be repeats set their bits in the
-            // seen-once word; the four returning atomics are issued back to
+            // seen-once word; the group's returning atomics are issued back to
             // back and their old values examined afterwards
-            unsigned long long old2[4];
+            unsigned long long old2[BLOOM_GROUP];
             uint32_t pending = 0;
 #pragma unroll
-            for (uint32_t u = 0; u < 4; ++u) {
+            for (uint32_t u = 0; u < BLOOM_GROUP; ++u) {
                 if ((uint64_t)(g + u) * 256 + tid >= n) continue;
                 unsigned long long *c = reinterpret_cast<unsigned long long *>(cell[u]);
                 if ((v[u].x & m[u]) == m[u]) continue;              // seen twice already
@@ -1428,7 +1463,7 @@ __global__ void __launch_bounds__(256, 4) k_bloom_buckets(const unsigned long lo
                 }
             }
 #pragma unroll
-            for (uint32_t u = 0; u < 4; ++u) {
+            for (uint32_t u = 0; u < BLOOM_GROUP; ++u) {
                 if ((uint64_t)(g + u) * 256 + tid >= n) continue;
                 bool first = false;
                 if ((pending >> u) & 1u) {
@@ -1462,16 +1497,18 @@ __global__ void __launch_bounds__(256, 4) k_bloom_buckets(const unsigned long lo
     }
 }
 
-__global__ void __launch_bounds__(256) k_insert_buckets(const unsigned long long *keys, const WorkItem *items,
+__global__ void __launch_bounds__(256) k_insert_buckets(const unsigned long long *keys, const BucketRanges *rg,
                                                         uint32_t n_items, unsigned int *next_item,
                                                         const BucketCfg *cfg, Slot *arena, uint32_t max_probe,
                                                         unsigned long long *bucket_ovf)
 {
+    __shared__ uint32_t s_item0[N_BUCKETS + 1];
+    load_item_starts(rg, s_item0);
     __shared__ uint32_t s_item;
     const int tid = threadIdx.x;
     uint32_t it;
     while (next_work(next_item, n_items, &s_item, it)) {
-        const WorkItem w = items[it];
+        const WorkItem w = work_item(rg, s_item0, it);
         const BucketCfg bc = cfg[w.bucket];
         const TableRef tr{arena + bc.slot_base, bc.slot_cap - 1};
         const uint64_t n = w.end - w.begin;
@@ -1491,20 +1528,22 @@ __global__ void __launch_bounds__(256) k_insert_buckets(const unsigned long long
     }
 }
 
-__global__ void __launch_bounds__(256) k_merge_buckets(const unsigned long long *keys, const WorkItem *items,
+__global__ void __launch_bounds__(256) k_merge_buckets(const unsigned long long *keys, const BucketRanges *rg,
                                                        uint32_t n_items, unsigned int *next_item,
                                                        const BucketCfg *cfg, Slot *arena, uint32_t max_probe,
                                                        uint32_t min_count, uint32_t max_count,
                                                        unsigned long long *rec_keys, uint32_t *rec_counts,
                                                        uint64_t rec_cap, unsigned long long *counters)
 {
+    __shared__ uint32_t s_item0[N_BUCKETS + 1];
+    load_item_starts(rg, s_item0);
     __shared__ uint32_t s_item, s_warp[8];
     __shared__ unsigned long long s_base;
     const int tid = threadIdx.x;
     const bool want1 = (min_count <= 1 && 1 <= max_count);
     uint32_t it;
     while (next_work(next_item, n_items, &s_item, it)) {
-        const WorkItem w = items[it];
+        const WorkItem w = work_item(rg, s_item0, it);
         const BucketCfg bc = cfg[w.bucket];
         const TableRef tr{arena + bc.slot_base, bc.slot_cap - 1};
         const uint64_t n = w.end - w.begin;
@@ -2039,7 +2078,18 @@ static int persistent_grid(K kernel)
     return sm_count() * per_sm;
 }
 
-cudaError_t launch_bloom_buckets(const unsigned long long *keys, const WorkItem *items, uint32_t n_items,
+uint32_t fill_item_starts(BucketRanges &r)
+{
+    uint32_t n = 0;
+    for (uint32_t b = 0; b < N_BUCKETS; ++b) {
+        r.item0[b] = n;
+        n += (uint32_t)((r.len[b] + WORK_ITEM_KEYS - 1) / WORK_ITEM_KEYS);
+    }
+    r.item0[N_BUCKETS] = n;
+    return n;
+}
+
+cudaError_t launch_bloom_buckets(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                  unsigned int *next_item, const BucketCfg *cfg, unsigned long long *bits,
                                  unsigned long long *out, unsigned long long *low_cnt, unsigned long long *high_cnt,
                                  uint32_t *hll_high, cudaStream_t st)
@@ -2049,11 +2099,11 @@ cudaError_t launch_bloom_buckets(const unsigned long long *keys, const WorkItem 
     if (e != cudaSuccess) return e;
     note_launch();
     k_bloom_buckets<<<std::min<int>(persistent_grid(k_bloom_buckets), n_items), 256, 0, st>>>(
-        keys, items, n_items, next_item, cfg, bits, out, low_cnt, high_cnt, hll_high);
+        keys, rg, n_items, next_item, cfg, bits, out, low_cnt, high_cnt, hll_high);
     return cudaGetLastError();
 }
 
-cudaError_t launch_insert_buckets(const unsigned long long *keys, const WorkItem *items, uint32_t n_items,
+cudaError_t launch_insert_buckets(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                   unsigned int *next_item, const BucketCfg *cfg, Slot *arena, uint32_t max_probe,
                                   unsigned long long *bucket_ovf, cudaStream_t st)
 {
@@ -2062,11 +2112,11 @@ cudaError_t launch_insert_buckets(const unsigned long long *keys, const WorkItem
     if (e != cudaSuccess) return e;
     note_launch();
     k_insert_buckets<<<std::min<int>(persistent_grid(k_insert_buckets), n_items), 256, 0, st>>>(
-        keys, items, n_items, next_item, cfg, arena, max_probe, bucket_ovf);
+        keys, rg, n_items, next_item, cfg, arena, max_probe, bucket_ovf);
     return cudaGetLastError();
 }
 
-cudaError_t launch_merge_buckets(const unsigned long long *keys, const WorkItem *items, uint32_t n_items,
+cudaError_t launch_merge_buckets(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                  unsigned int *next_item, const BucketCfg *cfg, Slot *arena, uint32_t max_probe,
                                  uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
                                  uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *counters, cudaStream_t st)
@@ -2076,7 +2126,7 @@ cudaError_t launch_merge_buckets(const unsigned long long *keys, const WorkItem 
     if (e != cudaSuccess) return e;
     note_launch();
     k_merge_buckets<<<std::min<int>(persistent_grid(k_merge_buckets), n_items), 256, 0, st>>>(
-        keys, items, n_items, next_item, cfg, arena, max_probe, min_count, max_count, rec_keys, rec_counts, rec_cap,
+        keys, rg, n_items, next_item, cfg, arena, max_probe, min_count, max_count, rec_keys, rec_counts, rec_cap,
         counters);
     return cudaGetLastError();
 }

@@ -135,6 +135,16 @@ struct WorkItem {
     uint32_t pad;
 };
 
+// The work of one bucket-major launch, 256 ranges instead of a list of work
+// items: bucket b's keys [begin[b], begin[b] + len[b]) in runs of
+// WORK_ITEM_KEYS, whose first run is item item0[b] (item0[N_BUCKETS] = all).
+// A block turns its item number into a bucket and range by itself.
+struct BucketRanges {
+    unsigned long long begin[N_BUCKETS], len[N_BUCKETS];
+    uint32_t item0[N_BUCKETS + 1];
+};
+uint32_t fill_item_starts(BucketRanges &r);   // sets item0 from len, returns the number of items
+
 // Per-bucket state of the partitioned pipeline.
 struct BucketCfg {
     unsigned long long key_base, key_len;    // bucket's range in the partitioned key array
@@ -215,14 +225,14 @@ cudaError_t launch_select_range(const unsigned long long *keys, const uint32_t *
                                 unsigned long long *counters, int counter_idx, cudaStream_t st);
 
 // Bucket-major kernels of the partitioned pipeline; each resets *next_item.
-cudaError_t launch_bloom_buckets(const unsigned long long *keys, const WorkItem *items, uint32_t n_items,
+cudaError_t launch_bloom_buckets(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                  unsigned int *next_item, const BucketCfg *cfg, unsigned long long *bits,
                                  unsigned long long *out, unsigned long long *low_cnt, unsigned long long *high_cnt,
                                  uint32_t *hll_high, cudaStream_t st);
-cudaError_t launch_insert_buckets(const unsigned long long *keys, const WorkItem *items, uint32_t n_items,
+cudaError_t launch_insert_buckets(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                   unsigned int *next_item, const BucketCfg *cfg, Slot *arena, uint32_t max_probe,
                                   unsigned long long *bucket_ovf, cudaStream_t st);
-cudaError_t launch_merge_buckets(const unsigned long long *keys, const WorkItem *items, uint32_t n_items,
+cudaError_t launch_merge_buckets(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                  unsigned int *next_item, const BucketCfg *cfg, Slot *arena, uint32_t max_probe,
                                  uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
                                  uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *counters, cudaStream_t st);

@@ -38,6 +38,7 @@ class RequestStats:
     run_ms: float                    # start -> end
     submit_late_ms: float            # actual submission - scheduled arrival
     device_ms: float                 # device time of the job's pipeline
+    passes: int                      # counting passes (more than one when the device was short of memory)
     occurrences: int
     distinct: int
     n_le2: int
@@ -77,17 +78,18 @@ def serve(counter, requests: Sequence[Request]):
         submitted[i].wait()
         r = requests[i]
         if errors[i]:
-            stats[i] = RequestStats(math.nan, 0, 0, late[i], 0, 0, 0, 0, 0, errors[i])
+            stats[i] = RequestStats(math.nan, 0, 0, late[i], 0, 0, 0, 0, 0, 0, errors[i])
             continue
         try:
             counter.wait(ids[i])
             res = counter.result(ids[i], r.k, copy=False)
         except Exception as e:
-            stats[i] = RequestStats(math.nan, 0, 0, late[i], 0, 0, 0, 0, 0, str(e))
+            stats[i] = RequestStats(math.nan, 0, 0, late[i], 0, 0, 0, 0, 0, 0, str(e))
             continue
         lat = late[i] + res.queue_ms + res.run_ms
         end_max = max(end_max, r.arrival_s * 1000.0 + lat)
-        stats[i] = RequestStats(lat, res.queue_ms, res.run_ms, late[i], res.device_ms, int(res.occurrences),
+        stats[i] = RequestStats(lat, res.queue_ms, res.run_ms, late[i], res.device_ms, int(getattr(res, "passes", 1)),
+                                int(res.occurrences),
                                 int(res.distinct),
                                 int(len(res.le2_keys)), int(np.asarray(res.hist).sum()))
         del res
@@ -105,4 +107,5 @@ def summarize(stats: Sequence[RequestStats], wall_s: float) -> dict:
             "mean_ms": float(lat.mean()), "kmers_per_s": occ / wall_s, "wall_s": wall_s, "occurrences": occ,
             "mean_queue_ms": float(np.mean([s.queue_ms for s in ok])) if ok else 0.0,
             "mean_run_ms": float(np.mean([s.run_ms for s in ok])) if ok else 0.0,
-            "mean_device_ms": float(np.mean([s.device_ms for s in ok])) if ok else 0.0}
+            "mean_device_ms": float(np.mean([s.device_ms for s in ok])) if ok else 0.0,
+            "multi_pass_jobs": sum(1 for s in ok if s.passes > 1)}
