@@ -11,7 +11,8 @@ public dataset).
 A step is one counting job over the whole FASTQ:
   value -- input resident in HBM (kc_input_upload once), device time of the
            job from CUDA events on its stream (sum over the timed steps);
-  e2e   -- the same job through the C ABI from pinned host buffers: upload,
+  e2e   -- the same job through the C ABI from pinned host buffers (after two
+           untimed warm-up jobs that bring the worker to steady state): upload,
            counting, and the sorted records + histogram copied back, timed by
            the host clock.
 --impl reference times the reference's own CPU programs (compiled from its
@@ -435,9 +436,12 @@ def run_ours(args):
     if args.e2e_steps > 0:
         walls, occ_e = [], 0
         r = None
-        # one untimed host-buffer job: the worker's device workspace and the
-        # pinned result pool grow to this job shape once
-        counter.count([fq], keep_records=True, copy=False, **JOB)
+        # untimed host-buffer jobs: the first one's device memory beyond the
+        # worker's workspace comes from the stream-ordered pool, the next job
+        # grows the workspace to fit it all (and the pinned result blocks are
+        # in the pool); from the third job on the worker is in steady state
+        for _ in range(2):
+            counter.count([fq], keep_records=True, copy=False, **JOB)
         for _ in range(args.e2e_steps):
             t0 = time.perf_counter()
             r = counter.count([fq], keep_records=True, copy=False, **JOB)

@@ -235,9 +235,14 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
     // ---- input -----------------------------------------------------------
     kc_input local;
     const kc_input *in = job.input;
+    static const bool trace_host = getenv("KC_TRACE") && getenv("KC_TRACE")[0] == '1';
+    const double th_start = now_ms();
     if (!in) {
         build_input(local, job.files.data(), (uint32_t)job.files.size(), st, &ds, tile_seg_host);
         in = &local;
+        if (trace_host)
+            fprintf(stderr, "[kc trace] job upload of %zu files enqueued after %.3f ms\n", job.files.size(),
+                    now_ms() - th_start);
     }
     cudaEvent_t ev0, ev1;
     CK(cudaEventCreate(&ev0));
@@ -836,6 +841,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
     CK(cudaEventRecord(ev1, st));
 
     // ---- records to host ------------------------------------------------------
+    if (trace_host) fprintf(stderr, "[kc trace] records to host from %.3f ms (host clock)\n", now_ms() - th_start);
     if (P.keep_records) {
         job.recs.allocate(n_rec);
         if (n_rec) {
@@ -844,6 +850,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
         }
     }
     CK(cudaStreamSynchronize(st));
+    if (trace_host) fprintf(stderr, "[kc trace] job done at %.3f ms (host clock)\n", now_ms() - th_start);
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, ev0, ev1));
     job.device_ms = ms;
