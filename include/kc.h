@@ -206,6 +206,14 @@ int kc_sort_records(uint64_t *keys, uint32_t *counts, uint64_t n, uint32_t bits)
 #define KC_SORT_NOALLOC_MAX (1u << 20)
 int kc_sort_records_noalloc(uint64_t *d_keys, uint32_t *d_counts, uint64_t n, uint32_t bits, void *stream);
 
+/* The sorted dump of the reference's dump_tool (tool/dump_tool.cpp:1172-1193,
+ * kmer_to_buf :103-124): one "KMER\tcount\n" line per record, the k-mer's
+ * printed string from its kmer<1> word, formatted on the device.  With out ==
+ * NULL only *n_bytes (the text's length) is computed; otherwise the text goes
+ * to out (cap bytes) and *n_bytes receives its length. */
+int kc_dump_text(const uint64_t *keys, const uint32_t *counts, uint64_t n, uint32_t k, char *out, uint64_t cap,
+                 uint64_t *n_bytes);
+
 /* Measurement aid, no counterpart in the reference: throughput of random
  * 32-bit atomicAdd (no return value) over a device buffer of buffer_bytes (a
  * power of two), averaged over `repeats` launches.  A buffer far larger than

@@ -109,6 +109,8 @@ SIGNATURES = [
     ("kc_kernel_launches", C.c_uint64, []),
     ("kc_sort_records_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]),
     ("kc_atomic_peak", C.c_int, [C.c_uint64, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    ("kc_dump_text", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p, C.c_uint64,
+                               C.POINTER(C.c_uint64)]),
     ("kc_plan_bloom", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p,
                                 C.POINTER(C.c_uint64)]),
     ("kc_merge_records", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_uint32,
@@ -463,5 +465,18 @@ def histogram_text(hist: np.ndarray, hist_min: int) -> str:
 
 
 def dump_text(keys: np.ndarray, counts: np.ndarray, k: int) -> str:
-    """dump_tool output: ``KMER\\tcount\\n`` lines (tool/dump_tool.cpp:1172-1193)."""
-    return "".join(f"{kmer_string(int(w), k)}\t{int(c)}\n" for w, c in zip(keys, counts))
+    """dump_tool output: ``KMER\\tcount\\n`` lines (tool/dump_tool.cpp:1172-1193),
+    formatted on the device (``kc_dump_text``)."""
+    return dump_bytes(keys, counts, k).decode("ascii")
+
+
+def dump_bytes(keys: np.ndarray, counts: np.ndarray, k: int) -> bytes:
+    keys = np.ascontiguousarray(keys, dtype=np.uint64)
+    counts = np.ascontiguousarray(counts, dtype=np.uint32)
+    n = len(keys)
+    need = C.c_uint64()
+    _check(lib().kc_dump_text(_ptr(keys), _ptr(counts), n, k, None, 0, C.byref(need)))
+    out = np.empty(max(need.value, 1), np.uint8)
+    got = C.c_uint64()
+    _check(lib().kc_dump_text(_ptr(keys), _ptr(counts), n, k, _ptr(out), out.nbytes, C.byref(got)))
+    return out[: got.value].tobytes()

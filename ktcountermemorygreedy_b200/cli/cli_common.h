@@ -140,27 +140,32 @@ inline bool read_tmpdir(const std::string &dir, TmpDir &t, std::string &err)
     return true;
 }
 
-// "KMER\tcount\n" lines (tool/dump_tool.cpp:1172-1193).
-inline bool write_dump(const std::string &path, const uint64_t *keys, const uint32_t *counts, uint64_t n, uint32_t k)
+// "KMER\tcount\n" lines (tool/dump_tool.cpp:1172-1193), formatted on the
+// device (kc_dump_text) into pinned host memory, then written out.
+inline bool write_dump(const std::string &path, const uint64_t *keys, const uint32_t *counts, uint64_t n, uint32_t k,
+                       std::string &err)
 {
-    FILE *f = std::fopen(path.c_str(), "wb");
-    if (!f) return false;
-    static const char B[4] = {'A', 'C', 'G', 'T'};
-    std::vector<char> buf;
-    buf.reserve(1 << 22);
-    char line[64];
-    for (uint64_t i = 0; i < n; ++i) {
-        uint64_t w = keys[i];
-        for (uint32_t j = 0; j < k; ++j) line[j] = B[(w >> (64 - 2 * k + 2 * j)) & 3];
-        int m = std::snprintf(line + k, sizeof(line) - k, "\t%u\n", counts[i]);
-        buf.insert(buf.end(), line, line + k + m);
-        if (buf.size() > (1 << 22)) {
-            if (std::fwrite(buf.data(), 1, buf.size(), f) != buf.size()) { std::fclose(f); return false; }
-            buf.clear();
-        }
+    uint64_t need = 0;
+    if (kc_dump_text(keys, counts, n, k, nullptr, 0, &need) != KC_OK) { err = kc_last_error(); return false; }
+    void *buf = nullptr;
+    if (need && kc_host_alloc(need, &buf) != KC_OK) { err = kc_last_error(); return false; }
+    uint64_t got = 0;
+    if (need && kc_dump_text(keys, counts, n, k, static_cast<char *>(buf), need, &got) != KC_OK) {
+        err = kc_last_error();
+        kc_host_free(buf);
+        return false;
     }
-    bool ok = buf.empty() || std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
-    return (std::fclose(f) == 0) && ok;
+    FILE *f = std::fopen(path.c_str(), "wb");
+    if (!f) {
+        err = "failed to open " + path;
+        if (buf) kc_host_free(buf);
+        return false;
+    }
+    bool ok = !got || std::fwrite(buf, 1, got, f) == got;
+    ok = (std::fclose(f) == 0) && ok;
+    if (buf) kc_host_free(buf);
+    if (!ok) err = "failed to write " + path;
+    return ok;
 }
 
 // "f\tcount\n" for every f in [min, max] (tool/histogram_tool.cpp:462-478).

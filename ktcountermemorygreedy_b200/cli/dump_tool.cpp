@@ -41,8 +41,8 @@ int main(int argc, char **argv)
                               precise ? t.low_keys.data() : nullptr, precise ? t.low_keys.size() : 0, t.k, t.count_max,
                               lo, hi, 1, 1, keys.data(), counts.data(), cap, &n, nullptr);
     if (rc != KC_OK) { std::cerr << "dump_tool: " << kc_last_error() << '\n'; return 2; }
-    if (!cli::write_dump(argv[5], keys.data(), counts.data(), std::min(n, cap), t.k)) {
-        std::cerr << "failed to open " << argv[5] << '\n';
+    if (!cli::write_dump(argv[5], keys.data(), counts.data(), std::min(n, cap), t.k, err)) {
+        std::cerr << "dump_tool: " << err << '\n';
         return 1;
     }
     std::cout << "progress 100%" << std::endl;

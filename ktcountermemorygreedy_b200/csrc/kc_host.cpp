@@ -528,6 +528,62 @@ int kc_sort_records(uint64_t *keys, uint32_t *counts, uint64_t n, uint32_t bits)
     }
 }
 
+int kc_dump_text(const uint64_t *keys, const uint32_t *counts, uint64_t n, uint32_t k, char *out, uint64_t cap,
+                 uint64_t *n_bytes)
+{
+    if (!n_bytes || (n && (!keys || !counts))) return set_error(KC_ERR_INVALID, "bad argument");
+    if (k < 1 || k > 32) return set_error(KC_ERR_INVALID, "k must be in 1..32");
+    if (!out) {
+        // size query: k bases, a tab, the decimal count and a newline per record
+        uint64_t need = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            uint32_t c = counts[i], d = 1;
+            while (c >= 10) { c /= 10; ++d; }
+            need += k + 2 + d;
+        }
+        *n_bytes = need;
+        return KC_OK;
+    }
+    *n_bytes = 0;
+    if (!n) return KC_OK;
+    try {
+        StreamGuard sg;
+        // records in chunks, so that device memory stays bounded
+        const uint64_t chunk = std::min<uint64_t>(n, 1ull << 25);
+        DevScope ds(sg.st);
+        unsigned long long *dk = ds.n<unsigned long long>(chunk);
+        uint32_t *dc = ds.n<uint32_t>(chunk);
+        uint32_t *len = ds.n<uint32_t>(chunk);
+        unsigned long long *off = ds.n<unsigned long long>(chunk);
+        unsigned long long *tmp = ds.n<unsigned long long>(scan_tmp_words(chunk));
+        char *dtxt = static_cast<char *>(ds.get(chunk * (size_t)(k + 12)));
+        uint64_t pos = 0;
+        for (uint64_t c0 = 0; c0 < n; c0 += chunk) {
+            const uint64_t m = std::min(chunk, n - c0);
+            CK(cudaMemcpyAsync(dk, keys + c0, m * 8, cudaMemcpyHostToDevice, sg.st));
+            CK(cudaMemcpyAsync(dc, counts + c0, m * 4, cudaMemcpyHostToDevice, sg.st));
+            CK(launch_dump_text(dk, dc, m, k, len, off, tmp, dtxt, sg.st));
+            unsigned long long last_off = 0;
+            uint32_t last_len = 0;
+            CK(cudaMemcpyAsync(&last_off, off + m - 1, 8, cudaMemcpyDeviceToHost, sg.st));
+            CK(cudaMemcpyAsync(&last_len, len + m - 1, 4, cudaMemcpyDeviceToHost, sg.st));
+            CK(cudaStreamSynchronize(sg.st));
+            const uint64_t bytes = last_off + last_len;
+            if (pos + bytes > cap) {
+                *n_bytes = pos;
+                return set_error(KC_ERR_INVALID, "output buffer too small for the dump text");
+            }
+            CK(cudaMemcpyAsync(out + pos, dtxt, bytes, cudaMemcpyDeviceToHost, sg.st));
+            CK(cudaStreamSynchronize(sg.st));
+            pos += bytes;
+        }
+        *n_bytes = pos;
+        return KC_OK;
+    } catch (const KcError &e) {
+        return set_error(e.code, e.msg);
+    }
+}
+
 int kc_atomic_peak(uint64_t buffer_bytes, uint32_t repeats, double *atomics_per_s, double *ms_per_launch)
 {
     if (!atomics_per_s || !ms_per_launch || !repeats) return set_error(KC_ERR_INVALID, "bad argument");

@@ -2139,6 +2139,75 @@ cudaError_t launch_hash_batch(const unsigned long long *keys, uint64_t n, unsign
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// text dump (the reference dump_tool's "KMER\tcount\n" lines)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t dec_digits(uint32_t v)
+{
+    uint32_t d = 1;
+    while (v >= 10) {
+        v /= 10;
+        ++d;
+    }
+    return d;
+}
+
+// Length of record i's line: k bases, a tab, the count in decimal, a newline.
+__global__ void k_dump_lengths(const uint32_t *counts, uint64_t n, uint32_t k, uint32_t *len)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        len[i] = k + 2 + dec_digits(counts[i]);
+}
+
+// Each block formats 256 consecutive lines into shared memory (base i of the
+// printed string is 2-bit group 64-2k+2i of the kmer<1> word) and copies them
+// out as one run of bytes starting at the first line's offset.
+constexpr uint32_t DUMP_MAX_LINE = 32 + 2 + 10;
+
+__global__ void __launch_bounds__(256) k_dump_write(const unsigned long long *keys, const uint32_t *counts,
+                                                    uint64_t n, uint32_t k, const unsigned long long *off,
+                                                    char *out)
+{
+    __shared__ char s_txt[256 * DUMP_MAX_LINE];
+    const uint64_t first = blockIdx.x * 256ull;
+    if (first >= n) return;
+    const uint64_t last = first + 256 < n ? first + 255 : n - 1;
+    const unsigned long long base = off[first];
+    const uint64_t i = first + threadIdx.x;
+    if (i < n) {
+        char *p = s_txt + (off[i] - base);
+        const unsigned long long w = keys[i];
+        const uint32_t sh0 = 64 - 2 * k;
+        for (uint32_t b = 0; b < k; ++b) p[b] = "ACGT"[(w >> (sh0 + 2 * b)) & 3];
+        p[k] = '\t';
+        uint32_t c = counts[i];
+        const uint32_t nd = dec_digits(c);
+        for (uint32_t d = nd; d > 0; --d) {
+            p[k + d] = (char)('0' + c % 10);
+            c /= 10;
+        }
+        p[k + 1 + nd] = '\n';
+    }
+    __syncthreads();
+    const uint64_t bytes = off[last] + k + 2 + dec_digits(counts[last]) - base;
+    for (uint64_t j = threadIdx.x; j < bytes; j += 256) out[base + j] = s_txt[j];
+}
+
+cudaError_t launch_dump_text(const unsigned long long *keys, const uint32_t *counts, uint64_t n, uint32_t k,
+                             uint32_t *len, unsigned long long *off, unsigned long long *scan_tmp, char *out,
+                             cudaStream_t st)
+{
+    if (!n) return cudaSuccess;
+    note_launch();
+    k_dump_lengths<<<grid_for(n, 256), 256, 0, st>>>(counts, n, k, len);
+    cudaError_t e = launch_scan_u32(len, off, n, scan_tmp, st);
+    if (e != cudaSuccess) return e;
+    note_launch();
+    k_dump_write<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(keys, counts, n, k, off, out);
+    return cudaGetLastError();
+}
+
 // Random 32-bit atomicAdd throughput: every thread adds 1 at `iters`
 // pseudo-random word indexes (xorshift64*, independent per thread) of a buffer
 // of mask+1 words.  With a buffer far larger than L2 each add is a DRAM

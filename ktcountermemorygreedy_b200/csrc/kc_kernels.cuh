@@ -242,6 +242,13 @@ cudaError_t launch_merge_buckets(const unsigned long long *keys, const BucketRan
 cudaError_t launch_hash_batch(const unsigned long long *keys, uint64_t n, unsigned long long *out,
                               cudaStream_t st);
 
+// "KMER\tcount\n" lines of n records (kmer<1> words, k <= 32) into out,
+// packed; len (n), off (n) and scan_tmp (scan_tmp_words(n)) are scratch, and
+// off[n-1] + len[n-1] is the text's length.
+cudaError_t launch_dump_text(const unsigned long long *keys, const uint32_t *counts, uint64_t n, uint32_t k,
+                             uint32_t *len, unsigned long long *off, unsigned long long *scan_tmp, char *out,
+                             cudaStream_t st);
+
 // Random 32-bit atomicAdd microbenchmark over `words` (a power of two) words;
 // *ops receives the number of adds the launch performs.
 cudaError_t launch_atomic_peak(uint32_t *buf, uint64_t words, uint32_t iters, uint64_t seed, uint64_t *ops,

@@ -181,6 +181,21 @@ def test_bloom_job_sampled_census(counter):
         assert np.array_equal(r.keys, want_k) and np.array_equal(r.counts, want_c)
 
 
+def test_dump_text_on_device_matches_oracle(kc):
+    """kc_dump_text formats records on the device exactly as the tool's text
+    (k from 1 to 32, counts from 0 to 2^32 - 1, more records than one block,
+    no records)."""
+    rng = np.random.default_rng(77)
+    for k, n in ((1, 3), (21, 1000), (31, 4099), (32, 257)):
+        keys = rng.integers(0, 2**63, size=n, dtype=np.uint64)
+        if k < 32:
+            keys &= np.uint64(((1 << (2 * k)) - 1) << (64 - 2 * k))
+        counts = rng.integers(0, 2**32, size=n, dtype=np.uint64).astype(np.uint32)
+        counts[: min(n, 5)] = [0, 1, 9, 10, 0xFFFFFFFF][: min(n, 5)]
+        assert kc.dump_bytes(keys, counts, k) == O.dump_text(keys, counts, k), k
+    assert kc.dump_bytes(np.zeros(0, np.uint64), np.zeros(0, np.uint32), 31) == b""
+
+
 def test_multi_pass_jobs_match_single_pass(counter):
     """A job whose pass budget is smaller than its k-mer arrays, filters and
     tables runs in several passes over ranges of root prefixes, each pass's
