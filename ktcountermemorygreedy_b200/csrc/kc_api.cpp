@@ -237,8 +237,10 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
     const kc_input *in = job.input;
     static const bool trace_host = getenv("KC_TRACE") && getenv("KC_TRACE")[0] == '1';
     const double th_start = now_ms();
+    std::vector<PinnedBlock> inflated;   // gzip files inflated on the host (kept until the job ends)
     if (!in) {
-        build_input(local, job.files.data(), (uint32_t)job.files.size(), st, &ds, tile_seg_host);
+        const std::vector<kc_buffer> files = inflate_inputs(job.files, inflated);
+        build_input(local, files.data(), (uint32_t)files.size(), st, &ds, tile_seg_host);
         in = &local;
         if (trace_host)
             fprintf(stderr, "[kc trace] job upload of %zu files enqueued after %.3f ms\n", job.files.size(),
@@ -877,7 +879,7 @@ uint64_t input_bytes(const kc_job &p)
 {
     if (p.input) return 0;
     uint64_t s = 0;
-    for (uint32_t i = 0; i < p.n_files; ++i) s += p.files[i].size;
+    for (uint32_t i = 0; i < p.n_files; ++i) s += gzip_size_hint(p.files[i]);
     return s;
 }
 
@@ -920,6 +922,8 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st, Workspa
     std::vector<uint32_t> tile_seg_host;
     static const bool trace = getenv("KC_TRACE") && getenv("KC_TRACE")[0] == '1';
     const double th0 = now_ms();
+    std::vector<PinnedBlock> inflated;   // gzip files inflated on the host (kept until the batch ends)
+    files = inflate_inputs(files, inflated);
     build_input(in, files.data(), (uint32_t)files.size(), st, &ds, tile_seg_host, fsample.data());
     if (trace) fprintf(stderr, "[kc trace] batch upload of %u files enqueued in %.3f ms\n", (uint32_t)files.size(),
                        now_ms() - th0);
@@ -1101,7 +1105,8 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st, Workspa
         Job &j = *jobs[i];
         j.n_records_total = len_h[i];
         j.input_bytes = 0;
-        for (const auto &f : j.files) j.input_bytes += f.size;
+        for (size_t f = 0; f < files.size(); ++f)   // sizes after gzip inflation
+            if (fsample[f] == i) j.input_bytes += files[f].size;
         if (!j.p.keep_records) continue;
         j.recs.allocate(len_h[i]);
         if (len_h[i]) {
@@ -1294,7 +1299,9 @@ int kc_input_upload(kc_handle *h, const kc_buffer *files, uint32_t n_files, kc_i
         cudaStream_t st;
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         try {
-            build_input(*in, files, n_files, st, nullptr, ts);
+            std::vector<PinnedBlock> inflated;
+            const std::vector<kc_buffer> fv = inflate_inputs(std::vector<kc_buffer>(files, files + n_files), inflated);
+            build_input(*in, fv.data(), (uint32_t)fv.size(), st, nullptr, ts);
             CK(cudaStreamSynchronize(st));
         } catch (...) {
             cudaStreamDestroy(st);

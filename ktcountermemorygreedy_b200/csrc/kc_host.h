@@ -110,6 +110,48 @@ private:
     PinnedPool();
 };
 
+// One pinned block from the pool, given back when it goes out of scope.
+struct PinnedBlock {
+    void *p = nullptr;
+    size_t bytes = 0;
+    PinnedBlock() = default;
+    PinnedBlock(const PinnedBlock &) = delete;
+    PinnedBlock &operator=(const PinnedBlock &) = delete;
+    PinnedBlock(PinnedBlock &&o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr, o.bytes = 0; }
+    PinnedBlock &operator=(PinnedBlock &&o) noexcept
+    {
+        if (this != &o) {
+            release();
+            p = o.p;
+            bytes = o.bytes;
+            o.p = nullptr;
+            o.bytes = 0;
+        }
+        return *this;
+    }
+    void reset(size_t n)   // throws KcError
+    {
+        release();
+        size_t got = 0;
+        p = PinnedPool::instance().get(n, got);
+        bytes = got;
+    }
+    void release()
+    {
+        if (p) PinnedPool::instance().put(p, bytes);
+        p = nullptr;
+        bytes = 0;
+    }
+    ~PinnedBlock() { release(); }
+};
+
+// gzip inputs (kc_gzip.cpp): detection, an upper estimate of the inflated
+// size, and inflation of a job's gzip files into pinned blocks held by `hold`
+// (the returned buffers replace the gzip files, the others are unchanged).
+bool is_gzip(const kc_buffer &b);
+uint64_t gzip_size_hint(const kc_buffer &b);
+std::vector<kc_buffer> inflate_inputs(const std::vector<kc_buffer> &files, std::vector<PinnedBlock> &hold);
+
 // (key, count) records of one job in a pinned block.
 struct HostRecords {
     void *block = nullptr;

@@ -181,6 +181,35 @@ def test_bloom_job_sampled_census(counter):
         assert np.array_equal(r.keys, want_k) and np.array_equal(r.counts, want_c)
 
 
+def test_gzip_inputs_count_like_plain_ones(counter):
+    """gzip FASTQ (one member, several concatenated members, mixed with an
+    uncompressed file) is inflated on the host and counts exactly like the
+    uncompressed input, in single, Bloom and batched jobs; corrupt or
+    truncated gzip data is reported as an error."""
+    import gzip
+    a = fixtures.random_fastq(501, 400, (100, 150), genome_len=5000)
+    b = fixtures.random_fastq(502, 300, (90, 150), genome_len=4000)
+    half = len(a) // 2
+    cut = a.index(b"\n@", half) + 1   # a record boundary
+    multi = gzip.compress(a[:cut]) + gzip.compress(a[cut:])
+    for kw in (dict(), dict(bloom=True, memory_gb=1, min_count=1)):
+        want = counter.count([a, b], k=25, count_max=U32, **kw)
+        for files in ([gzip.compress(a), b], [multi, gzip.compress(b)]):
+            got = counter.count(files, k=25, count_max=U32, **kw)
+            assert np.array_equal(got.keys, want.keys) and np.array_equal(got.counts, want.counts)
+            assert got.input_bytes == len(a) + len(b)
+    res = counter.count_batch([[gzip.compress(a)], [b], [multi]], [21, 31, 21], count_max=U32)
+    for files, k, r in zip([[a], [b], [a]], [21, 31, 21], res):
+        one = counter.count(files, k=k, count_max=U32)
+        assert np.array_equal(r.keys, one.keys) and np.array_equal(r.counts, one.counts)
+    bad = bytearray(gzip.compress(a))
+    bad[len(bad) // 2] ^= 0xFF
+    import ktcountermemorygreedy_b200 as kcm
+    for data in (bytes(bad), gzip.compress(a)[:-40]):
+        with pytest.raises(kcm.KcError):
+            counter.count([data], k=25)
+
+
 def test_dump_text_on_device_matches_oracle(kc):
     """kc_dump_text formats records on the device exactly as the tool's text
     (k from 1 to 32, counts from 0 to 2^32 - 1, more records than one block,
