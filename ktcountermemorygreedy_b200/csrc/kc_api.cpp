@@ -63,14 +63,24 @@ double hll_estimate(const uint32_t *regs, uint32_t m)
     return e;
 }
 
+// Slots per estimated key of the per-bucket tables of the partitioned path.
+// They are filled while they sit in L2, so memory is cheap and a low load
+// factor (short probe runs, fewer L2 operations per insert) pays.
+#ifndef KC_BUCKET_TABLE_FACTOR
+#define KC_BUCKET_TABLE_FACTOR 3.0
+#endif
+constexpr double BUCKET_TABLE_FACTOR = KC_BUCKET_TABLE_FACTOR;
+
 // A plain job whose table would hold more slots than this (64 MiB of slots,
 // half of L2) is counted through the root-prefix buckets.
 constexpr uint64_t PLAIN_PART_MIN_SLOTS = 1ull << 22;
 
-uint64_t table_capacity_for(double est)
+// Slots for an estimated `est` distinct keys: 1.6x (load factor <= 0.63 for
+// a fair estimate), rounded up to 256 slots; tables need not be powers of two.
+uint64_t table_capacity_for(double est, double factor = 1.6)
 {
-    uint64_t want = (uint64_t)std::ceil(std::max(est, 16.0) * 1.8);
-    return std::max<uint64_t>(1024, bit_ceil64(want));
+    const uint64_t want = (uint64_t)std::ceil(std::max(est, 16.0) * factor);
+    return std::max<uint64_t>(1024, (want + 255) & ~uint64_t(255));
 }
 
 int fail(int code, const std::string &msg) { return set_error(code, msg); }
@@ -636,7 +646,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census)
                     e = std::min(e, (double)hb);
                 }
                 e = std::max(e, (double)std::min<unsigned long long>(hb, 4096));
-                bcaps[b] = table_capacity_for(e);
+                bcaps[b] = table_capacity_for(e, BUCKET_TABLE_FACTOR);
             }
             low_len += pass_low;
             // per-bucket sub-tables in one arena; a bucket whose table

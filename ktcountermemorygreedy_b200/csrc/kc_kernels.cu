@@ -210,10 +210,22 @@ __device__ __forceinline__ void hll_add_shared(uint32_t *regs, unsigned long lon
     if (rank > regs[r]) atomicMax(&regs[r], rank);
 }
 
+// Tables have any capacity (mask = capacity - 1): a key's home slot is the
+// high half of hash * capacity, probing is linear and wraps at the end.
+__device__ __forceinline__ unsigned long long home_slot(unsigned long long key, unsigned long long mask)
+{
+    return __umul64hi(slot_hash(key), mask + 1);
+}
+
+__device__ __forceinline__ unsigned long long next_slot(unsigned long long i, unsigned long long mask)
+{
+    return i == mask ? 0 : i + 1;
+}
+
 __device__ __forceinline__ bool table_add(Slot *slots, unsigned long long mask, unsigned long long key,
                                           unsigned int c, uint32_t max_probe)
 {
-    unsigned long long i = slot_hash(key) & mask;
+    unsigned long long i = home_slot(key, mask);
     for (uint32_t n = 0; n < max_probe; ++n) {
         unsigned long long cur = __ldcg(&slots[i].key);
         if (cur == key) {
@@ -227,7 +239,7 @@ __device__ __forceinline__ bool table_add(Slot *slots, unsigned long long mask, 
                 return true;
             }
         }
-        i = (i + 1) & mask;
+        i = next_slot(i, mask);
     }
     return false;
 }
@@ -235,12 +247,12 @@ __device__ __forceinline__ bool table_add(Slot *slots, unsigned long long mask, 
 __device__ __forceinline__ Slot *table_find(Slot *slots, unsigned long long mask, unsigned long long key,
                                             uint32_t max_probe, bool &overflow)
 {
-    unsigned long long i = slot_hash(key) & mask;
+    unsigned long long i = home_slot(key, mask);
     for (uint32_t n = 0; n < max_probe; ++n) {
         unsigned long long cur = __ldcg(&slots[i].key);
         if (cur == key) return &slots[i];
         if (cur == EMPTY_KEY) return nullptr;
-        i = (i + 1) & mask;
+        i = next_slot(i, mask);
     }
     overflow = true;
     return nullptr;

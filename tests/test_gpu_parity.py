@@ -233,7 +233,7 @@ def test_multi_pass_jobs_match_single_pass(counter):
     same job in one pass."""
     import ktcountermemorygreedy_b200.synth as S
     g = S.genome(41, 2_000_000)
-    fq = S.reads(g, 41, 30_000, (150, 150), 0.01, 0.0).tobytes()
+    fq = S.reads(g, 41, 45_000, (150, 150), 0.01, 0.0).tobytes()   # ~3.5M distinct: partitioned
     kw = dict(count_max=U32, top_n=300, want_le2=True, hist_max=100)
     for bloom, mc in ((True, 2), (False, 1)):
         want_k, want_c = O.exact_records([fq], 31, U32, min_count=mc)
