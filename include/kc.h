@@ -139,6 +139,18 @@ typedef struct {
     uint32_t reserved0;
 } kc_result_t;
 
+/* Settings of a handle that trade memory for speed, chosen by kc_autotune or
+ * set by the caller; a job uses the settings in force when it starts. */
+typedef struct {
+    double bucket_table_factor;   /* table slots per estimated key, per-bucket tables of the partitioned
+                                     path (filled while in L2); default 3.0 */
+    double table_factor;          /* table slots per estimated key, one-table jobs and batched samples;
+                                     default 1.6 */
+    uint64_t sort_group_records;  /* records sorted together (kept in L2) by a batch's segmented sort;
+                                     default 4M */
+    uint64_t reserved[5];
+} kc_tuning;
+
 /* Kernel launches issued by this process so far (all handles). */
 uint64_t kc_kernel_launches(void);
 
@@ -147,6 +159,15 @@ int kc_open(const kc_config *cfg, kc_handle **out);
 void kc_close(kc_handle *h);
 const char *kc_last_error(void);
 void kc_job_defaults(kc_job *job);   /* reference defaults: count_max 255, filter 2..u32max, ... */
+
+int kc_get_tuning(kc_handle *h, kc_tuning *out);
+int kc_set_tuning(kc_handle *h, const kc_tuning *t);   /* values <= 0 keep the current one */
+/* Autotuner (no counterpart in the reference, whose map capacity is a fixed
+ * command-line value, src/main.cpp:539-542): runs the given jobs (as one
+ * batch when `batch` is 1) once per candidate setting, one setting at a time
+ * with the others fixed, and keeps the setting with the least device time.
+ * The handle then uses the best settings, which are also returned. */
+int kc_autotune(kc_handle *h, const kc_job *jobs, uint32_t n_jobs, uint32_t batch, kc_tuning *best);
 
 /* ---- device-resident input --------------------------------------------- */
 int kc_input_upload(kc_handle *h, const kc_buffer *files, uint32_t n_files, kc_input **out);

@@ -54,6 +54,11 @@ class kc_config(C.Structure):
                 ("reserved", C.c_uint64 * 4)]
 
 
+class kc_tuning(C.Structure):
+    _fields_ = [("bucket_table_factor", C.c_double), ("table_factor", C.c_double),
+                ("sort_group_records", C.c_uint64), ("reserved", C.c_uint64 * 5)]
+
+
 class kc_buffer(C.Structure):
     _fields_ = [("data", C.c_void_p), ("size", C.c_uint64)]
 
@@ -109,6 +114,9 @@ SIGNATURES = [
     ("kc_kernel_launches", C.c_uint64, []),
     ("kc_sort_records_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]),
     ("kc_atomic_peak", C.c_int, [C.c_uint64, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    ("kc_get_tuning", C.c_int, [C.c_void_p, C.POINTER(kc_tuning)]),
+    ("kc_set_tuning", C.c_int, [C.c_void_p, C.POINTER(kc_tuning)]),
+    ("kc_autotune", C.c_int, [C.c_void_p, C.POINTER(kc_job), C.c_uint32, C.c_uint32, C.POINTER(kc_tuning)]),
     ("kc_dump_text", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p, C.c_uint64,
                                C.POINTER(C.c_uint64)]),
     ("kc_plan_bloom", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p,
@@ -369,6 +377,41 @@ class KmerCounter:
         res = self.result(jid, kw.get("k", 31), copy=copy)
         res.hist_min = kw.get("hist_min", 1)
         return res
+
+    @property
+    def tuning(self) -> dict:
+        """The handle's speed/memory settings (``kc_get_tuning``)."""
+        t = kc_tuning()
+        _check(lib().kc_get_tuning(self._h, C.byref(t)))
+        return {"bucket_table_factor": t.bucket_table_factor, "table_factor": t.table_factor,
+                "sort_group_records": t.sort_group_records}
+
+    def set_tuning(self, bucket_table_factor: float = 0.0, table_factor: float = 0.0, sort_group_records: int = 0):
+        t = kc_tuning()
+        t.bucket_table_factor, t.table_factor, t.sort_group_records = bucket_table_factor, table_factor, \
+            sort_group_records
+        _check(lib().kc_set_tuning(self._h, C.byref(t)))
+
+    def autotune(self, samples: Sequence[Sequence[bytes]] = (), ks: Sequence[int] = (), batch: bool = False,
+                 inputs: Sequence = (), **kw) -> dict:
+        """Runs the given jobs (FASTQ files per job, or resident inputs) once
+        per candidate setting and keeps the fastest settings (``kc_autotune``)."""
+        n = len(inputs) if inputs else len(samples)
+        jobs = (kc_job * n)()
+        keep = []
+        for i in range(n):
+            j = self.make_job(k=ks[i] if ks else kw.get("k", 31), **{x: y for x, y in kw.items() if x != "k"})
+            if inputs:
+                j.input = inputs[i]
+            else:
+                arr, kk = _buffers(samples[i])
+                j.files = C.cast(arr, C.POINTER(kc_buffer))
+                j.n_files = len(samples[i])
+                keep.append((arr, kk))
+            jobs[i] = j
+        best = kc_tuning()
+        _check(lib().kc_autotune(self._h, jobs, n, int(batch), C.byref(best)))
+        return self.tuning
 
     def count_batch(self, samples: Sequence[Sequence[bytes]], ks: Sequence[int], copy: bool = True,
                     **kw) -> List[Result]:

@@ -1830,15 +1830,14 @@ size_t sort_tmp_bytes_in_scratch(uint64_t n) { return scratch_sort_bytes(n); }
 
 // Segments [seg_start[i], seg_start[i] + seg_len[i]) of the arrays are sorted
 // independently; they must be disjoint and in increasing address order.
-// Consecutive segments are sorted in groups of about SORT_GROUP_RECORDS
-// records, every pass of a group before the next group, so that a group's
-// keys and values stay in L2 across its passes.
-constexpr uint64_t SORT_GROUP_RECORDS = 4ull << 20;   // 48 MiB of keys + values
+// Consecutive segments are sorted in groups of about group_records records
+// (4M: 48 MiB of keys + values), every pass of a group before the next group,
+// so that a group's keys and values stay in L2 across its passes.
 
 cudaError_t launch_radix_sort_segmented(unsigned long long *keys, uint32_t *vals, uint64_t n_total,
                                         const uint64_t *seg_start, const uint64_t *seg_len, uint32_t n_segs,
                                         uint32_t bits, void *tmp, cudaStream_t st, unsigned long long *flags,
-                                        const uint32_t *seg_bits)
+                                        const uint32_t *seg_bits, uint64_t group_records_max)
 {
     const uint64_t n_tiles = sort_tiles_for(seg_len, n_segs);
     if (n_tiles == 0 || bits == 0) return cudaSuccess;
@@ -1857,7 +1856,7 @@ cudaError_t launch_radix_sort_segmented(unsigned long long *keys, uint32_t *vals
         if (!nt) continue;
         const uint32_t b = seg_bits ? std::min(seg_bits[sgi], bits) : bits;
         const uint32_t sp = (b + 7) / 8;
-        if (groups.empty() || group_records + seg_len[sgi] > SORT_GROUP_RECORDS) {
+        if (groups.empty() || group_records + seg_len[sgi] > group_records_max) {
             groups.push_back(Group{tiles.size(), tiles.size(), 0});
             group_records = 0;
         }

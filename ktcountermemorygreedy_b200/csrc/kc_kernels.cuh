@@ -191,7 +191,8 @@ size_t sort_tmp_bytes_segmented(uint64_t n_total, const uint64_t *seg_len, uint3
 cudaError_t launch_radix_sort_segmented(unsigned long long *keys, uint32_t *vals, uint64_t n_total,
                                         const uint64_t *seg_start, const uint64_t *seg_len, uint32_t n_segs,
                                         uint32_t bits, void *tmp, cudaStream_t st, unsigned long long *flags = nullptr,
-                                        const uint32_t *seg_bits = nullptr);   // per segment, <= bits
+                                        const uint32_t *seg_bits = nullptr,    // per segment, <= bits
+                                        uint64_t group_records = 4ull << 20);  // records per L2-sized group
 // One segment, one kernel per 8-bit pass; a look-back wait that gave up sets
 // ERR_WAIT_TIMEOUT in *flags (NULL: a word inside tmp).
 cudaError_t launch_radix_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,

@@ -210,6 +210,35 @@ def test_gzip_inputs_count_like_plain_ones(counter):
             counter.count([data], k=25)
 
 
+def test_tuning_changes_speed_not_results(kc):
+    """The handle's settings (table load factors, sort group size) and the
+    autotuner that picks them change no record: plain, partitioned and
+    batched jobs give the same results under every setting."""
+    import ktcountermemorygreedy_b200.synth as S
+    g = S.genome(61, 2_000_000)
+    big = S.reads(g, 61, 45_000, (150, 150), 0.01, 0.0).tobytes()
+    small = fixtures.random_fastq(62, 300, (100, 150), genome_len=3000)
+    with kc.KmerCounter(max_inflight_jobs=2) as c:
+        ref = [c.count([f], k=31, count_max=U32) for f in (big, small)]
+        refb = c.count_batch([[small], [big]], [21, 31], count_max=U32)
+        for t in (dict(bucket_table_factor=1.2, table_factor=1.1, sort_group_records=1000),
+                  dict(bucket_table_factor=5.0, table_factor=2.5, sort_group_records=1 << 24)):
+            c.set_tuning(**t)
+            assert c.tuning["table_factor"] == t["table_factor"]
+            for f, want in zip((big, small), ref):
+                got = c.count([f], k=31, count_max=U32)
+                assert np.array_equal(got.keys, want.keys) and np.array_equal(got.counts, want.counts)
+            for want, got in zip(refb, c.count_batch([[small], [big]], [21, 31], count_max=U32)):
+                assert np.array_equal(got.keys, want.keys) and np.array_equal(got.counts, want.counts)
+        best = c.autotune([[big]], [31], count_max=U32)
+        assert best["bucket_table_factor"] in (2.0, 3.0, 4.0) and best["table_factor"] in (1.3, 1.6, 2.2)
+        got = c.count([big], k=31, count_max=U32)
+        assert np.array_equal(got.keys, ref[0].keys) and np.array_equal(got.counts, ref[0].counts)
+        import ktcountermemorygreedy_b200 as kcm
+        with pytest.raises(kcm.KcError):
+            c.set_tuning(table_factor=1.0)
+
+
 def test_dump_text_on_device_matches_oracle(kc):
     """kc_dump_text formats records on the device exactly as the tool's text
     (k from 1 to 32, counts from 0 to 2^32 - 1, more records than one block,
