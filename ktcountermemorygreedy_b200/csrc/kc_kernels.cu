@@ -168,6 +168,28 @@ __device__ __forceinline__ KParams kparams(uint32_t k)
     return p;
 }
 
+// Forward and reverse-complement words of the window ending just before
+// position q0 (0..31) of the current segment (for q0 = 0, the window ending at
+// the previous segment's last position), the start of a roll along the
+// segment: for each next base c, fwd = fwd >> 2 | c << 62 and
+// rc = rc << 2 | (3 - c) << (64 - 2k), and the window's canonical word is
+// min(fwd & topmask, rc).  fwd has stale bits below bit 64 - 2k (dropped by
+// the mask); rc is exact.  The 128-bit value (cur:prev) shifted right by 2q0
+// puts the window's first base at bit 64 - 2k; the reverse complement is
+// (rprev:rcur) shifted right by 2k - 2q0 (left when negative), as below.
+__device__ __forceinline__ void window_words(uint64_t prev, uint64_t cur, uint64_t rprev, uint64_t rcur, uint32_t q0,
+                                             const KParams &kp, uint64_t &fwd, uint64_t &rc)
+{
+    fwd = q0 ? (prev >> (2 * q0)) | (cur << (64 - 2 * q0)) : prev;
+    const int t = 2 * (int)kp.k - 2 * (int)q0;
+    uint64_t r;
+    if (t == 0) r = rcur;
+    else if (t > 0 && t < 64) r = (rcur >> t) | (rprev << (64 - t));
+    else if (t >= 64) r = rprev;   // k = 32, q0 = 0
+    else r = rcur << (-t);
+    rc = r & kp.topmask;
+}
+
 // Canonical internal word of the window ending at position j (0..31) of the
 // current segment.  prev/cur hold the 2-bit codes of the previous and current
 // segments, base q at bits 2q.  The forward word puts base i of the window at
@@ -235,10 +257,10 @@ __device__ __forceinline__ unsigned long long next_slot(unsigned long long i, un
     return i == mask ? 0 : i + 1;
 }
 
-__device__ __forceinline__ bool table_add(Slot *slots, unsigned long long mask, unsigned long long key,
-                                          unsigned int c, uint32_t max_probe)
+// Adds c to key's count, probing at most max_probe slots from slot i.
+__device__ __forceinline__ bool table_add_at(Slot *slots, unsigned long long mask, unsigned long long key,
+                                             unsigned int c, uint32_t max_probe, unsigned long long i)
 {
-    unsigned long long i = home_slot(key, mask);
     for (uint32_t n = 0; n < max_probe; ++n) {
         unsigned long long cur = __ldcg(&slots[i].key);
         if (cur == key) {
@@ -257,10 +279,15 @@ __device__ __forceinline__ bool table_add(Slot *slots, unsigned long long mask, 
     return false;
 }
 
-__device__ __forceinline__ Slot *table_find(Slot *slots, unsigned long long mask, unsigned long long key,
-                                            uint32_t max_probe, bool &overflow)
+__device__ __forceinline__ bool table_add(Slot *slots, unsigned long long mask, unsigned long long key,
+                                          unsigned int c, uint32_t max_probe)
 {
-    unsigned long long i = home_slot(key, mask);
+    return table_add_at(slots, mask, key, c, max_probe, home_slot(key, mask));
+}
+
+__device__ __forceinline__ Slot *table_find_at(Slot *slots, unsigned long long mask, unsigned long long key,
+                                               uint32_t max_probe, bool &overflow, unsigned long long i)
+{
     for (uint32_t n = 0; n < max_probe; ++n) {
         unsigned long long cur = __ldcg(&slots[i].key);
         if (cur == key) return &slots[i];
@@ -269,6 +296,47 @@ __device__ __forceinline__ Slot *table_find(Slot *slots, unsigned long long mask
     }
     overflow = true;
     return nullptr;
+}
+
+__device__ __forceinline__ Slot *table_find(Slot *slots, unsigned long long mask, unsigned long long key,
+                                            uint32_t max_probe, bool &overflow)
+{
+    return table_find_at(slots, mask, key, max_probe, overflow, home_slot(key, mask));
+}
+
+// Grouped probes: the home slots of a thread's G keys are read with their
+// loads in flight together, then each key is resolved in turn.  A slot only
+// ever changes from empty to a key, so an early read is never wrong: a key
+// found there is final, an empty slot is claimed by CAS (which reports a key
+// that arrived meanwhile), and another key sends the probe on to the next slot.
+template <uint32_t G>
+__device__ __forceinline__ bool table_add_group(Slot *slots, unsigned long long mask, const unsigned long long *key,
+                                                uint32_t act, uint32_t max_probe)
+{
+    unsigned long long i[G], cur[G];
+#pragma unroll
+    for (uint32_t u = 0; u < G; ++u) {
+        i[u] = home_slot(key[u], mask);
+        cur[u] = ((act >> u) & 1u) ? __ldcg(&slots[i[u]].key) : EMPTY_KEY;
+    }
+    bool ok = true;
+#pragma unroll
+    for (uint32_t u = 0; u < G; ++u) {
+        if (!((act >> u) & 1u)) continue;
+        if (cur[u] == key[u]) {
+            atomicAdd(&slots[i[u]].count, 1u);
+            continue;
+        }
+        if (cur[u] == EMPTY_KEY) {
+            const unsigned long long prev = atomicCAS(&slots[i[u]].key, EMPTY_KEY, key[u]);
+            if (prev == EMPTY_KEY || prev == key[u]) {
+                atomicAdd(&slots[i[u]].count, 1u);
+                continue;
+            }
+        }
+        if (max_probe < 2 || !table_add_at(slots, mask, key[u], 1u, max_probe - 1, next_slot(i[u], mask))) ok = false;
+    }
+    return ok;
 }
 
 // Warp-aggregated insert: lanes holding the same k-mer elect one leader that
@@ -502,26 +570,66 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
                 if (lane == 0 && n) atomicAdd(&a.occ[sg.sample], (unsigned long long)n);
             }
         } else {
-            uint32_t tot;
-            const uint32_t off = block_excl_scan(__popc(ends), s_warp, tot);
-            for (uint32_t base = 0; base < tot; base += stage_cap) {
-                // list the windows of this round as (segment, end position),
-                // then form the k-mers with every thread busy: segments of
-                // header and quality lines have no windows, so forming keys
-                // per owning thread would leave most lanes idle
-                uint32_t e = ends, idx = off;
-                while (e) {
-                    uint32_t j = __ffs(e) - 1;
-                    e &= e - 1;
-                    if (idx >= base && idx < base + stage_cap) s_rank[idx - base] = (uint16_t)((tid << 5) | j);
-                    ++idx;
+            // the windows are emitted per chunk of 8 positions (a quarter of a
+            // segment) holding at least one window end: the chunks of all
+            // segments are listed (in the tile buffer, which is free once
+            // classified), then each thread rolls the forward and reverse-
+            // complement words along its chunks.  Segments of header and
+            // quality lines have no chunks, so working per owning segment
+            // would leave most lanes idle.  One scan gives each segment its
+            // first window index (low half) and first chunk (high half).
+            uint32_t nq = 0;
+#pragma unroll
+            for (uint32_t q = 0; q < 4; ++q) nq += ((ends >> (8 * q)) & 0xFFu) ? 1u : 0u;
+            uint32_t packed_tot;
+            const uint32_t packed = block_excl_scan((uint32_t)__popc(ends) | (nq << 16), s_warp, packed_tot);
+            const uint32_t tot = packed_tot & 0xFFFFu, n_chunks = packed_tot >> 16;
+            uint32_t *s_chunk = reinterpret_cast<uint32_t *>(sbuf[s]);   // <= 4 * EXT_THREADS entries
+            {
+                // chunk = first window index << 18 | segment << 10 | quarter << 8 | its 8 end bits
+                uint32_t idx = packed & 0xFFFFu, c = packed >> 16;
+#pragma unroll
+                for (uint32_t q = 0; q < 4; ++q) {
+                    const uint32_t e8 = (ends >> (8 * q)) & 0xFFu;
+                    if (e8) s_chunk[c++] = (idx << 18) | ((uint32_t)tid << 10) | (q << 8) | e8;
+                    idx += (uint32_t)__popc(e8);
                 }
-                __syncthreads();
+            }
+            if (MODE == MODE_PART) s_bhist[tid] = 0;
+            __syncthreads();
+            const uint32_t blo = a.bucket_lo, bhi = a.bucket_hi ? a.bucket_hi : N_BUCKETS;
+            for (uint32_t base = 0; base < tot; base += stage_cap) {
                 const uint32_t nr = min(stage_cap, tot - base);
-                for (uint32_t i = tid; i < nr; i += EXT_THREADS) {
-                    const uint32_t item = s_rank[i], sgm = item >> 5;
-                    s_stage[i] = window_key_rc(s_codes[sgm], s_codes[sgm + 1], s_rcodes[sgm], s_rcodes[sgm + 1],
-                                               item & 31u, kp);
+                for (uint32_t ci = tid; ci < n_chunks; ci += EXT_THREADS) {
+                    const uint32_t ch = s_chunk[ci], e8 = ch & 0xFFu;
+                    uint32_t idx = ch >> 18;
+                    if (idx >= base + nr || idx + (uint32_t)__popc(e8) <= base) continue;   // not in this round
+                    const uint32_t sgm = (ch >> 10) & 0xFFu, q0 = ((ch >> 8) & 3u) * 8;
+                    const uint64_t cur = s_codes[sgm + 1];
+                    uint64_t fwd, rc;
+                    window_words(s_codes[sgm], cur, s_rcodes[sgm], s_rcodes[sgm + 1], q0, kp, fwd, rc);
+                    const uint32_t cw = (uint32_t)(cur >> (2 * q0));
+#pragma unroll
+                    for (uint32_t p = 0; p < 8; ++p) {
+                        const uint32_t c = (cw >> (2 * p)) & 3u;
+                        fwd = (fwd >> 2) | ((uint64_t)c << 62);
+                        rc = (rc << 2) | ((uint64_t)(c ^ 3u) << kp.fwd_shift);
+                        if ((e8 >> p) & 1u) {
+                            if (idx >= base && idx < base + nr) {
+                                const uint64_t f = fwd & kp.topmask;
+                                const unsigned long long key = f < rc ? f : rc;
+                                s_stage[idx - base] = key;
+                                if (MODE == MODE_PART) {
+                                    // rank inside the tile's share of its bucket (a
+                                    // pass of a multi-pass job keeps only its range)
+                                    const uint32_t bk = (uint32_t)(key >> 56);
+                                    s_rank[idx - base] =
+                                        (bk >= blo && bk < bhi) ? (uint16_t)atomicAdd(&s_bhist[bk], 1u) : (uint16_t)0xFFFFu;
+                                }
+                            }
+                            ++idx;
+                        }
+                    }
                 }
                 __syncthreads();
                 if (MODE == MODE_INSERT) {
@@ -532,28 +640,15 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
                         warp_insert(act, act ? s_stage[i] : EMPTY_KEY, tr, a.max_probe, flags);
                     }
                 } else if (MODE == MODE_PART) {
-                    // scatter into the root-prefix buckets: rank inside the
-                    // tile's share of each bucket, one cursor update per bucket
-                    // (a pass of a multi-pass job keeps only its range of buckets)
-                    const uint32_t blo = a.bucket_lo, bhi = a.bucket_hi ? a.bucket_hi : N_BUCKETS;
-                    s_bhist[tid] = 0;
-                    __syncthreads();
-                    if (blo == 0 && bhi == N_BUCKETS) {
-                        for (uint32_t i = tid; i < nr; i += EXT_THREADS)
-                            s_rank[i] = (uint16_t)atomicAdd(&s_bhist[(uint32_t)(s_stage[i] >> 56)], 1u);
-                    } else {
-                        for (uint32_t i = tid; i < nr; i += EXT_THREADS) {
-                            const uint32_t b = (uint32_t)(s_stage[i] >> 56);
-                            s_rank[i] = (b >= blo && b < bhi) ? (uint16_t)atomicAdd(&s_bhist[b], 1u) : (uint16_t)0xFFFFu;
-                        }
-                    }
-                    __syncthreads();
+                    // scatter into the root-prefix buckets (ranks were taken
+                    // as the k-mers were formed), one cursor update per bucket;
                     // the round's k-mers are reordered by bucket in shared
                     // memory, so that consecutive threads store consecutive
                     // addresses of one bucket's region (a warp's store then
                     // touches a few sectors instead of one per k-mer)
                     uint32_t tot_b;
                     const uint32_t c = s_bhist[tid];
+                    s_bhist[tid] = 0;   // the next round's ranks (emission is done)
                     const uint32_t bstart = block_excl_scan(c, s_warp, tot_b);
                     s_hist[tid] = bstart;
                     // destination of sorted index i of bucket b: s_bpos[b] + i
@@ -645,6 +740,9 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
                 }
                 __syncthreads();
             }
+            // the chunk list went into the tile buffer through the generic
+            // proxy; the next bulk copy into that buffer is an async-proxy write
+            fence_proxy_async_smem();
         }
         __syncthreads();
     }
@@ -1361,6 +1459,8 @@ __global__ void k_scatter_selected(const unsigned long long *keys, const uint32_
 // ---------------------------------------------------------------------------
 
 constexpr uint32_t ITEM_PER_THREAD = WORK_ITEM_KEYS / 256;
+// keys per thread whose first table probes are in flight together
+constexpr uint32_t INSERT_GROUP = 2;
 
 // Claims the next work item for the whole block; false when none is left.
 // Work item `it` of a launch: its bucket is the last one whose first item is
@@ -1545,11 +1645,17 @@ __global__ void __launch_bounds__(256) k_insert_buckets(const unsigned long long
         }
         // a bucket list is in extraction order, so a warp almost never holds
         // two copies of one k-mer: every thread inserts its own k-mers (no
-        // warp aggregation)
+        // warp aggregation), INSERT_GROUP at a time
+        bool ok = true;
 #pragma unroll
-        for (uint32_t r = 0; r < ITEM_PER_THREAD; ++r)
-            if ((uint64_t)r * 256 + tid < n && !table_add(tr.slots, tr.mask, k[r], 1u, max_probe))
-                atomicOr(&bucket_ovf[w.bucket], ERR_TABLE_FULL);
+        for (uint32_t g = 0; g < ITEM_PER_THREAD; g += INSERT_GROUP) {
+            uint32_t act = 0;
+#pragma unroll
+            for (uint32_t u = 0; u < INSERT_GROUP; ++u)
+                if ((uint64_t)(g + u) * 256 + tid < n) act |= 1u << u;
+            if (act && !table_add_group<INSERT_GROUP>(tr.slots, tr.mask, k + g, act, max_probe)) ok = false;
+        }
+        if (!ok) atomicOr(&bucket_ovf[w.bucket], ERR_TABLE_FULL);
     }
 }
 
