@@ -405,34 +405,76 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     unsigned long long *rec_keys = nullptr;
     uint32_t *rec_counts = nullptr;
     uint64_t n_rec = 0;
+    // Slot-order records of a bucket arena are grouped by bucket, and the
+    // bucket (root prefix) is the lowest 8 bits of the printed-order sort key:
+    // the sort then skips that pass.
+    bool rec_by_bucket = true;
     auto compact_table = [&](const TableRef &t, uint64_t cap, uint64_t n_low, const unsigned long long *lst,
                              const BucketRanges *low_rg, uint32_t n_low_items, unsigned int *merge_next,
-                             const BucketCfg *d_cfg) {
-        CK(cudaMemsetAsync(n_keys, 0, 8, st));
+                             const BucketCfg *d_cfg, bool bucket_arena) {
         CK(cudaMemsetAsync(counters + C_REC_LEN, 0, 3 * 8, st));   // C_REC_LEN, C_LOW_ONLY, C_DISTINCT
-        clk.begin(5);
-        CK(launch_count_keys(t.slots, cap, n_keys, st));
-        clk.end();
-        unsigned long long in_table = 0;
-        CK(cudaMemcpyAsync(&in_table, n_keys, 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        const uint64_t rec_cap = std::max<uint64_t>(in_table + n_low, 1);
-        rec_keys = ds.n<unsigned long long>(rec_cap);
-        rec_counts = ds.n<uint32_t>(rec_cap);
-        if (n_low) {
+        const bool want1 = P.min_count <= 1 && 1 <= P.max_count;
+        bool ordered = true;
+        if (n_low && want1) {
+            // the FIRST-only k-mers are records too (count 1): the merge
+            // appends them as it finds them, then the table's records follow
+            ordered = false;
+            rec_by_bucket = false;
+            CK(cudaMemsetAsync(n_keys, 0, 8, st));
+            clk.begin(5);
+            CK(launch_count_keys(t.slots, cap, n_keys, st));
+            clk.end();
+            unsigned long long in_table = 0;
+            CK(cudaMemcpyAsync(&in_table, n_keys, 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            const uint64_t rec_cap = std::max<uint64_t>(in_table + n_low, 1);
+            rec_keys = ds.n<unsigned long long>(rec_cap);
+            rec_counts = ds.n<uint32_t>(rec_cap);
             clk.begin(4);
             CK(launch_merge_buckets(lst, low_rg, n_low_items, merge_next, d_cfg, t.slots, max_probe_cap,
                                     P.min_count, P.max_count, rec_keys, rec_counts, rec_cap, counters, st));
             clk.end();
+            clk.begin(5);
+            CK(launch_compact(t, cap, count_max, P.min_count, P.max_count, rec_keys, rec_counts, rec_cap, hist, ovf,
+                              ovf_cap, counters, st));
+            clk.end();
+        } else {
+            // merge (no records), count the records of every chunk of slots,
+            // place the chunks by a scan, then write the records in slot order
+            if (n_low) {
+                clk.begin(4);
+                CK(launch_merge_buckets(lst, low_rg, n_low_items, merge_next, d_cfg, t.slots, max_probe_cap,
+                                        P.min_count, P.max_count, nullptr, nullptr, 0, counters, st));
+                clk.end();
+            }
+            if (!bucket_arena) rec_by_bucket = false;
+            const uint64_t n_chunks = std::max<uint64_t>(compact_ordered_chunks(cap), 1);
+            uint32_t *chunk_keep = ds.n<uint32_t>(n_chunks);
+            unsigned long long *chunk_pos = ds.n<unsigned long long>(n_chunks);
+            unsigned long long *scan_tmp = ds.n<unsigned long long>(scan_tmp_words(n_chunks));
+            CK(cudaMemsetAsync(chunk_keep, 0, n_chunks * 4, st));
+            clk.begin(5);
+            CK(launch_compact_ordered(t.slots, cap, count_max, P.min_count, P.max_count, chunk_keep, nullptr, nullptr,
+                                      nullptr, 0, hist, ovf, ovf_cap, counters, 1, st));
+            CK(launch_scan_u32(chunk_keep, chunk_pos, n_chunks, scan_tmp, st));
+            clk.end();
+            unsigned long long last_pos = 0;
+            uint32_t last_keep = 0;
+            CK(cudaMemcpyAsync(&last_pos, chunk_pos + n_chunks - 1, 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(&last_keep, chunk_keep + n_chunks - 1, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            n_rec = last_pos + last_keep;
+            rec_keys = ds.n<unsigned long long>(std::max<uint64_t>(n_rec, 1));
+            rec_counts = ds.n<uint32_t>(std::max<uint64_t>(n_rec, 1));
+            clk.begin(5);
+            CK(launch_compact_ordered(t.slots, cap, count_max, P.min_count, P.max_count, chunk_keep, chunk_pos,
+                                      rec_keys, rec_counts, n_rec, hist, ovf, ovf_cap, counters, 0, st));
+            clk.end();
         }
-        clk.begin(5);
-        CK(launch_compact(t, cap, count_max, P.min_count, P.max_count, rec_keys, rec_counts, rec_cap, hist, ovf,
-                          ovf_cap, counters, st));
-        clk.end();
         Counters c2 = read_counters(counters, st);
         check_flags(c2.v[C_FLAGS], "compact");
         if (c2.v[C_FLAGS] & ERR_TABLE_FULL) throw KcError{KC_ERR_DEVICE, "counting table lookup overflow"};
-        n_rec = c2.v[C_REC_LEN];
+        if (!ordered) n_rec = c2.v[C_REC_LEN];
         job.distinct += c2.v[C_DISTINCT] + c2.v[C_LOW_ONLY];
         job.low_only += c2.v[C_LOW_ONLY];
     };
@@ -464,7 +506,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
             cap *= 2;
         }
         table_cap = cap;
-        compact_table(tr, cap, 0, nullptr, nullptr, 0, nullptr, nullptr);
+        compact_table(tr, cap, 0, nullptr, nullptr, 0, nullptr, nullptr, false);
     } else {
         // ---- root-prefix buckets (the reference's 256 root prefixes,
         // src/NewKmerTree.h:1488-1495): sizes from the SCAN census, one
@@ -676,8 +718,13 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
             TableRef tr{};
             uint64_t cap = 0;
             for (int attempt = 0;; ++attempt) {
+                // sub-tables in the order of the sort key's lowest byte: bucket
+                // b (the internal word's top byte, four bases) is that byte with
+                // its 2-bit groups reversed, so the slot-order records come out
+                // in order of the first sort digit
                 cap = 0;
-                for (uint32_t b = 0; b < N_BUCKETS; ++b) {
+                for (uint32_t r = 0; r < N_BUCKETS; ++r) {
+                    const uint32_t b = ((r & 3u) << 6) | (((r >> 2) & 3u) << 4) | (((r >> 4) & 3u) << 2) | (r >> 6);
                     cfg[b].slot_base = cap;
                     cfg[b].slot_cap = bcaps[b];
                     cap += bcaps[b];
@@ -706,7 +753,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                 if (attempt >= 3) throw KcError{KC_ERR_DEVICE, "counting table overflow"};
             }
             table_cap = std::max(table_cap, cap);
-            compact_table(tr, cap, pass_low, list, d_lr, n_low_items, merge_next, d_cfg);
+            compact_table(tr, cap, pass_low, list, d_lr, n_low_items, merge_next, d_cfg, true);
             if (multi) {
                 // this pass's records wait in pinned host memory; its device
                 // memory goes to the next pass
@@ -749,7 +796,8 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     clk.begin(6);
     if (n_rec > 1) {
         void *stmp = ds.get(sort_tmp_bytes(n_rec));
-        CK(launch_radix_sort(rec_keys, rec_counts, n_rec, 2 * k, stmp, st, counters + C_FLAGS));
+        CK(launch_radix_sort(rec_keys, rec_counts, n_rec, 2 * k, stmp, st, counters + C_FLAGS,
+                             rec_by_bucket && job.passes <= 1 ? 8u : 0u));
         ds.release(stmp);
     }
     CK(launch_pair_reverse(rec_keys, n_rec, st));

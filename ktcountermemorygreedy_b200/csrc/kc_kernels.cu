@@ -907,6 +907,109 @@ __global__ void __launch_bounds__(256) k_compact(TableRef t, uint64_t cap, uint3
         if (s_hist[i]) atomicAdd(&hist[i], (unsigned long long)s_hist[i]);
 }
 
+// Compaction of one table (or one bucket arena) in slot order, without a
+// global atomic per record or per chunk.  The slots are cut into chunks of
+// ORDERED_CHUNK, one per block at a time; warp w owns 256 consecutive slots
+// of a chunk, 8 per lane.  count_only: chunk_keep[c] = records chunk c keeps
+// and C_DISTINCT += the occupied slots.  Otherwise chunk c writes its records
+// from chunk_pos[c] (the exclusive scan of chunk_keep) on, in slot order, so
+// a bucket arena's records come out grouped by bucket, and adds every count
+// to the histogram.
+constexpr uint32_t ORDERED_CHUNK = 2048;
+constexpr uint32_t ORDERED_PER_LANE = ORDERED_CHUNK / 256;
+
+__global__ void __launch_bounds__(256) k_compact_ordered(const Slot *slots, uint64_t cap, uint32_t count_max,
+                                                         uint32_t min_count, uint32_t max_count,
+                                                         uint32_t *chunk_keep, const unsigned long long *chunk_pos,
+                                                         unsigned long long *rec_keys, uint32_t *rec_counts,
+                                                         uint64_t rec_cap, unsigned long long *hist, uint32_t *ovf,
+                                                         uint64_t ovf_cap, unsigned long long *counters, int count_only)
+{
+    __shared__ uint32_t s_hist[2048];
+    __shared__ uint32_t s_wk[2][8];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (!count_only)
+        for (int i = tid; i < 2048; i += 256) s_hist[i] = 0;
+    __syncthreads();
+    const uint64_t n_chunks = (cap + ORDERED_CHUNK - 1) / ORDERED_CHUNK;
+    const uint32_t lt = lanemask_lt();
+    uint32_t present = 0, par = 0;
+    bool full = false;
+    for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x, par ^= 1u) {
+        const uint64_t w0 = c * ORDERED_CHUNK + (uint64_t)warp * (32 * ORDERED_PER_LANE);
+        unsigned long long key[ORDERED_PER_LANE];
+        uint32_t cnt[ORDERED_PER_LANE];
+#pragma unroll
+        for (uint32_t r = 0; r < ORDERED_PER_LANE; ++r) {
+            const uint64_t i = w0 + r * 32 + lane;
+            key[r] = EMPTY_KEY;
+            cnt[r] = 0;
+            if (i < cap) {
+                const Slot sl = slots[i];
+                key[r] = sl.key;
+                cnt[r] = sl.count < count_max ? sl.count : count_max;
+            }
+        }
+        uint32_t keep = 0, wtot = 0;
+#pragma unroll
+        for (uint32_t r = 0; r < ORDERED_PER_LANE; ++r) {
+            const bool occ = key[r] != EMPTY_KEY;
+            present += occ ? 1u : 0u;
+            const bool k = occ && cnt[r] >= min_count && cnt[r] <= max_count;
+            keep |= (k ? 1u : 0u) << r;
+            wtot += (uint32_t)__popc(__ballot_sync(FULL, k));
+        }
+        if (lane == 0) s_wk[par][warp] = wtot;
+        __syncthreads();
+        uint32_t before = 0, ctot = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+            const uint32_t v = s_wk[par][w];
+            before += w < warp ? v : 0u;
+            ctot += v;
+        }
+        if (count_only) {
+            if (tid == 0) chunk_keep[c] = ctot;
+            continue;
+        }
+        unsigned long long pos = chunk_pos[c] + before;
+#pragma unroll
+        for (uint32_t r = 0; r < ORDERED_PER_LANE; ++r) {
+            const bool k = (keep >> r) & 1u;
+            const uint32_t b = __ballot_sync(FULL, k);
+            if (k) {
+                const unsigned long long q = pos + (uint32_t)__popc(b & lt);
+                if (q < rec_cap) {
+                    rec_keys[q] = pair_reverse(key[r]);
+                    rec_counts[q] = cnt[r];
+                } else {
+                    full = true;
+                }
+            }
+            pos += (uint32_t)__popc(b);
+            if (key[r] != EMPTY_KEY) {
+                const uint32_t cc = cnt[r];
+                if (cc < 2048) atomicAdd(&s_hist[cc], 1u);
+                else if (cc < HIST_BINS) atomicAdd(&hist[cc], 1ull);
+                else {
+                    const unsigned long long p = atomicAdd(&counters[C_OVF_LEN], 1ull);
+                    if (p < ovf_cap) ovf[p] = cc;
+                    else atomicOr(&counters[C_FLAGS], ERR_HIST_OVERFLOW_FULL);
+                }
+            }
+        }
+    }
+    if (full) atomicOr(&counters[C_FLAGS], ERR_RECORDS_FULL);
+    if (count_only) {
+        const unsigned d = __reduce_add_sync(FULL, present);
+        if (lane == 0 && d) atomicAdd(&counters[C_DISTINCT], (unsigned long long)d);
+        return;
+    }
+    __syncthreads();
+    for (int i = tid; i < 2048; i += 256)
+        if (s_hist[i]) atomicAdd(&hist[i], (unsigned long long)s_hist[i]);
+}
+
 // Batched jobs keep all samples' tables in one slot arena.  Sample s owns
 // slots [slot_base, slot_base + slot_cap), cut into chunks of COMPACT_CHUNK
 // slots; chunk0[s] is the index of its first chunk (chunk0[n] = all chunks),
@@ -1902,6 +2005,27 @@ cudaError_t launch_compact(TableRef t, uint64_t cap, uint32_t count_max, uint32_
     return cudaGetLastError();
 }
 
+uint64_t compact_ordered_chunks(uint64_t cap) { return (cap + ORDERED_CHUNK - 1) / ORDERED_CHUNK; }
+
+cudaError_t launch_compact_ordered(const Slot *slots, uint64_t cap, uint32_t count_max, uint32_t min_count,
+                                   uint32_t max_count, uint32_t *chunk_keep, const unsigned long long *chunk_pos,
+                                   unsigned long long *rec_keys, uint32_t *rec_counts, uint64_t rec_cap,
+                                   unsigned long long *hist, uint32_t *ovf, uint64_t ovf_cap,
+                                   unsigned long long *counters, int count_only, cudaStream_t st)
+{
+    if (!cap) return cudaSuccess;
+    const uint64_t n_chunks = compact_ordered_chunks(cap);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_compact_ordered, 256, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const uint64_t grid = std::min<uint64_t>(n_chunks, (uint64_t)sm_count() * per_sm);
+    note_launch();
+    k_compact_ordered<<<(unsigned)grid, 256, 0, st>>>(slots, cap, count_max, min_count, max_count, chunk_keep,
+                                                      chunk_pos, rec_keys, rec_counts, rec_cap, hist, ovf, ovf_cap,
+                                                      counters, count_only);
+    return cudaGetLastError();
+}
+
 static uint64_t sort_tiles_for(const uint64_t *seg_len, uint32_t n_segs)
 {
     uint64_t t = 0;
@@ -2112,11 +2236,12 @@ cudaError_t launch_radix_sort_in_scratch(unsigned long long *keys, uint32_t *val
 }
 
 cudaError_t launch_radix_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
-                              cudaStream_t st, unsigned long long *flags)
+                              cudaStream_t st, unsigned long long *flags, uint32_t skip_bits)
 {
     if (n <= 1 || bits == 0) return cudaSuccess;
-    if (bits > 64) return cudaErrorInvalidValue;
+    if (bits > 64 || skip_bits % 8) return cudaErrorInvalidValue;
     const uint32_t passes = (bits + 7) / 8;
+    if (skip_bits / 8 >= passes) return cudaSuccess;
     const uint64_t n_tiles = (n + RS_TILE - 1) / RS_TILE;
     uint8_t *p = static_cast<uint8_t *>(tmp);
     unsigned long long *k2 = reinterpret_cast<unsigned long long *>(p);
@@ -2141,7 +2266,7 @@ cudaError_t launch_radix_sort(unsigned long long *keys, uint32_t *vals, uint64_t
     if (e != cudaSuccess) return e;
     unsigned long long *ks = keys, *kd = k2;
     uint32_t *vs = vals, *vd = v2;
-    for (uint32_t pass = 0; pass < passes; ++pass) {
+    for (uint32_t pass = skip_bits / 8; pass < passes; ++pass) {
         note_launch();
         k_radix_onesweep<<<(unsigned)n_tiles, RS_THREADS, smem, st>>>(ks, vs, kd, vd, n, pass, hist, look, tile_ctr,
                                                                       flags, nullptr);

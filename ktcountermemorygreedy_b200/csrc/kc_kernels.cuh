@@ -184,6 +184,18 @@ cudaError_t launch_compact(TableRef t, uint64_t cap, uint32_t count_max, uint32_
                            unsigned long long *hist, uint32_t *ovf, uint64_t ovf_cap,
                            unsigned long long *counters, cudaStream_t st);
 
+// Slot-order compaction of one table or bucket arena (records in slot order,
+// so a bucket arena gives records grouped by bucket).  Run once with
+// count_only = 1 (chunk_keep[c] = records kept by chunk c, C_DISTINCT +=
+// occupied slots), scan chunk_keep into chunk_pos, then with count_only = 0
+// (records written from chunk_pos[c] on, histogram added to).
+uint64_t compact_ordered_chunks(uint64_t cap);
+cudaError_t launch_compact_ordered(const Slot *slots, uint64_t cap, uint32_t count_max, uint32_t min_count,
+                                   uint32_t max_count, uint32_t *chunk_keep, const unsigned long long *chunk_pos,
+                                   unsigned long long *rec_keys, uint32_t *rec_counts, uint64_t rec_cap,
+                                   unsigned long long *hist, uint32_t *ovf, uint64_t ovf_cap,
+                                   unsigned long long *counters, int count_only, cudaStream_t st);
+
 // LSD radix sort of (key, value) pairs on the low `bits` bits of the keys,
 // 8 bits per pass.  Result ends in keys/vals.
 size_t sort_tmp_bytes(uint64_t n);
@@ -194,9 +206,10 @@ cudaError_t launch_radix_sort_segmented(unsigned long long *keys, uint32_t *vals
                                         const uint32_t *seg_bits = nullptr,    // per segment, <= bits
                                         uint64_t group_records = 4ull << 20);  // records per L2-sized group
 // One segment, one kernel per 8-bit pass; a look-back wait that gave up sets
-// ERR_WAIT_TIMEOUT in *flags (NULL: a word inside tmp).
+// ERR_WAIT_TIMEOUT in *flags (NULL: a word inside tmp).  Keys already in
+// order of their low skip_bits bits (a multiple of 8) skip those passes.
 cudaError_t launch_radix_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
-                              cudaStream_t st, unsigned long long *flags = nullptr);
+                              cudaStream_t st, unsigned long long *flags = nullptr, uint32_t skip_bits = 0);
 
 // Compaction of a batched job's slot arena in chunks of slots that each
 // belong to one sample: count_only fills chunk_keep (records per chunk) and
