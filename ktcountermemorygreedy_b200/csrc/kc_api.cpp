@@ -408,10 +408,13 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     // Slot-order records of a bucket arena are grouped by bucket, and the
     // bucket (root prefix) is the lowest 8 bits of the printed-order sort key:
     // the sort then skips that pass.
-    bool rec_by_bucket = true;
+    // into_sort_tmp: the records are written into the sort's alternate
+    // buffers, from which an odd number of passes ends in rec_keys/rec_counts.
+    bool rec_by_bucket = true, rec_in_sort_tmp = false;
+    void *sort_tmp = nullptr;
     auto compact_table = [&](const TableRef &t, uint64_t cap, uint64_t n_low, const unsigned long long *lst,
                              const BucketRanges *low_rg, uint32_t n_low_items, unsigned int *merge_next,
-                             const BucketCfg *d_cfg, bool bucket_arena) {
+                             const BucketCfg *d_cfg, bool bucket_arena, bool into_sort_tmp) {
         CK(cudaMemsetAsync(counters + C_REC_LEN, 0, 3 * 8, st));   // C_REC_LEN, C_LOW_ONLY, C_DISTINCT
         const bool want1 = P.min_count <= 1 && 1 <= P.max_count;
         bool ordered = true;
@@ -466,9 +469,16 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
             n_rec = last_pos + last_keep;
             rec_keys = ds.n<unsigned long long>(std::max<uint64_t>(n_rec, 1));
             rec_counts = ds.n<uint32_t>(std::max<uint64_t>(n_rec, 1));
+            unsigned long long *wk = rec_keys;
+            uint32_t *wc = rec_counts;
+            if (into_sort_tmp && n_rec > 1) {
+                sort_tmp = ds.get(sort_tmp_bytes(n_rec));
+                sort_tmp_alt(sort_tmp, n_rec, &wk, &wc);
+                rec_in_sort_tmp = true;
+            }
             clk.begin(5);
-            CK(launch_compact_ordered(t.slots, cap, count_max, P.min_count, P.max_count, chunk_keep, chunk_pos,
-                                      rec_keys, rec_counts, n_rec, hist, ovf, ovf_cap, counters, 0, st));
+            CK(launch_compact_ordered(t.slots, cap, count_max, P.min_count, P.max_count, chunk_keep, chunk_pos, wk,
+                                      wc, n_rec, hist, ovf, ovf_cap, counters, 0, st));
             clk.end();
         }
         Counters c2 = read_counters(counters, st);
@@ -506,7 +516,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
             cap *= 2;
         }
         table_cap = cap;
-        compact_table(tr, cap, 0, nullptr, nullptr, 0, nullptr, nullptr, false);
+        compact_table(tr, cap, 0, nullptr, nullptr, 0, nullptr, nullptr, false, false);
     } else {
         // ---- root-prefix buckets (the reference's 256 root prefixes,
         // src/NewKmerTree.h:1488-1495): sizes from the SCAN census, one
@@ -753,7 +763,10 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                 if (attempt >= 3) throw KcError{KC_ERR_DEVICE, "counting table overflow"};
             }
             table_cap = std::max(table_cap, cap);
-            compact_table(tr, cap, pass_low, list, d_lr, n_low_items, merge_next, d_cfg, true);
+            // a single pass's records can go straight into the sort's buffers
+            // when the sort (first digit skipped) runs an odd number of passes
+            compact_table(tr, cap, pass_low, list, d_lr, n_low_items, merge_next, d_cfg, true,
+                          !multi && sort_passes_run(2 * k, 8) % 2 == 1);
             if (multi) {
                 // this pass's records wait in pinned host memory; its device
                 // memory goes to the next pass
@@ -795,10 +808,14 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     // ---- sort in printed-string order ---------------------------------------
     clk.begin(6);
     if (n_rec > 1) {
-        void *stmp = ds.get(sort_tmp_bytes(n_rec));
-        CK(launch_radix_sort(rec_keys, rec_counts, n_rec, 2 * k, stmp, st, counters + C_FLAGS,
-                             rec_by_bucket && job.passes <= 1 ? 8u : 0u));
-        ds.release(stmp);
+        const uint32_t skip = rec_by_bucket && job.passes <= 1 ? 8u : 0u;
+        if (rec_in_sort_tmp) {
+            CK(launch_radix_sort(rec_keys, rec_counts, n_rec, 2 * k, sort_tmp, st, counters + C_FLAGS, skip, true));
+        } else {
+            void *stmp = ds.get(sort_tmp_bytes(n_rec));
+            CK(launch_radix_sort(rec_keys, rec_counts, n_rec, 2 * k, stmp, st, counters + C_FLAGS, skip));
+            ds.release(stmp);
+        }
     }
     CK(launch_pair_reverse(rec_keys, n_rec, st));
     clk.end();

@@ -2069,6 +2069,19 @@ static size_t onesweep_tmp_bytes(uint64_t n)
 
 size_t sort_tmp_bytes(uint64_t n) { return onesweep_tmp_bytes(n); }
 
+void sort_tmp_alt(void *tmp, uint64_t n, unsigned long long **k2, uint32_t **v2)
+{
+    uint8_t *p = static_cast<uint8_t *>(tmp);
+    *k2 = reinterpret_cast<unsigned long long *>(p);
+    *v2 = reinterpret_cast<uint32_t *>(p + align256(n * 8));
+}
+
+uint32_t sort_passes_run(uint32_t bits, uint32_t skip_bits)
+{
+    const uint32_t passes = (bits + 7) / 8, skipped = skip_bits / 8;
+    return skipped < passes ? passes - skipped : 0;
+}
+
 size_t sort_tmp_bytes_in_scratch(uint64_t n) { return scratch_sort_bytes(n); }
 
 // Segments [seg_start[i], seg_start[i] + seg_len[i]) of the arrays are sorted
@@ -2236,12 +2249,10 @@ cudaError_t launch_radix_sort_in_scratch(unsigned long long *keys, uint32_t *val
 }
 
 cudaError_t launch_radix_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
-                              cudaStream_t st, unsigned long long *flags, uint32_t skip_bits)
+                              cudaStream_t st, unsigned long long *flags, uint32_t skip_bits, bool input_in_tmp)
 {
-    if (n <= 1 || bits == 0) return cudaSuccess;
     if (bits > 64 || skip_bits % 8) return cudaErrorInvalidValue;
     const uint32_t passes = (bits + 7) / 8;
-    if (skip_bits / 8 >= passes) return cudaSuccess;
     const uint64_t n_tiles = (n + RS_TILE - 1) / RS_TILE;
     uint8_t *p = static_cast<uint8_t *>(tmp);
     unsigned long long *k2 = reinterpret_cast<unsigned long long *>(p);
@@ -2255,25 +2266,34 @@ cudaError_t launch_radix_sort(unsigned long long *keys, uint32_t *vals, uint64_t
     unsigned int *tile_ctr = reinterpret_cast<unsigned int *>(p);
     unsigned long long *own_flags = reinterpret_cast<unsigned long long *>(p + OS_MAX_PASSES * 4);
     if (!flags) flags = own_flags;
-    cudaError_t e = cudaMemsetAsync(hist, 0, OS_MAX_PASSES * 256 * 8, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(look, 0, n_tiles * 256 * 8, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(tile_ctr, 0, OS_MAX_PASSES * 4 + 8, st);
-    if (e != cudaSuccess) return e;
-    note_launch();
-    k_radix_hist_all<<<grid_for(n, 256, 4), 256, 0, st>>>(keys, n, passes, hist);
+    // records placed in the alternate buffers (input_in_tmp) end in keys/vals
+    // after an odd number of passes without the final copy
+    unsigned long long *ks = keys, *kd = k2;
+    uint32_t *vs = vals, *vd = v2;
+    if (input_in_tmp) {
+        std::swap(ks, kd);
+        std::swap(vs, vd);
+    }
+    cudaError_t e = cudaSuccess;
+    if (n > 1 && bits && skip_bits / 8 < passes) {
+        e = cudaMemsetAsync(hist, 0, OS_MAX_PASSES * 256 * 8, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(look, 0, n_tiles * 256 * 8, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(tile_ctr, 0, OS_MAX_PASSES * 4 + 8, st);
+        if (e != cudaSuccess) return e;
+        note_launch();
+        k_radix_hist_all<<<grid_for(n, 256, 4), 256, 0, st>>>(ks, n, passes, hist);
+    }
     const size_t smem = RS_TILE * 8 + RS_TILE * 4 + 8 * 256 * 4;
     e = cudaFuncSetAttribute(k_radix_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    unsigned long long *ks = keys, *kd = k2;
-    uint32_t *vs = vals, *vd = v2;
-    for (uint32_t pass = skip_bits / 8; pass < passes; ++pass) {
+    for (uint32_t pass = skip_bits / 8; n > 1 && pass < passes; ++pass) {
         note_launch();
         k_radix_onesweep<<<(unsigned)n_tiles, RS_THREADS, smem, st>>>(ks, vs, kd, vd, n, pass, hist, look, tile_ctr,
                                                                       flags, nullptr);
         std::swap(ks, kd);
         std::swap(vs, vd);
     }
-    if (ks != keys) {
+    if (ks != keys && n) {
         e = cudaMemcpyAsync(keys, ks, n * 8, cudaMemcpyDeviceToDevice, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(vals, vs, n * 4, cudaMemcpyDeviceToDevice, st);
         if (e != cudaSuccess) return e;

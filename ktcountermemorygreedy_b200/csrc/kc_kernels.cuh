@@ -208,8 +208,14 @@ cudaError_t launch_radix_sort_segmented(unsigned long long *keys, uint32_t *vals
 // One segment, one kernel per 8-bit pass; a look-back wait that gave up sets
 // ERR_WAIT_TIMEOUT in *flags (NULL: a word inside tmp).  Keys already in
 // order of their low skip_bits bits (a multiple of 8) skip those passes.
+// input_in_tmp: the records are in the alternate buffers inside tmp
+// (sort_tmp_alt) instead of keys/vals; the result still ends in keys/vals,
+// without a final copy when sort_passes_run() is odd.
 cudaError_t launch_radix_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
-                              cudaStream_t st, unsigned long long *flags = nullptr, uint32_t skip_bits = 0);
+                              cudaStream_t st, unsigned long long *flags = nullptr, uint32_t skip_bits = 0,
+                              bool input_in_tmp = false);
+void sort_tmp_alt(void *tmp, uint64_t n, unsigned long long **k2, uint32_t **v2);
+uint32_t sort_passes_run(uint32_t bits, uint32_t skip_bits);
 
 // Compaction of a batched job's slot arena in chunks of slots that each
 // belong to one sample: count_only fills chunk_keep (records per chunk) and
