@@ -133,6 +133,10 @@ def algorithmic_bytes(phase: str, r):
         return S + 8 * O if r.low_len + r.high_len else S + 16 * O
     if phase == "bloom":               # bucketed k-mers read + list write (16 B) + two filter words (16 B)
         return 32 * O
+    if phase == "sub_partition":       # bucketed k-mers read + written in sub-bucket order
+        return 16 * O
+    if phase == "smem_count":          # sub-bucket k-mers read, FIRST ones written back and read again, records
+        return 8 * O + 16 * r.low_len + 12 * r.n_records_total
     if phase == "insert_high":         # list read (8 B) + slot key read and count update (16 B)
         return 24 * r.high_len
     if phase == "merge_low":

@@ -127,7 +127,9 @@ typedef struct {
      * (plain) or scatter into the root-prefix buckets (Bloom), [3] insert of
      * the non-FIRST k-mers, [4] merge of the FIRST k-mers, [5] compaction +
      * histogram, [6] radix sort, [7] queries, [8] Bloom classification,
-     * [9..11] unused */
+     * [9] scatter of the buckets into filter sub-buckets and [10] their
+     * shared-memory Bloom split + count + compaction (Bloom mode, min count
+     * >= 2), [11] unused */
     double phase_ms[KC_STAGES];
     uint64_t phase_launches[KC_STAGES];   /* kernel launches per stage */
     uint64_t low_len;             /* Bloom mode: FIRST occurrences (merged after the inserts) */
@@ -136,7 +138,8 @@ typedef struct {
     uint64_t input_bytes;         /* FASTQ bytes of the job */
     uint64_t n_records_total;     /* records on the device (also when keep_records = 0) */
     uint32_t passes;              /* counting passes over ranges of root prefixes (1: the whole job at once) */
-    uint32_t reserved0;
+    uint16_t smem_passes;         /* passes counted on the shared-memory sub-bucket path (Bloom mode) */
+    uint16_t smem_fallbacks;      /* passes that left it after a sub-bucket table overflowed */
 } kc_result_t;
 
 /* Settings of a handle that trade memory for speed, chosen by kc_autotune or
@@ -148,7 +151,10 @@ typedef struct {
                                      default 1.6 */
     uint64_t sort_group_records;  /* records sorted together (kept in L2) by a batch's segmented sort;
                                      default 4M */
-    uint64_t reserved[5];
+    uint64_t bloom_smem;          /* Bloom jobs with min_count >= 2: 1 counts each sub-bucket (a 64 KiB slice
+                                     of its filter) in shared memory, 2 uses global-memory filters and
+                                     tables; default 1 */
+    uint64_t reserved[4];
 } kc_tuning;
 
 /* Kernel launches issued by this process so far (all handles). */

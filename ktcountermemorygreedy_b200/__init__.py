@@ -56,7 +56,7 @@ class kc_config(C.Structure):
 
 class kc_tuning(C.Structure):
     _fields_ = [("bucket_table_factor", C.c_double), ("table_factor", C.c_double),
-                ("sort_group_records", C.c_uint64), ("reserved", C.c_uint64 * 5)]
+                ("sort_group_records", C.c_uint64), ("bloom_smem", C.c_uint64), ("reserved", C.c_uint64 * 4)]
 
 
 class kc_buffer(C.Structure):
@@ -82,11 +82,12 @@ class kc_result_t(C.Structure):
                 ("table_capacity", C.c_uint64), ("device_ms", C.c_double), ("queue_ms", C.c_double),
                 ("run_ms", C.c_double), ("phase_ms", C.c_double * 12), ("phase_launches", C.c_uint64 * 12),
                 ("low_len", C.c_uint64), ("high_len", C.c_uint64), ("input_bytes", C.c_uint64),
-                ("n_records_total", C.c_uint64), ("passes", C.c_uint32), ("reserved0", C.c_uint32)]
+                ("n_records_total", C.c_uint64), ("passes", C.c_uint32), ("smem_passes", C.c_uint16),
+                ("smem_fallbacks", C.c_uint16)]
 
 # stage names of kc_result_t.phase_ms
 PHASES = ["census", "scan", "count_pass", "insert_high", "merge_low", "compact", "sort", "queries", "bloom",
-          "stage9", "stage10", "stage11"]
+          "sub_partition", "smem_count", "stage11"]
 
 
 # (name, restype, argtypes) of every symbol include/kc.h declares
@@ -210,6 +211,8 @@ class Result:
     input_bytes: int = 0
     n_records_total: int = 0
     passes: int = 1
+    smem_passes: int = 0      # passes counted per sub-bucket in shared memory (Bloom mode)
+    smem_fallbacks: int = 0   # passes recounted on global-memory tables after a sub-bucket table overflowed
 
 
 def _copy(ptr, n, dtype):
@@ -358,7 +361,8 @@ class KmerCounter:
             occurrences=r.occurrences, distinct=r.distinct, low_only=r.low_only,
             table_capacity=r.table_capacity, device_ms=r.device_ms, queue_ms=r.queue_ms, run_ms=r.run_ms,
             phase_ms=tuple(r.phase_ms), phase_launches=tuple(r.phase_launches), low_len=r.low_len,
-            high_len=r.high_len, input_bytes=r.input_bytes, n_records_total=r.n_records_total, passes=r.passes)
+            high_len=r.high_len, input_bytes=r.input_bytes, n_records_total=r.n_records_total, passes=r.passes,
+            smem_passes=r.smem_passes, smem_fallbacks=r.smem_fallbacks)
         if release:
             self.release(jid)
         return out
@@ -384,12 +388,16 @@ class KmerCounter:
         t = kc_tuning()
         _check(lib().kc_get_tuning(self._h, C.byref(t)))
         return {"bucket_table_factor": t.bucket_table_factor, "table_factor": t.table_factor,
-                "sort_group_records": t.sort_group_records}
+                "sort_group_records": t.sort_group_records, "bloom_smem": t.bloom_smem}
 
-    def set_tuning(self, bucket_table_factor: float = 0.0, table_factor: float = 0.0, sort_group_records: int = 0):
+    def set_tuning(self, bucket_table_factor: float = 0.0, table_factor: float = 0.0, sort_group_records: int = 0,
+                   bloom_smem: int = 0):
+        """0 (or less) keeps a setting.  bloom_smem: 1 counts Bloom jobs (min
+        count >= 2) per sub-bucket in shared memory, 2 on global-memory tables."""
         t = kc_tuning()
         t.bucket_table_factor, t.table_factor, t.sort_group_records = bucket_table_factor, table_factor, \
             sort_group_records
+        t.bloom_smem = bloom_smem
         _check(lib().kc_set_tuning(self._h, C.byref(t)))
 
     def autotune(self, samples: Sequence[Sequence[bytes]] = (), ks: Sequence[int] = (), batch: bool = False,

@@ -74,8 +74,15 @@ kc_tuning default_tuning()
     t.bucket_table_factor = 3.0;
     t.table_factor = 1.6;
     t.sort_group_records = 4ull << 20;
+    t.bloom_smem = 1;
     return t;
 }
+
+// k-mers per sub-bucket the shared-memory Bloom path starts from.  Its table
+// (SUB_TABLE_SLOTS) holds the distinct non-FIRST k-mers: at 30x coverage with
+// 1% errors about 2k of 48k, a quarter of the table; a sub-bucket with more
+// is cut in two and counted again.
+constexpr uint64_t SUB_KEYS_TARGET = 48 * 1024;
 
 // A plain job whose table would hold more slots than this (64 MiB of slots,
 // half of L2) is counted through the root-prefix buckets.
@@ -119,7 +126,7 @@ struct Job {
     HostRecords le2;   // records with count <= 2 (pinned: often most of the records)
     uint64_t occurrences = 0, distinct = 0, low_only = 0, table_cap = 0;
     uint64_t low_len = 0, high_len = 0, input_bytes = 0, n_records_total = 0;
-    uint32_t passes = 1;
+    uint32_t passes = 1, smem_passes = 0, smem_fallbacks = 0;
     double device_ms = 0;
     double phase_ms[KC_STAGES] = {0};
     uint64_t phase_launches[KC_STAGES] = {0};
@@ -391,6 +398,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     const uint32_t max_probe_cap = 1u << 16;
     const double est = hll_estimate(hll_h.data(), HLL_M);
     unsigned long long *hist = ds.n<unsigned long long>(HIST_BINS);
+    std::vector<unsigned long long> hist_add(HIST_BINS, 0);   // histograms of shared-memory sub-bucket passes
     const uint64_t ovf_cap = 1 << 20;
     uint32_t *ovf = ds.n<uint32_t>(ovf_cap);
     unsigned long long *n_keys = ds.n<unsigned long long>(1);
@@ -398,6 +406,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     unsigned long long low_len = 0, high_len = 0;
     uint64_t table_cap = 0;
     job.distinct = job.low_only = 0;
+    job.smem_passes = job.smem_fallbacks = 0;
 
     // Records of one counted table: the FIRST occurrences are merged in (Bloom
     // mode), every occupied slot is compacted into new record arrays, and the
@@ -622,7 +631,6 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
             }
             CK(cudaMemsetAsync(cursor, 0, N_BUCKETS * 8, st));
             CK(cudaMemcpyAsync(bbase, bb.data(), 2 * N_BUCKETS * 8, cudaMemcpyHostToDevice, st));
-            if (P.bloom) CK(cudaMemsetAsync(bits, 0, words * 8, st));
             CK(cudaMemsetAsync(lh_cnt, 0, 2 * N_BUCKETS * 8, st));
             CK(cudaMemsetAsync(hll_high, 0, (size_t)N_BUCKETS * BUCKET_HLL_M * 4, st));
             a.hll = nullptr;
@@ -654,119 +662,245 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                 CK(cudaMemcpyAsync(d, &r, sizeof(BucketRanges), cudaMemcpyHostToDevice, st));
                 return d;
             };
-            std::vector<unsigned long long> lh(2 * N_BUCKETS, 0);
-            std::vector<uint32_t> hh;
-            if (P.bloom) {
-                clk.begin(8);
-                BucketRanges br{};
+            // Bloom jobs whose records need count >= 2: the Bloom split, the
+            // counting and the compaction run per sub-bucket (a slice of its
+            // bucket's filter) in shared memory.  A bucket starts with about
+            // SUB_KEYS_TARGET k-mers per sub-bucket (and slices of at most
+            // SUB_SLICE_BLOCKS blocks); a bucket whose table overflowed is
+            // counted again with twice the sub-buckets, and a bucket that
+            // cannot be cut further sends the pass to the global-memory path.
+            bool sub_done = false;
+            if (P.bloom && P.min_count >= 2 && tn.bloom_smem == 1) {
+                std::vector<uint32_t> nsub(N_BUCKETS, 0);
+                bool eligible = true;
                 for (uint32_t b = lo; b < hi; ++b) {
-                    br.begin[b] = cfg[b].key_base;
-                    br.len[b] = cfg[b].key_len;
-                }
-                uint32_t n_items = 0;
-                BucketRanges *d_br = upload_ranges(br, n_items);
-                CK(launch_bloom_buckets(keys, d_br, n_items, next_item, d_cfg_b, bits, list, lh_cnt, lh_cnt + N_BUCKETS,
-                                        hll_high, st));
-                clk.end();
-                hh.resize((size_t)N_BUCKETS * BUCKET_HLL_M);
-                CK(cudaMemcpyAsync(lh.data(), lh_cnt, 2 * N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
-                CK(cudaMemcpyAsync(hh.data(), hll_high, hh.size() * 4, cudaMemcpyDeviceToHost, st));
-                ds.release(d_br);
-            } else {
-                // every occurrence goes to the table: the whole bucket is "high"
-                for (uint32_t b = lo; b < hi; ++b) lh[N_BUCKETS + b] = cfg[b].key_len;
-            }
-            Counters c = read_counters(counters, st);
-            check_flags(c.v[C_FLAGS], "partition");
-            ds.release(next_item);
-            ds.release(hll_high);
-            ds.release(lh_cnt);
-            ds.release(bbase);
-            ds.release(cursor);
-            ds.release(d_cfg_b);
-            if (P.bloom) {
-                ds.release(keys);
-                ds.release(bits);
-            }
-            uint64_t pass_low = 0;
-            std::vector<uint64_t> bcaps(N_BUCKETS, 0);
-            for (uint32_t b = lo; b < hi; ++b) {
-                const unsigned long long hb = lh[N_BUCKETS + b];
-                pass_low += lh[b];
-                high_len += hb;
-                double e;
-                if (P.bloom) {
-                    // the registers hold a hash sample of the non-FIRST k-mers
-                    e = hb ? (double)(1u << BUCKET_HLL_SAMPLE_BITS) *
-                                 hll_estimate(&hh[(size_t)b * BUCKET_HLL_M], BUCKET_HLL_M)
-                           : 0.0;
-                } else {
-                    // the job's distinct estimate, shared out by occurrences
-                    e = O ? est * (double)hb / (double)O : 0.0;
-                    e = std::min(e, (double)hb);
-                }
-                e = std::max(e, (double)std::min<unsigned long long>(hb, 4096));
-                bcaps[b] = table_capacity_for(e, tn.bucket_table_factor);
-            }
-            low_len += pass_low;
-            // per-bucket sub-tables in one arena; a bucket whose table
-            // overflows gets twice the slots and the insert is repeated
-            BucketCfg *d_cfg = ds.n<BucketCfg>(N_BUCKETS);
-            unsigned long long *bucket_ovf = ds.n<unsigned long long>(N_BUCKETS);
-            next_item = ds.n<unsigned int>(1);
-            unsigned int *merge_next = ds.n<unsigned int>(1);
-            BucketRanges hr{}, lr{};
-            for (uint32_t b = lo; b < hi; ++b) {
-                hr.begin[b] = cfg[b].key_base + cfg[b].key_len - lh[N_BUCKETS + b];
-                hr.len[b] = lh[N_BUCKETS + b];
-                lr.begin[b] = cfg[b].key_base;
-                lr.len[b] = lh[b];
-            }
-            uint32_t n_high_items = 0, n_low_items = 0;
-            BucketRanges *d_hr = upload_ranges(hr, n_high_items);
-            BucketRanges *d_lr = upload_ranges(lr, n_low_items);
-            TableRef tr{};
-            uint64_t cap = 0;
-            for (int attempt = 0;; ++attempt) {
-                // sub-tables in the order of the sort key's lowest byte: bucket
-                // b (the internal word's top byte, four bases) is that byte with
-                // its 2-bit groups reversed, so the slot-order records come out
-                // in order of the first sort digit
-                cap = 0;
-                for (uint32_t r = 0; r < N_BUCKETS; ++r) {
-                    const uint32_t b = ((r & 3u) << 6) | (((r >> 2) & 3u) << 4) | (((r >> 4) & 3u) << 2) | (r >> 6);
-                    cfg[b].slot_base = cap;
-                    cfg[b].slot_cap = bcaps[b];
-                    cap += bcaps[b];
-                }
-                if (tr.slots) ds.release(tr.slots);
-                tr.slots = static_cast<Slot *>(ds.get(std::max<uint64_t>(cap, 1) * sizeof(Slot)));
-                tr.mask = 0;   // the arena is addressed per bucket
-                CK(launch_init_slots(tr.slots, cap, st));
-                CK(cudaMemcpyAsync(d_cfg, cfg.data(), N_BUCKETS * sizeof(BucketCfg), cudaMemcpyHostToDevice, st));
-                CK(cudaMemsetAsync(bucket_ovf, 0, N_BUCKETS * 8, st));
-                clk.begin(3);
-                CK(launch_insert_buckets(list, d_hr, n_high_items, next_item, d_cfg, tr.slots, max_probe_cap, bucket_ovf,
-                                         st));
-                clk.end();
-                std::vector<unsigned long long> ov(N_BUCKETS);
-                CK(cudaMemcpyAsync(ov.data(), bucket_ovf, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
-                Counters cc = read_counters(counters, st);
-                check_flags(cc.v[C_FLAGS], "insert");
-                bool any = false;
-                for (uint32_t b = 0; b < N_BUCKETS; ++b)
-                    if (ov[b]) {
-                        bcaps[b] *= 2;
-                        any = true;
+                    const uint64_t f = fcap[b];
+                    if (!f || (f & (f - 1))) {
+                        eligible = false;
+                        break;
                     }
-                if (!any) break;
-                if (attempt >= 3) throw KcError{KC_ERR_DEVICE, "counting table overflow"};
+                    uint64_t want = std::max<uint64_t>(f / SUB_SLICE_BLOCKS, (cfg[b].key_len + SUB_KEYS_TARGET - 1) / SUB_KEYS_TARGET);
+                    want = std::max<uint64_t>(bit_ceil64(want), 1);
+                    if (want > std::min<uint64_t>(f, SUB_MAX_PER_BUCKET)) {
+                        eligible = false;
+                        break;
+                    }
+                    nsub[b] = (uint32_t)want;
+                }
+                const Counters before = read_counters(counters, st);
+                for (int attempt = 0; eligible && !sub_done; ++attempt) {
+                    const DevScope::Mark m0 = ds.mark();
+                    std::vector<SubCfg> sc(N_BUCKETS);
+                    std::vector<uint8_t> sb;
+                    uint32_t n_sub = 0;
+                    uint64_t pass_keys = 0;
+                    for (uint32_t b = lo; b < hi; ++b) {
+                        sc[b].fcap = fcap[b];
+                        sc[b].sub_base = n_sub;
+                        sc[b].n_sub = nsub[b];
+                        sc[b].slice_shift = (uint32_t)__builtin_ctzll(fcap[b] / nsub[b]);
+                        n_sub += nsub[b];
+                        sb.insert(sb.end(), nsub[b], (uint8_t)b);
+                        pass_keys += cfg[b].key_len;
+                    }
+                    SubCfg *d_sc = ds.n<SubCfg>(N_BUCKETS);
+                    uint8_t *d_sb = ds.n<uint8_t>(std::max<uint32_t>(n_sub, 1));
+                    uint32_t *sub_count = ds.n<uint32_t>(std::max<uint32_t>(n_sub, 1));
+                    unsigned long long *sub_off = ds.n<unsigned long long>(std::max<uint32_t>(n_sub, 1));
+                    unsigned long long *sub_cur = ds.n<unsigned long long>(std::max<uint32_t>(n_sub, 1));
+                    unsigned long long *sub_tmp =
+                        ds.n<unsigned long long>(scan_tmp_words(std::max<uint32_t>(n_sub, 1)));
+                    unsigned int *sub_next = ds.n<unsigned int>(1);
+                    uint32_t *bucket_ovf = ds.n<uint32_t>(N_BUCKETS);
+                    unsigned long long *hist_sub = ds.n<unsigned long long>(HIST_BINS);
+                    // a record has count >= 2: at most half the occurrences, and at
+                    // most one table of slots per sub-bucket
+                    const uint64_t rcap = std::max<uint64_t>(
+                        std::min<uint64_t>((uint64_t)n_sub * SUB_TABLE_SLOTS, pass_keys / 2 + 1), 1);
+                    unsigned long long *rk = ds.n<unsigned long long>(rcap);
+                    uint32_t *rc = ds.n<uint32_t>(rcap);
+                    BucketRanges br{};
+                    for (uint32_t b = lo; b < hi; ++b) {
+                        br.begin[b] = cfg[b].key_base;
+                        br.len[b] = cfg[b].key_len;
+                    }
+                    uint32_t n_items = 0;
+                    BucketRanges *d_br = upload_ranges(br, n_items);
+                    CK(cudaMemcpyAsync(d_sc, sc.data(), N_BUCKETS * sizeof(SubCfg), cudaMemcpyHostToDevice, st));
+                    if (n_sub) CK(cudaMemcpyAsync(d_sb, sb.data(), n_sub, cudaMemcpyHostToDevice, st));
+                    CK(cudaMemsetAsync(sub_count, 0, std::max<uint32_t>(n_sub, 1) * 4, st));
+                    CK(cudaMemsetAsync(bucket_ovf, 0, N_BUCKETS * 4, st));
+                    CK(cudaMemsetAsync(hist_sub, 0, HIST_BINS * 8, st));
+                    CK(cudaMemsetAsync(counters + C_LOW_LEN, 0, 2 * 8, st));   // C_LOW_LEN, C_HIGH_LEN
+                    CK(cudaMemsetAsync(counters + C_REC_LEN, 0, 3 * 8, st));   // C_REC_LEN, C_LOW_ONLY, C_DISTINCT
+                    CK(cudaMemsetAsync(counters + C_SUB_OVF, 0, 8, st));
+                    clk.begin(9);
+                    CK(launch_subpart_count(keys, d_br, n_items, d_sc, sub_count, st));
+                    CK(launch_scan_u32(sub_count, sub_off, n_sub, sub_tmp, st));
+                    if (n_sub)
+                        CK(cudaMemcpyAsync(sub_cur, sub_off, (size_t)n_sub * 8, cudaMemcpyDeviceToDevice, st));
+                    CK(launch_subpart_scatter(keys, d_br, n_items, sub_next, d_sc, sub_cur, list, ocap, st));
+                    clk.end();
+                    clk.begin(10);
+                    CK(launch_count_subs(list, sub_off, sub_count, d_sb, n_sub, d_sc, sub_next, count_max,
+                                         P.min_count, P.max_count, rk, rc, rcap, hist_sub, ovf, ovf_cap, counters,
+                                         bucket_ovf, st));
+                    clk.end();
+                    const Counters cs = read_counters(counters, st);
+                    check_flags(cs.v[C_FLAGS], "sub-bucket count");
+                    if (cs.v[C_SUB_OVF] == 0) {
+                        std::vector<unsigned long long> hs(HIST_BINS);
+                        CK(cudaMemcpyAsync(hs.data(), hist_sub, HIST_BINS * 8, cudaMemcpyDeviceToHost, st));
+                        CK(cudaStreamSynchronize(st));
+                        for (size_t i = 0; i < HIST_BINS; ++i) hist_add[i] += hs[i];
+                        rec_keys = rk;
+                        rec_counts = rc;
+                        n_rec = cs.v[C_REC_LEN];
+                        rec_by_bucket = false;
+                        job.distinct += cs.v[C_DISTINCT] + cs.v[C_LOW_ONLY];
+                        job.low_only += cs.v[C_LOW_ONLY];
+                        low_len += cs.v[C_LOW_LEN];
+                        high_len += cs.v[C_HIGH_LEN];
+                        table_cap = std::max<uint64_t>(table_cap, (uint64_t)n_sub * SUB_TABLE_SLOTS);
+                        ++job.smem_passes;
+                        sub_done = true;
+                        break;
+                    }
+                    // buckets that held more distinct repeated k-mers than their
+                    // sub-buckets' tables: twice the sub-buckets next time
+                    std::vector<uint32_t> bo(N_BUCKETS);
+                    CK(cudaMemcpyAsync(bo.data(), bucket_ovf, N_BUCKETS * 4, cudaMemcpyDeviceToHost, st));
+                    unsigned long long ovf_len = before.v[C_OVF_LEN];
+                    CK(cudaMemcpyAsync(counters + C_OVF_LEN, &ovf_len, 8, cudaMemcpyHostToDevice, st));
+                    CK(cudaStreamSynchronize(st));
+                    ds.rewind(m0);
+                    bool any = false;
+                    for (uint32_t b = lo; b < hi; ++b) {
+                        if (!bo[b]) continue;
+                        any = true;
+                        if ((uint64_t)nsub[b] * 2 > std::min<uint64_t>(fcap[b], SUB_MAX_PER_BUCKET)) eligible = false;
+                        else nsub[b] *= 2;
+                    }
+                    if (!any) eligible = false;
+                    if (!eligible) ++job.smem_fallbacks;
+                }
             }
-            table_cap = std::max(table_cap, cap);
-            // a single pass's records can go straight into the sort's buffers
-            // when the sort (first digit skipped) runs an odd number of passes
-            compact_table(tr, cap, pass_low, list, d_lr, n_low_items, merge_next, d_cfg, true,
-                          !multi && sort_passes_run(2 * k, 8) % 2 == 1);
+            if (!sub_done) {
+                std::vector<unsigned long long> lh(2 * N_BUCKETS, 0);
+                std::vector<uint32_t> hh;
+                if (P.bloom) {
+                    CK(cudaMemsetAsync(bits, 0, words * 8, st));
+                    clk.begin(8);
+                    BucketRanges br{};
+                    for (uint32_t b = lo; b < hi; ++b) {
+                        br.begin[b] = cfg[b].key_base;
+                        br.len[b] = cfg[b].key_len;
+                    }
+                    uint32_t n_items = 0;
+                    BucketRanges *d_br = upload_ranges(br, n_items);
+                    CK(launch_bloom_buckets(keys, d_br, n_items, next_item, d_cfg_b, bits, list, lh_cnt, lh_cnt + N_BUCKETS,
+                                            hll_high, st));
+                    clk.end();
+                    hh.resize((size_t)N_BUCKETS * BUCKET_HLL_M);
+                    CK(cudaMemcpyAsync(lh.data(), lh_cnt, 2 * N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
+                    CK(cudaMemcpyAsync(hh.data(), hll_high, hh.size() * 4, cudaMemcpyDeviceToHost, st));
+                    ds.release(d_br);
+                } else {
+                    // every occurrence goes to the table: the whole bucket is "high"
+                    for (uint32_t b = lo; b < hi; ++b) lh[N_BUCKETS + b] = cfg[b].key_len;
+                }
+                Counters c = read_counters(counters, st);
+                check_flags(c.v[C_FLAGS], "partition");
+                ds.release(next_item);
+                ds.release(hll_high);
+                ds.release(lh_cnt);
+                ds.release(bbase);
+                ds.release(cursor);
+                ds.release(d_cfg_b);
+                if (P.bloom) {
+                    ds.release(keys);
+                    ds.release(bits);
+                }
+                uint64_t pass_low = 0;
+                std::vector<uint64_t> bcaps(N_BUCKETS, 0);
+                for (uint32_t b = lo; b < hi; ++b) {
+                    const unsigned long long hb = lh[N_BUCKETS + b];
+                    pass_low += lh[b];
+                    high_len += hb;
+                    double e;
+                    if (P.bloom) {
+                        // the registers hold a hash sample of the non-FIRST k-mers
+                        e = hb ? (double)(1u << BUCKET_HLL_SAMPLE_BITS) *
+                                     hll_estimate(&hh[(size_t)b * BUCKET_HLL_M], BUCKET_HLL_M)
+                               : 0.0;
+                    } else {
+                        // the job's distinct estimate, shared out by occurrences
+                        e = O ? est * (double)hb / (double)O : 0.0;
+                        e = std::min(e, (double)hb);
+                    }
+                    e = std::max(e, (double)std::min<unsigned long long>(hb, 4096));
+                    bcaps[b] = table_capacity_for(e, tn.bucket_table_factor);
+                }
+                low_len += pass_low;
+                // per-bucket sub-tables in one arena; a bucket whose table
+                // overflows gets twice the slots and the insert is repeated
+                BucketCfg *d_cfg = ds.n<BucketCfg>(N_BUCKETS);
+                unsigned long long *bucket_ovf = ds.n<unsigned long long>(N_BUCKETS);
+                next_item = ds.n<unsigned int>(1);
+                unsigned int *merge_next = ds.n<unsigned int>(1);
+                BucketRanges hr{}, lr{};
+                for (uint32_t b = lo; b < hi; ++b) {
+                    hr.begin[b] = cfg[b].key_base + cfg[b].key_len - lh[N_BUCKETS + b];
+                    hr.len[b] = lh[N_BUCKETS + b];
+                    lr.begin[b] = cfg[b].key_base;
+                    lr.len[b] = lh[b];
+                }
+                uint32_t n_high_items = 0, n_low_items = 0;
+                BucketRanges *d_hr = upload_ranges(hr, n_high_items);
+                BucketRanges *d_lr = upload_ranges(lr, n_low_items);
+                TableRef tr{};
+                uint64_t cap = 0;
+                for (int attempt = 0;; ++attempt) {
+                    // sub-tables in the order of the sort key's lowest byte: bucket
+                    // b (the internal word's top byte, four bases) is that byte with
+                    // its 2-bit groups reversed, so the slot-order records come out
+                    // in order of the first sort digit
+                    cap = 0;
+                    for (uint32_t r = 0; r < N_BUCKETS; ++r) {
+                        const uint32_t b = ((r & 3u) << 6) | (((r >> 2) & 3u) << 4) | (((r >> 4) & 3u) << 2) | (r >> 6);
+                        cfg[b].slot_base = cap;
+                        cfg[b].slot_cap = bcaps[b];
+                        cap += bcaps[b];
+                    }
+                    if (tr.slots) ds.release(tr.slots);
+                    tr.slots = static_cast<Slot *>(ds.get(std::max<uint64_t>(cap, 1) * sizeof(Slot)));
+                    tr.mask = 0;   // the arena is addressed per bucket
+                    CK(launch_init_slots(tr.slots, cap, st));
+                    CK(cudaMemcpyAsync(d_cfg, cfg.data(), N_BUCKETS * sizeof(BucketCfg), cudaMemcpyHostToDevice, st));
+                    CK(cudaMemsetAsync(bucket_ovf, 0, N_BUCKETS * 8, st));
+                    clk.begin(3);
+                    CK(launch_insert_buckets(list, d_hr, n_high_items, next_item, d_cfg, tr.slots, max_probe_cap, bucket_ovf,
+                                             st));
+                    clk.end();
+                    std::vector<unsigned long long> ov(N_BUCKETS);
+                    CK(cudaMemcpyAsync(ov.data(), bucket_ovf, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
+                    Counters cc = read_counters(counters, st);
+                    check_flags(cc.v[C_FLAGS], "insert");
+                    bool any = false;
+                    for (uint32_t b = 0; b < N_BUCKETS; ++b)
+                        if (ov[b]) {
+                            bcaps[b] *= 2;
+                            any = true;
+                        }
+                    if (!any) break;
+                    if (attempt >= 3) throw KcError{KC_ERR_DEVICE, "counting table overflow"};
+                }
+                table_cap = std::max(table_cap, cap);
+                // a single pass's records can go straight into the sort's buffers
+                // when the sort (first digit skipped) runs an odd number of passes
+                compact_table(tr, cap, pass_low, list, d_lr, n_low_items, merge_next, d_cfg, true,
+                              !multi && sort_passes_run(2 * k, 8) % 2 == 1);
+            }
             if (multi) {
                 // this pass's records wait in pinned host memory; its device
                 // memory goes to the next pass
@@ -828,6 +962,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     std::vector<uint32_t> ovf_h(n_ovf);
     if (n_ovf) CK(cudaMemcpyAsync(ovf_h.data(), ovf, n_ovf * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < HIST_BINS; ++i) hd[i] += hist_add[i];
     hd[1] += job.low_only;   // FIRST-only k-mers have count 1 (count_max >= 1)
     {
         uint32_t lo = P.hist_min, hi = P.hist_max;
@@ -1470,10 +1605,12 @@ int kc_set_tuning(kc_handle *h, const kc_tuning *t)
     if (t->bucket_table_factor > 0 && t->bucket_table_factor < 1.05)
         return fail(KC_ERR_INVALID, "bucket_table_factor must be at least 1.05");
     if (t->table_factor > 0 && t->table_factor < 1.05) return fail(KC_ERR_INVALID, "table_factor must be at least 1.05");
+    if (t->bloom_smem > 2) return fail(KC_ERR_INVALID, "bloom_smem must be 1 or 2");
     std::lock_guard<std::mutex> lk(h->mu);
     if (t->bucket_table_factor > 0) h->tuning.bucket_table_factor = t->bucket_table_factor;
     if (t->table_factor > 0) h->tuning.table_factor = t->table_factor;
     if (t->sort_group_records > 0) h->tuning.sort_group_records = t->sort_group_records;
+    if (t->bloom_smem > 0) h->tuning.bloom_smem = t->bloom_smem;
     return KC_OK;
 }
 
@@ -1511,13 +1648,14 @@ int kc_autotune(kc_handle *h, const kc_job *jobs, uint32_t n_jobs, uint32_t batc
     int rc = run(cur, cur_ms);   // warm-up: workspaces and pinned blocks reach this shape
     if (rc == KC_OK) rc = run(cur, cur_ms);
     const double bucket_c[] = {2.0, 3.0, 4.0}, table_c[] = {1.3, 1.6, 2.2};
-    const uint64_t group_c[] = {2ull << 20, 4ull << 20, 8ull << 20};
-    for (int param = 0; param < 3 && rc == KC_OK; ++param)
+    const uint64_t group_c[] = {2ull << 20, 4ull << 20, 8ull << 20}, smem_c[] = {1, 2, 1};
+    for (int param = 0; param < 4 && rc == KC_OK; ++param)
         for (int c = 0; c < 3 && rc == KC_OK; ++c) {
             kc_tuning t = cur;
             if (param == 0) t.bucket_table_factor = bucket_c[c];
             if (param == 1) t.table_factor = table_c[c];
             if (param == 2) t.sort_group_records = group_c[c];
+            if (param == 3) t.bloom_smem = smem_c[c];
             if (std::memcmp(&t, &cur, sizeof(t)) == 0) continue;
             rc = run(t, ms);
             if (rc == KC_OK && ms < 0.98 * cur_ms) {   // a clear gain only
@@ -1589,6 +1727,8 @@ int kc_result(kc_handle *h, kc_job_id id, kc_result_t *out)
     out->input_bytes = j.input_bytes;
     out->n_records_total = j.n_records_total;
     out->passes = j.passes;
+    out->smem_passes = (uint16_t)std::min<uint32_t>(j.smem_passes, 0xFFFF);
+    out->smem_fallbacks = (uint16_t)std::min<uint32_t>(j.smem_fallbacks, 0xFFFF);
     return KC_OK;
 }
 

@@ -1808,6 +1808,358 @@ __global__ void __launch_bounds__(256) k_merge_buckets(const unsigned long long 
     }
 }
 
+// ---------------------------------------------------------------------------
+// shared-memory sub-bucket path of the Bloom split
+// ---------------------------------------------------------------------------
+
+// Sub-bucket of a k-mer inside its bucket: its filter block (the reference's
+// block = XXH3-128.low64 & (cap - 1), src/BloomFilter.h:215-222) divided by
+// the slice size.
+__device__ __forceinline__ uint32_t sub_of(unsigned long long key, const SubCfg &c)
+{
+    uint64_t lo, hi;
+    xxh3_128_8(key, lo, hi);
+    return (uint32_t)((lo & (c.fcap - 1)) >> c.slice_shift);
+}
+
+// Each block counts a contiguous run of work items (bucket-major, so a block
+// meets one or two buckets) in a shared histogram, flushed per bucket.
+__global__ void __launch_bounds__(256) k_subpart_count(const unsigned long long *keys, const BucketRanges *rg,
+                                                       uint32_t n_items, const SubCfg *sc, uint32_t *sub_count)
+{
+    __shared__ uint32_t s_item0[N_BUCKETS + 1];
+    __shared__ uint32_t s_h[SUB_MAX_PER_BUCKET];
+    const int tid = threadIdx.x;
+    for (uint32_t i = tid; i < SUB_MAX_PER_BUCKET; i += 256) s_h[i] = 0;
+    load_item_starts(rg, s_item0);
+    const uint32_t per = (n_items + gridDim.x - 1) / gridDim.x;
+    const uint32_t it0 = blockIdx.x * per, it1 = min(n_items, it0 + per);
+    uint32_t cur = N_BUCKETS;
+    SubCfg c{};
+    for (uint32_t it = it0; it < it1; ++it) {
+        const WorkItem w = work_item(rg, s_item0, it);
+        if (w.bucket != cur) {
+            if (cur != N_BUCKETS) {
+                __syncthreads();
+                for (uint32_t i = tid; i < c.n_sub; i += 256)
+                    if (s_h[i]) {
+                        atomicAdd(&sub_count[c.sub_base + i], s_h[i]);
+                        s_h[i] = 0;
+                    }
+                __syncthreads();
+            }
+            cur = w.bucket;
+            c = sc[cur];
+        }
+        for (unsigned long long i = w.begin + tid; i < w.end; i += 256)
+            atomicAdd(&s_h[sub_of(__ldcs(&keys[i]), c)], 1u);
+    }
+    __syncthreads();
+    if (cur != N_BUCKETS)
+        for (uint32_t i = tid; i < c.n_sub; i += 256)
+            if (s_h[i]) atomicAdd(&sub_count[c.sub_base + i], s_h[i]);
+}
+
+// One work item (WORK_ITEM_KEYS keys of one bucket) per round: the keys are
+// ranked by sub-bucket in shared memory, every sub-bucket of the item takes
+// its range with one cursor update, and the item's keys are written
+// reordered by sub-bucket (consecutive threads store consecutive addresses).
+constexpr uint32_t SP_PER_THREAD = WORK_ITEM_KEYS / 256;
+
+__global__ void __launch_bounds__(256) k_subpart_scatter(const unsigned long long *keys, const BucketRanges *rg,
+                                                         uint32_t n_items, unsigned int *next_item,
+                                                         const SubCfg *sc, unsigned long long *sub_cursor,
+                                                         unsigned long long *out, uint64_t out_cap)
+{
+    extern __shared__ __align__(16) uint8_t sp_smem[];
+    unsigned long long *s_sorted = reinterpret_cast<unsigned long long *>(sp_smem);          // WORK_ITEM_KEYS
+    unsigned long long *s_dst = s_sorted + WORK_ITEM_KEYS;                                    // SUB_MAX_PER_BUCKET
+    uint32_t *s_cnt = reinterpret_cast<uint32_t *>(s_dst + SUB_MAX_PER_BUCKET);               // SUB_MAX_PER_BUCKET
+    uint32_t *s_start = s_cnt + SUB_MAX_PER_BUCKET;                                           // SUB_MAX_PER_BUCKET
+    uint16_t *s_sub = reinterpret_cast<uint16_t *>(s_start + SUB_MAX_PER_BUCKET);             // WORK_ITEM_KEYS
+    __shared__ uint32_t s_item0[N_BUCKETS + 1];
+    __shared__ uint32_t s_item, s_warp[8];
+    const int tid = threadIdx.x;
+    for (uint32_t i = tid; i < SUB_MAX_PER_BUCKET; i += 256) s_cnt[i] = 0;
+    load_item_starts(rg, s_item0);
+    uint32_t it;
+    while (next_work(next_item, n_items, &s_item, it)) {
+        const WorkItem w = work_item(rg, s_item0, it);
+        const SubCfg c = sc[w.bucket];
+        const uint32_t n = (uint32_t)(w.end - w.begin);
+        unsigned long long k[SP_PER_THREAD];
+        uint32_t sr[SP_PER_THREAD];   // rank << 16 | sub (sub 0xFFFF: no key)
+#pragma unroll
+        for (uint32_t r = 0; r < SP_PER_THREAD; ++r) {
+            const uint32_t i = r * 256 + tid;
+            sr[r] = 0xFFFFu;
+            if (i < n) {
+                k[r] = __ldcs(&keys[w.begin + i]);
+                const uint32_t sub = sub_of(k[r], c);
+                sr[r] = (atomicAdd(&s_cnt[sub], 1u) << 16) | sub;
+            }
+        }
+        __syncthreads();
+        // exclusive scan of the n_sub counts, up to 8 per thread
+        const uint32_t per = (c.n_sub + 255) / 256, b0 = tid * per;
+        uint32_t local = 0;
+        for (uint32_t j = 0; j < per; ++j)
+            if (b0 + j < c.n_sub) local += s_cnt[b0 + j];
+        uint32_t tot;
+        uint32_t run = block_excl_scan(local, s_warp, tot);
+        for (uint32_t j = 0; j < per; ++j) {
+            const uint32_t s = b0 + j;
+            if (s < c.n_sub) {
+                const uint32_t cnt = s_cnt[s];
+                s_start[s] = run;
+                // destination of sorted index i of sub-bucket s: s_dst[s] + i
+                s_dst[s] = cnt ? atomicAdd(&sub_cursor[c.sub_base + s], (unsigned long long)cnt) - run : 0ull;
+                run += cnt;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (uint32_t r = 0; r < SP_PER_THREAD; ++r) {
+            const uint32_t sub = sr[r] & 0xFFFFu;
+            if (sub != 0xFFFFu) {
+                const uint32_t p = s_start[sub] + (sr[r] >> 16);
+                s_sorted[p] = k[r];
+                s_sub[p] = (uint16_t)sub;
+            }
+        }
+        __syncthreads();
+        for (uint32_t i = tid; i < n; i += 256) {
+            const unsigned long long d = s_dst[s_sub[i]] + i;
+            if (d < out_cap) out[d] = s_sorted[i];
+        }
+        for (uint32_t i = tid; i < c.n_sub; i += 256) s_cnt[i] = 0;
+        __syncthreads();
+    }
+}
+
+// Shared-memory counting table of one sub-bucket: linear probing from the
+// key's hash, claims by CAS; a slot only changes from empty to a key.
+constexpr uint32_t SUB_MAX_PROBE = 512;
+
+__device__ __forceinline__ int sub_table_slot(unsigned long long key)
+{
+    return (int)(slot_hash(key) >> (64 - 13));   // SUB_TABLE_SLOTS = 2^13
+}
+
+__device__ __forceinline__ bool sub_table_add(unsigned long long *tk, uint32_t *tc, unsigned long long key)
+{
+    uint32_t i = (uint32_t)sub_table_slot(key);
+    for (uint32_t n = 0; n < SUB_MAX_PROBE; ++n) {
+        const unsigned long long cur = *(volatile unsigned long long *)&tk[i];
+        if (cur == key) {
+            atomicAdd(&tc[i], 1u);
+            return true;
+        }
+        if (cur == EMPTY_KEY) {
+            const unsigned long long prev = atomicCAS(&tk[i], EMPTY_KEY, key);
+            if (prev == EMPTY_KEY || prev == key) {
+                atomicAdd(&tc[i], 1u);
+                return true;
+            }
+        }
+        i = (i + 1) & (SUB_TABLE_SLOTS - 1);
+    }
+    return false;
+}
+
+__device__ __forceinline__ int sub_table_find(const unsigned long long *tk, unsigned long long key)
+{
+    uint32_t i = (uint32_t)sub_table_slot(key);
+    for (uint32_t n = 0; n < SUB_MAX_PROBE; ++n) {
+        const unsigned long long cur = tk[i];
+        if (cur == key) return (int)i;
+        if (cur == EMPTY_KEY) return -1;
+        i = (i + 1) & (SUB_TABLE_SLOTS - 1);
+    }
+    return -1;
+}
+
+constexpr uint32_t SUB_THREADS = 1024;
+constexpr uint32_t SUB_PER_THREAD = 4;
+constexpr uint32_t SUB_TILE = SUB_THREADS * SUB_PER_THREAD;
+
+__device__ __forceinline__ uint32_t block_excl_scan_1024(uint32_t v, uint32_t *s_warp, uint32_t &total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t s = s_warp[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL, s, o);
+            if (lane >= o) s += y;
+        }
+        s_warp[lane] = s;   // inclusive
+    }
+    __syncthreads();
+    total = s_warp[31];
+    const uint32_t base = warp ? s_warp[warp - 1] : 0u;
+    __syncthreads();
+    return base + x - v;
+}
+
+__global__ void __launch_bounds__(SUB_THREADS, 1) k_count_subs(
+    unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count, const uint8_t *sub_bucket,
+    uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub, uint32_t count_max, uint32_t min_count,
+    uint32_t max_count, unsigned long long *rec_keys, uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist,
+    uint32_t *ovf, uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf)
+{
+    extern __shared__ __align__(16) uint8_t cs_smem[];
+    unsigned long long *s_filter = reinterpret_cast<unsigned long long *>(cs_smem);   // 2 * SUB_SLICE_BLOCKS
+    unsigned long long *s_tk = s_filter + 2 * SUB_SLICE_BLOCKS;                       // SUB_TABLE_SLOTS
+    uint32_t *s_tc = reinterpret_cast<uint32_t *>(s_tk + SUB_TABLE_SLOTS);            // SUB_TABLE_SLOTS
+    uint32_t *s_hist = s_tc + SUB_TABLE_SLOTS;                                        // 2048
+    __shared__ uint32_t s_warp[32], s_sub;
+    __shared__ unsigned long long s_base;
+    const int tid = threadIdx.x;
+    for (uint32_t i = tid; i < 2048; i += SUB_THREADS) s_hist[i] = 0;
+    unsigned long long n_high = 0, n_low = 0, n_low_only = 0, n_distinct = 0;
+    uint32_t n_ovf_subs = 0;
+    bool rec_full = false;
+    for (;;) {
+        if (tid == 0) s_sub = atomicAdd(next_sub, 1u);
+        __syncthreads();
+        const uint32_t sub = s_sub;
+        __syncthreads();
+        if (sub >= n_sub) break;
+        const uint32_t n = sub_count[sub];
+        if (n == 0) continue;
+        const unsigned long long base = sub_off[sub];
+        const uint32_t bucket = sub_bucket[sub];
+        const unsigned long long fcap = sc[bucket].fcap;
+        const uint32_t slice = 1u << sc[bucket].slice_shift;
+        for (uint32_t i = tid; i < 2 * slice; i += SUB_THREADS) s_filter[i] = 0;
+        for (uint32_t i = tid; i < SUB_TABLE_SLOTS; i += SUB_THREADS) {
+            s_tk[i] = EMPTY_KEY;
+            s_tc[i] = 0;
+        }
+        __syncthreads();
+        // 1. the reference's two-level Bloom classification (src/BloomFilter.h:233-273)
+        // on the slice; non-FIRST occurrences counted in the table, FIRST ones
+        // written back over the front of the sub-bucket's keys
+        bool full = false;
+        uint32_t lo_cnt = 0;   // the same in every thread
+        for (uint32_t t0 = 0; t0 < n; t0 += SUB_TILE) {
+            unsigned long long k[SUB_PER_THREAD];
+            uint32_t firsts = 0;
+#pragma unroll
+            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
+                const uint32_t i = t0 + r * SUB_THREADS + tid;
+                k[r] = i < n ? __ldcs(&keys[base + i]) : EMPTY_KEY;
+            }
+#pragma unroll
+            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
+                if (t0 + r * SUB_THREADS + tid >= n) continue;
+                uint64_t block, m, hi;
+                bloom_probe_hi(k[r], fcap, block, m, hi);
+                unsigned long long *cell = s_filter + 2 * (block & (slice - 1));
+                bool first = false;
+                const unsigned long long bf1 = *(volatile unsigned long long *)&cell[0];
+                if ((bf1 & m) != m) {
+                    const unsigned long long bf2 = *(volatile unsigned long long *)&cell[1];
+                    if ((bf2 & m) == m) {
+                        atomicOr(&cell[0], (unsigned long long)m);
+                    } else {
+                        const unsigned long long old2 = atomicOr(&cell[1], (unsigned long long)m);
+                        if ((old2 & m) == m) atomicOr(&cell[0], (unsigned long long)m);
+                        else first = true;
+                    }
+                }
+                if (first) {
+                    firsts |= 1u << r;
+                } else {
+                    ++n_high;
+                    if (!sub_table_add(s_tk, s_tc, k[r])) full = true;
+                }
+            }
+            uint32_t tf;
+            const uint32_t of = block_excl_scan_1024((uint32_t)__popc(firsts), s_warp, tf);
+            // every key of this tile is in registers (the scan synchronised the
+            // block), so the FIRST ones may overwrite its front
+            unsigned long long p = base + lo_cnt + of;
+#pragma unroll
+            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r)
+                if ((firsts >> r) & 1u) keys[p++] = k[r];
+            lo_cnt += tf;
+            n_low += (uint64_t)__popc(firsts);
+        }
+        if (__syncthreads_or(full)) {
+            if (tid == 0) {
+                ++n_ovf_subs;
+                atomicOr(&bucket_ovf[bucket], 1u);
+            }
+            continue;   // incomplete: the host counts the pass again with more sub-buckets
+        }
+        // 2. FIRST occurrences: a hit adds one to the table count, a miss is a
+        // k-mer seen once (counted, not a record: min_count >= 2)
+        for (uint32_t i = tid; i < lo_cnt; i += SUB_THREADS) {
+            const unsigned long long key = __ldcg(&keys[base + i]);
+            const int sl = sub_table_find(s_tk, key);
+            if (sl >= 0) atomicAdd(&s_tc[sl], 1u);
+            else ++n_low_only;
+        }
+        __syncthreads();
+        // 3. the table's records and histogram
+        uint32_t keep = 0;
+        for (uint32_t i = tid; i < SUB_TABLE_SLOTS; i += SUB_THREADS) {
+            if (s_tk[i] == EMPTY_KEY) continue;
+            ++n_distinct;
+            const uint32_t c = s_tc[i] < count_max ? s_tc[i] : count_max;
+            if (c < 2048) atomicAdd(&s_hist[c], 1u);
+            else if (c < HIST_BINS) atomicAdd(&hist[c], 1ull);
+            else {
+                const unsigned long long q = atomicAdd(&counters[C_OVF_LEN], 1ull);
+                if (q < ovf_cap) ovf[q] = c;
+                else atomicOr(&counters[C_FLAGS], ERR_HIST_OVERFLOW_FULL);
+            }
+            keep += (c >= min_count && c <= max_count) ? 1u : 0u;
+        }
+        uint32_t tk;
+        const uint32_t ok = block_excl_scan_1024(keep, s_warp, tk);
+        if (tid == 0) s_base = tk ? atomicAdd(&counters[C_REC_LEN], (unsigned long long)tk) : 0ull;
+        __syncthreads();
+        unsigned long long q = s_base + ok;
+        for (uint32_t i = tid; i < SUB_TABLE_SLOTS; i += SUB_THREADS) {
+            if (s_tk[i] == EMPTY_KEY) continue;
+            const uint32_t c = s_tc[i] < count_max ? s_tc[i] : count_max;
+            if (c < min_count || c > max_count) continue;
+            if (q < rec_cap) {
+                rec_keys[q] = pair_reverse(s_tk[i]);
+                rec_counts[q] = c;
+            } else {
+                rec_full = true;
+            }
+            ++q;
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    for (uint32_t i = tid; i < 2048; i += SUB_THREADS)
+        if (s_hist[i]) atomicAdd(&hist[i], (unsigned long long)s_hist[i]);
+    if (rec_full) atomicOr(&counters[C_FLAGS], ERR_RECORDS_FULL);
+    const unsigned long long v[4] = {n_high, n_low, n_low_only, n_distinct};
+    const int idx[4] = {C_HIGH_LEN, C_LOW_LEN, C_LOW_ONLY, C_DISTINCT};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        unsigned long long x = v[j];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(FULL, x, o);
+        if ((tid & 31) == 0 && x) atomicAdd(&counters[idx[j]], x);
+    }
+    if (tid == 0 && n_ovf_subs) atomicAdd(&counters[C_SUB_OVF], (unsigned long long)n_ovf_subs);
+}
+
 __global__ void k_hash_batch(const unsigned long long *keys, uint64_t n, unsigned long long *out)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -2403,6 +2755,65 @@ cudaError_t launch_merge_buckets(const unsigned long long *keys, const BucketRan
     k_merge_buckets<<<std::min<int>(persistent_grid(k_merge_buckets), n_items), 256, 0, st>>>(
         keys, rg, n_items, next_item, cfg, arena, max_probe, min_count, max_count, rec_keys, rec_counts, rec_cap,
         counters);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_subpart_count(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
+                                 const SubCfg *sc, uint32_t *sub_count, cudaStream_t st)
+{
+    if (!n_items) return cudaSuccess;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_subpart_count, 256, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const uint32_t grid = std::min<uint32_t>(n_items, (uint32_t)(sm_count() * per_sm));
+    note_launch();
+    k_subpart_count<<<grid, 256, 0, st>>>(keys, rg, n_items, sc, sub_count);
+    return cudaGetLastError();
+}
+
+static size_t subpart_scatter_smem()
+{
+    return (size_t)WORK_ITEM_KEYS * 8 + (size_t)SUB_MAX_PER_BUCKET * (8 + 4 + 4) + (size_t)WORK_ITEM_KEYS * 2;
+}
+
+cudaError_t launch_subpart_scatter(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
+                                   unsigned int *next_item, const SubCfg *sc, unsigned long long *sub_cursor,
+                                   unsigned long long *out, uint64_t out_cap, cudaStream_t st)
+{
+    if (!n_items) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(next_item, 0, 4, st);
+    if (e != cudaSuccess) return e;
+    const size_t smem = subpart_scatter_smem();
+    e = cudaFuncSetAttribute(k_subpart_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_subpart_scatter, 256, smem) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    const uint32_t grid = std::min<uint32_t>(n_items, (uint32_t)(sm_count() * per_sm));
+    note_launch();
+    k_subpart_scatter<<<grid, 256, smem, st>>>(keys, rg, n_items, next_item, sc, sub_cursor, out, out_cap);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_count_subs(unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count,
+                              const uint8_t *sub_bucket, uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub,
+                              uint32_t count_max, uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
+                              uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist, uint32_t *ovf,
+                              uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, cudaStream_t st)
+{
+    if (!n_sub) return cudaSuccess;
+    if (min_count < 2) return cudaErrorInvalidValue;   // singletons are not records on this path
+    cudaError_t e = cudaMemsetAsync(next_sub, 0, 4, st);
+    if (e != cudaSuccess) return e;
+    const size_t smem = (size_t)2 * SUB_SLICE_BLOCKS * 8 + (size_t)SUB_TABLE_SLOTS * (8 + 4) + 2048 * 4;
+    e = cudaFuncSetAttribute(k_count_subs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const uint32_t grid = std::min<uint32_t>(n_sub, (uint32_t)sm_count());
+    note_launch();
+    k_count_subs<<<grid, SUB_THREADS, smem, st>>>(keys, sub_off, sub_count, sub_bucket, n_sub, sc, next_sub, count_max,
+                                                  min_count, max_count, rec_keys, rec_counts, rec_cap, hist, ovf,
+                                                  ovf_cap, counters, bucket_ovf);
     return cudaGetLastError();
 }
 

@@ -39,6 +39,7 @@ enum Counter : int {
     C_OVF_LEN = 7,       // histogram counts >= HIST_BINS
     C_SEL_A = 8,         // query selections
     C_SEL_B = 9,
+    C_SUB_OVF = 10,      // sub-buckets whose shared-memory table overflowed
     C_COUNT = 16
 };
 
@@ -145,6 +146,20 @@ struct BucketRanges {
 };
 uint32_t fill_item_starts(BucketRanges &r);   // sets item0 from len, returns the number of items
 
+// Shared-memory sub-bucket path of the Bloom split: every bucket is cut
+// into n_sub sub-buckets of 2^slice_shift consecutive blocks of its filter (a
+// k-mer's sub-bucket follows from its filter block), so one thread block
+// holds a sub-bucket's filter slice and counting table in shared memory.
+constexpr uint32_t SUB_SLICE_BLOCKS = 4096;     // largest slice (2 words a block): 64 KiB of filter
+constexpr uint32_t SUB_TABLE_SLOTS = 8192;      // counting-table slots of a sub-bucket
+constexpr uint32_t SUB_MAX_PER_BUCKET = 2048;   // sub-buckets of one bucket
+struct SubCfg {
+    unsigned long long fcap;    // the bucket's filter blocks (a power of two)
+    uint32_t sub_base, n_sub;   // its sub-buckets [sub_base, sub_base + n_sub), n_sub = fcap >> slice_shift
+    uint32_t slice_shift;       // log2 of the blocks of one slice, <= log2(SUB_SLICE_BLOCKS)
+    uint32_t pad;
+};
+
 // Per-bucket state of the partitioned pipeline.
 struct BucketCfg {
     unsigned long long key_base, key_len;    // bucket's range in the partitioned key array
@@ -245,6 +260,28 @@ cudaError_t launch_select_range(const unsigned long long *keys, const uint32_t *
                                 unsigned long long *counters, int counter_idx, cudaStream_t st);
 
 // Bucket-major kernels of the partitioned pipeline; each resets *next_item.
+// Sub-bucket path.  count: sub_count[sub_base + s] += the keys of bucket b
+// in sub-bucket s.  scatter: every key to out[sub_cursor[its sub-bucket]++]
+// (sub_cursor starts at the exclusive scan of sub_count).  count_subs: one
+// block per sub-bucket at a time runs the Bloom split with the filter slice in
+// shared memory, counts the non-FIRST occurrences in a shared-memory table,
+// merges the FIRST ones (written back over the front of the sub-bucket's
+// keys) and appends the table's records (counts saturated at count_max, kept
+// when min_count <= count <= max_count) at rec_keys[C_REC_LEN...]; every
+// table count goes to hist/ovf, the totals to counters (C_REC_LEN,
+// C_LOW_LEN, C_HIGH_LEN, C_LOW_ONLY, C_DISTINCT) and the sub-buckets whose
+// table overflowed to C_SUB_OVF and bucket_ovf[their bucket] (the results
+// are then incomplete).
+cudaError_t launch_subpart_count(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
+                                 const SubCfg *sc, uint32_t *sub_count, cudaStream_t st);
+cudaError_t launch_subpart_scatter(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
+                                   unsigned int *next_item, const SubCfg *sc, unsigned long long *sub_cursor,
+                                   unsigned long long *out, uint64_t out_cap, cudaStream_t st);
+cudaError_t launch_count_subs(unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count,
+                              const uint8_t *sub_bucket, uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub,
+                              uint32_t count_max, uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
+                              uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist, uint32_t *ovf,
+                              uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, cudaStream_t st);
 cudaError_t launch_bloom_buckets(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                  unsigned int *next_item, const BucketCfg *cfg, unsigned long long *bits,
                                  unsigned long long *out, unsigned long long *low_cnt, unsigned long long *high_cnt,

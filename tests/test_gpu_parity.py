@@ -456,3 +456,48 @@ def test_cli_round_trip():
         subprocess.run([os.path.join(bin_dir, "dump_tool"), "precise", d, "8", "1", o, "1", str(U32), "--sort"],
                        check=True, capture_output=True)
         assert hashlib.sha256(open(o, "rb").read()).hexdigest() == case["dump_sha256"]
+
+
+def test_bloom_shared_memory_path_matches_global_path(kc):
+    """Bloom jobs with min count >= 2 count each filter sub-bucket in shared
+    memory; the global-memory path (bloom_smem=2) and the oracle give the same
+    records, histogram, queries and totals, with saturated counts too."""
+    import ktcountermemorygreedy_b200.synth as S
+    g = S.genome(81, 1_500_000)
+    fq = S.reads(g, 81, 40_000, (100, 150), 0.01, 0.0).tobytes()
+    files = [fq, fixtures.random_fastq(82, 500, (80, 150), genome_len=3000)]
+    with kc.KmerCounter(max_inflight_jobs=2) as c:
+        for k, cm, mc in ((31, U32, 2), (21, 255, 3), (25, 9, 2)):
+            kw = dict(k=k, count_max=cm, bloom=True, memory_gb=1, min_count=mc, hist_min=1, hist_max=3000,
+                      top_n=100, want_le2=1)
+            c.set_tuning(bloom_smem=1)
+            a = c.count(files, **kw)
+            c.set_tuning(bloom_smem=2)
+            b = c.count(files, **kw)
+            assert a.smem_passes == a.passes == 1 and a.smem_fallbacks == 0
+            assert b.smem_passes == 0
+            for f in ("keys", "counts", "hist", "top_keys", "top_counts", "le2_keys", "le2_counts"):
+                assert np.array_equal(getattr(a, f), getattr(b, f)), (k, f)
+            # low_only (singletons the filter let through as FIRST) depends on
+            # the order the occurrences meet the filter, as in the reference;
+            # the count-1 histogram bin, which adds both kinds, is exact
+            assert (a.occurrences, a.distinct) == (b.occurrences, b.distinct)
+            assert a.low_len + a.high_len == a.occurrences
+            want_k, want_c = O.exact_records(files, k, cm, min_count=mc)
+            assert np.array_equal(a.keys, want_k) and np.array_equal(a.counts, want_c)
+        c.set_tuning(bloom_smem=1)
+
+
+def test_bloom_shared_memory_tables_overflow_and_split(counter):
+    """Every read twice: half the k-mers of a bucket are distinct repeated
+    ones, more than one sub-bucket table holds, so the overflowing buckets are
+    cut into more sub-buckets and counted again -- still exact."""
+    import ktcountermemorygreedy_b200.synth as S
+    g = S.genome(83, 4_000_000)
+    once = S.reads(g, 83, 20_000, (150, 150), 0.0, 0.0).tobytes()
+    files = [once, once]
+    want_k, want_c = O.exact_records(files, 31, U32, min_count=2)
+    r = counter.count(files, k=31, count_max=U32, bloom=True, memory_gb=1, min_count=2)
+    assert r.smem_passes == 1 and r.smem_fallbacks == 0
+    assert np.array_equal(r.keys, want_k) and np.array_equal(r.counts, want_c)
+    assert r.distinct == len(O.exact_records(files, 31, U32)[0])
