@@ -739,7 +739,8 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                     CK(launch_scan_u32(sub_count, sub_off, n_sub, sub_tmp, st));
                     if (n_sub)
                         CK(cudaMemcpyAsync(sub_cur, sub_off, (size_t)n_sub * 8, cudaMemcpyDeviceToDevice, st));
-                    CK(launch_subpart_scatter(keys, d_br, n_items, sub_next, d_sc, sub_cur, list, ocap, st));
+                    const uint32_t max_sub = *std::max_element(nsub.begin(), nsub.end());
+                    CK(launch_subpart_scatter(keys, d_br, n_items, sub_next, d_sc, sub_cur, list, ocap, max_sub, st));
                     clk.end();
                     clk.begin(10);
                     CK(launch_count_subs(list, sub_off, sub_count, d_sb, n_sub, d_sc, sub_next, count_max,

@@ -1869,18 +1869,20 @@ constexpr uint32_t SP_PER_THREAD = WORK_ITEM_KEYS / 256;
 __global__ void __launch_bounds__(256) k_subpart_scatter(const unsigned long long *keys, const BucketRanges *rg,
                                                          uint32_t n_items, unsigned int *next_item,
                                                          const SubCfg *sc, unsigned long long *sub_cursor,
-                                                         unsigned long long *out, uint64_t out_cap)
+                                                         unsigned long long *out, uint64_t out_cap, uint32_t max_sub)
 {
+    // shared arrays per sub-bucket hold max_sub entries (the most of any
+    // bucket of the launch)
     extern __shared__ __align__(16) uint8_t sp_smem[];
     unsigned long long *s_sorted = reinterpret_cast<unsigned long long *>(sp_smem);          // WORK_ITEM_KEYS
-    unsigned long long *s_dst = s_sorted + WORK_ITEM_KEYS;                                    // SUB_MAX_PER_BUCKET
-    uint32_t *s_cnt = reinterpret_cast<uint32_t *>(s_dst + SUB_MAX_PER_BUCKET);               // SUB_MAX_PER_BUCKET
-    uint32_t *s_start = s_cnt + SUB_MAX_PER_BUCKET;                                           // SUB_MAX_PER_BUCKET
-    uint16_t *s_sub = reinterpret_cast<uint16_t *>(s_start + SUB_MAX_PER_BUCKET);             // WORK_ITEM_KEYS
+    unsigned long long *s_dst = s_sorted + WORK_ITEM_KEYS;                                    // max_sub
+    uint32_t *s_cnt = reinterpret_cast<uint32_t *>(s_dst + max_sub);                          // max_sub
+    uint32_t *s_start = s_cnt + max_sub;                                                      // max_sub
+    uint16_t *s_sub = reinterpret_cast<uint16_t *>(s_start + max_sub);                        // WORK_ITEM_KEYS
     __shared__ uint32_t s_item0[N_BUCKETS + 1];
     __shared__ uint32_t s_item, s_warp[8];
     const int tid = threadIdx.x;
-    for (uint32_t i = tid; i < SUB_MAX_PER_BUCKET; i += 256) s_cnt[i] = 0;
+    for (uint32_t i = tid; i < max_sub; i += 256) s_cnt[i] = 0;
     load_item_starts(rg, s_item0);
     uint32_t it;
     while (next_work(next_item, n_items, &s_item, it)) {
@@ -2021,9 +2023,11 @@ __global__ void __launch_bounds__(SUB_THREADS, 1) k_count_subs(
     unsigned long long *s_tk = s_filter + 2 * SUB_SLICE_BLOCKS;                       // SUB_TABLE_SLOTS
     uint32_t *s_tc = reinterpret_cast<uint32_t *>(s_tk + SUB_TABLE_SLOTS);            // SUB_TABLE_SLOTS
     uint32_t *s_hist = s_tc + SUB_TABLE_SLOTS;                                        // 2048
+    unsigned long long *s_queue = reinterpret_cast<unsigned long long *>(s_hist + 2048);   // SUB_TILE
     __shared__ uint32_t s_warp[32], s_sub;
     __shared__ unsigned long long s_base;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t lt = lanemask_lt();
     for (uint32_t i = tid; i < 2048; i += SUB_THREADS) s_hist[i] = 0;
     unsigned long long n_high = 0, n_low = 0, n_low_only = 0, n_distinct = 0;
     uint32_t n_ovf_subs = 0;
@@ -2053,7 +2057,7 @@ __global__ void __launch_bounds__(SUB_THREADS, 1) k_count_subs(
         uint32_t lo_cnt = 0;   // the same in every thread
         for (uint32_t t0 = 0; t0 < n; t0 += SUB_TILE) {
             unsigned long long k[SUB_PER_THREAD];
-            uint32_t firsts = 0;
+            uint32_t firsts = 0, highs = 0;
 #pragma unroll
             for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
                 const uint32_t i = t0 + r * SUB_THREADS + tid;
@@ -2065,24 +2069,36 @@ __global__ void __launch_bounds__(SUB_THREADS, 1) k_count_subs(
                 uint64_t block, m, hi;
                 bloom_probe_hi(k[r], fcap, block, m, hi);
                 unsigned long long *cell = s_filter + 2 * (block & (slice - 1));
+                // a k-mer seen twice already (most of them) needs no update;
+                // otherwise it is FIRST exactly when the seen-once word lacked
+                // its bits (the seen-twice bits are always a subset of the
+                // seen-once bits, so this is the reference's three-way test,
+                // and setting bits already set changes nothing)
                 bool first = false;
-                const unsigned long long bf1 = *(volatile unsigned long long *)&cell[0];
-                if ((bf1 & m) != m) {
-                    const unsigned long long bf2 = *(volatile unsigned long long *)&cell[1];
-                    if ((bf2 & m) == m) {
-                        atomicOr(&cell[0], (unsigned long long)m);
-                    } else {
-                        const unsigned long long old2 = atomicOr(&cell[1], (unsigned long long)m);
-                        if ((old2 & m) == m) atomicOr(&cell[0], (unsigned long long)m);
-                        else first = true;
-                    }
+                if ((*(volatile unsigned long long *)&cell[0] & m) != m) {
+                    const unsigned long long old2 = atomicOr(&cell[1], (unsigned long long)m);
+                    first = (old2 & m) != m;
+                    if (!first) atomicOr(&cell[0], (unsigned long long)m);
                 }
-                if (first) {
-                    firsts |= 1u << r;
-                } else {
-                    ++n_high;
-                    if (!sub_table_add(s_tk, s_tc, k[r])) full = true;
+                if (first) firsts |= 1u << r;
+                else highs |= 1u << r;
+            }
+            n_high += (uint64_t)__popc(highs);
+            // the warp's non-FIRST k-mers are queued so that every lane inserts
+            {
+                unsigned long long *q = s_queue + warp * (32 * SUB_PER_THREAD);
+                uint32_t qn = 0;
+#pragma unroll
+                for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
+                    const bool h = (highs >> r) & 1u;
+                    const uint32_t b = __ballot_sync(FULL, h);
+                    if (h) q[qn + (uint32_t)__popc(b & lt)] = k[r];
+                    qn += (uint32_t)__popc(b);
                 }
+                __syncwarp();
+                for (uint32_t j = lane; j < qn; j += 32)
+                    if (!sub_table_add(s_tk, s_tc, q[j])) full = true;
+                __syncwarp();
             }
             uint32_t tf;
             const uint32_t of = block_excl_scan_1024((uint32_t)__popc(firsts), s_warp, tf);
@@ -2771,19 +2787,21 @@ cudaError_t launch_subpart_count(const unsigned long long *keys, const BucketRan
     return cudaGetLastError();
 }
 
-static size_t subpart_scatter_smem()
+static size_t subpart_scatter_smem(uint32_t max_sub)
 {
-    return (size_t)WORK_ITEM_KEYS * 8 + (size_t)SUB_MAX_PER_BUCKET * (8 + 4 + 4) + (size_t)WORK_ITEM_KEYS * 2;
+    return (size_t)WORK_ITEM_KEYS * 8 + (size_t)max_sub * (8 + 4 + 4) + (size_t)WORK_ITEM_KEYS * 2;
 }
 
 cudaError_t launch_subpart_scatter(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                    unsigned int *next_item, const SubCfg *sc, unsigned long long *sub_cursor,
-                                   unsigned long long *out, uint64_t out_cap, cudaStream_t st)
+                                   unsigned long long *out, uint64_t out_cap, uint32_t max_sub, cudaStream_t st)
 {
     if (!n_items) return cudaSuccess;
+    if (!max_sub || max_sub > SUB_MAX_PER_BUCKET) return cudaErrorInvalidValue;
+    max_sub = (max_sub + 1) & ~1u;   // keeps the 2-byte array after the 4-byte ones aligned
     cudaError_t e = cudaMemsetAsync(next_item, 0, 4, st);
     if (e != cudaSuccess) return e;
-    const size_t smem = subpart_scatter_smem();
+    const size_t smem = subpart_scatter_smem(max_sub);
     e = cudaFuncSetAttribute(k_subpart_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -2792,7 +2810,7 @@ cudaError_t launch_subpart_scatter(const unsigned long long *keys, const BucketR
         per_sm = 1;
     const uint32_t grid = std::min<uint32_t>(n_items, (uint32_t)(sm_count() * per_sm));
     note_launch();
-    k_subpart_scatter<<<grid, 256, smem, st>>>(keys, rg, n_items, next_item, sc, sub_cursor, out, out_cap);
+    k_subpart_scatter<<<grid, 256, smem, st>>>(keys, rg, n_items, next_item, sc, sub_cursor, out, out_cap, max_sub);
     return cudaGetLastError();
 }
 
@@ -2806,7 +2824,8 @@ cudaError_t launch_count_subs(unsigned long long *keys, const unsigned long long
     if (min_count < 2) return cudaErrorInvalidValue;   // singletons are not records on this path
     cudaError_t e = cudaMemsetAsync(next_sub, 0, 4, st);
     if (e != cudaSuccess) return e;
-    const size_t smem = (size_t)2 * SUB_SLICE_BLOCKS * 8 + (size_t)SUB_TABLE_SLOTS * (8 + 4) + 2048 * 4;
+    const size_t smem = (size_t)2 * SUB_SLICE_BLOCKS * 8 + (size_t)SUB_TABLE_SLOTS * (8 + 4) + 2048 * 4 +
+                        (size_t)SUB_TILE * 8;
     e = cudaFuncSetAttribute(k_count_subs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const uint32_t grid = std::min<uint32_t>(n_sub, (uint32_t)sm_count());

@@ -276,7 +276,7 @@ cudaError_t launch_subpart_count(const unsigned long long *keys, const BucketRan
                                  const SubCfg *sc, uint32_t *sub_count, cudaStream_t st);
 cudaError_t launch_subpart_scatter(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                    unsigned int *next_item, const SubCfg *sc, unsigned long long *sub_cursor,
-                                   unsigned long long *out, uint64_t out_cap, cudaStream_t st);
+                                   unsigned long long *out, uint64_t out_cap, uint32_t max_sub, cudaStream_t st);
 cudaError_t launch_count_subs(unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count,
                               const uint8_t *sub_bucket, uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub,
                               uint32_t count_max, uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
