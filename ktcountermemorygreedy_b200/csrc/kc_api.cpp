@@ -79,10 +79,10 @@ kc_tuning default_tuning()
 }
 
 // k-mers per sub-bucket the shared-memory Bloom path starts from.  Its table
-// (SUB_TABLE_SLOTS) holds the distinct non-FIRST k-mers: at 30x coverage with
-// 1% errors about 2k of 48k, a quarter of the table; a sub-bucket with more
-// is cut in two and counted again.
-constexpr uint64_t SUB_KEYS_TARGET = 48 * 1024;
+// (SUB_TABLE_SLOTS, 4096) holds the distinct non-FIRST k-mers: at 30x
+// coverage with 1% errors about 1k of 24k, a quarter of the table; a
+// sub-bucket with more is cut in two and counted again.
+constexpr uint64_t SUB_KEYS_TARGET = 24 * 1024;
 
 // A plain job whose table would hold more slots than this (64 MiB of slots,
 // half of L2) is counted through the root-prefix buckets.
@@ -740,7 +740,12 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                     if (n_sub)
                         CK(cudaMemcpyAsync(sub_cur, sub_off, (size_t)n_sub * 8, cudaMemcpyDeviceToDevice, st));
                     const uint32_t max_sub = *std::max_element(nsub.begin(), nsub.end());
-                    CK(launch_subpart_scatter(keys, d_br, n_items, sub_next, d_sc, sub_cur, list, ocap, max_sub, st));
+                    BucketRanges bs = br;
+                    const uint32_t n_sp_items = fill_item_starts_n(bs, SUB_SCATTER_ITEM_KEYS);
+                    BucketRanges *d_bs = ds.n<BucketRanges>(1);
+                    CK(cudaMemcpyAsync(d_bs, &bs, sizeof(BucketRanges), cudaMemcpyHostToDevice, st));
+                    CK(launch_subpart_scatter(keys, d_bs, n_sp_items, sub_next, d_sc, sub_cur, list, ocap, max_sub,
+                                              st));
                     clk.end();
                     clk.begin(10);
                     CK(launch_count_subs(list, sub_off, sub_count, d_sb, n_sub, d_sc, sub_next, count_max,

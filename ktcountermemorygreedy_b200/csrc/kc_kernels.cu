@@ -1568,7 +1568,8 @@ constexpr uint32_t INSERT_GROUP = 2;
 // Claims the next work item for the whole block; false when none is left.
 // Work item `it` of a launch: its bucket is the last one whose first item is
 // at or before it (empty buckets share their first item with the next one).
-__device__ __forceinline__ WorkItem work_item(const BucketRanges *rg, const uint32_t *s_item0, uint32_t it)
+__device__ __forceinline__ WorkItem work_item_n(const BucketRanges *rg, const uint32_t *s_item0, uint32_t it,
+                                                uint32_t item_keys)
 {
     uint32_t lo = 0, hi = N_BUCKETS;
     while (hi - lo > 1) {
@@ -1578,10 +1579,15 @@ __device__ __forceinline__ WorkItem work_item(const BucketRanges *rg, const uint
     WorkItem w;
     w.bucket = lo;
     const unsigned long long b0 = rg->begin[lo], e0 = b0 + rg->len[lo];
-    w.begin = b0 + (unsigned long long)(it - s_item0[lo]) * WORK_ITEM_KEYS;
-    w.end = w.begin + WORK_ITEM_KEYS < e0 ? w.begin + WORK_ITEM_KEYS : e0;
+    w.begin = b0 + (unsigned long long)(it - s_item0[lo]) * item_keys;
+    w.end = w.begin + item_keys < e0 ? w.begin + item_keys : e0;
     w.pad = 0;
     return w;
+}
+
+__device__ __forceinline__ WorkItem work_item(const BucketRanges *rg, const uint32_t *s_item0, uint32_t it)
+{
+    return work_item_n(rg, s_item0, it, WORK_ITEM_KEYS);
 }
 
 __device__ __forceinline__ void load_item_starts(const BucketRanges *rg, uint32_t *s_item0)
@@ -1860,55 +1866,93 @@ __global__ void __launch_bounds__(256) k_subpart_count(const unsigned long long 
             if (s_h[i]) atomicAdd(&sub_count[c.sub_base + i], s_h[i]);
 }
 
-// One work item (WORK_ITEM_KEYS keys of one bucket) per round: the keys are
-// ranked by sub-bucket in shared memory, every sub-bucket of the item takes
-// its range with one cursor update, and the item's keys are written
-// reordered by sub-bucket (consecutive threads store consecutive addresses).
-constexpr uint32_t SP_PER_THREAD = WORK_ITEM_KEYS / 256;
+// Exclusive scan of one value per thread over a block of up to 1024 threads
+// (a multiple of 32).
+__device__ __forceinline__ uint32_t block_excl_scan_1024(uint32_t v, uint32_t *s_warp, uint32_t &total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t s = lane < nw ? s_warp[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL, s, o);
+            if (lane >= o) s += y;
+        }
+        s_warp[lane] = s;   // inclusive
+    }
+    __syncthreads();
+    total = s_warp[nw - 1];
+    const uint32_t base = warp ? s_warp[warp - 1] : 0u;
+    __syncthreads();
+    return base + x - v;
+}
 
-__global__ void __launch_bounds__(256) k_subpart_scatter(const unsigned long long *keys, const BucketRanges *rg,
-                                                         uint32_t n_items, unsigned int *next_item,
-                                                         const SubCfg *sc, unsigned long long *sub_cursor,
-                                                         unsigned long long *out, uint64_t out_cap, uint32_t max_sub)
+// One work item (SUB_SCATTER_ITEM_KEYS keys of one bucket) per round: the
+// keys are ranked by sub-bucket in shared memory, every sub-bucket of the
+// item takes its range with one cursor update, and the item's keys are
+// written reordered by sub-bucket (consecutive threads store consecutive
+// addresses).  Items are larger than the other bucket kernels' so that a
+// sub-bucket's run in an item spans several sectors.
+constexpr uint32_t SP_THREADS = 512;
+constexpr uint32_t SP_PER_THREAD = SUB_SCATTER_ITEM_KEYS / SP_THREADS;
+static_assert(SUB_SCATTER_ITEM_KEYS % SP_THREADS == 0 && SUB_SCATTER_ITEM_KEYS <= 65536, "item layout");
+
+__global__ void __launch_bounds__(SP_THREADS) k_subpart_scatter(const unsigned long long *keys, const BucketRanges *rg,
+                                                                uint32_t n_items, unsigned int *next_item,
+                                                                const SubCfg *sc, unsigned long long *sub_cursor,
+                                                                unsigned long long *out, uint64_t out_cap,
+                                                                uint32_t max_sub)
 {
     // shared arrays per sub-bucket hold max_sub entries (the most of any
     // bucket of the launch)
     extern __shared__ __align__(16) uint8_t sp_smem[];
-    unsigned long long *s_sorted = reinterpret_cast<unsigned long long *>(sp_smem);          // WORK_ITEM_KEYS
-    unsigned long long *s_dst = s_sorted + WORK_ITEM_KEYS;                                    // max_sub
+    unsigned long long *s_sorted = reinterpret_cast<unsigned long long *>(sp_smem);          // SUB_SCATTER_ITEM_KEYS
+    unsigned long long *s_dst = s_sorted + SUB_SCATTER_ITEM_KEYS;                             // max_sub
     uint32_t *s_cnt = reinterpret_cast<uint32_t *>(s_dst + max_sub);                          // max_sub
     uint32_t *s_start = s_cnt + max_sub;                                                      // max_sub
-    uint16_t *s_sub = reinterpret_cast<uint16_t *>(s_start + max_sub);                        // WORK_ITEM_KEYS
+    uint16_t *s_sub = reinterpret_cast<uint16_t *>(s_start + max_sub);                        // SUB_SCATTER_ITEM_KEYS
     __shared__ uint32_t s_item0[N_BUCKETS + 1];
-    __shared__ uint32_t s_item, s_warp[8];
+    __shared__ uint32_t s_item, s_warp[32];
     const int tid = threadIdx.x;
-    for (uint32_t i = tid; i < max_sub; i += 256) s_cnt[i] = 0;
+    for (uint32_t i = tid; i < max_sub; i += SP_THREADS) s_cnt[i] = 0;
     load_item_starts(rg, s_item0);
     uint32_t it;
     while (next_work(next_item, n_items, &s_item, it)) {
-        const WorkItem w = work_item(rg, s_item0, it);
+        const WorkItem w = work_item_n(rg, s_item0, it, SUB_SCATTER_ITEM_KEYS);
         const SubCfg c = sc[w.bucket];
         const uint32_t n = (uint32_t)(w.end - w.begin);
         unsigned long long k[SP_PER_THREAD];
         uint32_t sr[SP_PER_THREAD];   // rank << 16 | sub (sub 0xFFFF: no key)
 #pragma unroll
         for (uint32_t r = 0; r < SP_PER_THREAD; ++r) {
-            const uint32_t i = r * 256 + tid;
+            const uint32_t i = r * SP_THREADS + tid;
+            if (i < n) k[r] = __ldcs(&keys[w.begin + i]);
+        }
+#pragma unroll
+        for (uint32_t r = 0; r < SP_PER_THREAD; ++r) {
+            const uint32_t i = r * SP_THREADS + tid;
             sr[r] = 0xFFFFu;
             if (i < n) {
-                k[r] = __ldcs(&keys[w.begin + i]);
                 const uint32_t sub = sub_of(k[r], c);
                 sr[r] = (atomicAdd(&s_cnt[sub], 1u) << 16) | sub;
             }
         }
         __syncthreads();
-        // exclusive scan of the n_sub counts, up to 8 per thread
-        const uint32_t per = (c.n_sub + 255) / 256, b0 = tid * per;
+        // exclusive scan of the n_sub counts, a few per thread
+        const uint32_t per = (c.n_sub + SP_THREADS - 1) / SP_THREADS, b0 = tid * per;
         uint32_t local = 0;
         for (uint32_t j = 0; j < per; ++j)
             if (b0 + j < c.n_sub) local += s_cnt[b0 + j];
         uint32_t tot;
-        uint32_t run = block_excl_scan(local, s_warp, tot);
+        uint32_t run = block_excl_scan_1024(local, s_warp, tot);
         for (uint32_t j = 0; j < per; ++j) {
             const uint32_t s = b0 + j;
             if (s < c.n_sub) {
@@ -1930,11 +1974,11 @@ __global__ void __launch_bounds__(256) k_subpart_scatter(const unsigned long lon
             }
         }
         __syncthreads();
-        for (uint32_t i = tid; i < n; i += 256) {
+        for (uint32_t i = tid; i < n; i += SP_THREADS) {
             const unsigned long long d = s_dst[s_sub[i]] + i;
             if (d < out_cap) out[d] = s_sorted[i];
         }
-        for (uint32_t i = tid; i < c.n_sub; i += 256) s_cnt[i] = 0;
+        for (uint32_t i = tid; i < c.n_sub; i += SP_THREADS) s_cnt[i] = 0;
         __syncthreads();
     }
 }
@@ -1945,7 +1989,7 @@ constexpr uint32_t SUB_MAX_PROBE = 512;
 
 __device__ __forceinline__ int sub_table_slot(unsigned long long key)
 {
-    return (int)(slot_hash(key) >> (64 - 13));   // SUB_TABLE_SLOTS = 2^13
+    return (int)(slot_hash(key) >> (64 - SUB_TABLE_BITS));
 }
 
 __device__ __forceinline__ bool sub_table_add(unsigned long long *tk, uint32_t *tc, unsigned long long key)
@@ -1981,38 +2025,14 @@ __device__ __forceinline__ int sub_table_find(const unsigned long long *tk, unsi
     return -1;
 }
 
-constexpr uint32_t SUB_THREADS = 1024;
+constexpr uint32_t SUB_THREADS = 512;   // blocks of the shared-memory count
+constexpr uint32_t SUB_BLOCKS_PER_SM = 2;
 constexpr uint32_t SUB_PER_THREAD = 4;
 constexpr uint32_t SUB_TILE = SUB_THREADS * SUB_PER_THREAD;
+constexpr uint32_t SUB_HIST_BINS = 2048;   // counts below this go to a shared histogram
 
-__device__ __forceinline__ uint32_t block_excl_scan_1024(uint32_t v, uint32_t *s_warp, uint32_t &total)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(FULL, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) s_warp[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t s = s_warp[lane];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(FULL, s, o);
-            if (lane >= o) s += y;
-        }
-        s_warp[lane] = s;   // inclusive
-    }
-    __syncthreads();
-    total = s_warp[31];
-    const uint32_t base = warp ? s_warp[warp - 1] : 0u;
-    __syncthreads();
-    return base + x - v;
-}
 
-__global__ void __launch_bounds__(SUB_THREADS, 1) k_count_subs(
+__global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
     unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count, const uint8_t *sub_bucket,
     uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub, uint32_t count_max, uint32_t min_count,
     uint32_t max_count, unsigned long long *rec_keys, uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist,
@@ -2022,13 +2042,13 @@ __global__ void __launch_bounds__(SUB_THREADS, 1) k_count_subs(
     unsigned long long *s_filter = reinterpret_cast<unsigned long long *>(cs_smem);   // 2 * SUB_SLICE_BLOCKS
     unsigned long long *s_tk = s_filter + 2 * SUB_SLICE_BLOCKS;                       // SUB_TABLE_SLOTS
     uint32_t *s_tc = reinterpret_cast<uint32_t *>(s_tk + SUB_TABLE_SLOTS);            // SUB_TABLE_SLOTS
-    uint32_t *s_hist = s_tc + SUB_TABLE_SLOTS;                                        // 2048
-    unsigned long long *s_queue = reinterpret_cast<unsigned long long *>(s_hist + 2048);   // SUB_TILE
+    uint32_t *s_hist = s_tc + SUB_TABLE_SLOTS;                                        // SUB_HIST_BINS
+    unsigned long long *s_queue = reinterpret_cast<unsigned long long *>(s_hist + SUB_HIST_BINS);   // SUB_TILE
     __shared__ uint32_t s_warp[32], s_sub;
     __shared__ unsigned long long s_base;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t lt = lanemask_lt();
-    for (uint32_t i = tid; i < 2048; i += SUB_THREADS) s_hist[i] = 0;
+    for (uint32_t i = tid; i < SUB_HIST_BINS; i += SUB_THREADS) s_hist[i] = 0;
     unsigned long long n_high = 0, n_low = 0, n_low_only = 0, n_distinct = 0;
     uint32_t n_ovf_subs = 0;
     bool rec_full = false;
@@ -2133,7 +2153,7 @@ __global__ void __launch_bounds__(SUB_THREADS, 1) k_count_subs(
             if (s_tk[i] == EMPTY_KEY) continue;
             ++n_distinct;
             const uint32_t c = s_tc[i] < count_max ? s_tc[i] : count_max;
-            if (c < 2048) atomicAdd(&s_hist[c], 1u);
+            if (c < SUB_HIST_BINS) atomicAdd(&s_hist[c], 1u);
             else if (c < HIST_BINS) atomicAdd(&hist[c], 1ull);
             else {
                 const unsigned long long q = atomicAdd(&counters[C_OVF_LEN], 1ull);
@@ -2162,7 +2182,7 @@ __global__ void __launch_bounds__(SUB_THREADS, 1) k_count_subs(
         __syncthreads();
     }
     __syncthreads();
-    for (uint32_t i = tid; i < 2048; i += SUB_THREADS)
+    for (uint32_t i = tid; i < SUB_HIST_BINS; i += SUB_THREADS)
         if (s_hist[i]) atomicAdd(&hist[i], (unsigned long long)s_hist[i]);
     if (rec_full) atomicOr(&counters[C_FLAGS], ERR_RECORDS_FULL);
     const unsigned long long v[4] = {n_high, n_low, n_low_only, n_distinct};
@@ -2721,16 +2741,18 @@ static int persistent_grid(K kernel)
     return sm_count() * per_sm;
 }
 
-uint32_t fill_item_starts(BucketRanges &r)
+uint32_t fill_item_starts_n(BucketRanges &r, uint64_t item_keys)
 {
     uint32_t n = 0;
     for (uint32_t b = 0; b < N_BUCKETS; ++b) {
         r.item0[b] = n;
-        n += (uint32_t)((r.len[b] + WORK_ITEM_KEYS - 1) / WORK_ITEM_KEYS);
+        n += (uint32_t)((r.len[b] + item_keys - 1) / item_keys);
     }
     r.item0[N_BUCKETS] = n;
     return n;
 }
+
+uint32_t fill_item_starts(BucketRanges &r) { return fill_item_starts_n(r, WORK_ITEM_KEYS); }
 
 cudaError_t launch_bloom_buckets(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                  unsigned int *next_item, const BucketCfg *cfg, unsigned long long *bits,
@@ -2789,7 +2811,7 @@ cudaError_t launch_subpart_count(const unsigned long long *keys, const BucketRan
 
 static size_t subpart_scatter_smem(uint32_t max_sub)
 {
-    return (size_t)WORK_ITEM_KEYS * 8 + (size_t)max_sub * (8 + 4 + 4) + (size_t)WORK_ITEM_KEYS * 2;
+    return (size_t)SUB_SCATTER_ITEM_KEYS * (8 + 2) + (size_t)max_sub * (8 + 4 + 4);
 }
 
 cudaError_t launch_subpart_scatter(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
@@ -2805,12 +2827,12 @@ cudaError_t launch_subpart_scatter(const unsigned long long *keys, const BucketR
     e = cudaFuncSetAttribute(k_subpart_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_subpart_scatter, 256, smem) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_subpart_scatter, SP_THREADS, smem) != cudaSuccess ||
         per_sm < 1)
         per_sm = 1;
     const uint32_t grid = std::min<uint32_t>(n_items, (uint32_t)(sm_count() * per_sm));
     note_launch();
-    k_subpart_scatter<<<grid, 256, smem, st>>>(keys, rg, n_items, next_item, sc, sub_cursor, out, out_cap, max_sub);
+    k_subpart_scatter<<<grid, SP_THREADS, smem, st>>>(keys, rg, n_items, next_item, sc, sub_cursor, out, out_cap, max_sub);
     return cudaGetLastError();
 }
 
@@ -2824,11 +2846,11 @@ cudaError_t launch_count_subs(unsigned long long *keys, const unsigned long long
     if (min_count < 2) return cudaErrorInvalidValue;   // singletons are not records on this path
     cudaError_t e = cudaMemsetAsync(next_sub, 0, 4, st);
     if (e != cudaSuccess) return e;
-    const size_t smem = (size_t)2 * SUB_SLICE_BLOCKS * 8 + (size_t)SUB_TABLE_SLOTS * (8 + 4) + 2048 * 4 +
+    const size_t smem = (size_t)2 * SUB_SLICE_BLOCKS * 8 + (size_t)SUB_TABLE_SLOTS * (8 + 4) + SUB_HIST_BINS * 4 +
                         (size_t)SUB_TILE * 8;
     e = cudaFuncSetAttribute(k_count_subs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const uint32_t grid = std::min<uint32_t>(n_sub, (uint32_t)sm_count());
+    const uint32_t grid = std::min<uint32_t>(n_sub, (uint32_t)sm_count() * SUB_BLOCKS_PER_SM);
     note_launch();
     k_count_subs<<<grid, SUB_THREADS, smem, st>>>(keys, sub_off, sub_count, sub_bucket, n_sub, sc, next_sub, count_max,
                                                   min_count, max_count, rec_keys, rec_counts, rec_cap, hist, ovf,

@@ -145,14 +145,17 @@ struct BucketRanges {
     uint32_t item0[N_BUCKETS + 1];
 };
 uint32_t fill_item_starts(BucketRanges &r);   // sets item0 from len, returns the number of items
+uint32_t fill_item_starts_n(BucketRanges &r, uint64_t item_keys);   // items of item_keys keys
+constexpr uint32_t SUB_SCATTER_ITEM_KEYS = 4096;   // keys per work item of the sub-bucket scatter
 
 // Shared-memory sub-bucket path of the Bloom split: every bucket is cut
 // into n_sub sub-buckets of 2^slice_shift consecutive blocks of its filter (a
 // k-mer's sub-bucket follows from its filter block), so one thread block
 // holds a sub-bucket's filter slice and counting table in shared memory.
-constexpr uint32_t SUB_SLICE_BLOCKS = 4096;     // largest slice (2 words a block): 64 KiB of filter
-constexpr uint32_t SUB_TABLE_SLOTS = 8192;      // counting-table slots of a sub-bucket
-constexpr uint32_t SUB_MAX_PER_BUCKET = 2048;   // sub-buckets of one bucket
+constexpr uint32_t SUB_SLICE_BLOCKS = 2048;     // largest slice (2 words a block): 32 KiB of filter
+constexpr uint32_t SUB_TABLE_BITS = 12;
+constexpr uint32_t SUB_TABLE_SLOTS = 1u << SUB_TABLE_BITS;   // counting-table slots of a sub-bucket
+constexpr uint32_t SUB_MAX_PER_BUCKET = 4096;   // sub-buckets of one bucket
 struct SubCfg {
     unsigned long long fcap;    // the bucket's filter blocks (a power of two)
     uint32_t sub_base, n_sub;   // its sub-buckets [sub_base, sub_base + n_sub), n_sub = fcap >> slice_shift
@@ -262,7 +265,8 @@ cudaError_t launch_select_range(const unsigned long long *keys, const uint32_t *
 // Bucket-major kernels of the partitioned pipeline; each resets *next_item.
 // Sub-bucket path.  count: sub_count[sub_base + s] += the keys of bucket b
 // in sub-bucket s.  scatter: every key to out[sub_cursor[its sub-bucket]++]
-// (sub_cursor starts at the exclusive scan of sub_count).  count_subs: one
+// (sub_cursor starts at the exclusive scan of sub_count); its ranges rg are
+// cut into items of SUB_SCATTER_ITEM_KEYS keys (fill_item_starts_n).  count_subs: one
 // block per sub-bucket at a time runs the Bloom split with the filter slice in
 // shared memory, counts the non-FIRST occurrences in a shared-memory table,
 // merges the FIRST ones (written back over the front of the sub-bucket's
