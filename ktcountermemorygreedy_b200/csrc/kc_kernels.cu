@@ -1456,6 +1456,7 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_radix_onesweep(const unsigned
 
     // stable rank of every key among the tile's keys with the same digit
     unsigned long long k[RS_ITEMS];
+    uint32_t v[RS_ITEMS];
     uint32_t rd[RS_ITEMS];   // rank << 16 | digit (digit 256: no key)
     uint32_t *wc = s_wcnt + warp * 256;
 #pragma unroll
@@ -1463,6 +1464,7 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_radix_onesweep(const unsigned
         const uint32_t li = warp * RS_WARP_ITEMS + r * 32 + lane;
         const bool act = li < tile_n;
         k[r] = act ? __ldcs(&kin[base + li]) : 0;
+        v[r] = act ? __ldcs(&vin[base + li]) : 0u;
         const uint32_t d = act ? (uint32_t)((k[r] >> shift) & 255) : 256u;
         const uint32_t peers = __match_any_sync(FULL, d);
         const uint32_t before = __popc(peers & lanemask_lt());
@@ -1519,7 +1521,7 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_radix_onesweep(const unsigned
             const uint32_t li = warp * RS_WARP_ITEMS + r * 32 + lane;
             const uint32_t pos = s_start[d] + s_wcnt[warp * 256 + d] + (rd[r] >> 16);
             s_keys[pos] = k[r];
-            s_vals[pos] = __ldcs(&vin[base + li]);
+            s_vals[pos] = v[r];
         }
     }
     __syncthreads();
