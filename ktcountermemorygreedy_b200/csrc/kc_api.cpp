@@ -398,7 +398,6 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     const uint32_t max_probe_cap = 1u << 16;
     const double est = hll_estimate(hll_h.data(), HLL_M);
     unsigned long long *hist = ds.n<unsigned long long>(HIST_BINS);
-    std::vector<unsigned long long> hist_add(HIST_BINS, 0);   // histograms of shared-memory sub-bucket passes
     const uint64_t ovf_cap = 1 << 20;
     uint32_t *ovf = ds.n<uint32_t>(ovf_cap);
     unsigned long long *n_keys = ds.n<unsigned long long>(1);
@@ -687,7 +686,10 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                     }
                     nsub[b] = (uint32_t)want;
                 }
-                const Counters before = read_counters(counters, st);
+                // the overflow list's length before the attempts, restored after
+                // a failed one (on the device: no round trip)
+                unsigned long long *ovf_len_saved = ds.n<unsigned long long>(1);
+                CK(cudaMemcpyAsync(ovf_len_saved, counters + C_OVF_LEN, 8, cudaMemcpyDeviceToDevice, st));
                 for (int attempt = 0; eligible && !sub_done; ++attempt) {
                     const DevScope::Mark m0 = ds.mark();
                     std::vector<SubCfg> sc(N_BUCKETS);
@@ -755,10 +757,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                     const Counters cs = read_counters(counters, st);
                     check_flags(cs.v[C_FLAGS], "sub-bucket count");
                     if (cs.v[C_SUB_OVF] == 0) {
-                        std::vector<unsigned long long> hs(HIST_BINS);
-                        CK(cudaMemcpyAsync(hs.data(), hist_sub, HIST_BINS * 8, cudaMemcpyDeviceToHost, st));
-                        CK(cudaStreamSynchronize(st));
-                        for (size_t i = 0; i < HIST_BINS; ++i) hist_add[i] += hs[i];
+                        CK(launch_add_u64(hist, hist_sub, HIST_BINS, st));
                         rec_keys = rk;
                         rec_counts = rc;
                         n_rec = cs.v[C_REC_LEN];
@@ -776,8 +775,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                     // sub-buckets' tables: twice the sub-buckets next time
                     std::vector<uint32_t> bo(N_BUCKETS);
                     CK(cudaMemcpyAsync(bo.data(), bucket_ovf, N_BUCKETS * 4, cudaMemcpyDeviceToHost, st));
-                    unsigned long long ovf_len = before.v[C_OVF_LEN];
-                    CK(cudaMemcpyAsync(counters + C_OVF_LEN, &ovf_len, 8, cudaMemcpyHostToDevice, st));
+                    CK(cudaMemcpyAsync(counters + C_OVF_LEN, ovf_len_saved, 8, cudaMemcpyDeviceToDevice, st));
                     CK(cudaStreamSynchronize(st));
                     ds.rewind(m0);
                     bool any = false;
@@ -968,7 +966,6 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     std::vector<uint32_t> ovf_h(n_ovf);
     if (n_ovf) CK(cudaMemcpyAsync(ovf_h.data(), ovf, n_ovf * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    for (size_t i = 0; i < HIST_BINS; ++i) hd[i] += hist_add[i];
     hd[1] += job.low_only;   // FIRST-only k-mers have count 1 (count_max >= 1)
     {
         uint32_t lo = P.hist_min, hi = P.hist_max;

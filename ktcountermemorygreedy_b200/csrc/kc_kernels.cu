@@ -1518,7 +1518,6 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_radix_onesweep(const unsigned
     for (uint32_t r = 0; r < RS_ITEMS; ++r) {
         const uint32_t d = rd[r] & 0xFFFFu;
         if (d < 256) {
-            const uint32_t li = warp * RS_WARP_ITEMS + r * 32 + lane;
             const uint32_t pos = s_start[d] + s_wcnt[warp * 256 + d] + (rd[r] >> 16);
             s_keys[pos] = k[r];
             s_vals[pos] = v[r];
@@ -2327,6 +2326,20 @@ cudaError_t launch_scan_u32(const uint32_t *in, unsigned long long *out, uint64_
     k_scan_top<<<1, 1024, 0, st>>>(tmp, nb);
     note_launch();
     k_scan_down<<<(unsigned)nb, 256, 0, st>>>(in, n, tmp, out);
+    return cudaGetLastError();
+}
+
+__global__ void k_add_u64(unsigned long long *dst, const unsigned long long *src, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if (src[i]) dst[i] += src[i];
+}
+
+cudaError_t launch_add_u64(unsigned long long *dst, const unsigned long long *src, uint64_t n, cudaStream_t st)
+{
+    if (!n) return cudaSuccess;
+    note_launch();
+    k_add_u64<<<grid_for(n, 256), 256, 0, st>>>(dst, src, n);
     return cudaGetLastError();
 }
 

@@ -189,6 +189,7 @@ cudaError_t launch_scan_u32(const uint32_t *in, unsigned long long *out, uint64_
 cudaError_t launch_init_slots(Slot *slots, uint64_t n, cudaStream_t st);
 cudaError_t launch_count_keys(const Slot *slots, uint64_t n, unsigned long long *out, cudaStream_t st);
 cudaError_t launch_fill_u64(unsigned long long *p, uint64_t n, unsigned long long v, cudaStream_t st);
+cudaError_t launch_add_u64(unsigned long long *dst, const unsigned long long *src, uint64_t n, cudaStream_t st);
 cudaError_t launch_insert_list(const unsigned long long *keys, uint64_t n, TableRef t, uint32_t max_probe,
                                unsigned long long *counters, cudaStream_t st);
 cudaError_t launch_insert_pairs(const unsigned long long *keys, const uint32_t *counts, uint64_t n, TableRef t,
