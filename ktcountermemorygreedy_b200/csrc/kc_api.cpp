@@ -247,6 +247,50 @@ Counters read_counters(const unsigned long long *d, cudaStream_t st)
     return c;
 }
 
+// Pinned host staging for one job's small uploads and read-backs.  Copies
+// between the device and pinned memory are asynchronous, so several
+// read-backs share one synchronisation and an upload does not stall the
+// host; a region is written by the host only before its copy is queued and
+// never reused.  The stream is drained before the blocks go back to the pool.
+struct HostStage {
+    cudaStream_t st;
+    std::vector<PinnedBlock> blocks;
+    size_t top = 0;
+    explicit HostStage(cudaStream_t s) : st(s) {}
+    HostStage(const HostStage &) = delete;
+    HostStage &operator=(const HostStage &) = delete;
+    void *get(size_t bytes)
+    {
+        bytes = (bytes + 255) & ~size_t(255);
+        if (blocks.empty() || top + bytes > blocks.back().bytes) {
+            PinnedBlock b;
+            b.reset(std::max<size_t>(bytes, size_t(1) << 21));
+            blocks.push_back(std::move(b));
+            top = 0;
+        }
+        void *p = static_cast<uint8_t *>(blocks.back().p) + top;
+        top += bytes;
+        return p;
+    }
+    template <class T>
+    T *n(size_t count)
+    {
+        return static_cast<T *>(get(count * sizeof(T)));
+    }
+    // a pinned copy of count objects, for an upload
+    template <class T>
+    const T *up(const T *src, size_t count)
+    {
+        T *p = n<T>(count);
+        if (count) std::memcpy(p, src, count * sizeof(T));
+        return p;
+    }
+    ~HostStage()
+    {
+        if (!blocks.empty()) cudaStreamSynchronize(st);
+    }
+};
+
 // A root-prefix bucket outgrew the region estimated from the sampled census.
 struct CensusOverflow {};
 
@@ -379,17 +423,34 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     }
     CK(launch_extract(MODE_SCAN, a, 0, st));
     clk.end();
-    std::vector<uint32_t> hll_h(HLL_M);
-    unsigned long long O = 0;
-    CK(cudaMemcpyAsync(&O, occ, 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(hll_h.data(), hll, HLL_M * 4, cudaMemcpyDeviceToHost, st));
+    // the SCAN's results (and the bucket census) come back under one sync
+    HostStage hs(st);
+    unsigned long long *p_occ = hs.n<unsigned long long>(1);
+    uint32_t *p_hll = hs.n<uint32_t>(HLL_M);
+    uint32_t *p_ph = hs.n<uint32_t>(256);
+    unsigned long long *p_qh = hs.n<unsigned long long>(2);
+    unsigned long long *p_bh = hs.n<unsigned long long>(N_BUCKETS);
+    unsigned long long *p_c0 = hs.n<unsigned long long>(C_COUNT);
+    CK(cudaMemcpyAsync(p_occ, occ, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(p_hll, hll, HLL_M * 4, cudaMemcpyDeviceToHost, st));
+    if (P.bloom) {
+        CK(cudaMemcpyAsync(p_ph, prefix_hist, 256 * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(p_qh, qual, 16, cudaMemcpyDeviceToHost, st));
+    }
+    if (bucket_hist) CK(cudaMemcpyAsync(p_bh, bucket_hist, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(p_c0, counters, C_COUNT * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::vector<uint32_t> hll_h(p_hll, p_hll + HLL_M);
+    unsigned long long O = *p_occ;
     std::vector<uint32_t> ph(256, 0);
     unsigned long long qh[2] = {0, 0};
     if (P.bloom) {
-        CK(cudaMemcpyAsync(ph.data(), prefix_hist, 256 * 4, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(qh, qual, 16, cudaMemcpyDeviceToHost, st));
+        ph.assign(p_ph, p_ph + 256);
+        qh[0] = p_qh[0];
+        qh[1] = p_qh[1];
     }
-    Counters c0 = read_counters(counters, st);
+    Counters c0{};
+    std::memcpy(c0.v, p_c0, sizeof(c0.v));
     check_flags(c0.v[C_FLAGS], "scan");
     job.occurrences = O;
 
@@ -530,9 +591,8 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
         // src/NewKmerTree.h:1488-1495): sizes from the SCAN census, one
         // scatter pass, then every bucket's Bloom filter and table slice is
         // processed while it sits in L2
-        std::vector<unsigned long long> bh(N_BUCKETS);
-        CK(cudaMemcpyAsync(bh.data(), bucket_hist, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
+        if (!bucket_hist) throw KcError{KC_ERR_DEVICE, "partitioned job without a bucket census"};
+        const std::vector<unsigned long long> bh(p_bh, p_bh + N_BUCKETS);
         std::vector<unsigned long long> region(N_BUCKETS);
         unsigned long long sampled = 0;
         for (uint32_t b = 0; b < N_BUCKETS; ++b) sampled += bh[b];
@@ -629,7 +689,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                 bb[N_BUCKETS + b] = cfg[b].key_base + region[b];
             }
             CK(cudaMemsetAsync(cursor, 0, N_BUCKETS * 8, st));
-            CK(cudaMemcpyAsync(bbase, bb.data(), 2 * N_BUCKETS * 8, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(bbase, hs.up(bb.data(), bb.size()), 2 * N_BUCKETS * 8, cudaMemcpyHostToDevice, st));
             CK(cudaMemsetAsync(lh_cnt, 0, 2 * N_BUCKETS * 8, st));
             CK(cudaMemsetAsync(hll_high, 0, (size_t)N_BUCKETS * BUCKET_HLL_M * 4, st));
             a.hll = nullptr;
@@ -645,20 +705,22 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
             clk.begin(2);
             CK(launch_extract(MODE_PART, a, 0, st));
             clk.end();
-            std::vector<unsigned long long> fill(N_BUCKETS);
-            CK(cudaMemcpyAsync(fill.data(), cursor, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
+            unsigned long long *p_fill = hs.n<unsigned long long>(N_BUCKETS);
+            CK(cudaMemcpyAsync(p_fill, cursor, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
+            const std::vector<unsigned long long> fill(p_fill, p_fill + N_BUCKETS);
             for (uint32_t b = lo; b < hi; ++b) {
                 if (fill[b] > region[b]) throw CensusOverflow{};
                 cfg[b].key_len = fill[b];
                 filled_total += fill[b];
             }
-            CK(cudaMemcpyAsync(d_cfg_b, cfg.data(), N_BUCKETS * sizeof(BucketCfg), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(d_cfg_b, hs.up(cfg.data(), N_BUCKETS), N_BUCKETS * sizeof(BucketCfg),
+                               cudaMemcpyHostToDevice, st));
             // each bucket-major launch gets its 256 ranges, not a list of items
             auto upload_ranges = [&](BucketRanges &r, uint32_t &n_items) {
                 n_items = fill_item_starts(r);
                 BucketRanges *d = ds.n<BucketRanges>(1);
-                CK(cudaMemcpyAsync(d, &r, sizeof(BucketRanges), cudaMemcpyHostToDevice, st));
+                CK(cudaMemcpyAsync(d, hs.up(&r, 1), sizeof(BucketRanges), cudaMemcpyHostToDevice, st));
                 return d;
             };
             // Bloom jobs whose records need count >= 2: the Bloom split, the
@@ -728,8 +790,9 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                     }
                     uint32_t n_items = 0;
                     BucketRanges *d_br = upload_ranges(br, n_items);
-                    CK(cudaMemcpyAsync(d_sc, sc.data(), N_BUCKETS * sizeof(SubCfg), cudaMemcpyHostToDevice, st));
-                    if (n_sub) CK(cudaMemcpyAsync(d_sb, sb.data(), n_sub, cudaMemcpyHostToDevice, st));
+                    CK(cudaMemcpyAsync(d_sc, hs.up(sc.data(), N_BUCKETS), N_BUCKETS * sizeof(SubCfg),
+                                       cudaMemcpyHostToDevice, st));
+                    if (n_sub) CK(cudaMemcpyAsync(d_sb, hs.up(sb.data(), n_sub), n_sub, cudaMemcpyHostToDevice, st));
                     CK(cudaMemsetAsync(sub_count, 0, std::max<uint32_t>(n_sub, 1) * 4, st));
                     CK(cudaMemsetAsync(bucket_ovf, 0, N_BUCKETS * 4, st));
                     CK(cudaMemsetAsync(hist_sub, 0, HIST_BINS * 8, st));
@@ -745,7 +808,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                     BucketRanges bs = br;
                     const uint32_t n_sp_items = fill_item_starts_n(bs, SUB_SCATTER_ITEM_KEYS);
                     BucketRanges *d_bs = ds.n<BucketRanges>(1);
-                    CK(cudaMemcpyAsync(d_bs, &bs, sizeof(BucketRanges), cudaMemcpyHostToDevice, st));
+                    CK(cudaMemcpyAsync(d_bs, hs.up(&bs, 1), sizeof(BucketRanges), cudaMemcpyHostToDevice, st));
                     CK(launch_subpart_scatter(keys, d_bs, n_sp_items, sub_next, d_sc, sub_cur, list, ocap, max_sub,
                                               st));
                     clk.end();
@@ -941,7 +1004,6 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
         }
     }
     job.table_cap = table_cap;
-    const Counters c2 = read_counters(counters, st);
 
     // ---- sort in printed-string order ---------------------------------------
     clk.begin(6);
@@ -957,15 +1019,23 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     }
     CK(launch_pair_reverse(rec_keys, n_rec, st));
     clk.end();
-    check_flags(read_counters(counters, st).v[C_FLAGS], "sort");
 
-    // ---- histogram ----------------------------------------------------------
-    std::vector<unsigned long long> hd(HIST_BINS);
-    CK(cudaMemcpyAsync(hd.data(), hist, HIST_BINS * 8, cudaMemcpyDeviceToHost, st));
+    // ---- histogram (with the counters, under one sync) ----------------------
+    unsigned long long *p_c2 = hs.n<unsigned long long>(C_COUNT);
+    unsigned long long *p_hd = hs.n<unsigned long long>(HIST_BINS);
+    CK(cudaMemcpyAsync(p_c2, counters, C_COUNT * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(p_hd, hist, HIST_BINS * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    Counters c2{};
+    std::memcpy(c2.v, p_c2, sizeof(c2.v));
+    check_flags(c2.v[C_FLAGS], "sort");
+    std::vector<unsigned long long> hd(p_hd, p_hd + HIST_BINS);
     const uint64_t n_ovf = std::min<uint64_t>(c2.v[C_OVF_LEN], ovf_cap);
     std::vector<uint32_t> ovf_h(n_ovf);
-    if (n_ovf) CK(cudaMemcpyAsync(ovf_h.data(), ovf, n_ovf * 4, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    if (n_ovf) {
+        CK(cudaMemcpyAsync(ovf_h.data(), ovf, n_ovf * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
     hd[1] += job.low_only;   // FIRST-only k-mers have count 1 (count_max >= 1)
     {
         uint32_t lo = P.hist_min, hi = P.hist_max;
