@@ -151,9 +151,9 @@ typedef struct {
                                      default 1.6 */
     uint64_t sort_group_records;  /* records sorted together (kept in L2) by a batch's segmented sort;
                                      default 4M */
-    uint64_t bloom_smem;          /* Bloom jobs with min_count >= 2: 1 counts each sub-bucket (a 64 KiB slice
-                                     of its filter) in shared memory, 2 uses global-memory filters and
-                                     tables; default 1 */
+    uint64_t bloom_smem;          /* Bloom jobs with min_count >= 2: 1 counts each filter sub-bucket (a slice
+                                     of at most 2048 blocks, 32 KiB) in shared memory, 2 uses global-memory
+                                     filters and tables; default 1 */
     uint64_t reserved[4];
 } kc_tuning;
 
