@@ -1831,6 +1831,7 @@ __device__ __forceinline__ uint32_t sub_of(unsigned long long key, const SubCfg 
 
 // Each block counts a contiguous run of work items (bucket-major, so a block
 // meets one or two buckets) in a shared histogram, flushed per bucket.
+constexpr uint32_t SPC_PER_THREAD = WORK_ITEM_KEYS / 256;
 __global__ void __launch_bounds__(256) k_subpart_count(const unsigned long long *keys, const BucketRanges *rg,
                                                        uint32_t n_items, const SubCfg *sc, uint32_t *sub_count)
 {
@@ -1858,8 +1859,18 @@ __global__ void __launch_bounds__(256) k_subpart_count(const unsigned long long 
             cur = w.bucket;
             c = sc[cur];
         }
-        for (unsigned long long i = w.begin + tid; i < w.end; i += 256)
-            atomicAdd(&s_h[sub_of(__ldcs(&keys[i]), c)], 1u);
+        // a work item is 8 keys per thread: their loads are issued together
+        for (unsigned long long i0 = w.begin + tid; i0 < w.end; i0 += 256 * SPC_PER_THREAD) {
+            unsigned long long kk[SPC_PER_THREAD];
+#pragma unroll
+            for (uint32_t r = 0; r < SPC_PER_THREAD; ++r) {
+                const unsigned long long i = i0 + r * 256;
+                kk[r] = i < w.end ? __ldcs(&keys[i]) : 0ull;
+            }
+#pragma unroll
+            for (uint32_t r = 0; r < SPC_PER_THREAD; ++r)
+                if (i0 + r * 256 < w.end) atomicAdd(&s_h[sub_of(kk[r], c)], 1u);
+        }
     }
     __syncthreads();
     if (cur != N_BUCKETS)

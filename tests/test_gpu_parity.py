@@ -271,6 +271,8 @@ def test_multi_pass_jobs_match_single_pass(counter):
         one = counter.count([fq], k=31, bloom=bloom, memory_gb=2, min_count=mc, **kw)
         many = counter.count([fq], k=31, bloom=bloom, memory_gb=2, min_count=mc, pass_bytes=24 << 20, **kw)
         assert one.passes == 1 and many.passes >= 4, (one.passes, many.passes)
+        if bloom:   # min count 2: every pass counts its sub-buckets in shared memory
+            assert many.smem_passes == many.passes and one.smem_passes == 1
         assert np.array_equal(many.keys, want_k) and np.array_equal(many.counts, want_c)
         for f in ("keys", "counts", "hist", "top_keys", "top_counts", "le2_keys", "le2_counts"):
             assert np.array_equal(getattr(many, f), getattr(one, f)), (bloom, f)
