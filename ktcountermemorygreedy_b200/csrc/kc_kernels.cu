@@ -2087,13 +2087,22 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
         // written back over the front of the sub-bucket's keys
         bool full = false;
         uint32_t lo_cnt = 0;   // the same in every thread
+        // the next tile's k-mers are loaded while this one is classified (a
+        // tile's FIRST write-back only reaches positions already loaded)
+        unsigned long long kn[SUB_PER_THREAD];
+#pragma unroll
+        for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
+            const uint32_t i = r * SUB_THREADS + tid;
+            kn[r] = i < n ? __ldcs(&keys[base + i]) : EMPTY_KEY;
+        }
         for (uint32_t t0 = 0; t0 < n; t0 += SUB_TILE) {
             unsigned long long k[SUB_PER_THREAD];
             uint32_t firsts = 0, highs = 0;
 #pragma unroll
             for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
-                const uint32_t i = t0 + r * SUB_THREADS + tid;
-                k[r] = i < n ? __ldcs(&keys[base + i]) : EMPTY_KEY;
+                k[r] = kn[r];
+                const uint32_t i = t0 + SUB_TILE + r * SUB_THREADS + tid;
+                kn[r] = i < n ? __ldcs(&keys[base + i]) : EMPTY_KEY;
             }
 #pragma unroll
             for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
@@ -2152,11 +2161,20 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
         }
         // 2. FIRST occurrences: a hit adds one to the table count, a miss is a
         // k-mer seen once (counted, not a record: min_count >= 2)
-        for (uint32_t i = tid; i < lo_cnt; i += SUB_THREADS) {
-            const unsigned long long key = __ldcg(&keys[base + i]);
-            const int sl = sub_table_find(s_tk, key);
-            if (sl >= 0) atomicAdd(&s_tc[sl], 1u);
-            else ++n_low_only;
+        for (uint32_t i0 = tid; i0 < lo_cnt; i0 += SUB_THREADS * SUB_PER_THREAD) {
+            unsigned long long kk[SUB_PER_THREAD];
+#pragma unroll
+            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
+                const uint32_t i = i0 + r * SUB_THREADS;
+                kk[r] = i < lo_cnt ? __ldcg(&keys[base + i]) : EMPTY_KEY;
+            }
+#pragma unroll
+            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
+                if (i0 + r * SUB_THREADS >= lo_cnt) continue;
+                const int sl = sub_table_find(s_tk, kk[r]);
+                if (sl >= 0) atomicAdd(&s_tc[sl], 1u);
+                else ++n_low_only;
+            }
         }
         __syncthreads();
         // 3. the table's records and histogram
