@@ -651,10 +651,9 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
                     s_bhist[tid] = 0;   // the next round's ranks (emission is done)
                     const uint32_t bstart = block_excl_scan(c, s_warp, tot_b);
                     s_hist[tid] = bstart;
-                    // destination of sorted index i of bucket b: s_bpos[b] + i
-                    s_bpos[tid] = c ? a.bucket_base[tid] + atomicAdd(&a.bucket_cursor[tid], (unsigned long long)c) -
-                                          bstart
-                                    : 0ull;
+                    // this tile's range of bucket tid: the cursor update is in
+                    // flight during the reorder and consumed only after it
+                    const unsigned long long cur = c ? atomicAdd(&a.bucket_cursor[tid], (unsigned long long)c) : 0ull;
                     __syncthreads();
                     unsigned long long kr[STAGE_CAP / EXT_THREADS];
 #pragma unroll
@@ -671,6 +670,8 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
                         const uint32_t i = tid + r * EXT_THREADS;
                         if (i < nr && s_rank[i] != 0xFFFFu) s_stage[s_rank[i]] = kr[r];
                     }
+                    // destination of sorted index i of bucket b: s_bpos[b] + i
+                    s_bpos[tid] = c ? a.bucket_base[tid] + cur - bstart : 0ull;
                     __syncthreads();
                     for (uint32_t i = tid; i < tot_b; i += EXT_THREADS) {
                         const unsigned long long key = s_stage[i];
@@ -1915,6 +1916,7 @@ __device__ __forceinline__ uint32_t block_excl_scan_1024(uint32_t v, uint32_t *s
 // sub-bucket's run in an item spans several sectors.
 constexpr uint32_t SP_THREADS = 512;
 constexpr uint32_t SP_PER_THREAD = SUB_SCATTER_ITEM_KEYS / SP_THREADS;
+constexpr uint32_t SP_MAX_BINS = (SUB_MAX_PER_BUCKET + SP_THREADS - 1) / SP_THREADS;   // sub-buckets per thread
 static_assert(SUB_SCATTER_ITEM_KEYS % SP_THREADS == 0 && SUB_SCATTER_ITEM_KEYS <= 65536, "item layout");
 
 __global__ void __launch_bounds__(SP_THREADS) k_subpart_scatter(const unsigned long long *keys, const BucketRanges *rg,
@@ -1965,13 +1967,19 @@ __global__ void __launch_bounds__(SP_THREADS) k_subpart_scatter(const unsigned l
             if (b0 + j < c.n_sub) local += s_cnt[b0 + j];
         uint32_t tot;
         uint32_t run = block_excl_scan_1024(local, s_warp, tot);
-        for (uint32_t j = 0; j < per; ++j) {
+        // the sub-buckets' cursor updates are in flight during the reorder
+        // and consumed only after it
+        unsigned long long cur[SP_MAX_BINS];
+        uint32_t first[SP_MAX_BINS];
+#pragma unroll
+        for (uint32_t j = 0; j < SP_MAX_BINS; ++j) {
             const uint32_t s = b0 + j;
-            if (s < c.n_sub) {
+            cur[j] = 0ull;
+            first[j] = run;
+            if (j < per && s < c.n_sub) {
                 const uint32_t cnt = s_cnt[s];
                 s_start[s] = run;
-                // destination of sorted index i of sub-bucket s: s_dst[s] + i
-                s_dst[s] = cnt ? atomicAdd(&sub_cursor[c.sub_base + s], (unsigned long long)cnt) - run : 0ull;
+                if (cnt) cur[j] = atomicAdd(&sub_cursor[c.sub_base + s], (unsigned long long)cnt);
                 run += cnt;
             }
         }
@@ -1985,6 +1993,10 @@ __global__ void __launch_bounds__(SP_THREADS) k_subpart_scatter(const unsigned l
                 s_sub[p] = (uint16_t)sub;
             }
         }
+        // destination of sorted index i of sub-bucket s: s_dst[s] + i
+#pragma unroll
+        for (uint32_t j = 0; j < SP_MAX_BINS; ++j)
+            if (j < per && b0 + j < c.n_sub) s_dst[b0 + j] = cur[j] - first[j];
         __syncthreads();
         for (uint32_t i = tid; i < n; i += SP_THREADS) {
             const unsigned long long d = s_dst[s_sub[i]] + i;
