@@ -251,24 +251,37 @@ Counters read_counters(const unsigned long long *d, cudaStream_t st)
 // between the device and pinned memory are asynchronous, so several
 // read-backs share one synchronisation and an upload does not stall the
 // host; a region is written by the host only before its copy is queued and
-// never reused.  The stream is drained before the blocks go back to the pool.
+// never reused within the job.  The blocks belong to the worker thread and
+// are reused job after job (no pinned allocation per job); the stream is
+// drained when the job's staging ends, before the next job reuses them.
 struct HostStage {
     cudaStream_t st;
-    std::vector<PinnedBlock> blocks;
-    size_t top = 0;
+    size_t blk = 0, top = 0;
+    bool used = false;
+    static std::vector<PinnedBlock> &blocks()
+    {
+        static thread_local std::vector<PinnedBlock> b;
+        return b;
+    }
     explicit HostStage(cudaStream_t s) : st(s) {}
     HostStage(const HostStage &) = delete;
     HostStage &operator=(const HostStage &) = delete;
     void *get(size_t bytes)
     {
         bytes = (bytes + 255) & ~size_t(255);
-        if (blocks.empty() || top + bytes > blocks.back().bytes) {
-            PinnedBlock b;
-            b.reset(std::max<size_t>(bytes, size_t(1) << 21));
-            blocks.push_back(std::move(b));
+        auto &bs = blocks();
+        while (blk < bs.size() && top + bytes > bs[blk].bytes) {
+            ++blk;
             top = 0;
         }
-        void *p = static_cast<uint8_t *>(blocks.back().p) + top;
+        if (blk == bs.size()) {
+            PinnedBlock b;
+            b.reset(std::max<size_t>(bytes, size_t(1) << 21));
+            bs.push_back(std::move(b));
+            top = 0;
+        }
+        used = true;
+        void *p = static_cast<uint8_t *>(bs[blk].p) + top;
         top += bytes;
         return p;
     }
@@ -287,7 +300,7 @@ struct HostStage {
     }
     ~HostStage()
     {
-        if (!blocks.empty()) cudaStreamSynchronize(st);
+        if (used) cudaStreamSynchronize(st);
     }
 };
 
