@@ -173,10 +173,15 @@ __device__ __forceinline__ KParams kparams(uint32_t k)
 // the previous segment's last position), the start of a roll along the
 // segment: for each next base c, fwd = fwd >> 2 | c << 62 and
 // rc = rc << 2 | (3 - c) << (64 - 2k), and the window's canonical word is
-// min(fwd & topmask, rc).  fwd has stale bits below bit 64 - 2k (dropped by
-// the mask); rc is exact.  The 128-bit value (cur:prev) shifted right by 2q0
-// puts the window's first base at bit 64 - 2k; the reverse complement is
-// (rprev:rcur) shifted right by 2k - 2q0 (left when negative), as below.
+// min(fwd & topmask, rc) (the smaller word, as GetKmer::canonicalize).  fwd
+// has stale bits below bit 64 - 2k (dropped by the mask); rc is exact.
+// prev/cur hold the 2-bit codes of the previous and current segments (base q
+// at bits 2q); the forward word puts base i of the window at bit 64-2k+2i (the
+// reference's kmer<1> layout), so the 128-bit value (cur:prev) shifted right
+// by 2q0 gives it.  rprev/rcur = pair_reverse(~codes) of the two segments: in
+// the 128-bit value (rprev:rcur) span position q sits at 2-bit group 63 - q,
+// so the reverse-complement word (complemented codes in reverse order) of the
+// window is that value shifted right by 2k - 2q0 (left when negative).
 __device__ __forceinline__ void window_words(uint64_t prev, uint64_t cur, uint64_t rprev, uint64_t rcur, uint32_t q0,
                                              const KParams &kp, uint64_t &fwd, uint64_t &rc)
 {
@@ -188,32 +193,6 @@ __device__ __forceinline__ void window_words(uint64_t prev, uint64_t cur, uint64
     else if (t >= 64) r = rprev;   // k = 32, q0 = 0
     else r = rcur << (-t);
     rc = r & kp.topmask;
-}
-
-// Canonical internal word of the window ending at position j (0..31) of the
-// current segment.  prev/cur hold the 2-bit codes of the previous and current
-// segments, base q at bits 2q.  The forward word puts base i of the window at
-// bit 64-2k+2i (the reference's kmer<1> layout); the reverse complement is the
-// 2-bit-group reversal with every code complemented.  The canonical word is
-// the smaller of the two, as GetKmer::canonicalize.
-// The reverse complement comes from the per-segment words rprev/rcur =
-// pair_reverse(~codes), computed once per segment: in the 128-bit value
-// (rprev:rcur) span position q sits at 2-bit group 63 - q, so the
-// reverse-complement word of the window starting at s is that value shifted
-// right by 64 - 2s (equal to pair_reverse(x) ^ topmask for the window x).
-__device__ __forceinline__ unsigned long long window_key_rc(uint64_t prev, uint64_t cur, uint64_t rprev,
-                                                            uint64_t rcur, uint32_t j, const KParams &kp)
-{
-    const int s = 33 + (int)j - (int)kp.k;
-    uint64_t x, rc;
-    if (s >= 32) x = cur >> (2 * (s - 32));
-    else x = (prev >> (2 * s)) | (cur << (64 - 2 * s));
-    if (s == 32) rc = rcur;
-    else if (s < 32) rc = (rcur >> (64 - 2 * s)) | (rprev << (2 * s));
-    else rc = rcur << (2 * s - 64);
-    const uint64_t fwd = (x & kp.kmask) << (kp.fwd_shift & 63);
-    rc &= kp.topmask;
-    return fwd < rc ? fwd : rc;
 }
 
 __device__ __forceinline__ void hll_add(uint32_t *regs, unsigned long long key)
@@ -539,8 +518,6 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
         __syncthreads();
 
         // windows of k valid bases ending in this thread's segment
-        const uint64_t prev = s_codes[tid], cur = s_codes[tid + 1];
-        const uint64_t rprev = s_rcodes[tid], rcur = s_rcodes[tid + 1];
         const uint64_t g = (uint64_t)s_good[tid] | ((uint64_t)s_good[tid + 1] << 32);
         uint32_t ends = run_ends(g, kp.k);
 
@@ -554,21 +531,63 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
             // tile, or a 1-in-2^n sample of the tiles) and the pre-pass
             // sample; otherwise only the windows are counted
             const bool census = a.bucket_hist && (t & a.bucket_sample_mask) == 0;
-            uint32_t e = (a.hll || census) ? ends : (ends & sample_ok);
-            uint32_t hll_base = sg.sample * HLL_M;
-            while (e) {
-                uint32_t j = __ffs(e) - 1;
-                e &= e - 1;
-                unsigned long long key = window_key_rc(prev, cur, rprev, rcur, j, kp);
-                if (hll_local) hll_add_shared(s_hll, key);
-                else if (a.hll) hll_add_sampled(a.hll + hll_base, key);
-                if (census) atomicAdd(&s_bhist[key >> 56], 1u);
-                if ((sample_ok >> j) & 1u) atomicAdd(&s_hist[key >> 56], 1u);
+            const uint32_t e = (a.hll || census) ? ends : (ends & sample_ok);
+            // the k-mers are formed per chunk of 8 positions holding such
+            // windows, rolled along the chunk, as in the staged modes (the
+            // chunk list goes to the tile buffer, free once classified)
+            uint32_t nq = 0;
+#pragma unroll
+            for (uint32_t q = 0; q < 4; ++q) nq += ((e >> (8 * q)) & 0xFFu) ? 1u : 0u;
+            uint32_t n_chunks;
+            const uint32_t coff = block_excl_scan(nq, s_warp, n_chunks);
+            uint32_t *s_chunk = reinterpret_cast<uint32_t *>(sbuf[s]);   // <= 4 * EXT_THREADS entries
+            {
+                uint32_t c = coff;
+#pragma unroll
+                for (uint32_t q = 0; q < 4; ++q) {
+                    const uint32_t e8 = (e >> (8 * q)) & 0xFFu;
+                    if (e8) s_chunk[c++] = ((uint32_t)tid << 10) | (q << 8) | e8;
+                }
+            }
+            __syncthreads();
+            const uint32_t hll_base = sg.sample * HLL_M;
+            for (uint32_t ci = tid; ci < n_chunks; ci += EXT_THREADS) {
+                const uint32_t ch = s_chunk[ci], e8 = ch & 0xFFu;
+                const uint32_t sgm = (ch >> 10) & 0xFFu, q0 = ((ch >> 8) & 3u) * 8;
+                uint32_t sok = 0;   // the chunk segment's pre-pass sample positions
+                if (a.prepass) {
+                    const uint64_t sp = fo + 32 * (uint64_t)sgm;
+                    if (sp < sg.sample_end) {
+                        const uint64_t lim = sg.sample_end - sp;
+                        sok = lim >= 32 ? FULL : ((1u << lim) - 1u);
+                    }
+                }
+                const uint64_t cseg = s_codes[sgm + 1];
+                uint64_t fwd, rc;
+                window_words(s_codes[sgm], cseg, s_rcodes[sgm], s_rcodes[sgm + 1], q0, kp, fwd, rc);
+                const uint32_t cw = (uint32_t)(cseg >> (2 * q0));
+#pragma unroll
+                for (uint32_t p = 0; p < 8; ++p) {
+                    const uint32_t cb = (cw >> (2 * p)) & 3u;
+                    fwd = (fwd >> 2) | ((uint64_t)cb << 62);
+                    rc = (rc << 2) | ((uint64_t)(cb ^ 3u) << kp.fwd_shift);
+                    if ((e8 >> p) & 1u) {
+                        const uint64_t f = fwd & kp.topmask;
+                        const unsigned long long key = f < rc ? f : rc;
+                        if (hll_local) hll_add_shared(s_hll, key);
+                        else if (a.hll) hll_add_sampled(a.hll + hll_base, key);
+                        if (census) atomicAdd(&s_bhist[key >> 56], 1u);
+                        if ((sok >> (q0 + p)) & 1u) atomicAdd(&s_hist[key >> 56], 1u);
+                    }
+                }
             }
             if (!a.visit || census) {
                 unsigned n = __reduce_add_sync(FULL, (unsigned)__popc(ends));
                 if (lane == 0 && n) atomicAdd(&a.occ[sg.sample], (unsigned long long)n);
             }
+            // the chunk list went into the tile buffer through the generic
+            // proxy; the next bulk copy into that buffer is an async-proxy write
+            fence_proxy_async_smem();
         } else {
             // the windows are emitted per chunk of 8 positions (a quarter of a
             // segment) holding at least one window end: the chunks of all
