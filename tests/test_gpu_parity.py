@@ -104,7 +104,8 @@ def test_job_matches_reference_tools(counter, kc, case):
     assert r.occurrences == sum(len(O.extract(f, case["k"])) for f in files)
 
 
-@pytest.mark.parametrize("name,k", [("plain_small", 31), ("repeat", 21), ("mixed", 21), ("edge", 25)])
+@pytest.mark.parametrize("name,k", [("plain_small", 31), ("repeat", 21), ("mixed", 21), ("edge", 25), ("edge", 5),
+                                    ("mixed", 11), ("plain_small", 32)])
 @pytest.mark.parametrize("min_count", [1, 2])
 def test_bloom_job_exact(counter, name, k, min_count):
     files = _case_files(name)
