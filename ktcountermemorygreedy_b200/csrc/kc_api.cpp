@@ -78,6 +78,10 @@ kc_tuning default_tuning()
     return t;
 }
 
+// Host inputs of a Bloom job from one file of at least this size are
+// uploaded in chunks that the census, SCAN and partition follow.
+constexpr uint64_t STREAMED_UPLOAD_MIN_BYTES = 512ull << 20;
+
 // k-mers per sub-bucket the shared-memory Bloom path starts from.  Its table
 // (SUB_TABLE_SLOTS, 4096) holds the distinct non-FIRST k-mers: at 30x
 // coverage with 1% errors about 1k of 24k, a quarter of the table; a
@@ -320,14 +324,24 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     static const bool trace_host = getenv("KC_TRACE") && getenv("KC_TRACE")[0] == '1';
     const double th_start = now_ms();
     std::vector<PinnedBlock> inflated;   // gzip files inflated on the host (kept until the job ends)
+    // a Bloom job's one large host file goes up in chunks while the census,
+    // SCAN and partition work on the chunks that have arrived (declared after
+    // the host and device buffers: it drains its copies before they go)
+    ChunkedUpload cu;
+    bool streamed = false;
     if (!in) {
         const std::vector<kc_buffer> files = inflate_inputs(job.files, inflated);
-        build_input(local, files.data(), (uint32_t)files.size(), st, &ds, tile_seg_host);
+        streamed = P.bloom && !exact_census && files.size() == 1 && files[0].size >= STREAMED_UPLOAD_MIN_BYTES;
+        build_input(local, files.data(), (uint32_t)files.size(), st, &ds, tile_seg_host, nullptr,
+                    streamed ? &cu : nullptr);
         in = &local;
         if (trace_host)
             fprintf(stderr, "[kc trace] job upload of %zu files enqueued after %.3f ms\n", job.files.size(),
                     now_ms() - th_start);
     }
+    // small uploads and read-backs through pinned staging: a pageable copy
+    // would hold the host (and, behind a streamed upload, wait for it)
+    HostStage hs(st);
     cudaEvent_t ev0, ev1;
     CK(cudaEventCreate(&ev0));
     CK(cudaEventCreate(&ev1));
@@ -354,7 +368,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
         n_chunks += (segs[i].len + PREPASS_CHUNK - 1) / PREPASS_CHUNK;
     }
     Seg *d_segs = ds.n<Seg>(std::max<uint32_t>(n_seg, 1));
-    if (n_seg) CK(cudaMemcpyAsync(d_segs, segs.data(), n_seg * sizeof(Seg), cudaMemcpyHostToDevice, st));
+    if (n_seg) CK(cudaMemcpyAsync(d_segs, hs.up(segs.data(), n_seg), n_seg * sizeof(Seg), cudaMemcpyHostToDevice, st));
 
     unsigned long long *counters = ds.n<unsigned long long>(C_COUNT);
     CK(cudaMemsetAsync(counters, 0, C_COUNT * 8, st));
@@ -364,9 +378,38 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     int32_t *tile_lastnl = ds.n<int32_t>(std::max<uint64_t>(T, 1));
     unsigned long long *tile_prefix = ds.n<unsigned long long>(std::max<uint64_t>(T, 1));
     unsigned long long *scan_tmp = ds.n<unsigned long long>(scan_tmp_words(std::max<uint64_t>(T, 1)));
+    // a streamed upload is censused chunk by chunk: the newline counts of the
+    // chunks that have arrived, then the line numbers of every tile so far
+    size_t chunks_done = 0;
+    uint64_t tiles_ready = streamed ? 0 : T;
+    auto census_chunks = [&](size_t upto) {
+        cu.enqueue(upto);   // (nothing when already queued)
+        for (; chunks_done < upto; ++chunks_done) {
+            const uint64_t t0 = chunks_done ? cu.tile_end[chunks_done - 1] : 0, t1 = cu.tile_end[chunks_done];
+            CK(cudaStreamWaitEvent(st, cu.ev[chunks_done], 0));
+            CK(launch_newlines(in->buf + t0 * TILE, t1 - t0, tile_nl + t0, tile_lastnl + t0, st));
+        }
+        tiles_ready = chunks_done ? cu.tile_end[chunks_done - 1] : 0;
+        CK(launch_scan_u32(tile_nl, tile_prefix, tiles_ready, scan_tmp, st));
+    };
     clk.begin(0);
-    CK(launch_newlines(in->buf, T, tile_nl, tile_lastnl, st));
-    CK(launch_scan_u32(tile_nl, tile_prefix, T, scan_tmp, st));
+    if (streamed) {
+        // first the chunks holding the pre-pass sample (with the 2 MiB chunks
+        // it ends in) and at least a quarter of the file: the bucket census
+        // and the Bloom sizing come from them
+        const uint64_t need = std::max<uint64_t>(
+            (segs[0].sample_end + PREPASS_CHUNK - 1) / PREPASS_CHUNK * PREPASS_CHUNK, in->total_bytes / 4);
+        size_t first = cu.ev.size();
+        for (size_t c = 0; c < cu.ev.size(); ++c)
+            if (cu.tile_end[c] * TILE >= need) {
+                first = c + 1;
+                break;
+            }
+        census_chunks(first);
+    } else {
+        CK(launch_newlines(in->buf, T, tile_nl, tile_lastnl, st));
+        CK(launch_scan_u32(tile_nl, tile_prefix, T, scan_tmp, st));
+    }
     clk.end();
 
     // ---- SCAN pass ---------------------------------------------------------
@@ -403,12 +446,13 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
             visit.reserve(T / (a.bucket_sample_mask + 1) + 1);
             for (uint32_t i = 0; i < n_seg; ++i) {
                 const uint64_t pre = (segs[i].sample_end + TILE - 1) / TILE;
-                for (uint64_t t = segs[i].first_tile; t < segs[i].first_tile + segs[i].n_tiles; ++t)
+                for (uint64_t t = segs[i].first_tile; t < segs[i].first_tile + segs[i].n_tiles && t < tiles_ready; ++t)
                     if ((t & a.bucket_sample_mask) == 0 || t - segs[i].first_tile < pre) visit.push_back((uint32_t)t);
             }
             uint32_t *d_visit = ds.n<uint32_t>(std::max<size_t>(visit.size(), 1));
             if (!visit.empty())
-                CK(cudaMemcpyAsync(d_visit, visit.data(), visit.size() * 4, cudaMemcpyHostToDevice, st));
+                CK(cudaMemcpyAsync(d_visit, hs.up(visit.data(), visit.size()), visit.size() * 4,
+                                   cudaMemcpyHostToDevice, st));
             a.visit = d_visit;
             a.n_visit = visit.size();
         }
@@ -417,10 +461,11 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
         prefix_hist = ds.n<uint32_t>(256);
         qual = ds.n<unsigned long long>(2);
         CK(cudaMemsetAsync(chunk_lastnl, 0xff, std::max<uint64_t>(n_chunks, 1) * 4, st));
-        CK(cudaMemcpyAsync(d_chunk0, seg_chunk0.data(), seg_chunk0.size() * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_chunk0, hs.up(seg_chunk0.data(), seg_chunk0.size()), seg_chunk0.size() * 8,
+                           cudaMemcpyHostToDevice, st));
         CK(cudaMemsetAsync(prefix_hist, 0, 256 * 4, st));
         CK(cudaMemsetAsync(qual, 0, 16, st));
-        CK(launch_chunk_lastnl(tile_lastnl, in->d_tile_seg, d_segs, d_chunk0, T, chunk_lastnl, st));
+        CK(launch_chunk_lastnl(tile_lastnl, in->d_tile_seg, d_segs, d_chunk0, tiles_ready, chunk_lastnl, st));
         a.prepass = 1;
         a.chunk_lastnl = chunk_lastnl;
         a.seg_chunk0 = d_chunk0;
@@ -437,7 +482,6 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     CK(launch_extract(MODE_SCAN, a, 0, st));
     clk.end();
     // the SCAN's results (and the bucket census) come back under one sync
-    HostStage hs(st);
     unsigned long long *p_occ = hs.n<unsigned long long>(1);
     uint32_t *p_hll = hs.n<uint32_t>(HLL_M);
     uint32_t *p_ph = hs.n<uint32_t>(256);
@@ -613,9 +657,10 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
         // SCAN counted the occurrences of the census tiles (all tiles when exact)
         if (sampled != O) throw KcError{KC_ERR_DEVICE, "bucket census does not add up to the occurrences"};
         if (!exact && sampled < 65536) throw CensusOverflow{};   // too thin a sample
-        // census tiles: t with (t & mask) == 0
+        // census tiles: t with (t & mask) == 0 among the tiles censused so far
         const double scale =
-            exact ? 1.0 : (double)T / (double)((T + a.bucket_sample_mask) / (a.bucket_sample_mask + 1));
+            exact ? 1.0
+                  : (double)T / (double)((tiles_ready + a.bucket_sample_mask) / (a.bucket_sample_mask + 1));
         for (uint32_t b = 0; b < N_BUCKETS; ++b)
             region[b] = exact ? bh[b] : (unsigned long long)std::ceil((double)bh[b] * scale * 1.15) + 8192;
         std::vector<uint64_t> fcap(N_BUCKETS, 0);
@@ -663,6 +708,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
             ranges.push_back({lo, N_BUCKETS});
         }
         const bool multi = ranges.size() > 1;
+        if (streamed && multi) census_chunks(cu.ev.size());   // every pass reads every tile
         std::vector<std::unique_ptr<HostRecords>> spilled;
         uint64_t spilled_total = 0, filled_total = 0;
         for (const auto &rg : ranges) {
@@ -716,7 +762,26 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
             a.bucket_lo = lo;
             a.bucket_hi = hi;
             clk.begin(2);
-            CK(launch_extract(MODE_PART, a, 0, st));
+            if (streamed && chunks_done < cu.ev.size()) {
+                // the rest of the file goes up behind this pass's small uploads;
+                // the tiles whose chunks have arrived are partitioned, then each
+                // later chunk once it has landed and has its line numbers
+                cu.enqueue(cu.ev.size());
+                a.tile0 = 0;
+                a.n_tiles = tiles_ready;
+                CK(launch_extract(MODE_PART, a, 0, st));
+                while (chunks_done < cu.ev.size()) {
+                    const uint64_t t0 = tiles_ready;
+                    census_chunks(chunks_done + 1);
+                    a.tile0 = t0;
+                    a.n_tiles = tiles_ready - t0;
+                    CK(launch_extract(MODE_PART, a, 0, st));
+                }
+                a.tile0 = 0;
+                a.n_tiles = T;
+            } else {
+                CK(launch_extract(MODE_PART, a, 0, st));
+            }
             clk.end();
             unsigned long long *p_fill = hs.n<unsigned long long>(N_BUCKETS);
             CK(cudaMemcpyAsync(p_fill, cursor, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));

@@ -334,9 +334,37 @@ void HostRecords::reset()
     n = 0;
 }
 
-void build_input(kc_input &in, const kc_buffer *files, uint32_t n_files, cudaStream_t st, DevScope *scope,
-                 std::vector<uint32_t> &tile_seg_host, const uint32_t *file_sample)
+void ChunkedUpload::enqueue(size_t upto)
 {
+    upto = std::min(upto, ev.size());
+    if (queued >= upto) return;
+    cudaEvent_t ready;
+    CK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    cudaError_t e = cudaEventRecord(ready, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, ready, 0);
+    cudaEventDestroy(ready);   // the wait keeps what it needs
+    CK(e);
+    for (; queued < upto; ++queued) {
+        const uint64_t t0 = queued ? tile_end[queued - 1] : 0, t1 = tile_end[queued];
+        const uint64_t b0 = t0 * TILE, b1 = std::min<uint64_t>(len, t1 * TILE);
+        if (b1 > b0) CK(cudaMemcpyAsync(dst + b0, src + b0, b1 - b0, cudaMemcpyHostToDevice, cs));
+        CK(cudaEventRecord(ev[queued], cs));
+    }
+}
+
+ChunkedUpload::~ChunkedUpload()
+{
+    if (cs) {
+        cudaStreamSynchronize(cs);
+        cudaStreamDestroy(cs);
+    }
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+}
+
+void build_input(kc_input &in, const kc_buffer *files, uint32_t n_files, cudaStream_t st, DevScope *scope,
+                 std::vector<uint32_t> &tile_seg_host, const uint32_t *file_sample, ChunkedUpload *chunked)
+{
+    if (chunked && n_files != 1) throw KcError{KC_ERR_INVALID, "a chunked upload takes one file"};
     in.segs.clear();
     in.sizes.clear();
     in.total_bytes = 0;
@@ -368,18 +396,36 @@ void build_input(kc_input &in, const kc_buffer *files, uint32_t n_files, cudaStr
     CK(cudaMemsetAsync(in.base, 0, FRONT_PAD, st));
     CK(cudaMemsetAsync(in.buf + tiles * (size_t)TILE, 0, 256, st));
     tile_seg_host.assign(std::max<uint64_t>(tiles, 1), 0);
+    for (uint32_t si = 0; si < in.segs.size(); ++si)
+        for (uint64_t t = 0; t < in.segs[si].n_tiles; ++t) tile_seg_host[in.segs[si].first_tile + t] = si;
+    // the small table goes before the file bytes: a pageable copy queued behind
+    // them would hold the host for the whole upload
+    CK(cudaMemcpyAsync(in.d_tile_seg, tile_seg_host.data(), tile_seg_host.size() * 4, cudaMemcpyHostToDevice, st));
     uint32_t si = 0;
     for (uint32_t f = 0; f < n_files; ++f) {
         if (files[f].size == 0) continue;
         const Seg &s = in.segs[si];
         uint8_t *dst = in.buf + s.first_tile * TILE;
-        CK(cudaMemcpyAsync(dst, files[f].data, files[f].size, cudaMemcpyHostToDevice, st));
+        if (chunked) {
+            // planned only: the job queues the copies (ChunkedUpload::enqueue)
+            CK(cudaStreamCreateWithFlags(&chunked->cs, cudaStreamNonBlocking));
+            chunked->st = st;
+            chunked->src = reinterpret_cast<const uint8_t *>(files[f].data);
+            chunked->dst = dst;
+            chunked->len = s.len;
+            for (uint64_t t0 = 0; t0 < s.n_tiles; t0 += CHUNKED_UPLOAD_TILES) {
+                cudaEvent_t e;
+                CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                chunked->ev.push_back(e);
+                chunked->tile_end.push_back(s.first_tile + std::min<uint64_t>(s.n_tiles, t0 + CHUNKED_UPLOAD_TILES));
+            }
+        } else {
+            CK(cudaMemcpyAsync(dst, files[f].data, files[f].size, cudaMemcpyHostToDevice, st));
+        }
         const uint64_t pad = s.n_tiles * TILE - s.len;
         if (pad) CK(cudaMemsetAsync(dst + s.len, 0, pad, st));
-        for (uint64_t t = 0; t < s.n_tiles; ++t) tile_seg_host[s.first_tile + t] = si;
         ++si;
     }
-    CK(cudaMemcpyAsync(in.d_tile_seg, tile_seg_host.data(), tile_seg_host.size() * 4, cudaMemcpyHostToDevice, st));
 }
 
 namespace {

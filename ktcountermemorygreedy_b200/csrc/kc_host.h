@@ -185,11 +185,38 @@ struct kc_input {
 
 namespace kc {
 
+// An upload of one file in chunks on its own stream: chunk c holds tiles
+// [c ? tile_end[c - 1] : 0, tile_end[c]) and is on the device once ev[c] has
+// completed, so the job's stream can wait for each chunk before working on
+// it.  build_input only plans the chunks; enqueue(upto) queues the copies of
+// the chunks before `upto` behind the work queued on the job's stream so far
+// (a small upload queued on the job's stream first is not held up behind the
+// file's bytes in the copy engine).  A chunk must be queued before the job's
+// stream waits for it.  The destructor drains the stream (the host data and
+// the device buffer must outlive it: declare it after both).
+struct ChunkedUpload {
+    cudaStream_t cs = nullptr, st = nullptr;
+    std::vector<cudaEvent_t> ev;
+    std::vector<uint64_t> tile_end;
+    const uint8_t *src = nullptr;
+    uint8_t *dst = nullptr;
+    uint64_t len = 0;
+    size_t queued = 0;
+    ChunkedUpload() = default;
+    ChunkedUpload(const ChunkedUpload &) = delete;
+    ChunkedUpload &operator=(const ChunkedUpload &) = delete;
+    void enqueue(size_t upto);   // throws KcError
+    ~ChunkedUpload();
+};
+constexpr uint64_t CHUNKED_UPLOAD_TILES = 16384;   // 128 MiB per chunk
+
 // Lays the files out tile-aligned in one device buffer.  When `scope` is
 // given the allocations belong to it (per-job upload), otherwise they are
 // long-lived (kc_input_upload).  `file_sample` (optional) assigns each file
-// to a sample.
+// to a sample.  With `chunked` (one file), the file's bytes are planned as
+// chunks for chunked->enqueue instead of one copy on st.
 void build_input(kc_input &in, const kc_buffer *files, uint32_t n_files, cudaStream_t st, DevScope *scope,
-                 std::vector<uint32_t> &tile_seg_host, const uint32_t *file_sample = nullptr);
+                 std::vector<uint32_t> &tile_seg_host, const uint32_t *file_sample = nullptr,
+                 ChunkedUpload *chunked = nullptr);
 
 }  // namespace kc

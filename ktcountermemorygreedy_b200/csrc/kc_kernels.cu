@@ -414,7 +414,7 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
     const uint64_t n_iter = (MODE == MODE_SCAN && a.visit) ? a.n_visit : a.n_tiles;
     uint64_t u = blockIdx.x;
     if (u >= n_iter) return;
-    uint64_t t = (MODE == MODE_SCAN && a.visit) ? (uint64_t)a.visit[u] : u;
+    uint64_t t = (MODE == MODE_SCAN && a.visit) ? (uint64_t)a.visit[u] : a.tile0 + u;
 
     if (tid == 0) {
         mbar_init(&mbar[0], 1);
@@ -441,12 +441,12 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
     uint32_t iter = 0;
     bool pending_next = false;
     for (; u < n_iter; u += gridDim.x, ++iter) {
-        t = (MODE == MODE_SCAN && a.visit) ? (uint64_t)a.visit[u] : u;
+        t = (MODE == MODE_SCAN && a.visit) ? (uint64_t)a.visit[u] : a.tile0 + u;
         const int s = iter & 1;
         const uint64_t un = u + gridDim.x;
         pending_next = un < n_iter;
         if (tid == 0 && pending_next) {
-            const uint64_t tn = (MODE == MODE_SCAN && a.visit) ? (uint64_t)a.visit[un] : un;
+            const uint64_t tn = (MODE == MODE_SCAN && a.visit) ? (uint64_t)a.visit[un] : a.tile0 + un;
             fence_proxy_async_smem();
             mbar_expect_tx(&mbar[s ^ 1], BUF_BYTES);
             bulk_load(sbuf[s ^ 1], a.buf + tn * TILE - HALO, BUF_BYTES, &mbar[s ^ 1]);

@@ -114,6 +114,7 @@ struct ExtractArgs {
     const uint32_t *visit;
     uint64_t n_visit;
     uint32_t bucket_lo, bucket_hi;            // PART keeps buckets lo <= b < hi (hi 0: all)
+    uint64_t tile0;                           // without visit: tiles tile0 .. tile0 + n_tiles - 1
     unsigned long long *bucket_cursor;        // 256 fill levels (PART)
     const unsigned long long *bucket_base;    // 256 start offsets in `list` (PART)
     const unsigned long long *bucket_end;     // 256 end offsets in `list` (PART)

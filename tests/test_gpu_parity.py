@@ -504,3 +504,26 @@ def test_bloom_shared_memory_tables_overflow_and_split(counter):
     assert r.smem_passes == 1 and r.smem_fallbacks == 0
     assert np.array_equal(r.keys, want_k) and np.array_equal(r.counts, want_c)
     assert r.distinct == len(O.exact_records(files, 31, U32)[0])
+
+
+def test_streamed_upload_counts_like_resident_input(kc):
+    """A Bloom job's single host file of 512 MiB or more goes up in 128 MiB
+    chunks that the census, the SCAN and the partition follow (bucket regions
+    from the first chunks' census); the results equal those of the same input
+    uploaded first and counted from device memory."""
+    import ktcountermemorygreedy_b200.synth as S
+    g = S.genome(91, 20_000_000)
+    fq = S.reads(g, 91, 1_900_000, (150, 150), 0.01, 0.0).tobytes()
+    assert len(fq) >= 512 << 20
+    with kc.KmerCounter(max_inflight_jobs=1) as c:
+        inp = c.upload([fq])
+        try:
+            for mc in (2, 1):
+                kw = dict(k=31, count_max=U32, bloom=True, memory_gb=8, min_count=mc, hist_max=2000)
+                host = c.count([fq], **kw)
+                dev = c.count(input=inp, **kw)
+                for f in ("keys", "counts", "hist"):
+                    assert np.array_equal(getattr(host, f), getattr(dev, f)), (mc, f)
+                assert (host.occurrences, host.distinct) == (dev.occurrences, dev.distinct)
+        finally:
+            c.free_input(inp)
