@@ -97,64 +97,333 @@ struct TmpDir {
     std::vector<uint64_t> low_keys;
 };
 
+// Record geometry of a tmp_dir, from infos.bin: a k-mer takes kb bytes (full
+// words, then the tail bytes of the last word), a high.bin record kb +
+// count_bytes (src/main.cpp:590-615, src/FinalDrainWriter.h:71-88).
+struct Layout {
+    uint32_t k = 0, count_max = 0, count_bytes = 4;
+    uint32_t full = 0, tail_bytes = 0, kb = 0, rec = 0;
+    uint64_t high_bytes = 0, low_bytes = 0;   // file sizes (read_layout)
+    uint64_t n_high() const { return high_bytes / rec; }
+    uint64_t n_low() const { return low_bytes / kb; }
+};
+
+inline bool read_infos(const std::string &dir, Layout &L, std::string &err)
+{
+    std::vector<char> b;
+    if (!read_file(dir + "infos.bin", b) || b.size() < 8) { err = "failed to read " + dir + "infos.bin"; return false; }
+    std::memcpy(&L.k, b.data(), 4);
+    std::memcpy(&L.count_max, b.data() + 4, 4);
+    L.count_bytes = count_bytes_for(L.count_max);
+    if (L.k == 0 || L.k > 128) { err = "invalid k_len from infos.bin: " + std::to_string(L.k); return false; }
+    if (L.k > 32) { err = "k_len " + std::to_string(L.k) + " is above 32, which this build does not support"; return false; }
+    L.tail_bytes = (2 * (L.k % 32) + 7) / 8;
+    L.full = L.k / 32;
+    L.kb = L.full * 8 + L.tail_bytes;
+    L.rec = L.kb + L.count_bytes;
+    return true;
+}
+
+// The k-mer word of one packed k-mer (the inverse of the reference's packing).
+inline uint64_t decode_key(const char *r, const Layout &L)
+{
+    uint64_t w = 0;
+    if (L.full) std::memcpy(&w, r, 8);
+    else std::memcpy(reinterpret_cast<char *>(&w) + (8 - L.tail_bytes), r, L.tail_bytes);
+    return w;
+}
+
 // infos.bin, high.bin, low.bin as written by the reference counter
 // (src/main.cpp:590-615, src/FinalDrainWriter.h:71-88, src/ExportWriter.h:296-313)
 // and read by its tools (tool/histogram_tool.cpp:239-366).
 inline bool read_tmpdir(const std::string &dir, TmpDir &t, std::string &err)
 {
+    Layout L;
+    if (!read_infos(dir, L, err)) return false;
+    t.k = L.k;
+    t.count_max = L.count_max;
+    t.count_bytes = L.count_bytes;
     std::vector<char> b;
-    if (!read_file(dir + "infos.bin", b) || b.size() < 8) { err = "failed to read " + dir + "infos.bin"; return false; }
-    std::memcpy(&t.k, b.data(), 4);
-    std::memcpy(&t.count_max, b.data() + 4, 4);
-    t.count_bytes = count_bytes_for(t.count_max);
-    if (t.k == 0 || t.k > 128) { err = "invalid k_len from infos.bin: " + std::to_string(t.k); return false; }
-    if (t.k > 32) { err = "k_len " + std::to_string(t.k) + " is above 32, which this build does not support"; return false; }
-    const uint32_t tail_bytes = (2 * (t.k % 32) + 7) / 8, full = t.k / 32;
-    const uint32_t kb = full * 8 + tail_bytes, rec = kb + t.count_bytes;
     if (!read_file(dir + "high.bin", b)) { err = "failed to open " + dir + "high.bin"; return false; }
     if (b.empty()) { err = "empty high.bin file"; return false; }
-    if (b.size() % rec) { err = "invalid high.bin file size"; return false; }
-    size_t n = b.size() / rec;
+    if (b.size() % L.rec) { err = "invalid high.bin file size"; return false; }
+    size_t n = b.size() / L.rec;
     t.high_keys.resize(n);
     t.high_counts.resize(n);
     for (size_t i = 0; i < n; ++i) {
-        const char *r = b.data() + i * rec;
-        uint64_t w = 0;
-        if (full) std::memcpy(&w, r, 8);
-        else std::memcpy(reinterpret_cast<char *>(&w) + (8 - tail_bytes), r, tail_bytes);
+        const char *r = b.data() + i * L.rec;
         uint32_t c = 0;
-        std::memcpy(&c, r + kb, t.count_bytes);
-        t.high_keys[i] = w;
+        std::memcpy(&c, r + L.kb, L.count_bytes);
+        t.high_keys[i] = decode_key(r, L);
         t.high_counts[i] = c;
     }
     if (!read_file(dir + "low.bin", b)) { err = "failed to open " + dir + "low.bin"; return false; }
-    if (b.size() % kb) { err = "invalid low.bin size"; return false; }
-    n = b.size() / kb;
+    if (b.size() % L.kb) { err = "invalid low.bin size"; return false; }
+    n = b.size() / L.kb;
     t.low_keys.resize(n);
-    for (size_t i = 0; i < n; ++i) {
-        uint64_t w = 0;
-        if (full) std::memcpy(&w, b.data() + i * kb, 8);
-        else std::memcpy(reinterpret_cast<char *>(&w) + (8 - tail_bytes), b.data() + i * kb, tail_bytes);
-        t.low_keys[i] = w;
+    for (size_t i = 0; i < n; ++i) t.low_keys[i] = decode_key(b.data() + i * L.kb, L);
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Segmented mode: records that do not fit in max_memory_gb
+// ---------------------------------------------------------------------------
+//
+// The reference tools fall back to a streaming histogram over segments of
+// high.bin (tool/histogram_tool.cpp:510-600, :801-813) and to a dump over
+// hash partitions written to tmp_dir and merged afterwards
+// (tool/dump_tool.cpp:938-1110, :1280-1290; tool/Partition.h:472-655) when
+// their estimated peak memory exceeds max_memory_gb.  Here a segment is a
+// contiguous range of the k-mers' first bases in printed-string order: every
+// k-mer's high.bin and low.bin parts fall in the same segment, each segment is
+// merged on its own, and the segments' sorted records follow one another in
+// the dump's order, so nothing is written to tmp_dir and nothing is merged
+// afterwards.  A counting pass over the files plans the segments; each
+// segment then reads the files again and keeps its own records.
+
+constexpr uint32_t SEG_LEAD_BASES = 8;                    // first bases that place a k-mer (4^8 ranges)
+constexpr uint64_t SEG_BLOCK_BYTES = 1ull << 20;          // file read block
+constexpr uint64_t SEG_SLACK_BYTES = 4ull << 20;
+
+inline uint32_t lead_bases(uint32_t k) { return std::min<uint32_t>(k, SEG_LEAD_BASES); }
+
+// The first m bases of the printed k-mer as a number, base 0 most significant
+// (base i of the printed string sits at bit 64 - 2k + 2i of the word).
+inline uint32_t lead_prefix(uint64_t w, uint32_t k, uint32_t m)
+{
+    uint32_t p = 0;
+    const uint32_t s0 = 64 - 2 * k;
+    for (uint32_t i = 0; i < m; ++i) p = (p << 2) | (uint32_t)((w >> (s0 + 2 * i)) & 3);
+    return p;
+}
+
+inline std::string prefix_string(uint32_t p, uint32_t m)
+{
+    std::string s(m, 'A');
+    for (uint32_t i = 0; i < m; ++i) s[m - 1 - i] = "ACGT"[(p >> (2 * i)) & 3];
+    return s;
+}
+
+// infos.bin plus the sizes of high.bin and low.bin, with read_tmpdir's checks.
+inline bool read_layout(const std::string &dir, Layout &L, std::string &err)
+{
+    if (!read_infos(dir, L, err)) return false;
+    struct stat sh, sl;
+    if (::stat((dir + "high.bin").c_str(), &sh) != 0 || !S_ISREG(sh.st_mode)) {
+        err = "failed to open " + dir + "high.bin";
+        return false;
+    }
+    if (sh.st_size == 0) { err = "empty high.bin file"; return false; }
+    if ((uint64_t)sh.st_size % L.rec) { err = "invalid high.bin file size"; return false; }
+    if (::stat((dir + "low.bin").c_str(), &sl) != 0 || !S_ISREG(sl.st_mode)) {
+        err = "failed to open " + dir + "low.bin";
+        return false;
+    }
+    if ((uint64_t)sl.st_size % L.kb) { err = "invalid low.bin size"; return false; }
+    L.high_bytes = (uint64_t)sh.st_size;
+    L.low_bytes = (uint64_t)sl.st_size;
+    return true;
+}
+
+// Calls f(key, count) for every record of high.bin (low = false) or every
+// k-mer of low.bin (low = true, count 0), reading whole records in blocks.
+template <class F>
+inline bool scan_file(const std::string &dir, const Layout &L, bool low, F &&f, std::string &err)
+{
+    const std::string path = dir + (low ? "low.bin" : "high.bin");
+    const uint64_t rec = low ? L.kb : L.rec;
+    FILE *fp = std::fopen(path.c_str(), "rb");
+    if (!fp) { err = "failed to open " + path; return false; }
+    std::vector<char> buf((size_t)(SEG_BLOCK_BYTES / rec * rec));
+    const uint64_t total = low ? L.low_bytes : L.high_bytes;
+    uint64_t done = 0;
+    while (done < total) {
+        const size_t want = (size_t)std::min<uint64_t>(buf.size(), total - done);
+        if (std::fread(buf.data(), 1, want, fp) != want) {
+            std::fclose(fp);
+            err = "failed to read " + path;
+            return false;
+        }
+        for (size_t o = 0; o < want; o += rec) {
+            uint32_t c = 0;
+            if (!low) std::memcpy(&c, buf.data() + o + L.kb, L.count_bytes);
+            f(decode_key(buf.data() + o, L), c);
+        }
+        done += want;
+    }
+    std::fclose(fp);
+    return true;
+}
+
+struct Segment {
+    uint32_t p0 = 0, p1 = 0;            // lead prefixes [p0, p1)
+    uint64_t n_high = 0, n_low = 0;
+};
+
+// Host bytes of one merge: per high.bin record, per low.bin k-mer (0 when
+// low.bin is not read), and fixed (read block, prefix counts, histogram, slack).
+struct SegCost {
+    uint64_t per_high = 0, per_low = 0, fixed = 0;
+};
+
+inline SegCost seg_cost(uint32_t k, bool dump, bool with_low, uint64_t hist_bins)
+{
+    SegCost c;
+    // input keys + counts; dump: output keys + counts and the text line (k bases, tab,
+    // at most 10 digits, newline)
+    const uint64_t out = dump ? 12 + (uint64_t)k + 12 : 0;
+    c.per_high = 12 + out;
+    c.per_low = with_low ? 8 + out : 0;
+    const uint64_t prefixes = 1ull << (2 * lead_bases(k));
+    c.fixed = SEG_SLACK_BYTES + SEG_BLOCK_BYTES + 2 * prefixes * 8 + hist_bins * 16;
+    return c;
+}
+
+// Contiguous prefix ranges, each as large as fits in `budget` bytes.  False
+// (with the prefix that alone does not fit in *worst) when no plan fits.
+inline bool plan_segments(const std::vector<uint64_t> &ph, const std::vector<uint64_t> &pl, const SegCost &c,
+                          uint64_t budget, std::vector<Segment> &out, uint32_t *worst)
+{
+    out.clear();
+    if (budget <= c.fixed) {
+        if (worst) *worst = ~0u;
+        return false;
+    }
+    const uint64_t room = budget - c.fixed;
+    Segment s;
+    uint64_t used = 0;
+    for (uint32_t p = 0; p < (uint32_t)ph.size(); ++p) {
+        const uint64_t b = ph[p] * c.per_high + pl[p] * c.per_low;
+        if (b > room) {
+            if (worst) *worst = p;
+            return false;
+        }
+        if (used + b > room) {
+            s.p1 = p;
+            out.push_back(s);
+            s = Segment{};
+            s.p0 = p;
+            used = 0;
+        }
+        used += b;
+        s.n_high += ph[p];
+        s.n_low += pl[p];
+    }
+    s.p1 = (uint32_t)ph.size();
+    out.push_back(s);
+    return true;
+}
+
+// Counting pass: records per lead prefix in high.bin and (with_low) low.bin.
+inline bool count_prefixes(const std::string &dir, const Layout &L, bool with_low, std::vector<uint64_t> &ph,
+                           std::vector<uint64_t> &pl, std::string &err)
+{
+    const uint32_t m = lead_bases(L.k);
+    ph.assign((size_t)1 << (2 * m), 0);
+    pl.assign((size_t)1 << (2 * m), 0);
+    if (!scan_file(dir, L, false, [&](uint64_t w, uint32_t) { ++ph[lead_prefix(w, L.k, m)]; }, err)) return false;
+    if (with_low && !scan_file(dir, L, true, [&](uint64_t w, uint32_t) { ++pl[lead_prefix(w, L.k, m)]; }, err))
+        return false;
+    return true;
+}
+
+// Reads segment s's records: high.bin keys and counts, low.bin keys (with_low).
+inline bool load_segment(const std::string &dir, const Layout &L, bool with_low, const Segment &s,
+                         std::vector<uint64_t> &hk, std::vector<uint32_t> &hc, std::vector<uint64_t> &lk,
+                         std::string &err)
+{
+    const uint32_t m = lead_bases(L.k);
+    hk.clear();
+    hc.clear();
+    lk.clear();
+    hk.reserve(s.n_high);
+    hc.reserve(s.n_high);
+    if (!scan_file(dir, L, false,
+                   [&](uint64_t w, uint32_t c) {
+                       const uint32_t p = lead_prefix(w, L.k, m);
+                       if (p >= s.p0 && p < s.p1) {
+                           hk.push_back(w);
+                           hc.push_back(c);
+                       }
+                   },
+                   err))
+        return false;
+    if (with_low) {
+        lk.reserve(s.n_low);
+        if (!scan_file(dir, L, true,
+                       [&](uint64_t w, uint32_t) {
+                           const uint32_t p = lead_prefix(w, L.k, m);
+                           if (p >= s.p0 && p < s.p1) lk.push_back(w);
+                       },
+                       err))
+            return false;
     }
     return true;
 }
 
-// "KMER\tcount\n" lines (tool/dump_tool.cpp:1172-1193), formatted on the
-// device (kc_dump_text) into pinned host memory, then written out.
-inline bool write_dump(const std::string &path, const uint64_t *keys, const uint32_t *counts, uint64_t n, uint32_t k,
-                       std::string &err)
+// Why no segment plan fits (return code 2, as the reference's tools give
+// when even their largest partition count does not fit).
+inline std::string no_fit_message(const Layout &L, const std::vector<uint64_t> &ph, const std::vector<uint64_t> &pl,
+                                  const SegCost &c, uint32_t worst, uint64_t budget)
 {
+    if (worst == ~0u)
+        return "insufficient memory: max_memory_bytes=" + std::to_string(budget) + " is below the " +
+               std::to_string(c.fixed) + " bytes every segment needs";
+    const uint64_t b = c.fixed + ph[worst] * c.per_high + pl[worst] * c.per_low;
+    return "insufficient memory: the " + std::to_string(ph[worst] + pl[worst]) + " records whose k-mers start with " +
+           prefix_string(worst, lead_bases(L.k)) + " need " + std::to_string(b) + " bytes, more than max_memory_bytes=" +
+           std::to_string(budget);
+}
+
+// max_memory_gb in bytes (tool/histogram_tool.cpp:157-174: GiB, fractions allowed).
+inline uint64_t memory_bytes(double gib)
+{
+    const long double b = (long double)gib * (long double)(1ull << 30);
+    return b >= 18446744073709551615.0L ? ~0ull : (uint64_t)b;
+}
+
+// "KMER\tcount\n" lines (tool/dump_tool.cpp:1172-1193), formatted on the
+// device (kc_dump_text) into pinned host memory (*buf, kc_host_free it).
+inline bool format_dump(const uint64_t *keys, const uint32_t *counts, uint64_t n, uint32_t k, void *&buf,
+                        uint64_t &got, std::string &err)
+{
+    buf = nullptr;
+    got = 0;
     uint64_t need = 0;
     if (kc_dump_text(keys, counts, n, k, nullptr, 0, &need) != KC_OK) { err = kc_last_error(); return false; }
-    void *buf = nullptr;
-    if (need && kc_host_alloc(need, &buf) != KC_OK) { err = kc_last_error(); return false; }
-    uint64_t got = 0;
+    if (need && kc_host_alloc(need, &buf) != KC_OK) {
+        buf = nullptr;
+        err = kc_last_error();
+        return false;
+    }
     if (need && kc_dump_text(keys, counts, n, k, static_cast<char *>(buf), need, &got) != KC_OK) {
         err = kc_last_error();
         kc_host_free(buf);
+        buf = nullptr;
         return false;
     }
+    return true;
+}
+
+// The dump lines of one segment, appended to an open file.
+inline bool append_dump(FILE *f, const uint64_t *keys, const uint32_t *counts, uint64_t n, uint32_t k,
+                        std::string &err)
+{
+    void *buf = nullptr;
+    uint64_t got = 0;
+    if (!format_dump(keys, counts, n, k, buf, got, err)) return false;
+    const bool ok = !got || std::fwrite(buf, 1, got, f) == got;
+    if (buf) kc_host_free(buf);
+    if (!ok) err = "failed to write the dump";
+    return ok;
+}
+
+inline bool write_dump(const std::string &path, const uint64_t *keys, const uint32_t *counts, uint64_t n, uint32_t k,
+                       std::string &err)
+{
+    void *buf = nullptr;
+    uint64_t got = 0;
+    if (!format_dump(keys, counts, n, k, buf, got, err)) return false;
     FILE *f = std::fopen(path.c_str(), "wb");
     if (!f) {
         err = "failed to open " + path;

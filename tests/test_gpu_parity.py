@@ -461,6 +461,71 @@ def test_cli_round_trip():
         assert hashlib.sha256(open(o, "rb").read()).hexdigest() == case["dump_sha256"]
 
 
+def _segment_budget_gb(k, dump, with_low, n_high, n_low, hist_bins, parts):
+    """A max_memory_gb that makes the tools merge in about `parts` segments:
+    their host bytes per high.bin record, per low.bin k-mer and fixed
+    (seg_cost in ktcountermemorygreedy_b200/cli/cli_common.h)."""
+    out = 24 + k if dump else 0
+    per_high, per_low = 12 + out, (8 + out) if with_low else 0
+    fixed = (4 << 20) + (1 << 20) + 2 * 4 ** min(k, 8) * 8 + hist_bins * 16
+    return (fixed + (n_high * per_high + n_low * per_low) // parts) / 2 ** 30
+
+
+def test_tools_segmented_mode_matches_whole_and_exact_counts():
+    """histogram_tool and dump_tool given a max_memory_gb too small for all
+    records merge them in segments of the k-mers' first bases: the outputs
+    are byte-identical to the whole-file path's and equal the exact counts
+    (precise) or the high.bin counts (approximate).  The tmp_dir is split like
+    the reference counter's: each k-mer in high.bin, low.bin or both."""
+    import re
+    from test_tool_segments_host import write_tmpdir
+    bin_dir = os.path.join(ROOT, "ktcountermemorygreedy_b200", "bin")
+    rng = np.random.default_rng(11)
+    k = 31
+    uk, uc = O.count(O.extract_files(_case_files("plain_small"), k))
+    in_low = rng.random(len(uk)) < 0.6
+    high_part = uc.astype(np.int64) - in_low
+    hm = high_part > 0
+    with tempfile.TemporaryDirectory() as tmp:
+        for cm in (U32, 255):
+            d = os.path.join(tmp, f"t{cm}")
+            hk, hc = uk[hm], high_part[hm].clip(0, cm).astype(np.uint32)
+            write_tmpdir(d, k, cm, hk, hc, uk[in_low])
+            for tool, mode in (("histogram_tool", "precise"), ("histogram_tool", "approximate"),
+                               ("dump_tool", "precise"), ("dump_tool", "approximate")):
+                dump, with_low = tool == "dump_tool", mode == "precise"
+                tail = ["2", str(U32), "--sort"] if dump else ["1", "10000"]
+                small = _segment_budget_gb(k, dump, with_low, len(hk), int(in_low.sum()), 0 if dump else 10000, 4)
+                outs = []
+                for mem in ("64", repr(small)):
+                    o = os.path.join(tmp, f"{tool}_{mode}_{cm}_{len(outs)}")
+                    p = subprocess.run([os.path.join(bin_dir, tool), mode, d, "8", mem, o] + tail,
+                                       capture_output=True, text=True)
+                    assert p.returncode == 0, p.stderr
+                    seg = re.search(r"Segmented mode: \d+ high records in (\d+) segment", p.stdout)
+                    if outs:
+                        assert seg and int(seg.group(1)) >= 2, p.stdout
+                    else:
+                        assert seg is None
+                    outs.append(open(o, "rb").read())
+                assert outs[0] == outs[1]
+                if with_low:
+                    want_k, want_c = O.sort_string_order(uk, np.minimum(uc, cm).astype(np.uint32), k)
+                else:
+                    want_k, want_c = O.sort_string_order(hk, hc, k)
+                if dump:
+                    m = want_c >= 2
+                    assert outs[0] == O.dump_text(want_k[m], want_c[m], k)
+                else:
+                    got = [int(line.split(b"\t")[1]) for line in outs[0].splitlines()]
+                    assert got == O.histogram(want_c, 1, 10000).tolist()
+        # below the fixed need of a segment: the reference tools' "insufficient memory" exit code
+        for tool in ("histogram_tool", "dump_tool"):
+            p = subprocess.run([os.path.join(bin_dir, tool), "precise", os.path.join(tmp, f"t{U32}"), "8", "0.001",
+                                os.path.join(tmp, "x")], capture_output=True, text=True)
+            assert p.returncode == 2 and "insufficient memory" in p.stderr
+
+
 def test_bloom_shared_memory_path_matches_global_path(kc):
     """Bloom jobs with min count >= 2 count each filter sub-bucket in shared
     memory; the global-memory path (bloom_smem=2) and the oracle give the same
