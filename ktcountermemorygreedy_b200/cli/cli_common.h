@@ -7,6 +7,7 @@
 #include <sys/stat.h>
 
 #include <algorithm>
+#include <cerrno>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -375,11 +376,19 @@ inline std::string no_fit_message(const Layout &L, const std::vector<uint64_t> &
            std::to_string(budget);
 }
 
-// max_memory_gb in bytes (tool/histogram_tool.cpp:157-174: GiB, fractions allowed).
-inline uint64_t memory_bytes(double gib)
+// max_memory_gb in bytes: GiB, fractions allowed, the whole argument a
+// positive number (tool/histogram_tool.cpp:157-174, tool/dump_tool.cpp:476-491).
+// 0 = ok, 1 = not a positive number, 2 = more bytes than 64 bits hold.
+inline int parse_memory_gib(const char *s, uint64_t &bytes)
 {
-    const long double b = (long double)gib * (long double)(1ull << 30);
-    return b >= 18446744073709551615.0L ? ~0ull : (uint64_t)b;
+    char *end = nullptr;
+    errno = 0;
+    const long double v = std::strtold(s, &end);
+    if (errno || !end || *end || end == s || !(v > 0.0L)) return 1;
+    const long double b = v * (long double)(1ull << 30);
+    if (b > 18446744073709551615.0L) return 2;
+    bytes = (uint64_t)b;
+    return 0;
 }
 
 // "KMER\tcount\n" lines (tool/dump_tool.cpp:1172-1193), formatted on the

@@ -76,8 +76,11 @@ int main(int argc, char **argv)
     else { std::cerr << "mode must be precise or approximate\n"; return 255; }
     uint32_t threads = 0, lo = 1, hi = 0xffffffffu;
     if (!cli::parse_u32(argv[3], threads) || threads == 0) { std::cerr << "invalid max_threads\n"; return 255; }
-    double mem = std::atof(argv[4]);
-    if (!(mem > 0)) { std::cerr << "invalid max_memory_gb: " << argv[4] << '\n'; return 255; }
+    uint64_t budget = 0;
+    if (const int e = cli::parse_memory_gib(argv[4], budget)) {
+        std::cerr << (e == 1 ? std::string("invalid max_memory_gb: ") + argv[4] : "max_memory_gb too large") << '\n';
+        return 255;
+    }
     int next = 6;
     if (argc > next && argv[next][0] != '-') { if (!cli::parse_u32(argv[next++], lo)) { std::cerr << "invalid min_freq\n"; return 255; } }
     if (argc > next && argv[next][0] != '-') { if (!cli::parse_u32(argv[next++], hi)) { std::cerr << "invalid max_freq\n"; return 255; } }
@@ -88,7 +91,6 @@ int main(int argc, char **argv)
     if (!cli::read_layout(dir, L, err)) { std::cerr << err << '\n'; return 255; }
     // all records at once: the larger file's bytes, every decoded record, and
     // the merged records with their text
-    const uint64_t budget = cli::memory_bytes(mem);
     const uint64_t n_out = L.n_high() + (precise ? L.n_low() : 0);
     const uint64_t whole = std::max(L.high_bytes, L.low_bytes) + 12 * L.n_high() + 8 * L.n_low() +
                            (24 + (uint64_t)L.k) * n_out + cli::seg_cost(L.k, true, precise, 0).fixed;

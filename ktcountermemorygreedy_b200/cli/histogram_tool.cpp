@@ -64,8 +64,12 @@ int main(int argc, char **argv)
     }
     uint32_t threads = 0, lo = 1, hi = 10000;
     if (!cli::parse_u32(argv[3], threads)) { std::cerr << "invalid max_threads" << std::endl; return 255; }
-    double mem = std::atof(argv[4]);
-    if (!(mem > 0)) { std::cerr << "invalid max_memory_gb: " << argv[4] << std::endl; return 255; }
+    uint64_t budget = 0;
+    if (const int e = cli::parse_memory_gib(argv[4], budget)) {
+        std::cerr << (e == 1 ? std::string("invalid max_memory_gb: ") + argv[4] : "max_memory_gb is too large")
+                  << std::endl;
+        return 255;
+    }
     if (argc >= 7 && !cli::parse_u32(argv[6], lo)) { std::cerr << "invalid min_freq" << std::endl; return 255; }
     if (argc >= 8 && !cli::parse_u32(argv[7], hi)) { std::cerr << "invalid max_freq" << std::endl; return 255; }
     if (threads == 0) { std::cerr << "invalid max_threads: must be greater than 0" << std::endl; return 255; }
@@ -75,7 +79,6 @@ int main(int argc, char **argv)
     cli::Layout L;
     if (!cli::read_layout(dir, L, err)) { std::cerr << err << std::endl; return 255; }
     // all records at once: the larger file's bytes, then every decoded record
-    const uint64_t budget = cli::memory_bytes(mem);
     const uint64_t whole = std::max(L.high_bytes, L.low_bytes) + 12 * L.n_high() + 8 * L.n_low() +
                            cli::seg_cost(L.k, false, precise, (uint64_t)hi - lo + 1).fixed;
     if (whole > budget) return segmented(dir, L, precise, lo, hi, whole, budget, argv[5]);

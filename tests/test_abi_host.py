@@ -107,6 +107,15 @@ def test_cli_argument_validation():
     dt = os.path.join(PKG, "bin", "dump_tool")
     r = _run([dt, "precise", "/tmp", "4", "1", "o.txt", "5", "3"])
     assert r.returncode == 255 and "max_freq < min_freq" in r.stderr
+    # max_memory_gb: the whole argument a positive number of GiB
+    for tool in (ht, dt):
+        for bad in ("1abc", "0", "-2", "", "x"):
+            r = _run([tool, "precise", "/tmp", "4", bad, "o.txt"])
+            assert r.returncode == 255 and f"invalid max_memory_gb: {bad}" in r.stderr
+        r = _run([tool, "precise", "/tmp", "4", "1e30", "o.txt"])
+        assert r.returncode == 255 and "too large" in r.stderr
+        r = _run([tool, "precise", "/nonexistent_dir", "4", "0.5", "o.txt"])
+        assert r.returncode == 255 and "infos.bin" in r.stderr
 
 
 def test_generator_is_deterministic_across_thread_counts():
