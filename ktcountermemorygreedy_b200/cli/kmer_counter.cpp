@@ -37,8 +37,11 @@ int main(int argc, char **argv)
         std::cerr << "n_thread must be >= 6" << std::endl;
         return 255;
     }
-    map_cap = std::max<uint32_t>(1024, map_cap);
-    if (map_cap >= 16u * 1024 * 1024 || fmax < fmin || cmax == 0) return usage(argv[0]);
+    // rounded up to a power of two, at least 1024, below 16M (src/main.cpp:541, :581)
+    uint64_t map_pow2 = 1;
+    while (map_pow2 < map_cap) map_pow2 <<= 1;
+    map_pow2 = std::max<uint64_t>(1024, map_pow2);
+    if (map_pow2 >= 16ull * 1024 * 1024 || fmax < fmin || cmax == 0) return usage(argv[0]);
     if (k == 0 || k > 128) {
         std::cerr << "k_len must be <= 128" << std::endl;
         return 1;

@@ -97,6 +97,8 @@ def test_cli_argument_validation():
     assert r.returncode == 255 and "n_thread must be >= 6" in r.stderr
     assert _run([kmc, "x.fq", "31", "8", "1", "/tmp", "1024", "5", "3"]).returncode == 1   # filter_max < filter_min
     assert _run([kmc, "x.fq", "31", "8", "1", "/tmp", "1024", "2", "9", "0"]).returncode == 1   # count_max 0
+    # map_capacity is rounded up to a power of two before the 16M limit (src/main.cpp:541, :581)
+    assert _run([kmc, "x.fq", "31", "8", "1", "/tmp", "9000000"]).returncode == 1
     r = _run([kmc, "x.fq", "40", "8", "1", "/tmp"])
     assert r.returncode == 1 and "above 32" in r.stderr
     ht = os.path.join(PKG, "bin", "histogram_tool")
