@@ -51,6 +51,20 @@ int main(int argc, char **argv)
         return 1;
     }
     const std::string tmp = cli::with_slash(argv[5]);
+    // infos.bin first, before any input is read (src/main.cpp:588-595)
+    {
+        FILE *f = std::fopen((tmp + "infos.bin").c_str(), "wb");
+        if (!f) {
+            std::cerr << "Open infos.bin failed : " << std::strerror(errno) << std::endl;
+            return 1;
+        }
+        const uint32_t info[2] = {k, cmax};
+        const bool ok = std::fwrite(info, sizeof(info), 1, f) == 1;
+        if ((std::fclose(f) != 0) || !ok) {
+            std::cerr << "Write infos.bin failed" << std::endl;
+            return 1;
+        }
+    }
     auto names = cli::input_files(argv[1]);
     if (names.empty()) {
         std::cerr << "No input files" << std::endl;

@@ -101,6 +101,9 @@ def test_cli_argument_validation():
     assert _run([kmc, "x.fq", "31", "8", "1", "/tmp", "9000000"]).returncode == 1
     r = _run([kmc, "x.fq", "40", "8", "1", "/tmp"])
     assert r.returncode == 1 and "above 32" in r.stderr
+    # infos.bin is written before any input is read (src/main.cpp:588-595)
+    r = _run([kmc, "x.fq", "31", "8", "1", "/nonexistent_dir"])
+    assert r.returncode == 1 and "Open infos.bin failed" in r.stderr
     ht = os.path.join(PKG, "bin", "histogram_tool")
     r = _run([ht, "fuzzy", "/tmp", "4", "1", "o.tsv"])
     assert r.returncode == 255 and "invalid mode" in r.stderr
