@@ -3,7 +3,9 @@ torch.distributed.run with the gloo backend, world size 2. Each rank counts
 its own replica of the workload (no collective on the data path); the only
 collectives are the barrier around the timed region and the reductions that
 turn per-rank device times and k-mer counts into the whole-job figure (the
-slowest rank's time, the sum of the ranks' k-mers)."""
+slowest rank's time, the sum of the ranks' k-mers). The reference arm runs
+on rank 0 alone, and times the oracle's port where the reference programs
+are absent."""
 import json
 import os
 import socket
@@ -54,6 +56,18 @@ def test_two_gloo_ranks_reduce_to_slowest_time_and_total_kmers(tmp_path):
         assert row["t_max"] == pytest.approx(107.5)
         assert row["occ"] == pytest.approx(3000.0)
         assert row["value"] == pytest.approx(3000.0 / 0.1075)
+
+
+def test_reference_arm_times_the_oracle_port_without_the_reference_programs():
+    env = dict(os.environ, KC_REF_BIN="/nonexistent_dir", CUDA_VISIBLE_DEVICES="")
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--ref-reads", "2000"], env=env, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr[-2000:]
+    line = json.loads(p.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "k-mers/s"
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] == 1
+    assert line["e2e"] == {"value": line["value"], "unit": "k-mers/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
 
 
 def test_reference_arm_runs_on_rank_zero_only():
