@@ -117,7 +117,7 @@ inline bool read_infos(const std::string &dir, Layout &L, std::string &err)
     std::memcpy(&L.count_max, b.data() + 4, 4);
     L.count_bytes = count_bytes_for(L.count_max);
     if (L.k == 0 || L.k > 128) { err = "invalid k_len from infos.bin: " + std::to_string(L.k); return false; }
-    if (L.k > 32) { err = "k_len " + std::to_string(L.k) + " is above 32, which this build does not support"; return false; }
+    if (L.k > 32) { err = "k_len " + std::to_string(L.k) + " is above 32; k-mers of more than 32 bases are not supported"; return false; }
     L.tail_bytes = (2 * (L.k % 32) + 7) / 8;
     L.full = L.k / 32;
     L.kb = L.full * 8 + L.tail_bytes;

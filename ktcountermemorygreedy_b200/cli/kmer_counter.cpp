@@ -47,7 +47,7 @@ int main(int argc, char **argv)
         return 1;
     }
     if (k > 32) {
-        std::cerr << "k_len " << k << " is above 32, which this build does not support" << std::endl;
+        std::cerr << "k_len " << k << " is above 32; k-mers of more than 32 bases are not supported" << std::endl;
         return 1;
     }
     const std::string tmp = cli::with_slash(argv[5]);
