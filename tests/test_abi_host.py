@@ -44,6 +44,33 @@ def test_python_binding_covers_the_header():
     kc.lib()   # binds every signature
 
 
+def test_binding_structs_have_the_header_layout(tmp_path):
+    """Every struct the binding passes through the C ABI has the size and the
+    field offsets that the C compiler gives include/kc.h."""
+    import ktcountermemorygreedy_b200 as kc
+    structs = [kc.kc_config, kc.kc_tuning, kc.kc_buffer, kc.kc_job, kc.kc_result_t]
+    src = ["#include <stdio.h>", "#include <stddef.h>", '#include "kc.h"', "int main(void) {"]
+    for S in structs:
+        n = S.__name__
+        src.append(f'printf("{n} sizeof %zu\\n", sizeof({n}));')
+        for f in S._fields_:
+            src.append(f'printf("{n} {f[0]} %zu\\n", offsetof({n}, {f[0]}));')
+    src.append("return 0; }")
+    c = tmp_path / "layout.c"
+    c.write_text("\n".join(src))
+    exe = str(tmp_path / "layout")
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(c), "-o", exe], check=True)
+    got = {}
+    for line in subprocess.run([exe], check=True, capture_output=True, text=True).stdout.splitlines():
+        n, field, v = line.split()
+        got[(n, field)] = int(v)
+    for S in structs:
+        n = S.__name__
+        assert got[(n, "sizeof")] == ctypes.sizeof(S), n
+        for f in S._fields_:
+            assert got[(n, f[0])] == getattr(S, f[0]).offset, (n, f[0])
+
+
 @pytest.mark.parametrize("rec", GOLDEN["prepass"], ids=lambda r: r["name"])
 def test_host_bloom_sizing_matches_reference(rec):
     import ktcountermemorygreedy_b200 as kc
