@@ -33,6 +33,18 @@ WORKER = textwrap.dedent("""
 """)
 
 
+FAILING_WORKER = textwrap.dedent("""
+    import os, sys, time
+    sys.path.insert(0, {root!r})
+    import bench
+    world, rank, local = bench.dist_setup(None)
+    if rank == 1:
+        raise RuntimeError("replica 1 failed before the timed region")
+    bench.barrier(world)          # rank 0 waits here for a rank that is gone
+    time.sleep(600)
+""")
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -56,6 +68,17 @@ def test_two_gloo_ranks_reduce_to_slowest_time_and_total_kmers(tmp_path):
         assert row["t_max"] == pytest.approx(107.5)
         assert row["occ"] == pytest.approx(3000.0)
         assert row["value"] == pytest.approx(3000.0 / 0.1075)
+
+
+def test_a_failing_replica_ends_the_job_instead_of_leaving_the_others_waiting(tmp_path):
+    import time
+    script = tmp_path / "failing.py"
+    script.write_text(FAILING_WORKER.format(root=ROOT))
+    t0 = time.monotonic()
+    p = _torchrun(str(script), 2)
+    assert p.returncode != 0
+    assert "replica 1 failed" in p.stderr + p.stdout
+    assert time.monotonic() - t0 < 120
 
 
 def test_reference_arm_times_the_oracle_port_without_the_reference_programs():
