@@ -178,9 +178,10 @@ def reference_programs_present() -> bool:
                for p in ("kmer_counter", "histogram_tool", "dump_tool"))
 
 
-def reference_run(fastq_path: str, threads: int, mem_gb: int, tmp: str):
-    """kmer_counter + histogram_tool precise + dump_tool precise --sort, as the
-    reference is used; returns (wall seconds, occurrences)."""
+def reference_run(fastq_path: str, threads: int, mem_gb: int, tmp: str, dump: bool = True):
+    """kmer_counter + histogram_tool precise (min 2) + dump_tool precise --sort
+    (min 1), as the reference is used; returns (wall seconds, occurrences).
+    The histogram is left in tmp/h.tsv and the dump in tmp/d.txt."""
     ref = reference_dir()
     d = os.path.join(tmp, "t")
     shutil.rmtree(d, ignore_errors=True)
@@ -192,8 +193,9 @@ def reference_run(fastq_path: str, threads: int, mem_gb: int, tmp: str):
         raise RuntimeError(f"reference kmer_counter failed: {p.stderr[-500:]}")
     subprocess.run([os.path.join(ref, "histogram_tool"), "precise", d, str(threads), str(mem_gb),
                     os.path.join(tmp, "h.tsv"), "2", "10000"], check=True, capture_output=True)
-    subprocess.run([os.path.join(ref, "dump_tool"), "precise", d, str(threads), str(mem_gb),
-                    os.path.join(tmp, "d.txt"), "1", str(U32), "--sort"], check=True, capture_output=True)
+    if dump:
+        subprocess.run([os.path.join(ref, "dump_tool"), "precise", d, str(threads), str(mem_gb),
+                        os.path.join(tmp, "d.txt"), "1", str(U32), "--sort"], check=True, capture_output=True)
     wall = time.perf_counter() - t0
     occ = 0
     for line in p.stdout.splitlines():
@@ -229,15 +231,24 @@ def cpu_sample_run(path: str, threads: int, mem_gb: int, tmp: str):
     return w, occ, "port", 1, "oracle port (extraction, exact counts, sort, histogram), one thread"
 
 
+GEN = os.path.join(ROOT, "ktcountermemorygreedy_b200", "bin", "fastq_gen")
+
+
+def write_workload(path: str, n_reads: int, first_read: int = 0, genome_bp: int = 100_000_000) -> int:
+    """Reads first_read .. first_read + n_reads - 1 of the large job's stream
+    written to `path` by the generator program (a separate process: the
+    caller maps no library of this project).  Returns the file's size."""
+    if not os.access(GEN, os.X_OK):
+        raise RuntimeError(f"{GEN} is missing; build it with __graft_entry__.build()")
+    subprocess.run([GEN, "large", str(genome_bp), str(first_read), str(n_reads), path], check=True)
+    return os.path.getsize(path)
+
+
 def reference_sample(sample_reads: int, tmp: str):
     """First `sample_reads` reads of the large job's stream (same genome and
     read generator) written to a file."""
-    import ktcountermemorygreedy_b200.synth as S
-    g = S.large_job_genome(100_000_000)
-    fq = S.reads(g, 2, sample_reads, (150, 150), 0.01, 0.0)
     path = os.path.join(tmp, "sample.fq")
-    fq.tofile(path)
-    return path, len(fq)
+    return path, write_workload(path, sample_reads)
 
 
 def cpu_info():
@@ -278,6 +289,95 @@ def run_reference_arm(args):
         "e2e": {"value": value, "unit": "k-mers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# CPU leg of our arm: the reference's programs timed on a sample of the
+# workload, and the parity checks of what the GPU counted (the oracle and the
+# reference programs are the checkers here; nothing of this is timed as ours
+# except the GPU's own runs on the sample)
+# ---------------------------------------------------------------------------
+
+def _checker():
+    for p in (os.path.join(ROOT, "tests"), os.path.join(ROOT, "tests", "golden")):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    import size_parity
+    return size_parity
+
+
+def sample_on_gpu(counter, kc, path: str, reps: int = 3):
+    """The GPU on the same sample file as the CPU baseline: device-resident
+    k-mers/s (CUDA events) and end to end from pinned host memory (host
+    clock), and the records + histogram of one run."""
+    import ctypes as C
+    import numpy as np
+    size = os.path.getsize(path)
+    p = C.c_void_p()
+    kc._check(kc.lib().kc_host_alloc(size, C.byref(p)))
+    buf = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint8)), shape=(size,))
+    buf[:] = np.fromfile(path, np.uint8)
+    inp = counter.upload([buf])
+    dev, occ = [], 0
+    for i in range(reps + 2):
+        r = counter.count(input=inp, keep_records=False, **JOB)
+        if i >= 2:
+            dev.append(r.device_ms)
+            occ = r.occurrences
+    counter.free_input(inp)
+    walls = []
+    res = None
+    for i in range(reps + 2):
+        res = None
+        t0 = time.perf_counter()
+        res = counter.count([buf], keep_records=True, **JOB)
+        if i >= 2:
+            walls.append(time.perf_counter() - t0)
+    kc.lib().kc_host_free(p)
+    value = {"device": occ / (statistics.median(dev) / 1000.0), "e2e": occ / statistics.median(walls),
+             "unit": "k-mers/s", "occurrences": occ,
+             "note": "the GPU on the cpu_baseline sample file (same bytes), median of "
+                     f"{reps}: device-resident (CUDA events) and from pinned host memory (host clock)"}
+    return value, res
+
+
+def cpu_leg(args, counter, fq, full):
+    import ktcountermemorygreedy_b200 as kc
+    SP = _checker()
+    threads, model = cpu_info()
+    mem = int(os.environ.get("KC_REF_MEM_GB", "32"))
+    cpu = sample_value = None
+    parity = {}
+    try:
+        with tempfile.TemporaryDirectory() as tmp:
+            path, nbytes = reference_sample(args.ref_reads, tmp)
+            w, o, kind, cores, what = cpu_sample_run(path, max(6, threads), mem, tmp)
+            cpu = {"value": o / w, "unit": "k-mers/s", "cores": cores, "kind": kind,
+                   "sample": f"first {args.ref_reads} reads of the workload ({nbytes} B, {o} k-mers), "
+                             f"{what}, {model}"}
+            sample_value, res = sample_on_gpu(counter, kc, path)
+            if kind == "reference":
+                chk = SP.reference_outputs_match(kc.histogram_text(res.hist, JOB["hist_min"]),
+                                                 kc.dump_bytes(res.keys, res.counts, JOB["k"]),
+                                                 os.path.join(tmp, "h.tsv"), os.path.join(tmp, "d.txt"),
+                                                 JOB["k"], JOB["min_count"])
+                parity["sample"] = "identical" if chk["identical"] else "DIFFERENT"
+                parity["sample_detail"] = chk
+            else:
+                parity["sample"] = "not checked (the reference programs are absent)"
+    except Exception as e:   # the baseline is reported, never required
+        cpu = cpu or {"value": None, "unit": "k-mers/s", "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
+        parity.setdefault("sample", f"failed: {e}")
+    try:
+        if full is None:
+            full = counter.count([fq], keep_records=True, copy=False, **JOB)
+        chk = SP.full_spot_check(fq, JOB["k"], full.keys, full.counts, full.hist, JOB["hist_min"],
+                                 JOB["min_count"], threads=max(1, threads))
+        parity["full"] = "identical" if chk["identical"] else "DIFFERENT"
+        parity["full_detail"] = chk
+    except Exception as e:
+        parity["full"] = f"failed: {e}"
+    return cpu, parity, sample_value
 
 
 # ---------------------------------------------------------------------------
@@ -480,6 +580,7 @@ def run_ours(args):
 
     # end to end through the C ABI from pinned host buffers
     e2e_val, h2d, d2h = None, 0, 0
+    last_full = None
     if args.e2e_steps > 0:
         walls, occ_e = [], 0
         r = None
@@ -491,13 +592,15 @@ def run_ours(args):
             r = counter.count([fq], keep_records=True, copy=False, **JOB)
             del r
         d2h = 0
-        for _ in range(args.e2e_steps):
+        for i in range(args.e2e_steps):
+            last_full = None   # its pinned block goes back to the pool before the next job
             t0 = time.perf_counter()
             r = counter.count([fq], keep_records=True, copy=False, **JOB)
             walls.append(time.perf_counter() - t0)
             occ_e += r.occurrences
             d2h = len(r.keys) * 12 + r.hist.nbytes
-            del r   # the caller is done with the records: their pinned block goes back to the pool
+            last_full = r   # the last job's records are checked below, outside the timed steps
+            del r
         h2d = len(fq)
         w = max_over_ranks(sum(walls), world)
         e2e_val = sum_over_ranks(occ_e, world) / w
@@ -533,20 +636,10 @@ def run_ours(args):
                    "frac_of_dram_peak": rate / pk_dram, "frac_of_l2_peak": rate / pk_l2,
                    "note": "one slot-key read and one count atomicAdd per non-FIRST occurrence"}
 
-    cpu = None
+    cpu = parity = sample_value = None
     if rank == 0 and world == 1 and args.cpu_baseline:
-        try:
-            threads, model = cpu_info()
-            with tempfile.TemporaryDirectory() as tmp:
-                path, nbytes = reference_sample(args.ref_reads, tmp)
-                w, o, kind, cores, what = cpu_sample_run(path, max(6, threads),
-                                                         int(os.environ.get("KC_REF_MEM_GB", "32")), tmp)
-            cpu = {"value": o / w, "unit": "k-mers/s", "cores": cores, "kind": kind,
-                   "sample": f"first {args.ref_reads} reads of the workload ({nbytes} B, {o} k-mers), "
-                             f"{what}, {model}"}
-        except Exception as e:   # the baseline is reported, never required
-            cpu = {"value": None, "unit": "k-mers/s", "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
-
+        cpu, parity, sample_value = cpu_leg(args, counter, fq, last_full)
+    last_full = None
     counter.free_input(inp)
     counter.close()
     kc.lib().kc_host_free(pinned)
@@ -567,7 +660,8 @@ def run_ours(args):
                        "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (FASTQ > 126 MB)",
                        "memory_gb": MEMORY_GB, "scale": args.scale, "tuning": tuning},
             "e2e": {"value": e2e_val, "unit": "k-mers/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": int(launches),
+            "roofline": roof, "cpu_baseline": cpu, "sample_value": sample_value, "parity": parity,
+            "clocks": clocks, "gpu_launches": int(launches),
             "stages": stages, "atomics": atomics, "served": served, "batched": batched,
         }
         print(json.dumps(line), flush=True)

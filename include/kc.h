@@ -226,8 +226,12 @@ int kc_sort_records(uint64_t *keys, uint32_t *counts, uint64_t n, uint32_t bits)
  * 13 MiB device array inside libkc.so that every GPU loading the library holds
  * until the process exits, so n is limited to KC_SORT_NOALLOC_MAX records
  * (larger n is rejected with KC_ERR_INVALID).  The first call on a device
- * looks up that array's device address (cudaGetSymbolAddress) with the device
- * current; make that first call before capturing a stream into a graph.  All
+ * does a one-time set-up with the device current: it looks up that array's
+ * device address (cudaGetSymbolAddress) and loads the array and the sort
+ * kernels onto the device (with CUDA's default lazy module loading they would
+ * otherwise be loaded, taking device memory, at first use); a call with n = 0
+ * does only this set-up.  Make that first call before any stream capture.
+ * Every call waits for its sort to finish on `stream` before returning.  All
  * calls share the one array: calls that overlap on the GPU (another host
  * thread, another stream) race and must be serialized by the caller. */
 #define KC_SORT_NOALLOC_MAX (1u << 20)

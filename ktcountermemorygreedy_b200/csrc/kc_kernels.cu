@@ -2666,6 +2666,22 @@ __global__ void k_single_segment_tiles(SortTile *tiles, uint64_t n, uint64_t n_t
     }
 }
 
+// Under lazy module loading a kernel's code is loaded (device memory taken)
+// at its first launch; querying each kernel's attributes loads them now.
+cudaError_t preload_sort_in_scratch()
+{
+    cudaFuncAttributes fa;
+    const void *fns[] = {reinterpret_cast<const void *>(k_single_segment_tiles),
+                         reinterpret_cast<const void *>(k_radix_count), reinterpret_cast<const void *>(k_radix_scatter),
+                         reinterpret_cast<const void *>(k_scan_reduce), reinterpret_cast<const void *>(k_scan_top),
+                         reinterpret_cast<const void *>(k_scan_down)};
+    for (const void *f : fns) {
+        const cudaError_t e = cudaFuncGetAttributes(&fa, f);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 cudaError_t launch_radix_sort_in_scratch(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits,
                                          void *tmp, cudaStream_t st)
 {

@@ -252,6 +252,9 @@ cudaError_t launch_compact_chunks(const Slot *slots, const SampleCfg *cfg, const
 // from tmp (sort_tmp_bytes_in_scratch(n) bytes) and nothing copied from the
 // host (digit counts, a scan and a scatter per pass).
 size_t sort_tmp_bytes_in_scratch(uint64_t n);
+// Loads the kernels launch_radix_sort_in_scratch uses (lazy module loading
+// would otherwise load them, and take device memory, at their first launch).
+cudaError_t preload_sort_in_scratch();
 cudaError_t launch_radix_sort_in_scratch(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits,
                                          void *tmp, cudaStream_t st);
 

@@ -10,11 +10,16 @@
 // sorts the caller's device arrays in place and takes its working memory from
 // a fixed array compiled into the library instead of allocating it.
 //
-// The scratch array is a file-scope __device__ array of KC_SORT_NOALLOC_SCRATCH
-// bytes.  Every GPU that loads libkc.so holds it until the process exits.  In
-// host code its name is only a host-side stand-in, not a device address, so
-// the address is looked up with cudaGetSymbolAddress once per device, with
-// that device current, on the first call made on that device.
+// The scratch array is a file-scope __device__ array of 13 MiB.  In host code
+// its name is only a host-side stand-in, not a device address, so the address
+// is looked up with cudaGetSymbolAddress once per device, with that device
+// current, on the first call made on that device.  With CUDA's lazy module
+// loading (the default) a module's code and __device__ arrays are placed in
+// device memory when the module is first used, so that first call also loads
+// the module of this file (the array) and the sort kernels it launches; from
+// then on the array and the kernels stay loaded on that device until the
+// process exits, and no later call loads or allocates anything.  A call with
+// n = 0 does only this set-up and can serve as a warm-up.
 #include <cuda_runtime.h>
 
 #include <array>
@@ -38,8 +43,8 @@ constexpr int MAX_DEVICES = 64;
 std::mutex g_mu;
 std::array<void *, MAX_DEVICES> g_scratch_ptr{};
 
-// Device address of the scratch array on the current device (looked up on the
-// first call for that device).
+// Device address of the scratch array on the current device (looked up, and
+// the sort kernels loaded, on the first call for that device).
 int scratch_for_current_device(void **out)
 {
     int dev = -1;
@@ -57,6 +62,11 @@ int scratch_for_current_device(void **out)
             cudaGetLastError();
             return kc::set_error(KC_ERR_CUDA, std::string("cudaGetSymbolAddress of the sort scratch failed: ") +
                                                   cudaGetErrorString(e));
+        }
+        e = kc::preload_sort_in_scratch();
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return kc::set_error(KC_ERR_CUDA, std::string("loading the sort kernels failed: ") + cudaGetErrorString(e));
         }
         g_scratch_ptr[dev] = p;
     }
@@ -86,6 +96,7 @@ extern "C" int kc_sort_records_noalloc(uint64_t *d_keys, uint32_t *d_counts, uin
     // digit counts, offsets and records it later reads
     cudaError_t e =
         kc::launch_radix_sort_in_scratch(reinterpret_cast<unsigned long long *>(d_keys), d_counts, n, bits, scratch, st);
+    // the call returns once the records are sorted
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         cudaGetLastError();

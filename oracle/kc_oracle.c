@@ -123,6 +123,44 @@ uint64_t kco_extract(const uint8_t *data, uint64_t len, uint32_t k,
 }
 
 /*
+ * Spot-check sample of the occurrences of one file: the same record splitting
+ * and extraction as kco_extract, keeping only the canonical k-mers whose
+ * sample hash has its low `sample_bits` bits zero.  The sample hash is the
+ * splitmix64 finaliser, unrelated to every hash on the counting path (Bloom
+ * block, table slots, buckets), so the kept k-mers fall in every bucket and
+ * filter slice, and every occurrence of a kept k-mer is kept: their exact
+ * counts are the full job's counts of those k-mers.
+ */
+uint64_t kco_sample_hash(uint64_t w)
+{
+    w ^= w >> 30;
+    w *= 0xbf58476d1ce4e5b9ULL;
+    w ^= w >> 27;
+    w *= 0x94d049bb133111ebULL;
+    return w ^ (w >> 31);
+}
+
+uint64_t kco_extract_sampled(const uint8_t *data, uint64_t len, uint32_t k, uint32_t sample_bits,
+                             uint64_t *out, uint64_t cap)
+{
+    const uint64_t smask = sample_bits >= 64 ? ~0ULL : ((1ULL << sample_bits) - 1ULL);
+    roll_t r;
+    roll_init(&r, k);
+    uint64_t line = 0, n = 0;
+    for (uint64_t i = 0; i < len; ++i) {
+        uint8_t c = data[i];
+        if (c == '\n') { line++; roll_clear(&r); continue; }
+        if ((line & 3) != 1) continue;
+        uint64_t canon;
+        if (roll_push(&r, c, &canon) && (kco_sample_hash(canon) & smask) == 0) {
+            if (n < cap) out[n] = canon;
+            n++;
+        }
+    }
+    return n;
+}
+
+/*
  * Pre-pass (FastqPreReader::pre_read :98-136, parse_loop :218-288,
  * FastqPrefixCounter::process_block :124-132).  The reader pulls 2 MiB chunks
  * until the limit is reached.  A quality line is summed only from the start of

@@ -32,6 +32,14 @@ extern "C" {
 uint64_t kco_extract(const uint8_t *data, uint64_t len, uint32_t k,
                      uint64_t *out, uint64_t cap);
 
+/* Spot-check sample: kco_extract keeping only k-mers w with
+ * (kco_sample_hash(w) & (2^sample_bits - 1)) == 0 -- every occurrence of a
+ * kept k-mer, so their counts are exact.  The input must start at a record
+ * start (a file, or a split point between two records). */
+uint64_t kco_sample_hash(uint64_t w);
+uint64_t kco_extract_sampled(const uint8_t *data, uint64_t len, uint32_t k, uint32_t sample_bits,
+                             uint64_t *out, uint64_t cap);
+
 /* Pre-pass statistics over the first `sample_limit` bytes of one file:
  * root-prefix histogram (top 8 bits of each canonical k-mer) and the sum and
  * count of quality bytes of complete quality lines. */

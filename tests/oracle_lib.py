@@ -24,6 +24,8 @@ def lib():
         vp, u32, u64, u8 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint8
         sig = {
             "kco_extract": (u64, [vp, u64, u32, vp, u64]),
+            "kco_sample_hash": (u64, [u64]),
+            "kco_extract_sampled": (u64, [vp, u64, u32, u32, vp, u64]),
             "kco_prepass": (None, [vp, u64, u32, u64, vp, U64P, U64P]),
             "kco_count_sorted": (u64, [vp, u64, vp, vp]),
             "kco_sort_records_string_order": (None, [vp, vp, u64, u32]),
@@ -65,6 +67,49 @@ def extract(data: bytes, k: int) -> np.ndarray:
     out = np.zeros(cap, np.uint64)
     n = lib().kco_extract(P(buf), len(data), k, P(out), cap)
     return out[:n].copy()
+
+
+def sample_hash_np(keys: np.ndarray) -> np.ndarray:
+    """kco_sample_hash of every word (the splitmix64 finaliser), vectorised."""
+    w = np.ascontiguousarray(keys, np.uint64).copy()
+    with np.errstate(over="ignore"):
+        w ^= w >> np.uint64(30)
+        w *= np.uint64(0xbf58476d1ce4e5b9)
+        w ^= w >> np.uint64(27)
+        w *= np.uint64(0x94d049bb133111eb)
+        w ^= w >> np.uint64(31)
+    return w
+
+
+def sampled_mask(keys: np.ndarray, sample_bits: int) -> np.ndarray:
+    return (sample_hash_np(keys) & np.uint64((1 << sample_bits) - 1)) == 0
+
+
+def extract_sampled(buf: np.ndarray, k: int, sample_bits: int, splits=None, threads: int = 1) -> np.ndarray:
+    """Occurrences of the sampled k-mers (kco_extract_sampled) of one FASTQ
+    held in the uint8 array `buf`.  `splits` are byte offsets of record starts
+    (ascending, inside buf); the pieces between them are extracted on
+    `threads` threads (ctypes releases the GIL) and concatenated."""
+    import concurrent.futures as cf
+    buf = np.ascontiguousarray(buf, np.uint8)
+    bounds = [0] + [int(x) for x in (splits or []) if 0 < int(x) < len(buf)] + [len(buf)]
+    L = lib()
+    base = buf.ctypes.data
+
+    def one(i):
+        a, b = bounds[i], bounds[i + 1]
+        # occurrences <= bytes of the piece; the sample keeps about 2^-bits of them
+        cap = max(1024, ((b - a) >> max(0, sample_bits - 2)) + 4096)
+        while True:
+            out = np.zeros(cap, np.uint64)
+            n = L.kco_extract_sampled(C.c_void_p(base + a), b - a, k, sample_bits, P(out), cap)
+            if n <= cap:
+                return out[:n]
+            cap = int(n)
+
+    with cf.ThreadPoolExecutor(max_workers=max(1, threads)) as ex:
+        parts = list(ex.map(one, range(len(bounds) - 1)))
+    return np.concatenate(parts) if parts else np.zeros(0, np.uint64)
 
 
 def extract_files(files, k):

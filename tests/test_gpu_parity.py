@@ -592,3 +592,80 @@ def test_streamed_upload_counts_like_resident_input(kc):
                 assert (host.occurrences, host.distinct) == (dev.occurrences, dev.distinct)
         finally:
             c.free_input(inp)
+
+
+REF_BIN = os.environ.get("KC_REF_BIN") or os.path.join(ROOT, "oracle", "_ref")
+GEN = os.path.join(ROOT, "ktcountermemorygreedy_b200", "bin", "fastq_gen")
+
+
+def _ref_programs():
+    progs = [os.path.join(REF_BIN, p) for p in ("kmer_counter", "histogram_tool", "dump_tool")]
+    if not all(os.access(p, os.X_OK) for p in progs):
+        pytest.skip("the reference programs (oracle/_ref) are not built here")
+    return progs
+
+
+def test_large_job_sample_matches_reference_programs(counter, kc):
+    """The benchmarked job's settings (k = 31, the reference's Bloom split and
+    sizing, min count 2, u32 counts) on the first 60k reads of its read stream:
+    the histogram text and the count >= 2 part of the sorted dump equal the
+    reference programs' own outputs on the same file."""
+    import size_parity as SP
+    kcnt, htool, dtool = _ref_programs()
+    with tempfile.TemporaryDirectory() as tmp:
+        fq = os.path.join(tmp, "s.fq")
+        subprocess.run([GEN, "large", "100000000", "0", "60000", fq], check=True)
+        d = os.path.join(tmp, "t")
+        os.makedirs(d)
+        subprocess.run([kcnt, fq, "31", "6", "2", d, "1024", "2", str(U32), str(U32)], check=True,
+                       capture_output=True)
+        subprocess.run([htool, "precise", d, "6", "2", os.path.join(tmp, "h.tsv"), "2", "10000"], check=True,
+                       capture_output=True)
+        subprocess.run([dtool, "precise", d, "6", "2", os.path.join(tmp, "d.txt"), "1", str(U32), "--sort"],
+                       check=True, capture_output=True)
+        data = np.fromfile(fq, np.uint8)
+        r = counter.count([data], k=31, count_max=U32, bloom=True, memory_gb=64, min_count=2, hist_min=2,
+                          hist_max=10000)
+        chk = SP.reference_outputs_match(kc.histogram_text(r.hist, 2), kc.dump_bytes(r.keys, r.counts, 31),
+                                         os.path.join(tmp, "h.tsv"), os.path.join(tmp, "d.txt"), 31, 2)
+        assert chk["histogram_identical"]
+        assert chk["dump_identical"], chk
+        assert chk["dump_lines"] == len(r.keys) > 0
+        # and the size-independent checks the benchmark applies to the full job
+        full = SP.full_spot_check(data, 31, r.keys, r.counts, r.hist, 2, 2, threads=4, sample_bits=3)
+        assert full["identical"], full
+
+
+def test_reference_tools_read_our_tmpdir():
+    """The unmodified reference tools (compiled from the reference's sources)
+    run on the tmp_dir our kmer_counter writes (infos.bin, exact counts in
+    high.bin, empty low.bin): their precise histogram and sorted dump equal
+    the golden outputs the reference produced from its own tmp_dir."""
+    _, htool, dtool = _ref_programs()
+    bin_dir = os.path.join(ROOT, "ktcountermemorygreedy_b200", "bin")
+    for name, k, cm in (("multi", 31, U32), ("repeat", 21, 255), ("repeat", 31, 1000), ("edge", 25, U32)):
+        cases = [c for c in GOLDEN["e2e"] if c["name"] == name and c["k"] == k and c["count_max"] == cm]
+        assert cases, (name, k, cm)
+        case = cases[0]
+        with tempfile.TemporaryDirectory() as tmp:
+            paths = []
+            for i, data in enumerate(_case_files(name)):
+                p = os.path.join(tmp, f"m{i}.fq")
+                open(p, "wb").write(data)
+                paths.append(p)
+            d = os.path.join(tmp, "t")
+            os.makedirs(d)
+            subprocess.run([os.path.join(bin_dir, "kmer_counter"), ",".join(paths), str(k), "8", "1", d, "1024",
+                            "2", str(U32), str(cm)], check=True, capture_output=True)
+            h = os.path.join(tmp, "h.tsv")
+            subprocess.run([htool, "precise", d, "6", "1", h, "1", "10000"], check=True, capture_output=True)
+            sparse = {}
+            for line in open(h):
+                a, b = line.split("\t")
+                if int(b):
+                    sparse[a] = int(b)
+            assert sparse == case["hist"], name
+            o = os.path.join(tmp, "d.txt")
+            subprocess.run([dtool, "precise", d, "6", "1", o, "1", str(U32), "--sort"], check=True,
+                           capture_output=True)
+            assert hashlib.sha256(open(o, "rb").read()).hexdigest() == case["dump_sha256"], name
