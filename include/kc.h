@@ -51,6 +51,22 @@ extern "C" {
 #define KC_ERR_IO 7          /* file write failed */
 #define KC_ERR_NO_DEVICE 8   /* no usable CUDA device */
 #define KC_ERR_FAILED 9      /* the job failed; kc_last_error after kc_wait says why */
+#define KC_ERR_CANCELLED 10  /* the job was cancelled (kc_cancel) before it finished */
+
+/* kc_job.fault_inject: failures a test can force on a job (no counterpart in
+ * the reference, whose failures end the process, e.g. src/FastqReader.h:195;
+ * its one give-up path is the bounded wait of
+ * src/NewKmerTree.h:1225-1254).  Each one goes through the path a real
+ * failure of that kind takes. */
+#define KC_INJECT_WAIT_TIMEOUT 1u    /* a device wait on a flag nothing sets gives up after a short poll
+                                        limit and sets the wait-timeout flag: the job ends KC_ERR_DEVICE */
+#define KC_INJECT_TABLE_FULL_ONCE 2u /* the first counting attempt reports its table full (plain jobs) or a
+                                        sub-bucket table overflowed (Bloom jobs, shared-memory path): the
+                                        job regrows / splits and counts again, with exact results */
+#define KC_INJECT_TABLE_FULL 4u      /* every counting attempt reports its table full: KC_ERR_DEVICE after
+                                        the retries (plain jobs of one table) */
+#define KC_INJECT_NOMEM 8u           /* the job's first device allocation fails as a failed cudaMalloc
+                                        does: the job ends KC_ERR_NOMEM, the handle stays usable */
 
 #define KC_STAGES 12         /* entries of kc_result_t.phase_ms */
 
@@ -95,7 +111,7 @@ typedef struct {
     uint32_t top_n;               /* 0: no top-N query */
     uint32_t want_le2;            /* 1: the records with count <= 2 */
     uint32_t keep_records;        /* 1: copy the sorted records to host memory */
-    uint32_t reserved0;
+    uint32_t fault_inject;        /* testing aid: KC_INJECT_* bits, 0 in normal use */
     uint64_t pass_bytes;          /* device memory one counting pass may use; a job that needs more
                                      runs in passes over ranges of root prefixes, each pass's records
                                      held in pinned host memory until the final sort; 0 -> 70% of the
@@ -154,7 +170,10 @@ typedef struct {
     uint64_t bloom_smem;          /* Bloom jobs with min_count >= 2: 1 counts each filter sub-bucket (a slice
                                      of at most 2048 blocks, 32 KiB) in shared memory, 2 uses global-memory
                                      filters and tables; default 1 */
-    uint64_t reserved[4];
+    uint64_t record_sort;         /* records of jobs with at least 1M of them: 1 sorts most significant bits
+                                     first (bucket scatter + shared-memory sort per bucket), 2 with the
+                                     8-bit LSD radix sort; default 1 */
+    uint64_t reserved[3];
 } kc_tuning;
 
 /* Kernel launches issued by this process so far (all handles). */
@@ -185,6 +204,12 @@ int kc_wait(kc_handle *h, kc_job_id id, int32_t timeout_ms);   /* <0: no limit *
 int kc_result(kc_handle *h, kc_job_id id, kc_result_t *out);
 int kc_write_tmpdir(kc_handle *h, kc_job_id id, const char *dir);
 int kc_release(kc_handle *h, kc_job_id id);
+/* Cancels a job (no counterpart in the reference, which runs one job per
+ * process).  A queued job is taken off the queue; a running job stops at its
+ * next stage boundary and gives back its device memory.  Either way kc_wait
+ * then returns KC_ERR_CANCELLED.  Returns KC_ERR_INVALID when the job had
+ * already finished (its results stand). */
+int kc_cancel(kc_handle *h, kc_job_id id);
 
 /* Batched jobs: every job of the array is counted in one set of device passes
  * (one persistent extraction kernel over all samples' tiles, per-sample
@@ -214,6 +239,15 @@ int kc_hash_kmers(const uint64_t *keys, uint64_t n, uint64_t *out);
 /* Stable LSD radix sort of (key, count) pairs on the low `bits` bits of the
  * keys (sort/ExportRecordRadixSort.h:225-269, tool/dump_tool.cpp:373-454). */
 int kc_sort_records(uint64_t *keys, uint32_t *counts, uint64_t n, uint32_t bits);
+
+/* Sort of (key, count) records whose keys are all distinct, such as a job's
+ * records or the tools' merged records (tool/dump_tool.cpp:373-454 sorts
+ * those with an 11-bit LSD radix sort), on the low `bits` bits of the keys.
+ * From 1M records and 24 bits on it sorts most significant bits first (a
+ * bucket histogram, two scatter passes, one shared-memory sort per bucket),
+ * below that with the LSD sort of kc_sort_records.  Equal keys are not
+ * allowed (their order is unspecified). */
+int kc_sort_distinct_records(uint64_t *keys, uint32_t *counts, uint64_t n, uint32_t bits);
 
 /* kc_sort_records for callers that cannot allocate device memory.  No
  * counterpart in the reference.  Some callers may not call cudaMalloc where

@@ -37,8 +37,11 @@ KC_OK = 0
 ERRORS = {
     1: "KC_ERR_INVALID", 2: "KC_ERR_CUDA", 3: "KC_ERR_NOMEM", 4: "KC_ERR_TIMEOUT",
     5: "KC_ERR_NOT_FOUND", 6: "KC_ERR_DEVICE", 7: "KC_ERR_IO", 8: "KC_ERR_NO_DEVICE",
-    9: "KC_ERR_FAILED",
+    9: "KC_ERR_FAILED", 10: "KC_ERR_CANCELLED",
 }
+KC_ERR_TIMEOUT, KC_ERR_CANCELLED = 4, 10
+# kc_job.fault_inject bits (testing aid)
+INJECT_WAIT_TIMEOUT, INJECT_TABLE_FULL_ONCE, INJECT_TABLE_FULL, INJECT_NOMEM = 1, 2, 4, 8
 U32_MAX = 0xFFFFFFFF
 
 
@@ -56,7 +59,8 @@ class kc_config(C.Structure):
 
 class kc_tuning(C.Structure):
     _fields_ = [("bucket_table_factor", C.c_double), ("table_factor", C.c_double),
-                ("sort_group_records", C.c_uint64), ("bloom_smem", C.c_uint64), ("reserved", C.c_uint64 * 4)]
+                ("sort_group_records", C.c_uint64), ("bloom_smem", C.c_uint64), ("record_sort", C.c_uint64),
+                ("reserved", C.c_uint64 * 3)]
 
 
 class kc_buffer(C.Structure):
@@ -69,7 +73,7 @@ class kc_job(C.Structure):
                 ("memory_gb", C.c_uint64), ("filter_min", C.c_uint32), ("filter_max", C.c_uint32),
                 ("min_count", C.c_uint32), ("max_count", C.c_uint32), ("hist_min", C.c_uint32),
                 ("hist_max", C.c_uint32), ("top_n", C.c_uint32), ("want_le2", C.c_uint32),
-                ("keep_records", C.c_uint32), ("reserved0", C.c_uint32), ("pass_bytes", C.c_uint64),
+                ("keep_records", C.c_uint32), ("fault_inject", C.c_uint32), ("pass_bytes", C.c_uint64),
                 ("reserved", C.c_uint64 * 5)]
 
 
@@ -103,6 +107,7 @@ SIGNATURES = [
     ("kc_result", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(kc_result_t)]),
     ("kc_write_tmpdir", C.c_int, [C.c_void_p, C.c_uint64, C.c_char_p]),
     ("kc_release", C.c_int, [C.c_void_p, C.c_uint64]),
+    ("kc_cancel", C.c_int, [C.c_void_p, C.c_uint64]),
     ("kc_submit_batch", C.c_int, [C.c_void_p, C.POINTER(kc_job), C.c_uint32, C.POINTER(C.c_uint64)]),
     ("kc_host_alloc", C.c_int, [C.c_uint64, C.POINTER(C.c_void_p)]),
     ("kc_host_free", C.c_int, [C.c_void_p]),
@@ -113,6 +118,7 @@ SIGNATURES = [
     ("kc_bloom_plan", C.c_int, [C.POINTER(kc_buffer), C.c_uint32, C.c_uint32, C.c_uint64, C.c_void_p,
                                 C.POINTER(C.c_uint32), C.c_void_p, C.POINTER(C.c_uint64)]),
     ("kc_kernel_launches", C.c_uint64, []),
+    ("kc_sort_distinct_records", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32]),
     ("kc_sort_records_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]),
     ("kc_atomic_peak", C.c_int, [C.c_uint64, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("kc_get_tuning", C.c_int, [C.c_void_p, C.POINTER(kc_tuning)]),
@@ -285,7 +291,8 @@ class KmerCounter:
     def make_job(k: int = 31, count_max: int = 255, bloom: bool = False, memory_gb: int = 4,
                  filter_min: int = 2, filter_max: int = U32_MAX, min_count: int = 1,
                  max_count: int = U32_MAX, hist_min: int = 1, hist_max: int = 10000, top_n: int = 0,
-                 want_le2: bool = False, keep_records: bool = True, pass_bytes: int = 0) -> kc_job:
+                 want_le2: bool = False, keep_records: bool = True, pass_bytes: int = 0,
+                 fault_inject: int = 0) -> kc_job:
         j = kc_job()
         lib().kc_job_defaults(C.byref(j))
         j.k, j.count_max, j.bloom, j.memory_gb = k, count_max, int(bloom), memory_gb
@@ -293,6 +300,7 @@ class KmerCounter:
         j.hist_min, j.hist_max, j.top_n, j.want_le2 = hist_min, hist_max, top_n, int(want_le2)
         j.keep_records = int(keep_records)
         j.pass_bytes = pass_bytes
+        j.fault_inject = fault_inject
         return j
 
     def upload(self, files: Sequence[bytes]):
@@ -367,6 +375,17 @@ class KmerCounter:
             self.release(jid)
         return out
 
+    def cancel(self, jid: int) -> bool:
+        """Cancels a queued or running job (``kc_cancel``); its wait() then
+        raises KC_ERR_CANCELLED.  False when the job had already finished."""
+        rc = lib().kc_cancel(self._h, jid)
+        if rc == KC_OK:
+            return True
+        if rc == 1:   # KC_ERR_INVALID: finished already, its results stand
+            return False
+        _check(rc)
+        return False
+
     def release(self, jid: int):
         self._inputs.pop(jid, None)
         _check(lib().kc_release(self._h, jid))
@@ -388,16 +407,19 @@ class KmerCounter:
         t = kc_tuning()
         _check(lib().kc_get_tuning(self._h, C.byref(t)))
         return {"bucket_table_factor": t.bucket_table_factor, "table_factor": t.table_factor,
-                "sort_group_records": t.sort_group_records, "bloom_smem": t.bloom_smem}
+                "sort_group_records": t.sort_group_records, "bloom_smem": t.bloom_smem, "record_sort": t.record_sort}
 
     def set_tuning(self, bucket_table_factor: float = 0.0, table_factor: float = 0.0, sort_group_records: int = 0,
-                   bloom_smem: int = 0):
+                   bloom_smem: int = 0, record_sort: int = 0):
         """0 (or less) keeps a setting.  bloom_smem: 1 counts Bloom jobs (min
-        count >= 2) per sub-bucket in shared memory, 2 on global-memory tables."""
+        count >= 2) per sub-bucket in shared memory, 2 on global-memory tables.
+        record_sort: 1 sorts large jobs' records most significant bits first,
+        2 with the LSD radix sort."""
         t = kc_tuning()
         t.bucket_table_factor, t.table_factor, t.sort_group_records = bucket_table_factor, table_factor, \
             sort_group_records
         t.bloom_smem = bloom_smem
+        t.record_sort = record_sort
         _check(lib().kc_set_tuning(self._h, C.byref(t)))
 
     def autotune(self, samples: Sequence[Sequence[bytes]] = (), ks: Sequence[int] = (), batch: bool = False,
@@ -471,6 +493,15 @@ def sort_records(keys: np.ndarray, counts: np.ndarray, bits: int):
     keys = np.ascontiguousarray(keys, dtype=np.uint64).copy()
     counts = np.ascontiguousarray(counts, dtype=np.uint32).copy()
     _check(lib().kc_sort_records(_ptr(keys), _ptr(counts), len(keys), bits))
+    return keys, counts
+
+
+def sort_distinct_records(keys: np.ndarray, counts: np.ndarray, bits: int):
+    """Records with distinct keys sorted on their low `bits` bits
+    (``kc_sort_distinct_records``)."""
+    keys = np.ascontiguousarray(keys, dtype=np.uint64).copy()
+    counts = np.ascontiguousarray(counts, dtype=np.uint32).copy()
+    _check(lib().kc_sort_distinct_records(_ptr(keys), _ptr(counts), len(keys), bits))
     return keys, counts
 
 

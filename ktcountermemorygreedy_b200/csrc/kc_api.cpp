@@ -75,6 +75,7 @@ kc_tuning default_tuning()
     t.table_factor = 1.6;
     t.sort_group_records = 4ull << 20;
     t.bloom_smem = 1;
+    t.record_sort = 1;
     return t;
 }
 
@@ -102,6 +103,14 @@ uint64_t table_capacity_for(double est, double factor = 1.6)
 
 int fail(int code, const std::string &msg) { return set_error(code, msg); }
 
+// Working memory of the sort of a job's n records (k-mers of k bases): the
+// MSD sort for large jobs, the LSD sort otherwise; both keep the alternate
+// arrays at the start (sort_tmp_alt).
+size_t record_sort_bytes(uint64_t n, uint32_t k)
+{
+    return msd_sort_applies(n, 2 * k) ? std::max(msd_sort_tmp_bytes(n, 2 * k), sort_tmp_bytes(n)) : sort_tmp_bytes(n);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -119,6 +128,7 @@ struct Job {
     const kc_input *input = nullptr;
     uint64_t reserve = 0;
     JobState state = JobState::QUEUED;
+    std::atomic<bool> cancel{false};   // kc_cancel: stop at the next stage boundary
     int err = KC_OK;
     std::string err_msg;
     double t_submit = 0, t_start = 0, t_end = 0;
@@ -236,6 +246,14 @@ void check_flags(unsigned long long flags, const char *where)
     if (flags & ERR_HIST_OVERFLOW_FULL) throw KcError{KC_ERR_DEVICE, std::string(where) + ": histogram overflow list full"};
 }
 
+// A running job that was cancelled stops here (between stages, with none of
+// its kernels depending on the host); the worker gives back its memory.
+void check_cancel(const Job &job, const char *where)
+{
+    if (job.cancel.load(std::memory_order_relaxed))
+        throw KcError{KC_ERR_CANCELLED, std::string("cancelled (") + where + ")"};
+}
+
 struct Counters {
     unsigned long long v[C_COUNT];
 };
@@ -315,6 +333,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
 {
     const kc_job &P = job.p;
     const uint32_t k = P.k;
+    if (P.fault_inject & KC_INJECT_NOMEM) ws.fail_next_get();
     DevScope ds(st, &ws);
     std::vector<uint32_t> tile_seg_host;
 
@@ -411,6 +430,13 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
         CK(launch_scan_u32(tile_nl, tile_prefix, T, scan_tmp, st));
     }
     clk.end();
+    if (P.fault_inject & KC_INJECT_WAIT_TIMEOUT) {
+        // a bounded device wait on a word nothing sets (the counter block's
+        // last word, zeroed above and never written): it gives up after 1024
+        // polls and the flag check after the SCAN ends the job
+        CK(launch_wait_flag(reinterpret_cast<const unsigned int *>(counters + C_COUNT - 1), 1024, counters + C_FLAGS,
+                            st));
+    }
 
     // ---- SCAN pass ---------------------------------------------------------
     unsigned long long *occ = ds.n<unsigned long long>(1);
@@ -509,6 +535,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     Counters c0{};
     std::memcpy(c0.v, p_c0, sizeof(c0.v));
     check_flags(c0.v[C_FLAGS], "scan");
+    check_cancel(job, "after the census");
     job.occurrences = O;
 
     // ---- counting ---------------------------------------------------------
@@ -598,7 +625,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
             unsigned long long *wk = rec_keys;
             uint32_t *wc = rec_counts;
             if (into_sort_tmp && n_rec > 1) {
-                sort_tmp = ds.get(sort_tmp_bytes(n_rec));
+                sort_tmp = ds.get(record_sort_bytes(n_rec, k));
                 sort_tmp_alt(sort_tmp, n_rec, &wk, &wc);
                 rec_in_sort_tmp = true;
             }
@@ -635,10 +662,13 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
             clk.begin(2);
             CK(launch_extract(MODE_INSERT, a, 0, st));
             clk.end();
+            if ((P.fault_inject & KC_INJECT_TABLE_FULL) || (attempt == 0 && (P.fault_inject & KC_INJECT_TABLE_FULL_ONCE)))
+                CK(launch_or_flags(counters + C_FLAGS, ERR_TABLE_FULL, st));
             Counters c = read_counters(counters, st);
             check_flags(c.v[C_FLAGS], "insert");
             if (!(c.v[C_FLAGS] & ERR_TABLE_FULL)) break;
             if (attempt >= 3) throw KcError{KC_ERR_DEVICE, "counting table overflow"};
+            check_cancel(job, "table regrowth");
             cap *= 2;
         }
         table_cap = cap;
@@ -787,6 +817,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
             CK(cudaMemcpyAsync(p_fill, cursor, N_BUCKETS * 8, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             const std::vector<unsigned long long> fill(p_fill, p_fill + N_BUCKETS);
+            check_cancel(job, "after the partition");
             for (uint32_t b = lo; b < hi; ++b) {
                 if (fill[b] > region[b]) throw CensusOverflow{};
                 cfg[b].key_len = fill[b];
@@ -895,6 +926,11 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                                          P.min_count, P.max_count, rk, rc, rcap, hist_sub, ovf, ovf_cap, counters,
                                          bucket_ovf, st));
                     clk.end();
+                    if (attempt == 0 && (P.fault_inject & KC_INJECT_TABLE_FULL_ONCE)) {
+                        // as if the first bucket's sub-bucket tables had overflowed
+                        CK(cudaMemsetAsync(bucket_ovf + lo, 0x01, 1, st));
+                        CK(launch_or_flags(counters + C_SUB_OVF, 1ull, st));
+                    }
                     const Counters cs = read_counters(counters, st);
                     check_flags(cs.v[C_FLAGS], "sub-bucket count");
                     if (cs.v[C_SUB_OVF] == 0) {
@@ -1082,18 +1118,19 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
         }
     }
     job.table_cap = table_cap;
+    check_cancel(job, "before the sort");
 
     // ---- sort in printed-string order ---------------------------------------
     clk.begin(6);
     if (n_rec > 1) {
         const uint32_t skip = rec_by_bucket && job.passes <= 1 ? 8u : 0u;
-        if (rec_in_sort_tmp) {
-            CK(launch_radix_sort(rec_keys, rec_counts, n_rec, 2 * k, sort_tmp, st, counters + C_FLAGS, skip, true));
-        } else {
-            void *stmp = ds.get(sort_tmp_bytes(n_rec));
-            CK(launch_radix_sort(rec_keys, rec_counts, n_rec, 2 * k, stmp, st, counters + C_FLAGS, skip));
-            ds.release(stmp);
-        }
+        void *stmp = rec_in_sort_tmp ? sort_tmp : ds.get(record_sort_bytes(n_rec, k));
+        if (msd_sort_applies(n_rec, 2 * k) && tn.record_sort != 2)
+            CK(launch_msd_sort(rec_keys, rec_counts, n_rec, 2 * k, stmp, st, counters + C_FLAGS, rec_in_sort_tmp));
+        else
+            CK(launch_radix_sort(rec_keys, rec_counts, n_rec, 2 * k, stmp, st, counters + C_FLAGS, skip,
+                                 rec_in_sort_tmp));
+        if (!rec_in_sort_tmp) ds.release(stmp);
     }
     CK(launch_pair_reverse(rec_keys, n_rec, st));
     clk.end();
@@ -1561,9 +1598,15 @@ void worker_main(kc_handle *h)
             std::lock_guard<std::mutex> lk(h->mu);
             for (auto &j : task->jobs) {
                 j->t_end = now_ms();
-                j->state = code == KC_OK ? JobState::DONE : JobState::FAILED;
-                j->err = code;
-                j->err_msg = msg;
+                int c = code;
+                std::string m = msg;
+                if (c == KC_OK && j->cancel.load(std::memory_order_relaxed)) {
+                    c = KC_ERR_CANCELLED;   // a cancelled sample of a batch that ran on for the others
+                    m = "cancelled";
+                }
+                j->state = c == KC_OK ? JobState::DONE : JobState::FAILED;
+                j->err = c;
+                j->err_msg = m;
             }
             h->reserved -= task->reserve;
             h->running--;
@@ -1757,11 +1800,13 @@ int kc_set_tuning(kc_handle *h, const kc_tuning *t)
         return fail(KC_ERR_INVALID, "bucket_table_factor must be at least 1.05");
     if (t->table_factor > 0 && t->table_factor < 1.05) return fail(KC_ERR_INVALID, "table_factor must be at least 1.05");
     if (t->bloom_smem > 2) return fail(KC_ERR_INVALID, "bloom_smem must be 1 or 2");
+    if (t->record_sort > 2) return fail(KC_ERR_INVALID, "record_sort must be 1 or 2");
     std::lock_guard<std::mutex> lk(h->mu);
     if (t->bucket_table_factor > 0) h->tuning.bucket_table_factor = t->bucket_table_factor;
     if (t->table_factor > 0) h->tuning.table_factor = t->table_factor;
     if (t->sort_group_records > 0) h->tuning.sort_group_records = t->sort_group_records;
     if (t->bloom_smem > 0) h->tuning.bloom_smem = t->bloom_smem;
+    if (t->record_sort > 0) h->tuning.record_sort = t->record_sort;
     return KC_OK;
 }
 
@@ -1799,14 +1844,15 @@ int kc_autotune(kc_handle *h, const kc_job *jobs, uint32_t n_jobs, uint32_t batc
     int rc = run(cur, cur_ms);   // warm-up: workspaces and pinned blocks reach this shape
     if (rc == KC_OK) rc = run(cur, cur_ms);
     const double bucket_c[] = {2.0, 3.0, 4.0}, table_c[] = {1.3, 1.6, 2.2};
-    const uint64_t group_c[] = {2ull << 20, 4ull << 20, 8ull << 20}, smem_c[] = {1, 2, 1};
-    for (int param = 0; param < 4 && rc == KC_OK; ++param)
+    const uint64_t group_c[] = {2ull << 20, 4ull << 20, 8ull << 20}, smem_c[] = {1, 2, 1}, sort_c[] = {1, 2, 1};
+    for (int param = 0; param < 5 && rc == KC_OK; ++param)
         for (int c = 0; c < 3 && rc == KC_OK; ++c) {
             kc_tuning t = cur;
             if (param == 0) t.bucket_table_factor = bucket_c[c];
             if (param == 1) t.table_factor = table_c[c];
             if (param == 2) t.sort_group_records = group_c[c];
             if (param == 3) t.bloom_smem = smem_c[c];
+            if (param == 4) t.record_sort = sort_c[c];
             if (std::memcmp(&t, &cur, sizeof(t)) == 0) continue;
             rc = run(t, ms);
             if (rc == KC_OK && ms < 0.98 * cur_ms) {   // a clear gain only
@@ -1880,6 +1926,46 @@ int kc_result(kc_handle *h, kc_job_id id, kc_result_t *out)
     out->passes = j.passes;
     out->smem_passes = (uint16_t)std::min<uint32_t>(j.smem_passes, 0xFFFF);
     out->smem_fallbacks = (uint16_t)std::min<uint32_t>(j.smem_fallbacks, 0xFFFF);
+    return KC_OK;
+}
+
+int kc_cancel(kc_handle *h, kc_job_id id)
+{
+    if (!h) return fail(KC_ERR_INVALID, "handle is NULL");
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        auto it = h->jobs.find(id);
+        if (it == h->jobs.end()) return fail(KC_ERR_NOT_FOUND, "unknown job id");
+        Job &j = *it->second;
+        if (j.state == JobState::DONE || j.state == JobState::FAILED)
+            return fail(KC_ERR_INVALID, "job already finished");
+        j.cancel.store(true, std::memory_order_relaxed);
+        if (j.state == JobState::QUEUED) {
+            // a queued task leaves the queue once every job in it is cancelled
+            for (auto q = h->queue.begin(); q != h->queue.end(); ++q) {
+                auto &jobs = (*q)->jobs;
+                if (std::find_if(jobs.begin(), jobs.end(), [&](const std::shared_ptr<Job> &x) { return x->id == id; }) ==
+                    jobs.end())
+                    continue;
+                const bool all = std::all_of(jobs.begin(), jobs.end(), [](const std::shared_ptr<Job> &x) {
+                    return x->cancel.load(std::memory_order_relaxed);
+                });
+                if (all) {
+                    const double t = now_ms();
+                    for (auto &x : jobs) {
+                        x->state = JobState::FAILED;
+                        x->err = KC_ERR_CANCELLED;
+                        x->err_msg = "cancelled before it started";
+                        x->t_start = x->t_end = t;
+                    }
+                    h->queue.erase(q);
+                }
+                break;
+            }
+        }
+    }
+    h->cv_work.notify_all();
+    h->cv_done.notify_all();
     return KC_OK;
 }
 

@@ -87,6 +87,10 @@ void Workspace::reserve(size_t bytes)
 
 void *Workspace::get(size_t bytes)
 {
+    if (fail_next_) {
+        fail_next_ = false;
+        throw KcError{KC_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed (injected)"};
+    }
     if (base_ && top_ + bytes <= cap_) {
         void *p = base_ + top_;
         top_ += bytes;
@@ -121,6 +125,7 @@ bool Workspace::release_top(void *p, size_t bytes)
 
 void Workspace::end_job()
 {
+    fail_next_ = false;
     for (void *p : spill_) cudaFreeAsync(p, st_);
     spill_.clear();
     spilled_ = 0;
@@ -562,6 +567,36 @@ int kc_sort_records(uint64_t *keys, uint32_t *counts, uint64_t n, uint32_t bits)
         CK(cudaMemcpyAsync(dk, keys, n * 8, cudaMemcpyHostToDevice, sg.st));
         CK(cudaMemcpyAsync(dv, counts, n * 4, cudaMemcpyHostToDevice, sg.st));
         CK(launch_radix_sort(dk, dv, n, bits, tmp, sg.st, dflags));
+        CK(cudaMemcpyAsync(keys, dk, n * 8, cudaMemcpyDeviceToHost, sg.st));
+        CK(cudaMemcpyAsync(counts, dv, n * 4, cudaMemcpyDeviceToHost, sg.st));
+        unsigned long long flags = 0;
+        CK(cudaMemcpyAsync(&flags, dflags, 8, cudaMemcpyDeviceToHost, sg.st));
+        CK(cudaStreamSynchronize(sg.st));
+        if (flags) return set_error(KC_ERR_DEVICE, "record sort reported error flags");
+        return KC_OK;
+    } catch (const KcError &e) {
+        return set_error(e.code, e.msg);
+    }
+}
+
+int kc_sort_distinct_records(uint64_t *keys, uint32_t *counts, uint64_t n, uint32_t bits)
+{
+    if ((!keys || !counts) && n) return set_error(KC_ERR_INVALID, "bad argument");
+    if (bits > 64) return set_error(KC_ERR_INVALID, "bits must be <= 64");
+    if (n <= 1) return KC_OK;
+    try {
+        StreamGuard sg;
+        DevScope ds(sg.st);
+        unsigned long long *dk = ds.n<unsigned long long>(n);
+        uint32_t *dv = ds.n<uint32_t>(n);
+        const bool msd = msd_sort_applies(n, bits);
+        void *tmp = ds.get(msd ? msd_sort_tmp_bytes(n, bits) : sort_tmp_bytes(n));
+        unsigned long long *dflags = ds.n<unsigned long long>(1);
+        CK(cudaMemsetAsync(dflags, 0, 8, sg.st));
+        CK(cudaMemcpyAsync(dk, keys, n * 8, cudaMemcpyHostToDevice, sg.st));
+        CK(cudaMemcpyAsync(dv, counts, n * 4, cudaMemcpyHostToDevice, sg.st));
+        if (msd) CK(launch_msd_sort(dk, dv, n, bits, tmp, sg.st, dflags, false));
+        else CK(launch_radix_sort(dk, dv, n, bits, tmp, sg.st, dflags));
         CK(cudaMemcpyAsync(keys, dk, n * 8, cudaMemcpyDeviceToHost, sg.st));
         CK(cudaMemcpyAsync(counts, dv, n * 4, cudaMemcpyDeviceToHost, sg.st));
         unsigned long long flags = 0;

@@ -55,12 +55,16 @@ public:
     void end_job();
     ~Workspace();
     size_t capacity() const { return cap_; }
+    // failure injection: the next get() fails as a failed device allocation
+    // does (KcError KC_ERR_NOMEM)
+    void fail_next_get() { fail_next_ = true; }
 
 private:
     cudaStream_t st_;
     uint8_t *base_ = nullptr;
     size_t cap_ = 0, top_ = 0, high_ = 0;
     size_t spilled_ = 0;   // bytes of this job's blocks taken from the pool
+    bool fail_next_ = false;
     std::vector<void *> spill_;
 };
 

@@ -2270,6 +2270,26 @@ __global__ void k_hash_batch(const unsigned long long *keys, uint64_t n, unsigne
     }
 }
 
+// Failure detection: a wait on a device word, polled at most poll_limit
+// times (about a microsecond apart), the same way every wait of the pipeline
+// is bounded.  A wait that runs out sets ERR_WAIT_TIMEOUT in *flags and
+// returns, so the host reads a status and the context stays usable.
+__global__ void k_wait_flag(const unsigned int *flag, uint32_t poll_limit, unsigned long long *flags)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const volatile unsigned int *f = flag;
+    for (uint32_t i = 0; i < poll_limit; ++i) {
+        if (*f != 0u) return;
+        __nanosleep(1000);
+    }
+    atomicOr(flags, ERR_WAIT_TIMEOUT);
+}
+
+__global__ void k_or_flags(unsigned long long *word, unsigned long long bits)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(word, bits);
+}
+
 std::atomic<unsigned long long> g_launches{0};
 thread_local unsigned long long t_launches = 0;
 
@@ -2308,6 +2328,8 @@ int grid_for(uint64_t n, int threads, int per_sm = 8)
 
 unsigned long long kernel_launches() { return g_launches.load(std::memory_order_relaxed); }
 unsigned long long thread_kernel_launches() { return t_launches; }
+
+void note_kernel_launch() { note_launch(); }
 
 size_t extract_smem_bytes_for(int mode, uint32_t stage_cap)
 {
@@ -2946,6 +2968,20 @@ cudaError_t launch_count_subs(unsigned long long *keys, const unsigned long long
     k_count_subs<<<grid, SUB_THREADS, smem, st>>>(keys, sub_off, sub_count, sub_bucket, n_sub, sc, next_sub, count_max,
                                                   min_count, max_count, rec_keys, rec_counts, rec_cap, hist, ovf,
                                                   ovf_cap, counters, bucket_ovf);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wait_flag(const unsigned int *flag, uint32_t poll_limit, unsigned long long *flags, cudaStream_t st)
+{
+    note_launch();
+    k_wait_flag<<<1, 32, 0, st>>>(flag, poll_limit, flags);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_or_flags(unsigned long long *word, unsigned long long bits, cudaStream_t st)
+{
+    note_launch();
+    k_or_flags<<<1, 32, 0, st>>>(word, bits);
     return cudaGetLastError();
 }
 

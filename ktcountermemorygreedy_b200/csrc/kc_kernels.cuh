@@ -258,6 +258,21 @@ cudaError_t preload_sort_in_scratch();
 cudaError_t launch_radix_sort_in_scratch(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits,
                                          void *tmp, cudaStream_t st);
 
+// Sort of distinct keys (a job's records) on their low `bits` bits, most
+// significant bits first: a bucket histogram of the top 8..16 bits, a scatter
+// pass by the top 8 bits and one by the next bits inside those ranges, then
+// every bucket sorted in shared memory (kc_msd_sort.cu).  Synchronizes the
+// stream once (the bucket sizes come to the host).  Result in keys/vals; with
+// input_in_tmp the records start in the alternate arrays (sort_tmp_alt).  For
+// n >= MSD_SORT_MIN_RECORDS and 24 <= bits <= 64 (msd_sort_applies).
+constexpr uint64_t MSD_SORT_MIN_RECORDS = 1ull << 20;
+bool msd_sort_applies(uint64_t n, uint32_t bits);
+size_t msd_sort_tmp_bytes(uint64_t n, uint32_t bits);
+cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
+                            cudaStream_t st, unsigned long long *flags, bool input_in_tmp);
+// Counts one kernel launch of this library (kernels launched outside kc_kernels.cu).
+void note_kernel_launch();
+
 cudaError_t launch_pair_reverse(unsigned long long *keys, uint64_t n, cudaStream_t st);
 
 // Stable selection of records whose count satisfies lo <= c <= hi: writes the
@@ -302,6 +317,13 @@ cudaError_t launch_merge_buckets(const unsigned long long *keys, const BucketRan
                                  unsigned int *next_item, const BucketCfg *cfg, Slot *arena, uint32_t max_probe,
                                  uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
                                  uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *counters, cudaStream_t st);
+
+// A bounded wait on the device word *flag (nonzero ends it): at most
+// poll_limit polls about a microsecond apart, then ERR_WAIT_TIMEOUT is set in
+// *flags and the kernel returns.
+cudaError_t launch_wait_flag(const unsigned int *flag, uint32_t poll_limit, unsigned long long *flags, cudaStream_t st);
+// *word |= bits on the device, in stream order.
+cudaError_t launch_or_flags(unsigned long long *word, unsigned long long bits, cudaStream_t st);
 
 // Batch of hash evaluations for the parity tests: out[5*i..5*i+4] =
 // xxh3_128.lo, xxh3_128.hi, xxh3_64, rapidhash, komihash (all of keys[i]).

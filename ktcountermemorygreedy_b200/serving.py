@@ -11,6 +11,10 @@ come back to pinned host memory.
 
 serve() returns one RequestStats per request (latency from the scheduled
 arrival to the end of the job, host clock) and the wall time of the stream.
+A request with a deadline that has not finished by then is cancelled
+(``kc_cancel``: taken off the queue, or stopped at its next stage boundary
+with its device memory given back) and reported with an error; the other
+jobs are not affected.
 """
 from __future__ import annotations
 
@@ -29,6 +33,7 @@ class Request:
     files: Sequence                  # FASTQ buffers (bytes or uint8 arrays), kept alive by the caller
     k: int
     job: dict = field(default_factory=dict)   # further KmerCounter.submit keywords
+    deadline_ms: float | None = None          # cancelled when not done this long after its arrival
 
 
 @dataclass
@@ -72,6 +77,32 @@ def serve(counter, requests: Sequence[Request]):
 
     th = threading.Thread(target=submitter, daemon=True)
     th.start()
+
+    # deadlines: a watchdog cancels every job still unfinished at its deadline
+    collected = set()
+    lock = threading.Lock()
+    cancelled = set()
+    timed = sorted((requests[i].arrival_s * 1000.0 + requests[i].deadline_ms, i) for i in range(len(requests))
+                   if requests[i].deadline_ms is not None)
+    stop = threading.Event()
+
+    def watchdog():
+        for when, i in timed:
+            delay = t0 + when / 1000.0 - time.perf_counter()
+            if delay > 0 and stop.wait(delay):
+                return
+            submitted[i].wait()
+            with lock:
+                if i in collected or errors[i]:
+                    continue
+                try:
+                    if counter.cancel(ids[i]):
+                        cancelled.add(i)
+                except Exception:   # finished and released meanwhile
+                    pass
+
+    wd = threading.Thread(target=watchdog, daemon=True)
+    wd.start()
     stats: List[RequestStats] = [None] * len(requests)
     end_max = 0.0
     for i in order:
@@ -82,9 +113,16 @@ def serve(counter, requests: Sequence[Request]):
             continue
         try:
             counter.wait(ids[i])
+            with lock:
+                collected.add(i)
             res = counter.result(ids[i], r.k, copy=False)
         except Exception as e:
-            stats[i] = RequestStats(math.nan, 0, 0, late[i], 0, 0, 0, 0, 0, 0, str(e))
+            with lock:
+                collected.add(i)
+            msg = str(e)
+            if i in cancelled:
+                msg = f"cancelled at its deadline ({r.deadline_ms} ms): {msg}"
+            stats[i] = RequestStats(math.nan, 0, 0, late[i], 0, 0, 0, 0, 0, 0, msg)
             continue
         lat = late[i] + res.queue_ms + res.run_ms
         end_max = max(end_max, r.arrival_s * 1000.0 + lat)
@@ -94,6 +132,8 @@ def serve(counter, requests: Sequence[Request]):
                                 int(len(res.le2_keys)), int(np.asarray(res.hist).sum()))
         del res
     th.join()
+    stop.set()
+    wd.join()
     first = min((r.arrival_s for r in requests), default=0.0)
     return stats, max(end_max / 1000.0 - first, 1e-9)
 

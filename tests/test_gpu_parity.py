@@ -669,3 +669,30 @@ def test_reference_tools_read_our_tmpdir():
             subprocess.run([dtool, "precise", d, "6", "1", o, "1", str(U32), "--sort"], check=True,
                            capture_output=True)
             assert hashlib.sha256(open(o, "rb").read()).hexdigest() == case["dump_sha256"], name
+
+
+def _distinct_keys(rng, n, bits):
+    k = np.unique(rng.integers(0, 1 << bits, size=int(n * 1.05) + 16, dtype=np.uint64))
+    rng.shuffle(k)
+    assert len(k) >= n
+    return k[:n]
+
+
+@pytest.mark.parametrize("n,bits,skew", [(1 << 20, 62, False), (3_000_001, 62, False), (2_000_000, 42, False),
+                                         (1_200_000, 24, False), (1_500_000, 62, True), (900_000, 50, False)])
+def test_distinct_record_sort_matches_numpy(kc, n, bits, skew):
+    """kc_sort_distinct_records (the most-significant-bits-first sort of the
+    job records) against numpy, with a skewed case whose largest bucket (40%
+    of the keys share their top 16 bits) goes to the per-bucket fallback."""
+    rng = np.random.default_rng(n + bits)
+    keys = _distinct_keys(rng, n, bits)
+    if skew:
+        m = int(0.4 * n)
+        low = _distinct_keys(rng, m, bits - 16)
+        keys = np.unique(np.concatenate([(np.uint64(0xBEEF) << np.uint64(bits - 16)) | low, keys[: n - m]]))
+        rng.shuffle(keys)
+    counts = rng.integers(1, 1 << 32, size=len(keys), dtype=np.uint64).astype(np.uint32)
+    got_k, got_c = kc.sort_distinct_records(keys, counts, bits)
+    order = np.argsort(keys)
+    assert np.array_equal(got_k, keys[order])
+    assert np.array_equal(got_c, counts[order])

@@ -39,7 +39,8 @@ class FakeCounter:
         def run():
             with self.worker:
                 rec["t_start"] = time.perf_counter()
-                time.sleep(self.service_ms / 1000.0)
+                if not rec.get("cancel"):
+                    time.sleep(self.service_ms / 1000.0)
                 rec["t_end"] = time.perf_counter()
             done.set()
 
@@ -48,6 +49,15 @@ class FakeCounter:
 
     def wait(self, jid):
         self.jobs[jid]["done"].wait()
+        if self.jobs[jid].get("cancel"):
+            raise RuntimeError("KC_ERR_CANCELLED: cancelled")
+
+    def cancel(self, jid):
+        r = self.jobs[jid]
+        if r["done"].is_set():
+            return False
+        r["cancel"] = True   # a job not yet on the worker is dropped when its turn comes
+        return True
 
     def result(self, jid, k, copy=True):
         r = self.jobs[jid]
@@ -93,3 +103,17 @@ def test_results_collected_in_arrival_order_when_listed_out_of_order():
     stats, _ = serving.serve(fc, reqs)
     assert stats[0].occurrences == 4 and stats[1].occurrences == 1
     assert fc.submit_times[0] <= fc.submit_times[1]
+
+
+def test_request_past_its_deadline_is_cancelled_and_others_complete():
+    """One 30 ms worker, five jobs arriving together: the fourth has a 40 ms
+    deadline and is still queued then, so it is cancelled (and reported as
+    such); the others complete with their results."""
+    fc = FakeCounter(service_ms=30.0)
+    reqs = [serving.Request(0.0, [b"x" * (10 + i)], 31, deadline_ms=(40.0 if i == 3 else None)) for i in range(5)]
+    stats, wall = serving.serve(fc, reqs)
+    assert "cancelled at its deadline" in stats[3].error
+    assert all(not stats[i].error for i in (0, 1, 2, 4))
+    assert [stats[i].occurrences for i in (0, 1, 2, 4)] == [10, 11, 12, 14]
+    summ = serving.summarize(stats, wall)
+    assert summ["failed"] == 1
