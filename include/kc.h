@@ -156,6 +156,9 @@ typedef struct {
     uint32_t passes;              /* counting passes over ranges of root prefixes (1: the whole job at once) */
     uint16_t smem_passes;         /* passes counted on the shared-memory sub-bucket path (Bloom mode) */
     uint16_t smem_fallbacks;      /* passes that left it after a sub-bucket table overflowed */
+    uint32_t region_redos;        /* shared-memory passes counted again because a sub-bucket outgrew the
+                                     region estimated from a sample of the pass's keys */
+    uint32_t reserved_r;
 } kc_result_t;
 
 /* Settings of a handle that trade memory for speed, chosen by kc_autotune or
@@ -173,7 +176,11 @@ typedef struct {
     uint64_t record_sort;         /* records of jobs with at least 1M of them: 1 sorts most significant bits
                                      first (bucket scatter + shared-memory sort per bucket), 2 with the
                                      8-bit LSD radix sort; default 1 */
-    uint64_t reserved[3];
+    uint64_t sampled_region_keys; /* Bloom passes (shared-memory path) with at least this many k-mers size
+                                     their sub-buckets from a 1-in-8 sample of the k-mers instead of
+                                     counting them all (a sub-bucket that outgrows its estimate sends the
+                                     pass back to exact counts); default 64M */
+    uint64_t reserved[2];
 } kc_tuning;
 
 /* Kernel launches issued by this process so far (all handles). */

@@ -60,7 +60,7 @@ class kc_config(C.Structure):
 class kc_tuning(C.Structure):
     _fields_ = [("bucket_table_factor", C.c_double), ("table_factor", C.c_double),
                 ("sort_group_records", C.c_uint64), ("bloom_smem", C.c_uint64), ("record_sort", C.c_uint64),
-                ("reserved", C.c_uint64 * 3)]
+                ("sampled_region_keys", C.c_uint64), ("reserved", C.c_uint64 * 2)]
 
 
 class kc_buffer(C.Structure):
@@ -87,7 +87,7 @@ class kc_result_t(C.Structure):
                 ("run_ms", C.c_double), ("phase_ms", C.c_double * 12), ("phase_launches", C.c_uint64 * 12),
                 ("low_len", C.c_uint64), ("high_len", C.c_uint64), ("input_bytes", C.c_uint64),
                 ("n_records_total", C.c_uint64), ("passes", C.c_uint32), ("smem_passes", C.c_uint16),
-                ("smem_fallbacks", C.c_uint16)]
+                ("smem_fallbacks", C.c_uint16), ("region_redos", C.c_uint32), ("reserved_r", C.c_uint32)]
 
 # stage names of kc_result_t.phase_ms
 PHASES = ["census", "scan", "count_pass", "insert_high", "merge_low", "compact", "sort", "queries", "bloom",
@@ -219,6 +219,7 @@ class Result:
     passes: int = 1
     smem_passes: int = 0      # passes counted per sub-bucket in shared memory (Bloom mode)
     smem_fallbacks: int = 0   # passes recounted on global-memory tables after a sub-bucket table overflowed
+    region_redos: int = 0     # shared-memory passes counted again after a sub-bucket outgrew its estimated region
 
 
 def _copy(ptr, n, dtype):
@@ -370,7 +371,7 @@ class KmerCounter:
             table_capacity=r.table_capacity, device_ms=r.device_ms, queue_ms=r.queue_ms, run_ms=r.run_ms,
             phase_ms=tuple(r.phase_ms), phase_launches=tuple(r.phase_launches), low_len=r.low_len,
             high_len=r.high_len, input_bytes=r.input_bytes, n_records_total=r.n_records_total, passes=r.passes,
-            smem_passes=r.smem_passes, smem_fallbacks=r.smem_fallbacks)
+            smem_passes=r.smem_passes, smem_fallbacks=r.smem_fallbacks, region_redos=r.region_redos)
         if release:
             self.release(jid)
         return out
@@ -407,10 +408,11 @@ class KmerCounter:
         t = kc_tuning()
         _check(lib().kc_get_tuning(self._h, C.byref(t)))
         return {"bucket_table_factor": t.bucket_table_factor, "table_factor": t.table_factor,
-                "sort_group_records": t.sort_group_records, "bloom_smem": t.bloom_smem, "record_sort": t.record_sort}
+                "sort_group_records": t.sort_group_records, "bloom_smem": t.bloom_smem, "record_sort": t.record_sort,
+                "sampled_region_keys": t.sampled_region_keys}
 
     def set_tuning(self, bucket_table_factor: float = 0.0, table_factor: float = 0.0, sort_group_records: int = 0,
-                   bloom_smem: int = 0, record_sort: int = 0):
+                   bloom_smem: int = 0, record_sort: int = 0, sampled_region_keys: int = 0):
         """0 (or less) keeps a setting.  bloom_smem: 1 counts Bloom jobs (min
         count >= 2) per sub-bucket in shared memory, 2 on global-memory tables.
         record_sort: 1 sorts large jobs' records most significant bits first,
@@ -420,6 +422,7 @@ class KmerCounter:
             sort_group_records
         t.bloom_smem = bloom_smem
         t.record_sort = record_sort
+        t.sampled_region_keys = sampled_region_keys
         _check(lib().kc_set_tuning(self._h, C.byref(t)))
 
     def autotune(self, samples: Sequence[Sequence[bytes]] = (), ks: Sequence[int] = (), batch: bool = False,

@@ -9,6 +9,12 @@
 //       substitutions; reads <first_read> .. <first_read> + <n_reads> - 1 of
 //       the stream (the same bytes libkcgen.so writes for those reads).
 //
+//   fastq_gen outofcore <genome_bp> <first_read> <n_reads> <out.fq>
+//       the out-of-core job's read stream (seed 5): 45% of the genome from
+//       2000 repeat families of 0.3-6 kbp with 1-10^5 copies (scaled to the
+//       45% total), each family at a divergence drawn from U[1%, 15%]; 150 bp
+//       reads at 1% substitutions.
+//
 // Exit status 0 on success, 1 on a usage error, 2 when the file cannot be
 // written.
 #include <cstdio>
@@ -23,7 +29,7 @@ namespace {
 
 int usage()
 {
-    std::fprintf(stderr, "usage: fastq_gen large <genome_bp> <first_read> <n_reads> <out.fq>\n");
+    std::fprintf(stderr, "usage: fastq_gen large|outofcore <genome_bp> <first_read> <n_reads> <out.fq>\n");
     return 1;
 }
 
@@ -38,13 +44,16 @@ bool parse_u64(const char *s, uint64_t &v)
 
 int main(int argc, char **argv)
 {
-    if (argc != 6 || std::string(argv[1]) != "large") return usage();
+    const std::string mode = argc == 6 ? argv[1] : "";
+    if (mode != "large" && mode != "outofcore") return usage();
+    const uint64_t seed = mode == "large" ? 2 : 5;
     uint64_t glen = 0, first = 0, n = 0;
     if (!parse_u64(argv[2], glen) || !parse_u64(argv[3], first) || !parse_u64(argv[4], n) || glen < 1000)
         return usage();
     const int threads = (int)std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
     std::vector<char> genome(glen);
-    kcgen_genome(2, glen, 0.05, 200, 1000, 5000, 10, 500, 0.02, genome.data(), threads);
+    if (mode == "large") kcgen_genome(2, glen, 0.05, 200, 1000, 5000, 10, 500, 0.02, genome.data(), threads);
+    else kcgen_genome_div(5, glen, 0.45, 2000, 300, 6000, 1, 100000, 0.01, 0.15, genome.data(), threads);
     FILE *f = std::fopen(argv[5], "wb");
     if (!f) {
         std::perror(argv[5]);
@@ -56,9 +65,9 @@ int main(int argc, char **argv)
     std::vector<char> buf;
     for (uint64_t a = 0; a < n; a += piece) {
         const uint64_t m = std::min(piece, n - a);
-        const uint64_t size = kcgen_reads_size(2, first + a, m, 150, 150);
+        const uint64_t size = kcgen_reads_size(seed, first + a, m, 150, 150);
         buf.resize(size);
-        if (kcgen_reads(genome.data(), glen, 2, first + a, m, 150, 150, 0.01, 0.0, buf.data(), size, threads) != size ||
+        if (kcgen_reads(genome.data(), glen, seed, first + a, m, 150, 150, 0.01, 0.0, buf.data(), size, threads) != size ||
             std::fwrite(buf.data(), 1, size, f) != size) {
             std::fclose(f);
             std::fprintf(stderr, "fastq_gen: writing %s failed\n", argv[5]);

@@ -104,13 +104,15 @@ void plan_reads(ReadPlan &p, uint64_t seed, uint64_t first_id)
 extern "C" {
 
 // Genome of `length` bases.  When repeat_frac > 0, n_families family
-// sequences of length U[fam_min, fam_max] are drawn, copy counts
+// sequences of length U[fam_min, fam_max] are drawn, each with a divergence
+// U[div_min, div_max] (no draw when they are equal), copy counts
 // U[copies_min, copies_max] are scaled so that all copies together cover
 // repeat_frac of the genome, and each copy is written at a uniform position
-// with `divergence` per-base substitutions.  Returns the repeat bases placed.
-uint64_t kcgen_genome(uint64_t seed, uint64_t length, double repeat_frac, uint32_t n_families,
-                      uint32_t fam_min, uint32_t fam_max, uint32_t copies_min, uint32_t copies_max,
-                      double divergence, char *out, int threads)
+// with its family's per-base substitution rate.  Returns the repeat bases
+// placed.
+uint64_t kcgen_genome_div(uint64_t seed, uint64_t length, double repeat_frac, uint32_t n_families,
+                          uint32_t fam_min, uint32_t fam_max, uint32_t copies_min, uint32_t copies_max,
+                          double div_min, double div_max, char *out, int threads)
 {
     parallel_for((length + 4095) / 4096, threads, [&](uint64_t a, uint64_t b) {
         for (uint64_t blk = a; blk < b; ++blk) {
@@ -125,13 +127,14 @@ uint64_t kcgen_genome(uint64_t seed, uint64_t length, double repeat_frac, uint32
     if (repeat_frac <= 0.0 || n_families == 0) return 0;
     Rng r(mix_seed(seed, 0xfa111e5ULL));
     std::vector<std::string> fams(n_families);
-    std::vector<double> copies(n_families);
+    std::vector<double> copies(n_families), div(n_families, div_min);
     double want = repeat_frac * (double)length, raw = 0.0;
     for (uint32_t f = 0; f < n_families; ++f) {
         uint32_t L = fam_min + (uint32_t)r.below(fam_max - fam_min + 1);
         fams[f].resize(L);
         for (uint32_t i = 0; i < L; ++i) fams[f][i] = BASES[r.next() & 3];
         copies[f] = copies_min + (double)r.below(copies_max - copies_min + 1);
+        if (div_max > div_min) div[f] = div_min + (div_max - div_min) * r.uniform();
         raw += copies[f] * L;
     }
     double scale = raw > 0 ? want / raw : 0.0;
@@ -144,13 +147,22 @@ uint64_t kcgen_genome(uint64_t seed, uint64_t length, double repeat_frac, uint32
             uint64_t pos = r.below(length - fam.size());
             for (size_t i = 0; i < fam.size(); ++i) {
                 char b = fam[i];
-                if (r.uniform() < divergence) b = BASES[(((b == 'A') ? 0 : (b == 'C') ? 1 : (b == 'G') ? 2 : 3) + 1 + r.below(3)) & 3];
+                if (r.uniform() < div[f]) b = BASES[(((b == 'A') ? 0 : (b == 'C') ? 1 : (b == 'G') ? 2 : 3) + 1 + r.below(3)) & 3];
                 out[pos + i] = b;
             }
             placed += fam.size();
         }
     }
     return placed;
+}
+
+// kcgen_genome_div with one divergence for every family.
+uint64_t kcgen_genome(uint64_t seed, uint64_t length, double repeat_frac, uint32_t n_families,
+                      uint32_t fam_min, uint32_t fam_max, uint32_t copies_min, uint32_t copies_max,
+                      double divergence, char *out, int threads)
+{
+    return kcgen_genome_div(seed, length, repeat_frac, n_families, fam_min, fam_max, copies_min, copies_max, divergence,
+                            divergence, out, threads);
 }
 
 // Exact FASTQ size of kcgen_reads with the same arguments.

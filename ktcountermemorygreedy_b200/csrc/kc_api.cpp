@@ -76,6 +76,7 @@ kc_tuning default_tuning()
     t.sort_group_records = 4ull << 20;
     t.bloom_smem = 1;
     t.record_sort = 1;
+    t.sampled_region_keys = 64ull << 20;
     return t;
 }
 
@@ -106,6 +107,10 @@ int fail(int code, const std::string &msg) { return set_error(code, msg); }
 // Working memory of the sort of a job's n records (k-mers of k bases): the
 // MSD sort for large jobs, the LSD sort otherwise; both keep the alternate
 // arrays at the start (sort_tmp_alt).
+// Sub-bucket regions of a large pass (kc_tuning.sampled_region_keys) are
+// sized from a 1-in-SUB_REGION_SAMPLE sample of its work items.
+constexpr uint32_t SUB_REGION_SAMPLE = 8;
+
 size_t record_sort_bytes(uint64_t n, uint32_t k)
 {
     return msd_sort_applies(n, 2 * k) ? std::max(msd_sort_tmp_bytes(n, 2 * k), sort_tmp_bytes(n)) : sort_tmp_bytes(n);
@@ -140,7 +145,7 @@ struct Job {
     HostRecords le2;   // records with count <= 2 (pinned: often most of the records)
     uint64_t occurrences = 0, distinct = 0, low_only = 0, table_cap = 0;
     uint64_t low_len = 0, high_len = 0, input_bytes = 0, n_records_total = 0;
-    uint32_t passes = 1, smem_passes = 0, smem_fallbacks = 0;
+    uint32_t passes = 1, smem_passes = 0, smem_fallbacks = 0, region_redos = 0;
     double device_ms = 0;
     double phase_ms[KC_STAGES] = {0};
     uint64_t phase_launches[KC_STAGES] = {0};
@@ -550,7 +555,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     unsigned long long low_len = 0, high_len = 0;
     uint64_t table_cap = 0;
     job.distinct = job.low_only = 0;
-    job.smem_passes = job.smem_fallbacks = 0;
+    job.smem_passes = job.smem_fallbacks = job.region_redos = 0;
 
     // Records of one counted table: the FIRST occurrences are merged in (Bloom
     // mode), every occupied slot is compacted into new record arrays, and the
@@ -721,7 +726,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
             cudaGetLastError();
             budget = (uint64_t)(0.7 * (double)(free_b + ws_free + pool_slack));
         }
-        const uint64_t per_occ = P.bloom ? 40 : 48;
+        const uint64_t per_occ = P.bloom ? 42 : 48;
         std::vector<std::pair<uint32_t, uint32_t>> ranges;
         {
             uint32_t lo = 0;
@@ -758,8 +763,12 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
             // given back before the tables are laid out (Bloom mode); without
             // the Bloom split the scattered k-mers are the insert's input
             unsigned long long *list = nullptr, *bits = nullptr, *keys = nullptr;
+            unsigned long long list_cap = ocap;
             if (P.bloom) {
-                list = ds.n<unsigned long long>(ocap);
+                // room for the sub-buckets' estimated regions (their sizes plus
+                // about 15% on a large pass)
+                list_cap = ocap + ocap / 4 + 65536;
+                list = ds.n<unsigned long long>(list_cap);
                 bits = ds.n<unsigned long long>(std::max<unsigned long long>(words, 1));
                 keys = ds.n<unsigned long long>(ocap);
             } else {
@@ -861,6 +870,10 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                 // a failed one (on the device: no round trip)
                 unsigned long long *ovf_len_saved = ds.n<unsigned long long>(1);
                 CK(cudaMemcpyAsync(ovf_len_saved, counters + C_OVF_LEN, 8, cudaMemcpyDeviceToDevice, st));
+                // a large pass sizes the sub-buckets' regions from a sample of
+                // its keys instead of counting them all; a sub-bucket that
+                // outgrows its region sends the pass back to exact counts
+                bool exact_regions = false;
                 for (int attempt = 0; eligible && !sub_done; ++attempt) {
                     const DevScope::Mark m0 = ds.mark();
                     std::vector<SubCfg> sc(N_BUCKETS);
@@ -907,24 +920,38 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                     CK(cudaMemsetAsync(hist_sub, 0, HIST_BINS * 8, st));
                     CK(cudaMemsetAsync(counters + C_LOW_LEN, 0, 2 * 8, st));   // C_LOW_LEN, C_HIGH_LEN
                     CK(cudaMemsetAsync(counters + C_REC_LEN, 0, 3 * 8, st));   // C_REC_LEN, C_LOW_ONLY, C_DISTINCT
-                    CK(cudaMemsetAsync(counters + C_SUB_OVF, 0, 8, st));
+                    CK(cudaMemsetAsync(counters + C_SUB_OVF, 0, 2 * 8, st));   // C_SUB_OVF, C_REGION_OVF
+                    const bool sampled = !exact_regions && pass_keys >= tn.sampled_region_keys;
+                    unsigned long long *sub_end = nullptr;
                     clk.begin(9);
-                    CK(launch_subpart_count(keys, d_br, n_items, d_sc, sub_count, st));
-                    CK(launch_scan_u32(sub_count, sub_off, n_sub, sub_tmp, st));
-                    if (n_sub)
-                        CK(cudaMemcpyAsync(sub_cur, sub_off, (size_t)n_sub * 8, cudaMemcpyDeviceToDevice, st));
+                    if (sampled) {
+                        uint32_t *region = ds.n<uint32_t>(std::max<uint32_t>(n_sub, 1));
+                        sub_end = ds.n<unsigned long long>(std::max<uint32_t>(n_sub, 1));
+                        CK(launch_subpart_count(keys, d_br, n_items, d_sc, sub_count, st, SUB_REGION_SAMPLE));
+                        CK(launch_subpart_regions(sub_count, n_sub, SUB_REGION_SAMPLE, region, sub_off, sub_end, sub_cur,
+                                                  sub_tmp, st));
+                    } else {
+                        CK(launch_subpart_count(keys, d_br, n_items, d_sc, sub_count, st));
+                        CK(launch_scan_u32(sub_count, sub_off, n_sub, sub_tmp, st));
+                        if (n_sub)
+                            CK(cudaMemcpyAsync(sub_cur, sub_off, (size_t)n_sub * 8, cudaMemcpyDeviceToDevice, st));
+                    }
                     const uint32_t max_sub = *std::max_element(nsub.begin(), nsub.end());
                     BucketRanges bs = br;
                     const uint32_t n_sp_items = fill_item_starts_n(bs, SUB_SCATTER_ITEM_KEYS);
                     BucketRanges *d_bs = ds.n<BucketRanges>(1);
                     CK(cudaMemcpyAsync(d_bs, hs.up(&bs, 1), sizeof(BucketRanges), cudaMemcpyHostToDevice, st));
-                    CK(launch_subpart_scatter(keys, d_bs, n_sp_items, sub_next, d_sc, sub_cur, list, ocap, max_sub,
-                                              st));
+                    CK(launch_subpart_scatter(keys, d_bs, n_sp_items, sub_next, d_sc, sub_cur, list, list_cap, max_sub,
+                                              st, sub_end));
+                    if (sampled)
+                        CK(launch_subpart_sizes(sub_off, sub_cur, sub_end, n_sub, list_cap, sub_count,
+                                                counters + C_REGION_OVF, st));
                     clk.end();
                     clk.begin(10);
+                    uint32_t *first_bits = ds.n<uint32_t>(count_subs_mask_words(list_cap, n_sub));
                     CK(launch_count_subs(list, sub_off, sub_count, d_sb, n_sub, d_sc, sub_next, count_max,
                                          P.min_count, P.max_count, rk, rc, rcap, hist_sub, ovf, ovf_cap, counters,
-                                         bucket_ovf, st));
+                                         bucket_ovf, first_bits, st));
                     clk.end();
                     if (attempt == 0 && (P.fault_inject & KC_INJECT_TABLE_FULL_ONCE)) {
                         // as if the first bucket's sub-bucket tables had overflowed
@@ -933,6 +960,16 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                     }
                     const Counters cs = read_counters(counters, st);
                     check_flags(cs.v[C_FLAGS], "sub-bucket count");
+                    if (cs.v[C_REGION_OVF]) {
+                        // a sub-bucket outgrew its estimated region: count again
+                        // with exact regions (same sub-buckets)
+                        CK(cudaMemcpyAsync(counters + C_OVF_LEN, ovf_len_saved, 8, cudaMemcpyDeviceToDevice, st));
+                        CK(cudaStreamSynchronize(st));
+                        ds.rewind(m0);
+                        exact_regions = true;
+                        ++job.region_redos;
+                        continue;
+                    }
                     if (cs.v[C_SUB_OVF] == 0) {
                         CK(launch_add_u64(hist, hist_sub, HIST_BINS, st));
                         rec_keys = rk;
@@ -1807,6 +1844,7 @@ int kc_set_tuning(kc_handle *h, const kc_tuning *t)
     if (t->sort_group_records > 0) h->tuning.sort_group_records = t->sort_group_records;
     if (t->bloom_smem > 0) h->tuning.bloom_smem = t->bloom_smem;
     if (t->record_sort > 0) h->tuning.record_sort = t->record_sort;
+    if (t->sampled_region_keys > 0) h->tuning.sampled_region_keys = t->sampled_region_keys;
     return KC_OK;
 }
 
@@ -1926,6 +1964,7 @@ int kc_result(kc_handle *h, kc_job_id id, kc_result_t *out)
     out->passes = j.passes;
     out->smem_passes = (uint16_t)std::min<uint32_t>(j.smem_passes, 0xFFFF);
     out->smem_fallbacks = (uint16_t)std::min<uint32_t>(j.smem_fallbacks, 0xFFFF);
+    out->region_redos = j.region_redos;
     return KC_OK;
 }
 

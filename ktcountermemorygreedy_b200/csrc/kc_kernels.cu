@@ -1853,7 +1853,8 @@ __device__ __forceinline__ uint32_t sub_of(unsigned long long key, const SubCfg 
 // meets one or two buckets) in a shared histogram, flushed per bucket.
 constexpr uint32_t SPC_PER_THREAD = WORK_ITEM_KEYS / 256;
 __global__ void __launch_bounds__(256) k_subpart_count(const unsigned long long *keys, const BucketRanges *rg,
-                                                       uint32_t n_items, const SubCfg *sc, uint32_t *sub_count)
+                                                       uint32_t n_items, const SubCfg *sc, uint32_t *sub_count,
+                                                       uint32_t stride)
 {
     __shared__ uint32_t s_item0[N_BUCKETS + 1];
     __shared__ uint32_t s_h[SUB_MAX_PER_BUCKET];
@@ -1865,6 +1866,7 @@ __global__ void __launch_bounds__(256) k_subpart_count(const unsigned long long 
     uint32_t cur = N_BUCKETS;
     SubCfg c{};
     for (uint32_t it = it0; it < it1; ++it) {
+        if (stride > 1 && it % stride) continue;   // a sample of the items
         const WorkItem w = work_item(rg, s_item0, it);
         if (w.bucket != cur) {
             if (cur != N_BUCKETS) {
@@ -1896,6 +1898,47 @@ __global__ void __launch_bounds__(256) k_subpart_count(const unsigned long long 
     if (cur != N_BUCKETS)
         for (uint32_t i = tid; i < c.n_sub; i += 256)
             if (s_h[i]) atomicAdd(&sub_count[c.sub_base + i], s_h[i]);
+}
+
+// Regions of the sub-buckets estimated from a 1-in-stride sample of the
+// keys: n = stride * sampled count, region = n + 20 sqrt(n) + 64 (the sampled
+// count's standard deviation is about sqrt(n * stride) / stride * stride).
+__global__ void k_subpart_regions(const uint32_t *sampled, uint32_t n_sub, uint32_t stride, uint32_t *region)
+{
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_sub; s += gridDim.x * blockDim.x) {
+        const double n = (double)sampled[s] * stride;
+        const double r = n + 20.0 * sqrt(n) + 64.0;
+        region[s] = r < 2.0e9 ? (uint32_t)r : 2000000000u;
+    }
+}
+
+// After the scatter into estimated regions: the cursors start at sub_off and
+// end past each sub-bucket's keys.  count[s] = keys of sub-bucket s; a
+// sub-bucket that outgrew its region (or a region past the key array's end)
+// sets *overflow, and its count is cut to what was written.
+__global__ void k_subpart_sizes(const unsigned long long *sub_off, const unsigned long long *sub_cursor,
+                                const unsigned long long *sub_end, uint32_t n_sub, uint64_t out_cap, uint32_t *count,
+                                unsigned long long *overflow)
+{
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_sub; s += gridDim.x * blockDim.x) {
+        const unsigned long long a = sub_off[s], e = sub_end[s] < out_cap ? sub_end[s] : out_cap;
+        unsigned long long b = sub_cursor[s];
+        if (b > e) {
+            atomicOr(overflow, 1ull);
+            b = e;
+        }
+        count[s] = (uint32_t)(b > a ? b - a : 0);
+    }
+}
+
+// sub_end[s] = sub_off[s] + region[s]; the cursors start at sub_off.
+__global__ void k_subpart_ends(const unsigned long long *sub_off, const uint32_t *region, uint32_t n_sub,
+                               unsigned long long *sub_end, unsigned long long *sub_cursor)
+{
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_sub; s += gridDim.x * blockDim.x) {
+        sub_end[s] = sub_off[s] + region[s];
+        sub_cursor[s] = sub_off[s];
+    }
 }
 
 // Exclusive scan of one value per thread over a block of up to 1024 threads
@@ -1941,6 +1984,7 @@ static_assert(SUB_SCATTER_ITEM_KEYS % SP_THREADS == 0 && SUB_SCATTER_ITEM_KEYS <
 __global__ void __launch_bounds__(SP_THREADS) k_subpart_scatter(const unsigned long long *keys, const BucketRanges *rg,
                                                                 uint32_t n_items, unsigned int *next_item,
                                                                 const SubCfg *sc, unsigned long long *sub_cursor,
+                                                                const unsigned long long *sub_end,
                                                                 unsigned long long *out, uint64_t out_cap,
                                                                 uint32_t max_sub)
 {
@@ -2018,8 +2062,11 @@ __global__ void __launch_bounds__(SP_THREADS) k_subpart_scatter(const unsigned l
             if (j < per && b0 + j < c.n_sub) s_dst[b0 + j] = cur[j] - first[j];
         __syncthreads();
         for (uint32_t i = tid; i < n; i += SP_THREADS) {
-            const unsigned long long d = s_dst[s_sub[i]] + i;
-            if (d < out_cap) out[d] = s_sorted[i];
+            const uint32_t sb = s_sub[i];
+            const unsigned long long d = s_dst[sb] + i;
+            // estimated regions: a sub-bucket that outgrew its region is
+            // reported by its cursor (k_subpart_sizes) and counted exactly
+            if (d < out_cap && (!sub_end || d < sub_end[c.sub_base + sb])) out[d] = s_sorted[i];
         }
         for (uint32_t i = tid; i < c.n_sub; i += SP_THREADS) s_cnt[i] = 0;
         __syncthreads();
@@ -2071,22 +2118,38 @@ __device__ __forceinline__ int sub_table_find(const unsigned long long *tk, unsi
 constexpr uint32_t SUB_THREADS = 512;   // blocks of the shared-memory count
 constexpr uint32_t SUB_BLOCKS_PER_SM = 2;
 constexpr uint32_t SUB_PER_THREAD = 4;
-constexpr uint32_t SUB_TILE = SUB_THREADS * SUB_PER_THREAD;
+constexpr uint32_t SUB_WARPS = SUB_THREADS / 32;
+constexpr uint32_t SUB_CHUNK = 32 * SUB_PER_THREAD;   // keys a warp takes at a time
 constexpr uint32_t SUB_HIST_BINS = 2048;   // counts below this go to a shared histogram
 
-
+// One sub-bucket at a time per block (persistent, two blocks per SM):
+//   1. the reference's two-level Bloom classification (src/BloomFilter.h:233-273)
+//      on the filter slice in shared memory, each warp on its own chunks of
+//      the sub-bucket's keys (no block-wide step inside the loop): a FIRST
+//      occurrence is marked in the sub-bucket's bit mask (one word per 32
+//      keys, first_bits), the others are counted in the shared-memory table
+//      through a per-warp queue (every lane inserts);
+//   2. the FIRST occurrences, read again where their bit is set: +1 on a
+//      table hit, otherwise a k-mer seen once (counted, no record: min count
+//      >= 2);
+//   3. the table's records and histogram.
+// Classification order inside a sub-bucket depends on the warps' timing, as
+// the reference's does on its threads'; at most one occurrence of a k-mer is
+// FIRST (the seen-once word is set by a returning atomicOr), so the merged
+// counts are exact in every order.
 __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
-    unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count, const uint8_t *sub_bucket,
-    uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub, uint32_t count_max, uint32_t min_count,
-    uint32_t max_count, unsigned long long *rec_keys, uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist,
-    uint32_t *ovf, uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf)
+    const unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count,
+    const uint8_t *sub_bucket, uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub, uint32_t count_max,
+    uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys, uint32_t *rec_counts, uint64_t rec_cap,
+    unsigned long long *hist, uint32_t *ovf, uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf,
+    uint32_t *first_bits)
 {
     extern __shared__ __align__(16) uint8_t cs_smem[];
     unsigned long long *s_filter = reinterpret_cast<unsigned long long *>(cs_smem);   // 2 * SUB_SLICE_BLOCKS
     unsigned long long *s_tk = s_filter + 2 * SUB_SLICE_BLOCKS;                       // SUB_TABLE_SLOTS
     uint32_t *s_tc = reinterpret_cast<uint32_t *>(s_tk + SUB_TABLE_SLOTS);            // SUB_TABLE_SLOTS
     uint32_t *s_hist = s_tc + SUB_TABLE_SLOTS;                                        // SUB_HIST_BINS
-    unsigned long long *s_queue = reinterpret_cast<unsigned long long *>(s_hist + SUB_HIST_BINS);   // SUB_TILE
+    unsigned long long *s_queue = reinterpret_cast<unsigned long long *>(s_hist + SUB_HIST_BINS);   // SUB_THREADS * 4
     __shared__ uint32_t s_warp[32], s_sub;
     __shared__ unsigned long long s_base;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -2095,6 +2158,7 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
     unsigned long long n_high = 0, n_low = 0, n_low_only = 0, n_distinct = 0;
     uint32_t n_ovf_subs = 0;
     bool rec_full = false;
+    unsigned long long *q = s_queue + warp * SUB_CHUNK;
     for (;;) {
         if (tid == 0) s_sub = atomicAdd(next_sub, 1u);
         __syncthreads();
@@ -2107,37 +2171,36 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
         const uint32_t bucket = sub_bucket[sub];
         const unsigned long long fcap = sc[bucket].fcap;
         const uint32_t slice = 1u << sc[bucket].slice_shift;
+        uint32_t *fb = first_bits + (base >> 5) + sub;   // bit j of word w: key 32 w + j is FIRST
+        const uint32_t n_chunks = (n + SUB_CHUNK - 1) / SUB_CHUNK;
         for (uint32_t i = tid; i < 2 * slice; i += SUB_THREADS) s_filter[i] = 0;
         for (uint32_t i = tid; i < SUB_TABLE_SLOTS; i += SUB_THREADS) {
             s_tk[i] = EMPTY_KEY;
             s_tc[i] = 0;
         }
         __syncthreads();
-        // 1. the reference's two-level Bloom classification (src/BloomFilter.h:233-273)
-        // on the slice; non-FIRST occurrences counted in the table, FIRST ones
-        // written back over the front of the sub-bucket's keys
+        // 1. classification; the warp's next chunk is loaded while this one is classified
         bool full = false;
-        uint32_t lo_cnt = 0;   // the same in every thread
-        // the next tile's k-mers are loaded while this one is classified (a
-        // tile's FIRST write-back only reaches positions already loaded)
         unsigned long long kn[SUB_PER_THREAD];
+        uint32_t c = warp;
 #pragma unroll
         for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
-            const uint32_t i = r * SUB_THREADS + tid;
-            kn[r] = i < n ? __ldcs(&keys[base + i]) : EMPTY_KEY;
+            const uint32_t i = c * SUB_CHUNK + r * 32 + lane;
+            kn[r] = (c < n_chunks && i < n) ? __ldcs(&keys[base + i]) : EMPTY_KEY;
         }
-        for (uint32_t t0 = 0; t0 < n; t0 += SUB_TILE) {
+        for (; c < n_chunks; c += SUB_WARPS) {
             unsigned long long k[SUB_PER_THREAD];
-            uint32_t firsts = 0, highs = 0;
+            const uint32_t cn = c + SUB_WARPS;
 #pragma unroll
             for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
                 k[r] = kn[r];
-                const uint32_t i = t0 + SUB_TILE + r * SUB_THREADS + tid;
-                kn[r] = i < n ? __ldcs(&keys[base + i]) : EMPTY_KEY;
+                const uint32_t i = cn * SUB_CHUNK + r * 32 + lane;
+                kn[r] = (cn < n_chunks && i < n) ? __ldcs(&keys[base + i]) : EMPTY_KEY;
             }
+            uint32_t firsts = 0, highs = 0;
 #pragma unroll
             for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
-                if (t0 + r * SUB_THREADS + tid >= n) continue;
+                if (c * SUB_CHUNK + r * 32 + lane >= n) continue;
                 uint64_t block, m, hi;
                 bloom_probe_hi(k[r], fcap, block, m, hi);
                 unsigned long long *cell = s_filter + 2 * (block & (slice - 1));
@@ -2156,32 +2219,25 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
                 else highs |= 1u << r;
             }
             n_high += (uint64_t)__popc(highs);
-            // the warp's non-FIRST k-mers are queued so that every lane inserts
-            {
-                unsigned long long *q = s_queue + warp * (32 * SUB_PER_THREAD);
-                uint32_t qn = 0;
-#pragma unroll
-                for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
-                    const bool h = (highs >> r) & 1u;
-                    const uint32_t b = __ballot_sync(FULL, h);
-                    if (h) q[qn + (uint32_t)__popc(b & lt)] = k[r];
-                    qn += (uint32_t)__popc(b);
-                }
-                __syncwarp();
-                for (uint32_t j = lane; j < qn; j += 32)
-                    if (!sub_table_add(s_tk, s_tc, q[j])) full = true;
-                __syncwarp();
-            }
-            uint32_t tf;
-            const uint32_t of = block_excl_scan_1024((uint32_t)__popc(firsts), s_warp, tf);
-            // every key of this tile is in registers (the scan synchronised the
-            // block), so the FIRST ones may overwrite its front
-            unsigned long long p = base + lo_cnt + of;
-#pragma unroll
-            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r)
-                if ((firsts >> r) & 1u) keys[p++] = k[r];
-            lo_cnt += tf;
             n_low += (uint64_t)__popc(firsts);
+#pragma unroll
+            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
+                const uint32_t b = __ballot_sync(FULL, (firsts >> r) & 1u);
+                if (lane == 0 && c * SUB_CHUNK + r * 32 < n) fb[c * SUB_PER_THREAD + r] = b;
+            }
+            // the warp's non-FIRST k-mers are queued so that every lane inserts
+            uint32_t qn = 0;
+#pragma unroll
+            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
+                const bool h = (highs >> r) & 1u;
+                const uint32_t b = __ballot_sync(FULL, h);
+                if (h) q[qn + (uint32_t)__popc(b & lt)] = k[r];
+                qn += (uint32_t)__popc(b);
+            }
+            __syncwarp();
+            for (uint32_t j = lane; j < qn; j += 32)
+                if (!sub_table_add(s_tk, s_tc, q[j])) full = true;
+            __syncwarp();
         }
         if (__syncthreads_or(full)) {
             if (tid == 0) {
@@ -2191,17 +2247,20 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
             continue;   // incomplete: the host counts the pass again with more sub-buckets
         }
         // 2. FIRST occurrences: a hit adds one to the table count, a miss is a
-        // k-mer seen once (counted, not a record: min_count >= 2)
-        for (uint32_t i0 = tid; i0 < lo_cnt; i0 += SUB_THREADS * SUB_PER_THREAD) {
+        // k-mer seen once (the mask words are this block's own writes, read
+        // after the barrier through L2)
+        for (uint32_t cc = warp; cc < n_chunks; cc += SUB_WARPS) {
+            uint32_t wb[SUB_PER_THREAD];
             unsigned long long kk[SUB_PER_THREAD];
 #pragma unroll
-            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
-                const uint32_t i = i0 + r * SUB_THREADS;
-                kk[r] = i < lo_cnt ? __ldcg(&keys[base + i]) : EMPTY_KEY;
-            }
+            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r)
+                wb[r] = cc * SUB_CHUNK + r * 32 < n ? __ldcg(&fb[cc * SUB_PER_THREAD + r]) : 0u;
+#pragma unroll
+            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r)
+                kk[r] = ((wb[r] >> lane) & 1u) ? __ldcs(&keys[base + cc * SUB_CHUNK + r * 32 + lane]) : EMPTY_KEY;
 #pragma unroll
             for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
-                if (i0 + r * SUB_THREADS >= lo_cnt) continue;
+                if (!((wb[r] >> lane) & 1u)) continue;
                 const int sl = sub_table_find(s_tk, kk[r]);
                 if (sl >= 0) atomicAdd(&s_tc[sl], 1u);
                 else ++n_low_only;
@@ -2213,32 +2272,32 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
         for (uint32_t i = tid; i < SUB_TABLE_SLOTS; i += SUB_THREADS) {
             if (s_tk[i] == EMPTY_KEY) continue;
             ++n_distinct;
-            const uint32_t c = s_tc[i] < count_max ? s_tc[i] : count_max;
-            if (c < SUB_HIST_BINS) atomicAdd(&s_hist[c], 1u);
-            else if (c < HIST_BINS) atomicAdd(&hist[c], 1ull);
+            const uint32_t cnt = s_tc[i] < count_max ? s_tc[i] : count_max;
+            if (cnt < SUB_HIST_BINS) atomicAdd(&s_hist[cnt], 1u);
+            else if (cnt < HIST_BINS) atomicAdd(&hist[cnt], 1ull);
             else {
-                const unsigned long long q = atomicAdd(&counters[C_OVF_LEN], 1ull);
-                if (q < ovf_cap) ovf[q] = c;
+                const unsigned long long qi = atomicAdd(&counters[C_OVF_LEN], 1ull);
+                if (qi < ovf_cap) ovf[qi] = cnt;
                 else atomicOr(&counters[C_FLAGS], ERR_HIST_OVERFLOW_FULL);
             }
-            keep += (c >= min_count && c <= max_count) ? 1u : 0u;
+            keep += (cnt >= min_count && cnt <= max_count) ? 1u : 0u;
         }
         uint32_t tk;
         const uint32_t ok = block_excl_scan_1024(keep, s_warp, tk);
         if (tid == 0) s_base = tk ? atomicAdd(&counters[C_REC_LEN], (unsigned long long)tk) : 0ull;
         __syncthreads();
-        unsigned long long q = s_base + ok;
+        unsigned long long qpos = s_base + ok;
         for (uint32_t i = tid; i < SUB_TABLE_SLOTS; i += SUB_THREADS) {
             if (s_tk[i] == EMPTY_KEY) continue;
-            const uint32_t c = s_tc[i] < count_max ? s_tc[i] : count_max;
-            if (c < min_count || c > max_count) continue;
-            if (q < rec_cap) {
-                rec_keys[q] = pair_reverse(s_tk[i]);
-                rec_counts[q] = c;
+            const uint32_t cnt = s_tc[i] < count_max ? s_tc[i] : count_max;
+            if (cnt < min_count || cnt > max_count) continue;
+            if (qpos < rec_cap) {
+                rec_keys[qpos] = pair_reverse(s_tk[i]);
+                rec_counts[qpos] = cnt;
             } else {
                 rec_full = true;
             }
-            ++q;
+            ++qpos;
         }
         __syncthreads();
     }
@@ -2910,7 +2969,7 @@ cudaError_t launch_merge_buckets(const unsigned long long *keys, const BucketRan
 }
 
 cudaError_t launch_subpart_count(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
-                                 const SubCfg *sc, uint32_t *sub_count, cudaStream_t st)
+                                 const SubCfg *sc, uint32_t *sub_count, cudaStream_t st, uint32_t stride)
 {
     if (!n_items) return cudaSuccess;
     int per_sm = 0;
@@ -2918,7 +2977,31 @@ cudaError_t launch_subpart_count(const unsigned long long *keys, const BucketRan
         per_sm = 1;
     const uint32_t grid = std::min<uint32_t>(n_items, (uint32_t)(sm_count() * per_sm));
     note_launch();
-    k_subpart_count<<<grid, 256, 0, st>>>(keys, rg, n_items, sc, sub_count);
+    k_subpart_count<<<grid, 256, 0, st>>>(keys, rg, n_items, sc, sub_count, stride < 1 ? 1u : stride);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_subpart_regions(const uint32_t *sampled, uint32_t n_sub, uint32_t stride, uint32_t *region,
+                                   unsigned long long *sub_off, unsigned long long *sub_end,
+                                   unsigned long long *sub_cursor, unsigned long long *scan_tmp, cudaStream_t st)
+{
+    if (!n_sub) return cudaSuccess;
+    note_launch();
+    k_subpart_regions<<<grid_for(n_sub, 256), 256, 0, st>>>(sampled, n_sub, stride, region);
+    cudaError_t e = launch_scan_u32(region, sub_off, n_sub, scan_tmp, st);
+    if (e != cudaSuccess) return e;
+    note_launch();
+    k_subpart_ends<<<grid_for(n_sub, 256), 256, 0, st>>>(sub_off, region, n_sub, sub_end, sub_cursor);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_subpart_sizes(const unsigned long long *sub_off, const unsigned long long *sub_cursor,
+                                 const unsigned long long *sub_end, uint32_t n_sub, uint64_t out_cap, uint32_t *count,
+                                 unsigned long long *overflow, cudaStream_t st)
+{
+    if (!n_sub) return cudaSuccess;
+    note_launch();
+    k_subpart_sizes<<<grid_for(n_sub, 256), 256, 0, st>>>(sub_off, sub_cursor, sub_end, n_sub, out_cap, count, overflow);
     return cudaGetLastError();
 }
 
@@ -2929,7 +3012,8 @@ static size_t subpart_scatter_smem(uint32_t max_sub)
 
 cudaError_t launch_subpart_scatter(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                    unsigned int *next_item, const SubCfg *sc, unsigned long long *sub_cursor,
-                                   unsigned long long *out, uint64_t out_cap, uint32_t max_sub, cudaStream_t st)
+                                   unsigned long long *out, uint64_t out_cap, uint32_t max_sub, cudaStream_t st,
+                                   const unsigned long long *sub_end)
 {
     if (!n_items) return cudaSuccess;
     if (!max_sub || max_sub > SUB_MAX_PER_BUCKET) return cudaErrorInvalidValue;
@@ -2945,29 +3029,31 @@ cudaError_t launch_subpart_scatter(const unsigned long long *keys, const BucketR
         per_sm = 1;
     const uint32_t grid = std::min<uint32_t>(n_items, (uint32_t)(sm_count() * per_sm));
     note_launch();
-    k_subpart_scatter<<<grid, SP_THREADS, smem, st>>>(keys, rg, n_items, next_item, sc, sub_cursor, out, out_cap, max_sub);
+    k_subpart_scatter<<<grid, SP_THREADS, smem, st>>>(keys, rg, n_items, next_item, sc, sub_cursor, sub_end, out,
+                                                      out_cap, max_sub);
     return cudaGetLastError();
 }
 
-cudaError_t launch_count_subs(unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count,
+cudaError_t launch_count_subs(const unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count,
                               const uint8_t *sub_bucket, uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub,
                               uint32_t count_max, uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
                               uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist, uint32_t *ovf,
-                              uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, cudaStream_t st)
+                              uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, uint32_t *first_bits,
+                              cudaStream_t st)
 {
     if (!n_sub) return cudaSuccess;
     if (min_count < 2) return cudaErrorInvalidValue;   // singletons are not records on this path
     cudaError_t e = cudaMemsetAsync(next_sub, 0, 4, st);
     if (e != cudaSuccess) return e;
     const size_t smem = (size_t)2 * SUB_SLICE_BLOCKS * 8 + (size_t)SUB_TABLE_SLOTS * (8 + 4) + SUB_HIST_BINS * 4 +
-                        (size_t)SUB_TILE * 8;
+                        (size_t)SUB_THREADS * SUB_PER_THREAD * 8;
     e = cudaFuncSetAttribute(k_count_subs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const uint32_t grid = std::min<uint32_t>(n_sub, (uint32_t)sm_count() * SUB_BLOCKS_PER_SM);
     note_launch();
     k_count_subs<<<grid, SUB_THREADS, smem, st>>>(keys, sub_off, sub_count, sub_bucket, n_sub, sc, next_sub, count_max,
                                                   min_count, max_count, rec_keys, rec_counts, rec_cap, hist, ovf,
-                                                  ovf_cap, counters, bucket_ovf);
+                                                  ovf_cap, counters, bucket_ovf, first_bits);
     return cudaGetLastError();
 }
 

@@ -40,6 +40,7 @@ enum Counter : int {
     C_SEL_A = 8,         // query selections
     C_SEL_B = 9,
     C_SUB_OVF = 10,      // sub-buckets whose shared-memory table overflowed
+    C_REGION_OVF = 11,   // nonzero: a sub-bucket outgrew its estimated region
     C_COUNT = 16
 };
 
@@ -289,23 +290,41 @@ cudaError_t launch_select_range(const unsigned long long *keys, const uint32_t *
 // cut into items of SUB_SCATTER_ITEM_KEYS keys (fill_item_starts_n).  count_subs: one
 // block per sub-bucket at a time runs the Bloom split with the filter slice in
 // shared memory, counts the non-FIRST occurrences in a shared-memory table,
-// merges the FIRST ones (written back over the front of the sub-bucket's
-// keys) and appends the table's records (counts saturated at count_max, kept
+// merges the FIRST ones (marked in a bit mask per sub-bucket) and appends the table's records (counts saturated at count_max, kept
 // when min_count <= count <= max_count) at rec_keys[C_REC_LEN...]; every
 // table count goes to hist/ovf, the totals to counters (C_REC_LEN,
 // C_LOW_LEN, C_HIGH_LEN, C_LOW_ONLY, C_DISTINCT) and the sub-buckets whose
 // table overflowed to C_SUB_OVF and bucket_ovf[their bucket] (the results
 // are then incomplete).
+// stride > 1: only every stride-th work item is counted (a sample).
 cudaError_t launch_subpart_count(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
-                                 const SubCfg *sc, uint32_t *sub_count, cudaStream_t st);
+                                 const SubCfg *sc, uint32_t *sub_count, cudaStream_t st, uint32_t stride = 1);
+// sub_end non-NULL: the sub-buckets' regions are estimates and a key is
+// written only inside its sub-bucket's region [.., sub_end[s]).
 cudaError_t launch_subpart_scatter(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                    unsigned int *next_item, const SubCfg *sc, unsigned long long *sub_cursor,
-                                   unsigned long long *out, uint64_t out_cap, uint32_t max_sub, cudaStream_t st);
-cudaError_t launch_count_subs(unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count,
+                                   unsigned long long *out, uint64_t out_cap, uint32_t max_sub, cudaStream_t st,
+                                   const unsigned long long *sub_end = nullptr);
+// Estimated regions from a 1-in-stride sampled count: region (u32 per
+// sub-bucket, scratch), sub_off (their exclusive scan), sub_end = sub_off +
+// region, sub_cursor = sub_off.  scan_tmp holds scan_tmp_words(n_sub) words.
+cudaError_t launch_subpart_regions(const uint32_t *sampled, uint32_t n_sub, uint32_t stride, uint32_t *region,
+                                   unsigned long long *sub_off, unsigned long long *sub_end,
+                                   unsigned long long *sub_cursor, unsigned long long *scan_tmp, cudaStream_t st);
+// Keys per sub-bucket after a scatter into estimated regions; a sub-bucket
+// that outgrew its region sets *overflow (its count is cut to its region).
+cudaError_t launch_subpart_sizes(const unsigned long long *sub_off, const unsigned long long *sub_cursor,
+                                 const unsigned long long *sub_end, uint32_t n_sub, uint64_t out_cap, uint32_t *count,
+                                 unsigned long long *overflow, cudaStream_t st);
+cudaError_t launch_count_subs(const unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count,
                               const uint8_t *sub_bucket, uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub,
                               uint32_t count_max, uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
                               uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist, uint32_t *ovf,
-                              uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, cudaStream_t st);
+                              uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, uint32_t *first_bits,
+                              cudaStream_t st);
+// words of the FIRST bit masks of count_subs for sub-buckets inside a key
+// array of key_cap keys (sub-bucket s at word (sub_off[s] >> 5) + s)
+inline uint64_t count_subs_mask_words(uint64_t key_cap, uint32_t n_sub) { return key_cap / 32 + n_sub + 2; }
 cudaError_t launch_bloom_buckets(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                  unsigned int *next_item, const BucketCfg *cfg, unsigned long long *bits,
                                  unsigned long long *out, unsigned long long *low_cnt, unsigned long long *high_cnt,

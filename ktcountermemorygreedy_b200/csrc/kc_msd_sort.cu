@@ -76,12 +76,13 @@ __device__ __forceinline__ uint32_t scan256(uint32_t v, uint32_t *s_warp, uint32
     return base + x - v;
 }
 
-// Records per bucket: hb[key >> shift] += 1.
+// Records per bucket: hb[(key >> shift) & bmask] += 1 (the mask keeps bits
+// above the sorted ones out of the index).
 __global__ void __launch_bounds__(256) k_msd_hist(const unsigned long long *keys, uint64_t n, uint32_t shift,
-                                                  uint32_t *hb)
+                                                  uint32_t bmask, uint32_t *hb)
 {
     for (uint64_t i = blockIdx.x * 256ull + threadIdx.x; i < n; i += (uint64_t)gridDim.x * 256)
-        atomicAdd(&hb[(uint32_t)(__ldcs(&keys[i]) >> shift)], 1u);
+        atomicAdd(&hb[(uint32_t)(__ldcs(&keys[i]) >> shift) & bmask], 1u);
 }
 
 // Stable ranks of the items of one block among the items with the same digit,
@@ -364,7 +365,7 @@ cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n
     if (e == cudaSuccess) e = cudaMemsetAsync(tile_ctr, 0, 16, st);
     if (e != cudaSuccess) return e;
     note_kernel_launch();
-    k_msd_hist<<<n_sms() * 8, 256, 0, st>>>(ka, n, shift2, hb);
+    k_msd_hist<<<n_sms() * 8, 256, 0, st>>>(ka, n, shift2, (uint32_t)(nb - 1), hb);
     e = launch_scan_u32(hb, ob, nb, stmp, st);
     if (e != cudaSuccess) return e;
     // the bucket sizes come to the host once: the second pass's tiles follow

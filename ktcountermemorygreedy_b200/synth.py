@@ -23,6 +23,9 @@ def gen() -> C.CDLL:
         L.kcgen_genome.restype = C.c_uint64
         L.kcgen_genome.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_uint32, C.c_uint32, C.c_uint32,
                                    C.c_uint32, C.c_uint32, C.c_double, C.c_void_p, C.c_int]
+        L.kcgen_genome_div.restype = C.c_uint64
+        L.kcgen_genome_div.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_uint32, C.c_uint32, C.c_uint32,
+                                       C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_void_p, C.c_int]
         L.kcgen_reads_size.restype = C.c_uint64
         L.kcgen_reads_size.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32]
         L.kcgen_reads.restype = C.c_uint64
@@ -41,6 +44,14 @@ def genome(seed: int, length: int, repeat_frac: float = 0.0, n_families: int = 0
     g = np.zeros(length, np.uint8)
     gen().kcgen_genome(seed, length, repeat_frac, n_families, fam_len[0], fam_len[1], copies[0], copies[1],
                        divergence, g.ctypes.data, threads())
+    return g
+
+
+def genome_div(seed: int, length: int, repeat_frac: float, n_families: int, fam_len, copies, divergence) -> np.ndarray:
+    """Genome whose repeat families each draw a divergence from U[divergence]."""
+    g = np.zeros(length, np.uint8)
+    gen().kcgen_genome_div(seed, length, repeat_frac, n_families, fam_len[0], fam_len[1], copies[0], copies[1],
+                           divergence[0], divergence[1], g.ctypes.data, threads())
     return g
 
 
@@ -87,6 +98,21 @@ def large_job(coverage: float = 30.0, genome_len: int = 100_000_000, out: np.nda
 
 
 def large_job_reads(coverage: float = 30.0, genome_len: int = 100_000_000) -> int:
+    return int(math.ceil(coverage * genome_len / 150))
+
+
+OUT_OF_CORE_GENOME_BP = 3_100_000_000
+
+
+def out_of_core_genome(genome_len: int = OUT_OF_CORE_GENOME_BP):
+    """Out-of-core job genome (seed 5): 45% from 2000 repeat families of
+    0.3-6 kbp with 1-10^5 copies (scaled to the 45% total), each family at a
+    divergence drawn from U[1%, 15%]."""
+    return genome_div(5, genome_len, 0.45, 2000, (300, 6000), (1, 100_000), (0.01, 0.15))
+
+
+def out_of_core_reads(coverage: float = 10.0, genome_len: int = OUT_OF_CORE_GENOME_BP) -> int:
+    """10x of 150 bp reads (about 207M for 3.1 Gbp); 1% substitutions, seed 5."""
     return int(math.ceil(coverage * genome_len / 150))
 
 

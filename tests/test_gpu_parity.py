@@ -696,3 +696,25 @@ def test_distinct_record_sort_matches_numpy(kc, n, bits, skew):
     order = np.argsort(keys)
     assert np.array_equal(got_k, keys[order])
     assert np.array_equal(got_c, counts[order])
+
+
+def test_sampled_subbucket_regions_give_exact_results(kc):
+    """The shared-memory Bloom path with sub-bucket regions estimated from a
+    1-in-8 sample (forced on small jobs here): exact records and histogram,
+    both when the estimates hold and when a sub-bucket outgrows its region
+    and the pass is counted again with exact regions."""
+    big = fixtures.random_fastq(31, 40000, (150, 150), genome_len=1_500_000, sub=0.01, n_rate=0.0)
+    small = fixtures.plain_small()
+    redos = 0
+    with kc.KmerCounter(max_inflight_jobs=1) as c:
+        c.set_tuning(bloom_smem=1, sampled_region_keys=1)
+        for data, k in ((big, 31), (small, 25), (big, 21)):
+            want_k, want_c = O.exact_records([data], k)
+            m = want_c >= 2
+            r = c.count([data], k=k, count_max=U32, bloom=True, memory_gb=2, min_count=2, hist_min=1, hist_max=500)
+            assert np.array_equal(r.keys, want_k[m]) and np.array_equal(r.counts, want_c[m]), k
+            assert r.hist.tolist() == O.histogram(want_c, 1, 500).tolist()
+            assert r.smem_passes == 1
+            redos += r.region_redos
+    # the small job's buckets are a few work items each: its estimates miss
+    assert redos >= 1
