@@ -158,7 +158,9 @@ typedef struct {
     uint16_t smem_fallbacks;      /* passes that left it after a sub-bucket table overflowed */
     uint32_t region_redos;        /* shared-memory passes counted again because a sub-bucket outgrew the
                                      region estimated from a sample of the pass's keys */
-    uint32_t reserved_r;
+    uint32_t batch_part;          /* batched jobs: the sub-batch (0, 1, ...) the sample was counted in; a
+                                     batch larger than a worker's share of the device-memory budget runs
+                                     as consecutive sub-batches, and device_ms is that sub-batch's time */
 } kc_result_t;
 
 /* Settings of a handle that trade memory for speed, chosen by kc_autotune or
@@ -220,8 +222,10 @@ int kc_cancel(kc_handle *h, kc_job_id id);
 
 /* Batched jobs: every job of the array is counted in one set of device passes
  * (one persistent extraction kernel over all samples' tiles, per-sample
- * tables in one arena).  Bloom mode is not available here.  ids[i] is the
- * id of jobs[i]; results are read per id as for kc_submit. */
+ * tables in one arena); a batch larger than a worker's share of the
+ * device-memory budget is cut into consecutive sub-batches of whole samples.
+ * Bloom mode is not available here.  ids[i] is the id of jobs[i]; results
+ * are read per id as for kc_submit. */
 int kc_submit_batch(kc_handle *h, const kc_job *jobs, uint32_t n_jobs, kc_job_id *ids);
 
 /* ---- pinned host memory (for zero-copy-speed uploads) -------------------- */

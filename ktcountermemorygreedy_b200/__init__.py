@@ -87,7 +87,7 @@ class kc_result_t(C.Structure):
                 ("run_ms", C.c_double), ("phase_ms", C.c_double * 12), ("phase_launches", C.c_uint64 * 12),
                 ("low_len", C.c_uint64), ("high_len", C.c_uint64), ("input_bytes", C.c_uint64),
                 ("n_records_total", C.c_uint64), ("passes", C.c_uint32), ("smem_passes", C.c_uint16),
-                ("smem_fallbacks", C.c_uint16), ("region_redos", C.c_uint32), ("reserved_r", C.c_uint32)]
+                ("smem_fallbacks", C.c_uint16), ("region_redos", C.c_uint32), ("batch_part", C.c_uint32)]
 
 # stage names of kc_result_t.phase_ms
 PHASES = ["census", "scan", "count_pass", "insert_high", "merge_low", "compact", "sort", "queries", "bloom",
@@ -220,6 +220,7 @@ class Result:
     smem_passes: int = 0      # passes counted per sub-bucket in shared memory (Bloom mode)
     smem_fallbacks: int = 0   # passes recounted on global-memory tables after a sub-bucket table overflowed
     region_redos: int = 0     # shared-memory passes counted again after a sub-bucket outgrew its estimated region
+    batch_part: int = 0       # batched jobs: the sub-batch the sample was counted in
 
 
 def _copy(ptr, n, dtype):
@@ -371,7 +372,8 @@ class KmerCounter:
             table_capacity=r.table_capacity, device_ms=r.device_ms, queue_ms=r.queue_ms, run_ms=r.run_ms,
             phase_ms=tuple(r.phase_ms), phase_launches=tuple(r.phase_launches), low_len=r.low_len,
             high_len=r.high_len, input_bytes=r.input_bytes, n_records_total=r.n_records_total, passes=r.passes,
-            smem_passes=r.smem_passes, smem_fallbacks=r.smem_fallbacks, region_redos=r.region_redos)
+            smem_passes=r.smem_passes, smem_fallbacks=r.smem_fallbacks, region_redos=r.region_redos,
+            batch_part=r.batch_part)
         if release:
             self.release(jid)
         return out

@@ -146,6 +146,7 @@ struct Job {
     uint64_t occurrences = 0, distinct = 0, low_only = 0, table_cap = 0;
     uint64_t low_len = 0, high_len = 0, input_bytes = 0, n_records_total = 0;
     uint32_t passes = 1, smem_passes = 0, smem_fallbacks = 0, region_redos = 0;
+    uint32_t batch_part = 0;   // sub-batch of a batched job
     double device_ms = 0;
     double phase_ms[KC_STAGES] = {0};
     uint64_t phase_launches[KC_STAGES] = {0};
@@ -1159,17 +1160,22 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
 
     // ---- sort in printed-string order ---------------------------------------
     clk.begin(6);
+    bool reversed = false;   // keys back in the k-mer word layout
     if (n_rec > 1) {
         const uint32_t skip = rec_by_bucket && job.passes <= 1 ? 8u : 0u;
         void *stmp = rec_in_sort_tmp ? sort_tmp : ds.get(record_sort_bytes(n_rec, k));
-        if (msd_sort_applies(n_rec, 2 * k) && tn.record_sort != 2)
-            CK(launch_msd_sort(rec_keys, rec_counts, n_rec, 2 * k, stmp, st, counters + C_FLAGS, rec_in_sort_tmp));
-        else
+        if (msd_sort_applies(n_rec, 2 * k) && tn.record_sort != 2) {
+            // the sort writes the k-mer words back (pair_reverse) as it stores
+            CK(launch_msd_sort(rec_keys, rec_counts, n_rec, 2 * k, stmp, st, counters + C_FLAGS, rec_in_sort_tmp,
+                               true));
+            reversed = true;
+        } else {
             CK(launch_radix_sort(rec_keys, rec_counts, n_rec, 2 * k, stmp, st, counters + C_FLAGS, skip,
                                  rec_in_sort_tmp));
+        }
         if (!rec_in_sort_tmp) ds.release(stmp);
     }
-    CK(launch_pair_reverse(rec_keys, n_rec, st));
+    if (!reversed) CK(launch_pair_reverse(rec_keys, n_rec, st));
     clk.end();
 
     // ---- histogram (with the counters, under one sync) ----------------------
@@ -1782,8 +1788,13 @@ void kc_input_free(kc_handle *h, kc_input *in)
 static int submit_task(kc_handle *h, const kc_job *jobs, uint32_t n, kc_job_id *ids, bool batch)
 {
     if (!h || !jobs || !ids || n == 0) return fail(KC_ERR_INVALID, "bad argument");
-    auto task = std::make_shared<Task>();
-    task->batch = batch;
+    // a batch larger than a worker's share of the device-memory budget runs
+    // as consecutive sub-batches (each one set of device passes), so that its
+    // samples stream through the device while earlier ones are counted
+    std::vector<std::shared_ptr<Task>> tasks(1, std::make_shared<Task>());
+    tasks[0]->batch = batch;
+    const uint64_t group_budget =
+        batch ? std::max<uint64_t>(h->budget / std::max<size_t>(h->workers.size(), 1), 1) : UINT64_MAX;
     try {
         for (uint32_t i = 0; i < n; ++i) {
             validate_job(jobs[i]);
@@ -1797,8 +1808,13 @@ static int submit_task(kc_handle *h, const kc_job *jobs, uint32_t n, kc_job_id *
             j->p.files = nullptr;
             j->input = jobs[i].input;
             j->reserve = reserve_for(jobs[i], jobs[i].input ? jobs[i].input->total_bytes : 0);
-            task->reserve += j->reserve;
-            task->jobs.push_back(j);
+            if (!tasks.back()->jobs.empty() && tasks.back()->reserve + j->reserve > group_budget) {
+                tasks.push_back(std::make_shared<Task>());
+                tasks.back()->batch = batch;
+            }
+            j->batch_part = (uint32_t)(tasks.size() - 1);
+            tasks.back()->reserve += j->reserve;
+            tasks.back()->jobs.push_back(j);
         }
     } catch (const KcError &e) {
         return fail(e.code, e.msg);
@@ -1807,14 +1823,16 @@ static int submit_task(kc_handle *h, const kc_job *jobs, uint32_t n, kc_job_id *
         std::lock_guard<std::mutex> lk(h->mu);
         if (h->closing) return fail(KC_ERR_INVALID, "handle is closing");
         double t = now_ms();
-        for (uint32_t i = 0; i < n; ++i) {
-            auto &j = task->jobs[i];
-            j->id = h->next_id++;
-            j->t_submit = t;
-            h->jobs[j->id] = j;
-            ids[i] = j->id;
+        uint32_t i = 0;
+        for (auto &task : tasks) {
+            for (auto &j : task->jobs) {
+                j->id = h->next_id++;
+                j->t_submit = t;
+                h->jobs[j->id] = j;
+                ids[i++] = j->id;
+            }
+            h->queue.push_back(task);
         }
-        h->queue.push_back(task);
     }
     h->cv_work.notify_all();
     return KC_OK;
@@ -1863,12 +1881,16 @@ int kc_autotune(kc_handle *h, const kc_job *jobs, uint32_t n_jobs, uint32_t batc
         if (!batch)
             for (uint32_t i = 0; i < n_jobs && rc == KC_OK; ++i) rc = kc_submit(h, &jobs[i], &ids[i]);
         ms = 0;
+        int64_t last_part = -1;   // a batch's sub-batches each report their device time once
         for (uint32_t i = 0; i < n_jobs; ++i) {
             if (!ids[i]) continue;
             const int w = kc_wait(h, ids[i], -1);
             if (w == KC_OK) {
                 kc_result_t r;
-                if (kc_result(h, ids[i], &r) == KC_OK && (!batch || i == 0)) ms += r.device_ms;
+                if (kc_result(h, ids[i], &r) == KC_OK && (!batch || (int64_t)r.batch_part != last_part)) {
+                    ms += r.device_ms;
+                    last_part = r.batch_part;
+                }
             } else if (rc == KC_OK) {
                 rc = w;
             }
@@ -1965,6 +1987,7 @@ int kc_result(kc_handle *h, kc_job_id id, kc_result_t *out)
     out->smem_passes = (uint16_t)std::min<uint32_t>(j.smem_passes, 0xFFFF);
     out->smem_fallbacks = (uint16_t)std::min<uint32_t>(j.smem_fallbacks, 0xFFFF);
     out->region_redos = j.region_redos;
+    out->batch_part = j.batch_part;
     return KC_OK;
 }
 

@@ -264,13 +264,15 @@ cudaError_t launch_radix_sort_in_scratch(unsigned long long *keys, uint32_t *val
 // pass by the top 8 bits and one by the next bits inside those ranges, then
 // every bucket sorted in shared memory (kc_msd_sort.cu).  Synchronizes the
 // stream once (the bucket sizes come to the host).  Result in keys/vals; with
-// input_in_tmp the records start in the alternate arrays (sort_tmp_alt).  For
-// n >= MSD_SORT_MIN_RECORDS and 24 <= bits <= 64 (msd_sort_applies).
+// input_in_tmp the records start in the alternate arrays (sort_tmp_alt);
+// with reverse_out the sorted keys are written with their 2-bit groups
+// reversed (pair_reverse).  For n >= MSD_SORT_MIN_RECORDS and
+// 24 <= bits <= 64 (msd_sort_applies).
 constexpr uint64_t MSD_SORT_MIN_RECORDS = 1ull << 20;
 bool msd_sort_applies(uint64_t n, uint32_t bits);
 size_t msd_sort_tmp_bytes(uint64_t n, uint32_t bits);
 cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
-                            cudaStream_t st, unsigned long long *flags, bool input_in_tmp);
+                            cudaStream_t st, unsigned long long *flags, bool input_in_tmp, bool reverse_out = false);
 // Counts one kernel launch of this library (kernels launched outside kc_kernels.cu).
 void note_kernel_launch();
 

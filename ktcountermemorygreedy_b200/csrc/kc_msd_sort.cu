@@ -218,10 +218,12 @@ __global__ void __launch_bounds__(MS_THREADS, 2) k_msd_scatter(const unsigned lo
 // Every bucket of at most MS_TILE records sorted in shared memory on the bits
 // below its prefix (low_bits), LSD with 8-bit digits; in place when kin ==
 // kout.  Larger buckets are copied unsorted (kin != kout) for the fallback.
+// reverse_out: the keys are written with their 2-bit groups reversed (the
+// printed-string order key back to the k-mer word).
 __global__ void __launch_bounds__(MS_THREADS, 3) k_bucket_sort(const unsigned long long *kin, const uint32_t *vin,
                                                                unsigned long long *kout, uint32_t *vout,
                                                                const uint32_t *hb, const unsigned long long *ob,
-                                                               uint32_t n_buckets, uint32_t low_bits)
+                                                               uint32_t n_buckets, uint32_t low_bits, int reverse_out)
 {
     extern __shared__ __align__(16) uint8_t bs_smem[];
     unsigned long long *s_keys = reinterpret_cast<unsigned long long *>(bs_smem);   // MS_TILE
@@ -233,12 +235,19 @@ __global__ void __launch_bounds__(MS_THREADS, 3) k_bucket_sort(const unsigned lo
     for (uint32_t b = blockIdx.x; b < n_buckets; b += gridDim.x) {
         const uint32_t m = hb[b];
         const unsigned long long base = ob[b];
-        if (m > MS_TILE || m <= 1 || passes == 0) {
+        if (m > MS_TILE) {   // sorted by the fallback, which also reverses the keys
             if (kin != kout)
                 for (uint32_t i = tid; i < m; i += MS_THREADS) {
                     kout[base + i] = kin[base + i];
                     vout[base + i] = vin[base + i];
                 }
+            continue;
+        }
+        if (m <= 1 || passes == 0) {
+            for (uint32_t i = tid; i < m; i += MS_THREADS) {
+                kout[base + i] = reverse_out ? pair_reverse(kin[base + i]) : kin[base + i];
+                vout[base + i] = vin[base + i];
+            }
             continue;
         }
         // items blocked per warp: warp w holds [w * per, (w + 1) * per)
@@ -281,7 +290,7 @@ __global__ void __launch_bounds__(MS_THREADS, 3) k_bucket_sort(const unsigned lo
         for (uint32_t r = 0; r < MS_ITEMS; ++r) {
             const uint32_t li = first + r * 32 + lane;
             if (r < steps && li < m) {
-                kout[base + li] = k[r];
+                kout[base + li] = reverse_out ? pair_reverse(k[r]) : k[r];
                 vout[base + li] = v[r];
             }
         }
@@ -328,7 +337,7 @@ size_t msd_sort_tmp_bytes(uint64_t n, uint32_t bits)
 }
 
 cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
-                            cudaStream_t st, unsigned long long *flags, bool input_in_tmp)
+                            cudaStream_t st, unsigned long long *flags, bool input_in_tmp, bool reverse_out)
 {
     if (!msd_sort_applies(n, bits)) return cudaErrorInvalidValue;
     const uint32_t P = msd_prefix_bits(n, bits), P2 = P - 8;
@@ -418,11 +427,13 @@ cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n
     uint32_t *vs = P2 ? va : vb;
     note_kernel_launch();
     k_bucket_sort<<<(unsigned)std::min<uint64_t>(nb, (uint64_t)n_sms() * 3), MS_THREADS, smem, st>>>(
-        ks, vs, keys, vals, hb, ob, (uint32_t)nb, shift2);
+        ks, vs, keys, vals, hb, ob, (uint32_t)nb, shift2, reverse_out ? 1 : 0);
     // buckets too large for one block: each sorted on its own on the bits
     // below the prefix, with the alternate arrays as working memory
-    for (size_t i = 0; i < big_start.size() && e == cudaSuccess; ++i)
+    for (size_t i = 0; i < big_start.size() && e == cudaSuccess; ++i) {
         e = launch_radix_sort_in_scratch(keys + big_start[i], vals + big_start[i], big_len[i], shift2, fallback_tmp, st);
+        if (e == cudaSuccess && reverse_out) e = launch_pair_reverse(keys + big_start[i], big_len[i], st);
+    }
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }

@@ -718,3 +718,20 @@ def test_sampled_subbucket_regions_give_exact_results(kc):
             redos += r.region_redos
     # the small job's buckets are a few work items each: its estimates miss
     assert redos >= 1
+
+
+def test_batch_larger_than_the_budget_runs_as_sub_batches(kc):
+    """A batch whose samples exceed a worker's share of the device-memory
+    budget is cut into consecutive sub-batches; every sample's results equal
+    the sample counted alone."""
+    samples = [fixtures.random_fastq(40 + i, 1500 + 300 * i, (100, 150), genome_len=60_000, sub=0.01, n_rate=0.0)
+               for i in range(6)]
+    ks = [21 if i % 2 == 0 else 31 for i in range(6)]
+    job = dict(count_max=U32, min_count=1, hist_min=1, hist_max=300)
+    with kc.KmerCounter(max_inflight_jobs=2, hbm_budget_bytes=300 << 20) as c:
+        res = c.count_batch([[s] for s in samples], ks, **job)
+        alone = [c.count([s], k=k, **job) for s, k in zip(samples, ks)]
+    assert len({r.batch_part for r in res}) > 1
+    for r, a in zip(res, alone):
+        assert np.array_equal(r.keys, a.keys) and np.array_equal(r.counts, a.counts)
+        assert r.hist.tolist() == a.hist.tolist()
