@@ -341,6 +341,37 @@ def sample_on_gpu(counter, kc, path: str, reps: int = 3):
     return value, res
 
 
+def full_reference_check(args, counter, fq, full):
+    """The reference programs once on the whole workload (its FASTQ written
+    to a file by the generator program): counter + histogram_tool precise
+    (min 2), wall time, and the histogram text against the GPU job's."""
+    import ktcountermemorygreedy_b200 as kc
+    threads, model = cpu_info()
+    mem = int(os.environ.get("KC_REF_MEM_GB", "64"))
+    ram_gb = None
+    try:
+        ram_gb = round(os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES") / 2**30)
+    except (ValueError, OSError):
+        pass
+    if not reference_programs_present():
+        return {"status": "not run: the reference programs are absent"}
+    with tempfile.TemporaryDirectory(dir=os.environ.get("KC_REF_TMP")) as tmp:
+        path = os.path.join(tmp, "full.fq")
+        n_reads = int(math.ceil(30.0 * 100_000_000 / 150))
+        nbytes = write_workload(path, n_reads)
+        if nbytes != len(fq):
+            return {"status": f"not run: the generator wrote {nbytes} B, the job has {len(fq)} B"}
+        w, occ = reference_run(path, max(6, threads), mem, tmp, dump=False)
+        if full is None:
+            full = counter.count([fq], keep_records=False, **JOB)
+        same = open(os.path.join(tmp, "h.tsv")).read() == kc.histogram_text(full.hist, JOB["hist_min"])
+    return {"histogram_identical": same, "wall_s": round(w, 2), "occurrences": occ,
+            "kmers_per_s": occ / w, "cores": max(6, threads), "cpu": model, "ram_gb": ram_gb, "memory_gb_arg": mem,
+            "how": "kmer_counter <fq> 31 <cores> <mem> <tmp> 1024 2 u32max u32max + histogram_tool precise "
+                   "<tmp> <cores> <mem> h.tsv 2 10000 on the whole 20M-read FASTQ; h.tsv against the GPU job's "
+                   "histogram text"}
+
+
 def cpu_leg(args, counter, fq, full):
     import ktcountermemorygreedy_b200 as kc
     SP = _checker()
@@ -368,6 +399,8 @@ def cpu_leg(args, counter, fq, full):
     except Exception as e:   # the baseline is reported, never required
         cpu = cpu or {"value": None, "unit": "k-mers/s", "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
         parity.setdefault("sample", f"failed: {e}")
+    if args.full_reference:
+        parity["full_reference"] = full_reference_check(args, counter, fq, full)
     try:
         if full is None:
             full = counter.count([fq], keep_records=True, copy=False, **JOB)
@@ -754,6 +787,9 @@ def main():
     ap.add_argument("--out-of-core", action="store_true",
                     help="also run the out-of-core job (3.1 Gbp, 10x, 65 GB FASTQ; minutes, host memory ~100 GB)")
     ap.add_argument("--ooc-scale", type=float, default=1.0, help="genome size factor of the out-of-core job")
+    ap.add_argument("--full-reference", action="store_true",
+                    help="also run the reference programs once on the whole workload (minutes; ~20 GB of disk "
+                         "under $KC_REF_TMP) and compare their histogram with the GPU's")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
