@@ -182,11 +182,7 @@ typedef struct {
                                      their sub-buckets from a 1-in-8 sample of the k-mers instead of
                                      counting them all (a sub-bucket that outgrows its estimate sends the
                                      pass back to exact counts); default 64M */
-    uint64_t part_scatter;        /* partition into root-prefix buckets: 1 reorders each tile's k-mers by
-                                     bucket in shared memory and stores runs of one bucket, 2 stores each
-                                     k-mer straight to its slot (one tile buffer, more blocks per SM);
-                                     default 1 */
-    uint64_t reserved[1];
+    uint64_t reserved[2];
 } kc_tuning;
 
 /* Kernel launches issued by this process so far (all handles). */

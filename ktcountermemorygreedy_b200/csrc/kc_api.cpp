@@ -77,7 +77,6 @@ kc_tuning default_tuning()
     t.bloom_smem = 1;
     t.record_sort = 1;
     t.sampled_region_keys = 64ull << 20;
-    t.part_scatter = 1;
     return t;
 }
 
@@ -802,7 +801,6 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
             a.bucket_end = bbase + N_BUCKETS;
             a.bucket_lo = lo;
             a.bucket_hi = hi;
-            const int part_mode = tn.part_scatter == 2 ? MODE_PART_DIRECT : MODE_PART;
             clk.begin(2);
             if (streamed && chunks_done < cu.ev.size()) {
                 // the rest of the file goes up behind this pass's small uploads;
@@ -811,18 +809,18 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                 cu.enqueue(cu.ev.size());
                 a.tile0 = 0;
                 a.n_tiles = tiles_ready;
-                CK(launch_extract(part_mode, a, 0, st));
+                CK(launch_extract(MODE_PART, a, 0, st));
                 while (chunks_done < cu.ev.size()) {
                     const uint64_t t0 = tiles_ready;
                     census_chunks(chunks_done + 1);
                     a.tile0 = t0;
                     a.n_tiles = tiles_ready - t0;
-                    CK(launch_extract(part_mode, a, 0, st));
+                    CK(launch_extract(MODE_PART, a, 0, st));
                 }
                 a.tile0 = 0;
                 a.n_tiles = T;
             } else {
-                CK(launch_extract(part_mode, a, 0, st));
+                CK(launch_extract(MODE_PART, a, 0, st));
             }
             clk.end();
             unsigned long long *p_fill = hs.n<unsigned long long>(N_BUCKETS);
@@ -1858,7 +1856,6 @@ int kc_set_tuning(kc_handle *h, const kc_tuning *t)
     if (t->table_factor > 0 && t->table_factor < 1.05) return fail(KC_ERR_INVALID, "table_factor must be at least 1.05");
     if (t->bloom_smem > 2) return fail(KC_ERR_INVALID, "bloom_smem must be 1 or 2");
     if (t->record_sort > 2) return fail(KC_ERR_INVALID, "record_sort must be 1 or 2");
-    if (t->part_scatter > 2) return fail(KC_ERR_INVALID, "part_scatter must be 1 or 2");
     std::lock_guard<std::mutex> lk(h->mu);
     if (t->bucket_table_factor > 0) h->tuning.bucket_table_factor = t->bucket_table_factor;
     if (t->table_factor > 0) h->tuning.table_factor = t->table_factor;
@@ -1866,7 +1863,6 @@ int kc_set_tuning(kc_handle *h, const kc_tuning *t)
     if (t->bloom_smem > 0) h->tuning.bloom_smem = t->bloom_smem;
     if (t->record_sort > 0) h->tuning.record_sort = t->record_sort;
     if (t->sampled_region_keys > 0) h->tuning.sampled_region_keys = t->sampled_region_keys;
-    if (t->part_scatter > 0) h->tuning.part_scatter = t->part_scatter;
     return KC_OK;
 }
 
@@ -1908,9 +1904,8 @@ int kc_autotune(kc_handle *h, const kc_job *jobs, uint32_t n_jobs, uint32_t batc
     int rc = run(cur, cur_ms);   // warm-up: workspaces and pinned blocks reach this shape
     if (rc == KC_OK) rc = run(cur, cur_ms);
     const double bucket_c[] = {2.0, 3.0, 4.0}, table_c[] = {1.3, 1.6, 2.2};
-    const uint64_t group_c[] = {2ull << 20, 4ull << 20, 8ull << 20}, smem_c[] = {1, 2, 1}, sort_c[] = {1, 2, 1},
-                   part_c[] = {1, 2, 1};
-    for (int param = 0; param < 6 && rc == KC_OK; ++param)
+    const uint64_t group_c[] = {2ull << 20, 4ull << 20, 8ull << 20}, smem_c[] = {1, 2, 1}, sort_c[] = {1, 2, 1};
+    for (int param = 0; param < 5 && rc == KC_OK; ++param)
         for (int c = 0; c < 3 && rc == KC_OK; ++c) {
             kc_tuning t = cur;
             if (param == 0) t.bucket_table_factor = bucket_c[c];
@@ -1918,7 +1913,6 @@ int kc_autotune(kc_handle *h, const kc_job *jobs, uint32_t n_jobs, uint32_t batc
             if (param == 2) t.sort_group_records = group_c[c];
             if (param == 3) t.bloom_smem = smem_c[c];
             if (param == 4) t.record_sort = sort_c[c];
-            if (param == 5) t.part_scatter = part_c[c];
             if (std::memcmp(&t, &cur, sizeof(t)) == 0) continue;
             rc = run(t, ms);
             if (rc == KC_OK && ms < 0.98 * cur_ms) {   // a clear gain only

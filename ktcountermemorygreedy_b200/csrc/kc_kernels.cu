@@ -384,23 +384,12 @@ __global__ void k_chunk_lastnl(const int32_t *tile_lastnl, const uint32_t *tile_
 // extraction
 // ---------------------------------------------------------------------------
 
-// MODE_PART_DIRECT: the partition with one tile buffer (the next tile's bulk
-// copy is issued as soon as the current tile is classified) and each k-mer
-// stored straight to its bucket slot (bucket base + rank) instead of a
-// reorder by bucket in shared memory: fewer barriers and registers, four
-// blocks per SM, stores not grouped by bucket.
 template <int MODE>
-__global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : (MODE == MODE_PART_DIRECT ? 4 : 3))
-    k_extract(ExtractArgs a, uint32_t stage_cap)
+__global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extract(ExtractArgs a, uint32_t stage_cap)
 {
-    constexpr bool PARTM = MODE == MODE_PART || MODE == MODE_PART_DIRECT;
-    constexpr bool SINGLE_BUF = MODE == MODE_PART_DIRECT;
     extern __shared__ __align__(128) uint8_t smem[];
-    uint8_t *sbuf[2] = {smem, SINGLE_BUF ? smem : smem + BUF_BYTES};
-    // the chunk list of the emission lives in the other tile buffer, or (one
-    // buffer) in an array of its own, since the next tile lands meanwhile
-    uint32_t *s_chunk_own = reinterpret_cast<uint32_t *>(smem + BUF_BYTES);   // SINGLE_BUF: 4 * EXT_THREADS
-    uint64_t *s_codes = reinterpret_cast<uint64_t *>(smem + (SINGLE_BUF ? BUF_BYTES + 16 * EXT_THREADS : 2 * BUF_BYTES));   // 257 used
+    uint8_t *sbuf[2] = {smem, smem + BUF_BYTES};
+    uint64_t *s_codes = reinterpret_cast<uint64_t *>(smem + 2 * BUF_BYTES);   // 257 used
     uint64_t *s_rcodes = s_codes + 264;                                       // 257 used
     uint32_t *s_good = reinterpret_cast<uint32_t *>(s_rcodes + 264);          // 257 used
     unsigned long long *s_stage = reinterpret_cast<unsigned long long *>(s_good + 264);
@@ -414,8 +403,8 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : (MODE == 
     __shared__ __align__(8) uint64_t mbar[2];
     __shared__ uint32_t s_warp[8];
     __shared__ uint32_t s_hist[256];
-    __shared__ uint32_t s_bhist[MODE == MODE_SCAN || PARTM ? 256 : 1];
-    __shared__ unsigned long long s_bpos[PARTM ? 256 : 1];
+    __shared__ uint32_t s_bhist[MODE == MODE_SCAN || MODE == MODE_PART ? 256 : 1];
+    __shared__ unsigned long long s_bpos[MODE == MODE_PART ? 256 : 1];
     __shared__ unsigned long long s_bcast[2];
     __shared__ unsigned long long s_boff[MODE == MODE_BLOOM ? 256 : 1];
     __shared__ unsigned long long s_bcap[MODE == MODE_BLOOM ? 256 : 1];
@@ -456,16 +445,16 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : (MODE == 
         const int s = iter & 1;
         const uint64_t un = u + gridDim.x;
         pending_next = un < n_iter;
-        const uint64_t tnext = pending_next ? ((MODE == MODE_SCAN && a.visit) ? (uint64_t)a.visit[un] : a.tile0 + un) : 0;
-        if (!SINGLE_BUF && tid == 0 && pending_next) {
+        if (tid == 0 && pending_next) {
+            const uint64_t tn = (MODE == MODE_SCAN && a.visit) ? (uint64_t)a.visit[un] : a.tile0 + un;
             fence_proxy_async_smem();
             mbar_expect_tx(&mbar[s ^ 1], BUF_BYTES);
-            bulk_load(sbuf[s ^ 1], a.buf + tnext * TILE - HALO, BUF_BYTES, &mbar[s ^ 1]);
+            bulk_load(sbuf[s ^ 1], a.buf + tn * TILE - HALO, BUF_BYTES, &mbar[s ^ 1]);
         }
-        bool ok = SINGLE_BUF ? mbar_wait(&mbar[0], iter & 1) : mbar_wait(&mbar[s], (iter >> 1) & 1);
+        bool ok = mbar_wait(&mbar[s], (iter >> 1) & 1);
         if (__syncthreads_or(!ok)) {
             if (tid == 0) atomicOr(flags, ERR_WAIT_TIMEOUT);
-            if (!SINGLE_BUF && pending_next) mbar_wait(&mbar[s ^ 1], ((iter + 1) >> 1) & 1);
+            if (pending_next) mbar_wait(&mbar[s ^ 1], ((iter + 1) >> 1) & 1);
             return;
         }
         const uint8_t *tb = sbuf[s];
@@ -527,12 +516,6 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : (MODE == 
             }
         }
         __syncthreads();
-        if (SINGLE_BUF && tid == 0 && pending_next) {
-            // the tile is classified: its buffer takes the next tile now
-            fence_proxy_async_smem();
-            mbar_expect_tx(&mbar[0], BUF_BYTES);
-            bulk_load(sbuf[0], a.buf + tnext * TILE - HALO, BUF_BYTES, &mbar[0]);
-        }
 
         // windows of k valid bases ending in this thread's segment
         const uint64_t g = (uint64_t)s_good[tid] | ((uint64_t)s_good[tid + 1] << 32);
@@ -620,7 +603,7 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : (MODE == 
             uint32_t packed_tot;
             const uint32_t packed = block_excl_scan((uint32_t)__popc(ends) | (nq << 16), s_warp, packed_tot);
             const uint32_t tot = packed_tot & 0xFFFFu, n_chunks = packed_tot >> 16;
-            uint32_t *s_chunk = SINGLE_BUF ? s_chunk_own : reinterpret_cast<uint32_t *>(sbuf[s]);   // <= 4 * EXT_THREADS
+            uint32_t *s_chunk = reinterpret_cast<uint32_t *>(sbuf[s]);   // <= 4 * EXT_THREADS entries
             {
                 // chunk = first window index << 18 | segment << 10 | quarter << 8 | its 8 end bits
                 uint32_t idx = packed & 0xFFFFu, c = packed >> 16;
@@ -631,7 +614,7 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : (MODE == 
                     idx += (uint32_t)__popc(e8);
                 }
             }
-            if (PARTM) s_bhist[tid] = 0;
+            if (MODE == MODE_PART) s_bhist[tid] = 0;
             __syncthreads();
             const uint32_t blo = a.bucket_lo, bhi = a.bucket_hi ? a.bucket_hi : N_BUCKETS;
             for (uint32_t base = 0; base < tot; base += stage_cap) {
@@ -655,7 +638,7 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : (MODE == 
                                 const uint64_t f = fwd & kp.topmask;
                                 const unsigned long long key = f < rc ? f : rc;
                                 s_stage[idx - base] = key;
-                                if (PARTM) {
+                                if (MODE == MODE_PART) {
                                     // rank inside the tile's share of its bucket (a
                                     // pass of a multi-pass job keeps only its range)
                                     const uint32_t bk = (uint32_t)(key >> 56);
@@ -715,22 +698,6 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : (MODE == 
                         const unsigned long long pos = s_bpos[b] + i;
                         // a bucket that outgrows its estimated region is
                         // reported (its cursor passes the end) and redone
-                        if (pos < a.bucket_end[b] && pos < a.list_cap) a.list[pos] = key;
-                    }
-                } else if (MODE == MODE_PART_DIRECT) {
-                    // this tile's range of bucket tid, then every k-mer to
-                    // its bucket base + rank (a bucket that outgrows its
-                    // estimated region is reported by its cursor and redone)
-                    const uint32_t c = s_bhist[tid];
-                    s_bhist[tid] = 0;   // the next round's ranks (emission is done)
-                    s_bpos[tid] = c ? a.bucket_base[tid] + atomicAdd(&a.bucket_cursor[tid], (unsigned long long)c) : 0ull;
-                    __syncthreads();
-                    for (uint32_t i = tid; i < nr; i += EXT_THREADS) {
-                        const uint32_t rk = s_rank[i];
-                        if (rk == 0xFFFFu) continue;
-                        const unsigned long long key = s_stage[i];
-                        const uint32_t b = (uint32_t)(key >> 56);
-                        const unsigned long long pos = s_bpos[b] + rk;
                         if (pos < a.bucket_end[b] && pos < a.list_cap) a.list[pos] = key;
                     }
                 } else if (MODE == MODE_EMIT) {
@@ -2425,7 +2392,7 @@ void note_kernel_launch() { note_launch(); }
 
 size_t extract_smem_bytes_for(int mode, uint32_t stage_cap)
 {
-    size_t b = (mode == MODE_PART_DIRECT ? BUF_BYTES + 16 * EXT_THREADS : 2 * BUF_BYTES) + 264 * 8 * 2 + 264 * 4;
+    size_t b = 2 * BUF_BYTES + 264 * 8 * 2 + 264 * 4;
     if (mode != MODE_SCAN) b += (size_t)stage_cap * 8;
     else b += HLL_M * 4;
     if (mode != MODE_SCAN) b += (size_t)stage_cap * 2;
@@ -2483,7 +2450,6 @@ cudaError_t launch_extract(int mode, const ExtractArgs &a, int grid, cudaStream_
     case MODE_BLOOM: return launch_extract_t<MODE_BLOOM>(a, grid, STAGE_CAP, st);
     case MODE_EMIT: return launch_extract_t<MODE_EMIT>(a, grid, STAGE_CAP, st);
     case MODE_PART: return launch_extract_t<MODE_PART>(a, grid, STAGE_CAP, st);
-    case MODE_PART_DIRECT: return launch_extract_t<MODE_PART_DIRECT>(a, grid, STAGE_CAP_DIRECT, st);
     default: return cudaErrorInvalidValue;
     }
 }

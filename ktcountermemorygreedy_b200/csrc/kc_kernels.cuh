@@ -121,9 +121,7 @@ struct ExtractArgs {
     const unsigned long long *bucket_end;     // 256 end offsets in `list` (PART)
 };
 
-enum ExtractMode : int { MODE_SCAN = 0, MODE_INSERT = 1, MODE_BLOOM = 2, MODE_EMIT = 3, MODE_PART = 4,
-                         MODE_PART_DIRECT = 5 };
-constexpr uint32_t STAGE_CAP_DIRECT = 3328;   // staged k-mers per round of MODE_PART_DIRECT (4 blocks per SM)
+enum ExtractMode : int { MODE_SCAN = 0, MODE_INSERT = 1, MODE_BLOOM = 2, MODE_EMIT = 3, MODE_PART = 4 };
 
 constexpr uint32_t WORK_ITEM_KEYS = 2048;   // k-mers per work item (8 per thread)
 constexpr uint32_t BUCKET_HLL_BITS = 10;    // HyperLogLog registers per bucket = 2^10

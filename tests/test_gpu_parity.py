@@ -735,30 +735,3 @@ def test_batch_larger_than_the_budget_runs_as_sub_batches(kc):
     for r, a in zip(res, alone):
         assert np.array_equal(r.keys, a.keys) and np.array_equal(r.counts, a.counts)
         assert r.hist.tolist() == a.hist.tolist()
-
-
-@pytest.mark.parametrize("part_scatter,record_sort", [(2, 1), (1, 2), (2, 2)])
-def test_partition_and_sort_variants_same_results(kc, part_scatter, record_sort):
-    """The partition's two scatter forms (a shared-memory reorder by bucket,
-    or every k-mer stored straight to its slot) and the two record sorts
-    (most significant bits first, LSD) give the same records and histogram:
-    Bloom jobs (one pass and several), a plain job on the partitioned path."""
-    import ktcountermemorygreedy_b200.synth as S
-    g = S.genome(71, 3_000_000)
-    big = S.reads(g, 71, 60_000, (150, 150), 0.01, 0.0)
-    jobs = [dict(k=31, count_max=U32, bloom=True, memory_gb=4, min_count=2, hist_min=1, hist_max=1000),
-            dict(k=25, count_max=U32, bloom=True, memory_gb=4, min_count=2, hist_min=1, hist_max=1000,
-                 pass_bytes=96 << 20),
-            dict(k=31, count_max=U32, min_count=1, hist_min=1, hist_max=1000)]
-    with kc.KmerCounter(max_inflight_jobs=1) as c:
-        ref = [c.count([big], **j) for j in jobs]
-        c.set_tuning(part_scatter=part_scatter, record_sort=record_sort)
-        assert c.tuning["part_scatter"] == part_scatter and c.tuning["record_sort"] == record_sort
-        for j, want in zip(jobs, ref):
-            got = c.count([big], **j)
-            assert np.array_equal(got.keys, want.keys) and np.array_equal(got.counts, want.counts), j
-            assert got.hist.tolist() == want.hist.tolist()
-    # and the first job against the oracle
-    wk, wc = O.exact_records([big.tobytes()], 31)
-    m = wc >= 2
-    assert np.array_equal(ref[0].keys, wk[m]) and np.array_equal(ref[0].counts, wc[m])
