@@ -97,8 +97,8 @@ def test_cancelled_queued_job_leaves_the_others_exact(kc, data, want):
         ra = c.result(a, 25)
         assert np.array_equal(ra.keys, big_want[0]) and np.array_equal(ra.counts, big_want[1])
         c.wait(b)
-        assert _exact(c.result(b, 31), want)
         assert not c.cancel(b)   # finished: nothing to cancel
+        assert _exact(c.result(b, 31), want)
 
 
 def test_cancelled_running_job_gives_back_its_memory(kc, data, want):

@@ -735,3 +735,26 @@ def test_batch_larger_than_the_budget_runs_as_sub_batches(kc):
     for r, a in zip(res, alone):
         assert np.array_equal(r.keys, a.keys) and np.array_equal(r.counts, a.counts)
         assert r.hist.tolist() == a.hist.tolist()
+
+
+@pytest.mark.parametrize("record_sort", [1, 2])
+def test_record_sort_variants_same_results(kc, record_sort):
+    """The two record sorts (most significant bits first, LSD) give the same
+    records and histogram: Bloom jobs (one pass and several), a plain job on
+    the partitioned path."""
+    import ktcountermemorygreedy_b200.synth as S
+    g = S.genome(71, 3_000_000)
+    big = S.reads(g, 71, 60_000, (150, 150), 0.01, 0.0)
+    jobs = [dict(k=31, count_max=U32, bloom=True, memory_gb=4, min_count=2, hist_min=1, hist_max=1000),
+            dict(k=25, count_max=U32, bloom=True, memory_gb=4, min_count=2, hist_min=1, hist_max=1000,
+                 pass_bytes=96 << 20),
+            dict(k=31, count_max=U32, min_count=1, hist_min=1, hist_max=1000)]
+    with kc.KmerCounter(max_inflight_jobs=1) as c:
+        c.set_tuning(record_sort=record_sort)
+        assert c.tuning["record_sort"] == record_sort
+        got = [c.count([big], **j) for j in jobs]
+    for j, r in zip(jobs, got):
+        wk, wc = O.exact_records([big.tobytes()], j["k"])
+        m = (wc >= j["min_count"])
+        assert np.array_equal(r.keys, wk[m]) and np.array_equal(r.counts, wc[m]), j
+        assert r.hist.tolist() == O.histogram(wc, 1, 1000).tolist()
