@@ -352,22 +352,27 @@ class KmerCounter:
 
     def result(self, jid: int, k: int, release: bool = True, copy: bool = True) -> Result:
         """Results of a finished job.  copy=False returns the sorted records
-        as views of the job's pinned host memory; the job is released when
-        the last view is gone."""
+        and the count <= 2 set as views of the job's pinned host memory; the
+        job is released when the last view is gone."""
         r = kc_result_t()
         _check(lib().kc_result(self._h, jid, C.byref(r)))
         if copy:
             keys, counts = _copy(r.keys, r.n_records, np.uint64), _copy(r.counts, r.n_records, np.uint32)
+            le2_keys, le2_counts = _copy(r.le2_keys, r.n_le2, np.uint64), _copy(r.le2_counts, r.n_le2, np.uint32)
         else:
+            # records and the count <= 2 set (often most of the k-mers) stay in
+            # the job's pinned memory until the last view is gone
             lease = _JobLease(self, jid)
             keys, counts = _view(r.keys, r.n_records, np.uint64, lease), _view(r.counts, r.n_records, np.uint32, lease)
+            le2_keys = _view(r.le2_keys, r.n_le2, np.uint64, lease)
+            le2_counts = _view(r.le2_counts, r.n_le2, np.uint32, lease)
             release = False
         out = Result(
             k=k,
             keys=keys, counts=counts,
             hist=_copy(r.hist, r.hist_len, np.int64), hist_min=0,
             top_keys=_copy(r.top_keys, r.n_top, np.uint64), top_counts=_copy(r.top_counts, r.n_top, np.uint32),
-            le2_keys=_copy(r.le2_keys, r.n_le2, np.uint64), le2_counts=_copy(r.le2_counts, r.n_le2, np.uint32),
+            le2_keys=le2_keys, le2_counts=le2_counts,
             occurrences=r.occurrences, distinct=r.distinct, low_only=r.low_only,
             table_capacity=r.table_capacity, device_ms=r.device_ms, queue_ms=r.queue_ms, run_ms=r.run_ms,
             phase_ms=tuple(r.phase_ms), phase_launches=tuple(r.phase_launches), low_len=r.low_len,

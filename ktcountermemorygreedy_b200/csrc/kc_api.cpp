@@ -949,10 +949,9 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                                                 counters + C_REGION_OVF, st));
                     clk.end();
                     clk.begin(10);
-                    uint32_t *first_bits = ds.n<uint32_t>(count_subs_mask_words(list_cap, n_sub));
                     CK(launch_count_subs(list, sub_off, sub_count, d_sb, n_sub, d_sc, sub_next, count_max,
                                          P.min_count, P.max_count, rk, rc, rcap, hist_sub, ovf, ovf_cap, counters,
-                                         bucket_ovf, first_bits, st));
+                                         bucket_ovf, st));
                     clk.end();
                     if (attempt == 0 && (P.fault_inject & KC_INJECT_TABLE_FULL_ONCE)) {
                         // as if the first bucket's sub-bucket tables had overflowed

@@ -1866,7 +1866,6 @@ __global__ void __launch_bounds__(256) k_subpart_count(const unsigned long long 
     uint32_t cur = N_BUCKETS;
     SubCfg c{};
     for (uint32_t it = it0; it < it1; ++it) {
-        if (stride > 1 && it % stride) continue;   // a sample of the items
         const WorkItem w = work_item(rg, s_item0, it);
         if (w.bucket != cur) {
             if (cur != N_BUCKETS) {
@@ -1880,6 +1879,19 @@ __global__ void __launch_bounds__(256) k_subpart_count(const unsigned long long 
             }
             cur = w.bucket;
             c = sc[cur];
+        }
+        if (stride > 1) {
+            // a sample: every stride-th run of 4 keys (one 32-byte sector).
+            // Sampling single sectors rather than whole work items keeps the
+            // sampled count of a sub-bucket close to binomial: a work item
+            // holds several keys of each sub-bucket, and sampling items would
+            // multiply the count's variance by about that number.
+            for (unsigned long long j = tid;; j += 256) {
+                const unsigned long long i = w.begin + 4ull * stride * (j >> 2) + (j & 3);
+                if (i >= w.end) break;
+                atomicAdd(&s_h[sub_of(__ldcs(&keys[i]), c)], 1u);
+            }
+            continue;
         }
         // a work item is 8 keys per thread: their loads are issued together
         for (unsigned long long i0 = w.begin + tid; i0 < w.end; i0 += 256 * SPC_PER_THREAD) {
@@ -1901,8 +1913,10 @@ __global__ void __launch_bounds__(256) k_subpart_count(const unsigned long long 
 }
 
 // Regions of the sub-buckets estimated from a 1-in-stride sample of the
-// keys: n = stride * sampled count, region = n + 20 sqrt(n) + 64 (the sampled
-// count's standard deviation is about sqrt(n * stride) / stride * stride).
+// keys (sectors of 4 keys): n = stride * sampled count, region = n +
+// 20 sqrt(n) + 64; the estimate's standard deviation is about
+// sqrt(stride * n), under 2.9 sqrt(n) for stride 8, so the margin is about
+// 7 of them.
 __global__ void k_subpart_regions(const uint32_t *sampled, uint32_t n_sub, uint32_t stride, uint32_t *region)
 {
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_sub; s += gridDim.x * blockDim.x) {
@@ -2118,38 +2132,22 @@ __device__ __forceinline__ int sub_table_find(const unsigned long long *tk, unsi
 constexpr uint32_t SUB_THREADS = 512;   // blocks of the shared-memory count
 constexpr uint32_t SUB_BLOCKS_PER_SM = 2;
 constexpr uint32_t SUB_PER_THREAD = 4;
-constexpr uint32_t SUB_WARPS = SUB_THREADS / 32;
-constexpr uint32_t SUB_CHUNK = 32 * SUB_PER_THREAD;   // keys a warp takes at a time
+constexpr uint32_t SUB_TILE = SUB_THREADS * SUB_PER_THREAD;
 constexpr uint32_t SUB_HIST_BINS = 2048;   // counts below this go to a shared histogram
 
-// One sub-bucket at a time per block (persistent, two blocks per SM):
-//   1. the reference's two-level Bloom classification (src/BloomFilter.h:233-273)
-//      on the filter slice in shared memory, each warp on its own chunks of
-//      the sub-bucket's keys (no block-wide step inside the loop): a FIRST
-//      occurrence is marked in the sub-bucket's bit mask (one word per 32
-//      keys, first_bits), the others are counted in the shared-memory table
-//      through a per-warp queue (every lane inserts);
-//   2. the FIRST occurrences, read again where their bit is set: +1 on a
-//      table hit, otherwise a k-mer seen once (counted, no record: min count
-//      >= 2);
-//   3. the table's records and histogram.
-// Classification order inside a sub-bucket depends on the warps' timing, as
-// the reference's does on its threads'; at most one occurrence of a k-mer is
-// FIRST (the seen-once word is set by a returning atomicOr), so the merged
-// counts are exact in every order.
+
 __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
-    const unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count,
-    const uint8_t *sub_bucket, uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub, uint32_t count_max,
-    uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys, uint32_t *rec_counts, uint64_t rec_cap,
-    unsigned long long *hist, uint32_t *ovf, uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf,
-    uint32_t *first_bits)
+    unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count, const uint8_t *sub_bucket,
+    uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub, uint32_t count_max, uint32_t min_count,
+    uint32_t max_count, unsigned long long *rec_keys, uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist,
+    uint32_t *ovf, uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf)
 {
     extern __shared__ __align__(16) uint8_t cs_smem[];
     unsigned long long *s_filter = reinterpret_cast<unsigned long long *>(cs_smem);   // 2 * SUB_SLICE_BLOCKS
     unsigned long long *s_tk = s_filter + 2 * SUB_SLICE_BLOCKS;                       // SUB_TABLE_SLOTS
     uint32_t *s_tc = reinterpret_cast<uint32_t *>(s_tk + SUB_TABLE_SLOTS);            // SUB_TABLE_SLOTS
     uint32_t *s_hist = s_tc + SUB_TABLE_SLOTS;                                        // SUB_HIST_BINS
-    unsigned long long *s_queue = reinterpret_cast<unsigned long long *>(s_hist + SUB_HIST_BINS);   // SUB_THREADS * 4
+    unsigned long long *s_queue = reinterpret_cast<unsigned long long *>(s_hist + SUB_HIST_BINS);   // SUB_TILE
     __shared__ uint32_t s_warp[32], s_sub;
     __shared__ unsigned long long s_base;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -2158,7 +2156,6 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
     unsigned long long n_high = 0, n_low = 0, n_low_only = 0, n_distinct = 0;
     uint32_t n_ovf_subs = 0;
     bool rec_full = false;
-    unsigned long long *q = s_queue + warp * SUB_CHUNK;
     for (;;) {
         if (tid == 0) s_sub = atomicAdd(next_sub, 1u);
         __syncthreads();
@@ -2171,36 +2168,37 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
         const uint32_t bucket = sub_bucket[sub];
         const unsigned long long fcap = sc[bucket].fcap;
         const uint32_t slice = 1u << sc[bucket].slice_shift;
-        uint32_t *fb = first_bits + (base >> 5) + sub;   // bit j of word w: key 32 w + j is FIRST
-        const uint32_t n_chunks = (n + SUB_CHUNK - 1) / SUB_CHUNK;
         for (uint32_t i = tid; i < 2 * slice; i += SUB_THREADS) s_filter[i] = 0;
         for (uint32_t i = tid; i < SUB_TABLE_SLOTS; i += SUB_THREADS) {
             s_tk[i] = EMPTY_KEY;
             s_tc[i] = 0;
         }
         __syncthreads();
-        // 1. classification; the warp's next chunk is loaded while this one is classified
+        // 1. the reference's two-level Bloom classification (src/BloomFilter.h:233-273)
+        // on the slice; non-FIRST occurrences counted in the table, FIRST ones
+        // written back over the front of the sub-bucket's keys
         bool full = false;
+        uint32_t lo_cnt = 0;   // the same in every thread
+        // the next tile's k-mers are loaded while this one is classified (a
+        // tile's FIRST write-back only reaches positions already loaded)
         unsigned long long kn[SUB_PER_THREAD];
-        uint32_t c = warp;
 #pragma unroll
         for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
-            const uint32_t i = c * SUB_CHUNK + r * 32 + lane;
-            kn[r] = (c < n_chunks && i < n) ? __ldcs(&keys[base + i]) : EMPTY_KEY;
+            const uint32_t i = r * SUB_THREADS + tid;
+            kn[r] = i < n ? __ldcs(&keys[base + i]) : EMPTY_KEY;
         }
-        for (; c < n_chunks; c += SUB_WARPS) {
+        for (uint32_t t0 = 0; t0 < n; t0 += SUB_TILE) {
             unsigned long long k[SUB_PER_THREAD];
-            const uint32_t cn = c + SUB_WARPS;
-#pragma unroll
-            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
-                k[r] = kn[r];
-                const uint32_t i = cn * SUB_CHUNK + r * 32 + lane;
-                kn[r] = (cn < n_chunks && i < n) ? __ldcs(&keys[base + i]) : EMPTY_KEY;
-            }
             uint32_t firsts = 0, highs = 0;
 #pragma unroll
             for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
-                if (c * SUB_CHUNK + r * 32 + lane >= n) continue;
+                k[r] = kn[r];
+                const uint32_t i = t0 + SUB_TILE + r * SUB_THREADS + tid;
+                kn[r] = i < n ? __ldcs(&keys[base + i]) : EMPTY_KEY;
+            }
+#pragma unroll
+            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
+                if (t0 + r * SUB_THREADS + tid >= n) continue;
                 uint64_t block, m, hi;
                 bloom_probe_hi(k[r], fcap, block, m, hi);
                 unsigned long long *cell = s_filter + 2 * (block & (slice - 1));
@@ -2219,25 +2217,32 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
                 else highs |= 1u << r;
             }
             n_high += (uint64_t)__popc(highs);
-            n_low += (uint64_t)__popc(firsts);
-#pragma unroll
-            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
-                const uint32_t b = __ballot_sync(FULL, (firsts >> r) & 1u);
-                if (lane == 0 && c * SUB_CHUNK + r * 32 < n) fb[c * SUB_PER_THREAD + r] = b;
-            }
             // the warp's non-FIRST k-mers are queued so that every lane inserts
-            uint32_t qn = 0;
+            {
+                unsigned long long *q = s_queue + warp * (32 * SUB_PER_THREAD);
+                uint32_t qn = 0;
 #pragma unroll
-            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
-                const bool h = (highs >> r) & 1u;
-                const uint32_t b = __ballot_sync(FULL, h);
-                if (h) q[qn + (uint32_t)__popc(b & lt)] = k[r];
-                qn += (uint32_t)__popc(b);
+                for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
+                    const bool h = (highs >> r) & 1u;
+                    const uint32_t b = __ballot_sync(FULL, h);
+                    if (h) q[qn + (uint32_t)__popc(b & lt)] = k[r];
+                    qn += (uint32_t)__popc(b);
+                }
+                __syncwarp();
+                for (uint32_t j = lane; j < qn; j += 32)
+                    if (!sub_table_add(s_tk, s_tc, q[j])) full = true;
+                __syncwarp();
             }
-            __syncwarp();
-            for (uint32_t j = lane; j < qn; j += 32)
-                if (!sub_table_add(s_tk, s_tc, q[j])) full = true;
-            __syncwarp();
+            uint32_t tf;
+            const uint32_t of = block_excl_scan_1024((uint32_t)__popc(firsts), s_warp, tf);
+            // every key of this tile is in registers (the scan synchronised the
+            // block), so the FIRST ones may overwrite its front
+            unsigned long long p = base + lo_cnt + of;
+#pragma unroll
+            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r)
+                if ((firsts >> r) & 1u) keys[p++] = k[r];
+            lo_cnt += tf;
+            n_low += (uint64_t)__popc(firsts);
         }
         if (__syncthreads_or(full)) {
             if (tid == 0) {
@@ -2247,20 +2252,17 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
             continue;   // incomplete: the host counts the pass again with more sub-buckets
         }
         // 2. FIRST occurrences: a hit adds one to the table count, a miss is a
-        // k-mer seen once (the mask words are this block's own writes, read
-        // after the barrier through L2)
-        for (uint32_t cc = warp; cc < n_chunks; cc += SUB_WARPS) {
-            uint32_t wb[SUB_PER_THREAD];
+        // k-mer seen once (counted, not a record: min_count >= 2)
+        for (uint32_t i0 = tid; i0 < lo_cnt; i0 += SUB_THREADS * SUB_PER_THREAD) {
             unsigned long long kk[SUB_PER_THREAD];
 #pragma unroll
-            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r)
-                wb[r] = cc * SUB_CHUNK + r * 32 < n ? __ldcg(&fb[cc * SUB_PER_THREAD + r]) : 0u;
-#pragma unroll
-            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r)
-                kk[r] = ((wb[r] >> lane) & 1u) ? __ldcs(&keys[base + cc * SUB_CHUNK + r * 32 + lane]) : EMPTY_KEY;
+            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
+                const uint32_t i = i0 + r * SUB_THREADS;
+                kk[r] = i < lo_cnt ? __ldcg(&keys[base + i]) : EMPTY_KEY;
+            }
 #pragma unroll
             for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
-                if (!((wb[r] >> lane) & 1u)) continue;
+                if (i0 + r * SUB_THREADS >= lo_cnt) continue;
                 const int sl = sub_table_find(s_tk, kk[r]);
                 if (sl >= 0) atomicAdd(&s_tc[sl], 1u);
                 else ++n_low_only;
@@ -2272,32 +2274,32 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
         for (uint32_t i = tid; i < SUB_TABLE_SLOTS; i += SUB_THREADS) {
             if (s_tk[i] == EMPTY_KEY) continue;
             ++n_distinct;
-            const uint32_t cnt = s_tc[i] < count_max ? s_tc[i] : count_max;
-            if (cnt < SUB_HIST_BINS) atomicAdd(&s_hist[cnt], 1u);
-            else if (cnt < HIST_BINS) atomicAdd(&hist[cnt], 1ull);
+            const uint32_t c = s_tc[i] < count_max ? s_tc[i] : count_max;
+            if (c < SUB_HIST_BINS) atomicAdd(&s_hist[c], 1u);
+            else if (c < HIST_BINS) atomicAdd(&hist[c], 1ull);
             else {
-                const unsigned long long qi = atomicAdd(&counters[C_OVF_LEN], 1ull);
-                if (qi < ovf_cap) ovf[qi] = cnt;
+                const unsigned long long q = atomicAdd(&counters[C_OVF_LEN], 1ull);
+                if (q < ovf_cap) ovf[q] = c;
                 else atomicOr(&counters[C_FLAGS], ERR_HIST_OVERFLOW_FULL);
             }
-            keep += (cnt >= min_count && cnt <= max_count) ? 1u : 0u;
+            keep += (c >= min_count && c <= max_count) ? 1u : 0u;
         }
         uint32_t tk;
         const uint32_t ok = block_excl_scan_1024(keep, s_warp, tk);
         if (tid == 0) s_base = tk ? atomicAdd(&counters[C_REC_LEN], (unsigned long long)tk) : 0ull;
         __syncthreads();
-        unsigned long long qpos = s_base + ok;
+        unsigned long long q = s_base + ok;
         for (uint32_t i = tid; i < SUB_TABLE_SLOTS; i += SUB_THREADS) {
             if (s_tk[i] == EMPTY_KEY) continue;
-            const uint32_t cnt = s_tc[i] < count_max ? s_tc[i] : count_max;
-            if (cnt < min_count || cnt > max_count) continue;
-            if (qpos < rec_cap) {
-                rec_keys[qpos] = pair_reverse(s_tk[i]);
-                rec_counts[qpos] = cnt;
+            const uint32_t c = s_tc[i] < count_max ? s_tc[i] : count_max;
+            if (c < min_count || c > max_count) continue;
+            if (q < rec_cap) {
+                rec_keys[q] = pair_reverse(s_tk[i]);
+                rec_counts[q] = c;
             } else {
                 rec_full = true;
             }
-            ++qpos;
+            ++q;
         }
         __syncthreads();
     }
@@ -3034,26 +3036,25 @@ cudaError_t launch_subpart_scatter(const unsigned long long *keys, const BucketR
     return cudaGetLastError();
 }
 
-cudaError_t launch_count_subs(const unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count,
+cudaError_t launch_count_subs(unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count,
                               const uint8_t *sub_bucket, uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub,
                               uint32_t count_max, uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
                               uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist, uint32_t *ovf,
-                              uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, uint32_t *first_bits,
-                              cudaStream_t st)
+                              uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, cudaStream_t st)
 {
     if (!n_sub) return cudaSuccess;
     if (min_count < 2) return cudaErrorInvalidValue;   // singletons are not records on this path
     cudaError_t e = cudaMemsetAsync(next_sub, 0, 4, st);
     if (e != cudaSuccess) return e;
     const size_t smem = (size_t)2 * SUB_SLICE_BLOCKS * 8 + (size_t)SUB_TABLE_SLOTS * (8 + 4) + SUB_HIST_BINS * 4 +
-                        (size_t)SUB_THREADS * SUB_PER_THREAD * 8;
+                        (size_t)SUB_TILE * 8;
     e = cudaFuncSetAttribute(k_count_subs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const uint32_t grid = std::min<uint32_t>(n_sub, (uint32_t)sm_count() * SUB_BLOCKS_PER_SM);
     note_launch();
     k_count_subs<<<grid, SUB_THREADS, smem, st>>>(keys, sub_off, sub_count, sub_bucket, n_sub, sc, next_sub, count_max,
                                                   min_count, max_count, rec_keys, rec_counts, rec_cap, hist, ovf,
-                                                  ovf_cap, counters, bucket_ovf, first_bits);
+                                                  ovf_cap, counters, bucket_ovf);
     return cudaGetLastError();
 }
 

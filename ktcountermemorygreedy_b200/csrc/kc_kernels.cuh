@@ -292,13 +292,14 @@ cudaError_t launch_select_range(const unsigned long long *keys, const uint32_t *
 // cut into items of SUB_SCATTER_ITEM_KEYS keys (fill_item_starts_n).  count_subs: one
 // block per sub-bucket at a time runs the Bloom split with the filter slice in
 // shared memory, counts the non-FIRST occurrences in a shared-memory table,
-// merges the FIRST ones (marked in a bit mask per sub-bucket) and appends the table's records (counts saturated at count_max, kept
+// merges the FIRST ones (written back over the front of the sub-bucket's
+// keys) and appends the table's records (counts saturated at count_max, kept
 // when min_count <= count <= max_count) at rec_keys[C_REC_LEN...]; every
 // table count goes to hist/ovf, the totals to counters (C_REC_LEN,
 // C_LOW_LEN, C_HIGH_LEN, C_LOW_ONLY, C_DISTINCT) and the sub-buckets whose
 // table overflowed to C_SUB_OVF and bucket_ovf[their bucket] (the results
 // are then incomplete).
-// stride > 1: only every stride-th work item is counted (a sample).
+// stride > 1: only every stride-th run of 4 keys is counted (a sample).
 cudaError_t launch_subpart_count(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                  const SubCfg *sc, uint32_t *sub_count, cudaStream_t st, uint32_t stride = 1);
 // sub_end non-NULL: the sub-buckets' regions are estimates and a key is
@@ -318,15 +319,11 @@ cudaError_t launch_subpart_regions(const uint32_t *sampled, uint32_t n_sub, uint
 cudaError_t launch_subpart_sizes(const unsigned long long *sub_off, const unsigned long long *sub_cursor,
                                  const unsigned long long *sub_end, uint32_t n_sub, uint64_t out_cap, uint32_t *count,
                                  unsigned long long *overflow, cudaStream_t st);
-cudaError_t launch_count_subs(const unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count,
+cudaError_t launch_count_subs(unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count,
                               const uint8_t *sub_bucket, uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub,
                               uint32_t count_max, uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
                               uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist, uint32_t *ovf,
-                              uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, uint32_t *first_bits,
-                              cudaStream_t st);
-// words of the FIRST bit masks of count_subs for sub-buckets inside a key
-// array of key_cap keys (sub-bucket s at word (sub_off[s] >> 5) + s)
-inline uint64_t count_subs_mask_words(uint64_t key_cap, uint32_t n_sub) { return key_cap / 32 + n_sub + 2; }
+                              uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, cudaStream_t st);
 cudaError_t launch_bloom_buckets(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                  unsigned int *next_item, const BucketCfg *cfg, unsigned long long *bits,
                                  unsigned long long *out, unsigned long long *low_cnt, unsigned long long *high_cnt,

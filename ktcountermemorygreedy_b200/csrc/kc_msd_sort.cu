@@ -11,8 +11,9 @@
 //      across tiles by decoupled look-back, output offsets from the scanned
 //      bucket histogram, records reordered in shared memory so that runs of one
 //      digit are written to consecutive addresses);
-//   3. every bucket sorted in shared memory by the bits below the prefix
-//      (LSD, 8 bits a pass, warp-match ranks), written back in place.
+//   3. every bucket sorted in shared memory: placed by the next 8 bits (warp
+//      match ranks), then each of the 256 resulting runs of a few records
+//      sorted by insertion; written back in place.
 // Buckets larger than one block's shared memory (rare: the keys come from
 // genome sequence, spread over the prefixes) are sorted afterwards one by one
 // by the count/scan/scatter LSD sort on the bits below the prefix.
@@ -215,27 +216,38 @@ __global__ void __launch_bounds__(MS_THREADS, 2) k_msd_scatter(const unsigned lo
     }
 }
 
-// Every bucket of at most MS_TILE records sorted in shared memory on the bits
-// below its prefix (low_bits), LSD with 8-bit digits; in place when kin ==
-// kout.  Larger buckets are copied unsorted (kin != kout) for the fallback.
-// reverse_out: the keys are written with their 2-bit groups reversed (the
-// printed-string order key back to the k-mer word).
-__global__ void __launch_bounds__(MS_THREADS, 3) k_bucket_sort(const unsigned long long *kin, const uint32_t *vin,
+// Every bucket of at most BS_CAP records is sorted in shared memory.  Its
+// records are placed by the 8 bits just below the bucket prefix (per-warp
+// match ranks in record order: one pass over the records to count, one to
+// place, both reading them from global memory, the second from L2), which cuts
+// the bucket into 256 runs of a few records each; thread t then sorts run t by
+// insertion on the key's low `bits` bits (all records of a run share every bit
+// above the 8 placed ones, so this orders the whole bucket).  Written back in
+// place when kin == kout, with the 2-bit groups reversed when reverse_out.
+// Larger buckets are copied unsorted (kin != kout) for the fallback.
+constexpr uint32_t BS_CAP = 8192;
+
+__global__ void __launch_bounds__(MS_THREADS, 2) k_bucket_sort(const unsigned long long *kin, const uint32_t *vin,
                                                                unsigned long long *kout, uint32_t *vout,
                                                                const uint32_t *hb, const unsigned long long *ob,
-                                                               uint32_t n_buckets, uint32_t low_bits, int reverse_out)
+                                                               uint32_t n_buckets, uint32_t low_bits, uint32_t bits,
+                                                               int reverse_out)
 {
     extern __shared__ __align__(16) uint8_t bs_smem[];
-    unsigned long long *s_keys = reinterpret_cast<unsigned long long *>(bs_smem);   // MS_TILE
-    uint32_t *s_vals = reinterpret_cast<uint32_t *>(s_keys + MS_TILE);              // MS_TILE
-    uint32_t *s_wcnt = s_vals + MS_TILE;                                            // 8 x 256
-    __shared__ uint32_t s_start[256], s_warp[8];
+    unsigned long long *s_keys = reinterpret_cast<unsigned long long *>(bs_smem);   // BS_CAP
+    uint32_t *s_vals = reinterpret_cast<uint32_t *>(s_keys + BS_CAP);               // BS_CAP
+    uint32_t *s_wcnt = s_vals + BS_CAP;                                             // 8 x 256
+    __shared__ uint32_t s_start[257], s_warp[8];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t passes = (low_bits + 7) / 8;
+    const uint32_t dsh = low_bits > 8 ? low_bits - 8 : 0;
+    const uint32_t dmask = low_bits >= 8 ? 255u : ((1u << low_bits) - 1u);
+    const unsigned long long kmask = bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);
+    const uint32_t lt = lanes_below();
+    uint32_t *wc = s_wcnt + warp * 256;
     for (uint32_t b = blockIdx.x; b < n_buckets; b += gridDim.x) {
         const uint32_t m = hb[b];
         const unsigned long long base = ob[b];
-        if (m > MS_TILE) {   // sorted by the fallback, which also reverses the keys
+        if (m > BS_CAP) {   // sorted by the fallback, which also reverses the keys
             if (kin != kout)
                 for (uint32_t i = tid; i < m; i += MS_THREADS) {
                     kout[base + i] = kin[base + i];
@@ -243,57 +255,84 @@ __global__ void __launch_bounds__(MS_THREADS, 3) k_bucket_sort(const unsigned lo
                 }
             continue;
         }
-        if (m <= 1 || passes == 0) {
+        if (m <= 1 || low_bits == 0) {
             for (uint32_t i = tid; i < m; i += MS_THREADS) {
                 kout[base + i] = reverse_out ? pair_reverse(kin[base + i]) : kin[base + i];
                 vout[base + i] = vin[base + i];
             }
             continue;
         }
-        // items blocked per warp: warp w holds [w * per, (w + 1) * per)
+        // records blocked per warp: warp w holds [w * per, (w + 1) * per)
         const uint32_t per = ((m + 8 * 32 - 1) / (8 * 32)) * 32;
-        const uint32_t steps = per / 32, first = warp * per;
-        unsigned long long k[MS_ITEMS];
-        uint32_t v[MS_ITEMS], rd[MS_ITEMS];
-#pragma unroll
-        for (uint32_t r = 0; r < MS_ITEMS; ++r) {
-            const uint32_t li = first + r * 32 + lane;
-            const bool act = r < steps && li < m;
-            k[r] = act ? kin[base + li] : 0ull;
-            v[r] = act ? vin[base + li] : 0u;
+        const uint32_t first = warp * per;
+        for (int i = tid; i < 8 * 256; i += MS_THREADS) s_wcnt[i] = 0;
+        __syncthreads();
+        // 1. count the records of every digit, per warp
+        for (uint32_t li = first + lane; li < first + per; li += 32) {
+            const bool act = li < m;
+            const uint32_t d = act ? (uint32_t)((kin[base + li] >> dsh) & dmask) : 256u;
+            const uint32_t peers = __match_any_sync(FULLW, d);
+            const uint32_t before = __popc(peers & lt);
+            const uint32_t cnt = act ? wc[d] : 0u;
+            __syncwarp();
+            if (act && before == 0) wc[d] = cnt + __popc(peers);
+            __syncwarp();
         }
-        for (uint32_t p = 0; p < passes; ++p) {
-            uint32_t own;
-            rank_items(k, rd, first, m, 8 * p, 255u, steps, s_wcnt, s_start, s_warp, own);
+        __syncthreads();
+        uint32_t own = 0;
 #pragma unroll
-            for (uint32_t r = 0; r < MS_ITEMS; ++r) {
-                if (r >= steps) break;
-                const uint32_t d = rd[r] & 0xFFFFu;
-                if (d < 256) {
-                    const uint32_t pos = s_start[d] + s_wcnt[warp * 256 + d] + (rd[r] >> 16);
-                    s_keys[pos] = k[r];
-                    s_vals[pos] = v[r];
+        for (int w = 0; w < 8; ++w) {
+            const uint32_t c = s_wcnt[w * 256 + tid];
+            s_wcnt[w * 256 + tid] = own;
+            own += c;
+        }
+        uint32_t tot;
+        s_start[tid] = scan256(own, s_warp, tot);
+        if (tid == 0) s_start[256] = m;
+        __syncthreads();
+        // 2. place every record after the records of smaller digits and of
+        // earlier warps, in record order within the warp
+        for (uint32_t li = first + lane; li < first + per; li += 32) {
+            const bool act = li < m;
+            const unsigned long long key = act ? kin[base + li] : 0ull;
+            const uint32_t val = act ? vin[base + li] : 0u;
+            const uint32_t d = act ? (uint32_t)((key >> dsh) & dmask) : 256u;
+            const uint32_t peers = __match_any_sync(FULLW, d);
+            const uint32_t before = __popc(peers & lt);
+            const uint32_t cnt = act ? wc[d] : 0u;
+            __syncwarp();
+            if (act && before == 0) wc[d] = cnt + __popc(peers);
+            __syncwarp();
+            if (act) {
+                const uint32_t pos = s_start[d] + cnt + before;
+                s_keys[pos] = key;
+                s_vals[pos] = val;
+            }
+        }
+        __syncthreads();
+        // 3. run tid sorted by insertion
+        {
+            const uint32_t lo = s_start[tid], hi = s_start[tid + 1];
+            for (uint32_t i = lo + 1; i < hi; ++i) {
+                const unsigned long long key = s_keys[i];
+                const unsigned long long km = key & kmask;
+                const uint32_t val = s_vals[i];
+                uint32_t j = i;
+                while (j > lo && (s_keys[j - 1] & kmask) > km) {
+                    s_keys[j] = s_keys[j - 1];
+                    s_vals[j] = s_vals[j - 1];
+                    --j;
                 }
-            }
-            __syncthreads();
-#pragma unroll
-            for (uint32_t r = 0; r < MS_ITEMS; ++r) {
-                const uint32_t li = first + r * 32 + lane;
-                if (r < steps && li < m) {
-                    k[r] = s_keys[li];
-                    v[r] = s_vals[li];
-                }
-            }
-            __syncthreads();
-        }
-#pragma unroll
-        for (uint32_t r = 0; r < MS_ITEMS; ++r) {
-            const uint32_t li = first + r * 32 + lane;
-            if (r < steps && li < m) {
-                kout[base + li] = reverse_out ? pair_reverse(k[r]) : k[r];
-                vout[base + li] = v[r];
+                s_keys[j] = key;
+                s_vals[j] = val;
             }
         }
+        __syncthreads();
+        for (uint32_t i = tid; i < m; i += MS_THREADS) {
+            kout[base + i] = reverse_out ? pair_reverse(s_keys[i]) : s_keys[i];
+            vout[base + i] = s_vals[i];
+        }
+        __syncthreads();
     }
 }
 
@@ -320,7 +359,13 @@ uint64_t msd_max_tiles(uint64_t n) { return (n + MS_TILE - 1) / MS_TILE + 256; }
 
 }  // namespace
 
-bool msd_sort_applies(uint64_t n, uint32_t bits) { return n >= MSD_SORT_MIN_RECORDS && bits >= 24 && bits <= 64; }
+// Up to 2^16 buckets of about 3K records on average (BS_CAP leaves room for
+// the skew of canonical k-mers' prefixes, whose first base is A or C more
+// often); larger record sets take the LSD sort.
+bool msd_sort_applies(uint64_t n, uint32_t bits)
+{
+    return n >= MSD_SORT_MIN_RECORDS && n <= (3072ull << 16) && bits >= 24 && bits <= 64;
+}
 
 // Working memory: the alternate key/value arrays at its start (the layout
 // sort_tmp_alt describes), inside a region large enough for the fallback
@@ -387,13 +432,13 @@ cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n
     tiles.reserve(2 * nt_max);
     const uint64_t nt1 = (n + MS_TILE - 1) / MS_TILE;
     for (uint64_t t = 0; t < nt1; ++t) tiles.push_back(MsdTile{t * MS_TILE, std::min<uint64_t>(n, (t + 1) * MS_TILE), 0, 0});
-    std::vector<uint64_t> big_start, big_len;   // buckets of more than MS_TILE records
+    std::vector<uint64_t> big_start, big_len;   // buckets of more than BS_CAP records
     uint64_t at = 0;
     for (uint32_t s = 0; s < 256; ++s) {
         uint64_t len = 0;
         for (uint64_t d = 0; d < (1ull << P2); ++d) {
             const uint64_t b = ((uint64_t)s << P2) | d, m = h[b];
-            if (m > MS_TILE) {
+            if (m > BS_CAP) {
                 big_start.push_back(at + len);
                 big_len.push_back(m);
             }
@@ -409,9 +454,10 @@ cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n
     e = cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(MsdTile), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(look, 0, (nt1 + nt2) * 256 * 8, st);
     if (e != cudaSuccess) return e;
-    const size_t smem = MS_TILE * 12 + 8 * 256 * 4;
+    const size_t smem = MS_TILE * 12 + 8 * 256 * 4, bs_smem = BS_CAP * 12 + 8 * 256 * 4;
     e = cudaFuncSetAttribute(k_msd_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_bucket_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_bucket_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bs_smem);
     if (e != cudaSuccess) return e;
     // pass 1: top 8 bits, A -> B; pass 2: the next P2 bits inside each top-8 range, B -> A
     note_kernel_launch();
@@ -426,8 +472,8 @@ cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n
     unsigned long long *ks = P2 ? ka : kb;   // where the bucketed records are
     uint32_t *vs = P2 ? va : vb;
     note_kernel_launch();
-    k_bucket_sort<<<(unsigned)std::min<uint64_t>(nb, (uint64_t)n_sms() * 3), MS_THREADS, smem, st>>>(
-        ks, vs, keys, vals, hb, ob, (uint32_t)nb, shift2, reverse_out ? 1 : 0);
+    k_bucket_sort<<<(unsigned)std::min<uint64_t>(nb, (uint64_t)n_sms() * 2), MS_THREADS, bs_smem, st>>>(
+        ks, vs, keys, vals, hb, ob, (uint32_t)nb, shift2, bits, reverse_out ? 1 : 0);
     // buckets too large for one block: each sorted on its own on the bits
     // below the prefix, with the alternate arrays as working memory
     for (size_t i = 0; i < big_start.size() && e == cudaSuccess; ++i) {
