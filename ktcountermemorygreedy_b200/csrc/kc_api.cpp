@@ -549,7 +549,10 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     const uint32_t max_probe_cap = 1u << 16;
     const double est = hll_estimate(hll_h.data(), HLL_M);
     unsigned long long *hist = ds.n<unsigned long long>(HIST_BINS);
-    const uint64_t ovf_cap = 1 << 20;
+    // counts of HIST_BINS or more go to a list: a k-mer that often needs
+    // HIST_BINS occurrences, so O / HIST_BINS bounds the list (heavily
+    // repeated genomes reach millions of such k-mers)
+    const uint64_t ovf_cap = std::max<uint64_t>(1ull << 20, O / HIST_BINS + 1);
     uint32_t *ovf = ds.n<uint32_t>(ovf_cap);
     unsigned long long *n_keys = ds.n<unsigned long long>(1);
     CK(cudaMemsetAsync(hist, 0, HIST_BINS * 8, st));
@@ -1515,7 +1518,11 @@ void run_batch(std::vector<std::shared_ptr<Job>> &jobs, cudaStream_t st, Workspa
     unsigned long long *rec_keys = ds.n<unsigned long long>(std::max<uint64_t>(total_rec, 1));
     uint32_t *rec_counts = ds.n<uint32_t>(std::max<uint64_t>(total_rec, 1));
     unsigned long long *hist = ds.n<unsigned long long>((size_t)n * HIST_BINS_BATCH);
-    const uint64_t ovf_cap = 1 << 20;
+    uint64_t occ_total = 0;
+    for (uint32_t i = 0; i < n; ++i) occ_total += occ_h[i];
+    // counts of HIST_BINS_BATCH or more go to a list, bounded by the
+    // occurrences over HIST_BINS_BATCH
+    const uint64_t ovf_cap = std::max<uint64_t>(1ull << 20, occ_total / HIST_BINS_BATCH + 1);
     unsigned long long *ovf = ds.n<unsigned long long>(ovf_cap);
     CK(cudaMemsetAsync(hist, 0, (size_t)n * HIST_BINS_BATCH * 8, st));
     clk.begin(5);

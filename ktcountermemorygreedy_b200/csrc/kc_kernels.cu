@@ -689,16 +689,21 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
                         const uint32_t i = tid + r * EXT_THREADS;
                         if (i < nr && s_rank[i] != 0xFFFFu) s_stage[s_rank[i]] = kr[r];
                     }
-                    // destination of sorted index i of bucket b: s_bpos[b] + i
-                    s_bpos[tid] = c ? a.bucket_base[tid] + cur - bstart : 0ull;
+                    // destination of sorted index i of bucket b: s_bpos[b] + i,
+                    // written while i < s_hist[b] (inside the bucket's region
+                    // and the list: a bucket that outgrows its estimated
+                    // region is reported by its cursor and redone)
+                    {
+                        const unsigned long long bp = c ? a.bucket_base[tid] + cur - bstart : 0ull;
+                        s_bpos[tid] = bp;
+                        const unsigned long long lim = a.bucket_end[tid] < a.list_cap ? a.bucket_end[tid] : a.list_cap;
+                        s_hist[tid] = lim > bp ? (uint32_t)(lim - bp < 0xFFFFFFFFull ? lim - bp : 0xFFFFFFFFull) : 0u;
+                    }
                     __syncthreads();
                     for (uint32_t i = tid; i < tot_b; i += EXT_THREADS) {
                         const unsigned long long key = s_stage[i];
                         const uint32_t b = (uint32_t)(key >> 56);
-                        const unsigned long long pos = s_bpos[b] + i;
-                        // a bucket that outgrows its estimated region is
-                        // reported (its cursor passes the end) and redone
-                        if (pos < a.bucket_end[b] && pos < a.list_cap) a.list[pos] = key;
+                        if (i < s_hist[b]) a.list[s_bpos[b] + i] = key;
                     }
                 } else if (MODE == MODE_EMIT) {
                     if (tid == 0) s_bcast[0] = atomicAdd(&a.counters[C_EMIT_LEN], (unsigned long long)nr);
