@@ -2153,7 +2153,7 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
     uint32_t *s_tc = reinterpret_cast<uint32_t *>(s_tk + SUB_TABLE_SLOTS);            // SUB_TABLE_SLOTS
     uint32_t *s_hist = s_tc + SUB_TABLE_SLOTS;                                        // SUB_HIST_BINS
     unsigned long long *s_queue = reinterpret_cast<unsigned long long *>(s_hist + SUB_HIST_BINS);   // SUB_TILE
-    __shared__ uint32_t s_warp[32], s_sub;
+    __shared__ uint32_t s_warp[32], s_sub, s_lo;   // s_lo: FIRST keys written back
     __shared__ unsigned long long s_base;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t lt = lanemask_lt();
@@ -2173,6 +2173,7 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
         const uint32_t bucket = sub_bucket[sub];
         const unsigned long long fcap = sc[bucket].fcap;
         const uint32_t slice = 1u << sc[bucket].slice_shift;
+        if (tid == 0) s_lo = 0;
         for (uint32_t i = tid; i < 2 * slice; i += SUB_THREADS) s_filter[i] = 0;
         for (uint32_t i = tid; i < SUB_TABLE_SLOTS; i += SUB_THREADS) {
             s_tk[i] = EMPTY_KEY;
@@ -2183,7 +2184,6 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
         // on the slice; non-FIRST occurrences counted in the table, FIRST ones
         // written back over the front of the sub-bucket's keys
         bool full = false;
-        uint32_t lo_cnt = 0;   // the same in every thread
         // the next tile's k-mers are loaded while this one is classified (a
         // tile's FIRST write-back only reaches positions already loaded)
         unsigned long long kn[SUB_PER_THREAD];
@@ -2192,6 +2192,7 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
             const uint32_t i = r * SUB_THREADS + tid;
             kn[r] = i < n ? __ldcs(&keys[base + i]) : EMPTY_KEY;
         }
+        __syncthreads();   // the first tile is loaded by every warp before any write-back
         for (uint32_t t0 = 0; t0 < n; t0 += SUB_TILE) {
             unsigned long long k[SUB_PER_THREAD];
             uint32_t firsts = 0, highs = 0;
@@ -2238,16 +2239,30 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
                     if (!sub_table_add(s_tk, s_tc, q[j])) full = true;
                 __syncwarp();
             }
-            uint32_t tf;
-            const uint32_t of = block_excl_scan_1024((uint32_t)__popc(firsts), s_warp, tf);
-            // every key of this tile is in registers (the scan synchronised the
-            // block), so the FIRST ones may overwrite its front
-            unsigned long long p = base + lo_cnt + of;
+            // FIRST write-back: each warp takes its positions with one
+            // shared-memory atomic.  They lie below the keys classified so
+            // far, i.e. in this tile or earlier ones, whose keys every warp
+            // holds in registers (the barrier at the end of the previous tile
+            // came after every warp's loads of this one)
+            {
+                uint32_t wb[SUB_PER_THREAD], wtot = 0;
 #pragma unroll
-            for (uint32_t r = 0; r < SUB_PER_THREAD; ++r)
-                if ((firsts >> r) & 1u) keys[p++] = k[r];
-            lo_cnt += tf;
+                for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
+                    wb[r] = __ballot_sync(FULL, (firsts >> r) & 1u);
+                    wtot += (uint32_t)__popc(wb[r]);
+                }
+                uint32_t wbase = 0;
+                if (lane == 0 && wtot) wbase = atomicAdd(&s_lo, wtot);
+                wbase = __shfl_sync(FULL, wbase, 0);
+                uint32_t before = 0;
+#pragma unroll
+                for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
+                    if ((firsts >> r) & 1u) keys[base + wbase + before + (uint32_t)__popc(wb[r] & lt)] = k[r];
+                    before += (uint32_t)__popc(wb[r]);
+                }
+            }
             n_low += (uint64_t)__popc(firsts);
+            __syncthreads();
         }
         if (__syncthreads_or(full)) {
             if (tid == 0) {
@@ -2258,6 +2273,7 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
         }
         // 2. FIRST occurrences: a hit adds one to the table count, a miss is a
         // k-mer seen once (counted, not a record: min_count >= 2)
+        const uint32_t lo_cnt = s_lo;
         for (uint32_t i0 = tid; i0 < lo_cnt; i0 += SUB_THREADS * SUB_PER_THREAD) {
             unsigned long long kk[SUB_PER_THREAD];
 #pragma unroll
