@@ -573,6 +573,9 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     // into_sort_tmp: the records are written into the sort's alternate
     // buffers, from which an odd number of passes ends in rec_keys/rec_counts.
     bool rec_by_bucket = true, rec_in_sort_tmp = false;
+    // the records per value of their keys' top 16 bits, when the count made
+    // it as it wrote them (a one-pass Bloom job): the sort's bucket histogram
+    uint32_t *rec_hist16 = nullptr;
     void *sort_tmp = nullptr;
     auto compact_table = [&](const TableRef &t, uint64_t cap, uint64_t n_low, const unsigned long long *lst,
                              const BucketRanges *low_rg, uint32_t n_low_items, unsigned int *merge_next,
@@ -952,9 +955,14 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                                                 counters + C_REGION_OVF, st));
                     clk.end();
                     clk.begin(10);
+                    uint32_t *hb16 = nullptr;
+                    if (!multi && 2 * k >= 24) {
+                        hb16 = ds.n<uint32_t>(1u << 16);
+                        CK(cudaMemsetAsync(hb16, 0, (1u << 16) * 4, st));
+                    }
                     CK(launch_count_subs(list, sub_off, sub_count, d_sb, n_sub, d_sc, sub_next, count_max,
                                          P.min_count, P.max_count, rk, rc, rcap, hist_sub, ovf, ovf_cap, counters,
-                                         bucket_ovf, st));
+                                         bucket_ovf, st, hb16, 2 * k - 16));
                     clk.end();
                     if (attempt == 0 && (P.fault_inject & KC_INJECT_TABLE_FULL_ONCE)) {
                         // as if the first bucket's sub-bucket tables had overflowed
@@ -979,6 +987,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                         rec_counts = rc;
                         n_rec = cs.v[C_REC_LEN];
                         rec_by_bucket = false;
+                        rec_hist16 = hb16;
                         job.distinct += cs.v[C_DISTINCT] + cs.v[C_LOW_ONLY];
                         job.low_only += cs.v[C_LOW_ONLY];
                         low_len += cs.v[C_LOW_LEN];
@@ -1169,7 +1178,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
         if (msd_sort_applies(n_rec, 2 * k) && tn.record_sort != 2) {
             // the sort writes the k-mer words back (pair_reverse) as it stores
             CK(launch_msd_sort(rec_keys, rec_counts, n_rec, 2 * k, stmp, st, counters + C_FLAGS, rec_in_sort_tmp,
-                               true));
+                               true, rec_hist16));
             reversed = true;
         } else {
             CK(launch_radix_sort(rec_keys, rec_counts, n_rec, 2 * k, stmp, st, counters + C_FLAGS, skip,

@@ -2145,7 +2145,8 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
     unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count, const uint8_t *sub_bucket,
     uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub, uint32_t count_max, uint32_t min_count,
     uint32_t max_count, unsigned long long *rec_keys, uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist,
-    uint32_t *ovf, uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf)
+    uint32_t *ovf, uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, uint32_t *hb16,
+    uint32_t hb16_shift)
 {
     extern __shared__ __align__(16) uint8_t cs_smem[];
     unsigned long long *s_filter = reinterpret_cast<unsigned long long *>(cs_smem);   // 2 * SUB_SLICE_BLOCKS
@@ -2315,8 +2316,10 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
             const uint32_t c = s_tc[i] < count_max ? s_tc[i] : count_max;
             if (c < min_count || c > max_count) continue;
             if (q < rec_cap) {
-                rec_keys[q] = pair_reverse(s_tk[i]);
+                const unsigned long long sk = pair_reverse(s_tk[i]);
+                rec_keys[q] = sk;
                 rec_counts[q] = c;
+                if (hb16) atomicAdd(&hb16[(uint32_t)(sk >> hb16_shift) & 0xFFFFu], 1u);   // the record sort's buckets
             } else {
                 rec_full = true;
             }
@@ -3061,7 +3064,8 @@ cudaError_t launch_count_subs(unsigned long long *keys, const unsigned long long
                               const uint8_t *sub_bucket, uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub,
                               uint32_t count_max, uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
                               uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist, uint32_t *ovf,
-                              uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, cudaStream_t st)
+                              uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, cudaStream_t st,
+                              uint32_t *hb16, uint32_t hb16_shift)
 {
     if (!n_sub) return cudaSuccess;
     if (min_count < 2) return cudaErrorInvalidValue;   // singletons are not records on this path
@@ -3075,7 +3079,7 @@ cudaError_t launch_count_subs(unsigned long long *keys, const unsigned long long
     note_launch();
     k_count_subs<<<grid, SUB_THREADS, smem, st>>>(keys, sub_off, sub_count, sub_bucket, n_sub, sc, next_sub, count_max,
                                                   min_count, max_count, rec_keys, rec_counts, rec_cap, hist, ovf,
-                                                  ovf_cap, counters, bucket_ovf);
+                                                  ovf_cap, counters, bucket_ovf, hb16, hb16_shift);
     return cudaGetLastError();
 }
 

@@ -272,7 +272,11 @@ constexpr uint64_t MSD_SORT_MIN_RECORDS = 1ull << 20;
 bool msd_sort_applies(uint64_t n, uint32_t bits);
 size_t msd_sort_tmp_bytes(uint64_t n, uint32_t bits);
 cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
-                            cudaStream_t st, unsigned long long *flags, bool input_in_tmp, bool reverse_out = false);
+                            cudaStream_t st, unsigned long long *flags, bool input_in_tmp, bool reverse_out = false,
+                            const uint32_t *hist16 = nullptr);
+// hist16: when not NULL, the records per value of the keys' top 16 bits
+// (key >> (bits - 16), 65536 counts) made while the records were written;
+// the sort then reads no key for its bucket histogram.
 // Counts one kernel launch of this library (kernels launched outside kc_kernels.cu).
 void note_kernel_launch();
 
@@ -293,7 +297,8 @@ cudaError_t launch_select_range(const unsigned long long *keys, const uint32_t *
 // block per sub-bucket at a time runs the Bloom split with the filter slice in
 // shared memory, counts the non-FIRST occurrences in a shared-memory table,
 // merges the FIRST ones (written back over the front of the sub-bucket's
-// keys) and appends the table's records (counts saturated at count_max, kept
+// keys) and appends (and, with hb16, counts every record's printed-order key
+// >> hb16_shift, the record sort's buckets, into hb16[65536]) the table's records (counts saturated at count_max, kept
 // when min_count <= count <= max_count) at rec_keys[C_REC_LEN...]; every
 // table count goes to hist/ovf, the totals to counters (C_REC_LEN,
 // C_LOW_LEN, C_HIGH_LEN, C_LOW_ONLY, C_DISTINCT) and the sub-buckets whose
@@ -323,7 +328,8 @@ cudaError_t launch_count_subs(unsigned long long *keys, const unsigned long long
                               const uint8_t *sub_bucket, uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub,
                               uint32_t count_max, uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
                               uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist, uint32_t *ovf,
-                              uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, cudaStream_t st);
+                              uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, cudaStream_t st,
+                              uint32_t *hb16 = nullptr, uint32_t hb16_shift = 0);
 cudaError_t launch_bloom_buckets(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                  unsigned int *next_item, const BucketCfg *cfg, unsigned long long *bits,
                                  unsigned long long *out, unsigned long long *low_cnt, unsigned long long *high_cnt,

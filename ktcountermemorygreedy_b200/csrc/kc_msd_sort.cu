@@ -86,6 +86,18 @@ __global__ void __launch_bounds__(256) k_msd_hist(const unsigned long long *keys
         atomicAdd(&hb[(uint32_t)(__ldcs(&keys[i]) >> shift) & bmask], 1u);
 }
 
+// hb[b] = the 2^(16 - P) counts of hist16 under bucket b (the top P of the
+// key's top 16 bits).
+__global__ void k_msd_hist_fold(const uint32_t *hist16, uint32_t p_bits, uint32_t *hb)
+{
+    const uint32_t nb = 1u << p_bits, per = 1u << (16 - p_bits);
+    for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        uint32_t c = 0;
+        for (uint32_t j = 0; j < per; ++j) c += hist16[b * per + j];
+        hb[b] = c;
+    }
+}
+
 // Stable ranks of the items of one block among the items with the same digit,
 // in item order: items are blocked per warp (warp w holds items
 // w * per_warp + r * 32 + lane, r < steps), so per-warp digit counters taken
@@ -225,7 +237,8 @@ __global__ void __launch_bounds__(MS_THREADS, 2) k_msd_scatter(const unsigned lo
 // above the 8 placed ones, so this orders the whole bucket).  Written back in
 // place when kin == kout, with the 2-bit groups reversed when reverse_out.
 // Larger buckets are copied unsorted (kin != kout) for the fallback.
-constexpr uint32_t BS_CAP = 8192;
+constexpr uint32_t BS_ITEMS = 32;                     // records per thread
+constexpr uint32_t BS_CAP = MS_THREADS * BS_ITEMS;    // 8192
 
 __global__ void __launch_bounds__(MS_THREADS, 2) k_bucket_sort(const unsigned long long *kin, const uint32_t *vin,
                                                                unsigned long long *kout, uint32_t *vout,
@@ -262,15 +275,27 @@ __global__ void __launch_bounds__(MS_THREADS, 2) k_bucket_sort(const unsigned lo
             }
             continue;
         }
-        // records blocked per warp: warp w holds [w * per, (w + 1) * per)
+        // records blocked per warp: warp w holds [w * per, (w + 1) * per),
+        // loaded into registers together (one memory latency per bucket)
         const uint32_t per = ((m + 8 * 32 - 1) / (8 * 32)) * 32;
-        const uint32_t first = warp * per;
+        const uint32_t steps = per / 32, first = warp * per;
+        unsigned long long k[BS_ITEMS];
+        uint32_t v[BS_ITEMS];
+#pragma unroll
+        for (uint32_t r = 0; r < BS_ITEMS; ++r) {
+            const uint32_t li = first + r * 32 + lane;
+            const bool act = r < steps && li < m;
+            k[r] = act ? kin[base + li] : 0ull;
+            v[r] = act ? vin[base + li] : 0u;
+        }
         for (int i = tid; i < 8 * 256; i += MS_THREADS) s_wcnt[i] = 0;
         __syncthreads();
         // 1. count the records of every digit, per warp
-        for (uint32_t li = first + lane; li < first + per; li += 32) {
-            const bool act = li < m;
-            const uint32_t d = act ? (uint32_t)((kin[base + li] >> dsh) & dmask) : 256u;
+#pragma unroll
+        for (uint32_t r = 0; r < BS_ITEMS; ++r) {
+            if (r >= steps) break;
+            const bool act = first + r * 32 + lane < m;
+            const uint32_t d = act ? (uint32_t)((k[r] >> dsh) & dmask) : 256u;
             const uint32_t peers = __match_any_sync(FULLW, d);
             const uint32_t before = __popc(peers & lt);
             const uint32_t cnt = act ? wc[d] : 0u;
@@ -292,11 +317,11 @@ __global__ void __launch_bounds__(MS_THREADS, 2) k_bucket_sort(const unsigned lo
         __syncthreads();
         // 2. place every record after the records of smaller digits and of
         // earlier warps, in record order within the warp
-        for (uint32_t li = first + lane; li < first + per; li += 32) {
-            const bool act = li < m;
-            const unsigned long long key = act ? kin[base + li] : 0ull;
-            const uint32_t val = act ? vin[base + li] : 0u;
-            const uint32_t d = act ? (uint32_t)((key >> dsh) & dmask) : 256u;
+#pragma unroll
+        for (uint32_t r = 0; r < BS_ITEMS; ++r) {
+            if (r >= steps) break;
+            const bool act = first + r * 32 + lane < m;
+            const uint32_t d = act ? (uint32_t)((k[r] >> dsh) & dmask) : 256u;
             const uint32_t peers = __match_any_sync(FULLW, d);
             const uint32_t before = __popc(peers & lt);
             const uint32_t cnt = act ? wc[d] : 0u;
@@ -305,8 +330,8 @@ __global__ void __launch_bounds__(MS_THREADS, 2) k_bucket_sort(const unsigned lo
             __syncwarp();
             if (act) {
                 const uint32_t pos = s_start[d] + cnt + before;
-                s_keys[pos] = key;
-                s_vals[pos] = val;
+                s_keys[pos] = k[r];
+                s_vals[pos] = v[r];
             }
         }
         __syncthreads();
@@ -382,7 +407,8 @@ size_t msd_sort_tmp_bytes(uint64_t n, uint32_t bits)
 }
 
 cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
-                            cudaStream_t st, unsigned long long *flags, bool input_in_tmp, bool reverse_out)
+                            cudaStream_t st, unsigned long long *flags, bool input_in_tmp, bool reverse_out,
+                            const uint32_t *hist16)
 {
     if (!msd_sort_applies(n, bits)) return cudaErrorInvalidValue;
     const uint32_t P = msd_prefix_bits(n, bits), P2 = P - 8;
@@ -419,7 +445,10 @@ cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n
     if (e == cudaSuccess) e = cudaMemsetAsync(tile_ctr, 0, 16, st);
     if (e != cudaSuccess) return e;
     note_kernel_launch();
-    k_msd_hist<<<n_sms() * 8, 256, 0, st>>>(ka, n, shift2, (uint32_t)(nb - 1), hb);
+    if (hist16 && P <= 16)
+        k_msd_hist_fold<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(hist16, P, hb);
+    else
+        k_msd_hist<<<n_sms() * 8, 256, 0, st>>>(ka, n, shift2, (uint32_t)(nb - 1), hb);
     e = launch_scan_u32(hb, ob, nb, stmp, st);
     if (e != cudaSuccess) return e;
     // the bucket sizes come to the host once: the second pass's tiles follow
