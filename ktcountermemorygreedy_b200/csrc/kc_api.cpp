@@ -221,6 +221,7 @@ struct kc_handle {
     kc_tuning tuning = default_tuning();   // settings for jobs that start from now on (guarded by mu)
     uint64_t budget = 0;
     uint64_t workspace_bytes = 0;   // per worker, allocated when the worker starts
+    uint32_t workers_n = 1;
     uint64_t reserved = 0;
     uint32_t running = 0;
     bool closing = false;
@@ -1615,6 +1616,10 @@ void worker_main(kc_handle *h)
     cudaStream_t st;
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     auto ws = std::make_unique<Workspace>(st);
+    // several workers: each keeps at most its share of the budget between
+    // jobs, so that one large job does not leave its memory idle in one
+    // worker while the others need it
+    if (h->workers_n > 1 && !h->workspace_bytes) ws->set_max_keep(h->budget / h->workers_n);
     if (h->workspace_bytes) ws->reserve(h->workspace_bytes);
     for (;;) {
         std::shared_ptr<Task> task;
@@ -1735,6 +1740,7 @@ int kc_open(const kc_config *cfg, kc_handle **out)
         }
     }
     uint32_t nw = (cfg && cfg->max_inflight_jobs) ? cfg->max_inflight_jobs : 4;
+    h->workers_n = nw;
     for (uint32_t i = 0; i < nw; ++i) h->workers.emplace_back(worker_main, h);
     *out = h;
     return KC_OK;

@@ -57,6 +57,7 @@ void *pool_alloc(size_t bytes, cudaStream_t st)
 void Workspace::begin_job()
 {
     top_ = 0;
+    if (max_keep_ && high_ > max_keep_) high_ = max_keep_;
     if (high_ > cap_) {
         // grow once to the high-water mark (plus headroom for jobs that vary)
         CK(cudaStreamSynchronize(st_));
@@ -69,6 +70,7 @@ void Workspace::begin_job()
         if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess)
             cudaMemPoolTrimTo(pool, 0);
         size_t want = (high_ + high_ / 8 + (64u << 20)) & ~size_t((2u << 20) - 1);
+        if (max_keep_ && want > max_keep_) want = max_keep_ & ~size_t((2u << 20) - 1);
         if (cudaMalloc(&base_, want) != cudaSuccess) {
             cudaGetLastError();
             base_ = nullptr;   // keep going from the pool

@@ -58,6 +58,10 @@ public:
     // failure injection: the next get() fails as a failed device allocation
     // does (KcError KC_ERR_NOMEM)
     void fail_next_get() { fail_next_ = true; }
+    // the block kept between jobs is at most this large (0: no limit); a job
+    // that needs more takes the rest from the stream-ordered pool, which the
+    // other workers of a handle share
+    void set_max_keep(size_t bytes) { max_keep_ = bytes; }
 
 private:
     cudaStream_t st_;
@@ -65,6 +69,7 @@ private:
     size_t cap_ = 0, top_ = 0, high_ = 0;
     size_t spilled_ = 0;   // bytes of this job's blocks taken from the pool
     bool fail_next_ = false;
+    size_t max_keep_ = 0;
     std::vector<void *> spill_;
 };
 
