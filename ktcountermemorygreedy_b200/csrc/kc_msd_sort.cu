@@ -228,28 +228,30 @@ __global__ void __launch_bounds__(MS_THREADS, 2) k_msd_scatter(const unsigned lo
     }
 }
 
-// Every bucket of at most BS_CAP records is sorted in shared memory.  Its
-// records are placed by the 8 bits just below the bucket prefix (per-warp
-// match ranks in record order: one pass over the records to count, one to
-// place, both reading them from global memory, the second from L2), which cuts
-// the bucket into 256 runs of a few records each; thread t then sorts run t by
-// insertion on the key's low `bits` bits (all records of a run share every bit
-// above the 8 placed ones, so this orders the whole bucket).  Written back in
-// place when kin == kout, with the 2-bit groups reversed when reverse_out.
-// Larger buckets are copied unsorted (kin != kout) for the fallback.
-constexpr uint32_t BS_ITEMS = 32;                     // records per thread
-constexpr uint32_t BS_CAP = MS_THREADS * BS_ITEMS;    // 8192
+// A bucket of at most ITEMS * 256 records is sorted in shared memory by one
+// block.  Its records are loaded into registers in one batch (one memory
+// latency per bucket) and placed by the 8 bits just below the bucket prefix
+// (per-warp match ranks in record order: a pass to count, a pass to place),
+// which cuts the bucket into 256 runs of a few records each; thread t then
+// sorts run t by insertion on the key's low `bits` bits (all records of a run
+// share every bit above the 8 placed ones, so this orders the whole bucket).
+// Written back in place when kin == kout, with the 2-bit groups reversed when
+// reverse_out.  The buckets come in size classes (blist: the buckets of this
+// class), each class with as many blocks per SM as its registers and shared
+// memory allow; buckets larger than BS_CAP go to the fallback.
+constexpr uint32_t BS_CAP = MS_THREADS * 32;   // 8192
 
-__global__ void __launch_bounds__(MS_THREADS, 2) k_bucket_sort(const unsigned long long *kin, const uint32_t *vin,
-                                                               unsigned long long *kout, uint32_t *vout,
-                                                               const uint32_t *hb, const unsigned long long *ob,
-                                                               uint32_t n_buckets, uint32_t low_bits, uint32_t bits,
-                                                               int reverse_out)
+template <uint32_t ITEMS>
+__global__ void __launch_bounds__(MS_THREADS, ITEMS <= 8 ? 5 : (ITEMS <= 16 ? 3 : 2))
+    k_bucket_sort(const unsigned long long *kin, const uint32_t *vin, unsigned long long *kout, uint32_t *vout,
+                  const uint32_t *hb, const unsigned long long *ob, const uint32_t *blist, uint32_t n_list,
+                  uint32_t low_bits, uint32_t bits, int reverse_out)
 {
+    constexpr uint32_t BS_ITEMS = ITEMS, CAP = MS_THREADS * ITEMS;
     extern __shared__ __align__(16) uint8_t bs_smem[];
-    unsigned long long *s_keys = reinterpret_cast<unsigned long long *>(bs_smem);   // BS_CAP
-    uint32_t *s_vals = reinterpret_cast<uint32_t *>(s_keys + BS_CAP);               // BS_CAP
-    uint32_t *s_wcnt = s_vals + BS_CAP;                                             // 8 x 256
+    unsigned long long *s_keys = reinterpret_cast<unsigned long long *>(bs_smem);   // CAP
+    uint32_t *s_vals = reinterpret_cast<uint32_t *>(s_keys + CAP);                  // CAP
+    uint32_t *s_wcnt = s_vals + CAP;                                                // 8 x 256
     __shared__ uint32_t s_start[257], s_warp[8];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t dsh = low_bits > 8 ? low_bits - 8 : 0;
@@ -257,17 +259,11 @@ __global__ void __launch_bounds__(MS_THREADS, 2) k_bucket_sort(const unsigned lo
     const unsigned long long kmask = bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);
     const uint32_t lt = lanes_below();
     uint32_t *wc = s_wcnt + warp * 256;
-    for (uint32_t b = blockIdx.x; b < n_buckets; b += gridDim.x) {
+    for (uint32_t bi = blockIdx.x; bi < n_list; bi += gridDim.x) {
+        const uint32_t b = blist[bi];
         const uint32_t m = hb[b];
         const unsigned long long base = ob[b];
-        if (m > BS_CAP) {   // sorted by the fallback, which also reverses the keys
-            if (kin != kout)
-                for (uint32_t i = tid; i < m; i += MS_THREADS) {
-                    kout[base + i] = kin[base + i];
-                    vout[base + i] = vin[base + i];
-                }
-            continue;
-        }
+        if (m > CAP) continue;   // not in this class (the host lists never do this)
         if (m <= 1 || low_bits == 0) {
             for (uint32_t i = tid; i < m; i += MS_THREADS) {
                 kout[base + i] = reverse_out ? pair_reverse(kin[base + i]) : kin[base + i];
@@ -382,6 +378,24 @@ uint32_t msd_prefix_bits(uint64_t n, uint32_t bits)
 
 uint64_t msd_max_tiles(uint64_t n) { return (n + MS_TILE - 1) / MS_TILE + 256; }
 
+template <uint32_t ITEMS>
+cudaError_t launch_bucket_class(const unsigned long long *kin, const uint32_t *vin, unsigned long long *kout,
+                                uint32_t *vout, const uint32_t *hb, const unsigned long long *ob, const uint32_t *blist,
+                                uint32_t n_list, uint32_t low_bits, uint32_t bits, bool reverse_out, cudaStream_t st)
+{
+    const size_t smem = (size_t)MS_THREADS * ITEMS * 12 + 8 * 256 * 4;
+    cudaError_t e = cudaFuncSetAttribute(k_bucket_sort<ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bucket_sort<ITEMS>, MS_THREADS, smem) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    note_kernel_launch();
+    k_bucket_sort<ITEMS><<<(unsigned)std::min<uint64_t>(n_list, (uint64_t)n_sms() * per_sm), MS_THREADS, smem, st>>>(
+        kin, vin, kout, vout, hb, ob, blist, n_list, low_bits, bits, reverse_out ? 1 : 0);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 // Up to 2^16 buckets of about 3K records on average (BS_CAP leaves room for
@@ -403,7 +417,7 @@ size_t msd_sort_tmp_bytes(uint64_t n, uint32_t bits)
     const uint64_t nt = msd_max_tiles(n);
     return align256(std::max<size_t>(sort_tmp_bytes_in_scratch(n), align256(n * 8) + align256(n * 4))) +
            align256(nb * 4) + align256(nb * 8) + align256(scan_tmp_words(nb) * 8) + align256(2 * nt * 256 * 8) +
-           align256(2 * nt * sizeof(MsdTile)) + align256(16);
+           align256(2 * nt * sizeof(MsdTile)) + align256(16) + align256(nb * 4);
 }
 
 cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n, uint32_t bits, void *tmp,
@@ -431,6 +445,7 @@ cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n
     p += align256(2 * nt_max * sizeof(MsdTile));
     unsigned int *tile_ctr = reinterpret_cast<unsigned int *>(p);
     unsigned long long *own_flags = reinterpret_cast<unsigned long long *>(p + 8);
+    uint32_t *d_blist = reinterpret_cast<uint32_t *>(p + align256(16));   // the buckets by size class
     if (!flags) flags = own_flags;
 
     // the records start in keys/vals (A), or in the alternate arrays (B)
@@ -462,6 +477,7 @@ cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n
     const uint64_t nt1 = (n + MS_TILE - 1) / MS_TILE;
     for (uint64_t t = 0; t < nt1; ++t) tiles.push_back(MsdTile{t * MS_TILE, std::min<uint64_t>(n, (t + 1) * MS_TILE), 0, 0});
     std::vector<uint64_t> big_start, big_len;   // buckets of more than BS_CAP records
+    std::vector<uint32_t> lists[3];               // buckets of at most 2048, 4096, 8192 records
     uint64_t at = 0;
     for (uint32_t s = 0; s < 256; ++s) {
         uint64_t len = 0;
@@ -470,6 +486,8 @@ cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n
             if (m > BS_CAP) {
                 big_start.push_back(at + len);
                 big_len.push_back(m);
+            } else {
+                lists[m <= 2048 ? 0 : (m <= 4096 ? 1 : 2)].push_back((uint32_t)b);
             }
             len += m;
         }
@@ -480,13 +498,16 @@ cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n
     }
     if (at != n) return cudaErrorInvalidValue;
     const uint64_t nt2 = tiles.size() - nt1;
+    std::vector<uint32_t> blist;
+    blist.reserve(nb);
+    for (auto &l : lists) blist.insert(blist.end(), l.begin(), l.end());
+    if (!blist.empty()) e = cudaMemcpyAsync(d_blist, blist.data(), blist.size() * 4, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
     e = cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(MsdTile), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(look, 0, (nt1 + nt2) * 256 * 8, st);
     if (e != cudaSuccess) return e;
-    const size_t smem = MS_TILE * 12 + 8 * 256 * 4, bs_smem = BS_CAP * 12 + 8 * 256 * 4;
+    const size_t smem = MS_TILE * 12 + 8 * 256 * 4;
     e = cudaFuncSetAttribute(k_msd_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_bucket_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bs_smem);
     if (e != cudaSuccess) return e;
     // pass 1: top 8 bits, A -> B; pass 2: the next P2 bits inside each top-8 range, B -> A
     note_kernel_launch();
@@ -500,9 +521,24 @@ cudaError_t launch_msd_sort(unsigned long long *keys, uint32_t *vals, uint64_t n
     }
     unsigned long long *ks = P2 ? ka : kb;   // where the bucketed records are
     uint32_t *vs = P2 ? va : vb;
-    note_kernel_launch();
-    k_bucket_sort<<<(unsigned)std::min<uint64_t>(nb, (uint64_t)n_sms() * 2), MS_THREADS, bs_smem, st>>>(
-        ks, vs, keys, vals, hb, ob, (uint32_t)nb, shift2, bits, reverse_out ? 1 : 0);
+    uint32_t off = 0;
+    for (int c = 0; c < 3 && e == cudaSuccess; ++c) {
+        const uint32_t nl = (uint32_t)lists[c].size();
+        if (nl) {
+            if (c == 0) e = launch_bucket_class<8>(ks, vs, keys, vals, hb, ob, d_blist + off, nl, shift2, bits, reverse_out, st);
+            if (c == 1) e = launch_bucket_class<16>(ks, vs, keys, vals, hb, ob, d_blist + off, nl, shift2, bits, reverse_out, st);
+            if (c == 2) e = launch_bucket_class<32>(ks, vs, keys, vals, hb, ob, d_blist + off, nl, shift2, bits, reverse_out, st);
+        }
+        off += nl;
+    }
+    // the buckets too large for a block start where the fallback sorts them
+    if (ks != keys)
+        for (size_t i = 0; i < big_start.size() && e == cudaSuccess; ++i) {
+            e = cudaMemcpyAsync(keys + big_start[i], ks + big_start[i], big_len[i] * 8, cudaMemcpyDeviceToDevice, st);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(vals + big_start[i], vs + big_start[i], big_len[i] * 4, cudaMemcpyDeviceToDevice, st);
+        }
+    if (e != cudaSuccess) return e;
     // buckets too large for one block: each sorted on its own on the bits
     // below the prefix, with the alternate arrays as working memory
     for (size_t i = 0; i < big_start.size() && e == cudaSuccess; ++i) {
