@@ -135,8 +135,9 @@ def algorithmic_bytes(phase: str, r):
         return S + 8 * O if r.low_len + r.high_len else S + 16 * O
     if phase == "bloom":               # bucketed k-mers read + list write (16 B) + two filter words (16 B)
         return 32 * O
-    if phase == "sub_partition":       # bucketed k-mers read + written in sub-bucket order
-        return 16 * O
+    if phase == "sub_partition":       # bucketed k-mers read + written in sub-bucket order, plus the
+        # count that sizes the sub-buckets: 1 in 8 keys sampled on a large pass, every key otherwise
+        return 16 * O + (O if O >= (64 << 20) else 8 * O)
     if phase == "smem_count":          # sub-bucket k-mers read, FIRST ones written back and read again, records
         return 8 * O + 16 * r.low_len + 12 * r.n_records_total
     if phase == "insert_high":         # list read (8 B) + slot key read and count update (16 B)
@@ -146,9 +147,19 @@ def algorithmic_bytes(phase: str, r):
     if phase == "compact":
         return 16 * r.table_capacity + 12 * r.n_records_total
     if phase == "sort":
-        return math.ceil(2 * 31 / 8) * 24 * r.n_records_total
-    if phase in ("census", "scan"):
+        # most significant bits first (1M-201M records): bucket histogram (key
+        # read, skipped when the count made it) + two scatter passes + the
+        # bucket sort, each reading and writing a 12 B record; LSD otherwise
+        R = r.n_records_total
+        if (1 << 20) <= R <= (3072 << 16):
+            return (8 * R if r.smem_passes == 0 else 0) + 3 * 24 * R
+        return math.ceil(2 * 31 / 8) * 24 * R
+    if phase == "census":
         return S
+    if phase == "scan":
+        # Bloom jobs read the 1-in-8 census tiles and the pre-pass sample
+        # (the first 256 MiB); plain jobs every tile
+        return S // 8 + min(S, 256 << 20) if r.low_len + r.high_len else S
     return 0
 
 
