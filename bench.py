@@ -726,19 +726,51 @@ def run_ours(args):
                           "alg_GBps": (algorithmic_bytes(phases[i], r0) / (mean_ms[i] / 1000.0) / 1e9)
                           if mean_ms[i] > 0 else None} for i in range(ns) if mean_ms[i] > 0}
 
-    # atomic throughput of the table insert against random-atomicAdd peaks
-    # measured here: a 4 GiB buffer (DRAM sector RMW) and a 32 MiB buffer
-    # (L2-resident, like one bucket's sub-table)
+    # atomic throughput of the table inserts against random-atomicAdd peaks
+    # measured here.  The job's own path (shared-memory sub-bucket tables):
+    # one count atomicAdd per non-FIRST occurrence and one per FIRST
+    # occurrence of a k-mer in the table, against random adds on a 16 KiB
+    # shared-memory table per block (the sub-bucket table's count array).
+    # The global-memory tables (kc_tuning.bloom_smem = 2), timed on one more
+    # untimed job: one count atomicAdd per non-FIRST occurrence, against a
+    # 4 GiB buffer (DRAM sector RMW) and a 32 MiB one (L2-resident, like one
+    # bucket's table).
     atomics = None
-    ih = phases.index("insert_high")
-    if mean_ms[ih] > 0:
-        pk_dram, _ = kc.atomic_peak(4 << 30)
-        pk_l2, _ = kc.atomic_peak(32 << 20)
-        rate = r0.high_len / (mean_ms[ih] / 1000.0)
-        atomics = {"kernel": "insert_high", "inserts_per_s": rate, "unit": "atomics/s",
-                   "peak_dram_random": pk_dram, "peak_l2_random": pk_l2,
-                   "frac_of_dram_peak": rate / pk_dram, "frac_of_l2_peak": rate / pk_l2,
-                   "note": "one slot-key read and one count atomicAdd per non-FIRST occurrence"}
+    sc = phases.index("smem_count")
+    if mean_ms[sc] > 0:
+        pk_smem, _ = kc.atomic_peak_shared(16384)
+        adds = r0.high_len + (r0.low_len - r0.low_only)
+        rate = adds / (mean_ms[sc] / 1000.0)
+        atomics = {"kernel": "smem_count", "table_adds_per_s": rate, "unit": "atomics/s",
+                   "table_adds_per_job": int(adds), "peak_smem_random": pk_smem, "frac_of_smem_peak": rate / pk_smem,
+                   "note": "count atomicAdds on the shared-memory sub-bucket tables (non-FIRST occurrences and "
+                           "FIRST occurrences found in the table); the kernel also reads and hashes every key "
+                           "and updates the filter slice, so the fraction is a floor on the insert's share"}
+        prev = counter.tuning["bloom_smem"]
+        counter.set_tuning(bloom_smem=2)
+        rg = counter.count(input=inp, keep_records=False, **JOB)
+        counter.set_tuning(bloom_smem=prev)
+        ih = phases.index("insert_high")
+        if rg.phase_ms[ih] > 0:
+            pk_dram, _ = kc.atomic_peak(4 << 30)
+            pk_l2, _ = kc.atomic_peak(32 << 20)
+            g = rg.high_len / (rg.phase_ms[ih] / 1000.0)
+            atomics["global_tables"] = {"kernel": "insert_high", "inserts_per_s": g, "inserts_per_job": int(rg.high_len),
+                                        "ms": rg.phase_ms[ih], "peak_dram_random": pk_dram, "peak_l2_random": pk_l2,
+                                        "frac_of_dram_peak": g / pk_dram, "frac_of_l2_peak": g / pk_l2,
+                                        "same_counts": bool(rg.occurrences == r0.occurrences and
+                                                            rg.distinct == r0.distinct and
+                                                            np.array_equal(rg.hist, r0.hist))}
+    else:
+        ih = phases.index("insert_high")
+        if mean_ms[ih] > 0:
+            pk_dram, _ = kc.atomic_peak(4 << 30)
+            pk_l2, _ = kc.atomic_peak(32 << 20)
+            rate = r0.high_len / (mean_ms[ih] / 1000.0)
+            atomics = {"kernel": "insert_high", "inserts_per_s": rate, "unit": "atomics/s",
+                       "peak_dram_random": pk_dram, "peak_l2_random": pk_l2,
+                       "frac_of_dram_peak": rate / pk_dram, "frac_of_l2_peak": rate / pk_l2,
+                       "note": "one slot-key read and one count atomicAdd per non-FIRST occurrence"}
 
     cpu = parity = sample_value = None
     if rank == 0 and world == 1 and args.cpu_baseline:

@@ -298,6 +298,12 @@ int kc_dump_text(const uint64_t *keys, const uint32_t *counts, uint64_t n, uint3
  * to stay L2-resident). */
 int kc_atomic_peak(uint64_t buffer_bytes, uint32_t repeats, double *atomics_per_s, double *ms_per_launch);
 
+/* Measurement aid, no counterpart in the reference: the same random atomicAdd
+ * on a table of table_bytes (a power of two, 4 KiB..64 KiB) in shared memory,
+ * one table per block of the shared-memory count's shape.  The peak that
+ * count's table inserts are compared with. */
+int kc_atomic_peak_shared(uint32_t table_bytes, uint32_t repeats, double *atomics_per_s, double *ms_per_launch);
+
 /* Pre-pass statistics and Bloom sizing of a job (src/main.cpp:262-335 with
  * get_MAX_BLOOM_FILTER_CAPACITY :41 and calculate_bloom_filter_capacity :111):
  * raw root-prefix counts over the sample, average quality, capacities. */

@@ -121,6 +121,7 @@ SIGNATURES = [
     ("kc_sort_distinct_records", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32]),
     ("kc_sort_records_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]),
     ("kc_atomic_peak", C.c_int, [C.c_uint64, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    ("kc_atomic_peak_shared", C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("kc_get_tuning", C.c_int, [C.c_void_p, C.POINTER(kc_tuning)]),
     ("kc_set_tuning", C.c_int, [C.c_void_p, C.POINTER(kc_tuning)]),
     ("kc_autotune", C.c_int, [C.c_void_p, C.POINTER(kc_job), C.c_uint32, C.c_uint32, C.POINTER(kc_tuning)]),
@@ -479,6 +480,14 @@ def atomic_peak(buffer_bytes: int, repeats: int = 5):
     buffer of buffer_bytes (power of two)."""
     rate, ms = C.c_double(), C.c_double()
     _check(lib().kc_atomic_peak(buffer_bytes, repeats, C.byref(rate), C.byref(ms)))
+    return rate.value, ms.value
+
+
+def atomic_peak_shared(table_bytes: int = 16384, repeats: int = 5):
+    """(atomics/s, ms per launch) of random 32-bit atomicAdd on a
+    shared-memory table of table_bytes per block."""
+    rate, ms = C.c_double(), C.c_double()
+    _check(lib().kc_atomic_peak_shared(table_bytes, repeats, C.byref(rate), C.byref(ms)))
     return rate.value, ms.value
 
 

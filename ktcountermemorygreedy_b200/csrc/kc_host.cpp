@@ -700,6 +700,38 @@ int kc_atomic_peak(uint64_t buffer_bytes, uint32_t repeats, double *atomics_per_
     }
 }
 
+int kc_atomic_peak_shared(uint32_t table_bytes, uint32_t repeats, double *atomics_per_s, double *ms_per_launch)
+{
+    if (!atomics_per_s || !ms_per_launch || !repeats) return set_error(KC_ERR_INVALID, "bad argument");
+    if (table_bytes < 4096 || table_bytes > (64u << 10) || (table_bytes & (table_bytes - 1)))
+        return set_error(KC_ERR_INVALID, "table_bytes must be a power of two in [4096, 65536]");
+    try {
+        StreamGuard sg;
+        DevScope ds(sg.st);
+        uint32_t *out = ds.n<uint32_t>(1);
+        CK(cudaMemsetAsync(out, 0, 4, sg.st));
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        uint64_t ops = 0;
+        const uint32_t iters = 4096, words = table_bytes / 4;
+        CK(launch_atomic_peak_shared(out, words, iters, 1, &ops, sg.st));   // warm-up
+        CK(cudaEventRecord(e0, sg.st));
+        for (uint32_t r = 0; r < repeats; ++r) CK(launch_atomic_peak_shared(out, words, iters, 2 + r, &ops, sg.st));
+        CK(cudaEventRecord(e1, sg.st));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *ms_per_launch = ms / repeats;
+        *atomics_per_s = (double)ops * repeats / (ms * 1e-3);
+        return KC_OK;
+    } catch (const KcError &e) {
+        return set_error(e.code, e.msg);
+    }
+}
+
 int kc_plan_bloom(const uint32_t *raw_prefix_counts, uint32_t avg_quality, uint64_t est_file_size,
                   uint64_t memory_gb, uint32_t k, uint64_t *capacities, uint64_t *max_capacity)
 {

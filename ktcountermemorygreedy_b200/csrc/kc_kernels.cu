@@ -3204,4 +3204,44 @@ cudaError_t launch_atomic_peak(uint32_t *buf, uint64_t words, uint32_t iters, ui
     return cudaGetLastError();
 }
 
+// The same random atomicAdd on a table of mask+1 words in shared memory, one
+// table per block, with the shared-memory count's block shape (512 threads,
+// two blocks per SM).  Each block adds its table into `out` at the end so
+// that the adds are not dead code.
+__global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_atomic_peak_shared(uint32_t *out, uint32_t mask,
+                                                                                        uint32_t iters, uint64_t seed)
+{
+    extern __shared__ uint32_t s_tab[];
+    for (uint32_t i = threadIdx.x; i <= mask; i += blockDim.x) s_tab[i] = 0;
+    __syncthreads();
+    uint64_t x = seed ^ ((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x + 1) * 0x9E3779B97F4A7C15ull);
+    x ^= x >> 31;
+    if (!x) x = 1;
+#pragma unroll 4
+    for (uint32_t i = 0; i < iters; ++i) {
+        x ^= x >> 12;
+        x ^= x << 25;
+        x ^= x >> 27;
+        atomicAdd(&s_tab[(uint32_t)((x * 0x2545F4914F6CDD1Dull) >> 32) & mask], 1u);
+    }
+    __syncthreads();
+    uint32_t sum = 0;
+    for (uint32_t i = threadIdx.x; i <= mask; i += blockDim.x) sum += s_tab[i];
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(FULL, sum, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, sum);
+}
+
+cudaError_t launch_atomic_peak_shared(uint32_t *out, uint32_t words, uint32_t iters, uint64_t seed, uint64_t *ops,
+                                      cudaStream_t st)
+{
+    const unsigned grid = (unsigned)sm_count() * SUB_BLOCKS_PER_SM * 4;
+    const size_t smem = (size_t)words * 4;
+    cudaError_t e = cudaFuncSetAttribute(k_atomic_peak_shared, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    *ops = (uint64_t)grid * SUB_THREADS * iters;
+    note_launch();
+    k_atomic_peak_shared<<<grid, SUB_THREADS, smem, st>>>(out, words - 1, iters, seed);
+    return cudaGetLastError();
+}
+
 }  // namespace kc

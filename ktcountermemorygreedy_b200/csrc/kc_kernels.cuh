@@ -365,5 +365,7 @@ cudaError_t launch_dump_text(const unsigned long long *keys, const uint32_t *cou
 // *ops receives the number of adds the launch performs.
 cudaError_t launch_atomic_peak(uint32_t *buf, uint64_t words, uint32_t iters, uint64_t seed, uint64_t *ops,
                                cudaStream_t st);
+cudaError_t launch_atomic_peak_shared(uint32_t *out, uint32_t words, uint32_t iters, uint64_t seed, uint64_t *ops,
+                                      cudaStream_t st);
 
 }  // namespace kc
