@@ -123,6 +123,113 @@ uint64_t kco_extract(const uint8_t *data, uint64_t len, uint32_t k,
 }
 
 /*
+ * k-mers of 33..128 bases (kmer<2> for k <= 64, kmer<4> for k <= 128).  The
+ * rolling state restates GetKmer<N> (GetKmer.h:58-84, batch form :86-130) on
+ * N words: seq shifts right by one base across the words (kmer.h:102-118,
+ * data[i] takes data[i-1]'s low bits) and takes the new base at data[0]'s top,
+ * then data[last] is masked to its top 2*(k%32) bits (all of it when k%32 ==
+ * 0); rev shifts left across the words (kmer.h:59-75) and takes the
+ * complement at data[last] bit 2*(32 - k%32) (0 when k%32 == 0).  The
+ * canonical k-mer is the lexicographically smaller word array
+ * (GetKmer.h:181-206, kmer.h:21 defaulted <=>).
+ *
+ * One deviation, on purpose: words above data[last] (data[3] when k <= 96 in
+ * kmer<4>) are zero here.  In GetKmer<4> at k = 96 (last = 2, k%32 = 0, so
+ * data[2] is not masked) the seq shift carries bases that left the window into
+ * data[3], which nothing clears, so the same 96-mer gets different keys in
+ * different reads and its count is split.  Exact counts are what the path
+ * defines, so the words outside the k-mer stay zero.
+ */
+static inline uint32_t wide_words(uint32_t k) { return k <= 32 ? 1u : (k <= 64 ? 2u : 4u); }
+
+uint32_t kco_key_words(uint32_t k) { return wide_words(k); }
+
+typedef struct {
+    uint32_t k, nw, last;
+    uint64_t back_mask;
+    uint32_t rev_shift;
+    uint64_t seq[4], rev[4], have;
+} wroll_t;
+
+static void wroll_clear(wroll_t *r)
+{
+    memset(r->seq, 0, sizeof(r->seq));
+    memset(r->rev, 0, sizeof(r->rev));
+    r->have = 0;
+}
+
+static void wroll_init(wroll_t *r, uint32_t k)
+{
+    r->k = k;
+    r->nw = wide_words(k);
+    r->last = (k - 1) / 32;
+    const uint32_t rem = k % 32;
+    r->back_mask = rem ? ((1ULL << (2 * rem)) - 1ULL) << (64 - 2 * rem) : ~0ULL;
+    r->rev_shift = rem ? 2 * (32 - rem) : 0;
+    wroll_clear(r);
+}
+
+static inline int wroll_push(wroll_t *r, uint8_t c, uint64_t *canon)
+{
+    const int code = base_code(c);
+    r->have++;
+    if (code < 0) { wroll_clear(r); return 0; }
+    for (int i = (int)r->nw - 1; i > 0; --i) r->seq[i] = (r->seq[i] >> 2) | (r->seq[i - 1] << 62);
+    r->seq[0] = (r->seq[0] >> 2) | ((uint64_t)code << 62);
+    r->seq[r->last] &= r->back_mask;
+    for (uint32_t i = r->last + 1; i < r->nw; ++i) r->seq[i] = 0;   /* the deviation above */
+    for (uint32_t i = 0; i + 1 < r->nw; ++i) r->rev[i] = (r->rev[i] << 2) | (r->rev[i + 1] >> 62);
+    r->rev[r->nw - 1] <<= 2;
+    r->rev[r->last] |= (uint64_t)(code ^ 3) << r->rev_shift;
+    if (r->have < r->k) return 0;
+    int less = 0;
+    for (uint32_t i = 0; i < r->nw; ++i)
+        if (r->seq[i] != r->rev[i]) { less = r->seq[i] < r->rev[i]; break; }
+    memcpy(canon, less ? r->seq : r->rev, r->nw * 8);
+    return 1;
+}
+
+uint64_t kco_extract_wide(const uint8_t *data, uint64_t len, uint32_t k, uint64_t *out, uint64_t cap)
+{
+    wroll_t r;
+    wroll_init(&r, k);
+    const uint32_t nw = r.nw;
+    uint64_t line = 0, n = 0, canon[4];
+    for (uint64_t i = 0; i < len; ++i) {
+        const uint8_t c = data[i];
+        if (c == '\n') { line++; wroll_clear(&r); continue; }
+        if ((line & 3) != 1) continue;
+        if (wroll_push(&r, c, canon)) {
+            if (n < cap) memcpy(out + n * nw, canon, nw * 8);
+            n++;
+        }
+    }
+    return n;
+}
+
+/* Printed-string order key of an N-word k-mer: the 2-bit groups of the whole
+ * word array reversed (the first base most significant), as N words, most
+ * significant first.  Base i of the printed string is extracted as
+ * kmer_to_buf does (dump_tool.cpp:103-124). */
+void kco_string_key_wide(const uint64_t *words, uint32_t k, uint64_t *out)
+{
+    const uint32_t nw = wide_words(k), full = k / 32, tail = k % 32;
+    memset(out, 0, nw * 8);
+    for (uint32_t i = 0; i < k; ++i) {
+        uint32_t w, sh;
+        if (tail > 0 && i < tail) { w = full; sh = 64 - 2 * tail + 2 * i; }
+        else {
+            const uint32_t off = i - (tail > 0 ? tail : 0);
+            w = full - 1 - off / 32;
+            sh = 2 * (off % 32);
+        }
+        const uint64_t b = (words[w] >> sh) & 3ULL;
+        const uint32_t pos = k - 1 - i;   /* 2-bit group from the least significant end */
+        out[nw - 1 - pos / 32] |= b << (2 * (pos % 32));
+    }
+}
+
+/*
  * Spot-check sample of the occurrences of one file: the same record splitting
  * and extraction as kco_extract, keeping only the canonical k-mers whose
  * sample hash has its low `sample_bits` bits zero.  The sample hash is the

@@ -32,6 +32,15 @@ extern "C" {
 uint64_t kco_extract(const uint8_t *data, uint64_t len, uint32_t k,
                      uint64_t *out, uint64_t cap);
 
+/* k-mers of 33..128 bases: kmer<N> word arrays (N = kco_key_words(k): 1 for
+ * k <= 32, 2 for k <= 64, 4 for k <= 128), N words per occurrence in `out`
+ * (cap occurrences).  Words above the k-mer's last word are zero (GetKmer<4>
+ * leaves stale bases in data[3] at k = 96; see kc_oracle.c). */
+uint32_t kco_key_words(uint32_t k);
+uint64_t kco_extract_wide(const uint8_t *data, uint64_t len, uint32_t k, uint64_t *out, uint64_t cap);
+/* Printed-string order key of one k-mer: N words, most significant first. */
+void kco_string_key_wide(const uint64_t *words, uint32_t k, uint64_t *out);
+
 /* Spot-check sample: kco_extract keeping only k-mers w with
  * (kco_sample_hash(w) & (2^sample_bits - 1)) == 0 -- every occurrence of a
  * kept k-mer, so their counts are exact.  The input must start at a record

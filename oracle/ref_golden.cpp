@@ -9,8 +9,9 @@
 //   ref_golden hashes <n> <seed>          per key: w xxh128.lo xxh128.hi xxh64
 //                                         rapidhash komihash mix_hash
 //                                         bloom_block(cap 2^20) bloom_mask
-//   ref_golden getkmer <k> <bases>        canonical k-mer after each base that
-//                                         completes one (GetKmer<1>::get_next_one)
+//   ref_golden getkmer <k> <bases>        canonical k-mer (all words of kmer<N>)
+//                                         after each base that completes one
+//                                         (GetKmer<N>::get_next_one, N by k)
 //   ref_golden prepass <k> <mem_gb> <f>.. root-prefix counts, avgQuality,
 //                                         estimated size, Bloom capacities
 #define main kc_reference_counter_main
@@ -54,14 +55,28 @@ static int run_hashes(uint64_t n, uint64_t seed)
     return 0;
 }
 
-static int run_getkmer(uint32_t k, const char *bases)
+// GetKmer<N> for the reference's dispatch (main.cpp:617-633): N = 1 for
+// k <= 32, 2 for k <= 64, 4 for k <= 128.  Prints every word of the canonical
+// kmer<N> after each base that completes one.
+template <uint32_t N>
+static int run_getkmer_n(uint32_t k, const char *bases)
 {
-    GetKmer<1> g(k);
+    GetKmer<N> g(k);
     for (const char *p = bases; *p; ++p) {
-        if (g.get_next_one(static_cast<unsigned char>(*p)))
-            std::printf("%zu %016" PRIx64 "\n", static_cast<size_t>(p - bases), g.canonical_kmer.data[0]);
+        if (g.get_next_one(static_cast<unsigned char>(*p))) {
+            std::printf("%zu", static_cast<size_t>(p - bases));
+            for (uint32_t w = 0; w < N; ++w) std::printf(" %016" PRIx64, g.canonical_kmer.data[w]);
+            std::printf("\n");
+        }
     }
     return 0;
+}
+
+static int run_getkmer(uint32_t k, const char *bases)
+{
+    if (k <= 32) return run_getkmer_n<1>(k, bases);
+    if (k <= 64) return run_getkmer_n<2>(k, bases);
+    return run_getkmer_n<4>(k, bases);
 }
 
 // Mirrors the pre-pass section of process_main<1> (main.cpp:262-335) by

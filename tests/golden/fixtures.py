@@ -88,6 +88,7 @@ def plain_small() -> bytes:
 
 
 # (name, files, k values) checked end to end against the reference programs
+# (k <= 32)
 E2E_CASES = [
     ("edge", [edge_fastq()], [5, 21, 25, 31]),
     ("crlf", [crlf_fastq()], [21, 31]),
@@ -98,9 +99,45 @@ E2E_CASES = [
                random_fastq(15, 200, (80, 120), genome_len=2000)], [21, 31]),
 ]
 
+# The same for k-mers of 33..128 bases.  The reference's histogram is an
+# oracle at every k except 96, its sorted dump only up to k = 64 (above 64
+# its sort key is 128 bits wide and the text is printed from that key,
+# tool/dump_tool.cpp:320-324, :1181-1185).
+E2E_WIDE_CASES = [
+    ("edge", [edge_fastq()], [33, 63]),
+    ("repeat", [repeat_fastq()], [33, 64, 65, 128]),
+    ("plain_small", [plain_small()], [33, 47, 63, 64, 65, 95, 96, 97, 127, 128]),
+    ("multi", [random_fastq(14, 200, (80, 120), genome_len=2000, final_newline=False),
+               random_fastq(15, 200, (80, 120), genome_len=2000)], [40, 70]),
+]
+
 
 def getkmer_cases():
     r = random.Random(5)
     s1 = "".join(r.choice("ACGTacgtUuNn") for _ in range(400))
     s2 = "".join(r.choice(BASES) for _ in range(300))
     return [(k, s) for k in (1, 2, 5, 15, 16, 17, 21, 25, 31, 32) for s in (s1, s2)]
+
+
+# k values of the reference's kmer<2> (33..64) and kmer<4> (65..128) paths
+WIDE_KS = (33, 34, 47, 63, 64, 65, 80, 95, 96, 97, 127, 128)
+
+
+def _revcomp(s: str) -> str:
+    return s.translate(str.maketrans("ACGT", "TGCA"))[::-1]
+
+
+def getkmer_wide_cases():
+    """Base strings for the multi-word extraction: long valid runs with rare
+    invalid bytes and mixed case, and reverse-complement palindromes of 32,
+    48 and 64 bases (k-mers equal to their reverse complement, and windows
+    whose forward and reverse words tie on their first words)."""
+    r = random.Random(6)
+    s3 = "".join(r.choice("ACGTacgtU") if r.random() > 0.004 else "N" for _ in range(900))
+    parts = []
+    for n in (16, 24, 32):
+        h = "".join(r.choice(BASES) for _ in range(n))
+        parts.append(h + _revcomp(h))
+    parts.append("A" * 32 + "T" * 32)
+    s4 = "".join(parts + ["".join(r.choice(BASES) for _ in range(40)) for _ in range(3)]) * 2
+    return [(k, s) for k in WIDE_KS for s in (s3, s4)]

@@ -80,6 +80,18 @@ def main():
         out = run([os.path.join(REF, "ref_golden"), "getkmer", str(k), s])
         gk.append({"k": k, "bases": s, "canonical": [l.split()[1] for l in out.split("\n") if l.strip()]})
     g["getkmer"] = gk
+    gw = []
+    for k, s in fixtures.getkmer_wide_cases():
+        out = run([os.path.join(REF, "ref_golden"), "getkmer", str(k), s])
+        rows = [l.split() for l in out.split("\n") if l.strip()]
+        last = (k - 1) // 32
+        # the words of the k-mer (data[0..last]); words above it are counted
+        # where nonzero (stale bases of GetKmer<4> at k = 96)
+        text = "".join(" ".join(r[1: 2 + last]) + "\n" for r in rows)
+        gw.append({"k": k, "bases": s, "n": len(rows), "sha256": hashlib.sha256(text.encode()).hexdigest(),
+                   "beyond_nonzero": sum(1 for r in rows if any(int(w, 16) for w in r[2 + last:])),
+                   "head": [r[1:] for r in rows[:8]]})
+    g["getkmer_wide"] = gw
     with tempfile.TemporaryDirectory() as tmp:
         # pre-pass statistics and Bloom sizing
         pre = []
@@ -115,6 +127,11 @@ def main():
         cases.append(e2e("repeat", [fixtures.repeat_fastq()], 21, 255, tmp))
         cases.append(e2e("repeat", [fixtures.repeat_fastq()], 31, 1000, tmp))
         g["e2e"] = cases
+        wide = []
+        for name, files, ks in fixtures.E2E_WIDE_CASES:
+            for k in ks:
+                wide.append(e2e(name, files, k, 4294967295, tmp))
+        g["e2e_wide"] = wide
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(g, f, indent=0, sort_keys=True)
     print("wrote", os.path.join(HERE, "golden.json"))

@@ -24,6 +24,9 @@ def lib():
         vp, u32, u64, u8 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint8
         sig = {
             "kco_extract": (u64, [vp, u64, u32, vp, u64]),
+            "kco_key_words": (u32, [u32]),
+            "kco_extract_wide": (u64, [vp, u64, u32, vp, u64]),
+            "kco_string_key_wide": (None, [vp, u32, vp]),
             "kco_sample_hash": (u64, [u64]),
             "kco_extract_sampled": (u64, [vp, u64, u32, u32, vp, u64]),
             "kco_prepass": (None, [vp, u64, u32, u64, vp, U64P, U64P]),
@@ -67,6 +70,69 @@ def extract(data: bytes, k: int) -> np.ndarray:
     out = np.zeros(cap, np.uint64)
     n = lib().kco_extract(P(buf), len(data), k, P(out), cap)
     return out[:n].copy()
+
+
+def key_words(k: int) -> int:
+    """Words of the reference's kmer<N> for k: 1 (k <= 32), 2 (<= 64), 4."""
+    return 1 if k <= 32 else (2 if k <= 64 else 4)
+
+
+def extract_wide(data: bytes, k: int) -> np.ndarray:
+    """Canonical k-mer occurrences as kmer<N> word arrays, shape (n, N)."""
+    nw = key_words(k)
+    buf = np.frombuffer(data, np.uint8) if data else np.zeros(1, np.uint8)
+    cap = max(len(data), 1)
+    out = np.zeros(cap * nw, np.uint64)
+    n = lib().kco_extract_wide(P(buf), len(data), k, P(out), cap)
+    return out[: n * nw].reshape(n, nw).copy()
+
+
+def string_keys_wide(words: np.ndarray, k: int) -> np.ndarray:
+    """Printed-string order keys of kmer<N> word arrays, shape (n, N), most
+    significant word first: the 2-bit groups of the whole array reversed."""
+    w = np.ascontiguousarray(words, np.uint64)
+    m1 = np.uint64(0x3333333333333333)
+    m2 = np.uint64(0x0F0F0F0F0F0F0F0F)
+    x = w.copy()
+    x = ((x >> np.uint64(2)) & m1) | ((x & m1) << np.uint64(2))
+    x = ((x >> np.uint64(4)) & m2) | ((x & m2) << np.uint64(4))
+    return np.ascontiguousarray(x.byteswap()[:, ::-1])
+
+
+def count_wide(keys: np.ndarray):
+    """Distinct rows and their counts."""
+    keys = np.ascontiguousarray(keys, np.uint64)
+    if len(keys) == 0:
+        return keys.reshape(0, keys.shape[1] if keys.ndim == 2 else 1), np.zeros(0, np.uint32)
+    uk, uc = np.unique(keys, axis=0, return_counts=True)
+    return uk, uc.astype(np.uint32)
+
+
+def sort_string_order_wide(keys, counts, k):
+    sk = string_keys_wide(keys, k)
+    order = np.lexsort(sk.T[::-1])   # the last key passed to lexsort is the primary one
+    return np.ascontiguousarray(keys[order]), np.ascontiguousarray(counts[order])
+
+
+def exact_records_wide(files, k, count_max=0xFFFFFFFF, min_count=1, max_count=0xFFFFFFFF):
+    """exact_records for any k: (keys (n, N), counts) in printed-string order."""
+    nw = key_words(k)
+    occ = np.concatenate([extract_wide(f, k) for f in files]) if files else np.zeros((0, nw), np.uint64)
+    uk, uc = count_wide(occ)
+    uc = np.minimum(uc, np.uint32(count_max)).astype(np.uint32)
+    m = (uc >= min_count) & (uc <= max_count)
+    return sort_string_order_wide(uk[m], uc[m], k)
+
+
+def kmer_string_wide(words, k: int) -> str:
+    w = np.ascontiguousarray(words, np.uint64)
+    buf = C.create_string_buffer(k + 1)
+    lib().kco_kmer_to_string(P(w), k, buf)
+    return buf.value.decode()
+
+
+def dump_text_wide(keys, counts, k) -> bytes:
+    return "".join(f"{kmer_string_wide(w, k)}\t{int(c)}\n" for w, c in zip(keys, counts)).encode()
 
 
 def sample_hash_np(keys: np.ndarray) -> np.ndarray:

@@ -94,6 +94,63 @@ def test_exact_counts_match_reference_tools(case):
     assert hashlib.sha256(text).hexdigest() == case["dump_sha256"]
 
 
+# ---- k-mers of 33..128 bases (kmer<2>, kmer<4>) ------------------------------
+
+@pytest.mark.parametrize("case", GOLDEN["getkmer_wide"], ids=lambda c: f"k{c['k']}-n{c['n']}")
+def test_wide_rolling_extraction_matches_getkmer(case):
+    k = case["k"]
+    got = O.extract_wide(_wrap(case["bases"]), k)
+    last = (k - 1) // 32
+    assert len(got) == case["n"]
+    text = "".join(" ".join(f"{int(v):016x}" for v in row[: last + 1]) + "\n" for row in got)
+    assert hashlib.sha256(text.encode()).hexdigest() == case["sha256"]
+    for row, want in zip(got, case["head"]):
+        assert [f"{int(v):016x}" for v in row[: last + 1]] == want[: last + 1]
+    # words above the k-mer's last word are zero here; GetKmer<4> leaves stale
+    # bases there at k = 96 only (its data[2] is not masked when k % 32 == 0)
+    assert not got[:, last + 1:].any()
+    assert (case["beyond_nonzero"] > 0) == (k == 96)
+
+
+def test_wide_string_keys_agree():
+    r = np.random.default_rng(3)
+    for k in (33, 47, 63, 64, 65, 96, 127, 128):
+        nw = O.key_words(k)
+        occ = O.extract_wide(fixtures.random_fastq(40 + k, 30, (150, 200), genome_len=5000), k)
+        sk = O.string_keys_wide(occ, k)
+        one = np.zeros(nw, np.uint64)
+        for i in r.choice(len(occ), 50):
+            O.lib().kco_string_key_wide(O.P(np.ascontiguousarray(occ[i])), k, O.P(one))
+            assert one.tolist() == sk[i].tolist()
+            # the key's bases read back give the printed string
+            s = "".join("ACGT"[(int(sk[i][nw - 1 - (k - 1 - j) // 32]) >> (2 * ((k - 1 - j) % 32))) & 3]
+                        for j in range(k))
+            assert s == O.kmer_string_wide(occ[i], k)
+
+
+@pytest.mark.parametrize("case", GOLDEN["e2e_wide"], ids=lambda c: f"{c['name']}-k{c['k']}")
+def test_wide_exact_counts_match_reference_tools(case):
+    k = case["k"]
+    files = _case_files(case["name"])
+    keys, counts = O.exact_records_wide(files, k)
+    hist = O.histogram(counts, 1, 10000)
+    sparse = {str(i + 1): int(v) for i, v in enumerate(hist) if v}
+    if k == 96:
+        # GetKmer<4>'s stale data[3] at k = 96 gives one 96-mer several keys:
+        # the reference reports more distinct k-mers, the same occurrences
+        ref_occ = sum(int(c) * int(v) for c, v in case["hist"].items())
+        assert sum(case["hist"].values()) > len(keys)
+        assert ref_occ == int(counts.astype(np.int64).sum())
+        return
+    assert sparse == case["hist"]
+    if k <= 64:
+        # the reference's sorted dump is an oracle up to k = 64
+        text = O.dump_text_wide(keys, counts, k)
+        assert text[:2000].decode() == case["dump_head"]
+        assert text.count(b"\n") == case["dump_lines"]
+        assert hashlib.sha256(text).hexdigest() == case["dump_sha256"]
+
+
 # ---- the reference's own test fixtures ------------------------------------
 
 def _words(*w):
