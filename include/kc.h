@@ -27,10 +27,15 @@
  * concurrently on the device (one CUDA stream each), admitted in submission
  * order as device memory frees up.
  *
- * k-mer words: a k-mer (k <= 32) is the reference's kmer<1> word
- * (src/kmer.h:15): base i of the printed canonical string sits at bit
- * 64 - 2k + 2i, padding bits are zero.  Record arrays are sorted in
- * printed-string order (the order of dump_tool --sort).
+ * k-mer words: a k-mer is the reference's kmer<N> word array (src/kmer.h:15),
+ * N = kc_key_words(k): 1 for k <= 32, 2 for k <= 64, 4 for k <= 128 (the
+ * dispatch of src/main.cpp:617-633).  For k <= 32, base i of the printed
+ * canonical string sits at bit 64 - 2k + 2i of the one word, padding bits
+ * are zero.  For k > 32 the newest base sits at data[0]'s top bits and older
+ * bases follow towards data[last] (last = (k - 1) / 32), whose low
+ * 64 - 2 * (k % 32) bits are zero; words above data[last] are zero.  Key
+ * arrays hold N consecutive words per k-mer, data[0] first.  Record arrays
+ * are sorted in printed-string order (the order of dump_tool --sort).
  */
 #ifndef KC_H
 #define KC_H
@@ -97,7 +102,7 @@ typedef struct {
     /* input: either host files or a device-resident input from kc_input_upload */
     const kc_buffer *files;
     uint32_t n_files;
-    uint32_t k;                   /* 1..32 (reference: <k_len>) */
+    uint32_t k;                   /* 1..128 (reference: <k_len>); batched jobs 1..32 */
     const kc_input *input;        /* non-NULL: use this resident input, ignore files */
     uint32_t count_max;           /* saturation of counts (reference [count_max], default 255) */
     uint32_t bloom;               /* 1: reference Bloom singleton split (src/BloomFilter.h) */
@@ -161,6 +166,8 @@ typedef struct {
     uint32_t batch_part;          /* batched jobs: the sub-batch (0, 1, ...) the sample was counted in; a
                                      batch larger than a worker's share of the device-memory budget runs
                                      as consecutive sub-batches, and device_ms is that sub-batch's time */
+    uint32_t key_words;           /* 64-bit words per k-mer in keys, top_keys and le2_keys (kc_key_words) */
+    uint32_t reserved_u32;
 } kc_result_t;
 
 /* Settings of a handle that trade memory for speed, chosen by kc_autotune or
@@ -184,6 +191,10 @@ typedef struct {
                                      pass back to exact counts); default 64M */
     uint64_t reserved[2];
 } kc_tuning;
+
+/* 64-bit words of one k-mer: 1 for k <= 32, 2 for k <= 64, 4 for k <= 128,
+ * 0 otherwise (the reference's kmer<N>, src/main.cpp:617-633). */
+uint32_t kc_key_words(uint32_t k);
 
 /* Kernel launches issued by this process so far (all handles). */
 uint64_t kc_kernel_launches(void);
@@ -236,7 +247,8 @@ int kc_host_free(void *p);
 
 /* Canonical k-mer occurrences of one FASTQ file (src/FastqReader.h:559-698
  * record splitting + src/GetKmer.h:58-130 extraction), in no particular
- * order.  *n_out receives the number of occurrences even if it exceeds cap. */
+ * order, kc_key_words(k) words each (k 1..128; out holds cap occurrences).
+ * *n_out receives the number of occurrences even if it exceeds cap. */
 int kc_extract_kmers(const char *fastq, uint64_t len, uint32_t k, uint64_t *out, uint64_t cap,
                      uint64_t *n_out);
 
@@ -284,7 +296,8 @@ int kc_sort_records_noalloc(uint64_t *d_keys, uint32_t *d_counts, uint64_t n, ui
 
 /* The sorted dump of the reference's dump_tool (tool/dump_tool.cpp:1172-1193,
  * kmer_to_buf :103-124): one "KMER\tcount\n" line per record, the k-mer's
- * printed string from its kmer<1> word, formatted on the device.  With out ==
+ * printed string from its kmer<N> words (kc_key_words(k) per record, k
+ * 1..128), formatted on the device.  With out ==
  * NULL only *n_bytes (the text's length) is computed; otherwise the text goes
  * to out (cap bytes) and *n_bytes receives its length. */
 int kc_dump_text(const uint64_t *keys, const uint32_t *counts, uint64_t n, uint32_t k, char *out, uint64_t cap,
@@ -325,7 +338,8 @@ int kc_plan_bloom(const uint32_t *raw_prefix_counts /*256*/, uint32_t avg_qualit
  * with min_count <= count <= max_count are written sorted in printed-string
  * order (*n_out receives their number even if it exceeds out_cap); hist
  * (hist_max - hist_min + 1 entries, may be NULL) receives the histogram of
- * all merged counts. */
+ * all merged counts.  k is 1..128; every key array holds kc_key_words(k)
+ * words per k-mer. */
 int kc_merge_records(const uint64_t *high_keys, const uint32_t *high_counts, uint64_t n_high,
                      const uint64_t *low_keys, uint64_t n_low, uint32_t k, uint32_t count_max,
                      uint32_t min_count, uint32_t max_count, uint32_t hist_min, uint32_t hist_max,

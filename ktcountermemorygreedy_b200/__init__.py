@@ -87,7 +87,8 @@ class kc_result_t(C.Structure):
                 ("run_ms", C.c_double), ("phase_ms", C.c_double * 12), ("phase_launches", C.c_uint64 * 12),
                 ("low_len", C.c_uint64), ("high_len", C.c_uint64), ("input_bytes", C.c_uint64),
                 ("n_records_total", C.c_uint64), ("passes", C.c_uint32), ("smem_passes", C.c_uint16),
-                ("smem_fallbacks", C.c_uint16), ("region_redos", C.c_uint32), ("batch_part", C.c_uint32)]
+                ("smem_fallbacks", C.c_uint16), ("region_redos", C.c_uint32), ("batch_part", C.c_uint32),
+                ("key_words", C.c_uint32), ("reserved_u32", C.c_uint32)]
 
 # stage names of kc_result_t.phase_ms
 PHASES = ["census", "scan", "count_pass", "insert_high", "merge_low", "compact", "sort", "queries", "bloom",
@@ -118,6 +119,7 @@ SIGNATURES = [
     ("kc_bloom_plan", C.c_int, [C.POINTER(kc_buffer), C.c_uint32, C.c_uint32, C.c_uint64, C.c_void_p,
                                 C.POINTER(C.c_uint32), C.c_void_p, C.POINTER(C.c_uint64)]),
     ("kc_kernel_launches", C.c_uint64, []),
+    ("kc_key_words", C.c_uint32, [C.c_uint32]),
     ("kc_sort_distinct_records", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32]),
     ("kc_sort_records_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]),
     ("kc_atomic_peak", C.c_int, [C.c_uint64, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
@@ -196,7 +198,8 @@ def string_key(key: int, k: int) -> int:
 class Result:
     """Outputs of one job: the precise histogram/dump of the reference tools."""
     k: int
-    keys: np.ndarray               # uint64 kmer<1> words, printed-string order
+    keys: np.ndarray               # uint64 kmer<N> words, printed-string order: shape (n,) for k <= 32,
+                                   # (n, N) for k > 32 (N = 2 up to k = 64, else 4; data[0] first)
     counts: np.ndarray             # uint32 exact counts (saturated at count_max)
     hist: np.ndarray               # int64, bins hist_min..hist_max
     hist_min: int
@@ -228,6 +231,16 @@ def _copy(ptr, n, dtype):
     if n == 0 or not ptr:
         return np.zeros(0, dtype)
     return np.ctypeslib.as_array(ptr, shape=(n,)).copy()
+
+
+def key_words(k: int) -> int:
+    """64-bit words of one k-mer (the reference's kmer<N>): 1, 2 or 4."""
+    return 1 if k <= 32 else (2 if k <= 64 else 4)
+
+
+def _keys(flat: np.ndarray, words: int) -> np.ndarray:
+    """k-mer key arrays: 1-D for one word per k-mer, (n, words) otherwise."""
+    return flat if words <= 1 else flat.reshape(-1, words)
 
 
 class _JobLease:
@@ -357,23 +370,26 @@ class KmerCounter:
         job is released when the last view is gone."""
         r = kc_result_t()
         _check(lib().kc_result(self._h, jid, C.byref(r)))
+        w = max(1, r.key_words)
         if copy:
-            keys, counts = _copy(r.keys, r.n_records, np.uint64), _copy(r.counts, r.n_records, np.uint32)
-            le2_keys, le2_counts = _copy(r.le2_keys, r.n_le2, np.uint64), _copy(r.le2_counts, r.n_le2, np.uint32)
+            keys, counts = _copy(r.keys, r.n_records * w, np.uint64), _copy(r.counts, r.n_records, np.uint32)
+            le2_keys, le2_counts = _copy(r.le2_keys, r.n_le2 * w, np.uint64), _copy(r.le2_counts, r.n_le2, np.uint32)
         else:
             # records and the count <= 2 set (often most of the k-mers) stay in
             # the job's pinned memory until the last view is gone
             lease = _JobLease(self, jid)
-            keys, counts = _view(r.keys, r.n_records, np.uint64, lease), _view(r.counts, r.n_records, np.uint32, lease)
-            le2_keys = _view(r.le2_keys, r.n_le2, np.uint64, lease)
+            keys = _view(r.keys, r.n_records * w, np.uint64, lease)
+            counts = _view(r.counts, r.n_records, np.uint32, lease)
+            le2_keys = _view(r.le2_keys, r.n_le2 * w, np.uint64, lease)
             le2_counts = _view(r.le2_counts, r.n_le2, np.uint32, lease)
             release = False
         out = Result(
             k=k,
-            keys=keys, counts=counts,
+            keys=_keys(keys, w), counts=counts,
             hist=_copy(r.hist, r.hist_len, np.int64), hist_min=0,
-            top_keys=_copy(r.top_keys, r.n_top, np.uint64), top_counts=_copy(r.top_counts, r.n_top, np.uint32),
-            le2_keys=le2_keys, le2_counts=le2_counts,
+            top_keys=_keys(_copy(r.top_keys, r.n_top * w, np.uint64), w),
+            top_counts=_copy(r.top_counts, r.n_top, np.uint32),
+            le2_keys=_keys(le2_keys, w), le2_counts=le2_counts,
             occurrences=r.occurrences, distinct=r.distinct, low_only=r.low_only,
             table_capacity=r.table_capacity, device_ms=r.device_ms, queue_ms=r.queue_ms, run_ms=r.run_ms,
             phase_ms=tuple(r.phase_ms), phase_launches=tuple(r.phase_launches), low_len=r.low_len,
@@ -492,13 +508,15 @@ def atomic_peak_shared(table_bytes: int = 16384, repeats: int = 5):
 
 
 def extract_kmers(fastq: bytes, k: int) -> np.ndarray:
-    """Canonical k-mer occurrences of one FASTQ file (unordered)."""
+    """Canonical k-mer occurrences of one FASTQ file (unordered): shape (n,)
+    for k <= 32, (n, N) kmer<N> word arrays for k > 32."""
     data = np.frombuffer(fastq, dtype=np.uint8) if len(fastq) else np.zeros(1, np.uint8)
+    w = key_words(k)
     cap = max(len(fastq), 1)
-    out = np.zeros(cap, np.uint64)
+    out = np.zeros(cap * w, np.uint64)
     n = C.c_uint64()
     _check(lib().kc_extract_kmers(_ptr(data), len(fastq), k, _ptr(out), cap, C.byref(n)))
-    return out[: n.value].copy()
+    return _keys(out[: n.value * w].copy(), w)
 
 
 def hash_kmers(keys: np.ndarray) -> np.ndarray:
@@ -545,17 +563,19 @@ def plan_bloom(raw_prefix_counts, avg_quality: int, est_file_size: int, memory_g
 
 def merge_records(high_keys, high_counts, low_keys, k: int, count_max: int, min_count: int = 1,
                   max_count: int = U32_MAX, hist_min: int = 1, hist_max: int = 10000):
-    hk = np.ascontiguousarray(high_keys, dtype=np.uint64)
+    w = key_words(k)
+    hk = np.ascontiguousarray(high_keys, dtype=np.uint64).reshape(-1)
     hc = np.ascontiguousarray(high_counts, dtype=np.uint32)
-    lk = np.ascontiguousarray(low_keys, dtype=np.uint64)
-    cap = max(len(hk) + len(lk), 1)
-    ok = np.zeros(cap, np.uint64)
+    lk = np.ascontiguousarray(low_keys, dtype=np.uint64).reshape(-1)
+    nh, nl = len(hc), len(lk) // w
+    cap = max(nh + nl, 1)
+    ok = np.zeros(cap * w, np.uint64)
     oc = np.zeros(cap, np.uint32)
     hist = np.zeros(hist_max - hist_min + 1, np.int64)
     n = C.c_uint64()
-    _check(lib().kc_merge_records(_ptr(hk), _ptr(hc), len(hk), _ptr(lk), len(lk), k, count_max, min_count,
+    _check(lib().kc_merge_records(_ptr(hk), _ptr(hc), nh, _ptr(lk), nl, k, count_max, min_count,
                                   max_count, hist_min, hist_max, _ptr(ok), _ptr(oc), cap, C.byref(n), _ptr(hist)))
-    return ok[: n.value], oc[: n.value], hist
+    return _keys(ok[: n.value * w], w), oc[: n.value], hist
 
 
 # ---- text outputs of the reference tools -------------------------------------
@@ -574,7 +594,7 @@ def dump_text(keys: np.ndarray, counts: np.ndarray, k: int) -> str:
 def dump_bytes(keys: np.ndarray, counts: np.ndarray, k: int) -> bytes:
     keys = np.ascontiguousarray(keys, dtype=np.uint64)
     counts = np.ascontiguousarray(counts, dtype=np.uint32)
-    n = len(keys)
+    n = len(counts)   # k > 32: keys has shape (n, N)
     need = C.c_uint64()
     _check(lib().kc_dump_text(_ptr(keys), _ptr(counts), n, k, None, 0, C.byref(need)))
     out = np.empty(max(need.value, 1), np.uint8)

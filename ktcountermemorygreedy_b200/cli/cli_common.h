@@ -86,24 +86,32 @@ inline std::vector<std::string> input_files(const std::string &arg)
     return names;
 }
 
+// 64-bit words of one decoded k-mer: the reference's kmer<N>, N = 1 for
+// k <= 32, 2 for k <= 64, 4 for k <= 128 (src/main.cpp:617-633).
+inline uint32_t key_words_for(uint32_t k) { return k <= 32 ? 1u : (k <= 64 ? 2u : 4u); }
+
 inline uint32_t count_bytes_for(uint32_t count_max)
 {
     return count_max <= 0xFF ? 1 : count_max <= 0xFFFF ? 2 : count_max <= 0xFFFFFF ? 3 : 4;
 }
 
+// The records of a tmp_dir; keys are kmer<N> word arrays, nw words each.
 struct TmpDir {
-    uint32_t k = 0, count_max = 0, count_bytes = 4;
+    uint32_t k = 0, count_max = 0, count_bytes = 4, nw = 1;
     std::vector<uint64_t> high_keys;
     std::vector<uint32_t> high_counts;
     std::vector<uint64_t> low_keys;
+    uint64_t n_high() const { return high_counts.size(); }
+    uint64_t n_low() const { return low_keys.size() / nw; }
 };
 
 // Record geometry of a tmp_dir, from infos.bin: a k-mer takes kb bytes (full
-// words, then the tail bytes of the last word), a high.bin record kb +
-// count_bytes (src/main.cpp:590-615, src/FinalDrainWriter.h:71-88).
+// words, then the tail bytes of the next word), a high.bin record kb +
+// count_bytes (src/main.cpp:590-615, src/FinalDrainWriter.h:71-88); decoded,
+// a k-mer is nw words (the reference's kmer<N>, src/main.cpp:617-633).
 struct Layout {
     uint32_t k = 0, count_max = 0, count_bytes = 4;
-    uint32_t full = 0, tail_bytes = 0, kb = 0, rec = 0;
+    uint32_t full = 0, tail_bytes = 0, kb = 0, rec = 0, nw = 1;
     uint64_t high_bytes = 0, low_bytes = 0;   // file sizes (read_layout)
     uint64_t n_high() const { return high_bytes / rec; }
     uint64_t n_low() const { return low_bytes / kb; }
@@ -117,21 +125,21 @@ inline bool read_infos(const std::string &dir, Layout &L, std::string &err)
     std::memcpy(&L.count_max, b.data() + 4, 4);
     L.count_bytes = count_bytes_for(L.count_max);
     if (L.k == 0 || L.k > 128) { err = "invalid k_len from infos.bin: " + std::to_string(L.k); return false; }
-    if (L.k > 32) { err = "k_len " + std::to_string(L.k) + " is above 32; k-mers of more than 32 bases are not supported"; return false; }
     L.tail_bytes = (2 * (L.k % 32) + 7) / 8;
     L.full = L.k / 32;
     L.kb = L.full * 8 + L.tail_bytes;
     L.rec = L.kb + L.count_bytes;
+    L.nw = key_words_for(L.k);
     return true;
 }
 
-// The k-mer word of one packed k-mer (the inverse of the reference's packing).
-inline uint64_t decode_key(const char *r, const Layout &L)
+// The kmer<N> words of one packed k-mer (the inverse of the reference's
+// packing): the full words, then the tail bytes at the top of the next word.
+inline void decode_key(const char *r, const Layout &L, uint64_t *w)
 {
-    uint64_t w = 0;
-    if (L.full) std::memcpy(&w, r, 8);
-    else std::memcpy(reinterpret_cast<char *>(&w) + (8 - L.tail_bytes), r, L.tail_bytes);
-    return w;
+    for (uint32_t i = 0; i < L.nw; ++i) w[i] = 0;
+    std::memcpy(w, r, L.full * 8);
+    if (L.tail_bytes) std::memcpy(reinterpret_cast<char *>(w + L.full) + (8 - L.tail_bytes), r + L.full * 8, L.tail_bytes);
 }
 
 // infos.bin, high.bin, low.bin as written by the reference counter
@@ -149,20 +157,21 @@ inline bool read_tmpdir(const std::string &dir, TmpDir &t, std::string &err)
     if (b.empty()) { err = "empty high.bin file"; return false; }
     if (b.size() % L.rec) { err = "invalid high.bin file size"; return false; }
     size_t n = b.size() / L.rec;
-    t.high_keys.resize(n);
+    t.nw = L.nw;
+    t.high_keys.resize(n * L.nw);
     t.high_counts.resize(n);
     for (size_t i = 0; i < n; ++i) {
         const char *r = b.data() + i * L.rec;
         uint32_t c = 0;
         std::memcpy(&c, r + L.kb, L.count_bytes);
-        t.high_keys[i] = decode_key(r, L);
+        decode_key(r, L, t.high_keys.data() + i * L.nw);
         t.high_counts[i] = c;
     }
     if (!read_file(dir + "low.bin", b)) { err = "failed to open " + dir + "low.bin"; return false; }
     if (b.size() % L.kb) { err = "invalid low.bin size"; return false; }
     n = b.size() / L.kb;
-    t.low_keys.resize(n);
-    for (size_t i = 0; i < n; ++i) t.low_keys[i] = decode_key(b.data() + i * L.kb, L);
+    t.low_keys.resize(n * L.nw);
+    for (size_t i = 0; i < n; ++i) decode_key(b.data() + i * L.kb, L, t.low_keys.data() + i * L.nw);
     return true;
 }
 
@@ -188,13 +197,24 @@ constexpr uint64_t SEG_SLACK_BYTES = 4ull << 20;
 
 inline uint32_t lead_bases(uint32_t k) { return std::min<uint32_t>(k, SEG_LEAD_BASES); }
 
-// The first m bases of the printed k-mer as a number, base 0 most significant
-// (base i of the printed string sits at bit 64 - 2k + 2i of the word).
-inline uint32_t lead_prefix(uint64_t w, uint32_t k, uint32_t m)
+// Base i of the printed k-mer (kmer_to_buf, tool/dump_tool.cpp:103-124): for
+// k <= 32 bit 64 - 2k + 2i of the word; otherwise the first k % 32 bases from
+// the top of word k / 32, the others from word k / 32 - 1 downwards, each
+// word from its low bits up.
+inline uint32_t key_base(const uint64_t *w, uint32_t k, uint32_t i)
+{
+    if (k <= 32) return (uint32_t)(w[0] >> (64 - 2 * k + 2 * i)) & 3u;
+    const uint32_t full = k / 32, tail = k % 32;
+    if (i < tail) return (uint32_t)(w[full] >> (64 - 2 * tail + 2 * i)) & 3u;
+    const uint32_t off = i - tail;
+    return (uint32_t)(w[full - 1 - off / 32] >> (2 * (off % 32))) & 3u;
+}
+
+// The first m bases of the printed k-mer as a number, base 0 most significant.
+inline uint32_t lead_prefix(const uint64_t *w, uint32_t k, uint32_t m)
 {
     uint32_t p = 0;
-    const uint32_t s0 = 64 - 2 * k;
-    for (uint32_t i = 0; i < m; ++i) p = (p << 2) | (uint32_t)((w >> (s0 + 2 * i)) & 3);
+    for (uint32_t i = 0; i < m; ++i) p = (p << 2) | key_base(w, k, i);
     return p;
 }
 
@@ -226,8 +246,8 @@ inline bool read_layout(const std::string &dir, Layout &L, std::string &err)
     return true;
 }
 
-// Calls f(key, count) for every record of high.bin (low = false) or every
-// k-mer of low.bin (low = true, count 0), reading whole records in blocks.
+// Calls f(key words, count) for every record of high.bin (low = false) or
+// every k-mer of low.bin (low = true, count 0), reading whole records in blocks.
 template <class F>
 inline bool scan_file(const std::string &dir, const Layout &L, bool low, F &&f, std::string &err)
 {
@@ -245,10 +265,12 @@ inline bool scan_file(const std::string &dir, const Layout &L, bool low, F &&f, 
             err = "failed to read " + path;
             return false;
         }
+        uint64_t w[4];
         for (size_t o = 0; o < want; o += rec) {
             uint32_t c = 0;
             if (!low) std::memcpy(&c, buf.data() + o + L.kb, L.count_bytes);
-            f(decode_key(buf.data() + o, L), c);
+            decode_key(buf.data() + o, L, w);
+            f(static_cast<const uint64_t *>(w), c);
         }
         done += want;
     }
@@ -272,9 +294,10 @@ inline SegCost seg_cost(uint32_t k, bool dump, bool with_low, uint64_t hist_bins
     SegCost c;
     // input keys + counts; dump: output keys + counts and the text line (k bases, tab,
     // at most 10 digits, newline)
-    const uint64_t out = dump ? 12 + (uint64_t)k + 12 : 0;
-    c.per_high = 12 + out;
-    c.per_low = with_low ? 8 + out : 0;
+    const uint64_t kw = 8ull * key_words_for(k);
+    const uint64_t out = dump ? kw + 4 + (uint64_t)k + 12 : 0;
+    c.per_high = kw + 4 + out;
+    c.per_low = with_low ? kw + out : 0;
     const uint64_t prefixes = 1ull << (2 * lead_bases(k));
     c.fixed = SEG_SLACK_BYTES + SEG_BLOCK_BYTES + 2 * prefixes * 8 + hist_bins * 16;
     return c;
@@ -322,13 +345,15 @@ inline bool count_prefixes(const std::string &dir, const Layout &L, bool with_lo
     const uint32_t m = lead_bases(L.k);
     ph.assign((size_t)1 << (2 * m), 0);
     pl.assign((size_t)1 << (2 * m), 0);
-    if (!scan_file(dir, L, false, [&](uint64_t w, uint32_t) { ++ph[lead_prefix(w, L.k, m)]; }, err)) return false;
-    if (with_low && !scan_file(dir, L, true, [&](uint64_t w, uint32_t) { ++pl[lead_prefix(w, L.k, m)]; }, err))
+    if (!scan_file(dir, L, false, [&](const uint64_t *w, uint32_t) { ++ph[lead_prefix(w, L.k, m)]; }, err))
+        return false;
+    if (with_low && !scan_file(dir, L, true, [&](const uint64_t *w, uint32_t) { ++pl[lead_prefix(w, L.k, m)]; }, err))
         return false;
     return true;
 }
 
-// Reads segment s's records: high.bin keys and counts, low.bin keys (with_low).
+// Reads segment s's records: high.bin keys (L.nw words each) and counts,
+// low.bin keys (with_low).
 inline bool load_segment(const std::string &dir, const Layout &L, bool with_low, const Segment &s,
                          std::vector<uint64_t> &hk, std::vector<uint32_t> &hc, std::vector<uint64_t> &lk,
                          std::string &err)
@@ -337,24 +362,24 @@ inline bool load_segment(const std::string &dir, const Layout &L, bool with_low,
     hk.clear();
     hc.clear();
     lk.clear();
-    hk.reserve(s.n_high);
+    hk.reserve(s.n_high * L.nw);
     hc.reserve(s.n_high);
     if (!scan_file(dir, L, false,
-                   [&](uint64_t w, uint32_t c) {
+                   [&](const uint64_t *w, uint32_t c) {
                        const uint32_t p = lead_prefix(w, L.k, m);
                        if (p >= s.p0 && p < s.p1) {
-                           hk.push_back(w);
+                           hk.insert(hk.end(), w, w + L.nw);
                            hc.push_back(c);
                        }
                    },
                    err))
         return false;
     if (with_low) {
-        lk.reserve(s.n_low);
+        lk.reserve(s.n_low * L.nw);
         if (!scan_file(dir, L, true,
-                       [&](uint64_t w, uint32_t) {
+                       [&](const uint64_t *w, uint32_t) {
                            const uint32_t p = lead_prefix(w, L.k, m);
-                           if (p >= s.p0 && p < s.p1) lk.push_back(w);
+                           if (p >= s.p0 && p < s.p1) lk.insert(lk.end(), w, w + L.nw);
                        },
                        err))
             return false;

@@ -40,13 +40,13 @@ static int segmented(const std::string &dir, const cli::Layout &L, bool precise,
             std::cerr << err << '\n';
             return 255;
         }
-        const uint64_t cap = hk.size() + lk.size();
-        keys.resize(std::max<uint64_t>(cap, 1));
+        const uint64_t cap = hc.size() + lk.size() / L.nw;
+        keys.resize(std::max<uint64_t>(cap, 1) * L.nw);
         counts.resize(std::max<uint64_t>(cap, 1));
         uint64_t n = 0;
-        int rc = kc_merge_records(hk.data(), hc.data(), hk.size(), precise ? lk.data() : nullptr,
-                                  precise ? lk.size() : 0, L.k, L.count_max, lo, hi, 1, 1, keys.data(), counts.data(),
-                                  cap, &n, nullptr);
+        int rc = kc_merge_records(hk.data(), hc.data(), hc.size(), precise ? lk.data() : nullptr,
+                                  precise ? lk.size() / L.nw : 0, L.k, L.count_max, lo, hi, 1, 1, keys.data(),
+                                  counts.data(), cap, &n, nullptr);
         if (rc != KC_OK) {
             std::fclose(f);
             std::cerr << "dump_tool: " << kc_last_error() << '\n';
@@ -92,17 +92,18 @@ int main(int argc, char **argv)
     // all records at once: the larger file's bytes, every decoded record, and
     // the merged records with their text
     const uint64_t n_out = L.n_high() + (precise ? L.n_low() : 0);
-    const uint64_t whole = std::max(L.high_bytes, L.low_bytes) + 12 * L.n_high() + 8 * L.n_low() +
-                           (24 + (uint64_t)L.k) * n_out + cli::seg_cost(L.k, true, precise, 0).fixed;
+    const uint64_t kw = 8ull * L.nw;
+    const uint64_t whole = std::max(L.high_bytes, L.low_bytes) + (kw + 4) * L.n_high() + kw * L.n_low() +
+                           (kw + 16 + (uint64_t)L.k) * n_out + cli::seg_cost(L.k, true, precise, 0).fixed;
     if (whole > budget) return segmented(dir, L, precise, lo, hi, whole, budget, argv[5]);
     cli::TmpDir t;
     if (!cli::read_tmpdir(dir, t, err)) { std::cerr << err << '\n'; return 255; }
-    const uint64_t cap = t.high_keys.size() + (precise ? t.low_keys.size() : 0);
-    std::vector<uint64_t> keys(std::max<uint64_t>(cap, 1));
+    const uint64_t cap = t.n_high() + (precise ? t.n_low() : 0);
+    std::vector<uint64_t> keys(std::max<uint64_t>(cap, 1) * t.nw);
     std::vector<uint32_t> counts(std::max<uint64_t>(cap, 1));
     uint64_t n = 0;
-    int rc = kc_merge_records(t.high_keys.data(), t.high_counts.data(), t.high_keys.size(),
-                              precise ? t.low_keys.data() : nullptr, precise ? t.low_keys.size() : 0, t.k, t.count_max,
+    int rc = kc_merge_records(t.high_keys.data(), t.high_counts.data(), t.n_high(),
+                              precise ? t.low_keys.data() : nullptr, precise ? t.n_low() : 0, t.k, t.count_max,
                               lo, hi, 1, 1, keys.data(), counts.data(), cap, &n, nullptr);
     if (rc != KC_OK) { std::cerr << "dump_tool: " << kc_last_error() << '\n'; return 2; }
     if (!cli::write_dump(argv[5], keys.data(), counts.data(), std::min(n, cap), t.k, err)) {

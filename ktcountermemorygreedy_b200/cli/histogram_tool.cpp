@@ -33,9 +33,9 @@ static int segmented(const std::string &dir, const cli::Layout &L, bool precise,
     for (const cli::Segment &s : segs) {
         if (!cli::load_segment(dir, L, precise, s, hk, hc, lk, err)) { std::cerr << err << std::endl; return 255; }
         uint64_t n = 0;
-        int rc = kc_merge_records(hk.data(), hc.data(), hk.size(), precise ? lk.data() : nullptr,
-                                  precise ? lk.size() : 0, L.k, L.count_max, 1, 0xffffffffu, lo, hi, nullptr, nullptr, 0,
-                                  &n, part.data());
+        int rc = kc_merge_records(hk.data(), hc.data(), hc.size(), precise ? lk.data() : nullptr,
+                                  precise ? lk.size() / L.nw : 0, L.k, L.count_max, 1, 0xffffffffu, lo, hi, nullptr,
+                                  nullptr, 0, &n, part.data());
         if (rc != KC_OK) { std::cerr << "histogram_tool: " << kc_last_error() << std::endl; return 2; }
         for (size_t i = 0; i < hist.size(); ++i) hist[i] += part[i];
     }
@@ -79,15 +79,16 @@ int main(int argc, char **argv)
     cli::Layout L;
     if (!cli::read_layout(dir, L, err)) { std::cerr << err << std::endl; return 255; }
     // all records at once: the larger file's bytes, then every decoded record
-    const uint64_t whole = std::max(L.high_bytes, L.low_bytes) + 12 * L.n_high() + 8 * L.n_low() +
+    const uint64_t kw = 8ull * L.nw;
+    const uint64_t whole = std::max(L.high_bytes, L.low_bytes) + (kw + 4) * L.n_high() + kw * L.n_low() +
                            cli::seg_cost(L.k, false, precise, (uint64_t)hi - lo + 1).fixed;
     if (whole > budget) return segmented(dir, L, precise, lo, hi, whole, budget, argv[5]);
     cli::TmpDir t;
     if (!cli::read_tmpdir(dir, t, err)) { std::cerr << err << std::endl; return 255; }
     std::vector<int64_t> hist((uint64_t)hi - lo + 1, 0);
     uint64_t n = 0;
-    int rc = kc_merge_records(t.high_keys.data(), t.high_counts.data(), t.high_keys.size(),
-                              precise ? t.low_keys.data() : nullptr, precise ? t.low_keys.size() : 0, t.k, t.count_max,
+    int rc = kc_merge_records(t.high_keys.data(), t.high_counts.data(), t.n_high(),
+                              precise ? t.low_keys.data() : nullptr, precise ? t.n_low() : 0, t.k, t.count_max,
                               1, 0xffffffffu, lo, hi, nullptr, nullptr, 0, &n, hist.data());
     if (rc != KC_OK) { std::cerr << "histogram_tool: " << kc_last_error() << std::endl; return 2; }
     if (!cli::write_hist(argv[5], hist.data(), lo, hi)) {

@@ -46,10 +46,6 @@ int main(int argc, char **argv)
         std::cerr << "k_len must be <= 128" << std::endl;
         return 1;
     }
-    if (k > 32) {
-        std::cerr << "k_len " << k << " is above 32; k-mers of more than 32 bases are not supported" << std::endl;
-        return 1;
-    }
     const std::string tmp = cli::with_slash(argv[5]);
     // infos.bin first, before any input is read (src/main.cpp:588-595)
     {

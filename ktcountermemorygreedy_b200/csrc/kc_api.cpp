@@ -38,6 +38,7 @@
 #include "kc_host.h"
 #include "kc_kernels.cuh"
 #include "kc_plan.h"
+#include "kc_wide.cuh"
 
 using namespace kc;
 
@@ -147,6 +148,7 @@ struct Job {
     uint64_t low_len = 0, high_len = 0, input_bytes = 0, n_records_total = 0;
     uint32_t passes = 1, smem_passes = 0, smem_fallbacks = 0, region_redos = 0;
     uint32_t batch_part = 0;   // sub-batch of a batched job
+    uint32_t key_words = 1;    // 64-bit words per k-mer in the records (kmer<N>)
     double device_ms = 0;
     double phase_ms[KC_STAGES] = {0};
     uint64_t phase_launches[KC_STAGES] = {0};
@@ -335,6 +337,27 @@ struct HostStage {
 
 // A root-prefix bucket outgrew the region estimated from the sampled census.
 struct CensusOverflow {};
+
+// Device memory one counting pass may use: 70% of the free device memory, the
+// part of this worker's workspace the job has not used yet, and what the
+// stream-ordered pool holds unused.
+uint64_t default_pass_budget(Workspace &ws)
+{
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    const size_t ws_free = ws.capacity() > ws.mark().top ? ws.capacity() - ws.mark().top : 0;
+    uint64_t pool_slack = 0;
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t reserved = 0, used = 0;
+        if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+            cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+            pool_slack = reserved - used;
+    }
+    cudaGetLastError();
+    return (uint64_t)(0.7 * (double)(free_b + ws_free + pool_slack));
+}
 
 void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, const kc_tuning &tn)
 {
@@ -715,25 +738,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
         }
         // passes over ranges of buckets, each within the device-memory budget
         // of a pass (k-mer arrays, filters, tables, records of its buckets)
-        uint64_t budget = P.pass_bytes;
-        if (!budget) {
-            // free device memory, the part of this worker's workspace the job
-            // has not used yet, and what the stream-ordered pool holds unused
-            size_t free_b = 0, total_b = 0;
-            CK(cudaMemGetInfo(&free_b, &total_b));
-            const size_t ws_free = ws.capacity() > ws.mark().top ? ws.capacity() - ws.mark().top : 0;
-            uint64_t pool_slack = 0;
-            int dev = 0;
-            cudaMemPool_t pool;
-            if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-                uint64_t reserved = 0, used = 0;
-                if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
-                    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
-                    pool_slack = reserved - used;
-            }
-            cudaGetLastError();
-            budget = (uint64_t)(0.7 * (double)(free_b + ws_free + pool_slack));
-        }
+        const uint64_t budget = P.pass_bytes ? P.pass_bytes : default_pass_budget(ws);
         const uint64_t per_occ = P.bloom ? 42 : 48;
         std::vector<std::pair<uint32_t, uint32_t>> ranges;
         {
@@ -1324,9 +1329,365 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
     job.n_records_total = n_rec;
 }
 
+// ---------------------------------------------------------------------------
+// k-mers of 33..128 bases (the reference's process_main<2> / <4>,
+// src/main.cpp:617-633)
+// ---------------------------------------------------------------------------
+//
+// One job: upload -> newline census -> SCAN (occurrences, HyperLogLog,
+// occurrences per root prefix) -> per pass over a range of root prefixes:
+// INSERT into an N-word table sized from the estimate (regrown when full) ->
+// compaction (count, then records + histogram) -> sort of all records in
+// printed-string order -> queries -> host.  Jobs whose tables do not fit in
+// one pass's memory run in passes, each pass's records held in pinned host
+// memory until the final sort.  The Bloom split (kc_job.bloom) only chooses
+// which occurrences the reference keeps in memory; the counts are exact
+// either way, so these jobs count every occurrence in the table.
+void run_wide_job(Job &job, cudaStream_t st, Workspace &ws, const kc_tuning &tn)
+{
+    const kc_job &P = job.p;
+    const uint32_t k = P.k, nw = key_words(k);
+    if (P.fault_inject & KC_INJECT_NOMEM) ws.fail_next_get();
+    DevScope ds(st, &ws);
+    std::vector<uint32_t> tile_seg_host;
+    kc_input local;
+    const kc_input *in = job.input;
+    std::vector<PinnedBlock> inflated;
+    if (!in) {
+        const std::vector<kc_buffer> files = inflate_inputs(job.files, inflated);
+        build_input(local, files.data(), (uint32_t)files.size(), st, &ds, tile_seg_host);
+        in = &local;
+    }
+    HostStage hs(st);
+    cudaEvent_t ev0, ev1;
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); }
+    } evg{ev0, ev1};
+    CK(cudaEventRecord(ev0, st));
+    PhaseClock clk(st);
+
+    const uint64_t T = in->n_tiles;
+    const uint32_t n_seg = (uint32_t)in->segs.size();
+    std::vector<Seg> segs = in->segs;
+    for (auto &sg : segs) {
+        sg.k = k;
+        sg.sample = 0;
+        sg.sample_end = 0;
+    }
+    Seg *d_segs = ds.n<Seg>(std::max<uint32_t>(n_seg, 1));
+    if (n_seg) CK(cudaMemcpyAsync(d_segs, hs.up(segs.data(), n_seg), n_seg * sizeof(Seg), cudaMemcpyHostToDevice, st));
+    unsigned long long *counters = ds.n<unsigned long long>(C_COUNT);
+    CK(cudaMemsetAsync(counters, 0, C_COUNT * 8, st));
+
+    // ---- line numbers of tile starts ---------------------------------------
+    uint32_t *tile_nl = ds.n<uint32_t>(std::max<uint64_t>(T, 1));
+    int32_t *tile_lastnl = ds.n<int32_t>(std::max<uint64_t>(T, 1));
+    unsigned long long *tile_prefix = ds.n<unsigned long long>(std::max<uint64_t>(T, 1));
+    unsigned long long *scan_tmp = ds.n<unsigned long long>(scan_tmp_words(std::max<uint64_t>(T, 1)));
+    clk.begin(0);
+    CK(launch_newlines(in->buf, T, tile_nl, tile_lastnl, st));
+    CK(launch_scan_u32(tile_nl, tile_prefix, T, scan_tmp, st));
+    clk.end();
+    if (P.fault_inject & KC_INJECT_WAIT_TIMEOUT)
+        CK(launch_wait_flag(reinterpret_cast<const unsigned int *>(counters + C_COUNT - 1), 1024, counters + C_FLAGS,
+                            st));
+
+    // ---- SCAN: occurrences, distinct estimate, root-prefix histogram ---------
+    unsigned long long *scan_out = ds.n<unsigned long long>(1 + N_BUCKETS);   // occurrences, 256 bucket counts
+    uint32_t *hll = ds.n<uint32_t>(HLL_M);
+    CK(cudaMemsetAsync(scan_out, 0, (1 + N_BUCKETS) * 8, st));
+    CK(cudaMemsetAsync(hll, 0, HLL_M * 4, st));
+    WideArgs a{};
+    a.buf = in->buf;
+    a.n_tiles = T;
+    a.tile_prefix = reinterpret_cast<const uint64_t *>(tile_prefix);
+    a.tile_seg = in->d_tile_seg;
+    a.segs = d_segs;
+    a.counters = counters;
+    a.occ = scan_out;
+    a.bucket_hist = scan_out + 1;
+    a.hll = hll;
+    clk.begin(1);
+    CK(launch_wide_extract(WMODE_SCAN, k, a, st));
+    clk.end();
+    unsigned long long *h_scan = hs.n<unsigned long long>(1 + N_BUCKETS);
+    uint32_t *h_hll = hs.n<uint32_t>(HLL_M);
+    CK(cudaMemcpyAsync(h_scan, scan_out, (1 + N_BUCKETS) * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(h_hll, hll, HLL_M * 4, cudaMemcpyDeviceToHost, st));
+    Counters c0 = read_counters(counters, st);
+    check_flags(c0.v[C_FLAGS], "scan");
+    const uint64_t O = h_scan[0];
+    std::vector<uint64_t> bh(h_scan + 1, h_scan + 1 + N_BUCKETS);
+    const double est = hll_estimate(h_hll, HLL_M);
+    job.occurrences = O;
+    check_cancel(job, "after the scan");
+
+    // ---- passes over ranges of root prefixes ------------------------------------
+    // a pass holds its table (slots per estimated distinct k-mer at the
+    // handle's table factor) and its records (count pass, then the written
+    // records); the final sort holds every record twice plus its temporaries
+    const uint64_t slot_bytes = 8ull * nw + 8, rec_bytes = 8ull * nw + 4;
+    const double factor = std::max(tn.table_factor, 1.25);
+    const uint64_t budget = P.pass_bytes ? P.pass_bytes : default_pass_budget(ws);
+    std::vector<std::pair<uint32_t, uint32_t>> ranges;
+    {
+        uint32_t lo = 0;
+        uint64_t need = 0;
+        for (uint32_t b = 0; b < N_BUCKETS; ++b) {
+            const double share = O ? (double)bh[b] / (double)O : 0.0;
+            const uint64_t nb = (uint64_t)(share * est * (factor * slot_bytes + rec_bytes)) + 4096;
+            if (b > lo && need + nb > budget) {
+                ranges.push_back({lo, b});
+                lo = b;
+                need = 0;
+            }
+            need += nb;
+        }
+        ranges.push_back({lo, N_BUCKETS});
+    }
+    const bool multi = ranges.size() > 1;
+    unsigned long long *hist = ds.n<unsigned long long>(HIST_BINS);
+    CK(cudaMemsetAsync(hist, 0, HIST_BINS * 8, st));
+    const uint64_t ovf_cap = std::max<uint64_t>(1ull << 20, (uint64_t)(est / HIST_BINS) + 1);
+    uint32_t *ovf = ds.n<uint32_t>(ovf_cap);
+    std::vector<std::unique_ptr<HostRecords>> spilled;
+    uint64_t n_rec = 0, inserted_total = 0, table_cap = 0;
+    unsigned long long *rec_keys = nullptr;
+    uint32_t *rec_counts = nullptr;
+    bool injected_full = false;
+    for (const auto &rg : ranges) {
+        const DevScope::Mark mk = ds.mark();
+        uint64_t occ_r = 0;
+        for (uint32_t b = rg.first; b < rg.second; ++b) occ_r += bh[b];
+        const double est_r = O ? est * (double)occ_r / (double)O : 0.0;
+        uint64_t cap = table_capacity_for(est_r * 1.1, factor);
+        WideTable tab{};
+        for (int attempt = 0;; ++attempt) {
+            check_cancel(job, "before a counting pass");
+            tab.cap = cap;
+            tab.keys = ds.n<unsigned long long>(cap * nw);
+            tab.meta = ds.n<uint32_t>(cap * 2);
+            CK(launch_wide_init(tab, st));
+            CK(cudaMemsetAsync(counters + C_FLAGS, 0, 8, st));
+            CK(cudaMemsetAsync(counters + C_HIGH_LEN, 0, 8, st));
+            a.table = tab;
+            a.max_probe = (uint32_t)std::min<uint64_t>(cap, 1u << 16);
+            a.bucket_lo = rg.first;
+            a.bucket_hi = rg.second == N_BUCKETS ? 0 : rg.second;
+            clk.begin(2);
+            CK(launch_wide_extract(WMODE_INSERT, k, a, st));
+            clk.end();
+            Counters ci = read_counters(counters, st);
+            bool full = (ci.v[C_FLAGS] & ERR_TABLE_FULL) != 0;
+            if ((P.fault_inject & KC_INJECT_TABLE_FULL) || ((P.fault_inject & KC_INJECT_TABLE_FULL_ONCE) && !injected_full)) {
+                injected_full = true;
+                full = true;
+            }
+            check_flags(ci.v[C_FLAGS] & ~ERR_TABLE_FULL, "insert");
+            if (!full) {
+                inserted_total += ci.v[C_HIGH_LEN];
+                break;
+            }
+            if (attempt >= 3) throw KcError{KC_ERR_DEVICE, "counting table overflow"};
+            ds.release(tab.meta);
+            ds.release(tab.keys);
+            cap *= 2;
+        }
+        table_cap = std::max(table_cap, cap);
+        // compaction: the records kept, then the records and the histogram
+        clk.begin(5);
+        CK(cudaMemsetAsync(counters + C_KEPT, 0, 8, st));
+        CK(launch_wide_compact(k, tab, P.count_max, P.min_count, P.max_count, nullptr, nullptr, 0, nullptr, nullptr, 0,
+                               counters, 1, st));
+        Counters ck = read_counters(counters, st);
+        const uint64_t kept = ck.v[C_KEPT];
+        const uint64_t rec0 = ck.v[C_REC_LEN];
+        unsigned long long *rk = ds.n<unsigned long long>(std::max<uint64_t>(kept, 1) * nw);
+        uint32_t *rc = ds.n<uint32_t>(std::max<uint64_t>(kept, 1));
+        CK(cudaMemsetAsync(counters + C_REC_LEN, 0, 8, st));
+        CK(launch_wide_compact(k, tab, P.count_max, P.min_count, P.max_count, rk, rc, kept, hist, ovf, ovf_cap, counters,
+                               0, st));
+        clk.end();
+        (void)rec0;
+        if (multi) {
+            auto hr = std::make_unique<HostRecords>();
+            hr->allocate(kept, nw);
+            if (kept) {
+                CK(cudaMemcpyAsync(hr->keys(), rk, kept * nw * 8, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(hr->counts(), rc, kept * 4, cudaMemcpyDeviceToHost, st));
+            }
+            Counters cw = read_counters(counters, st);
+            check_flags(cw.v[C_FLAGS], "compaction");
+            n_rec += kept;
+            spilled.push_back(std::move(hr));
+            ds.rewind(mk);
+        } else {
+            n_rec = kept;
+            rec_keys = rk;
+            rec_counts = rc;
+        }
+    }
+    if (inserted_total != O) throw KcError{KC_ERR_DEVICE, "counting passes do not add up to the occurrences"};
+    job.passes = (uint32_t)ranges.size();
+    job.table_cap = table_cap;
+    job.high_len = inserted_total;
+    if (multi) {
+        rec_keys = ds.n<unsigned long long>(std::max<uint64_t>(n_rec, 1) * nw);
+        rec_counts = ds.n<uint32_t>(std::max<uint64_t>(n_rec, 1));
+        uint64_t at = 0;
+        for (auto &hr : spilled) {
+            if (hr->n) {
+                CK(cudaMemcpyAsync(rec_keys + at * nw, hr->keys(), hr->n * nw * 8, cudaMemcpyHostToDevice, st));
+                CK(cudaMemcpyAsync(rec_counts + at, hr->counts(), hr->n * 4, cudaMemcpyHostToDevice, st));
+            }
+            at += hr->n;
+        }
+        CK(cudaStreamSynchronize(st));
+        spilled.clear();
+    }
+    check_cancel(job, "before the sort");
+
+    // ---- sort in printed-string order -----------------------------------------
+    clk.begin(6);
+    unsigned long long *sk = ds.n<unsigned long long>(std::max<uint64_t>(n_rec, 1) * nw);
+    uint32_t *sc = ds.n<uint32_t>(std::max<uint64_t>(n_rec, 1));
+    {
+        void *stmp = ds.get(wide_sort_tmp_bytes(n_rec));
+        CK(launch_wide_sort(k, rec_keys, rec_counts, n_rec, sk, sc, stmp, counters + C_FLAGS, st));
+        ds.release(stmp);
+    }
+    clk.end();
+
+    // ---- histogram and counters ---------------------------------------------------
+    unsigned long long *p_c2 = hs.n<unsigned long long>(C_COUNT);
+    unsigned long long *p_hd = hs.n<unsigned long long>(HIST_BINS);
+    CK(cudaMemcpyAsync(p_c2, counters, C_COUNT * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(p_hd, hist, HIST_BINS * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    Counters c2{};
+    std::memcpy(c2.v, p_c2, sizeof(c2.v));
+    check_flags(c2.v[C_FLAGS], "sort");
+    job.distinct = c2.v[C_DISTINCT];
+    std::vector<unsigned long long> hd(p_hd, p_hd + HIST_BINS);
+    const uint64_t n_ovf = std::min<uint64_t>(c2.v[C_OVF_LEN], ovf_cap);
+    std::vector<uint32_t> ovf_h(n_ovf);
+    if (n_ovf) {
+        CK(cudaMemcpyAsync(ovf_h.data(), ovf, n_ovf * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    {
+        uint32_t lo = P.hist_min, hi = P.hist_max;
+        if (hi < lo) hi = lo;
+        job.hist.assign((uint64_t)hi - lo + 1, 0);
+        for (uint64_t c = std::max<uint64_t>(lo, 1); c < HIST_BINS && c <= hi; ++c) job.hist[c - lo] = (int64_t)hd[c];
+        for (uint32_t c : ovf_h)
+            if (c >= lo && c <= hi) job.hist[c - lo]++;
+    }
+
+    // ---- queries: record positions selected by count, their keys gathered --------
+    if ((P.top_n || P.want_le2) && n_rec) {
+        clk.begin(7);
+        unsigned long long *idx = ds.n<unsigned long long>(n_rec);
+        CK(launch_iota_u64(idx, n_rec, st));
+        uint32_t *flags = ds.n<uint32_t>(n_rec);
+        unsigned long long *pos = ds.n<unsigned long long>(n_rec);
+        unsigned long long *qtmp = ds.n<unsigned long long>(scan_tmp_words(n_rec));
+        auto select = [&](uint32_t lo, uint32_t hi, uint64_t limit, int ctr, std::vector<uint64_t> &keys_out,
+                          std::vector<uint32_t> &counts_out) {
+            unsigned long long *si = ds.n<unsigned long long>(std::max<uint64_t>(limit, 1));
+            uint32_t *scn = ds.n<uint32_t>(std::max<uint64_t>(limit, 1));
+            CK(cudaMemsetAsync(&counters[ctr], 0, 8, st));
+            CK(launch_select_range(idx, sc, n_rec, lo, hi, limit, si, scn, flags, pos, qtmp, counters, ctr, st));
+            Counters cs = read_counters(counters, st);
+            const uint64_t m = std::min<uint64_t>(cs.v[ctr], limit);
+            unsigned long long *rows = ds.n<unsigned long long>(std::max<uint64_t>(m, 1) * nw);
+            CK(launch_wide_gather_rows(k, sk, si, m, rows, st));
+            keys_out.resize(m * nw);
+            counts_out.resize(m);
+            if (m) {
+                CK(cudaMemcpyAsync(keys_out.data(), rows, m * nw * 8, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(counts_out.data(), scn, m * 4, cudaMemcpyDeviceToHost, st));
+            }
+            CK(cudaStreamSynchronize(st));
+        };
+        if (P.top_n) {
+            // the count threshold from the histogram: records above it, then
+            // the first ones at it in printed-string order
+            std::vector<uint32_t> big;
+            for (uint32_t c : ovf_h)
+                if (c >= P.min_count && c <= P.max_count) big.push_back(c);
+            std::sort(big.begin(), big.end(), std::greater<uint32_t>());
+            uint64_t above = 0;
+            uint32_t thr = std::max<uint32_t>(P.min_count, 1);
+            bool found = false;
+            for (size_t i = 0; i < big.size(); ++i) {
+                if (above + 1 >= P.top_n) { thr = big[i]; found = true; break; }
+                ++above;
+            }
+            if (!found) {
+                const uint64_t hi = std::min<uint64_t>((uint64_t)P.max_count, HIST_BINS - 1);
+                for (uint64_t c = hi; c >= std::max<uint32_t>(P.min_count, 1); --c) {
+                    const uint64_t h = hd[c];
+                    if (above + h >= P.top_n) { thr = (uint32_t)c; break; }
+                    above += h;
+                    if (c == 0) break;
+                }
+            }
+            std::vector<uint64_t> ka, kb;
+            std::vector<uint32_t> ca, cb;
+            if (thr < 0xffffffffu) select(thr + 1, 0xffffffffu, P.top_n, C_SEL_A, ka, ca);
+            const uint64_t need = P.top_n - std::min<uint64_t>(ca.size(), P.top_n);
+            if (need) select(thr, thr, need, C_SEL_B, kb, cb);
+            // count desc, then printed string asc (a stable sort of records
+            // already in printed-string order)
+            std::vector<size_t> order(ca.size());
+            for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+            std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return ca[x] > ca[y]; });
+            for (size_t i : order) {
+                job.top_keys.insert(job.top_keys.end(), ka.begin() + i * nw, ka.begin() + (i + 1) * nw);
+                job.top_counts.push_back(ca[i]);
+            }
+            job.top_keys.insert(job.top_keys.end(), kb.begin(), kb.end());
+            job.top_counts.insert(job.top_counts.end(), cb.begin(), cb.end());
+        }
+        if (P.want_le2) {
+            std::vector<uint64_t> kl;
+            std::vector<uint32_t> cl;
+            select(0, 2, n_rec, C_SEL_A, kl, cl);
+            job.le2.allocate(cl.size(), nw);
+            if (!cl.empty()) {
+                std::memcpy(job.le2.keys(), kl.data(), kl.size() * 8);
+                std::memcpy(job.le2.counts(), cl.data(), cl.size() * 4);
+            }
+        }
+        clk.end();
+    }
+    CK(cudaEventRecord(ev1, st));
+
+    // ---- records to host ----------------------------------------------------------
+    if (P.keep_records) {
+        job.recs.allocate(n_rec, nw);
+        if (n_rec) {
+            CK(cudaMemcpyAsync(job.recs.keys(), sk, n_rec * nw * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(job.recs.counts(), sc, n_rec * 4, cudaMemcpyDeviceToHost, st));
+        }
+    }
+    CK(cudaStreamSynchronize(st));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ev0, ev1));
+    job.device_ms = ms;
+    clk.collect(job.phase_ms, job.phase_launches, ev0);
+    job.input_bytes = in->total_bytes;
+    job.n_records_total = n_rec;
+    job.key_words = nw;
+}
+
 void validate_job(const kc_job &p)
 {
-    if (p.k < 1 || p.k > 32) throw KcError{KC_ERR_INVALID, "k must be in 1..32"};
+    if (p.k < 1 || p.k > 128) throw KcError{KC_ERR_INVALID, "k must be in 1..128"};
     if (!p.input && p.n_files && !p.files) throw KcError{KC_ERR_INVALID, "files is NULL"};
     if (p.count_max == 0) throw KcError{KC_ERR_INVALID, "count_max must be >= 1"};
     if (p.filter_max < p.filter_min) throw KcError{KC_ERR_INVALID, "filter_max < filter_min"};
@@ -1348,11 +1709,16 @@ uint64_t reserve_for(const kc_job &p, uint64_t resident_bytes)
 {
     uint64_t s = p.input ? resident_bytes : input_bytes(p);
     // input + per-tile tables + table/records/sort sized for distinct <= s/2
-    return (p.input ? 0 : s) + s / 256 + 24 * s + (64ULL << 20);
+    // (k-mers of more than 32 bases take 2 or 4 words)
+    return (p.input ? 0 : s) + s / 256 + 24 * (uint64_t)key_words(p.k) * s + (64ULL << 20);
 }
 
 void run_job(Job &job, cudaStream_t st, Workspace &ws, const kc_tuning &tn)
 {
+    if (job.p.k > 32) {
+        run_wide_job(job, st, ws, tn);
+        return;
+    }
     try {
         run_job_once(job, st, ws, false, tn);
     } catch (const CensusOverflow &) {
@@ -1691,6 +2057,8 @@ extern "C" {
 
 uint64_t kc_kernel_launches(void) { return kernel_launches(); }
 
+uint32_t kc_key_words(uint32_t k) { return (k >= 1 && k <= 128) ? key_words(k) : 0u; }
+
 void kc_job_defaults(kc_job *job)
 {
     if (!job) return;
@@ -1820,6 +2188,8 @@ static int submit_task(kc_handle *h, const kc_job *jobs, uint32_t n, kc_job_id *
         for (uint32_t i = 0; i < n; ++i) {
             validate_job(jobs[i]);
             if (batch && jobs[i].bloom) throw KcError{KC_ERR_INVALID, "Bloom mode is not available for batched jobs"};
+            if (batch && jobs[i].k > 32)
+                throw KcError{KC_ERR_INVALID, "k-mers of more than 32 bases are not available for batched jobs"};
             if (batch && (jobs[i].top_n || jobs[i].want_le2))
                 throw KcError{KC_ERR_INVALID, "count queries are not available for batched jobs"};
             if (batch && jobs[i].input) throw KcError{KC_ERR_INVALID, "batched jobs take host files"};
@@ -2009,6 +2379,7 @@ int kc_result(kc_handle *h, kc_job_id id, kc_result_t *out)
     out->smem_fallbacks = (uint16_t)std::min<uint32_t>(j.smem_fallbacks, 0xFFFF);
     out->region_redos = j.region_redos;
     out->batch_part = j.batch_part;
+    out->key_words = j.key_words;
     return KC_OK;
 }
 
@@ -2116,10 +2487,11 @@ extern "C" int kc_write_tmpdir(kc_handle *h, kc_job_id id, const char *dir)
     bool ok = write_all(f, info, sizeof(info));
     ok = (fclose(f) == 0) && ok;
     if (!ok) return fail(KC_ERR_IO, "write failed: infos.bin");
-    // high.bin: exact counts, record = tail bytes of the masked word + count
-    // bytes (src/FinalDrainWriter.h:71-88); the counter-side filter
+    // high.bin: exact counts, record = the full words (k / 32 of them), the
+    // tail bytes of the masked next word, the count bytes
+    // (src/FinalDrainWriter.h:71-88); the counter-side filter
     // (src/FinalDrainWriter.h:101) is applied to the exact count
-    const uint32_t k = j.p.k;
+    const uint32_t k = j.p.k, nw = j.recs.words;
     const uint32_t tail_bits = 2 * (k % 32), tail_bytes = (tail_bits + 7) / 8, full = k / 32;
     const uint64_t tmask = tail_bits ? (~0ULL << (64 - tail_bits)) : 0;
     const uint32_t cb = j.p.count_max <= 0xFF ? 1 : j.p.count_max <= 0xFFFF ? 2 : j.p.count_max <= 0xFFFFFF ? 3 : 4;
@@ -2131,12 +2503,12 @@ extern "C" int kc_write_tmpdir(kc_handle *h, kc_job_id id, const char *dir)
     for (size_t i = 0; i < j.recs.n; ++i) {
         uint32_t c = j.recs.counts()[i];
         if ((uint64_t)c + 1 < j.p.filter_min || c > j.p.filter_max) continue;
-        uint8_t r[16];
-        uint64_t w = j.recs.keys()[i];
-        if (full) std::memcpy(r, &w, 8);
-        else {
-            uint64_t t = w & tmask;
-            std::memcpy(r, reinterpret_cast<const uint8_t *>(&t) + (8 - tail_bytes), tail_bytes);
+        uint8_t r[48];
+        const uint64_t *w = j.recs.keys() + i * nw;
+        std::memcpy(r, w, full * 8);
+        if (tail_bytes) {
+            const uint64_t t = w[full] & tmask;
+            std::memcpy(r + full * 8, reinterpret_cast<const uint8_t *>(&t) + (8 - tail_bytes), tail_bytes);
         }
         std::memcpy(r + full * 8 + tail_bytes, &c, cb);
         buf.insert(buf.end(), r, r + rec);

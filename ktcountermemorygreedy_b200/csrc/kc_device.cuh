@@ -35,6 +35,77 @@ __device__ __forceinline__ uint64_t slot_hash(uint64_t x)
 }
 
 // ---------------------------------------------------------------------------
+// FASTQ bytes
+// ---------------------------------------------------------------------------
+
+// Bit i of the result is bit 0 of byte i of x (x's bytes hold 0 or 1).
+__device__ __forceinline__ uint32_t byte_bits4(uint32_t x)
+{
+    return (x * 0x01020408u) >> 24 & 0xFu;
+}
+
+// 2-bit codes (A0 C1 G2 T/U3, case-insensitive, as the reference's
+// char_to_2bit table and its AVX2 classifier), valid-base mask and newline
+// mask of 32 bytes at p (16-byte aligned shared memory), four bytes per
+// 32-bit word at a time.  With u = byte & 0xDF (upper case), the valid
+// letters A C G T U are 0x41 0x43 0x47 0x54 0x55: bit 7 clear, bit 6 set,
+// bit 3 clear, and either bit 4 clear, bit 0 set and not (bit 2 set with
+// bit 1 clear) -- 00001 00011 00111 -- or bit 4 set, bit 2 set, bit 1 clear
+// -- 10100 10101.  The code is ((u >> 1) & 3) ^ ((u >> 2) & 1).
+__device__ __forceinline__ void classify32(const uint8_t *p, uint64_t &codes, uint32_t &valid, uint32_t &nl)
+{
+    const uint4 a = *reinterpret_cast<const uint4 *>(p);
+    const uint4 b = *reinterpret_cast<const uint4 *>(p + 16);
+    const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    uint64_t c = 0;
+    uint32_t v = 0, n = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const uint32_t x = w[i];
+        // newline bytes: zero bytes of x ^ 0x0a0a0a0a (exact, no borrow)
+        const uint32_t z = x ^ 0x0a0a0a0au;
+        const uint32_t nz = (((z & 0x7f7f7f7fu) + 0x7f7f7f7fu) | z) & 0x80808080u;   // 0x80 where byte != 0
+        n |= byte_bits4((~nz & 0x80808080u) >> 7) << (4 * i);
+        const uint32_t u = x & 0xdfdfdfdfu;
+        const uint32_t x0 = u, x1 = u >> 1, x2 = u >> 2, x3 = u >> 3, x4 = u >> 4, x6 = u >> 6, x7 = u >> 7;
+        const uint32_t ok = x6 & ~x7 & ~x3 & ((~x4 & x0 & ~(x2 & ~x1)) | (x4 & x2 & ~x1)) & 0x01010101u;
+        v |= byte_bits4(ok) << (4 * i);
+        // four 2-bit codes, one per byte, packed into 8 bits
+        const uint32_t c4 = ((u >> 1) & 0x03030303u) ^ ((u >> 2) & 0x01010101u);
+        const uint32_t c2 = c4 | (c4 >> 6);                       // bytes 0 and 2 hold two codes each
+        const uint32_t c8 = (c2 & 0xfu) | ((c2 >> 12) & 0xf0u);
+        c |= (uint64_t)c8 << (8 * i);
+    }
+    codes = c;
+    valid = v;
+    nl = n;
+}
+
+__device__ __forceinline__ uint32_t range_mask(uint32_t a, uint32_t b)
+{
+    uint32_t hi = b >= 32 ? 0xffffffffu : ((1u << b) - 1u);
+    uint32_t lo = a >= 32 ? 0xffffffffu : ((1u << a) - 1u);
+    return hi & ~lo;
+}
+
+// Bytes of the 32-byte segment that lie in lines whose number is
+// `want` mod 4, given the line number at the segment start.
+__device__ __forceinline__ uint32_t line_mask(uint64_t line0, uint32_t nl, uint32_t want)
+{
+    uint32_t m = 0, pos = 0, bits = nl;
+    uint64_t cur = line0;
+    while (bits) {
+        uint32_t j = __ffs(bits) - 1;
+        if ((cur & 3) == want) m |= range_mask(pos, j);
+        ++cur;
+        pos = j + 1;
+        bits &= bits - 1;
+    }
+    if ((cur & 3) == want) m |= range_mask(pos, 32);
+    return m;
+}
+
+// ---------------------------------------------------------------------------
 // Reference hashes on the 8-byte kmer<1> word (little-endian bytes of w)
 // ---------------------------------------------------------------------------
 

@@ -3,6 +3,7 @@
 // kc_bloom_plan).  The single-step calls run synchronously on the current
 // device with a private stream.
 #include "kc_host.h"
+#include "kc_wide.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -325,11 +326,12 @@ PinnedPool::~PinnedPool()
     delete impl_;
 }
 
-void HostRecords::allocate(uint64_t count)
+void HostRecords::allocate(uint64_t count, uint32_t key_words)
 {
     reset();
     n = count;
-    const size_t need = ((count * 8 + 255) & ~size_t(255)) + count * 4 + 256;
+    words = key_words;
+    const size_t need = ((count * 8 * key_words + 255) & ~size_t(255)) + count * 4 + 256;
     block = PinnedPool::instance().get(need, bytes);
 }
 
@@ -339,6 +341,7 @@ void HostRecords::reset()
     block = nullptr;
     bytes = 0;
     n = 0;
+    words = 1;
 }
 
 void ChunkedUpload::enqueue(size_t upto)
@@ -496,8 +499,9 @@ const char *kc_last_error(void) { return kc::g_err.c_str(); }
 int kc_extract_kmers(const char *fastq, uint64_t len, uint32_t k, uint64_t *out, uint64_t cap, uint64_t *n_out)
 {
     if ((!fastq && len) || (!out && cap) || !n_out) return set_error(KC_ERR_INVALID, "bad argument");
-    if (k < 1 || k > 32) return set_error(KC_ERR_INVALID, "k must be in 1..32");
+    if (k < 1 || k > 128) return set_error(KC_ERR_INVALID, "k must be in 1..128");
     try {
+        const uint32_t nw = key_words(k);
         StreamGuard sg;
         cudaStream_t st = sg.st;
         DevScope ds(st);
@@ -509,24 +513,37 @@ int kc_extract_kmers(const char *fastq, uint64_t len, uint32_t k, uint64_t *out,
         unsigned long long *counters = ds.n<unsigned long long>(C_COUNT);
         CK(cudaMemsetAsync(counters, 0, C_COUNT * 8, st));
         const uint64_t lcap = std::max<uint64_t>(cap, 1);
-        unsigned long long *list = ds.n<unsigned long long>(lcap);
-        ExtractArgs a{};
-        a.buf = in.buf;
-        a.n_tiles = in.n_tiles;
-        a.tile_prefix = reinterpret_cast<const uint64_t *>(pr.tile_prefix);
-        a.tile_seg = in.d_tile_seg;
-        a.segs = pr.d_segs;
-        a.counters = counters;
-        a.list = list;
-        a.list_cap = cap;
-        CK(launch_extract(MODE_EMIT, a, 0, st));
+        unsigned long long *list = ds.n<unsigned long long>(lcap * nw);
+        if (nw == 1) {
+            ExtractArgs a{};
+            a.buf = in.buf;
+            a.n_tiles = in.n_tiles;
+            a.tile_prefix = reinterpret_cast<const uint64_t *>(pr.tile_prefix);
+            a.tile_seg = in.d_tile_seg;
+            a.segs = pr.d_segs;
+            a.counters = counters;
+            a.list = list;
+            a.list_cap = cap;
+            CK(launch_extract(MODE_EMIT, a, 0, st));
+        } else {
+            WideArgs a{};
+            a.buf = in.buf;
+            a.n_tiles = in.n_tiles;
+            a.tile_prefix = reinterpret_cast<const uint64_t *>(pr.tile_prefix);
+            a.tile_seg = in.d_tile_seg;
+            a.segs = pr.d_segs;
+            a.counters = counters;
+            a.list = list;
+            a.list_cap = cap;
+            CK(launch_wide_extract(WMODE_EMIT, k, a, st));
+        }
         unsigned long long c[C_COUNT];
         CK(cudaMemcpyAsync(c, counters, sizeof(c), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         if (c[C_FLAGS] & ERR_WAIT_TIMEOUT) return set_error(KC_ERR_DEVICE, "bounded wait expired");
         *n_out = c[C_EMIT_LEN];
         uint64_t n = std::min<uint64_t>(c[C_EMIT_LEN], cap);
-        if (n) CK(cudaMemcpyAsync(out, list, n * 8, cudaMemcpyDeviceToHost, st));
+        if (n) CK(cudaMemcpyAsync(out, list, n * nw * 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         return KC_OK;
     } catch (const KcError &e) {
@@ -615,7 +632,8 @@ int kc_dump_text(const uint64_t *keys, const uint32_t *counts, uint64_t n, uint3
                  uint64_t *n_bytes)
 {
     if (!n_bytes || (n && (!keys || !counts))) return set_error(KC_ERR_INVALID, "bad argument");
-    if (k < 1 || k > 32) return set_error(KC_ERR_INVALID, "k must be in 1..32");
+    if (k < 1 || k > 128) return set_error(KC_ERR_INVALID, "k must be in 1..128");
+    const uint32_t nw = key_words(k);
     if (!out) {
         // size query: k bases, a tab, the decimal count and a newline per record
         uint64_t need = 0;
@@ -634,7 +652,7 @@ int kc_dump_text(const uint64_t *keys, const uint32_t *counts, uint64_t n, uint3
         // records in chunks, so that device memory stays bounded
         const uint64_t chunk = std::min<uint64_t>(n, 1ull << 25);
         DevScope ds(sg.st);
-        unsigned long long *dk = ds.n<unsigned long long>(chunk);
+        unsigned long long *dk = ds.n<unsigned long long>(chunk * nw);
         uint32_t *dc = ds.n<uint32_t>(chunk);
         uint32_t *len = ds.n<uint32_t>(chunk);
         unsigned long long *off = ds.n<unsigned long long>(chunk);
@@ -643,7 +661,7 @@ int kc_dump_text(const uint64_t *keys, const uint32_t *counts, uint64_t n, uint3
         uint64_t pos = 0;
         for (uint64_t c0 = 0; c0 < n; c0 += chunk) {
             const uint64_t m = std::min(chunk, n - c0);
-            CK(cudaMemcpyAsync(dk, keys + c0, m * 8, cudaMemcpyHostToDevice, sg.st));
+            CK(cudaMemcpyAsync(dk, keys + c0 * nw, m * nw * 8, cudaMemcpyHostToDevice, sg.st));
             CK(cudaMemcpyAsync(dc, counts + c0, m * 4, cudaMemcpyHostToDevice, sg.st));
             CK(launch_dump_text(dk, dc, m, k, len, off, tmp, dtxt, sg.st));
             unsigned long long last_off = 0;

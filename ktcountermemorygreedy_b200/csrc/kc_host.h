@@ -161,19 +161,21 @@ bool is_gzip(const kc_buffer &b);
 uint64_t gzip_size_hint(const kc_buffer &b);
 std::vector<kc_buffer> inflate_inputs(const std::vector<kc_buffer> &files, std::vector<PinnedBlock> &hold);
 
-// (key, count) records of one job in a pinned block.
+// (key, count) records of one job in a pinned block; a key is `words`
+// 64-bit words (kmer<N>, N = 1, 2 or 4).
 struct HostRecords {
     void *block = nullptr;
     size_t bytes = 0;
     uint64_t n = 0;
+    uint32_t words = 1;
     HostRecords() = default;
     HostRecords(const HostRecords &) = delete;
     HostRecords &operator=(const HostRecords &) = delete;
-    void allocate(uint64_t count);
+    void allocate(uint64_t count, uint32_t key_words = 1);
     uint64_t *keys() const { return static_cast<uint64_t *>(block); }
     uint32_t *counts() const
     {
-        return reinterpret_cast<uint32_t *>(static_cast<uint8_t *>(block) + ((n * 8 + 255) & ~uint64_t(255)));
+        return reinterpret_cast<uint32_t *>(static_cast<uint8_t *>(block) + ((n * 8 * words + 255) & ~uint64_t(255)));
     }
     void reset();
     ~HostRecords() { reset(); }

@@ -41,6 +41,7 @@ enum Counter : int {
     C_SEL_B = 9,
     C_SUB_OVF = 10,      // sub-buckets whose shared-memory table overflowed
     C_REGION_OVF = 11,   // nonzero: a sub-bucket outgrew its estimated region
+    C_KEPT = 12,         // records a counting compaction pass would keep
     C_COUNT = 16
 };
 
@@ -354,7 +355,7 @@ cudaError_t launch_or_flags(unsigned long long *word, unsigned long long bits, c
 cudaError_t launch_hash_batch(const unsigned long long *keys, uint64_t n, unsigned long long *out,
                               cudaStream_t st);
 
-// "KMER\tcount\n" lines of n records (kmer<1> words, k <= 32) into out,
+// "KMER\tcount\n" lines of n records (kmer<N> keys of N words, k <= 128) into out,
 // packed; len (n), off (n) and scan_tmp (scan_tmp_words(n)) are scratch, and
 // off[n-1] + len[n-1] is the text's length.
 cudaError_t launch_dump_text(const unsigned long long *keys, const uint32_t *counts, uint64_t n, uint32_t k,

@@ -1,0 +1,80 @@
+// kc_wide.cuh -- k-mers of 33..128 bases: the reference's kmer<2> (k <= 64)
+// and kmer<4> (k <= 128) paths (src/main.cpp:617-633).
+//
+// A k-mer is its kmer<N> word array (src/kmer.h:15, data[0] first): the
+// newest base of the window at data[0]'s top bits, older bases towards
+// data[last] (last = (k - 1) / 32), whose low 64 - 2 * (k % 32) bits are
+// zero; words above data[last] are zero.  Records are N words + a u32 count,
+// the words of record i at keys[i * N .. i * N + N).
+#pragma once
+
+#include "kc_kernels.cuh"
+
+namespace kc {
+
+constexpr uint32_t WIDE_HALO = 128;   // bytes before a tile read with it: k - 1 <= 127
+
+inline uint32_t key_words(uint32_t k) { return k <= 32 ? 1u : (k <= 64 ? 2u : 4u); }
+
+// Open-addressing table of N-word keys.  A slot is claimed by one CAS of its
+// state (0 -> 1), its key written and then published (state 2, release);
+// every other thread compares keys only in published slots.  A thread that
+// meets a claimed, unpublished slot waits for it (bounded, ERR_WAIT_TIMEOUT).
+struct WideTable {
+    unsigned long long *keys;   // cap * N words, slot i at keys[i * N]
+    uint32_t *meta;             // 2 words per slot: state, count
+    unsigned long long cap;
+};
+
+enum WideMode : int { WMODE_SCAN = 0, WMODE_INSERT = 1, WMODE_EMIT = 2 };
+
+struct WideArgs {
+    const uint8_t *buf;               // first byte of tile 0 (FRONT_PAD >= WIDE_HALO zero bytes before it)
+    uint64_t n_tiles;
+    const uint64_t *tile_prefix;      // exclusive newline count before each tile
+    const uint32_t *tile_seg;
+    const Seg *segs;
+    unsigned long long *counters;     // C_COUNT words
+    // SCAN: occurrences, HyperLogLog registers (HLL_M), root-prefix histogram
+    unsigned long long *occ;
+    uint32_t *hll;
+    unsigned long long *bucket_hist;  // 256: occurrences per top byte of data[0]
+    // INSERT: the table; a pass keeps root prefixes lo <= b < hi (hi 0: all)
+    WideTable table;
+    uint32_t max_probe;
+    uint32_t bucket_lo, bucket_hi;
+    // EMIT: occurrences appended at list[C_EMIT_LEN * N], list_cap k-mers
+    unsigned long long *list;
+    unsigned long long list_cap;
+};
+
+cudaError_t launch_wide_extract(int mode, uint32_t k, const WideArgs &a, cudaStream_t st);
+cudaError_t launch_wide_init(WideTable t, cudaStream_t st);
+// (key, count) records into the table (the tools' merge: high.bin records
+// with their counts, low.bin k-mers with count 1).
+cudaError_t launch_wide_insert_pairs(uint32_t k, const unsigned long long *keys, const uint32_t *counts,
+                                     uint32_t count_if_null, uint64_t n, WideTable t, uint32_t max_probe,
+                                     unsigned long long *counters, cudaStream_t st);
+// Published slots: *kept = slots whose saturated count is in [min, max],
+// counters[C_DISTINCT] += published slots.  count_only = 1 writes nothing
+// else; 0 appends the kept records at rec_keys / rec_counts (C_REC_LEN, at
+// most rec_cap) and adds every slot's count to hist / ovf.
+cudaError_t launch_wide_compact(uint32_t k, WideTable t, uint32_t count_max, uint32_t min_count, uint32_t max_count,
+                                unsigned long long *rec_keys, uint32_t *rec_counts, uint64_t rec_cap,
+                                unsigned long long *hist, uint32_t *ovf, uint64_t ovf_cap,
+                                unsigned long long *counters, int count_only, cudaStream_t st);
+// Sort of n records in printed-string order: LSD by words (data[0] first,
+// each a stable radix sort of its pair-reversed word, data[last] on its
+// 2 * (k % 32) bits), then the records permuted into out_keys / out_counts.
+// tmp holds wide_sort_tmp_bytes(n) bytes.
+size_t wide_sort_tmp_bytes(uint64_t n);
+cudaError_t launch_wide_sort(uint32_t k, const unsigned long long *keys, const uint32_t *counts, uint64_t n,
+                             unsigned long long *out_keys, uint32_t *out_counts, void *tmp,
+                             unsigned long long *flags, cudaStream_t st);
+// out rows i = keys rows idx[i] (idx: record positions as 64-bit words).
+cudaError_t launch_wide_gather_rows(uint32_t k, const unsigned long long *keys, const unsigned long long *idx,
+                                    uint64_t n, unsigned long long *out, cudaStream_t st);
+// 0, 1, 2, ... n - 1
+cudaError_t launch_iota_u64(unsigned long long *p, uint64_t n, cudaStream_t st);
+
+}  // namespace kc

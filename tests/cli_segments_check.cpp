@@ -2,10 +2,11 @@
 // (ktcountermemorygreedy_b200/cli/cli_common.h): no library call, no GPU.
 //   cli_segments_check <tmp_dir> <budget_bytes> <dump 0|1> <with_low 0|1> <out_dir>
 // writes to out_dir:
-//   all_high.bin   u64 key, u32 count per record as read_tmpdir decodes high.bin
-//   all_low.bin    u64 key per low.bin k-mer as read_tmpdir decodes it
-//   seg_high.bin   u64 key, u32 count, u32 segment for every record load_segment returns
-//   seg_low.bin    u64 key, u32 segment (with_low)
+//   all_high.bin   key words (N u64), u32 count per record as read_tmpdir decodes high.bin
+//   all_low.bin    key words per low.bin k-mer as read_tmpdir decodes it
+//   seg_high.bin   key words, u32 count, u32 segment for every record load_segment returns
+//   seg_low.bin    key words, u32 segment (with_low)
+// (N = 1, 2 or 4 words per key by k)
 //   plan.txt       "ok <n> <fixed> <per_high> <per_low>" then "p0 p1 n_high n_low" per segment,
 //                  or "nofit <worst>"
 #include <cstdio>
@@ -25,13 +26,13 @@ int main(int argc, char **argv)
     cli::TmpDir t;
     if (!cli::read_tmpdir(dir, t, err)) { std::fprintf(stderr, "%s\n", err.c_str()); return 2; }
     FILE *f = std::fopen((out + "all_high.bin").c_str(), "wb");
-    for (size_t i = 0; i < t.high_keys.size(); ++i) {
-        std::fwrite(&t.high_keys[i], 8, 1, f);
+    for (size_t i = 0; i < t.high_counts.size(); ++i) {
+        std::fwrite(&t.high_keys[i * t.nw], 8, t.nw, f);
         std::fwrite(&t.high_counts[i], 4, 1, f);
     }
     std::fclose(f);
     f = std::fopen((out + "all_low.bin").c_str(), "wb");
-    for (uint64_t w : t.low_keys) std::fwrite(&w, 8, 1, f);
+    if (!t.low_keys.empty()) std::fwrite(t.low_keys.data(), 8, t.low_keys.size(), f);
     std::fclose(f);
 
     cli::Layout L;
@@ -58,13 +59,13 @@ int main(int argc, char **argv)
         const cli::Segment &s = segs[si];
         std::fprintf(plan, "%u %u %llu %llu\n", s.p0, s.p1, (unsigned long long)s.n_high, (unsigned long long)s.n_low);
         if (!cli::load_segment(dir, L, with_low, s, hk, hc, lk, err)) { std::fprintf(stderr, "%s\n", err.c_str()); return 5; }
-        for (size_t i = 0; i < hk.size(); ++i) {
-            std::fwrite(&hk[i], 8, 1, sh);
+        for (size_t i = 0; i < hc.size(); ++i) {
+            std::fwrite(&hk[i * L.nw], 8, L.nw, sh);
             std::fwrite(&hc[i], 4, 1, sh);
             std::fwrite(&si, 4, 1, sh);
         }
-        for (uint64_t w : lk) {
-            std::fwrite(&w, 8, 1, sl);
+        for (size_t i = 0; i < lk.size() / L.nw; ++i) {
+            std::fwrite(&lk[i * L.nw], 8, L.nw, sl);
             std::fwrite(&si, 4, 1, sl);
         }
     }

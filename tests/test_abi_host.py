@@ -126,8 +126,8 @@ def test_cli_argument_validation():
     assert _run([kmc, "x.fq", "31", "8", "1", "/tmp", "1024", "2", "9", "0"]).returncode == 1   # count_max 0
     # map_capacity is rounded up to a power of two before the 16M limit (src/main.cpp:541, :581)
     assert _run([kmc, "x.fq", "31", "8", "1", "/tmp", "9000000"]).returncode == 1
-    r = _run([kmc, "x.fq", "40", "8", "1", "/tmp"])
-    assert r.returncode == 1 and "above 32" in r.stderr
+    r = _run([kmc, "x.fq", "129", "8", "1", "/tmp"])
+    assert r.returncode == 1 and "k_len must be <= 128" in r.stderr   # src/main.cpp:629-632
     # infos.bin is written before any input is read (src/main.cpp:588-595)
     r = _run([kmc, "x.fq", "31", "8", "1", "/nonexistent_dir"])
     assert r.returncode == 1 and "Open infos.bin failed" in r.stderr

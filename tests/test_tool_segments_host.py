@@ -30,11 +30,21 @@ def key_bytes(k):
     return 8 * (k // 32) + (2 * (k % 32) + 7) // 8
 
 
+def key_words(k):
+    return 1 if k <= 32 else (2 if k <= 64 else 4)
+
+
 def pack_keys(words, k):
-    """The reference's k-mer packing (src/FinalDrainWriter.h:71-88): full
-    words, then the last word's top tail bytes, little-endian."""
-    b = words.astype("<u8").view(np.uint8).reshape(-1, 8)
-    return b if k // 32 else b[:, 8 - key_bytes(k):]
+    """The reference's k-mer packing (src/FinalDrainWriter.h:71-88): the full
+    words, then the top tail bytes of the next word, little-endian."""
+    words = words.reshape(len(words), key_words(k))
+    b = words.astype("<u8").view(np.uint8).reshape(len(words), 8 * key_words(k))
+    full, kb = k // 32, key_bytes(k)
+    tail = kb - 8 * full
+    parts = [b[:, : 8 * full]]
+    if tail:
+        parts.append(b[:, 8 * full + 8 - tail: 8 * full + 8])
+    return np.concatenate(parts, axis=1)
 
 
 def write_tmpdir(d, k, count_max, hk, hc, lk):
@@ -46,30 +56,47 @@ def write_tmpdir(d, k, count_max, hk, hc, lk):
     pack_keys(lk, k).tofile(os.path.join(d, "low.bin"))
 
 
+def base_pos(k, i):
+    """(word, bit) of base i of the printed k-mer (kmer_to_buf, tool/dump_tool.cpp:103-124)."""
+    if k <= 32:
+        return 0, 64 - 2 * k + 2 * i
+    full, tail = k // 32, k % 32
+    if i < tail:
+        return full, 64 - 2 * tail + 2 * i
+    off = i - tail
+    return full - 1 - off // 32, 2 * (off % 32)
+
+
 def random_words(rng, n, k, lead_zero=0):
-    """k-mer words (base i at bit 64-2k+2i, low padding zero); lead_zero > 0
-    makes the first bases A, so many k-mers share one lead prefix."""
-    w = rng.integers(0, 1 << 62, size=n, dtype=np.uint64) * np.uint64(4) + rng.integers(0, 4, size=n, dtype=np.uint64)
-    pad = 64 - 2 * k
-    if pad:
-        w = (w >> np.uint64(pad)) << np.uint64(pad)
-    if lead_zero:
-        w &= ~np.uint64(((1 << (2 * lead_zero)) - 1) << pad)
+    """kmer<N> word arrays, shape (n, N) (N = 1 for k <= 32): every base
+    random, every other bit zero; lead_zero > 0 makes the first bases A, so
+    many k-mers share one lead prefix."""
+    w = np.zeros((n, key_words(k)), np.uint64)
+    for i in range(k):
+        if i < lead_zero:
+            continue
+        wi, sh = base_pos(k, i)
+        w[:, wi] |= rng.integers(0, 4, size=n, dtype=np.uint64) << np.uint64(sh)
     return w
 
 
 def string_value(w, k):
     """The printed k-mer as a base-4 number (base 0 most significant)."""
+    w = w.reshape(len(w), -1)
     v = np.zeros(len(w), dtype=object)
-    s0 = 64 - 2 * k
     for i in range(k):
-        v = v * 4 + ((w >> np.uint64(s0 + 2 * i)) & np.uint64(3)).astype(object)
+        wi, sh = base_pos(k, i)
+        v = v * 4 + ((w[:, wi] >> np.uint64(sh)) & np.uint64(3)).astype(object)
     return v
 
 
 def lead(w, k):
     m = min(k, 8)
     return np.array([int(x) >> (2 * (k - m)) for x in string_value(w, k)], dtype=np.int64), m
+
+
+def rows(a):
+    return [tuple(r) for r in a.reshape(len(a), -1).tolist()]
 
 
 def make_case(k, count_max, seed):
@@ -88,7 +115,8 @@ def run_checker(exe, d, out, budget, dump, with_low):
 
 
 CASES = [(31, U32, True, True), (21, 255, False, True), (5, 0xFFFF, True, False), (32, 0xFFFFFF, False, False),
-         (13, U32, True, True)]
+         (13, U32, True, True), (33, U32, True, True), (64, 255, False, True), (70, U32, True, False),
+         (128, 0xFFFF, True, True)]
 
 
 @pytest.mark.parametrize("k,count_max,dump,with_low", CASES)
@@ -107,9 +135,10 @@ def test_segments_cover_every_record_in_printed_string_order(checker, tmp_path, 
     lines = run_checker(checker, d, out, budget, dump, with_low)
 
     # high.bin / low.bin decoded as packed
-    ah = np.fromfile(os.path.join(out, "all_high.bin"), np.dtype([("k", "<u8"), ("c", "<u4")]))
-    assert np.array_equal(ah["k"], hk) and np.array_equal(ah["c"], hc)
-    assert np.array_equal(np.fromfile(os.path.join(out, "all_low.bin"), "<u8"), lk)
+    nw = key_words(k)
+    ah = np.fromfile(os.path.join(out, "all_high.bin"), np.dtype([("k", "<u8", (nw,)), ("c", "<u4")]))
+    assert np.array_equal(ah["k"].reshape(-1, nw), hk) and np.array_equal(ah["c"], hc)
+    assert np.array_equal(np.fromfile(os.path.join(out, "all_low.bin"), "<u8").reshape(-1, nw), lk)
 
     head = lines[0].split()
     assert head[0] == "ok"
@@ -120,12 +149,12 @@ def test_segments_cover_every_record_in_printed_string_order(checker, tmp_path, 
     # contiguous ranges over every lead prefix
     assert segs[0][0] == 0 and segs[-1][1] == 4 ** m
     assert all(a[1] == b[0] for a, b in zip(segs, segs[1:]))
-    sh = np.fromfile(os.path.join(out, "seg_high.bin"), np.dtype([("k", "<u8"), ("c", "<u4"), ("s", "<u4")]))
-    sl = np.fromfile(os.path.join(out, "seg_low.bin"), np.dtype([("k", "<u8"), ("s", "<u4")]))
+    sh = np.fromfile(os.path.join(out, "seg_high.bin"), np.dtype([("k", "<u8", (nw,)), ("c", "<u4"), ("s", "<u4")]))
+    sl = np.fromfile(os.path.join(out, "seg_low.bin"), np.dtype([("k", "<u8", (nw,)), ("s", "<u4")]))
     # every record exactly once, in the segment of its lead prefix
-    assert sorted(zip(sh["k"].tolist(), sh["c"].tolist())) == sorted(zip(hk.tolist(), hc.tolist()))
+    assert sorted(zip(rows(sh["k"]), sh["c"].tolist())) == sorted(zip(rows(hk), hc.tolist()))
     if with_low:
-        assert sorted(sl["k"].tolist()) == sorted(lk.tolist())
+        assert sorted(rows(sl["k"])) == sorted(rows(lk))
     else:
         assert len(sl) == 0
     p0 = np.array([s[0] for s in segs])
@@ -180,6 +209,6 @@ def test_no_plan_below_the_fixed_need_or_for_a_crowded_prefix(checker, tmp_path)
 
 def test_errors_match_read_tmpdir(checker, tmp_path):
     d = str(tmp_path / "t")
-    write_tmpdir(d, 31, U32, np.zeros(0, np.uint64), np.zeros(0, np.uint32), np.zeros(0, np.uint64))
+    write_tmpdir(d, 31, U32, np.zeros((0, 1), np.uint64), np.zeros(0, np.uint32), np.zeros((0, 1), np.uint64))
     p = subprocess.run([checker, d, "1000000", "1", "1", str(tmp_path)], capture_output=True, text=True)
     assert p.returncode == 2 and "empty high.bin file" in p.stderr
