@@ -226,6 +226,11 @@ struct kc_handle {
     uint32_t workers_n = 1;
     uint64_t reserved = 0;
     uint32_t running = 0;
+    // a job larger than one worker's share of the budget runs alone: it is
+    // admitted when nothing else runs, the idle workers give their kept
+    // workspaces back first, and nothing else starts until it ends
+    bool exclusive = false;
+    std::vector<kc::Workspace *> spaces;   // every worker's workspace (guarded by mu)
     bool closing = false;
     kc_job_id next_id = 1;
     std::mutex mu;
@@ -1987,19 +1992,34 @@ void worker_main(kc_handle *h)
     // worker while the others need it
     if (h->workers_n > 1 && !h->workspace_bytes) ws->set_max_keep(h->budget / h->workers_n);
     if (h->workspace_bytes) ws->reserve(h->workspace_bytes);
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        h->spaces.push_back(ws.get());
+    }
+    const uint64_t share = h->workers_n > 1 ? h->budget / h->workers_n : UINT64_MAX;
     for (;;) {
         std::shared_ptr<Task> task;
+        bool alone = false;
         {
             std::unique_lock<std::mutex> lk(h->mu);
             h->cv_work.wait(lk, [&] {
                 if (h->closing) return true;
-                if (h->queue.empty()) return false;
+                if (h->queue.empty() || h->exclusive) return false;
                 const auto &f = h->queue.front();
+                if (f->reserve > share) return h->running == 0;
                 return h->running == 0 || h->reserved + f->reserve <= h->budget;
             });
             if (h->closing) break;
             task = h->queue.front();
             h->queue.pop_front();
+            alone = task->reserve > share;
+            if (alone) {
+                // the other workers are idle (nothing runs): their kept
+                // blocks go back to the device for this job's passes
+                h->exclusive = true;
+                for (Workspace *o : h->spaces)
+                    if (o != ws.get()) o->trim();
+            }
             h->reserved += task->reserve;
             h->running++;
             task->tuning = h->tuning;
@@ -2039,9 +2059,14 @@ void worker_main(kc_handle *h)
             }
             h->reserved -= task->reserve;
             h->running--;
+            if (alone) h->exclusive = false;
         }
         h->cv_work.notify_all();
         h->cv_done.notify_all();
+    }
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        h->spaces.erase(std::find(h->spaces.begin(), h->spaces.end(), ws.get()));
     }
     ws.reset();
     cudaStreamDestroy(st);

@@ -135,6 +135,15 @@ void Workspace::end_job()
     top_ = 0;
 }
 
+void Workspace::trim()
+{
+    end_job();
+    cudaStreamSynchronize(st_);
+    if (base_) cudaFree(base_);
+    base_ = nullptr;
+    cap_ = 0;
+}
+
 Workspace::~Workspace()
 {
     end_job();

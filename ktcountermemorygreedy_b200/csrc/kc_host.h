@@ -62,6 +62,9 @@ public:
     // that needs more takes the rest from the stream-ordered pool, which the
     // other workers of a handle share
     void set_max_keep(size_t bytes) { max_keep_ = bytes; }
+    // gives the kept block back to the device between jobs (the next job
+    // grows it again to the high-water mark)
+    void trim();
 
 private:
     cudaStream_t st_;

@@ -54,30 +54,51 @@ def string_keys(words: np.ndarray) -> np.ndarray:
     return x.byteswap()
 
 
+CHUNK = 1 << 26   # records per step of the checks below (a few GB of temporaries at most)
+
+
 def full_spot_check(fq: np.ndarray, k: int, keys: np.ndarray, counts: np.ndarray, hist: np.ndarray,
                     hist_min: int, min_count: int, threads: int = 8, sample_bits: int = 6) -> dict:
     """Checks a job's records (kmer<1> words in printed-string order, exact
     counts >= min_count) and histogram (bins hist_min..) against the oracle
-    on the 2^-sample_bits hash sample of the k-mers of the FASTQ `fq`."""
+    on the 2^-sample_bits hash sample of the k-mers of the FASTQ `fq`.  The
+    records are read in chunks, so that a job of billions of records is
+    checked in bounded host memory."""
     t0 = time.perf_counter()
     occ = O.extract_sampled(fq, k, sample_bits, record_splits(fq, 4 * threads), threads)
     uk, uc = O.count(occ)
+    n_occ = len(occ)
+    del occ
     m = uc >= min_count
     want_k, want_c = O.sort_string_order(uk[m], uc[m], k)
     keys = np.asarray(keys)
     counts = np.asarray(counts)
-    sel = O.sampled_mask(keys, sample_bits)
-    got_k, got_c = keys[sel], counts[sel]
-    same = bool(np.array_equal(got_k, want_k) and np.array_equal(got_c, want_c))
-    sk = string_keys(keys)
-    ordered = bool(len(sk) < 2 or np.all(sk[1:] > sk[:-1]))
+    n = len(keys)
+    got_k, got_c = [], []
+    ordered = True
+    prev = None
     hmax = hist_min + len(hist) - 1
-    c = counts[(counts >= hist_min) & (counts <= hmax)].astype(np.int64)
-    hist_ok = bool(np.array_equal(np.bincount(c - hist_min, minlength=len(hist)), np.asarray(hist)))
+    rec_hist = np.zeros(len(hist), np.int64)
+    for a in range(0, n, CHUNK):
+        kc_, cc = keys[a:a + CHUNK], counts[a:a + CHUNK]
+        sel = O.sampled_mask(kc_, sample_bits)
+        got_k.append(kc_[sel])
+        got_c.append(cc[sel])
+        sk = string_keys(kc_)
+        ordered = ordered and bool(np.all(sk[1:] > sk[:-1])) and (prev is None or len(sk) == 0 or sk[0] > prev)
+        if len(sk):
+            prev = sk[-1]
+        del sk
+        c = cc[(cc >= hist_min) & (cc <= hmax)]
+        rec_hist += np.bincount(c - np.uint32(hist_min), minlength=len(hist))[: len(hist)]
+    got_k = np.concatenate(got_k) if got_k else np.zeros(0, np.uint64)
+    got_c = np.concatenate(got_c) if got_c else np.zeros(0, np.uint32)
+    same = bool(np.array_equal(got_k, want_k) and np.array_equal(got_c, want_c))
+    hist_ok = bool(np.array_equal(rec_hist, np.asarray(hist)))
     return {
         "identical": same and ordered and hist_ok,
         "sampled_records_identical": same, "records_sorted": ordered, "hist_equals_records_hist": hist_ok,
-        "sampled_kmers": int(len(want_k)), "sampled_occurrences": int(len(occ)), "records": int(len(keys)),
+        "sampled_kmers": int(len(want_k)), "sampled_occurrences": int(n_occ), "records": int(n),
         "how": f"oracle (C restatement) on the whole FASTQ, {threads} threads, keeping the k-mers whose "
                f"splitmix64 hash is 0 mod {1 << sample_bits} (all their occurrences): their exact counts "
                f">= {min_count} equal the job's records of those k-mers; every record in strictly "
