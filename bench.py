@@ -633,6 +633,36 @@ def batched_bench(kc, args, local):
             "speedup_vs_plain": t_p / t_b, "identical_to_plain": bool(same), "tuning": tuning}
 
 
+def wide_bench(kc, args, counter, inp, fq):
+    """k-mers of more than 32 bases (the reference's kmer<2>/kmer<4> paths)
+    on the same resident workload and job settings (Bloom flag, min count 2):
+    device k-mers/s over 3 timed jobs after one warm-up, then one job with
+    records whose hash sample is checked against the oracle (CPU leg)."""
+    out = {}
+    for k in args.wide:
+        job = dict(JOB, k=k)
+        counter.count(input=inp, keep_records=False, **job)
+        rs = [counter.count(input=inp, keep_records=False, **job) for _ in range(3)]
+        dev = sum(r.device_ms for r in rs) / len(rs)
+        r0 = rs[-1]
+        o = {"k": k, "key_words": kc.key_words(k), "occurrences": r0.occurrences, "device_ms": dev,
+             "kmers_per_s": r0.occurrences / (dev / 1000.0), "records": r0.n_records_total, "passes": r0.passes,
+             "stages_ms": {kc.PHASES[i]: r0.phase_ms[i] for i in range(len(kc.PHASES)) if r0.phase_ms[i] > 0}}
+        if args.cpu_baseline:
+            try:
+                r = counter.count(input=inp, keep_records=True, copy=False, **job)
+                threads, _ = cpu_info()
+                chk = _checker().full_spot_check_wide(fq, k, r.keys, r.counts, r.hist, JOB["hist_min"],
+                                                      JOB["min_count"], threads=max(1, threads), sample_bits=8)
+                o["parity"] = "identical" if chk["identical"] else "DIFFERENT"
+                o["parity_detail"] = chk
+                del r
+            except Exception as e:
+                o["parity"] = f"failed: {e}"
+        out[str(k)] = o
+    return out
+
+
 def out_of_core_bench(kc, args, local):
     """Out-of-core single job: a seeded 3.1 Gbp genome with 45% repeats
     (2000 families of 0.3-6 kbp, 1-10^5 copies, 1-15% divergence), 10x of
@@ -806,6 +836,7 @@ def run_ours(args):
     if rank == 0 and world == 1 and args.cpu_baseline:
         cpu, parity, sample_value = cpu_leg(args, counter, fq, last_full)
     last_full = None
+    wide = wide_bench(kc, args, counter, inp, fq) if (rank == 0 and world == 1 and args.wide) else None
     counter.free_input(inp)
     counter.close()
     kc.lib().kc_host_free(pinned)
@@ -831,6 +862,7 @@ def run_ours(args):
             "roofline": roof, "cpu_baseline": cpu, "sample_value": sample_value, "parity": parity,
             "clocks": clocks, "gpu_launches": int(launches),
             "stages": stages, "atomics": atomics, "served": served, "batched": batched, "out_of_core": ooc,
+            "wide": wide,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -857,6 +889,8 @@ def main():
     ap.add_argument("--no-batched", dest="batched", action="store_false")
     ap.add_argument("--batch-samples", type=int, default=256)
     ap.add_argument("--batch-scale", type=float, default=0.125)
+    ap.add_argument("--wide", type=int, nargs="*", default=[],
+                    help="also time k-mers of more than 32 bases (e.g. 63 127) on the same workload")
     ap.add_argument("--out-of-core", action="store_true",
                     help="also run the out-of-core job (3.1 Gbp, 10x, 65 GB FASTQ; minutes, host memory ~100 GB)")
     ap.add_argument("--ooc-scale", type=float, default=1.0, help="genome size factor of the out-of-core job")

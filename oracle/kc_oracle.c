@@ -207,6 +207,35 @@ uint64_t kco_extract_wide(const uint8_t *data, uint64_t len, uint32_t k, uint64_
     return n;
 }
 
+/* Spot-check sample of N-word k-mers: the sample hash folded over the
+ * words (data[0] first); every occurrence of a kept k-mer is kept. */
+uint64_t kco_sample_hash_wide(const uint64_t *words, uint32_t n_words)
+{
+    uint64_t h = kco_sample_hash(words[0]);
+    for (uint32_t i = 1; i < n_words; ++i) h = kco_sample_hash(h ^ words[i]);
+    return h;
+}
+
+uint64_t kco_extract_wide_sampled(const uint8_t *data, uint64_t len, uint32_t k, uint32_t sample_bits,
+                                  uint64_t *out, uint64_t cap)
+{
+    const uint64_t smask = sample_bits >= 64 ? ~0ULL : ((1ULL << sample_bits) - 1ULL);
+    wroll_t r;
+    wroll_init(&r, k);
+    const uint32_t nw = r.nw;
+    uint64_t line = 0, n = 0, canon[4];
+    for (uint64_t i = 0; i < len; ++i) {
+        const uint8_t c = data[i];
+        if (c == '\n') { line++; wroll_clear(&r); continue; }
+        if ((line & 3) != 1) continue;
+        if (wroll_push(&r, c, canon) && (kco_sample_hash_wide(canon, nw) & smask) == 0) {
+            if (n < cap) memcpy(out + n * nw, canon, nw * 8);
+            n++;
+        }
+    }
+    return n;
+}
+
 /* Printed-string order key of an N-word k-mer: the 2-bit groups of the whole
  * word array reversed (the first base most significant), as N words, most
  * significant first.  Base i of the printed string is extracted as

@@ -38,6 +38,11 @@ uint64_t kco_extract(const uint8_t *data, uint64_t len, uint32_t k,
  * leaves stale bases in data[3] at k = 96; see kc_oracle.c). */
 uint32_t kco_key_words(uint32_t k);
 uint64_t kco_extract_wide(const uint8_t *data, uint64_t len, uint32_t k, uint64_t *out, uint64_t cap);
+/* Hash-sampled extraction of N-word k-mers (kco_extract_sampled's rule with
+ * the sample hash folded over the words). */
+uint64_t kco_sample_hash_wide(const uint64_t *words, uint32_t n_words);
+uint64_t kco_extract_wide_sampled(const uint8_t *data, uint64_t len, uint32_t k, uint32_t sample_bits,
+                                  uint64_t *out, uint64_t cap);
 /* Printed-string order key of one k-mer: N words, most significant first. */
 void kco_string_key_wide(const uint64_t *words, uint32_t k, uint64_t *out);
 

@@ -27,6 +27,8 @@ def lib():
             "kco_key_words": (u32, [u32]),
             "kco_extract_wide": (u64, [vp, u64, u32, vp, u64]),
             "kco_string_key_wide": (None, [vp, u32, vp]),
+            "kco_sample_hash_wide": (u64, [vp, u32]),
+            "kco_extract_wide_sampled": (u64, [vp, u64, u32, u32, vp, u64]),
             "kco_sample_hash": (u64, [u64]),
             "kco_extract_sampled": (u64, [vp, u64, u32, u32, vp, u64]),
             "kco_prepass": (None, [vp, u64, u32, u64, vp, U64P, U64P]),
@@ -176,6 +178,39 @@ def extract_sampled(buf: np.ndarray, k: int, sample_bits: int, splits=None, thre
     with cf.ThreadPoolExecutor(max_workers=max(1, threads)) as ex:
         parts = list(ex.map(one, range(len(bounds) - 1)))
     return np.concatenate(parts) if parts else np.zeros(0, np.uint64)
+
+
+def sample_hash_wide_np(keys: np.ndarray) -> np.ndarray:
+    """kco_sample_hash_wide of every row of (n, N) word arrays."""
+    keys = np.ascontiguousarray(keys, np.uint64)
+    h = sample_hash_np(keys[:, 0])
+    for i in range(1, keys.shape[1]):
+        h = sample_hash_np(h ^ keys[:, i])
+    return h
+
+
+def extract_wide_sampled(buf: np.ndarray, k: int, sample_bits: int, splits=None, threads: int = 1) -> np.ndarray:
+    """extract_sampled for N-word k-mers: rows of the sampled occurrences."""
+    import concurrent.futures as cf
+    nw = key_words(k)
+    buf = np.ascontiguousarray(buf, np.uint8)
+    bounds = [0] + [int(x) for x in (splits or []) if 0 < int(x) < len(buf)] + [len(buf)]
+    L = lib()
+    base = buf.ctypes.data
+
+    def one(i):
+        a, b = bounds[i], bounds[i + 1]
+        cap = max(1024, ((b - a) >> max(0, sample_bits - 2)) + 4096)
+        while True:
+            out = np.zeros(cap * nw, np.uint64)
+            n = L.kco_extract_wide_sampled(C.c_void_p(base + a), b - a, k, sample_bits, P(out), cap)
+            if n <= cap:
+                return out[: n * nw].reshape(n, nw)
+            cap = int(n)
+
+    with cf.ThreadPoolExecutor(max_workers=max(1, threads)) as ex:
+        parts = list(ex.map(one, range(len(bounds) - 1)))
+    return np.concatenate(parts) if parts else np.zeros((0, nw), np.uint64)
 
 
 def extract_files(files, k):

@@ -107,6 +107,60 @@ def full_spot_check(fq: np.ndarray, k: int, keys: np.ndarray, counts: np.ndarray
     }
 
 
+def full_spot_check_wide(fq: np.ndarray, k: int, keys: np.ndarray, counts: np.ndarray, hist: np.ndarray,
+                         hist_min: int, min_count: int, threads: int = 8, sample_bits: int = 6) -> dict:
+    """full_spot_check for k-mers of 33..128 bases: records are (n, N) kmer<N>
+    word arrays in printed-string order."""
+    t0 = time.perf_counter()
+    occ = O.extract_wide_sampled(fq, k, sample_bits, record_splits(fq, 4 * threads), threads)
+    uk, uc = O.count_wide(occ)
+    n_occ = len(occ)
+    del occ
+    m = uc >= min_count
+    want_k, want_c = O.sort_string_order_wide(uk[m], uc[m], k)
+    keys = np.asarray(keys)
+    counts = np.asarray(counts)
+    n = len(counts)
+    smask = np.uint64((1 << sample_bits) - 1)
+    got_k, got_c = [], []
+    ordered, prev = True, None
+    hmax = hist_min + len(hist) - 1
+    rec_hist = np.zeros(len(hist), np.int64)
+    for a in range(0, n, CHUNK // 4):
+        kc_, cc = keys[a:a + CHUNK // 4], counts[a:a + CHUNK // 4]
+        sel = (O.sample_hash_wide_np(kc_) & smask) == 0
+        got_k.append(kc_[sel])
+        got_c.append(cc[sel])
+        sk = O.string_keys_wide(kc_, k)
+        if len(sk):
+            # strictly increasing rows: the first differing word decides
+            cmp = np.zeros(len(sk) - 1, np.int8)
+            for w in range(sk.shape[1]):
+                und = cmp == 0
+                cmp[und & (sk[1:, w] > sk[:-1, w])] = 1
+                cmp[und & (sk[1:, w] < sk[:-1, w])] = -1
+            ordered = ordered and bool(np.all(cmp == 1))
+            if prev is not None:
+                ordered = ordered and tuple(sk[0].tolist()) > prev
+            prev = tuple(sk[-1].tolist())
+        c = cc[(cc >= hist_min) & (cc <= hmax)]
+        rec_hist += np.bincount(c - np.uint32(hist_min), minlength=len(hist))[: len(hist)]
+    got_k = np.concatenate(got_k) if got_k else np.zeros((0, keys.shape[1]), np.uint64)
+    got_c = np.concatenate(got_c) if got_c else np.zeros(0, np.uint32)
+    same = bool(np.array_equal(got_k, want_k) and np.array_equal(got_c, want_c))
+    hist_ok = bool(np.array_equal(rec_hist, np.asarray(hist)))
+    return {
+        "identical": same and ordered and hist_ok,
+        "sampled_records_identical": same, "records_sorted": ordered, "hist_equals_records_hist": hist_ok,
+        "sampled_kmers": int(len(want_k)), "sampled_occurrences": int(n_occ), "records": int(n),
+        "how": f"oracle (C restatement of GetKmer<N>) on the whole FASTQ, {threads} threads, keeping the k-mers "
+               f"whose word-folded splitmix64 hash is 0 mod {1 << sample_bits}: their exact counts >= "
+               f"{min_count} equal the job's records of those k-mers; records in strictly increasing "
+               f"printed-string order; the job's histogram equals its records' histogram",
+        "check_s": round(time.perf_counter() - t0, 2),
+    }
+
+
 def filtered_dump(path: str, k: int, min_count: int) -> bytes:
     """The reference's `dump_tool precise ... 1 <max> --sort` text with the
     lines whose count is below min_count removed."""
