@@ -2378,7 +2378,7 @@ int kc_result(kc_handle *h, kc_job_id id, kc_result_t *out)
     out->counts = j.recs.n ? j.recs.counts() : nullptr;
     out->hist_len = j.hist.size();
     out->hist = j.hist.data();
-    out->n_top = j.top_keys.size();
+    out->n_top = j.top_counts.size();   // top_keys holds key_words words per record
     out->top_keys = j.top_keys.data();
     out->top_counts = j.top_counts.data();
     out->n_le2 = j.le2.n;
