@@ -121,7 +121,11 @@ typedef struct {
                                      runs in passes over ranges of root prefixes, each pass's records
                                      held in pinned host memory until the final sort; 0 -> 70% of the
                                      device memory free for the job when its counting starts */
-    uint64_t reserved[5];
+    uint32_t pack_high;           /* 1: the job packs the high.bin records (src/FinalDrainWriter.h:71-101,
+                                     filter_min/filter_max applied) on the device, and kc_write_tmpdir
+                                     writes those bytes (keep_records may then be 0); single jobs */
+    uint32_t reserved_u32;
+    uint64_t reserved[4];
 } kc_job;
 
 typedef struct {
@@ -150,7 +154,7 @@ typedef struct {
      * histogram, [6] radix sort, [7] queries, [8] Bloom classification,
      * [9] scatter of the buckets into filter sub-buckets and [10] their
      * shared-memory Bloom split + count + compaction (Bloom mode, min count
-     * >= 2), [11] unused */
+     * >= 2), [11] packing of the high.bin records (kc_job.pack_high) */
     double phase_ms[KC_STAGES];
     uint64_t phase_launches[KC_STAGES];   /* kernel launches per stage */
     uint64_t low_len;             /* Bloom mode: FIRST occurrences (merged after the inserts) */

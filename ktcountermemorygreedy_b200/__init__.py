@@ -74,7 +74,7 @@ class kc_job(C.Structure):
                 ("min_count", C.c_uint32), ("max_count", C.c_uint32), ("hist_min", C.c_uint32),
                 ("hist_max", C.c_uint32), ("top_n", C.c_uint32), ("want_le2", C.c_uint32),
                 ("keep_records", C.c_uint32), ("fault_inject", C.c_uint32), ("pass_bytes", C.c_uint64),
-                ("reserved", C.c_uint64 * 5)]
+                ("pack_high", C.c_uint32), ("reserved_u32", C.c_uint32), ("reserved", C.c_uint64 * 4)]
 
 
 class kc_result_t(C.Structure):
@@ -92,7 +92,7 @@ class kc_result_t(C.Structure):
 
 # stage names of kc_result_t.phase_ms
 PHASES = ["census", "scan", "count_pass", "insert_high", "merge_low", "compact", "sort", "queries", "bloom",
-          "sub_partition", "smem_count", "stage11"]
+          "sub_partition", "smem_count", "pack_high"]
 
 
 # (name, restype, argtypes) of every symbol include/kc.h declares
@@ -308,7 +308,7 @@ class KmerCounter:
                  filter_min: int = 2, filter_max: int = U32_MAX, min_count: int = 1,
                  max_count: int = U32_MAX, hist_min: int = 1, hist_max: int = 10000, top_n: int = 0,
                  want_le2: bool = False, keep_records: bool = True, pass_bytes: int = 0,
-                 fault_inject: int = 0) -> kc_job:
+                 fault_inject: int = 0, pack_high: bool = False) -> kc_job:
         j = kc_job()
         lib().kc_job_defaults(C.byref(j))
         j.k, j.count_max, j.bloom, j.memory_gb = k, count_max, int(bloom), memory_gb
@@ -317,6 +317,7 @@ class KmerCounter:
         j.keep_records = int(keep_records)
         j.pass_bytes = pass_bytes
         j.fault_inject = fault_inject
+        j.pack_high = int(pack_high)
         return j
 
     def upload(self, files: Sequence[bytes]):

@@ -93,6 +93,9 @@ int main(int argc, char **argv)
     job.filter_max = fmax;
     const char *bl = std::getenv("KC_BLOOM");
     job.bloom = (bl && bl[0] == '1') ? 1 : 0;
+    // high.bin is packed on the device; the records themselves stay there
+    job.pack_high = 1;
+    job.keep_records = 0;
     kc_job_id id = 0;
     int rc = kc_submit(h, &job, &id);
     if (rc == KC_OK) rc = kc_wait(h, id, -1);
@@ -107,7 +110,7 @@ int main(int argc, char **argv)
     auto us = std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::steady_clock::now() - t0).count();
     std::cout << "Total read k-mer count: " << r.occurrences << std::endl;
     std::cout << "Total elapsed us: " << us << std::endl;
-    std::cout << "High frequency unique k-mer : " << r.n_records << std::endl;
+    std::cout << "High frequency unique k-mer : " << r.n_records_total << std::endl;
     kc_close(h);
     return 0;
 }

@@ -144,6 +144,9 @@ struct Job {
     std::vector<uint64_t> top_keys;
     std::vector<uint32_t> top_counts;
     HostRecords le2;   // records with count <= 2 (pinned: often most of the records)
+    PinnedBlock packed;        // kc_job.pack_high: high.bin bytes packed on the device
+    uint64_t packed_bytes = 0;
+    bool has_packed = false;
     uint64_t occurrences = 0, distinct = 0, low_only = 0, table_cap = 0;
     uint64_t low_len = 0, high_len = 0, input_bytes = 0, n_records_total = 0;
     uint32_t passes = 1, smem_passes = 0, smem_fallbacks = 0, region_redos = 0;
@@ -362,6 +365,33 @@ uint64_t default_pass_budget(Workspace &ws)
     }
     cudaGetLastError();
     return (uint64_t)(0.7 * (double)(free_b + ws_free + pool_slack));
+}
+
+// kc_job.pack_high: the high.bin bytes of the job's sorted records (k-mer
+// words, printed-string order) packed on the device and copied to pinned host
+// memory, for kc_write_tmpdir (stage [11]).
+void pack_high_on_device(Job &job, DevScope &ds, const unsigned long long *keys, const uint32_t *counts, uint64_t n,
+                         cudaStream_t st, PhaseClock &clk)
+{
+    const kc_job &P = job.p;
+    const uint32_t cb = P.count_max <= 0xFF ? 1 : P.count_max <= 0xFFFF ? 2 : P.count_max <= 0xFFFFFF ? 3 : 4;
+    const uint64_t rec = packed_record_bytes(P.k, cb);
+    const uint64_t m = std::max<uint64_t>(n, 1);
+    clk.begin(11);
+    uint32_t *flags = ds.n<uint32_t>(m);
+    unsigned long long *pos = ds.n<unsigned long long>(m);
+    unsigned long long *tmp = ds.n<unsigned long long>(scan_tmp_words(m));
+    uint8_t *out = ds.n<uint8_t>(m * rec);
+    unsigned long long *nb = ds.n<unsigned long long>(1);
+    CK(launch_pack_high(P.k, keys, counts, n, cb, P.filter_min, P.filter_max, flags, pos, tmp, out, nb, st));
+    clk.end();
+    unsigned long long hb = 0;
+    CK(cudaMemcpyAsync(&hb, nb, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    job.packed.reset(std::max<uint64_t>(hb, 1));
+    job.packed_bytes = hb;
+    if (hb) CK(cudaMemcpyAsync(job.packed.p, out, hb, cudaMemcpyDeviceToHost, st));
+    job.has_packed = true;
 }
 
 void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, const kc_tuning &tn)
@@ -1311,6 +1341,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
         }
         clk.end();
     }
+    if (P.pack_high) pack_high_on_device(job, ds, rec_keys, rec_counts, n_rec, st, clk);
     CK(cudaEventRecord(ev1, st));
 
     // ---- records to host ------------------------------------------------------
@@ -1670,6 +1701,7 @@ void run_wide_job(Job &job, cudaStream_t st, Workspace &ws, const kc_tuning &tn)
         }
         clk.end();
     }
+    if (P.pack_high) pack_high_on_device(job, ds, sk, sc, n_rec, st, clk);
     CK(cudaEventRecord(ev1, st));
 
     // ---- records to host ----------------------------------------------------------
@@ -2502,7 +2534,8 @@ extern "C" int kc_write_tmpdir(kc_handle *h, kc_job_id id, const char *dir)
         if (jp->state != JobState::DONE) return fail(KC_ERR_INVALID, "job not finished");
     }
     const Job &j = *jp;
-    if (!j.p.keep_records) return fail(KC_ERR_INVALID, "job was run without keep_records");
+    if (!j.p.keep_records && !j.has_packed)
+        return fail(KC_ERR_INVALID, "job was run without keep_records or pack_high");
     std::string d(dir);
     if (!d.empty() && d.back() != '/') d += '/';
     // infos.bin: u32 k, u32 count_max (src/main.cpp:590-597)
@@ -2523,6 +2556,16 @@ extern "C" int kc_write_tmpdir(kc_handle *h, kc_job_id id, const char *dir)
     const uint32_t rec = full * 8 + tail_bytes + cb;
     f = fopen((d + "high.bin").c_str(), "wb");
     if (!f) return fail(KC_ERR_IO, "cannot open " + d + "high.bin");
+    if (j.has_packed) {
+        // packed on the device (kc_job.pack_high)
+        ok = write_all(f, j.packed.p, j.packed_bytes);
+        ok = (fclose(f) == 0) && ok;
+        if (!ok) return fail(KC_ERR_IO, "write failed: high.bin");
+        f = fopen((d + "low.bin").c_str(), "wb");
+        if (!f) return fail(KC_ERR_IO, "cannot open " + d + "low.bin");
+        if (fclose(f) != 0) return fail(KC_ERR_IO, "write failed: low.bin");
+        return KC_OK;
+    }
     std::vector<uint8_t> buf;
     buf.reserve(std::min<size_t>(j.recs.n, 1 << 20) * rec);
     for (size_t i = 0; i < j.recs.n; ++i) {

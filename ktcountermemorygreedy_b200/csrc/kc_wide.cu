@@ -544,6 +544,42 @@ __global__ void k_wide_gather_rows(const unsigned long long *keys, const unsigne
 
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+__global__ void k_pack_flags(const uint32_t *counts, uint64_t n, uint32_t filter_min, uint32_t filter_max,
+                             uint32_t *flags)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = counts[i];
+        flags[i] = (c + 1 >= filter_min && c <= filter_max) ? 1u : 0u;
+    }
+}
+
+// One record per thread; consecutive threads write consecutive records, so a
+// warp's byte stores cover one contiguous run.
+template <uint32_t N>
+__global__ void k_pack_write(const unsigned long long *keys, const uint32_t *counts, const uint32_t *flags,
+                             const unsigned long long *pos, uint64_t n, uint32_t full, uint32_t tail_bytes,
+                             uint32_t count_bytes, uint8_t *out, unsigned long long *n_bytes)
+{
+    const uint32_t rec = full * 8 + tail_bytes + count_bytes;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (i == n - 1) *n_bytes = (pos[i] + flags[i]) * rec;
+        if (!flags[i]) continue;
+        uint8_t *o = out + pos[i] * rec;
+        uint32_t b = 0;
+        for (uint32_t w = 0; w < full; ++w) {
+            const uint64_t x = keys[i * N + w];
+#pragma unroll
+            for (uint32_t j = 0; j < 8; ++j) o[b++] = (uint8_t)(x >> (8 * j));
+        }
+        if (tail_bytes) {
+            const uint64_t x = keys[i * N + full];   // its low bits below the k-mer are zero
+            for (uint32_t j = 8 - tail_bytes; j < 8; ++j) o[b++] = (uint8_t)(x >> (8 * j));
+        }
+        const uint32_t c = counts[i];
+        for (uint32_t j = 0; j < count_bytes; ++j) o[b++] = (uint8_t)(c >> (8 * j));
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_wide_extract(int mode, uint32_t k, const WideArgs &a, cudaStream_t st)
@@ -643,6 +679,30 @@ cudaError_t launch_wide_gather_rows(uint32_t k, const unsigned long long *keys, 
     note_kernel_launch();
     if (key_words(k) == 2) k_wide_gather_rows<2><<<wide_grid(n, 256), 256, 0, st>>>(keys, idx, n, out);
     else k_wide_gather_rows<4><<<wide_grid(n, 256), 256, 0, st>>>(keys, idx, n, out);
+    return cudaGetLastError();
+}
+
+uint32_t packed_record_bytes(uint32_t k, uint32_t count_bytes)
+{
+    return (k / 32) * 8 + (2 * (k % 32) + 7) / 8 + count_bytes;
+}
+
+cudaError_t launch_pack_high(uint32_t k, const unsigned long long *keys, const uint32_t *counts, uint64_t n,
+                             uint32_t count_bytes, uint32_t filter_min, uint32_t filter_max, uint32_t *flags,
+                             unsigned long long *pos, unsigned long long *scan_tmp, uint8_t *out,
+                             unsigned long long *n_bytes, cudaStream_t st)
+{
+    if (!n) return cudaMemsetAsync(n_bytes, 0, 8, st);
+    const unsigned g = wide_grid(n, 256);
+    note_kernel_launch();
+    k_pack_flags<<<g, 256, 0, st>>>(counts, n, filter_min, filter_max, flags);
+    cudaError_t e = launch_scan_u32(flags, pos, n, scan_tmp, st);
+    if (e != cudaSuccess) return e;
+    const uint32_t full = k / 32, tail = (2 * (k % 32) + 7) / 8;
+    note_kernel_launch();
+    if (k <= 32) k_pack_write<1><<<g, 256, 0, st>>>(keys, counts, flags, pos, n, full, tail, count_bytes, out, n_bytes);
+    else if (k <= 64) k_pack_write<2><<<g, 256, 0, st>>>(keys, counts, flags, pos, n, full, tail, count_bytes, out, n_bytes);
+    else k_pack_write<4><<<g, 256, 0, st>>>(keys, counts, flags, pos, n, full, tail, count_bytes, out, n_bytes);
     return cudaGetLastError();
 }
 

@@ -77,4 +77,18 @@ cudaError_t launch_wide_gather_rows(uint32_t k, const unsigned long long *keys, 
 // 0, 1, 2, ... n - 1
 cudaError_t launch_iota_u64(unsigned long long *p, uint64_t n, cudaStream_t st);
 
+// high.bin bytes of sorted records (src/FinalDrainWriter.h:71-88): for each
+// record whose count c has c + 1 >= filter_min and c <= filter_max
+// (src/FinalDrainWriter.h:101), the k / 32 full words (little-endian), the
+// top (2 * (k % 32) + 7) / 8 bytes of the next word, the count's low
+// count_bytes bytes, written in record order.  keys hold key_words(k)
+// words per record.  flags (n) and pos (n) and scan_tmp
+// (scan_tmp_words(n)) are scratch; *n_bytes (device) receives the length.
+// out holds n * packed_record_bytes(k, count_bytes) bytes.
+uint32_t packed_record_bytes(uint32_t k, uint32_t count_bytes);
+cudaError_t launch_pack_high(uint32_t k, const unsigned long long *keys, const uint32_t *counts, uint64_t n,
+                             uint32_t count_bytes, uint32_t filter_min, uint32_t filter_max, uint32_t *flags,
+                             unsigned long long *pos, unsigned long long *scan_tmp, uint8_t *out,
+                             unsigned long long *n_bytes, cudaStream_t st);
+
 }  // namespace kc

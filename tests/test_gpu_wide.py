@@ -219,3 +219,42 @@ def test_wide_larger_job_matches_oracle(counter):
         assert np.array_equal(r.keys, want_k) and np.array_equal(r.counts, want_c)
         order = sorted(range(len(want_c)), key=lambda i: (-int(want_c[i]), i))[:100]
         assert np.array_equal(r.top_counts, want_c[order]) and np.array_equal(r.top_keys, want_k[order])
+
+
+@pytest.mark.parametrize("k,count_max,fmin,fmax", [(21, 255, 2, U32), (31, U32, 2, U32), (33, 0xFFFF, 3, 40),
+                                                   (64, 0xFFFFFF, 2, U32), (100, U32, 1, 7), (17, 1000, 5, 60)])
+def test_high_bin_packed_on_the_device_equals_the_host_packing(counter, k, count_max, fmin, fmax):
+    """kc_job.pack_high: high.bin made on the device byte-identical to the
+    host packing of the records and to the oracle's restatement of the
+    reference's record layout (src/FinalDrainWriter.h:71-101)."""
+    files = _case_files("plain_small") + _case_files("repeat")
+    job = dict(k=k, count_max=count_max, filter_min=fmin, filter_max=fmax)
+    with tempfile.TemporaryDirectory() as tmp:
+        a, b = os.path.join(tmp, "dev"), os.path.join(tmp, "host")
+        os.makedirs(a)
+        os.makedirs(b)
+        j = counter.submit(files, pack_high=True, keep_records=False, **job)
+        counter.wait(j)
+        counter.write_tmpdir(j, a)
+        counter.release(j)
+        j = counter.submit(files, keep_records=True, **job)
+        counter.wait(j)
+        counter.write_tmpdir(j, b)
+        r = counter.result(j, k)
+        dev = open(os.path.join(a, "high.bin"), "rb").read()
+        assert dev == open(os.path.join(b, "high.bin"), "rb").read()
+        assert os.path.getsize(os.path.join(a, "low.bin")) == 0
+        assert open(os.path.join(a, "infos.bin"), "rb").read() == open(os.path.join(b, "infos.bin"), "rb").read()
+    # the oracle's packing of the exact records
+    nw = O.key_words(k)
+    keys, counts = O.exact_records_wide(files, k, count_max=count_max)
+    keep = (counts.astype(np.int64) + 1 >= fmin) & (counts <= fmax)
+    cb = O.lib().kco_count_bytes(count_max)
+    kb = O.lib().kco_packed_kmer_bytes(k)
+    want = bytearray()
+    one = np.zeros(kb, np.uint8)
+    for w, c in zip(keys[keep], counts[keep]):
+        O.lib().kco_pack_kmer(O.P(np.ascontiguousarray(w, np.uint64)), k, O.P(one))
+        want += one.tobytes() + int(c).to_bytes(4, "little")[:cb]
+    assert dev == bytes(want)
+    assert r.keys.reshape(len(r.counts), -1).shape[1] == nw
