@@ -193,7 +193,12 @@ typedef struct {
                                      their sub-buckets from a 1-in-8 sample of the k-mers instead of
                                      counting them all (a sub-bucket that outgrows its estimate sends the
                                      pass back to exact counts); default 64M */
-    uint64_t reserved[2];
+    uint64_t count_shape;         /* block shape of the shared-memory count: 1 = 512-thread blocks, two per
+                                     SM, filter slices of up to 2048 blocks, 4096-slot tables; 2 = 256-thread
+                                     blocks, four per SM, slices of up to 1024 blocks, 2048-slot tables
+                                     (sub-buckets of half the k-mers); 3, 4 = 1, 2 with table slots from one
+                                     multiply instead of a 64-bit mix; default 1 */
+    uint64_t reserved[1];
 } kc_tuning;
 
 /* 64-bit words of one k-mer: 1 for k <= 32, 2 for k <= 64, 4 for k <= 128,

@@ -78,6 +78,7 @@ kc_tuning default_tuning()
     t.bloom_smem = 1;
     t.record_sort = 1;
     t.sampled_region_keys = 64ull << 20;
+    t.count_shape = 1;
     return t;
 }
 
@@ -898,6 +899,10 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
             // cannot be cut further sends the pass to the global-memory path.
             bool sub_done = false;
             if (P.bloom && P.min_count >= 2 && tn.bloom_smem == 1) {
+                // the count kernel's block shape: its slice and table sizes
+                // set the sub-buckets (a table of 2048 slots takes half the k-mers)
+                const uint32_t shape = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tn.count_shape, 4));
+                const uint64_t keys_target = SUB_KEYS_TARGET * sub_table_slots(shape) / SUB_TABLE_SLOTS;
                 std::vector<uint32_t> nsub(N_BUCKETS, 0);
                 bool eligible = true;
                 for (uint32_t b = lo; b < hi; ++b) {
@@ -906,7 +911,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                         eligible = false;
                         break;
                     }
-                    uint64_t want = std::max<uint64_t>(f / SUB_SLICE_BLOCKS, (cfg[b].key_len + SUB_KEYS_TARGET - 1) / SUB_KEYS_TARGET);
+                    uint64_t want = std::max<uint64_t>(f / sub_slice_blocks(shape), (cfg[b].key_len + keys_target - 1) / keys_target);
                     want = std::max<uint64_t>(bit_ceil64(want), 1);
                     if (want > std::min<uint64_t>(f, SUB_MAX_PER_BUCKET)) {
                         eligible = false;
@@ -950,7 +955,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                     // a record has count >= 2: at most half the occurrences, and at
                     // most one table of slots per sub-bucket
                     const uint64_t rcap = std::max<uint64_t>(
-                        std::min<uint64_t>((uint64_t)n_sub * SUB_TABLE_SLOTS, pass_keys / 2 + 1), 1);
+                        std::min<uint64_t>((uint64_t)n_sub * sub_table_slots(shape), pass_keys / 2 + 1), 1);
                     unsigned long long *rk = ds.n<unsigned long long>(rcap);
                     uint32_t *rc = ds.n<uint32_t>(rcap);
                     BucketRanges br{};
@@ -1003,7 +1008,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                     }
                     CK(launch_count_subs(list, sub_off, sub_count, d_sb, n_sub, d_sc, sub_next, count_max,
                                          P.min_count, P.max_count, rk, rc, rcap, hist_sub, ovf, ovf_cap, counters,
-                                         bucket_ovf, st, hb16, 2 * k - 16));
+                                         bucket_ovf, st, hb16, 2 * k - 16, shape));
                     clk.end();
                     if (attempt == 0 && (P.fault_inject & KC_INJECT_TABLE_FULL_ONCE)) {
                         // as if the first bucket's sub-bucket tables had overflowed
@@ -1033,7 +1038,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                         job.low_only += cs.v[C_LOW_ONLY];
                         low_len += cs.v[C_LOW_LEN];
                         high_len += cs.v[C_HIGH_LEN];
-                        table_cap = std::max<uint64_t>(table_cap, (uint64_t)n_sub * SUB_TABLE_SLOTS);
+                        table_cap = std::max<uint64_t>(table_cap, (uint64_t)n_sub * sub_table_slots(shape));
                         ++job.smem_passes;
                         sub_done = true;
                         break;
@@ -2304,6 +2309,7 @@ int kc_set_tuning(kc_handle *h, const kc_tuning *t)
     if (t->table_factor > 0 && t->table_factor < 1.05) return fail(KC_ERR_INVALID, "table_factor must be at least 1.05");
     if (t->bloom_smem > 2) return fail(KC_ERR_INVALID, "bloom_smem must be 1 or 2");
     if (t->record_sort > 2) return fail(KC_ERR_INVALID, "record_sort must be 1 or 2");
+    if (t->count_shape > 4) return fail(KC_ERR_INVALID, "count_shape must be 1..4");
     std::lock_guard<std::mutex> lk(h->mu);
     if (t->bucket_table_factor > 0) h->tuning.bucket_table_factor = t->bucket_table_factor;
     if (t->table_factor > 0) h->tuning.table_factor = t->table_factor;
@@ -2311,6 +2317,7 @@ int kc_set_tuning(kc_handle *h, const kc_tuning *t)
     if (t->bloom_smem > 0) h->tuning.bloom_smem = t->bloom_smem;
     if (t->record_sort > 0) h->tuning.record_sort = t->record_sort;
     if (t->sampled_region_keys > 0) h->tuning.sampled_region_keys = t->sampled_region_keys;
+    if (t->count_shape > 0) h->tuning.count_shape = t->count_shape;
     return KC_OK;
 }
 
@@ -2351,16 +2358,18 @@ int kc_autotune(kc_handle *h, const kc_job *jobs, uint32_t n_jobs, uint32_t batc
     double cur_ms = 0, ms = 0;
     int rc = run(cur, cur_ms);   // warm-up: workspaces and pinned blocks reach this shape
     if (rc == KC_OK) rc = run(cur, cur_ms);
-    const double bucket_c[] = {2.0, 3.0, 4.0}, table_c[] = {1.3, 1.6, 2.2};
-    const uint64_t group_c[] = {2ull << 20, 4ull << 20, 8ull << 20}, smem_c[] = {1, 2, 1}, sort_c[] = {1, 2, 1};
-    for (int param = 0; param < 5 && rc == KC_OK; ++param)
-        for (int c = 0; c < 3 && rc == KC_OK; ++c) {
+    const double bucket_c[] = {2.0, 3.0, 4.0, 3.0}, table_c[] = {1.3, 1.6, 2.2, 1.6};
+    const uint64_t group_c[] = {2ull << 20, 4ull << 20, 8ull << 20, 4ull << 20}, smem_c[] = {1, 2, 1, 1},
+                   sort_c[] = {1, 2, 1, 1}, shape_c[] = {1, 2, 3, 4};
+    for (int param = 0; param < 6 && rc == KC_OK; ++param)
+        for (int c = 0; c < 4 && rc == KC_OK; ++c) {
             kc_tuning t = cur;
             if (param == 0) t.bucket_table_factor = bucket_c[c];
             if (param == 1) t.table_factor = table_c[c];
             if (param == 2) t.sort_group_records = group_c[c];
             if (param == 3) t.bloom_smem = smem_c[c];
             if (param == 4) t.record_sort = sort_c[c];
+            if (param == 5) t.count_shape = shape_c[c];
             if (std::memcmp(&t, &cur, sizeof(t)) == 0) continue;
             rc = run(t, ms);
             if (rc == KC_OK && ms < 0.98 * cur_ms) {   // a clear gain only

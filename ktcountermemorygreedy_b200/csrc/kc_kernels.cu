@@ -2025,18 +2025,24 @@ __global__ void __launch_bounds__(SP_THREADS) k_subpart_scatter(const unsigned l
     }
 }
 
-// Shared-memory counting table of one sub-bucket: linear probing from the
-// key's hash, claims by CAS; a slot only changes from empty to a key.
+// Shared-memory counting table of one sub-bucket (2^TBITS slots): linear
+// probing from the key's hash, claims by CAS; a slot only changes from empty
+// to a key.  The home slot is the top TBITS bits of the 64-bit mix
+// (slot_hash), or with FIB of the key times 2^64 / golden ratio (one
+// multiply: placement only, it never affects a count).
 constexpr uint32_t SUB_MAX_PROBE = 512;
 
-__device__ __forceinline__ int sub_table_slot(unsigned long long key)
+template <uint32_t TBITS, bool FIB>
+__device__ __forceinline__ uint32_t sub_table_slot(unsigned long long key)
 {
-    return (int)(slot_hash(key) >> (64 - SUB_TABLE_BITS));
+    return FIB ? (uint32_t)((key * 0x9E3779B97F4A7C15ULL) >> (64 - TBITS))
+               : (uint32_t)(slot_hash(key) >> (64 - TBITS));
 }
 
+template <uint32_t TBITS, bool FIB>
 __device__ __forceinline__ bool sub_table_add(unsigned long long *tk, uint32_t *tc, unsigned long long key)
 {
-    uint32_t i = (uint32_t)sub_table_slot(key);
+    uint32_t i = sub_table_slot<TBITS, FIB>(key);
     for (uint32_t n = 0; n < SUB_MAX_PROBE; ++n) {
         const unsigned long long cur = *(volatile unsigned long long *)&tk[i];
         if (cur == key) {
@@ -2050,31 +2056,31 @@ __device__ __forceinline__ bool sub_table_add(unsigned long long *tk, uint32_t *
                 return true;
             }
         }
-        i = (i + 1) & (SUB_TABLE_SLOTS - 1);
+        i = (i + 1) & ((1u << TBITS) - 1);
     }
     return false;
 }
 
+template <uint32_t TBITS, bool FIB>
 __device__ __forceinline__ int sub_table_find(const unsigned long long *tk, unsigned long long key)
 {
-    uint32_t i = (uint32_t)sub_table_slot(key);
+    uint32_t i = sub_table_slot<TBITS, FIB>(key);
     for (uint32_t n = 0; n < SUB_MAX_PROBE; ++n) {
         const unsigned long long cur = tk[i];
         if (cur == key) return (int)i;
         if (cur == EMPTY_KEY) return -1;
-        i = (i + 1) & (SUB_TABLE_SLOTS - 1);
+        i = (i + 1) & ((1u << TBITS) - 1);
     }
     return -1;
 }
 
-constexpr uint32_t SUB_THREADS = 512;   // blocks of the shared-memory count
-constexpr uint32_t SUB_BLOCKS_PER_SM = 2;
 constexpr uint32_t SUB_PER_THREAD = 4;
-constexpr uint32_t SUB_TILE = SUB_THREADS * SUB_PER_THREAD;
-constexpr uint32_t SUB_HIST_BINS = 2048;   // counts below this go to a shared histogram
 
-
-__global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
+// THREADS per block, BPSM blocks per SM, filter slices of at most SLICE
+// blocks, tables of 2^TBITS slots, counts below HBINS histogrammed in shared
+// memory (the two shapes are SubShape 1 and 2 in kc_kernels.cuh).
+template <uint32_t THREADS, uint32_t BPSM, uint32_t SLICE, uint32_t TBITS, uint32_t HBINS, bool FIB>
+__global__ void __launch_bounds__(THREADS, BPSM) k_count_subs(
     unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count, const uint8_t *sub_bucket,
     uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub, uint32_t count_max, uint32_t min_count,
     uint32_t max_count, unsigned long long *rec_keys, uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist,
@@ -2082,16 +2088,16 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
     uint32_t hb16_shift)
 {
     extern __shared__ __align__(16) uint8_t cs_smem[];
-    unsigned long long *s_filter = reinterpret_cast<unsigned long long *>(cs_smem);   // 2 * SUB_SLICE_BLOCKS
-    unsigned long long *s_tk = s_filter + 2 * SUB_SLICE_BLOCKS;                       // SUB_TABLE_SLOTS
-    uint32_t *s_tc = reinterpret_cast<uint32_t *>(s_tk + SUB_TABLE_SLOTS);            // SUB_TABLE_SLOTS
-    uint32_t *s_hist = s_tc + SUB_TABLE_SLOTS;                                        // SUB_HIST_BINS
-    unsigned long long *s_queue = reinterpret_cast<unsigned long long *>(s_hist + SUB_HIST_BINS);   // SUB_TILE
+    unsigned long long *s_filter = reinterpret_cast<unsigned long long *>(cs_smem);   // 2 * SLICE
+    unsigned long long *s_tk = s_filter + 2 * SLICE;                       // (1u << TBITS)
+    uint32_t *s_tc = reinterpret_cast<uint32_t *>(s_tk + (1u << TBITS));            // (1u << TBITS)
+    uint32_t *s_hist = s_tc + (1u << TBITS);                                        // HBINS
+    unsigned long long *s_queue = reinterpret_cast<unsigned long long *>(s_hist + HBINS);   // (THREADS * SUB_PER_THREAD)
     __shared__ uint32_t s_warp[32], s_sub, s_lo;   // s_lo: FIRST keys written back
     __shared__ unsigned long long s_base;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t lt = lanemask_lt();
-    for (uint32_t i = tid; i < SUB_HIST_BINS; i += SUB_THREADS) s_hist[i] = 0;
+    for (uint32_t i = tid; i < HBINS; i += THREADS) s_hist[i] = 0;
     unsigned long long n_high = 0, n_low = 0, n_low_only = 0, n_distinct = 0;
     uint32_t n_ovf_subs = 0;
     bool rec_full = false;
@@ -2108,8 +2114,8 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
         const unsigned long long fcap = sc[bucket].fcap;
         const uint32_t slice = 1u << sc[bucket].slice_shift;
         if (tid == 0) s_lo = 0;
-        for (uint32_t i = tid; i < 2 * slice; i += SUB_THREADS) s_filter[i] = 0;
-        for (uint32_t i = tid; i < SUB_TABLE_SLOTS; i += SUB_THREADS) {
+        for (uint32_t i = tid; i < 2 * slice; i += THREADS) s_filter[i] = 0;
+        for (uint32_t i = tid; i < (1u << TBITS); i += THREADS) {
             s_tk[i] = EMPTY_KEY;
             s_tc[i] = 0;
         }
@@ -2123,22 +2129,22 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
         unsigned long long kn[SUB_PER_THREAD];
 #pragma unroll
         for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
-            const uint32_t i = r * SUB_THREADS + tid;
+            const uint32_t i = r * THREADS + tid;
             kn[r] = i < n ? __ldcs(&keys[base + i]) : EMPTY_KEY;
         }
         __syncthreads();   // the first tile is loaded by every warp before any write-back
-        for (uint32_t t0 = 0; t0 < n; t0 += SUB_TILE) {
+        for (uint32_t t0 = 0; t0 < n; t0 += (THREADS * SUB_PER_THREAD)) {
             unsigned long long k[SUB_PER_THREAD];
             uint32_t firsts = 0, highs = 0;
 #pragma unroll
             for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
                 k[r] = kn[r];
-                const uint32_t i = t0 + SUB_TILE + r * SUB_THREADS + tid;
+                const uint32_t i = t0 + (THREADS * SUB_PER_THREAD) + r * THREADS + tid;
                 kn[r] = i < n ? __ldcs(&keys[base + i]) : EMPTY_KEY;
             }
 #pragma unroll
             for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
-                if (t0 + r * SUB_THREADS + tid >= n) continue;
+                if (t0 + r * THREADS + tid >= n) continue;
                 uint64_t block, m, hi;
                 bloom_probe_hi(k[r], fcap, block, m, hi);
                 unsigned long long *cell = s_filter + 2 * (block & (slice - 1));
@@ -2170,7 +2176,7 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
                 }
                 __syncwarp();
                 for (uint32_t j = lane; j < qn; j += 32)
-                    if (!sub_table_add(s_tk, s_tc, q[j])) full = true;
+                    if (!sub_table_add<TBITS, FIB>(s_tk, s_tc, q[j])) full = true;
                 __syncwarp();
             }
             // FIRST write-back: each warp takes its positions with one
@@ -2208,17 +2214,17 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
         // 2. FIRST occurrences: a hit adds one to the table count, a miss is a
         // k-mer seen once (counted, not a record: min_count >= 2)
         const uint32_t lo_cnt = s_lo;
-        for (uint32_t i0 = tid; i0 < lo_cnt; i0 += SUB_THREADS * SUB_PER_THREAD) {
+        for (uint32_t i0 = tid; i0 < lo_cnt; i0 += THREADS * SUB_PER_THREAD) {
             unsigned long long kk[SUB_PER_THREAD];
 #pragma unroll
             for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
-                const uint32_t i = i0 + r * SUB_THREADS;
+                const uint32_t i = i0 + r * THREADS;
                 kk[r] = i < lo_cnt ? __ldcg(&keys[base + i]) : EMPTY_KEY;
             }
 #pragma unroll
             for (uint32_t r = 0; r < SUB_PER_THREAD; ++r) {
-                if (i0 + r * SUB_THREADS >= lo_cnt) continue;
-                const int sl = sub_table_find(s_tk, kk[r]);
+                if (i0 + r * THREADS >= lo_cnt) continue;
+                const int sl = sub_table_find<TBITS, FIB>(s_tk, kk[r]);
                 if (sl >= 0) atomicAdd(&s_tc[sl], 1u);
                 else ++n_low_only;
             }
@@ -2226,11 +2232,11 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
         __syncthreads();
         // 3. the table's records and histogram
         uint32_t keep = 0;
-        for (uint32_t i = tid; i < SUB_TABLE_SLOTS; i += SUB_THREADS) {
+        for (uint32_t i = tid; i < (1u << TBITS); i += THREADS) {
             if (s_tk[i] == EMPTY_KEY) continue;
             ++n_distinct;
             const uint32_t c = s_tc[i] < count_max ? s_tc[i] : count_max;
-            if (c < SUB_HIST_BINS) atomicAdd(&s_hist[c], 1u);
+            if (c < HBINS) atomicAdd(&s_hist[c], 1u);
             else if (c < HIST_BINS) atomicAdd(&hist[c], 1ull);
             else {
                 const unsigned long long q = atomicAdd(&counters[C_OVF_LEN], 1ull);
@@ -2244,7 +2250,7 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
         if (tid == 0) s_base = tk ? atomicAdd(&counters[C_REC_LEN], (unsigned long long)tk) : 0ull;
         __syncthreads();
         unsigned long long q = s_base + ok;
-        for (uint32_t i = tid; i < SUB_TABLE_SLOTS; i += SUB_THREADS) {
+        for (uint32_t i = tid; i < (1u << TBITS); i += THREADS) {
             if (s_tk[i] == EMPTY_KEY) continue;
             const uint32_t c = s_tc[i] < count_max ? s_tc[i] : count_max;
             if (c < min_count || c > max_count) continue;
@@ -2261,7 +2267,7 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_count_subs(
         __syncthreads();
     }
     __syncthreads();
-    for (uint32_t i = tid; i < SUB_HIST_BINS; i += SUB_THREADS)
+    for (uint32_t i = tid; i < HBINS; i += THREADS)
         if (s_hist[i]) atomicAdd(&hist[i], (unsigned long long)s_hist[i]);
     if (rec_full) atomicOr(&counters[C_FLAGS], ERR_RECORDS_FULL);
     const unsigned long long v[4] = {n_high, n_low, n_low_only, n_distinct};
@@ -2993,27 +2999,49 @@ cudaError_t launch_subpart_scatter(const unsigned long long *keys, const BucketR
     return cudaGetLastError();
 }
 
+template <uint32_t THREADS, uint32_t BPSM, uint32_t SLICE, uint32_t TBITS, uint32_t HBINS, bool FIB>
+static cudaError_t launch_count_subs_t(unsigned long long *keys, const unsigned long long *sub_off,
+                                       const uint32_t *sub_count, const uint8_t *sub_bucket, uint32_t n_sub,
+                                       const SubCfg *sc, unsigned int *next_sub, uint32_t count_max,
+                                       uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
+                                       uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist, uint32_t *ovf,
+                                       uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf,
+                                       cudaStream_t st, uint32_t *hb16, uint32_t hb16_shift)
+{
+    const size_t smem = (size_t)2 * SLICE * 8 + ((size_t)1 << TBITS) * (8 + 4) + HBINS * 4 +
+                        (size_t)THREADS * SUB_PER_THREAD * 8;
+    auto kern = k_count_subs<THREADS, BPSM, SLICE, TBITS, HBINS, FIB>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const uint32_t grid = std::min<uint32_t>(n_sub, (uint32_t)sm_count() * BPSM);
+    note_launch();
+    kern<<<grid, THREADS, smem, st>>>(keys, sub_off, sub_count, sub_bucket, n_sub, sc, next_sub, count_max, min_count,
+                                      max_count, rec_keys, rec_counts, rec_cap, hist, ovf, ovf_cap, counters, bucket_ovf,
+                                      hb16, hb16_shift);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_count_subs(unsigned long long *keys, const unsigned long long *sub_off, const uint32_t *sub_count,
                               const uint8_t *sub_bucket, uint32_t n_sub, const SubCfg *sc, unsigned int *next_sub,
                               uint32_t count_max, uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
                               uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist, uint32_t *ovf,
                               uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, cudaStream_t st,
-                              uint32_t *hb16, uint32_t hb16_shift)
+                              uint32_t *hb16, uint32_t hb16_shift, uint32_t shape)
 {
     if (!n_sub) return cudaSuccess;
     if (min_count < 2) return cudaErrorInvalidValue;   // singletons are not records on this path
     cudaError_t e = cudaMemsetAsync(next_sub, 0, 4, st);
     if (e != cudaSuccess) return e;
-    const size_t smem = (size_t)2 * SUB_SLICE_BLOCKS * 8 + (size_t)SUB_TABLE_SLOTS * (8 + 4) + SUB_HIST_BINS * 4 +
-                        (size_t)SUB_TILE * 8;
-    e = cudaFuncSetAttribute(k_count_subs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    const uint32_t grid = std::min<uint32_t>(n_sub, (uint32_t)sm_count() * SUB_BLOCKS_PER_SM);
-    note_launch();
-    k_count_subs<<<grid, SUB_THREADS, smem, st>>>(keys, sub_off, sub_count, sub_bucket, n_sub, sc, next_sub, count_max,
-                                                  min_count, max_count, rec_keys, rec_counts, rec_cap, hist, ovf,
-                                                  ovf_cap, counters, bucket_ovf, hb16, hb16_shift);
-    return cudaGetLastError();
+#define KC_COUNT_SUBS_ARGS                                                                                         \
+    keys, sub_off, sub_count, sub_bucket, n_sub, sc, next_sub, count_max, min_count, max_count, rec_keys, rec_counts, \
+        rec_cap, hist, ovf, ovf_cap, counters, bucket_ovf, st, hb16, hb16_shift
+    switch (shape) {
+    case 2: return launch_count_subs_t<256, 4, 1024, 11, 1024, false>(KC_COUNT_SUBS_ARGS);
+    case 3: return launch_count_subs_t<512, 2, 2048, 12, 2048, true>(KC_COUNT_SUBS_ARGS);
+    case 4: return launch_count_subs_t<256, 4, 1024, 11, 1024, true>(KC_COUNT_SUBS_ARGS);
+    default: return launch_count_subs_t<512, 2, 2048, 12, 2048, false>(KC_COUNT_SUBS_ARGS);
+    }
+#undef KC_COUNT_SUBS_ARGS
 }
 
 cudaError_t launch_wait_flag(const unsigned int *flag, uint32_t poll_limit, unsigned long long *flags, cudaStream_t st)
@@ -3159,7 +3187,7 @@ cudaError_t launch_atomic_peak(uint32_t *buf, uint64_t words, uint32_t iters, ui
 // table per block, with the shared-memory count's block shape (512 threads,
 // two blocks per SM).  Each block adds its table into `out` at the end so
 // that the adds are not dead code.
-__global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_atomic_peak_shared(uint32_t *out, uint32_t mask,
+__global__ void __launch_bounds__(512, 2) k_atomic_peak_shared(uint32_t *out, uint32_t mask,
                                                                                         uint32_t iters, uint64_t seed)
 {
     extern __shared__ uint32_t s_tab[];
@@ -3185,13 +3213,13 @@ __global__ void __launch_bounds__(SUB_THREADS, SUB_BLOCKS_PER_SM) k_atomic_peak_
 cudaError_t launch_atomic_peak_shared(uint32_t *out, uint32_t words, uint32_t iters, uint64_t seed, uint64_t *ops,
                                       cudaStream_t st)
 {
-    const unsigned grid = (unsigned)sm_count() * SUB_BLOCKS_PER_SM * 4;
+    const unsigned grid = (unsigned)sm_count() * 2 * 4;
     const size_t smem = (size_t)words * 4;
     cudaError_t e = cudaFuncSetAttribute(k_atomic_peak_shared, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    *ops = (uint64_t)grid * SUB_THREADS * iters;
+    *ops = (uint64_t)grid * 512 * iters;
     note_launch();
-    k_atomic_peak_shared<<<grid, SUB_THREADS, smem, st>>>(out, words - 1, iters, seed);
+    k_atomic_peak_shared<<<grid, 512, smem, st>>>(out, words - 1, iters, seed);
     return cudaGetLastError();
 }
 

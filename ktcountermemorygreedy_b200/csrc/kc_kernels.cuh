@@ -330,7 +330,14 @@ cudaError_t launch_count_subs(unsigned long long *keys, const unsigned long long
                               uint32_t count_max, uint32_t min_count, uint32_t max_count, unsigned long long *rec_keys,
                               uint32_t *rec_counts, uint64_t rec_cap, unsigned long long *hist, uint32_t *ovf,
                               uint64_t ovf_cap, unsigned long long *counters, uint32_t *bucket_ovf, cudaStream_t st,
-                              uint32_t *hb16 = nullptr, uint32_t hb16_shift = 0);
+                              uint32_t *hb16 = nullptr, uint32_t hb16_shift = 0, uint32_t shape = 1);
+// Block shapes of the shared-memory count (kc_tuning.count_shape): 1 and 3
+// run 512-thread blocks, two per SM, filter slices of up to 2048 blocks and
+// 4096-slot tables; 2 and 4 run 256-thread blocks, four per SM, slices of up
+// to 1024 blocks and 2048-slot tables (sub-buckets of half the k-mers).  3
+// and 4 place keys in the table by one multiply instead of the 64-bit mix.
+inline uint32_t sub_slice_blocks(uint32_t shape) { return (shape == 2 || shape == 4) ? 1024u : 2048u; }
+inline uint32_t sub_table_slots(uint32_t shape) { return (shape == 2 || shape == 4) ? 2048u : 4096u; }
 cudaError_t launch_bloom_buckets(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                  unsigned int *next_item, const BucketCfg *cfg, unsigned long long *bits,
                                  unsigned long long *out, unsigned long long *low_cnt, unsigned long long *high_cnt,

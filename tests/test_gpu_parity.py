@@ -556,6 +556,34 @@ def test_bloom_shared_memory_path_matches_global_path(kc):
         c.set_tuning(bloom_smem=1)
 
 
+@pytest.mark.parametrize("shape", [1, 2, 3, 4])
+def test_count_shapes_give_exact_results(kc, shape):
+    """Every block shape of the shared-memory count (kc_tuning.count_shape:
+    512- or 256-thread blocks, 4096- or 2048-slot tables, two table hashes):
+    exact records, histogram and queries, including a job whose tables
+    overflow and are split."""
+    import ktcountermemorygreedy_b200.synth as S
+    g = S.genome(84, 2_000_000)
+    fq = S.reads(g, 84, 50_000, (100, 150), 0.01, 0.0).tobytes()
+    once = S.reads(S.genome(85, 3_000_000), 85, 15_000, (150, 150), 0.0, 0.0).tobytes()
+    with kc.KmerCounter(max_inflight_jobs=1) as c:
+        c.set_tuning(bloom_smem=1, count_shape=shape)
+        assert c.tuning["count_shape"] == shape
+        for files, k, cm in (([fq], 31, U32), ([fq], 21, 255), ([once, once], 31, U32)):
+            want_k, want_c = O.exact_records(files, k, cm)
+            m = want_c >= 2
+            r = c.count(files, k=k, count_max=cm, bloom=True, memory_gb=1, min_count=2, hist_min=1, hist_max=400,
+                        top_n=64, want_le2=1)
+            assert r.smem_passes == 1 and r.smem_fallbacks == 0
+            assert np.array_equal(r.keys, want_k[m]) and np.array_equal(r.counts, want_c[m]), (shape, k)
+            assert np.array_equal(r.hist, O.histogram(want_c, 1, 400))
+            order = sorted(range(int(m.sum())), key=lambda i: (-int(want_c[m][i]), i))[:64]
+            assert np.array_equal(r.top_keys, want_k[m][order]) and np.array_equal(r.top_counts, want_c[m][order])
+            le = want_c[m] <= 2
+            assert np.array_equal(r.le2_keys, want_k[m][le])
+            assert r.distinct == len(want_k)
+
+
 def test_bloom_shared_memory_tables_overflow_and_split(counter):
     """Every read twice: half the k-mers of a bucket are distinct repeated
     ones, more than one sub-bucket table holds, so the overflowing buckets are
