@@ -198,7 +198,8 @@ typedef struct {
                                      blocks, four per SM, slices of up to 1024 blocks, 2048-slot tables
                                      (sub-buckets of half the k-mers); 3, 4 = 1, 2 with table slots from one
                                      multiply instead of a 64-bit mix; default 1 */
-    uint64_t reserved[1];
+    uint64_t part_shape;          /* the partition's rounds: 1 = 4096 k-mers staged per round (three blocks
+                                     per SM), 2 = 2048 (four blocks per SM); default 1 */
 } kc_tuning;
 
 /* 64-bit words of one k-mer: 1 for k <= 32, 2 for k <= 64, 4 for k <= 128,

@@ -79,6 +79,7 @@ kc_tuning default_tuning()
     t.record_sort = 1;
     t.sampled_region_keys = 64ull << 20;
     t.count_shape = 1;
+    t.part_shape = 1;
     return t;
 }
 
@@ -857,18 +858,18 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                 cu.enqueue(cu.ev.size());
                 a.tile0 = 0;
                 a.n_tiles = tiles_ready;
-                CK(launch_extract(MODE_PART, a, 0, st));
+                CK(launch_extract(MODE_PART, a, 0, st, (uint32_t)tn.part_shape));
                 while (chunks_done < cu.ev.size()) {
                     const uint64_t t0 = tiles_ready;
                     census_chunks(chunks_done + 1);
                     a.tile0 = t0;
                     a.n_tiles = tiles_ready - t0;
-                    CK(launch_extract(MODE_PART, a, 0, st));
+                    CK(launch_extract(MODE_PART, a, 0, st, (uint32_t)tn.part_shape));
                 }
                 a.tile0 = 0;
                 a.n_tiles = T;
             } else {
-                CK(launch_extract(MODE_PART, a, 0, st));
+                CK(launch_extract(MODE_PART, a, 0, st, (uint32_t)tn.part_shape));
             }
             clk.end();
             unsigned long long *p_fill = hs.n<unsigned long long>(N_BUCKETS);
@@ -2310,6 +2311,7 @@ int kc_set_tuning(kc_handle *h, const kc_tuning *t)
     if (t->bloom_smem > 2) return fail(KC_ERR_INVALID, "bloom_smem must be 1 or 2");
     if (t->record_sort > 2) return fail(KC_ERR_INVALID, "record_sort must be 1 or 2");
     if (t->count_shape > 4) return fail(KC_ERR_INVALID, "count_shape must be 1..4");
+    if (t->part_shape > 2) return fail(KC_ERR_INVALID, "part_shape must be 1 or 2");
     std::lock_guard<std::mutex> lk(h->mu);
     if (t->bucket_table_factor > 0) h->tuning.bucket_table_factor = t->bucket_table_factor;
     if (t->table_factor > 0) h->tuning.table_factor = t->table_factor;
@@ -2318,6 +2320,7 @@ int kc_set_tuning(kc_handle *h, const kc_tuning *t)
     if (t->record_sort > 0) h->tuning.record_sort = t->record_sort;
     if (t->sampled_region_keys > 0) h->tuning.sampled_region_keys = t->sampled_region_keys;
     if (t->count_shape > 0) h->tuning.count_shape = t->count_shape;
+    if (t->part_shape > 0) h->tuning.part_shape = t->part_shape;
     return KC_OK;
 }
 
@@ -2360,8 +2363,8 @@ int kc_autotune(kc_handle *h, const kc_job *jobs, uint32_t n_jobs, uint32_t batc
     if (rc == KC_OK) rc = run(cur, cur_ms);
     const double bucket_c[] = {2.0, 3.0, 4.0, 3.0}, table_c[] = {1.3, 1.6, 2.2, 1.6};
     const uint64_t group_c[] = {2ull << 20, 4ull << 20, 8ull << 20, 4ull << 20}, smem_c[] = {1, 2, 1, 1},
-                   sort_c[] = {1, 2, 1, 1}, shape_c[] = {1, 2, 3, 4};
-    for (int param = 0; param < 6 && rc == KC_OK; ++param)
+                   sort_c[] = {1, 2, 1, 1}, shape_c[] = {1, 2, 3, 4}, part_c[] = {1, 2, 1, 1};
+    for (int param = 0; param < 7 && rc == KC_OK; ++param)
         for (int c = 0; c < 4 && rc == KC_OK; ++c) {
             kc_tuning t = cur;
             if (param == 0) t.bucket_table_factor = bucket_c[c];
@@ -2370,6 +2373,7 @@ int kc_autotune(kc_handle *h, const kc_job *jobs, uint32_t n_jobs, uint32_t batc
             if (param == 3) t.bloom_smem = smem_c[c];
             if (param == 4) t.record_sort = sort_c[c];
             if (param == 5) t.count_shape = shape_c[c];
+            if (param == 6) t.part_shape = part_c[c];
             if (std::memcmp(&t, &cur, sizeof(t)) == 0) continue;
             rc = run(t, ms);
             if (rc == KC_OK && ms < 0.98 * cur_ms) {   // a clear gain only

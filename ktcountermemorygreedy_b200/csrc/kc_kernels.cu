@@ -317,8 +317,12 @@ __global__ void k_chunk_lastnl(const int32_t *tile_lastnl, const uint32_t *tile_
 // extraction
 // ---------------------------------------------------------------------------
 
-template <int MODE>
-__global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extract(ExtractArgs a, uint32_t stage_cap)
+// SCAP: the most k-mers staged per round (the PART reorder holds SCAP /
+// EXT_THREADS of them per thread in registers); a PART launch with
+// SCAP = 2048 fits four blocks per SM instead of three.
+template <int MODE, uint32_t SCAP = STAGE_CAP>
+__global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : (SCAP <= 2048 ? 4 : 3))
+    k_extract(ExtractArgs a, uint32_t stage_cap)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t *sbuf[2] = {smem, smem + BUF_BYTES};
@@ -607,9 +611,9 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
                     // flight during the reorder and consumed only after it
                     const unsigned long long cur = c ? atomicAdd(&a.bucket_cursor[tid], (unsigned long long)c) : 0ull;
                     __syncthreads();
-                    unsigned long long kr[STAGE_CAP / EXT_THREADS];
+                    unsigned long long kr[SCAP / EXT_THREADS];
 #pragma unroll
-                    for (uint32_t r = 0; r < STAGE_CAP / EXT_THREADS; ++r) {
+                    for (uint32_t r = 0; r < SCAP / EXT_THREADS; ++r) {
                         const uint32_t i = tid + r * EXT_THREADS;
                         if (i < nr && s_rank[i] != 0xFFFFu) {
                             kr[r] = s_stage[i];
@@ -618,7 +622,7 @@ __global__ void __launch_bounds__(EXT_THREADS, MODE == MODE_SCAN ? 5 : 3) k_extr
                     }
                     __syncthreads();
 #pragma unroll
-                    for (uint32_t r = 0; r < STAGE_CAP / EXT_THREADS; ++r) {
+                    for (uint32_t r = 0; r < SCAP / EXT_THREADS; ++r) {
                         const uint32_t i = tid + r * EXT_THREADS;
                         if (i < nr && s_rank[i] != 0xFFFFu) s_stage[s_rank[i]] = kr[r];
                     }
@@ -2385,15 +2389,16 @@ cudaError_t launch_chunk_lastnl(const int32_t *tile_lastnl, const uint32_t *tile
     return cudaGetLastError();
 }
 
-template <int M>
+template <int M, uint32_t SCAP = STAGE_CAP>
 static cudaError_t launch_extract_t(const ExtractArgs &a, int grid, uint32_t stage_cap, cudaStream_t st)
 {
     size_t smem = extract_smem_bytes_for(M, stage_cap);
-    cudaError_t e = cudaFuncSetAttribute(k_extract<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    auto kern = k_extract<M, SCAP>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if (grid <= 0) {
         int per_sm = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_extract<M>, EXT_THREADS, smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, EXT_THREADS, smem);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) per_sm = 1;
         grid = sm_count() * per_sm;
@@ -2402,11 +2407,11 @@ static cudaError_t launch_extract_t(const ExtractArgs &a, int grid, uint32_t sta
     if (!n_iter) return cudaSuccess;
     if ((uint64_t)grid > n_iter) grid = (int)n_iter;
     note_launch();
-    k_extract<M><<<grid, EXT_THREADS, smem, st>>>(a, stage_cap);
+    kern<<<grid, EXT_THREADS, smem, st>>>(a, stage_cap);
     return cudaGetLastError();
 }
 
-cudaError_t launch_extract(int mode, const ExtractArgs &a, int grid, cudaStream_t st)
+cudaError_t launch_extract(int mode, const ExtractArgs &a, int grid, cudaStream_t st, uint32_t part_shape)
 {
     if (!a.n_tiles) return cudaSuccess;
     switch (mode) {
@@ -2414,7 +2419,9 @@ cudaError_t launch_extract(int mode, const ExtractArgs &a, int grid, cudaStream_
     case MODE_INSERT: return launch_extract_t<MODE_INSERT>(a, grid, STAGE_CAP, st);
     case MODE_BLOOM: return launch_extract_t<MODE_BLOOM>(a, grid, STAGE_CAP, st);
     case MODE_EMIT: return launch_extract_t<MODE_EMIT>(a, grid, STAGE_CAP, st);
-    case MODE_PART: return launch_extract_t<MODE_PART>(a, grid, STAGE_CAP, st);
+    case MODE_PART:
+        return part_shape == 2 ? launch_extract_t<MODE_PART, 2048>(a, grid, 2048, st)
+                               : launch_extract_t<MODE_PART>(a, grid, STAGE_CAP, st);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -181,7 +181,9 @@ cudaError_t launch_newlines(const uint8_t *buf, uint64_t n_tiles, uint32_t *tile
 cudaError_t launch_chunk_lastnl(const int32_t *tile_lastnl, const uint32_t *tile_seg, const Seg *segs,
                                 const uint64_t *seg_chunk0, uint64_t n_tiles, int32_t *chunk_lastnl,
                                 cudaStream_t st);
-cudaError_t launch_extract(int mode, const ExtractArgs &a, int grid, cudaStream_t st);
+// part_shape (MODE_PART, kc_tuning.part_shape): 1 stages 4096 k-mers a round
+// (three blocks per SM), 2 stages 2048 (four blocks per SM).
+cudaError_t launch_extract(int mode, const ExtractArgs &a, int grid, cudaStream_t st, uint32_t part_shape = 1);
 
 // Exclusive prefix sum of n 32-bit values into 64-bit outputs.  tmp must
 // hold scan_tmp_words(n) 64-bit words.

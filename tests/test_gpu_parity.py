@@ -584,6 +584,23 @@ def test_count_shapes_give_exact_results(kc, shape):
             assert r.distinct == len(want_k)
 
 
+@pytest.mark.parametrize("part_shape", [1, 2])
+def test_partition_round_sizes_give_exact_results(kc, part_shape):
+    """The partition's two round sizes (kc_tuning.part_shape: 4096 or 2048
+    k-mers staged per round) on Bloom and large plain jobs: exact records."""
+    import ktcountermemorygreedy_b200.synth as S
+    fq = S.reads(S.genome(86, 2_000_000), 86, 60_000, (100, 150), 0.01, 0.0).tobytes()
+    with kc.KmerCounter(max_inflight_jobs=1) as c:
+        c.set_tuning(part_shape=part_shape)
+        assert c.tuning["part_shape"] == part_shape
+        for kw in (dict(k=31, bloom=True, memory_gb=1, min_count=2), dict(k=25, bloom=True, memory_gb=1,
+                                                                          min_count=2, pass_bytes=64 << 20),
+                   dict(k=21)):
+            want_k, want_c = O.exact_records([fq], kw["k"], U32, min_count=kw.get("min_count", 1))
+            r = c.count([fq], count_max=U32, **kw)
+            assert np.array_equal(r.keys, want_k) and np.array_equal(r.counts, want_c), (part_shape, kw)
+
+
 def test_bloom_shared_memory_tables_overflow_and_split(counter):
     """Every read twice: half the k-mers of a bucket are distinct repeated
     ones, more than one sub-bucket table holds, so the overflowing buckets are
