@@ -299,7 +299,7 @@ def run_reference_arm(args):
                          "sample": sample, "cpu": model},
         "e2e": {"value": value, "unit": "k-mers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
+    print(json.dumps(line, default=_json_default), flush=True)
 
 
 # ---------------------------------------------------------------------------
@@ -534,6 +534,13 @@ def served_bench(kc, args, local):
             out["rates"][str(rate)] = serving.summarize(stats, wall)
     kc.lib().kc_host_free(p)
     return out
+
+
+def _json_default(o):
+    """numpy scalars (and anything else with .item()) as plain JSON values."""
+    if hasattr(o, "item"):
+        return o.item()
+    raise TypeError(f"not JSON serializable: {type(o).__name__}")
 
 
 def records_digest(r):
@@ -864,7 +871,7 @@ def run_ours(args):
             "stages": stages, "atomics": atomics, "served": served, "batched": batched, "out_of_core": ooc,
             "wide": wide,
         }
-        print(json.dumps(line), flush=True)
+        print(json.dumps(line, default=_json_default), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -85,7 +85,7 @@ def full_spot_check(fq: np.ndarray, k: int, keys: np.ndarray, counts: np.ndarray
         got_k.append(kc_[sel])
         got_c.append(cc[sel])
         sk = string_keys(kc_)
-        ordered = ordered and bool(np.all(sk[1:] > sk[:-1])) and (prev is None or len(sk) == 0 or sk[0] > prev)
+        ordered = ordered and bool(np.all(sk[1:] > sk[:-1])) and bool(prev is None or len(sk) == 0 or sk[0] > prev)
         if len(sk):
             prev = sk[-1]
         del sk
@@ -141,7 +141,7 @@ def full_spot_check_wide(fq: np.ndarray, k: int, keys: np.ndarray, counts: np.nd
                 cmp[und & (sk[1:, w] < sk[:-1, w])] = -1
             ordered = ordered and bool(np.all(cmp == 1))
             if prev is not None:
-                ordered = ordered and tuple(sk[0].tolist()) > prev
+                ordered = ordered and bool(tuple(sk[0].tolist()) > prev)
             prev = tuple(sk[-1].tolist())
         c = cc[(cc >= hist_min) & (cc <= hmax)]
         rec_hist += np.bincount(c - np.uint32(hist_min), minlength=len(hist))[: len(hist)]
