@@ -803,3 +803,25 @@ def test_record_sort_variants_same_results(kc, record_sort):
         m = (wc >= j["min_count"])
         assert np.array_equal(r.keys, wk[m]) and np.array_equal(r.counts, wc[m]), j
         assert r.hist.tolist() == O.histogram(wc, 1, 1000).tolist()
+
+
+def test_large_jobs_run_alone_among_small_ones(kc):
+    """A job whose reservation exceeds one worker's share of the budget runs
+    alone (the idle workers give their kept workspaces back first; nothing
+    else starts until it ends); small jobs around it still run concurrently.
+    Every job's results equal the job counted alone."""
+    big = fixtures.random_fastq(91, 120_000, (150, 150), genome_len=3_000_000, sub=0.01, n_rate=0.0)
+    smalls = [fixtures.random_fastq(92 + i, 2000, (100, 150), genome_len=50_000, sub=0.01, n_rate=0.0)
+              for i in range(6)]
+    plan = [(smalls[0], 21), (smalls[1], 31), (big, 31), (smalls[2], 25), (smalls[3], 21), (big, 25),
+            (smalls[4], 31), (smalls[5], 21)]
+    job = dict(count_max=U32, hist_min=1, hist_max=500)
+    # a 1.2 GB budget over three workers: the 38 MB file reserves about 1 GB
+    with kc.KmerCounter(max_inflight_jobs=3, hbm_budget_bytes=1_200_000_000) as c:
+        ids = [c.submit([f], k=k, **job) for f, k in plan]
+        for jid, (f, k) in zip(ids, plan):
+            c.wait(jid)
+            r = c.result(jid, k)
+            want_k, want_c = O.exact_records([f], k)
+            assert np.array_equal(r.keys, want_k) and np.array_equal(r.counts, want_c), k
+            assert np.array_equal(r.hist, O.histogram(want_c, 1, 500))
