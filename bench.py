@@ -729,8 +729,14 @@ def run_ours(args):
     fq, pinned, genome_len, n_reads = make_input(args.scale, kc)
     counter = kc.KmerCounter(device=local, max_inflight_jobs=1)
     inp = counter.upload([fq])
-    # settings chosen by the project's autotuner on this workload (untimed)
-    tuning = counter.autotune(inputs=[inp], keep_records=False, **JOB)
+    if args.tuning:
+        # settings given on the command line (name=value), no autotuner run
+        counter.set_tuning(**{k: (float(v) if "factor" in k else int(v))
+                              for k, v in (t.split("=", 1) for t in args.tuning)})
+        tuning = counter.tuning
+    else:
+        # settings chosen by the project's autotuner on this workload (untimed)
+        tuning = counter.autotune(inputs=[inp], keep_records=False, **JOB)
     for _ in range(args.warmup):
         counter.count(input=inp, keep_records=False, **JOB)
     barrier(world)
@@ -896,6 +902,8 @@ def main():
     ap.add_argument("--no-batched", dest="batched", action="store_false")
     ap.add_argument("--batch-samples", type=int, default=256)
     ap.add_argument("--batch-scale", type=float, default=0.125)
+    ap.add_argument("--tuning", nargs="*", default=[],
+                    help="handle settings name=value (kc_tuning fields) instead of the autotuner's")
     ap.add_argument("--wide", type=int, nargs="*", default=[],
                     help="also time k-mers of more than 32 bases (e.g. 63 127) on the same workload")
     ap.add_argument("--out-of-core", action="store_true",
