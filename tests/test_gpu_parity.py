@@ -577,8 +577,9 @@ def test_count_shapes_give_exact_results(kc, shape):
             assert r.smem_passes == 1 and r.smem_fallbacks == 0
             assert np.array_equal(r.keys, want_k[m]) and np.array_equal(r.counts, want_c[m]), (shape, k)
             assert np.array_equal(r.hist, O.histogram(want_c, 1, 400))
-            order = sorted(range(int(m.sum())), key=lambda i: (-int(want_c[m][i]), i))[:64]
-            assert np.array_equal(r.top_keys, want_k[m][order]) and np.array_equal(r.top_counts, want_c[m][order])
+            rk, rc = want_k[m], want_c[m]
+            order = np.argsort(-rc.astype(np.int64), kind="stable")[:64]   # count desc, then printed order
+            assert np.array_equal(r.top_keys, rk[order]) and np.array_equal(r.top_counts, rc[order])
             le = want_c[m] <= 2
             assert np.array_equal(r.le2_keys, want_k[m][le])
             assert r.distinct == len(want_k)
