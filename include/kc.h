@@ -200,6 +200,10 @@ typedef struct {
                                      multiply instead of a 64-bit mix; default 1 */
     uint64_t part_shape;          /* the partition's rounds: 1 = 4096 k-mers staged per round (three blocks
                                      per SM), 2 = 2048 (four blocks per SM); default 1 */
+    uint64_t scatter_shape;       /* the sub-bucket scatter: 1 = two blocks per SM, 2 = a variant with fewer
+                                     registers, three per SM (passes whose buckets have at most 1024
+                                     sub-buckets); default 1 */
+    uint64_t reserved[3];
 } kc_tuning;
 
 /* 64-bit words of one k-mer: 1 for k <= 32, 2 for k <= 64, 4 for k <= 128,

@@ -60,7 +60,8 @@ class kc_config(C.Structure):
 class kc_tuning(C.Structure):
     _fields_ = [("bucket_table_factor", C.c_double), ("table_factor", C.c_double),
                 ("sort_group_records", C.c_uint64), ("bloom_smem", C.c_uint64), ("record_sort", C.c_uint64),
-                ("sampled_region_keys", C.c_uint64), ("count_shape", C.c_uint64), ("part_shape", C.c_uint64)]
+                ("sampled_region_keys", C.c_uint64), ("count_shape", C.c_uint64), ("part_shape", C.c_uint64),
+                ("scatter_shape", C.c_uint64), ("reserved", C.c_uint64 * 3)]
 
 
 class kc_buffer(C.Structure):
@@ -435,17 +436,18 @@ class KmerCounter:
         return {"bucket_table_factor": t.bucket_table_factor, "table_factor": t.table_factor,
                 "sort_group_records": t.sort_group_records, "bloom_smem": t.bloom_smem, "record_sort": t.record_sort,
                 "sampled_region_keys": t.sampled_region_keys, "count_shape": t.count_shape,
-                "part_shape": t.part_shape}
+                "part_shape": t.part_shape, "scatter_shape": t.scatter_shape}
 
     def set_tuning(self, bucket_table_factor: float = 0.0, table_factor: float = 0.0, sort_group_records: int = 0,
                    bloom_smem: int = 0, record_sort: int = 0, sampled_region_keys: int = 0, count_shape: int = 0,
-                   part_shape: int = 0):
+                   part_shape: int = 0, scatter_shape: int = 0):
         """0 (or less) keeps a setting.  bloom_smem: 1 counts Bloom jobs (min
         count >= 2) per sub-bucket in shared memory, 2 on global-memory tables.
         record_sort: 1 sorts large jobs' records most significant bits first,
         2 with the LSD radix sort.  count_shape: the shared-memory count's
-        block shape, 1..4; part_shape: the partition's round size, 1 or 2
-        (kc_tuning in include/kc.h)."""
+        block shape, 1..4; part_shape: the partition's round size, 1 or 2;
+        scatter_shape: the sub-bucket scatter's variant, 1 or 2 (kc_tuning in
+        include/kc.h)."""
         t = kc_tuning()
         t.bucket_table_factor, t.table_factor, t.sort_group_records = bucket_table_factor, table_factor, \
             sort_group_records
@@ -454,6 +456,7 @@ class KmerCounter:
         t.sampled_region_keys = sampled_region_keys
         t.count_shape = count_shape
         t.part_shape = part_shape
+        t.scatter_shape = scatter_shape
         _check(lib().kc_set_tuning(self._h, C.byref(t)))
 
     def autotune(self, samples: Sequence[Sequence[bytes]] = (), ks: Sequence[int] = (), batch: bool = False,

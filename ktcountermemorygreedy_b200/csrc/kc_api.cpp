@@ -80,6 +80,7 @@ kc_tuning default_tuning()
     t.sampled_region_keys = 64ull << 20;
     t.count_shape = 1;
     t.part_shape = 1;
+    t.scatter_shape = 1;
     return t;
 }
 
@@ -996,7 +997,7 @@ void run_job_once(Job &job, cudaStream_t st, Workspace &ws, bool exact_census, c
                     BucketRanges *d_bs = ds.n<BucketRanges>(1);
                     CK(cudaMemcpyAsync(d_bs, hs.up(&bs, 1), sizeof(BucketRanges), cudaMemcpyHostToDevice, st));
                     CK(launch_subpart_scatter(keys, d_bs, n_sp_items, sub_next, d_sc, sub_cur, list, list_cap, max_sub,
-                                              st, sub_end));
+                                              st, sub_end, (uint32_t)tn.scatter_shape));
                     if (sampled)
                         CK(launch_subpart_sizes(sub_off, sub_cur, sub_end, n_sub, list_cap, sub_count,
                                                 counters + C_REGION_OVF, st));
@@ -2312,6 +2313,7 @@ int kc_set_tuning(kc_handle *h, const kc_tuning *t)
     if (t->record_sort > 2) return fail(KC_ERR_INVALID, "record_sort must be 1 or 2");
     if (t->count_shape > 4) return fail(KC_ERR_INVALID, "count_shape must be 1..4");
     if (t->part_shape > 2) return fail(KC_ERR_INVALID, "part_shape must be 1 or 2");
+    if (t->scatter_shape > 2) return fail(KC_ERR_INVALID, "scatter_shape must be 1 or 2");
     std::lock_guard<std::mutex> lk(h->mu);
     if (t->bucket_table_factor > 0) h->tuning.bucket_table_factor = t->bucket_table_factor;
     if (t->table_factor > 0) h->tuning.table_factor = t->table_factor;
@@ -2321,6 +2323,7 @@ int kc_set_tuning(kc_handle *h, const kc_tuning *t)
     if (t->sampled_region_keys > 0) h->tuning.sampled_region_keys = t->sampled_region_keys;
     if (t->count_shape > 0) h->tuning.count_shape = t->count_shape;
     if (t->part_shape > 0) h->tuning.part_shape = t->part_shape;
+    if (t->scatter_shape > 0) h->tuning.scatter_shape = t->scatter_shape;
     return KC_OK;
 }
 
@@ -2363,8 +2366,9 @@ int kc_autotune(kc_handle *h, const kc_job *jobs, uint32_t n_jobs, uint32_t batc
     if (rc == KC_OK) rc = run(cur, cur_ms);
     const double bucket_c[] = {2.0, 3.0, 4.0, 3.0}, table_c[] = {1.3, 1.6, 2.2, 1.6};
     const uint64_t group_c[] = {2ull << 20, 4ull << 20, 8ull << 20, 4ull << 20}, smem_c[] = {1, 2, 1, 1},
-                   sort_c[] = {1, 2, 1, 1}, shape_c[] = {1, 2, 3, 4}, part_c[] = {1, 2, 1, 1};
-    for (int param = 0; param < 7 && rc == KC_OK; ++param)
+                   sort_c[] = {1, 2, 1, 1}, shape_c[] = {1, 2, 3, 4}, part_c[] = {1, 2, 1, 1},
+                   scatter_c[] = {1, 2, 1, 1};
+    for (int param = 0; param < 8 && rc == KC_OK; ++param)
         for (int c = 0; c < 4 && rc == KC_OK; ++c) {
             kc_tuning t = cur;
             if (param == 0) t.bucket_table_factor = bucket_c[c];
@@ -2374,6 +2378,7 @@ int kc_autotune(kc_handle *h, const kc_job *jobs, uint32_t n_jobs, uint32_t batc
             if (param == 4) t.record_sort = sort_c[c];
             if (param == 5) t.count_shape = shape_c[c];
             if (param == 6) t.part_shape = part_c[c];
+            if (param == 7) t.scatter_shape = scatter_c[c];
             if (std::memcmp(&t, &cur, sizeof(t)) == 0) continue;
             rc = run(t, ms);
             if (rc == KC_OK && ms < 0.98 * cur_ms) {   // a clear gain only

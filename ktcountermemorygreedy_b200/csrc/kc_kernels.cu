@@ -1937,12 +1937,17 @@ constexpr uint32_t SP_PER_THREAD = SUB_SCATTER_ITEM_KEYS / SP_THREADS;
 constexpr uint32_t SP_MAX_BINS = (SUB_MAX_PER_BUCKET + SP_THREADS - 1) / SP_THREADS;   // sub-buckets per thread
 static_assert(SUB_SCATTER_ITEM_KEYS % SP_THREADS == 0 && SUB_SCATTER_ITEM_KEYS <= 65536, "item layout");
 
-__global__ void __launch_bounds__(SP_THREADS) k_subpart_scatter(const unsigned long long *keys, const BucketRanges *rg,
-                                                                uint32_t n_items, unsigned int *next_item,
-                                                                const SubCfg *sc, unsigned long long *sub_cursor,
-                                                                const unsigned long long *sub_end,
-                                                                unsigned long long *out, uint64_t out_cap,
-                                                                uint32_t max_sub)
+// MAXB: sub-buckets per thread in the rank scan (the cursor updates held in
+// registers until after the reorder); launches whose buckets have at most
+// 2 * SP_THREADS sub-buckets use MAXB = 2 and fit three blocks per SM.
+template <uint32_t MAXB, uint32_t BPSM>
+__global__ void __launch_bounds__(SP_THREADS, BPSM) k_subpart_scatter(const unsigned long long *keys,
+                                                                      const BucketRanges *rg, uint32_t n_items,
+                                                                      unsigned int *next_item, const SubCfg *sc,
+                                                                      unsigned long long *sub_cursor,
+                                                                      const unsigned long long *sub_end,
+                                                                      unsigned long long *out, uint64_t out_cap,
+                                                                      uint32_t max_sub)
 {
     // shared arrays per sub-bucket hold max_sub entries (the most of any
     // bucket of the launch)
@@ -1988,10 +1993,10 @@ __global__ void __launch_bounds__(SP_THREADS) k_subpart_scatter(const unsigned l
         uint32_t run = block_excl_scan_1024(local, s_warp, tot);
         // the sub-buckets' cursor updates are in flight during the reorder
         // and consumed only after it
-        unsigned long long cur[SP_MAX_BINS];
-        uint32_t first[SP_MAX_BINS];
+        unsigned long long cur[MAXB];
+        uint32_t first[MAXB];
 #pragma unroll
-        for (uint32_t j = 0; j < SP_MAX_BINS; ++j) {
+        for (uint32_t j = 0; j < MAXB; ++j) {
             const uint32_t s = b0 + j;
             cur[j] = 0ull;
             first[j] = run;
@@ -2014,7 +2019,7 @@ __global__ void __launch_bounds__(SP_THREADS) k_subpart_scatter(const unsigned l
         }
         // destination of sorted index i of sub-bucket s: s_dst[s] + i
 #pragma unroll
-        for (uint32_t j = 0; j < SP_MAX_BINS; ++j)
+        for (uint32_t j = 0; j < MAXB; ++j)
             if (j < per && b0 + j < c.n_sub) s_dst[b0 + j] = cur[j] - first[j];
         __syncthreads();
         for (uint32_t i = tid; i < n; i += SP_THREADS) {
@@ -2985,7 +2990,7 @@ static size_t subpart_scatter_smem(uint32_t max_sub)
 cudaError_t launch_subpart_scatter(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                    unsigned int *next_item, const SubCfg *sc, unsigned long long *sub_cursor,
                                    unsigned long long *out, uint64_t out_cap, uint32_t max_sub, cudaStream_t st,
-                                   const unsigned long long *sub_end)
+                                   const unsigned long long *sub_end, uint32_t scatter_shape)
 {
     if (!n_items) return cudaSuccess;
     if (!max_sub || max_sub > SUB_MAX_PER_BUCKET) return cudaErrorInvalidValue;
@@ -2993,16 +2998,16 @@ cudaError_t launch_subpart_scatter(const unsigned long long *keys, const BucketR
     cudaError_t e = cudaMemsetAsync(next_item, 0, 4, st);
     if (e != cudaSuccess) return e;
     const size_t smem = subpart_scatter_smem(max_sub);
-    e = cudaFuncSetAttribute(k_subpart_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    auto kern = (scatter_shape == 2 && max_sub <= 2 * SP_THREADS) ? k_subpart_scatter<2, 3>
+                                                                  : k_subpart_scatter<SP_MAX_BINS, 2>;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_subpart_scatter, SP_THREADS, smem) != cudaSuccess ||
-        per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SP_THREADS, smem) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     const uint32_t grid = std::min<uint32_t>(n_items, (uint32_t)(sm_count() * per_sm));
     note_launch();
-    k_subpart_scatter<<<grid, SP_THREADS, smem, st>>>(keys, rg, n_items, next_item, sc, sub_cursor, sub_end, out,
-                                                      out_cap, max_sub);
+    kern<<<grid, SP_THREADS, smem, st>>>(keys, rg, n_items, next_item, sc, sub_cursor, sub_end, out, out_cap, max_sub);
     return cudaGetLastError();
 }
 

@@ -315,7 +315,9 @@ cudaError_t launch_subpart_count(const unsigned long long *keys, const BucketRan
 cudaError_t launch_subpart_scatter(const unsigned long long *keys, const BucketRanges *rg, uint32_t n_items,
                                    unsigned int *next_item, const SubCfg *sc, unsigned long long *sub_cursor,
                                    unsigned long long *out, uint64_t out_cap, uint32_t max_sub, cudaStream_t st,
-                                   const unsigned long long *sub_end = nullptr);
+                                   const unsigned long long *sub_end = nullptr, uint32_t scatter_shape = 1);
+// scatter_shape 2 (kc_tuning.scatter_shape): launches whose buckets have at
+// most 1024 sub-buckets run a variant with fewer registers, three blocks per SM.
 // Estimated regions from a 1-in-stride sampled count: region (u32 per
 // sub-bucket, scratch), sub_off (their exclusive scan), sub_end = sub_off +
 // region, sub_cursor = sub_off.  scan_tmp holds scan_tmp_words(n_sub) words.

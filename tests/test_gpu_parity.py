@@ -588,12 +588,13 @@ def test_count_shapes_give_exact_results(kc, shape):
 @pytest.mark.parametrize("part_shape", [1, 2])
 def test_partition_round_sizes_give_exact_results(kc, part_shape):
     """The partition's two round sizes (kc_tuning.part_shape: 4096 or 2048
-    k-mers staged per round) on Bloom and large plain jobs: exact records."""
+    k-mers staged per round) and the sub-bucket scatter's two variants
+    (scatter_shape) on Bloom and large plain jobs: exact records."""
     import ktcountermemorygreedy_b200.synth as S
     fq = S.reads(S.genome(86, 2_000_000), 86, 60_000, (100, 150), 0.01, 0.0).tobytes()
     with kc.KmerCounter(max_inflight_jobs=1) as c:
-        c.set_tuning(part_shape=part_shape)
-        assert c.tuning["part_shape"] == part_shape
+        c.set_tuning(part_shape=part_shape, scatter_shape=part_shape)
+        assert c.tuning["part_shape"] == part_shape and c.tuning["scatter_shape"] == part_shape
         for kw in (dict(k=31, bloom=True, memory_gb=1, min_count=2), dict(k=25, bloom=True, memory_gb=1,
                                                                           min_count=2, pass_bytes=64 << 20),
                    dict(k=21)):
