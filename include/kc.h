@@ -301,8 +301,10 @@ int kc_sort_distinct_records(uint64_t *keys, uint32_t *counts, uint64_t n, uint3
  * device address (cudaGetSymbolAddress) and loads the array and the sort
  * kernels onto the device (with CUDA's default lazy module loading they would
  * otherwise be loaded, taking device memory, at first use); a call with n = 0
- * does only this set-up.  Make that first call before any stream capture.
- * Every call waits for its sort to finish on `stream` before returning.  All
+ * does only this set-up.  Every call waits for its sort to finish on
+ * `stream` before returning, so it cannot be part of a CUDA graph: on a
+ * stream that is being captured it returns KC_ERR_INVALID and enqueues
+ * nothing (make the first, set-up call before any capture).  All
  * calls share the one array: calls that overlap on the GPU (another host
  * thread, another stream) race and must be serialized by the caller. */
 #define KC_SORT_NOALLOC_MAX (1u << 20)

@@ -90,8 +90,18 @@ extern "C" int kc_sort_records_noalloc(uint64_t *d_keys, uint32_t *d_counts, uin
     void *scratch = nullptr;
     int rc = scratch_for_current_device(&scratch);
     if (rc != KC_OK) return rc;
-    if (n <= 1) return KC_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the call waits for its sort, which a stream being captured into a
+    // graph cannot do: refuse before enqueuing anything
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+        cudaGetLastError();
+        return kc::set_error(KC_ERR_CUDA, "kc_sort_records_noalloc: cannot query the stream's capture status");
+    }
+    if (cap != cudaStreamCaptureStatusNone)
+        return kc::set_error(KC_ERR_INVALID, "kc_sort_records_noalloc waits for its sort and cannot be called on a "
+                                             "stream that is being captured");
+    if (n <= 1) return KC_OK;
     // nothing in the scratch has to start at zero: every pass writes all the
     // digit counts, offsets and records it later reads
     cudaError_t e =
