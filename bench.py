@@ -901,7 +901,10 @@ def main():
     ap.add_argument("--no-served", dest="served", action="store_false")
     ap.add_argument("--served-jobs", type=int, default=200)
     ap.add_argument("--served-rates", type=float, nargs="+", default=[10.0, 50.0, 200.0])
-    ap.add_argument("--served-inflight", type=int, default=4)
+    # one job on the device at a time: each served job already fills the GPU, and concurrent jobs
+    # slowed each other (a 2000-job stream at 100-500 jobs/s: 3.7-4.0 G k-mers/s with one worker,
+    # 0.8-1.1 G with four)
+    ap.add_argument("--served-inflight", type=int, default=1)
     ap.add_argument("--served-pool-reads", type=int, default=4_000_000)
     ap.add_argument("--served-pinned-gb", type=int, default=24)
     ap.add_argument("--no-batched", dest="batched", action="store_false")
