@@ -1472,7 +1472,7 @@ void run_wide_job(Job &job, cudaStream_t st, Workspace &ws, const kc_tuning &tn)
     // a pass holds its table (slots per estimated distinct k-mer at the
     // handle's table factor) and its records (count pass, then the written
     // records); the final sort holds every record twice plus its temporaries
-    const uint64_t slot_bytes = 8ull * wide_slot_words(nw), rec_bytes = 8ull * nw + 4;
+    const uint64_t slot_bytes = 8ull * nw + 8, rec_bytes = 8ull * nw + 4;
     const double factor = std::max(tn.table_factor, 1.25);
     const uint64_t budget = P.pass_bytes ? P.pass_bytes : default_pass_budget(ws);
     std::vector<std::pair<uint32_t, uint32_t>> ranges;
@@ -1511,8 +1511,9 @@ void run_wide_job(Job &job, cudaStream_t st, Workspace &ws, const kc_tuning &tn)
         for (int attempt = 0;; ++attempt) {
             check_cancel(job, "before a counting pass");
             tab.cap = cap;
-            tab.slots = ds.n<unsigned long long>(cap * wide_slot_words(nw));
-            CK(launch_wide_init(k, tab, st));
+            tab.keys = ds.n<unsigned long long>(cap * nw);
+            tab.meta = ds.n<uint32_t>(cap * 2);
+            CK(launch_wide_init(tab, st));
             CK(cudaMemsetAsync(counters + C_FLAGS, 0, 8, st));
             CK(cudaMemsetAsync(counters + C_HIGH_LEN, 0, 8, st));
             a.table = tab;
@@ -1534,7 +1535,8 @@ void run_wide_job(Job &job, cudaStream_t st, Workspace &ws, const kc_tuning &tn)
                 break;
             }
             if (attempt >= 3) throw KcError{KC_ERR_DEVICE, "counting table overflow"};
-            ds.release(tab.slots);
+            ds.release(tab.meta);
+            ds.release(tab.keys);
             cap *= 2;
         }
         table_cap = std::max(table_cap, cap);

@@ -27,8 +27,9 @@ int merge_wide(const uint64_t *high_keys, const uint32_t *high_counts, uint64_t 
     const uint64_t total = n_high + n_low;
     WideTable t{};
     t.cap = std::max<uint64_t>(1024, (uint64_t)std::ceil((double)std::max<uint64_t>(total, 16) * 1.6));
-    t.slots = ds.n<unsigned long long>(t.cap * wide_slot_words(nw));
-    CK(launch_wide_init(k, t, st));
+    t.keys = ds.n<unsigned long long>(t.cap * nw);
+    t.meta = ds.n<uint32_t>(t.cap * 2);
+    CK(launch_wide_init(t, st));
     const uint32_t mp = (uint32_t)std::min<uint64_t>(t.cap, 1u << 16);
     if (n_high) {
         unsigned long long *hk = ds.n<unsigned long long>(n_high * nw);

@@ -123,17 +123,15 @@ template <uint32_t N>
 __device__ bool wide_add(const WideTable &t, const uint64_t (&key)[N], uint32_t c, uint32_t max_probe,
                          unsigned long long *flags)
 {
-    constexpr uint32_t S = WideSlot<N>::words;
     unsigned long long i = __umul64hi(wide_hash<N>(key), t.cap);
     for (uint32_t n = 0; n < max_probe; ++n) {
-        unsigned long long *sl = t.slots + i * S;
-        uint32_t *st = reinterpret_cast<uint32_t *>(sl + N);
+        uint32_t *st = t.meta + 2 * i;
         uint32_t s = ld_acquire(st);
         if (s == 0) {
             s = atomicCAS(st, 0u, 1u);
             if (s == 0) {
 #pragma unroll
-                for (uint32_t w = 0; w < N; ++w) sl[w] = key[w];
+                for (uint32_t w = 0; w < N; ++w) t.keys[i * N + w] = key[w];
                 st_release(st, 2u);   // the key words are visible before the state says so
                 atomicAdd(st + 1, c);
                 return true;
@@ -151,13 +149,9 @@ __device__ bool wide_add(const WideTable &t, const uint64_t (&key)[N], uint32_t 
                 return true;
             }
         }
-        // the key words share the state's sector: an L2 hit after the acquire
         bool eq = true;
 #pragma unroll
-        for (uint32_t w = 0; w < N; w += 2) {
-            const ulonglong2 kw = __ldcg(reinterpret_cast<const ulonglong2 *>(sl + w));
-            eq = eq && kw.x == key[w] && kw.y == key[w + 1];
-        }
+        for (uint32_t w = 0; w < N; ++w) eq = eq && (__ldcg(&t.keys[i * N + w]) == key[w]);
         if (eq) {
             atomicAdd(st + 1, c);
             return true;
@@ -414,15 +408,11 @@ cudaError_t launch_wide_extract_t(uint32_t k, const WideArgs &a, cudaStream_t st
     return cudaGetLastError();
 }
 
-// Every slot zeroed (state 0: empty), whole slots so each sector is written once.
 template <uint32_t N>
 __global__ void __launch_bounds__(256) k_wide_init(WideTable t)
 {
-    constexpr uint32_t V = WideSlot<N>::words / 2;   // 16-byte stores per slot
-    const uint64_t n = t.cap * V;
-    uint4 *p = reinterpret_cast<uint4 *>(t.slots);
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        p[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < t.cap; i += (uint64_t)gridDim.x * blockDim.x)
+        reinterpret_cast<uint2 *>(t.meta)[i] = make_uint2(0u, 0u);
 }
 
 template <uint32_t N>
@@ -446,7 +436,6 @@ __global__ void __launch_bounds__(256) k_wide_compact(WideTable t, uint32_t coun
                                                       uint32_t *ovf, uint64_t ovf_cap, unsigned long long *counters,
                                                       int count_only)
 {
-    constexpr uint32_t S = WideSlot<N>::words;
     __shared__ uint32_t s_hist[2048];
     if (!count_only)
         for (int i = threadIdx.x; i < 2048; i += blockDim.x) s_hist[i] = 0;
@@ -460,7 +449,7 @@ __global__ void __launch_bounds__(256) k_wide_compact(WideTable t, uint32_t coun
         bool keep = false;
         uint32_t c = 0;
         if (i < t.cap) {
-            const uint2 m = *reinterpret_cast<const uint2 *>(t.slots + i * S + N);
+            const uint2 m = reinterpret_cast<const uint2 *>(t.meta)[i];
             if (m.x == 2u) {
                 ++distinct;
                 c = m.y < count_max ? m.y : count_max;
@@ -488,7 +477,7 @@ __global__ void __launch_bounds__(256) k_wide_compact(WideTable t, uint32_t coun
                     const unsigned long long pos = base + (unsigned)__popc(b & lanes_lt());
                     if (pos < rec_cap) {
 #pragma unroll
-                        for (uint32_t w = 0; w < N; ++w) rec_keys[pos * N + w] = t.slots[i * S + w];
+                        for (uint32_t w = 0; w < N; ++w) rec_keys[pos * N + w] = t.keys[i * N + w];
                         rec_counts[pos] = c;
                     } else {
                         atomicOr(&counters[C_FLAGS], ERR_RECORDS_FULL);
@@ -608,15 +597,11 @@ cudaError_t launch_wide_extract(int mode, uint32_t k, const WideArgs &a, cudaStr
     return launch_wide_extract_t<4, WMODE_EMIT>(k, a, st);
 }
 
-cudaError_t launch_wide_init(uint32_t k, WideTable t, cudaStream_t st)
+cudaError_t launch_wide_init(WideTable t, cudaStream_t st)
 {
     if (!t.cap) return cudaSuccess;
     note_kernel_launch();
-    const uint64_t v = t.cap * (wide_slot_words(key_words(k)) / 2);
-    if (key_words(k) == 2)
-        k_wide_init<2><<<wide_grid(v, 256), 256, 0, st>>>(t);
-    else
-        k_wide_init<4><<<wide_grid(v, 256), 256, 0, st>>>(t);
+    k_wide_init<1><<<wide_grid(t.cap, 256), 256, 0, st>>>(t);
     return cudaGetLastError();
 }
 

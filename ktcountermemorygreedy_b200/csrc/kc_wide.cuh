@@ -20,22 +20,11 @@ inline uint32_t key_words(uint32_t k) { return k <= 32 ? 1u : (k <= 64 ? 2u : 4u
 // state (0 -> 1), its key written and then published (state 2, release);
 // every other thread compares keys only in published slots.  A thread that
 // meets a claimed, unpublished slot waits for it (bounded, ERR_WAIT_TIMEOUT).
-//
-// Slot i is slots[i * S .. i * S + S), S = N + 1 rounded up to a power of two:
-// the key words first, then one word holding the state (low 32 bits) and the
-// count (high 32 bits), then padding.  A slot is one 32-byte sector (N = 2)
-// or one aligned 64-byte half line (N = 4), so a probe reads its state, key
-// and count from one place in DRAM.
 struct WideTable {
-    unsigned long long *slots;  // cap * S words
+    unsigned long long *keys;   // cap * N words, slot i at keys[i * N]
+    uint32_t *meta;             // 2 words per slot: state, count
     unsigned long long cap;
 };
-
-template <uint32_t N>
-struct WideSlot {
-    static constexpr uint32_t words = N <= 1 ? 2u : (N <= 3 ? 4u : 8u);
-};
-inline uint32_t wide_slot_words(uint32_t nw) { return nw <= 1 ? 2u : (nw <= 3 ? 4u : 8u); }
 
 enum WideMode : int { WMODE_SCAN = 0, WMODE_INSERT = 1, WMODE_EMIT = 2 };
 
@@ -60,7 +49,7 @@ struct WideArgs {
 };
 
 cudaError_t launch_wide_extract(int mode, uint32_t k, const WideArgs &a, cudaStream_t st);
-cudaError_t launch_wide_init(uint32_t k, WideTable t, cudaStream_t st);
+cudaError_t launch_wide_init(WideTable t, cudaStream_t st);
 // (key, count) records into the table (the tools' merge: high.bin records
 // with their counts, low.bin k-mers with count 1).
 cudaError_t launch_wide_insert_pairs(uint32_t k, const unsigned long long *keys, const uint32_t *counts,
