@@ -1512,8 +1512,8 @@ void run_wide_job(Job &job, cudaStream_t st, Workspace &ws, const kc_tuning &tn)
             check_cancel(job, "before a counting pass");
             tab.cap = cap;
             tab.keys = ds.n<unsigned long long>(cap * nw);
-            tab.meta = ds.n<uint32_t>(cap * 2);
-            CK(launch_wide_init(tab, st));
+            tab.meta = ds.n<uint32_t>(cap * 2 + 2);
+            CK(launch_wide_init(k, tab, st));
             CK(cudaMemsetAsync(counters + C_FLAGS, 0, 8, st));
             CK(cudaMemsetAsync(counters + C_HIGH_LEN, 0, 8, st));
             a.table = tab;

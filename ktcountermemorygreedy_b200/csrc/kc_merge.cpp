@@ -28,8 +28,8 @@ int merge_wide(const uint64_t *high_keys, const uint32_t *high_counts, uint64_t 
     WideTable t{};
     t.cap = std::max<uint64_t>(1024, (uint64_t)std::ceil((double)std::max<uint64_t>(total, 16) * 1.6));
     t.keys = ds.n<unsigned long long>(t.cap * nw);
-    t.meta = ds.n<uint32_t>(t.cap * 2);
-    CK(launch_wide_init(t, st));
+    t.meta = ds.n<uint32_t>(t.cap * 2 + 2);
+    CK(launch_wide_init(k, t, st));
     const uint32_t mp = (uint32_t)std::min<uint64_t>(t.cap, 1u << 16);
     if (n_high) {
         unsigned long long *hk = ds.n<unsigned long long>(n_high * nw);

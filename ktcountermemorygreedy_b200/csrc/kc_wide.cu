@@ -99,6 +99,36 @@ __device__ __forceinline__ void st_release(uint32_t *p, uint32_t v)
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// One 16-byte slot read as a single access (relaxed, device scope).
+__device__ __forceinline__ ulonglong2 ld_slot128(const ulonglong2 *p)
+{
+    ulonglong2 v;
+    asm volatile("{\n\t.reg .b128 d;\n\t"
+                 "ld.relaxed.gpu.global.b128 d, [%2];\n\t"
+                 "mov.b128 {%0, %1}, d;\n\t}"
+                 : "=l"(v.x), "=l"(v.y)
+                 : "l"(p)
+                 : "memory");
+    return v;
+}
+
+// 16-byte compare-and-swap: writes val where *p == cmp; returns the old slot.
+__device__ __forceinline__ ulonglong2 cas_slot128(ulonglong2 *p, ulonglong2 cmp, ulonglong2 val)
+{
+    ulonglong2 old;
+    asm volatile("{\n\t.reg .b128 d, c, v;\n\t"
+                 "mov.b128 c, {%3, %4};\n\t"
+                 "mov.b128 v, {%5, %6};\n\t"
+                 "atom.relaxed.gpu.global.cas.b128 d, [%2], c, v;\n\t"
+                 "mov.b128 {%0, %1}, d;\n\t}"
+                 : "=l"(old.x), "=l"(old.y)
+                 : "l"(p), "l"(cmp.x), "l"(cmp.y), "l"(val.x), "l"(val.y)
+                 : "memory");
+    return old;
+}
+
+constexpr unsigned long long WIDE_EMPTY = ~0ull;   // both words of an empty 16-byte slot
+
 // Placement hash of an N-word key (table slots, HyperLogLog); never affects a count.
 template <uint32_t N>
 __device__ __forceinline__ uint64_t wide_hash(const uint64_t (&key)[N])
@@ -124,41 +154,67 @@ __device__ bool wide_add(const WideTable &t, const uint64_t (&key)[N], uint32_t 
                          unsigned long long *flags)
 {
     unsigned long long i = __umul64hi(wide_hash<N>(key), t.cap);
-    for (uint32_t n = 0; n < max_probe; ++n) {
-        uint32_t *st = t.meta + 2 * i;
-        uint32_t s = ld_acquire(st);
-        if (s == 0) {
-            s = atomicCAS(st, 0u, 1u);
+    if constexpr (N == 2) {
+        if (key[0] == WIDE_EMPTY && key[1] == WIDE_EMPTY) {
+            atomicAdd(&t.meta[t.cap], c);
+            atomicOr(&t.meta[t.cap + 1], 1u);
+            return true;
+        }
+        const ulonglong2 want = make_ulonglong2(key[0], key[1]);
+        const ulonglong2 empty = make_ulonglong2(WIDE_EMPTY, WIDE_EMPTY);
+        ulonglong2 *slots = reinterpret_cast<ulonglong2 *>(t.keys);
+        for (uint32_t n = 0; n < max_probe; ++n) {
+            // a slot goes from empty to one key once and never changes again
+            ulonglong2 v = ld_slot128(slots + i);
+            bool vacant = v.x == WIDE_EMPTY && v.y == WIDE_EMPTY;
+            if (vacant) {
+                v = cas_slot128(slots + i, empty, want);
+                vacant = v.x == WIDE_EMPTY && v.y == WIDE_EMPTY;   // claimed by this thread
+            }
+            if (vacant || (v.x == want.x && v.y == want.y)) {
+                atomicAdd(&t.meta[i], c);
+                return true;
+            }
+            i = (i + 1 == t.cap) ? 0 : i + 1;
+        }
+        return false;
+    } else {
+        for (uint32_t n = 0; n < max_probe; ++n) {
+            uint32_t *st = t.meta + 2 * i;
+            uint32_t s = ld_acquire(st);
             if (s == 0) {
+                s = atomicCAS(st, 0u, 1u);
+                if (s == 0) {
 #pragma unroll
-                for (uint32_t w = 0; w < N; ++w) t.keys[i * N + w] = key[w];
-                st_release(st, 2u);   // the key words are visible before the state says so
+                    for (uint32_t w = 0; w < N; ++w) t.keys[i * N + w] = key[w];
+                    st_release(st, 2u);   // the key words are visible before the state says so
+                    atomicAdd(st + 1, c);
+                    return true;
+                }
+            }
+            if (s == 1) {
+                // another thread is writing this slot's key: a few stores away
+                uint32_t it = 0;
+                do {
+                    __nanosleep(32);
+                    s = ld_acquire(st);
+                } while (s == 1 && ++it < SPIN_LIMIT);
+                if (s == 1) {
+                    atomicOr(flags, ERR_WAIT_TIMEOUT);
+                    return true;
+                }
+            }
+            bool eq = true;
+#pragma unroll
+            for (uint32_t w = 0; w < N; ++w) eq = eq && (__ldcg(&t.keys[i * N + w]) == key[w]);
+            if (eq) {
                 atomicAdd(st + 1, c);
                 return true;
             }
+            i = (i + 1 == t.cap) ? 0 : i + 1;
         }
-        if (s == 1) {
-            // another thread is writing this slot's key: a few stores away
-            uint32_t it = 0;
-            do {
-                __nanosleep(32);
-                s = ld_acquire(st);
-            } while (s == 1 && ++it < SPIN_LIMIT);
-            if (s == 1) {
-                atomicOr(flags, ERR_WAIT_TIMEOUT);
-                return true;
-            }
-        }
-        bool eq = true;
-#pragma unroll
-        for (uint32_t w = 0; w < N; ++w) eq = eq && (__ldcg(&t.keys[i * N + w]) == key[w]);
-        if (eq) {
-            atomicAdd(st + 1, c);
-            return true;
-        }
-        i = (i + 1 == t.cap) ? 0 : i + 1;
+        return false;
     }
-    return false;
 }
 
 // The 32 codes of positions e-31..e (e >= 31), position e at bits 62..63.
@@ -408,11 +464,15 @@ cudaError_t launch_wide_extract_t(uint32_t k, const WideArgs &a, cudaStream_t st
     return cudaGetLastError();
 }
 
+// N = 2: every key slot all ones, every count 0; N = 4: every state and count 0.
 template <uint32_t N>
 __global__ void __launch_bounds__(256) k_wide_init(WideTable t)
 {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < t.cap; i += (uint64_t)gridDim.x * blockDim.x)
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= t.cap; i += (uint64_t)gridDim.x * blockDim.x) {
         reinterpret_cast<uint2 *>(t.meta)[i] = make_uint2(0u, 0u);
+        if (N == 2 && i < t.cap)
+            reinterpret_cast<ulonglong2 *>(t.keys)[i] = make_ulonglong2(WIDE_EMPTY, WIDE_EMPTY);
+    }
 }
 
 template <uint32_t N>
@@ -442,17 +502,34 @@ __global__ void __launch_bounds__(256) k_wide_compact(WideTable t, uint32_t coun
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    const uint64_t rounds = (t.cap + stride - 1) / stride;
+    // N = 2 also visits index cap: the all-ones key's own count
+    const uint64_t n_slots = t.cap + (N == 2 ? 1 : 0);
+    const uint64_t rounds = (n_slots + stride - 1) / stride;
     uint32_t distinct = 0, kept = 0;
     for (uint64_t r = 0; r < rounds; ++r) {
         const uint64_t i = r * stride + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
         bool keep = false;
         uint32_t c = 0;
-        if (i < t.cap) {
-            const uint2 m = reinterpret_cast<const uint2 *>(t.meta)[i];
-            if (m.x == 2u) {
+        if (i < n_slots) {
+            bool used;
+            uint32_t cnt;
+            if (N == 2) {
+                if (i < t.cap) {
+                    const ulonglong2 kw = reinterpret_cast<const ulonglong2 *>(t.keys)[i];
+                    used = !(kw.x == WIDE_EMPTY && kw.y == WIDE_EMPTY);
+                    cnt = used ? t.meta[i] : 0u;
+                } else {
+                    used = t.meta[t.cap + 1] != 0u;
+                    cnt = t.meta[t.cap];
+                }
+            } else {
+                const uint2 m = reinterpret_cast<const uint2 *>(t.meta)[i];
+                used = m.x == 2u;
+                cnt = m.y;
+            }
+            if (used) {
                 ++distinct;
-                c = m.y < count_max ? m.y : count_max;
+                c = cnt < count_max ? cnt : count_max;
                 keep = c >= min_count && c <= max_count;
                 if (!count_only) {
                     if (c < 2048) atomicAdd(&s_hist[c], 1u);
@@ -477,7 +554,7 @@ __global__ void __launch_bounds__(256) k_wide_compact(WideTable t, uint32_t coun
                     const unsigned long long pos = base + (unsigned)__popc(b & lanes_lt());
                     if (pos < rec_cap) {
 #pragma unroll
-                        for (uint32_t w = 0; w < N; ++w) rec_keys[pos * N + w] = t.keys[i * N + w];
+                        for (uint32_t w = 0; w < N; ++w) rec_keys[pos * N + w] = i < t.cap ? t.keys[i * N + w] : WIDE_EMPTY;
                         rec_counts[pos] = c;
                     } else {
                         atomicOr(&counters[C_FLAGS], ERR_RECORDS_FULL);
@@ -597,11 +674,14 @@ cudaError_t launch_wide_extract(int mode, uint32_t k, const WideArgs &a, cudaStr
     return launch_wide_extract_t<4, WMODE_EMIT>(k, a, st);
 }
 
-cudaError_t launch_wide_init(WideTable t, cudaStream_t st)
+cudaError_t launch_wide_init(uint32_t k, WideTable t, cudaStream_t st)
 {
     if (!t.cap) return cudaSuccess;
     note_kernel_launch();
-    k_wide_init<1><<<wide_grid(t.cap, 256), 256, 0, st>>>(t);
+    if (key_words(k) == 2)
+        k_wide_init<2><<<wide_grid(t.cap + 1, 256), 256, 0, st>>>(t);
+    else
+        k_wide_init<4><<<wide_grid(t.cap + 1, 256), 256, 0, st>>>(t);
     return cudaGetLastError();
 }
 

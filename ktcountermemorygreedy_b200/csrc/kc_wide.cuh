@@ -16,13 +16,27 @@ constexpr uint32_t WIDE_HALO = 128;   // bytes before a tile read with it: k - 1
 
 inline uint32_t key_words(uint32_t k) { return k <= 32 ? 1u : (k <= 64 ? 2u : 4u); }
 
-// Open-addressing table of N-word keys.  A slot is claimed by one CAS of its
-// state (0 -> 1), its key written and then published (state 2, release);
-// every other thread compares keys only in published slots.  A thread that
-// meets a claimed, unpublished slot waits for it (bounded, ERR_WAIT_TIMEOUT).
+// Open-addressing table of N-word keys.
+//
+// N = 2: a slot is its key, one 16-byte word, all ones when empty (never a
+// canonical key: k < 64 leaves low bits of data[1] zero, and at k = 64 the
+// all-T key's reverse complement, all A, is smaller).  A probe reads the slot
+// with one 128-bit load; an empty slot is claimed by one 128-bit CAS that
+// writes the whole key, so no reader can see half a key and nothing waits.
+// meta[i] is slot i's count; meta[cap] / meta[cap + 1] hold the count / the
+// presence of the all-ones key itself, which only a merge of foreign records
+// can bring.
+//
+// N = 4: a slot is claimed by one CAS of its state (0 -> 1), its key written
+// and then published (state 2, release); every other thread compares keys
+// only in published slots.  A thread that meets a claimed, unpublished slot
+// waits for it (bounded, ERR_WAIT_TIMEOUT).  meta[2i], meta[2i + 1] = state,
+// count of slot i.
+//
+// keys holds cap * N words (slot i at keys[i * N]), meta 2 * cap + 2 words.
 struct WideTable {
-    unsigned long long *keys;   // cap * N words, slot i at keys[i * N]
-    uint32_t *meta;             // 2 words per slot: state, count
+    unsigned long long *keys;
+    uint32_t *meta;
     unsigned long long cap;
 };
 
@@ -49,7 +63,7 @@ struct WideArgs {
 };
 
 cudaError_t launch_wide_extract(int mode, uint32_t k, const WideArgs &a, cudaStream_t st);
-cudaError_t launch_wide_init(WideTable t, cudaStream_t st);
+cudaError_t launch_wide_init(uint32_t k, WideTable t, cudaStream_t st);
 // (key, count) records into the table (the tools' merge: high.bin records
 // with their counts, low.bin k-mers with count 1).
 cudaError_t launch_wide_insert_pairs(uint32_t k, const unsigned long long *keys, const uint32_t *counts,
