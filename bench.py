@@ -17,8 +17,11 @@ A step is one counting job over the whole FASTQ:
            the host clock.
 --impl reference times the reference's own CPU programs (compiled from its
 sources into oracle/_ref, or the directory KC_REF_BIN names) on a bounded
-sample of the same workload; where they are absent it times the oracle's C
-restatement of the path instead ("kind": "port").
+sample of the same workload (the first --ref-reads reads): kmer_counter and
+histogram_tool precise, i.e. the records seen at least twice (high.bin) and
+the histogram, the same outputs as a job here less the sort; where they are
+absent it times the oracle's C restatement of the path instead ("kind":
+"port").  Both arms print the same "config".
 
 Multi-GPU: the path is run as independent replicas (one job per GPU); value is
 all replicas' k-mers over the slowest replica's time.
@@ -43,6 +46,32 @@ sys.path.insert(0, ROOT)
 U32 = 0xFFFFFFFF
 METRIC = "k-mers counted/s (bit-exact)"
 MEMORY_GB = 64          # reference <memory_limit_gb>: sizes the Bloom filters
+READ_LEN = 150
+WORKLOAD = ("single large job (100 Mbp genome, 5% repeats from 200 families, 30x 150 bp, 1% errors, k=31, "
+            "Bloom singleton filter, min count 2)")
+
+
+def large_job_fastq_bytes(n_reads: int) -> int:
+    """Bytes of the generator's FASTQ of n_reads reads of READ_LEN bases:
+    "@r<i>\n", the bases, "\n+\n", the qualities, "\n" for i = 0 .. n - 1."""
+    digits, lo, width = 0, 0, 1
+    while lo < n_reads:
+        hi = min(n_reads, 10 ** width)
+        digits += (hi - lo) * width
+        lo, width = hi, width + 1
+    return n_reads * (2 * READ_LEN + 7) + digits
+
+
+def workload_config(scale: float, world: int) -> dict:
+    """The "config" object of both arms' lines: the large job at this scale
+    (genome, reads, FASTQ bytes, occurrences; the reads carry no N, so every
+    read holds READ_LEN - 31 + 1 windows)."""
+    genome_len = max(1_000_000, int(100_000_000 * scale))
+    n_reads = int(math.ceil(30.0 * genome_len / READ_LEN))
+    return {"workload": WORKLOAD, "genome_bp": genome_len, "reads": n_reads,
+            "fastq_bytes": large_job_fastq_bytes(n_reads), "occurrences_per_step": n_reads * (READ_LEN - 31 + 1),
+            "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (FASTQ > 126 MB)",
+            "memory_gb": MEMORY_GB, "scale": scale}
 
 
 def peaks():
@@ -188,10 +217,13 @@ def reference_programs_present() -> bool:
                for p in ("kmer_counter", "histogram_tool", "dump_tool"))
 
 
-def reference_run(fastq_path: str, threads: int, mem_gb: int, tmp: str, dump: bool = True):
-    """kmer_counter + histogram_tool precise (min 2) + dump_tool precise --sort
-    (min 1), as the reference is used; returns (wall seconds, occurrences).
-    The histogram is left in tmp/h.tsv and the dump in tmp/d.txt."""
+def reference_run(fastq_path: str, threads: int, mem_gb: int, tmp: str, dump: bool = False):
+    """kmer_counter + histogram_tool precise (min 2), timed: the records seen
+    at least twice (high.bin) and the histogram.  dump: then, untimed,
+    dump_tool precise --sort (min 1: the tool's output above min 1 is not
+    deterministic), for a byte comparison.  Returns (wall seconds of the
+    timed programs, occurrences); the histogram is left in tmp/h.tsv and the
+    dump in tmp/d.txt."""
     ref = reference_dir()
     d = os.path.join(tmp, "t")
     shutil.rmtree(d, ignore_errors=True)
@@ -203,10 +235,10 @@ def reference_run(fastq_path: str, threads: int, mem_gb: int, tmp: str, dump: bo
         raise RuntimeError(f"reference kmer_counter failed: {p.stderr[-500:]}")
     subprocess.run([os.path.join(ref, "histogram_tool"), "precise", d, str(threads), str(mem_gb),
                     os.path.join(tmp, "h.tsv"), "2", "10000"], check=True, capture_output=True)
+    wall = time.perf_counter() - t0
     if dump:
         subprocess.run([os.path.join(ref, "dump_tool"), "precise", d, str(threads), str(mem_gb),
                         os.path.join(tmp, "d.txt"), "1", str(U32), "--sort"], check=True, capture_output=True)
-    wall = time.perf_counter() - t0
     occ = 0
     for line in p.stdout.splitlines():
         if line.startswith("Total read k-mer count:"):
@@ -232,11 +264,12 @@ def port_run(fastq_path: str):
     return time.perf_counter() - t0, len(keys)
 
 
-def cpu_sample_run(path: str, threads: int, mem_gb: int, tmp: str):
+def cpu_sample_run(path: str, threads: int, mem_gb: int, tmp: str, dump: bool = False):
     """(wall seconds, occurrences, kind, cores, what ran) for one sample."""
     if reference_programs_present():
-        w, occ = reference_run(path, threads, mem_gb, tmp)
-        return w, occ, "reference", threads, "counter + precise tools"
+        w, occ = reference_run(path, threads, mem_gb, tmp, dump=dump)
+        return w, occ, "reference", threads, ("kmer_counter + histogram_tool precise: the records seen at least "
+                                                "twice (high.bin) and the histogram")
     w, occ = port_run(path)
     return w, occ, "port", 1, "oracle port (extraction, exact counts, sort, histogram), one thread"
 
@@ -292,8 +325,7 @@ def run_reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "k-mers/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": "single large job (100 Mbp genome, 5% repeats, 30x 150 bp, k=31, Bloom, min count 2)",
-                   "sample_reads": args.ref_reads},
+        "config": workload_config(args.scale, int(os.environ.get("WORLD_SIZE", "1"))),
         "cpu_baseline": {"value": value, "unit": "k-mers/s", "cores": cores, "kind": kind,
                          "sample": sample, "cpu": model},
         "e2e": {"value": value, "unit": "k-mers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -383,6 +415,12 @@ def full_reference_check(args, counter, fq, full):
 
 
 def cpu_leg(args, counter, fq, full):
+    """cpu_baseline: the reference programs (or the oracle port) timed on the
+    first --ref-reads reads, and the GPU on the same file (sample_value);
+    parity: the GPU's histogram text and sorted dump against the reference
+    programs' on the first --parity-reads reads (their dump lists every
+    k-mer, singletons included, so its sample is the smaller one), and the
+    whole job against the oracle's hash sample."""
     import ktcountermemorygreedy_b200 as kc
     SP = _checker()
     threads, model = cpu_info()
@@ -396,12 +434,18 @@ def cpu_leg(args, counter, fq, full):
             cpu = {"value": o / w, "unit": "k-mers/s", "cores": cores, "kind": kind,
                    "sample": f"first {args.ref_reads} reads of the workload ({nbytes} B, {o} k-mers), "
                              f"{what}, {model}"}
-            sample_value, res = sample_on_gpu(counter, kc, path)
+            sample_value, _ = sample_on_gpu(counter, kc, path)
+            os.unlink(path)
             if kind == "reference":
+                ppath = os.path.join(tmp, "parity.fq")
+                write_workload(ppath, args.parity_reads)
+                reference_run(ppath, max(6, threads), mem, tmp, dump=True)
+                res = counter.count([open(ppath, "rb").read()], keep_records=True, **JOB)
                 chk = SP.reference_outputs_match(kc.histogram_text(res.hist, JOB["hist_min"]),
                                                  kc.dump_bytes(res.keys, res.counts, JOB["k"]),
                                                  os.path.join(tmp, "h.tsv"), os.path.join(tmp, "d.txt"),
                                                  JOB["k"], JOB["min_count"])
+                chk["reads"] = args.parity_reads
                 parity["sample"] = "identical" if chk["identical"] else "DIFFERENT"
                 parity["sample_detail"] = chk
             else:
@@ -866,16 +910,15 @@ def run_ours(args):
     if rank == 0 and world == 1 and args.batched:
         batched = batched_bench(kc, args, local)
     if rank == 0:
+        config = workload_config(args.scale, world)
+        # the measured job, should the generator ever differ from the formula
+        config.update(genome_bp=genome_len, reads=n_reads, fastq_bytes=len(fq),
+                      occurrences_per_step=results[0].occurrences)
         line = {
             "metric": METRIC, "value": value, "unit": "k-mers/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": "single large job (100 Mbp genome, 5% repeats from 200 families, 30x 150 bp, "
-                                   "1% errors, k=31, Bloom singleton filter, min count 2)",
-                       "genome_bp": genome_len, "reads": n_reads, "fastq_bytes": len(fq),
-                       "occurrences_per_step": results[0].occurrences, "records": results[0].n_records_total,
-                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (FASTQ > 126 MB)",
-                       "memory_gb": MEMORY_GB, "scale": args.scale, "tuning": tuning},
+            "config": config, "records": results[0].n_records_total, "tuning": tuning,
             "e2e": {"value": e2e_val, "unit": "k-mers/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roof, "cpu_baseline": cpu, "sample_value": sample_value, "parity": parity,
             "clocks": clocks, "gpu_launches": int(launches),
@@ -896,7 +939,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="genome size factor (1.0 = the 100 Mbp workload)")
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--ref-reads", type=int, default=1_000_000)
+    # the CPU baseline's sample: 4M reads (1.25 GB, 480M k-mers), large enough that the reference's
+    # fixed start-up (its memory map, the pre-pass) is a small share of a step
+    ap.add_argument("--ref-reads", type=int, default=4_000_000)
+    ap.add_argument("--parity-reads", type=int, default=1_000_000,
+                    help="reads of the sample whose histogram and sorted dump are compared with the reference's")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-served", dest="served", action="store_false")
     ap.add_argument("--served-jobs", type=int, default=200)
