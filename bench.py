@@ -696,27 +696,35 @@ def wide_bench(kc, args, counter, inp, fq):
     records whose hash sample is checked against the oracle (CPU leg)."""
     out = {}
     for k in args.wide:
-        job = dict(JOB, k=k)
-        counter.count(input=inp, keep_records=False, **job)
-        rs = [counter.count(input=inp, keep_records=False, **job) for _ in range(3)]
-        dev = sum(r.device_ms for r in rs) / len(rs)
-        r0 = rs[-1]
-        o = {"k": k, "key_words": kc.key_words(k), "occurrences": r0.occurrences, "device_ms": dev,
-             "kmers_per_s": r0.occurrences / (dev / 1000.0), "records": r0.n_records_total, "passes": r0.passes,
-             "stages_ms": {kc.PHASES[i]: r0.phase_ms[i] for i in range(len(kc.PHASES)) if r0.phase_ms[i] > 0}}
-        if args.cpu_baseline:
-            try:
-                r = counter.count(input=inp, keep_records=True, copy=False, **job)
-                threads, _ = cpu_info()
-                chk = _checker().full_spot_check_wide(fq, k, r.keys, r.counts, r.hist, JOB["hist_min"],
-                                                      JOB["min_count"], threads=max(1, threads), sample_bits=8)
-                o["parity"] = "identical" if chk["identical"] else "DIFFERENT"
-                o["parity_detail"] = chk
-                del r
-            except Exception as e:
-                o["parity"] = f"failed: {e}"
-        out[str(k)] = o
+        try:
+            out[str(k)] = wide_one(kc, args, counter, inp, fq, k)
+        except Exception as e:   # reported in the line, never fatal to the headline
+            out[str(k)] = {"k": k, "failed": str(e)}
     return out
+
+
+def wide_one(kc, args, counter, inp, fq, k):
+    """One k of wide_bench."""
+    job = dict(JOB, k=k)
+    counter.count(input=inp, keep_records=False, **job)
+    rs = [counter.count(input=inp, keep_records=False, **job) for _ in range(3)]
+    dev = sum(r.device_ms for r in rs) / len(rs)
+    r0 = rs[-1]
+    o = {"k": k, "key_words": kc.key_words(k), "occurrences": r0.occurrences, "device_ms": dev,
+         "kmers_per_s": r0.occurrences / (dev / 1000.0), "records": r0.n_records_total, "passes": r0.passes,
+         "stages_ms": {kc.PHASES[i]: r0.phase_ms[i] for i in range(len(kc.PHASES)) if r0.phase_ms[i] > 0}}
+    if args.cpu_baseline:
+        try:
+            r = counter.count(input=inp, keep_records=True, copy=False, **job)
+            threads, _ = cpu_info()
+            chk = _checker().full_spot_check_wide(fq, k, r.keys, r.counts, r.hist, JOB["hist_min"],
+                                                  JOB["min_count"], threads=max(1, threads), sample_bits=8)
+            o["parity"] = "identical" if chk["identical"] else "DIFFERENT"
+            o["parity_detail"] = chk
+            del r
+        except Exception as e:
+            o["parity"] = f"failed: {e}"
+    return o
 
 
 def out_of_core_bench(kc, args, local):
@@ -959,8 +967,8 @@ def main():
     ap.add_argument("--batch-scale", type=float, default=0.125)
     ap.add_argument("--tuning", nargs="*", default=[],
                     help="handle settings name=value (kc_tuning fields) instead of the autotuner's")
-    ap.add_argument("--wide", type=int, nargs="*", default=[],
-                    help="also time k-mers of more than 32 bases (e.g. 63 127) on the same workload")
+    ap.add_argument("--wide", type=int, nargs="*", default=[63, 127],
+                    help="also time k-mers of more than 32 bases on the same workload (none: --wide)")
     ap.add_argument("--out-of-core", action="store_true",
                     help="also run the out-of-core job (3.1 Gbp, 10x, 65 GB FASTQ; minutes, host memory ~100 GB)")
     ap.add_argument("--ooc-scale", type=float, default=1.0, help="genome size factor of the out-of-core job")
