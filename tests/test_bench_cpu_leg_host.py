@@ -1,6 +1,7 @@
-"""bench.py's CPU leg on the CPU: the reference programs timed on one sample
-(counter + histogram, no text), their histogram and sorted dump compared
-with a job's on a second, smaller sample, and the whole-job hash-sample check.
+"""bench.py's CPU leg and k > 32 leg on the CPU: the reference programs
+timed on one sample (counter + histogram, no text), their histogram and
+sorted dump compared with a job's on a second, smaller sample, the whole-job
+hash-sample check, and the k > 32 entries with their hash-sample checks.
 The GPU job is stood in for by the oracle (exact counts, records in printed
 order, histogram) and the device-side steps (the GPU's own timing of the
 sample, the dump formatted on the device) by host equivalents, so that the
@@ -86,3 +87,48 @@ def test_reference_run_times_counter_and_histogram_only(tmp_path):
     assert (tmp_path / "h.tsv").exists() and not (tmp_path / "d.txt").exists()
     bench.reference_run(p, 6, 4, str(tmp_path), dump=True)
     assert (tmp_path / "d.txt").stat().st_size > 0
+
+
+class OracleWideCounter:
+    """count(input=...) of the resident workload for any k, answered by the
+    oracle; device_ms and the stage times are placeholders."""
+
+    def __init__(self, fq: np.ndarray):
+        self.fq = fq.tobytes()
+
+    def count(self, files=(), input=None, keep_records=True, copy=True, **kw):
+        import ktcountermemorygreedy_b200 as kc
+        k = kw["k"]
+        occ = O.extract_wide(self.fq, k)
+        uk, uc = O.count_wide(occ)
+        uc = np.minimum(uc, np.uint32(kw["count_max"])).astype(np.uint32)
+        m = uc >= kw["min_count"]
+        r = _Job()
+        r.keys, r.counts = O.sort_string_order_wide(uk[m], uc[m], k)
+        r.hist = O.histogram(uc, kw["hist_min"], kw["hist_max"])
+        r.occurrences = len(occ)
+        r.n_records_total = int(m.sum())
+        r.device_ms, r.passes = 1.0, 1
+        r.phase_ms = [0.0] * len(kc.PHASES)
+        return r
+
+
+def test_wide_leg_reports_each_k_and_checks_its_hash_sample(leg):
+    args = types.SimpleNamespace(wide=[63, 127], cpu_baseline=True)
+    import ktcountermemorygreedy_b200 as kc
+    out = bench.wide_bench(kc, args, OracleWideCounter(leg), None, leg)
+    assert set(out) == {"63", "127"}
+    for k, o in out.items():
+        assert o["k"] == int(k) and o["key_words"] == (2 if k == "63" else 4)
+        assert o["occurrences"] == 20_000 * (150 - int(k) + 1)
+        assert o["parity"] == "identical", o.get("parity_detail")
+
+
+def test_a_failing_wide_k_is_reported_not_raised(leg):
+    class Failing:
+        def count(self, **kw):
+            raise RuntimeError("no device")
+
+    import ktcountermemorygreedy_b200 as kc
+    out = bench.wide_bench(kc, types.SimpleNamespace(wide=[63], cpu_baseline=True), Failing(), None, leg)
+    assert out == {"63": {"k": 63, "failed": "no device"}}
