@@ -132,3 +132,17 @@ def test_a_failing_wide_k_is_reported_not_raised(leg):
     import ktcountermemorygreedy_b200 as kc
     out = bench.wide_bench(kc, types.SimpleNamespace(wide=[63], cpu_baseline=True), Failing(), None, leg)
     assert out == {"63": {"k": 63, "failed": "no device"}}
+
+
+def test_reference_arm_shrinks_its_sample_to_its_time_budget():
+    import json
+    import subprocess
+    if not bench.reference_programs_present() or not os.access(bench.GEN, os.X_OK):
+        pytest.skip("the reference programs or the generator are not built")
+    env = dict(os.environ, KC_REF_BUDGET_S="1", KC_REF_MEM_GB="4", CUDA_VISIBLE_DEVICES="")
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--ref-reads", "400000"], env=env, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr[-2000:]
+    line = json.loads(p.stdout.strip().splitlines()[-1])
+    assert line["cpu_baseline"]["sample"].startswith(f"first {bench.REF_ARM_MIN_READS} reads")
+    assert line["config"] == bench.workload_config(1.0, 1)
